@@ -1,0 +1,193 @@
+/*
+ * rs_b200.h - C ABI of the B200 Reservoir Splatting pass.
+ *
+ * One rs_pass is the drop-in replacement for one instance of the reference
+ * render pass class `ReservoirSplatting : RenderPass`
+ * (Source/RenderPasses/ReservoirSplatting/ReservoirSplatting.h:48-279).  The
+ * calls map onto that class as follows:
+ *
+ *   rs_create / rs_destroy      registerPlugin + constructor           ReservoirSplatting.cpp:136-175
+ *   rs_set_options              setProperties / parseProperties        ReservoirSplatting.cpp:177-261
+ *   rs_set_scene                setScene (scene + light collection)    ReservoirSplatting.cpp:378-397
+ *   rs_execute                  execute (one frame)                    ReservoirSplatting.cpp:399-509
+ *   rs_reset                    reset()                                ReservoirSplatting.cpp:813-820
+ *   rs_set_seed                 Python useFixedSeed / fixedSeed        ReservoirSplatting.cpp:142-156
+ *   rs_freeze                   Scene::isFrozen (no frame advance)     ReservoirSplatting.cpp:1672-1679
+ *   rs_get_buffer / rs_set_buffer  read / restore the pass-owned buffers (reservoirs,
+ *                               reconnection data, splat cell lists) ReservoirSplatting.h:236-278
+ *   rs_default_options          the defaults of StaticParams / ReSTIRParams / CameraParams
+ *                               ReservoirSplatting.h:124-184
+ *
+ * Threading: one host thread per rs_pass; all device work of a call is issued
+ * on the caller's CUDA stream (passed as void*).  No call throws; every call
+ * returns an rs_status and rs_last_error_string() describes the last failure
+ * on the calling thread.
+ */
+#ifndef RS_B200_H
+#define RS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(_WIN32)
+#define RS_API __declspec(dllexport)
+#else
+#define RS_API __attribute__((visibility("default")))
+#endif
+
+typedef enum rs_status {
+    RS_OK = 0,
+    RS_INVALID_ARG = 1,   /* bad pointer, size or option value */
+    RS_OOM = 2,           /* device allocation failed */
+    RS_CUDA_ERROR = 3,    /* a CUDA runtime call failed */
+    RS_DEVICE_FAULT = 4,  /* a kernel set the device status word (iteration cap hit) */
+    RS_NOT_READY = 5      /* no scene set */
+} rs_status;
+
+/* TemporalReuse (ShiftOptions.slang:34-40) */
+enum { RS_GATHER_ONLY = 0, RS_SCATTER_ONLY = 1, RS_SCATTER_BACKUP = 2, RS_MULTI_SCATTER = 3 };
+/* GatherMechanism (ShiftOptions.slang:62-67) */
+enum { RS_GATHER_FAST = 0, RS_GATHER_CLAMPED = 1, RS_GATHER_ROBUST = 2 };
+/* ScatterBackupMIS (ShiftOptions.slang:49-53) */
+enum { RS_MIS_BALANCE = 0, RS_MIS_PAIRWISE = 1 };
+/* MISHeuristic (Params.slang:48-53); PowerExp is not supported */
+enum { RS_MIS_HEURISTIC_BALANCE = 0, RS_MIS_HEURISTIC_POWER_TWO = 1 };
+/* sampleGenerator: SAMPLE_GENERATOR_TINY_UNIFORM = 0 (reference default); 2 = PCG32 */
+enum { RS_SG_TINY_UNIFORM = 0, RS_SG_PCG32 = 2 };
+
+/* Property keys of ReservoirSplatting.cpp:99-131 plus the UI-only knobs of
+ * ReservoirSplatting.h:159-184.  Field names follow the property names. */
+typedef struct rs_options {
+    uint32_t samplesPerPixel;            /* 1..16 */
+    uint32_t maxSurfaceBounces;          /* <= 254 */
+    uint32_t maxDiffuseBounces;
+    uint32_t maxSpecularBounces;
+    uint32_t maxTransmissionBounces;
+    uint32_t sampleGenerator;            /* RS_SG_* */
+    uint32_t useFixedSeed;
+    uint32_t fixedSeed;
+    uint32_t useRussianRoulette;
+    uint32_t misHeuristic;               /* RS_MIS_HEURISTIC_* */
+    float misPowerExponent;
+    uint32_t disableCaustics;
+    float specularRoughnessThreshold;
+    uint32_t enableTemporalResampling;
+    uint32_t enableSpatialResampling;
+    uint32_t temporalReuse;              /* RS_GATHER_ONLY .. RS_MULTI_SCATTER */
+    uint32_t scatterBackupMISOption;     /* RS_MIS_BALANCE / RS_MIS_PAIRWISE */
+    uint32_t gatherOption;               /* RS_GATHER_FAST / CLAMPED / ROBUST */
+    uint32_t numTimePartitions;          /* 1..8 */
+    uint32_t useConfidenceWeightsTemporally;
+    uint32_t numSpatialIterations;
+    float spatialGatherRadius;
+    uint32_t neighborCount;
+    uint32_t useConfidenceWeightsSpatially;
+    float artificialFrameTime;           /* seconds between two frames' cameras */
+    uint32_t frameWidth;                 /* outputSize, <= 4096 */
+    uint32_t frameHeight;                /* <= 4096 */
+} rs_options;
+
+/* StandardMaterial metal-rough parameters; 64 bytes.  flags bit 0 = double sided. */
+typedef struct rs_material {
+    float baseColor[3];
+    float roughness;
+    float emissive[3];                   /* radiance, emissive factor included */
+    float metallic;
+    float ior;
+    uint32_t flags;
+    float reserved[6];
+} rs_material;
+
+/* Flattened world-space triangle soup (the ray-traced geometry of a Falcor scene). */
+typedef struct rs_scene_desc {
+    uint32_t numTriangles;
+    const float* positions;              /* host, 9 floats per triangle (p0, p1, p2) */
+    const uint32_t* materialIds;         /* host, one per triangle */
+    uint32_t numMaterials;
+    const rs_material* materials;        /* host */
+} rs_scene_desc;
+
+/* Camera of the current frame (CameraData.slang:35-72 subset). */
+typedef struct rs_camera {
+    float position[3];
+    float target[3];
+    float up[3];
+    float focalLength;                   /* mm */
+    float frameHeight;                   /* mm */
+    float aspectRatio;
+    float focalDistance;
+    float apertureRadius;
+    float shutterSpeed;                  /* seconds */
+    float nearZ;
+    float farZ;
+} rs_camera;
+
+/* Per-frame inputs/outputs (the reflect() channels, ReservoirSplatting.cpp:64-96). */
+typedef struct rs_frame_desc {
+    rs_camera camera;
+    const float* mvec;                   /* optional device float2[W*H]; NULL: computed by the pass */
+    const uint32_t* vbuffer;             /* optional device uint4[W*H] packed hits; NULL: computed */
+    float* color;                        /* device float4[W*H] output (may be NULL if colorHost set) */
+    float* colorHost;                    /* optional host float4[W*H]; copied back and synchronised */
+    uint32_t sceneShouldReset;           /* Scene::shouldReset(): restart the temporal history */
+} rs_frame_desc;
+
+/* Buffers readable with rs_get_buffer (canonical host layouts):
+ *   reservoirs      8 floats / pixel: integrand.xyz, totalWeight, subPixel.xy, confidence, 0
+ *   reconnection    28 words / pixel (layout in rs_get_buffer's documentation)
+ *   cellCounters    uint32 / pixel        cellOffsets  uint32 / pixel
+ *   sortedSplats    uint32 source-pixel index per splat, cells in pixel order, sources ascending
+ *   floatingCoords  float2 / pixel        mvec float2 / pixel      vbuffer uint4 / pixel
+ *   splatTargets    uint32 / source pixel: destination cell or 0xffffffff */
+typedef enum rs_buffer_id {
+    RS_BUF_CURR_RESERVOIRS = 0,
+    RS_BUF_CURR_RECONNECTION = 1,
+    RS_BUF_PREV_RESERVOIRS = 2,
+    RS_BUF_PREV_RECONNECTION = 3,
+    RS_BUF_CELL_COUNTERS = 4,
+    RS_BUF_CELL_OFFSETS = 5,
+    RS_BUF_SORTED_SPLATS = 6,
+    RS_BUF_FLOATING_COORDS = 7,
+    RS_BUF_MVEC = 8,
+    RS_BUF_VBUFFER = 9,
+    RS_BUF_SPLAT_TARGETS = 10,
+    RS_BUF_CANDIDATE_RESERVOIRS = 11,
+    RS_BUF_CANDIDATE_RECONNECTION = 12,
+    RS_BUF_BACKUP_RESERVOIRS = 13,
+    RS_BUF_BACKUP_RECONNECTION = 14
+} rs_buffer_id;
+
+typedef struct rs_pass rs_pass;
+
+RS_API void rs_default_options(rs_options* opts);
+RS_API rs_status rs_create(const rs_options* opts, rs_pass** out);
+RS_API rs_status rs_destroy(rs_pass* pass);
+RS_API rs_status rs_set_options(rs_pass* pass, const rs_options* opts);
+RS_API rs_status rs_set_scene(rs_pass* pass, const rs_scene_desc* scene);
+RS_API rs_status rs_execute(rs_pass* pass, const rs_frame_desc* frame, void* cudaStream);
+RS_API rs_status rs_reset(rs_pass* pass);
+RS_API rs_status rs_set_seed(rs_pass* pass, uint32_t useFixedSeed, uint32_t fixedSeed);
+RS_API rs_status rs_freeze(rs_pass* pass, uint32_t frozen);
+/* Copies a pass buffer to host memory (synchronises the pass's last stream).
+ * *bytes is the destination capacity in, and the number of bytes written (or
+ * needed when dst is NULL) out. */
+RS_API rs_status rs_get_buffer(rs_pass* pass, rs_buffer_id id, void* dst, size_t* bytes);
+/* Restores a reservoir / reconnection buffer from host memory (checkpoint restore). */
+RS_API rs_status rs_set_buffer(rs_pass* pass, rs_buffer_id id, const void* src, size_t bytes);
+/* Kernel timing of the last rs_execute: per-stage device milliseconds (CUDA events)
+ * when timing is enabled with rs_enable_stage_timing.  Names are NUL-separated. */
+RS_API rs_status rs_enable_stage_timing(rs_pass* pass, uint32_t enable);
+RS_API rs_status rs_get_stage_times(rs_pass* pass, float* ms, uint32_t* count, char* names, size_t namesBytes);
+/* Number of kernel launches issued by the last rs_execute. */
+RS_API uint32_t rs_last_launch_count(rs_pass* pass);
+RS_API const char* rs_last_error_string(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RS_B200_H */

@@ -1,0 +1,141 @@
+"""ctypes wrapper of the CPU oracle (oracle/rs_oracle.cpp).
+
+TEST INFRASTRUCTURE: used by tests/, the smoke check and the bench's CPU-baseline
+leg only.  It mirrors the buffer names and layouts of the CUDA pass so a parity
+test compares the same arrays.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import importlib.util
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+import numpy as np
+
+ORACLE_DIR = Path(__file__).resolve().parent
+ORACLE_SO = ORACLE_DIR / "_build" / "librs_oracle.so"
+PKG_DIR = ORACLE_DIR.parent / "reservoir-splatting_b200"
+
+
+def _abi():
+    name = "reservoir_splatting_b200.abi"
+    if name in sys.modules:
+        return sys.modules[name]
+    if "reservoir_splatting_b200" not in sys.modules:
+        spec = importlib.util.spec_from_file_location("reservoir_splatting_b200", PKG_DIR / "__init__.py",
+                                                      submodule_search_locations=[str(PKG_DIR)])
+        mod = importlib.util.module_from_spec(spec)
+        sys.modules["reservoir_splatting_b200"] = mod
+        spec.loader.exec_module(mod)
+    return sys.modules[name]
+
+
+def build(force: bool = False) -> Path:
+    """Compiles the oracle with the host compiler (no contraction, IEEE float)."""
+    src = ORACLE_DIR / "rs_oracle.cpp"
+    deps = [src] + sorted((PKG_DIR / "csrc" / "core").glob("*.h")) + [ORACLE_DIR.parent / "include" / "rs_b200.h"]
+    if not force and ORACLE_SO.exists() and ORACLE_SO.stat().st_mtime >= max(d.stat().st_mtime for d in deps):
+        return ORACLE_SO
+    ORACLE_SO.parent.mkdir(exist_ok=True)
+    cmd = ["g++", "-std=c++17", "-O2", "-fopenmp", "-ffp-contract=off", "-fno-fast-math", "-fPIC", "-shared",
+           "-o", str(ORACLE_SO), str(src)]
+    subprocess.run(cmd, check=True)
+    return ORACLE_SO
+
+
+_lib = None
+
+
+def load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    build()
+    lib = C.CDLL(str(ORACLE_SO))
+    a = _abi()
+    lib.ro_create.argtypes = [C.POINTER(a.RsOptions)]
+    lib.ro_create.restype = C.c_void_p
+    lib.ro_destroy.argtypes = [C.c_void_p]
+    lib.ro_set_threads.argtypes = [C.c_int]
+    lib.ro_set_threads.restype = C.c_int
+    lib.ro_set_scene.argtypes = [C.c_void_p, C.POINTER(a.RsSceneDesc)]
+    lib.ro_execute.argtypes = [C.c_void_p, C.POINTER(a.RsFrameDesc), C.c_void_p, C.c_void_p]
+    lib.ro_freeze.argtypes = [C.c_void_p, C.c_int]
+    lib.ro_reset.argtypes = [C.c_void_p]
+    lib.ro_get_buffer.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]
+    lib.ro_get_buffer.restype = C.c_long
+    lib.ro_set_buffer.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]
+    lib.ro_frame_count.argtypes = [C.c_void_p]
+    lib.ro_frame_count.restype = C.c_uint32
+    _lib = lib
+    return lib
+
+
+def set_threads(n: int) -> int:
+    return load().ro_set_threads(n)
+
+
+class OraclePass:
+    """CPU restatement of one ReservoirSplatting pass instance."""
+
+    def __init__(self, props: dict | None = None, width: int = 256, height: int = 256, options=None):
+        self._lib = load()
+        a = _abi()
+        self._abi = a
+        self.options = options if options is not None else a.options_from_properties(props, width, height)
+        self.width, self.height = self.options.frameWidth, self.options.frameHeight
+        self._h = self._lib.ro_create(C.byref(self.options))
+
+    def __del__(self):
+        try:
+            if self._h:
+                self._lib.ro_destroy(self._h)
+                self._h = None
+        except Exception:
+            pass
+
+    def set_scene(self, scene):
+        desc, keep = self._abi.scene_struct(scene)
+        st = self._lib.ro_set_scene(self._h, C.byref(desc))
+        if st != 0:
+            raise RuntimeError(f"oracle set_scene failed: {st}")
+
+    def execute(self, camera, mvec: np.ndarray | None = None, should_reset: bool = False) -> np.ndarray:
+        f = self._abi.RsFrameDesc()
+        f.camera = self._abi.camera_struct(camera)
+        f.sceneShouldReset = 1 if should_reset else 0
+        out = np.empty((self.height, self.width, 4), np.float32)
+        mp = None
+        if mvec is not None:
+            mvec = np.ascontiguousarray(mvec, np.float32)
+            mp = mvec.ctypes.data
+        st = self._lib.ro_execute(self._h, C.byref(f), mp, out.ctypes.data)
+        if st != 0:
+            raise RuntimeError(f"oracle execute failed: {st}")
+        return out
+
+    def freeze(self, frozen: bool = True):
+        self._lib.ro_freeze(self._h, 1 if frozen else 0)
+
+    def reset(self):
+        self._lib.ro_reset(self._h)
+
+    def get_buffer(self, name: str) -> np.ndarray:
+        bid = self._abi.BUF[name]
+        n = self._lib.ro_get_buffer(self._h, bid, None, 0)
+        if n < 0:
+            raise KeyError(name)
+        dtype, width = self._abi.BUFFER_LAYOUT[name]
+        out = np.empty(n // 4, dtype)
+        if n:
+            self._lib.ro_get_buffer(self._h, bid, out.ctypes.data, n)
+        return out.reshape(-1, width) if width > 1 else out
+
+    def set_buffer(self, name: str, data: np.ndarray):
+        data = np.ascontiguousarray(data)
+        st = self._lib.ro_set_buffer(self._h, self._abi.BUF[name], data.ctypes.data, data.nbytes)
+        if st != 0:
+            raise RuntimeError(f"oracle set_buffer failed: {st}")

@@ -1,0 +1,190 @@
+"""B200 Reservoir Splatting: Python host mirror of the reference render pass.
+
+`ReservoirSplatting` follows the Python surface of the reference pass
+(``createPass("ReservoirSplatting", props)``, ``reset()``, ``useFixedSeed``,
+``fixedSeed``; ReservoirSplatting.cpp:142-156, scripts/ReservoirSplatting.py)
+and drives the CUDA library ``lib/librs_b200.so`` through its C ABI
+(include/rs_b200.h).  There is no CPU fallback: without the built library the
+constructor raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+from . import abi
+from .abi import BUF, BUFFER_LAYOUT
+
+PACKAGE_DIR = Path(__file__).resolve().parent
+LIB_PATH = PACKAGE_DIR / "lib" / "librs_b200.so"
+
+_lib = None
+
+
+class RsError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{abi.STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+def load_library():
+    """Loads the CUDA library (raises when it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError(f"CUDA library missing: {LIB_PATH} (run __graft_entry__.build())")
+    lib = C.CDLL(str(LIB_PATH))
+    lib.rs_default_options.argtypes = [C.POINTER(abi.RsOptions)]
+    lib.rs_default_options.restype = None
+    lib.rs_create.argtypes = [C.POINTER(abi.RsOptions), C.POINTER(C.c_void_p)]
+    lib.rs_destroy.argtypes = [C.c_void_p]
+    lib.rs_set_options.argtypes = [C.c_void_p, C.POINTER(abi.RsOptions)]
+    lib.rs_set_scene.argtypes = [C.c_void_p, C.POINTER(abi.RsSceneDesc)]
+    lib.rs_execute.argtypes = [C.c_void_p, C.POINTER(abi.RsFrameDesc), C.c_void_p]
+    lib.rs_reset.argtypes = [C.c_void_p]
+    lib.rs_set_seed.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32]
+    lib.rs_freeze.argtypes = [C.c_void_p, C.c_uint32]
+    lib.rs_get_buffer.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_size_t)]
+    lib.rs_set_buffer.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]
+    lib.rs_enable_stage_timing.argtypes = [C.c_void_p, C.c_uint32]
+    lib.rs_get_stage_times.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_uint32), C.c_char_p, C.c_size_t]
+    lib.rs_last_launch_count.argtypes = [C.c_void_p]
+    lib.rs_last_launch_count.restype = C.c_uint32
+    lib.rs_last_error_string.restype = C.c_char_p
+    lib.rs_debug_keep_candidates.argtypes = [C.c_void_p, C.c_uint32]
+    for name in ("rs_create", "rs_destroy", "rs_set_options", "rs_set_scene", "rs_execute", "rs_reset", "rs_set_seed",
+                 "rs_freeze", "rs_get_buffer", "rs_set_buffer", "rs_enable_stage_timing", "rs_get_stage_times",
+                 "rs_debug_keep_candidates"):
+        getattr(lib, name).restype = C.c_int
+    _lib = lib
+    return lib
+
+
+def _check(status: int):
+    if status != abi.RS_OK:
+        raise RsError(status, load_library().rs_last_error_string().decode())
+
+
+class ReservoirSplatting:
+    """One instance of the pass (ReservoirSplatting.h:48-279) on the current CUDA device."""
+
+    def __init__(self, props: dict | None = None, width: int = 1920, height: int = 1080):
+        lib = load_library()
+        self._lib = lib
+        self.options = abi.options_from_properties(props, width, height)
+        h = C.c_void_p()
+        _check(lib.rs_create(C.byref(self.options), C.byref(h)))
+        self._h = h
+        self.width, self.height = self.options.frameWidth, self.options.frameHeight
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.rs_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- reference-facing API
+    def set_properties(self, props: dict):
+        self.options = abi.options_from_properties(props, self.width, self.height)
+        _check(self._lib.rs_set_options(self._h, C.byref(self.options)))
+        self.width, self.height = self.options.frameWidth, self.options.frameHeight
+
+    def set_scene(self, scene):
+        desc, keep = abi.scene_struct(scene)
+        _check(self._lib.rs_set_scene(self._h, C.byref(desc)))
+        del keep
+
+    def reset(self):
+        _check(self._lib.rs_reset(self._h))
+
+    @property
+    def useFixedSeed(self) -> bool:
+        return bool(self.options.useFixedSeed)
+
+    @useFixedSeed.setter
+    def useFixedSeed(self, value: bool):
+        self.options.useFixedSeed = 1 if value else 0
+        _check(self._lib.rs_set_seed(self._h, self.options.useFixedSeed, self.options.fixedSeed))
+
+    @property
+    def fixedSeed(self) -> int:
+        return int(self.options.fixedSeed)
+
+    @fixedSeed.setter
+    def fixedSeed(self, value: int):
+        self.options.fixedSeed = int(value)
+        _check(self._lib.rs_set_seed(self._h, self.options.useFixedSeed, self.options.fixedSeed))
+
+    def freeze(self, frozen: bool = True):
+        _check(self._lib.rs_freeze(self._h, 1 if frozen else 0))
+
+    def execute(self, camera, color_ptr: int | None = None, color_host: np.ndarray | None = None, stream: int = 0,
+                mvec_ptr: int | None = None, should_reset: bool = False):
+        """Renders one frame.  `color_ptr` is a device float4[W*H]; or pass `color_host` (float32 [H, W, 4])."""
+        f = abi.RsFrameDesc()
+        f.camera = abi.camera_struct(camera)
+        f.mvec = mvec_ptr or None
+        f.vbuffer = None
+        f.color = color_ptr or None
+        if color_host is not None:
+            assert color_host.dtype == np.float32 and color_host.flags.c_contiguous and color_host.size == 4 * self.width * self.height
+            f.colorHost = color_host.ctypes.data
+        else:
+            f.colorHost = None
+        f.sceneShouldReset = 1 if should_reset else 0
+        _check(self._lib.rs_execute(self._h, C.byref(f), C.c_void_p(stream)))
+
+    def render(self, camera, **kw) -> np.ndarray:
+        out = np.empty((self.height, self.width, 4), np.float32)
+        self.execute(camera, color_host=out, **kw)
+        return out
+
+    # ---- buffers (parity / checkpoint)
+    def get_buffer(self, name: str) -> np.ndarray:
+        n = C.c_size_t(0)
+        _check(self._lib.rs_get_buffer(self._h, BUF[name], None, C.byref(n)))
+        dtype, width = BUFFER_LAYOUT[name]
+        out = np.empty(n.value // 4, dtype)
+        if n.value:
+            _check(self._lib.rs_get_buffer(self._h, BUF[name], out.ctypes.data, C.byref(n)))
+        return out.reshape(-1, width) if width > 1 else out
+
+    def set_buffer(self, name: str, data: np.ndarray):
+        data = np.ascontiguousarray(data)
+        _check(self._lib.rs_set_buffer(self._h, BUF[name], data.ctypes.data, data.nbytes))
+
+    def keep_candidates(self, keep: bool = True):
+        _check(self._lib.rs_debug_keep_candidates(self._h, 1 if keep else 0))
+
+    def enable_stage_timing(self, enable: bool = True):
+        _check(self._lib.rs_enable_stage_timing(self._h, 1 if enable else 0))
+
+    def stage_times(self) -> dict:
+        cnt = C.c_uint32(64)
+        ms = (C.c_float * 64)()
+        names = C.create_string_buffer(4096)
+        _check(self._lib.rs_get_stage_times(self._h, ms, C.byref(cnt), names, 4096))
+        labels = names.raw.split(b"\0")[: cnt.value]
+        out = {}
+        for k, v in zip(labels, ms[: cnt.value]):
+            out[k.decode()] = out.get(k.decode(), 0.0) + float(v)
+        return out
+
+    def last_launch_count(self) -> int:
+        return int(self._lib.rs_last_launch_count(self._h))
+
+
+def createPass(name: str, props: dict | None = None, width: int = 1920, height: int = 1080) -> ReservoirSplatting:
+    """Falcor-style factory: createPass("ReservoirSplatting", {...})."""
+    if name != "ReservoirSplatting":
+        raise ValueError(f"unknown pass {name!r}")
+    return ReservoirSplatting(props, width, height)

@@ -1,0 +1,167 @@
+"""ctypes mirror of include/rs_b200.h and the property parsing of the reference pass.
+
+`options_from_properties` accepts the property dictionary a Falcor render-graph
+script passes to ``createPass("ReservoirSplatting", {...})``
+(scripts/ReservoirSplatting.py:13-21, keys of ReservoirSplatting.cpp:99-131),
+including the enum values by name ("ScatterBackup", "Clamped", "Pairwise", ...).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+RS_OK, RS_INVALID_ARG, RS_OOM, RS_CUDA_ERROR, RS_DEVICE_FAULT, RS_NOT_READY = range(6)
+STATUS_NAMES = {0: "RS_OK", 1: "RS_INVALID_ARG", 2: "RS_OOM", 3: "RS_CUDA_ERROR", 4: "RS_DEVICE_FAULT", 5: "RS_NOT_READY"}
+
+TEMPORAL_REUSE = {"GatherOnly": 0, "ScatterOnly": 1, "ScatterBackup": 2, "MultiScatter": 3}
+GATHER_MECHANISM = {"Fast": 0, "Clamped": 1, "Robust": 2}
+SCATTER_BACKUP_MIS = {"Balance": 0, "Pairwise": 1}
+MIS_HEURISTIC = {"Balance": 0, "PowerTwo": 1}
+SAMPLE_GENERATOR = {"TinyUniform": 0, "PCG32": 2}
+
+BUF = {
+    "curr_reservoirs": 0, "curr_reconnection": 1, "prev_reservoirs": 2, "prev_reconnection": 3,
+    "cell_counters": 4, "cell_offsets": 5, "sorted_splats": 6, "floating_coords": 7, "mvec": 8, "vbuffer": 9,
+    "splat_targets": 10, "candidate_reservoirs": 11, "candidate_reconnection": 12,
+    "backup_reservoirs": 13, "backup_reconnection": 14,
+}
+
+
+class RsOptions(C.Structure):
+    _fields_ = [
+        ("samplesPerPixel", C.c_uint32), ("maxSurfaceBounces", C.c_uint32), ("maxDiffuseBounces", C.c_uint32),
+        ("maxSpecularBounces", C.c_uint32), ("maxTransmissionBounces", C.c_uint32), ("sampleGenerator", C.c_uint32),
+        ("useFixedSeed", C.c_uint32), ("fixedSeed", C.c_uint32), ("useRussianRoulette", C.c_uint32),
+        ("misHeuristic", C.c_uint32), ("misPowerExponent", C.c_float), ("disableCaustics", C.c_uint32),
+        ("specularRoughnessThreshold", C.c_float), ("enableTemporalResampling", C.c_uint32),
+        ("enableSpatialResampling", C.c_uint32), ("temporalReuse", C.c_uint32), ("scatterBackupMISOption", C.c_uint32),
+        ("gatherOption", C.c_uint32), ("numTimePartitions", C.c_uint32), ("useConfidenceWeightsTemporally", C.c_uint32),
+        ("numSpatialIterations", C.c_uint32), ("spatialGatherRadius", C.c_float), ("neighborCount", C.c_uint32),
+        ("useConfidenceWeightsSpatially", C.c_uint32), ("artificialFrameTime", C.c_float), ("frameWidth", C.c_uint32),
+        ("frameHeight", C.c_uint32),
+    ]
+
+
+class RsSceneDesc(C.Structure):
+    _fields_ = [("numTriangles", C.c_uint32), ("positions", C.c_void_p), ("materialIds", C.c_void_p),
+                ("numMaterials", C.c_uint32), ("materials", C.c_void_p)]
+
+
+class RsCamera(C.Structure):
+    _fields_ = [("position", C.c_float * 3), ("target", C.c_float * 3), ("up", C.c_float * 3),
+                ("focalLength", C.c_float), ("frameHeight", C.c_float), ("aspectRatio", C.c_float),
+                ("focalDistance", C.c_float), ("apertureRadius", C.c_float), ("shutterSpeed", C.c_float),
+                ("nearZ", C.c_float), ("farZ", C.c_float)]
+
+
+class RsFrameDesc(C.Structure):
+    _fields_ = [("camera", RsCamera), ("mvec", C.c_void_p), ("vbuffer", C.c_void_p), ("color", C.c_void_p),
+                ("colorHost", C.c_void_p), ("sceneShouldReset", C.c_uint32)]
+
+
+def default_options(width: int = 1920, height: int = 1080) -> RsOptions:
+    """ReservoirSplatting.h:124-184 defaults (the C library's rs_default_options, restated for CPU-only use)."""
+    o = RsOptions()
+    o.samplesPerPixel = 1
+    o.maxSurfaceBounces = o.maxDiffuseBounces = o.maxSpecularBounces = o.maxTransmissionBounces = 9
+    o.sampleGenerator = 0
+    o.useFixedSeed = 0
+    o.fixedSeed = 1
+    o.useRussianRoulette = 1
+    o.misHeuristic = 0
+    o.misPowerExponent = 2.0
+    o.disableCaustics = 0
+    o.specularRoughnessThreshold = 0.25
+    o.enableTemporalResampling = 1
+    o.enableSpatialResampling = 1
+    o.temporalReuse = TEMPORAL_REUSE["GatherOnly"]
+    o.scatterBackupMISOption = 0
+    o.gatherOption = GATHER_MECHANISM["Fast"]
+    o.numTimePartitions = 2
+    o.useConfidenceWeightsTemporally = 1
+    o.numSpatialIterations = 1
+    o.spatialGatherRadius = 30.0
+    o.neighborCount = 1
+    o.useConfidenceWeightsSpatially = 1
+    o.artificialFrameTime = 1.0 / 60.0
+    o.frameWidth = width
+    o.frameHeight = height
+    return o
+
+
+_ENUMS = {"temporalReuse": TEMPORAL_REUSE, "gatherOption": GATHER_MECHANISM, "scatterBackupMISOption": SCATTER_BACKUP_MIS,
+          "hybridMISOption": SCATTER_BACKUP_MIS, "misHeuristic": MIS_HEURISTIC, "sampleGenerator": SAMPLE_GENERATOR}
+_ALIASES = {"hybridMISOption": "scatterBackupMISOption"}
+
+
+def options_from_properties(props: dict | None, width: int, height: int) -> RsOptions:
+    """parseProperties (ReservoirSplatting.cpp:192-261) for a createPass() property dict."""
+    o = default_options(width, height)
+    props = dict(props or {})
+    names = {f for f, _ in RsOptions._fields_}
+    for key, value in props.items():
+        field = _ALIASES.get(key, key)
+        if key in _ENUMS and isinstance(value, str):
+            if value not in _ENUMS[key]:
+                raise ValueError(f"unknown value {value!r} for property {key!r}")
+            value = _ENUMS[key][value]
+        if key == "fixedSeed":
+            o.fixedSeed = int(value)
+            o.useFixedSeed = 1
+            continue
+        if key == "outputSize":
+            o.frameWidth, o.frameHeight = int(value[0]), int(value[1])
+            continue
+        if field not in names:
+            raise KeyError(f"Unknown property '{key}' in ReservoirSplatting properties.")
+        setattr(o, field, type(getattr(o, field))(value))
+    # maxSurfaceBounces initialises the per-type limits that are not given explicitly (:236-247)
+    if "maxSurfaceBounces" in props:
+        for k in ("maxDiffuseBounces", "maxSpecularBounces", "maxTransmissionBounces"):
+            if k not in props:
+                setattr(o, k, o.maxSurfaceBounces)
+    else:
+        o.maxSurfaceBounces = max(o.maxDiffuseBounces, o.maxSpecularBounces, o.maxTransmissionBounces)
+    o.maxSurfaceBounces = max(o.maxSurfaceBounces, o.maxDiffuseBounces, o.maxSpecularBounces, o.maxTransmissionBounces)
+    return o
+
+
+def camera_struct(cam) -> RsCamera:
+    c = RsCamera()
+    c.position[:] = [float(v) for v in cam.position]
+    c.target[:] = [float(v) for v in cam.target]
+    c.up[:] = [float(v) for v in cam.up]
+    c.focalLength = cam.focal_length
+    c.frameHeight = cam.frame_height
+    c.aspectRatio = cam.aspect_ratio
+    c.focalDistance = cam.focal_distance
+    c.apertureRadius = cam.aperture_radius
+    c.shutterSpeed = cam.shutter_speed
+    c.nearZ = cam.near_z
+    c.farZ = cam.far_z
+    return c
+
+
+def scene_struct(scene) -> tuple[RsSceneDesc, tuple]:
+    """Returns the descriptor and the arrays it points into (keep them alive during the call)."""
+    pos = np.ascontiguousarray(scene.positions, np.float32)
+    mid = np.ascontiguousarray(scene.material_ids, np.uint32)
+    mats = np.ascontiguousarray(scene.materials, np.float32)
+    d = RsSceneDesc()
+    d.numTriangles = pos.shape[0]
+    d.positions = pos.ctypes.data
+    d.materialIds = mid.ctypes.data
+    d.numMaterials = mats.shape[0]
+    d.materials = mats.ctypes.data
+    return d, (pos, mid, mats)
+
+
+BUFFER_LAYOUT = {
+    "curr_reservoirs": (np.float32, 8), "prev_reservoirs": (np.float32, 8), "candidate_reservoirs": (np.float32, 8),
+    "backup_reservoirs": (np.float32, 8),
+    "curr_reconnection": (np.uint32, 28), "prev_reconnection": (np.uint32, 28), "candidate_reconnection": (np.uint32, 28),
+    "backup_reconnection": (np.uint32, 28),
+    "cell_counters": (np.uint32, 1), "cell_offsets": (np.uint32, 1), "sorted_splats": (np.uint32, 1),
+    "splat_targets": (np.uint32, 1), "floating_coords": (np.float32, 2), "mvec": (np.float32, 2), "vbuffer": (np.uint32, 4),
+}

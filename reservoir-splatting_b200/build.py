@@ -1,0 +1,47 @@
+"""Builds the sm_100a CUDA library lib/librs_b200.so with nvcc (in-tree, no JIT cache).
+
+Flags that the parity contract depends on: -fmad=false (no contraction on the
+device), -prec-div=true -prec-sqrt=true (IEEE division and square root) and
+-ffp-contract=off for the host compiler, so host and device round identically.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+CSRC = PKG / "csrc"
+LIB = PKG / "lib" / "librs_b200.so"
+SOURCES = ["kernels.cu", "pass.cu", "bvh_build.cu"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-fmad=false", "-prec-div=true", "-prec-sqrt=true",
+         "-Xcompiler", "-fPIC,-ffp-contract=off,-fvisibility=hidden", "-shared"]
+
+
+def nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and Path(cand).exists():
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def _deps():
+    return [CSRC / s for s in SOURCES] + sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.h")) + \
+        sorted((CSRC / "core").glob("*.h")) + [PKG.parent / "include" / "rs_b200.h"]
+
+
+def build(force: bool = False, verbose: bool = False) -> Path:
+    if not force and LIB.exists() and LIB.stat().st_mtime >= max(p.stat().st_mtime for p in _deps()):
+        return LIB
+    LIB.parent.mkdir(exist_ok=True)
+    cmd = [nvcc()] + ARCH + FLAGS + ["-o", str(LIB)] + [str(CSRC / s) for s in SOURCES]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True, cwd=str(CSRC))
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(force=True, verbose=True))

@@ -1,0 +1,202 @@
+// Scalar float semantics shared by the sm_100a kernels and the host code.
+//
+// Every function here is built only from IEEE-754 binary32 operations that are
+// correctly rounded on both x86-64 (SSE, -ffp-contract=off) and sm_100a
+// (-fmad=false -prec-div=true -prec-sqrt=true): + - * / sqrtf floorf rintf
+// fabsf and comparisons.  The transcendental functions are written from their
+// Taylor series after a Cody-Waite range reduction (constants derived from pi
+// in this file's comments), so a host build and a device build of the same
+// expression produce the same bits.  They are accurate to a few ulp over the
+// argument ranges the renderer uses (|x| < 24 for sin/cos).
+//
+// Reference correspondence: these replace the Slang intrinsics sin/cos/acos/
+// atan/tan/pow used by Utils/Math/MathHelpers.slang:269-277, 323-355,
+// Utils/Math/Quaternion.slang:54-59, RenderPasses/ReservoirSplatting/
+// CameraManager.slang:50-82 and Rendering/Materials/Fresnel.slang:42-51.
+#pragma once
+#include <stdint.h>
+#include <string.h>
+#include <math.h>
+
+#if defined(__CUDACC__)
+#define RS_HD __host__ __device__ __forceinline__
+#define RS_HDI __host__ __device__ inline
+#else
+#define RS_HD inline
+#define RS_HDI inline
+#endif
+
+namespace rs {
+
+// pi and friends rounded to binary32 (bit patterns in the comments).
+constexpr float kPi = 3.14159274101257324f;      // 0x40490fdb
+constexpr float k1OverPi = 0.318309873342514038f; // 0x3ea2f983
+constexpr float k2Pi = 6.28318548202514648f;     // 0x40c90fdb
+constexpr float kPiOver2 = 1.57079637050628662f; // 0x3fc90fdb
+constexpr float kPiOver4 = 0.785398185253143311f; // 0x3f490fdb
+constexpr float kPiOver6 = 0.523598790168762207f; // 0x3f060a92
+constexpr float kSqrt3 = 1.73205077648162842f;   // 0x3fddb3d7
+constexpr float kFltMin = 1.17549435e-38f;       // FLT_MIN
+constexpr float kRayTMax = 1e30f;                 // PathStates.slang:40
+
+RS_HD uint32_t f2u(float f) { uint32_t u; memcpy(&u, &f, 4); return u; }
+RS_HD float u2f(uint32_t u) { float f; memcpy(&f, &u, 4); return f; }
+RS_HD int32_t f2i_bits(float f) { int32_t u; memcpy(&u, &f, 4); return u; }
+RS_HD float i2f_bits(int32_t u) { float f; memcpy(&f, &u, 4); return f; }
+
+RS_HD bool f_isnan(float x) { return x != x; }
+RS_HD float f_min(float a, float b) { return (b < a) ? b : a; }  // HLSL min with non-NaN args
+RS_HD float f_max(float a, float b) { return (a < b) ? b : a; }
+RS_HD float f_abs(float x) { return fabsf(x); }
+RS_HD float f_sqrt(float x) { return sqrtf(x); }
+RS_HD float f_floor(float x) { return floorf(x); }
+RS_HD float f_round(float x) { return rintf(x); }  // HLSL round(): nearest, ties to even
+RS_HD float f_saturate(float x) { return f_min(f_max(x, 0.f), 1.f); }
+RS_HD float f_clamp(float x, float lo, float hi) { return f_min(f_max(x, lo), hi); }
+RS_HD float f_lerp(float a, float b, float t) { return a + t * (b - a); }
+RS_HD float f_sign(float x) { return x > 0.f ? 1.f : (x < 0.f ? -1.f : 0.f); }
+
+// Range reduction x = k * pi/2 + r with pi/2 = P1 + P2 + P3, P1 holding the
+// top 20 significand bits of pi/2 so that k * P1 is exact for |k| < 16.
+// P1 = 0x3fc90fd0, P2 = 0x35aa2217, P3 = 0xa967b967 (pi/2 - P1 - P2).
+RS_HD float reduce_half_pi(float x, int& quadrant)
+{
+    const float kTwoOverPi = 0.636619746685028076f; // 0x3f22f983
+    const float P1 = 1.57079505920410156f;
+    const float P2 = 1.26759084650984730e-06f;
+    const float P3 = -5.14531146367843560e-14f;
+    float k = rintf(x * kTwoOverPi);
+    quadrant = (int)k;
+    float r = x - k * P1;
+    r = r - k * P2;
+    r = r - k * P3;
+    return r;
+}
+
+// Taylor polynomials on |r| <= pi/4 (coefficients +-1/n!).
+RS_HD float sin_poly(float r)
+{
+    float r2 = r * r;
+    float p = -2.50521083854417188e-08f;             // -1/11!
+    p = p * r2 + 2.75573192239858907e-06f;          //  1/9!
+    p = p * r2 + -1.98412698412698413e-04f;         // -1/7!
+    p = p * r2 + 8.33333333333333333e-03f;          //  1/5!
+    p = p * r2 + -1.66666666666666667e-01f;         // -1/3!
+    return r + r * (r2 * p);
+}
+
+RS_HD float cos_poly(float r)
+{
+    float r2 = r * r;
+    float p = 2.08767569878680990e-09f;              //  1/12!
+    p = p * r2 + -2.75573192239858907e-07f;         // -1/10!
+    p = p * r2 + 2.48015873015873016e-05f;          //  1/8!
+    p = p * r2 + -1.38888888888888889e-03f;         // -1/6!
+    p = p * r2 + 4.16666666666666667e-02f;          //  1/4!
+    p = p * r2 + -0.5f;                             // -1/2!
+    return 1.f + r2 * p;
+}
+
+RS_HD void f_sincos(float x, float& s, float& c)
+{
+    int q;
+    float r = reduce_half_pi(x, q);
+    float sr = sin_poly(r), cr = cos_poly(r);
+    switch (q & 3)
+    {
+    case 0: s = sr; c = cr; break;
+    case 1: s = cr; c = -sr; break;
+    case 2: s = -sr; c = -cr; break;
+    default: s = -cr; c = sr; break;
+    }
+}
+RS_HD float f_sin(float x) { float s, c; f_sincos(x, s, c); return s; }
+RS_HD float f_cos(float x) { float s, c; f_sincos(x, s, c); return c; }
+RS_HD float f_tan(float x) { float s, c; f_sincos(x, s, c); return s / c; }
+
+// atan via atan(x) = pi/2 - atan(1/x) for |x| > 1 and
+// atan(x) = pi/6 + atan((sqrt(3) x - 1) / (x + sqrt(3))) for x > tan(pi/12),
+// then the Taylor series of atan on |t| <= tan(pi/12) = 0.2679.
+RS_HD float f_atan(float x)
+{
+    float ax = fabsf(x);
+    if (f_isnan(x)) return x;
+    bool inv = ax > 1.f;
+    if (inv) ax = 1.f / ax;
+    bool red = ax > 0.267949194f;
+    float t = red ? (ax * kSqrt3 - 1.f) / (ax + kSqrt3) : ax;
+    float t2 = t * t;
+    float p = 0.0666666666666666667f;   //  1/15
+    p = p * t2 + -0.0769230769230769231f; // -1/13
+    p = p * t2 + 0.0909090909090909091f;  //  1/11
+    p = p * t2 + -0.111111111111111111f;  // -1/9
+    p = p * t2 + 0.142857142857142857f;   //  1/7
+    p = p * t2 + -0.2f;                   // -1/5
+    p = p * t2 + 0.333333333333333333f;   //  1/3
+    float a = t - t * (t2 * p);
+    if (red) a = kPiOver6 + a;
+    if (inv) a = kPiOver2 - a;
+    return x < 0.f ? -a : a;
+}
+
+// acos(x) = atan(sqrt(1-x^2)/x) folded to [0, pi].  The argument is clamped to
+// [-1, 1] first, so a dot product of unit vectors that rounds to 1 + ulp gives 0
+// instead of NaN (a documented restatement choice: HLSL acos is undefined there).
+RS_HD float f_acos(float x)
+{
+    if (f_isnan(x)) return x;
+    x = f_clamp(x, -1.f, 1.f);
+    float s = f_sqrt((1.f - x) * (1.f + x));
+    if (x == 0.f) return kPiOver2;
+    if (x > 0.f) return f_atan(s / x);
+    return kPi - f_atan(s / -x);
+}
+
+// Integer powers written out as products (replaces pow(x, 3) / pow(x, 5)).
+RS_HD float f_pow3(float x) { return x * x * x; }
+RS_HD float f_pow5(float x) { float x2 = x * x; return x2 * x2 * x; }
+
+// binary16 <-> binary32 (round to nearest even), written from the IEEE-754
+// encodings; used for the alias-table thresholds (EmissivePowerSampler.cpp:154-160).
+RS_HDI uint16_t f32_to_f16(float f)
+{
+    uint32_t x = f2u(f);
+    uint32_t sign = (x >> 16) & 0x8000u;
+    int32_t exp = (int32_t)((x >> 23) & 0xffu);
+    uint32_t mant = x & 0x7fffffu;
+    if (exp == 0xff) return (uint16_t)(sign | 0x7c00u | (mant ? 0x200u : 0u));
+    int32_t e = exp - 127 + 15;
+    if (e >= 0x1f) return (uint16_t)(sign | 0x7c00u);
+    if (e <= 0)
+    {
+        if (e < -10) return (uint16_t)sign;
+        mant |= 0x800000u;
+        uint32_t shift = (uint32_t)(14 - e);
+        uint32_t half = mant >> shift;
+        uint32_t rem = mant & ((1u << shift) - 1u);
+        uint32_t mid = 1u << (shift - 1u);
+        if (rem > mid || (rem == mid && (half & 1u))) half++;
+        return (uint16_t)(sign | half);
+    }
+    uint32_t half = sign | ((uint32_t)e << 10) | (mant >> 13);
+    uint32_t rem = mant & 0x1fffu;
+    if (rem > 0x1000u || (rem == 0x1000u && (half & 1u))) half++;
+    return (uint16_t)half;
+}
+
+RS_HDI float f16_to_f32(uint16_t h)
+{
+    uint32_t sign = ((uint32_t)h & 0x8000u) << 16;
+    uint32_t exp = ((uint32_t)h >> 10) & 0x1fu;
+    uint32_t mant = (uint32_t)h & 0x3ffu;
+    if (exp == 0)
+    {
+        if (mant == 0) return u2f(sign);
+        float m = (float)mant * (1.f / 16777216.f); // mant * 2^-24
+        return sign ? -m : m;
+    }
+    if (exp == 0x1f) return u2f(sign | 0x7f800000u | (mant << 13));
+    return u2f(sign | ((exp + 112u) << 23) | (mant << 13));
+}
+
+} // namespace rs

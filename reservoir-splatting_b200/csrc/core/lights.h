@@ -1,0 +1,116 @@
+// Emissive-triangle light sampling for next-event estimation.
+//
+//   Rendering/Lights/EmissivePowerSampler.slang:61-96, 113-120  power-proportional pick via a
+//       packed alias table (16-bit threshold, 2 x 24-bit indices) then uniform area sampling
+//   Rendering/Lights/EmissiveLightSamplerHelpers.slang:54-85, 111-124  triangle sample / pdf
+//   Utils/Math/MathHelpers.slang:391-396  sample_triangle
+//   PathTracer.slang:543-565, 606-701     light-type selection (emissive only here) and the
+//       hemisphere rejection applied to the sample
+#pragma once
+#include "material.h"
+
+namespace rs {
+
+// One emissive triangle of the light collection (LightCollectionShared.slang EmissiveTriangle +
+// EmissiveFlux): positions, face normal, area, radiance, flux and the scene triangle it came from.
+struct alignas(16) LightTriangle
+{
+    float p0[3]; uint32_t sceneTri;
+    float p1[3]; float area;
+    float p2[3]; float flux;
+    float normal[3]; uint32_t materialID;
+    float Le[3]; float pad;
+};
+
+struct LightView
+{
+    const LightTriangle* tris;
+    const u2* aliasTable;
+    uint32_t count;
+    float invWeightsSum;
+};
+
+struct TriangleLightSample
+{
+    uint32_t triangleIndex;
+    f3 posW;
+    f3 normalW;
+    f3 dir;
+    float distance;
+    f3 Le;
+    float pdf;
+    f2 uv;
+    float geometryTerm;
+};
+
+RS_HD bool sample_triangle_light(const LightView& L, f3 posW, uint32_t triangleIndex, f2 u, TriangleLightSample& ls)
+{
+    ls.triangleIndex = triangleIndex;
+    const LightTriangle& tri = L.tris[triangleIndex];
+    float su = f_sqrt(u.x);
+    f2 b = mk2(1.f - su, u.y * su);
+    f3 bary = mk3(1.f - b.x - b.y, b.x, b.y);
+    f3 p0 = mk3(tri.p0[0], tri.p0[1], tri.p0[2]);
+    f3 p1 = mk3(tri.p1[0], tri.p1[1], tri.p1[2]);
+    f3 p2 = mk3(tri.p2[0], tri.p2[1], tri.p2[2]);
+    ls.posW = p0 * bary.x + p1 * bary.y + p2 * bary.z;
+    f3 toLight = ls.posW - posW;
+    const float distSqr = f_max(kFltMin, dot(toLight, toLight));
+    ls.distance = f_sqrt(distSqr);
+    ls.dir = toLight / ls.distance;
+    ls.normalW = mk3(tri.normal[0], tri.normal[1], tri.normal[2]);
+    float cosTheta = dot(ls.normalW, -ls.dir);
+    if (cosTheta <= 0.f) return false;
+    ls.Le = mk3(tri.Le[0], tri.Le[1], tri.Le[2]);
+    float denom = f_max(kFltMin, cosTheta * tri.area);
+    ls.pdf = distSqr / denom;
+    float su2 = f_sqrt(u.x);
+    ls.uv = mk2(1.f - su2, u.y * su2);
+    ls.geometryTerm = cosTheta / distSqr;
+    return true;
+}
+
+// EmissivePowerSampler::sampleLight.  Draw order: uLight, uAlias, then 2D on the triangle.
+RS_HD bool sample_emissive_power(const LightView& L, f3 posW, SampleGen& sg, TriangleLightSample& ls)
+{
+    if (L.count == 0) return false;
+    float uLight = sampleNext1D(sg);
+    uint32_t triangleCount = L.count;
+    uint32_t idx = (uint32_t)(uLight * (float)triangleCount);
+    uint32_t triangleIndex = idx < triangleCount - 1 ? idx : triangleCount - 1;
+    u2 packed = L.aliasTable[triangleIndex];
+    float threshold = f16_to_f32((uint16_t)(packed.x >> 16u));
+    uint32_t selectAbove = ((packed.x & 0xFFFFu) << 8u) | ((packed.y >> 24u) & 0xFFu);
+    uint32_t selectBelow = packed.y & 0xFFFFFFu;
+    triangleIndex = (sampleNext1D(sg) >= threshold) ? selectAbove : selectBelow;
+    float triangleSelectionPdf = L.tris[triangleIndex].flux * L.invWeightsSum;
+    f2 u; u.x = sampleNext1D(sg); u.y = sampleNext1D(sg);
+    if (!sample_triangle_light(L, posW, triangleIndex, u, ls)) return false;
+    ls.pdf *= triangleSelectionPdf;
+    return true;
+}
+
+// EmissivePowerSampler::evalPdf + evalTrianglePdf: solid-angle pdf at posW of a hit on light triangleIndex.
+RS_HD float eval_emissive_pdf(const LightView& L, f3 posW, uint32_t triangleIndex, f3 hitPosW, f3 hitNormalW)
+{
+    if (triangleIndex == kInvalidIndex) return 0.f;
+    float triangleSelectionPdf = L.tris[triangleIndex].flux * L.invWeightsSum;
+    f3 toLight = hitPosW - posW;
+    const float distSqr = dot(toLight, toLight);
+    float trianglePdf;
+    if (distSqr <= kFltMin) trianglePdf = 0.f;
+    else
+    {
+        f3 Ld = toLight / f_sqrt(distSqr);
+        float cosTheta = dot(hitNormalW, -Ld);
+        if (cosTheta <= 0.f) trianglePdf = 0.f;
+        else
+        {
+            float denom = f_max(kFltMin, cosTheta * L.tris[triangleIndex].area);
+            trianglePdf = distSqr / denom;
+        }
+    }
+    return triangleSelectionPdf * trianglePdf;
+}
+
+} // namespace rs

@@ -1,0 +1,1230 @@
+// sm_100a kernels of the Reservoir Splatting per-frame path.  One thread per
+// pixel (or per source pixel / cell); all state lives in structure-of-arrays
+// planes so every warp load and store is a coalesced 512-byte transaction.
+// Nothing here is a dense contraction, so no tensor-core path exists; the
+// bounds are HBM bandwidth (splat, scan, fill, resolve) and BVH traversal
+// latency (candidates, reprojection visibility, resampling shifts).
+#include "kernels.h"
+
+namespace rs {
+
+// ============================================================ primary hits + motion vectors
+// VBufferRT.slang:71-150 (samplePattern Center, pinhole): hit of the pixel-centre ray of the
+// frame's camera and mvec = prevScreen - (pixel + 0.5) / dim, prevScreen being the film
+// projection of the hit point through the previous frame's camera.
+__global__ void __launch_bounds__(256) k_vbuffer(DevCtx C, uint4* __restrict__ vbuffer, float2* __restrict__ mvec)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= C.W * C.H) return;
+    uint32_t x = i % C.W, y = i / C.W;
+    const CameraData& cam = C.camera;
+    const CameraData& pc = C.prevCamera;
+    f2 p = mk2(((float)x + 0.5f) / (float)C.W, ((float)y + 0.5f) / (float)C.H);
+    f2 ndc = mk2(2.f * p.x + -1.f, -2.f * p.y + 1.f);
+    f3 dir = normalize(cam.cameraU * ndc.x + cam.cameraV * ndc.y + cam.cameraW);
+    HitInfo h; float t;
+    if (trace_closest(C.bvh, mk_ray(cam.posW, dir, 0.f, kRayTMax), h, t, C.fault))
+    {
+        vbuffer[i] = make_uint4(h.w[0], h.w[1], h.w[2], h.w[3]);
+        f3 prevPosW = dev_sd(C, h, dir).posW;
+        f3 d = prevPosW - pc.posW;
+        f3 camRay = mk3(dot(normalize(pc.cameraU), d), dot(normalize(pc.cameraV), d), dot(normalize(pc.cameraW), d));
+        float lw = length(pc.cameraW);
+        f2 film = mk2(lw * (camRay.x / camRay.z), lw * (camRay.y / camRay.z));
+        f2 pndc = mk2(film.x / length(pc.cameraU), film.y / length(pc.cameraV));
+        f2 prevCrd = mk2(0.5f * pndc.x + 0.5f, -0.5f * pndc.y + 0.5f);
+        mvec[i] = make_float2(prevCrd.x - p.x, prevCrd.y - p.y);
+    }
+    else
+    {
+        vbuffer[i] = make_uint4(0u, 0u, 0u, 0u);
+        mvec[i] = make_float2(0.f, 0.f);
+    }
+}
+
+// ============================================================ initial candidates
+// Path state of the candidate tracer (PathStates.slang:85-219, the fields the pass uses).
+struct PState
+{
+    uint32_t flags;      // PathFlags bits (unshifted)
+    uint32_t vertex;     // vertex index
+    uint32_t bounces;    // packed 8-bit counters: diffuse, specular, transmission
+    f3 origin, dir;
+    float pdf, totalPdf;
+    HitInfo hit;
+    f3 prevHitPos;
+    f3 thp;
+    f3 earlyThroughput;
+    SampleGen sg;
+    Recon rec;           // path.reconnection
+    float candTotalWeight; // path.reservoir (CandidateReservoir)
+    f3 candIntegrand;
+    Recon candRec;       // path.reservoir.selectedReconnection
+};
+enum : uint32_t { kPActive = 1u, kPHit = 2u, kPSpecular = 8u, kPDelta = 16u, kPLightUpper = 64u, kPLightLower = 128u };
+
+__device__ __forceinline__ uint32_t pbounces(const PState& p, uint32_t type) { return (p.bounces >> (type << 3)) & 0xffu; }
+__device__ __forceinline__ bool finished_bounces(const DevCtx& C, const PState& p) // PathTracer.slang:161-172
+{
+    uint32_t d = pbounces(p, 0), s = pbounces(p, 1), t = pbounces(p, 2);
+    return (d + s + t) > C.maxSurfaceBounces || d > C.maxDiffuseBounces || s > C.maxSpecularBounces || t > C.maxTransmissionBounces;
+}
+
+// CandidateReservoir::addVertex (Reservoir.slang:43-58)
+__device__ __forceinline__ bool cand_add_vertex(PState& p, float sampleMIS, f3 sampleIntegrand)
+{
+    float samplePHat = luminance(sampleIntegrand);
+    float sampleWeight = sampleMIS * samplePHat;
+    sampleWeight = f_isnan(sampleWeight) ? 0.f : sampleWeight;
+    p.candTotalWeight += sampleWeight;
+    float rng = sampleNext1D(p.sg);
+    bool selected = (rng * p.candTotalWeight < sampleWeight);
+    p.candIntegrand = selected ? sampleIntegrand : p.candIntegrand;
+    return selected;
+}
+
+__device__ __forceinline__ void next_hit(const DevCtx& C, PState& p) // PathTracer.slang:278-299
+{
+    p.vertex += 1;
+    HitInfo h; float t;
+    if (trace_closest(C.bvh, mk_ray(p.origin, p.dir, 0.f, kRayTMax), h, t, C.fault)) { p.hit = h; p.flags |= kPHit; }
+    else p.flags &= ~kPHit;
+}
+
+// handleHit (PathTracer.slang:783-1168)
+__device__ void handle_hit(const DevCtx& C, PState& path)
+{
+    const bool isPrimaryHit = path.vertex == 1;
+    ShadingData sd = dev_sd(C, path.hit, path.dir);
+    float distanceToPrevVertex = length(sd.posW - path.prevHitPos);
+    float geometryFactor = f_abs(dot(sd.faceN, sd.V)) / (distanceToPrevVertex * distanceToPrevVertex);
+    float prevScatterPdf = path.pdf;
+    path.prevHitPos = sd.posW;
+    if (path.vertex == 1)
+    {
+        path.rec.firstHit = path.hit;
+        path.rec.firstWi = -path.dir;
+        CameraData cam; dev_orient(C, cam, 0.f); // path.time is never set by generatePath
+        f3 x0 = camera_lens_point(cam, path.rec.lensSample);
+        float dist = length(sd.posW - x0);
+        float distSquared = dist * dist;
+        float cosNormal = dot(-path.dir, sd.faceN);
+        float cosSensor = dot(normalize(cam.cameraW), path.dir);
+        path.rec.subPixelJacobian = f_abs(cosNormal / distSquared) / f_abs(f_pow3(cosSensor));
+        f3 camDir = normalize(cam.cameraW);
+        float camZ = dot(sd.posW - cam.posW, camDir);
+        float d0 = (length(cam.cameraW) / f_abs(camZ) * dist);
+        float d1 = dist - d0;
+        path.rec.lensVertexJacobian = (d0 * d0) / (d1 * d1) * (f_abs(dot(-path.dir, sd.faceN))) / (f_abs(dot(-path.dir, camDir)));
+    }
+    else if (path.vertex == 2)
+    {
+        path.rec.secondHit = path.hit;
+        path.rec.secondaryPathJacobian = prevScatterPdf * geometryFactor;
+    }
+    else if (path.vertex == 3)
+    {
+        path.rec.secondaryPathJacobian *= prevScatterPdf;
+    }
+
+    BsdfData d = dev_instance(C, sd);
+    const bool isLightSamplable = !(path.flags & kPDelta);
+    const bool isLightSampled = (path.flags & (kPLightUpper | kPLightLower)) != 0;
+    const bool haveLights = C.lights.count > 0;
+    bool computeEmissive = isPrimaryHit || (haveLights && (!isLightSampled || !isLightSamplable));
+    if (computeEmissive && any_gt0(d.emission))
+    {
+        float misWeight = 1.f;
+        float lightPdf = 0.f;
+        if (haveLights && !isPrimaryHit && isLightSampled && isLightSamplable)
+        {
+            lightPdf = 1.f * eval_emissive_pdf(C.lights, path.origin, sd.lightIndex, sd.posW, sd_oriented_face_normal(sd));
+            misWeight = dev_mis(C, path.totalPdf, lightPdf);
+        }
+        bool selected = cand_add_vertex(path, 1.f, path.earlyThroughput * path.thp * d.emission * misWeight);
+        if (selected)
+        {
+            path.candRec = path.rec;
+            path.candRec.pathLength = path.vertex;
+            path.candRec.lightIsNEE = false;
+            path.candRec.lightIsDistant = false;
+            path.candRec.lightPdf = lightPdf;
+            if (path.vertex == 2) path.candRec.lightPdf *= geometryFactor;
+            if (path.vertex == 2 || path.vertex == 3) path.candRec.irradiance = d.emission;
+            else path.candRec.irradiance = path.thp * d.emission * misWeight;
+        }
+    }
+
+    if (finished_bounces(C, path)) { path.flags &= ~kPActive; return; }
+
+    path.origin = sd_ray_origin(sd, true);
+
+    const uint32_t lobeTypes = mi_lobe_types(d);
+    path.flags &= ~(kPLightUpper | kPLightLower);
+    if ((lobeTypes & kLobeNonDelta) != 0)
+    {
+        bool sampleUpper = (lobeTypes & kLobeNonDeltaReflection) != 0;
+        bool sampleLower = (lobeTypes & kLobeNonDeltaTransmission) != 0;
+        // generateLightSample (:668-701) with p = {0, haveLights, 0}: the type-selection draw is always taken.
+        bool validSample = false;
+        TriangleLightSample tls;
+        f3 lsLi = mk3(0.f), lsOrigin = mk3(0.f), lsDir = mk3(0.f);
+        float lsPdf = 0.f, lsDistance = 0.f;
+        float u = sampleNext1D(path.sg);
+        if (!(u < 0.f) && (u < (haveLights ? 1.f : 0.f)))
+        {
+            const float selectionPdf = 1.f;
+            if (sample_emissive_power(C.lights, sd.posW, path.sg, tls))
+            {
+                lsLi = tls.pdf > 0.f ? tls.Le / tls.pdf : mk3(0.f);
+                lsPdf = tls.pdf;
+                f3 lightPos = computeRayOrigin(tls.posW, tls.normalW);
+                f3 toL = lightPos - sd.posW;
+                lsOrigin = computeRayOrigin(sd.posW, dot(sd.faceN, toL) >= 0.f ? sd.faceN : -sd.faceN);
+                f3 toLight = lightPos - lsOrigin;
+                lsDistance = length(toLight);
+                lsDir = normalize(toLight);
+                if (any_gt0(lsLi))
+                {
+                    float NdotL = dot(sd_oriented_face_normal(sd), lsDir);
+                    if (!((!sampleUpper && NdotL >= -kMinCosTheta) || (!sampleLower && NdotL <= kMinCosTheta)))
+                    {
+                        lsPdf *= selectionPdf;
+                        lsLi /= selectionPdf;
+                        validSample = true;
+                    }
+                }
+            }
+        }
+        if (sampleUpper) path.flags |= kPLightUpper;
+        if (sampleLower) path.flags |= kPLightLower;
+        if (validSample)
+        {
+            f3 Le = lsLi * lsPdf;
+            float scatterPdf = mi_pdf(sd, d, 0u, lsDir);
+            float misWeight = dev_mis(C, lsPdf, scatterPdf);
+            f3 weight = mi_eval(sd, d, 0u, lsDir);
+            f3 Lr = weight * misWeight * lsLi;
+            if (any_gt0(Lr) && dev_visible(C, mk_ray(lsOrigin, lsDir, 0.f, lsDistance)))
+            {
+                bool selected = cand_add_vertex(path, 1.f, path.earlyThroughput * path.thp * weight * lsLi * misWeight);
+                if (selected)
+                {
+                    path.candRec = path.rec;
+                    path.candRec.pathLength = path.vertex + 1;
+                    path.candRec.lightIsNEE = true;
+                    path.candRec.irradiance = Le;
+                    if (path.vertex == 1) path.candRec.transmissionEvent = dot(sd.faceN, sd.V) * dot(sd.faceN, lsDir) < 0.f;
+                    path.candRec.lightIsDistant = false;
+                    if (path.vertex == 1)
+                    {
+                        path.candRec.secondHit = hit_tri(C.lights.tris[tls.triangleIndex].sceneTri, tls.uv.x, tls.uv.y);
+                        path.candRec.secondaryPathJacobian = lsPdf * tls.geometryTerm;
+                        path.candRec.lightPdf = lsPdf * tls.geometryTerm;
+                    }
+                    else if (path.vertex == 2)
+                    {
+                        path.candRec.secondWo = lsDir;
+                        path.candRec.lightPdf = lsPdf;
+                    }
+                    else
+                    {
+                        path.candRec.irradiance = path.thp * Lr;
+                    }
+                }
+            }
+        }
+    }
+
+    if (C.useRussianRoulette)
+    {
+        float u = sampleNext1D(path.sg);
+        const float rrVal = luminance(path.thp);
+        const float prob = f_max(0.f, 1.f - rrVal);
+        if (u < prob) { path.flags &= ~kPActive; return; }
+        path.thp /= 1.f - prob;
+    }
+
+    // generateScatterRay (:331-382)
+    BSDFSample result;
+    result.wo = mk3(0.f); result.pdf = 0.f; result.weight = mk3(0.f); result.lobeType = 0;
+    bool valid = mi_sample(sd, d, 1u, path.sg, result);
+    path.pdf = result.pdf;
+    uint32_t componentType = 0;
+    if (result.lobeType & kLobeDiffuseReflection)
+    {
+        if ((result.lobeType & kLobeSpecular) || (result.lobeType & kLobeDelta)) { componentType = 3; result.lobeType &= ~kLobeDiffuseReflection; }
+    }
+    else
+    {
+        if (result.lobeType & kLobeDiffuseTransmission) componentType = 1;
+        else if ((result.lobeType & kLobeSpecular) || (result.lobeType & kLobeDelta)) componentType = 2;
+    }
+    if (path.vertex == 1) path.rec.firstComp = componentType;
+    else if (path.vertex == 2) { path.rec.secondComp = componentType; path.rec.secondWo = result.wo; }
+    path.totalPdf = mi_pdf(sd, d, 0xFu, result.wo);
+    if (valid)
+    {
+        // generateScatterRay(bs, ...) (:391-471)
+        path.dir = result.wo;
+        path.thp *= result.weight;
+        path.flags &= ~(4u | kPSpecular | kPDelta);
+        if (result.lobeType & kLobeReflection)
+        {
+            float roughness = mi_roughness(d);
+            bool isDiffuse = (result.lobeType & kLobeDiffuseReflection) || roughness > C.specularRoughnessThreshold;
+            if (isDiffuse) path.bounces += 1u;
+            else { path.bounces += (1u << 8); path.flags |= kPSpecular; }
+        }
+        if (result.lobeType & kLobeDelta) path.flags |= kPDelta;
+    }
+    if (path.vertex == 1 || path.vertex == 2)
+    {
+        path.earlyThroughput *= result.weight;
+        path.thp = mk3(1.f);
+    }
+    const bool isLastVertex = finished_bounces(C, path);
+    if (isLastVertex && !(path.flags & kPDelta)) valid = false;
+    if (C.disableCaustics && pbounces(path, 0) > 0 && (path.flags & kPSpecular)) valid = false;
+    if (!valid) path.flags &= ~kPActive;
+}
+
+// InitialCandidates.cs.slang:80-141 + addCandidateReservoir (:52-75)
+__global__ void __launch_bounds__(128) k_candidates(DevCtx C, ResPlanes curr, RecPlanes currRec)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= C.W * C.H) return;
+    uint32_t x = i % C.W, y = i / C.W;
+    const uint32_t spp = C.spp;
+    for (uint32_t sIdx = 0; sIdx < spp; sIdx++)
+    {
+        PState path;
+        // generatePath (PathTracer.slang:194-221)
+        path.flags = kPActive;
+        path.vertex = 0;
+        path.bounces = 0;
+        path.thp = mk3(1.f);
+        path.earlyThroughput = mk3(1.f);
+        path.pdf = 0.f; path.totalPdf = 0.f;
+        path.hit = hit_none();
+        path.rec = recon_default();
+        path.candTotalWeight = 0.f;
+        path.candIntegrand = mk3(0.f);
+        path.candRec = recon_default();
+        path.sg = sg_create(x, y, C.useFixedSeed ? C.fixedSeed + 0 : kNumRenderPasses * (C.frameCount + C.seed) + 0, C.sgKind);
+        CameraData cam = C.camera;
+        path.rec.time = sampleNext1D(path.sg) * cam.shutterSpeed;
+        path.rec.subPixel.x = sampleNext1D(path.sg);
+        path.rec.subPixel.y = sampleNext1D(path.sg);
+        if (cam.apertureRadius > 0.f)
+        {
+            f2 u; u.x = sampleNext1D(path.sg); u.y = sampleNext1D(path.sg);
+            path.rec.lensSample = sample_disk(u);
+        }
+        else path.rec.lensSample = mk2(0.f, 0.f);
+        orient_camera(C.cm, cam, C.frameCount, path.rec.time);
+        Ray r = camera_ray_thinlens(cam, C.W, C.H, mk2((float)x + path.rec.subPixel.x, (float)y + path.rec.subPixel.y), path.rec.lensSample);
+        path.origin = r.origin;
+        path.dir = r.dir;
+        path.prevHitPos = camera_lens_point(cam, path.rec.lensSample);
+
+        next_hit(C, path);
+        if (path.flags & kPHit)
+        {
+            handle_hit(C, path);
+            while (path.flags & kPActive)
+            {
+                next_hit(C, path);
+                if (path.flags & kPHit) handle_hit(C, path);
+                else
+                {
+                    // handleMiss (:1433-1524) without an environment map
+                    if (path.vertex == 2) path.rec.secondaryPathJacobian = path.pdf * 1.f;
+                    else if (path.vertex == 3) path.rec.secondaryPathJacobian *= path.pdf;
+                    path.flags &= ~kPActive;
+                }
+            }
+        }
+        // addCandidateReservoir
+        const bool isFirstSample = (sIdx == spp - 1) || spp == 1;
+        Res ex = isFirstSample ? res_default() : load_res_rw(curr, i);
+        float weight = (1.f / (float)spp) * path.candTotalWeight;
+        ex.totalWeight = ex.totalWeight + weight;
+        ex.confidence = f_min(ex.confidence + 1.f, kConfidenceCap);
+        float rng = sampleNext1D(path.sg);
+        bool selected = (rng * ex.totalWeight < weight);
+        ex.integrand = selected ? path.candIntegrand : ex.integrand;
+        ex.subPixel = selected ? path.rec.subPixel : ex.subPixel;
+        ex.confidence = 1.f;
+        store_res(curr, i, ex);
+        Recon exr = isFirstSample ? recon_default() : load_rec_rw(currRec, i);
+        store_rec(currRec, i, selected ? path.candRec : exr);
+    }
+}
+
+// ============================================================ forward reprojection (splat)
+// ReprojectTemporalSamples.rt.slang:64-175.  Writes the destination cell of every source pixel
+// and counts splats per cell; the cell lists are built by k_fill / k_rank_cells.
+__global__ void __launch_bounds__(256) k_reproject(DevCtx C, ResPlanes prev, RecPlanes prevRec,
+                                                   uint32_t* __restrict__ targets, uint32_t* __restrict__ counts)
+{
+    uint32_t ci = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ci >= C.W * C.H) return;
+    uint32_t target = kInvalidIndex;
+    f3 integrand = load_integrand(prev, ci);
+    if (!all_eq0(integrand))
+    {
+        const uint4* p = prevRec.p + ci;
+        uint4 q0 = __ldg(p), q1 = __ldg(p + prevRec.stride), q2 = __ldg(p + 2 * prevRec.stride);
+        f2 lensSample = mk2(u2f(q0.z), u2f(q0.w));
+        float time = u2f(q1.x);
+        HitInfo firstHit; firstHit.w[0] = q2.x; firstHit.w[1] = q2.y; firstHit.w[2] = q2.z; firstHit.w[3] = q2.w;
+        if (hit_valid(firstHit))
+        {
+            CameraData cc; dev_orient(C, cc, time);
+            f2 lensLocal = mk2(cc.apertureRadius * lensSample.x, cc.apertureRadius * lensSample.y);
+            f3 lensWorld = normalize(cc.cameraU) * lensLocal.x + normalize(cc.cameraV) * lensLocal.y;
+            Ray nr;
+            nr.origin = cc.posW + lensWorld;
+            f3 x1 = dev_sd(C, firstHit, mk3(0.f)).posW;
+            nr.dir = normalize(x1 - nr.origin);
+            nr.tMin = 0.001f * length(x1 - nr.origin);
+            nr.tMax = 0.999f * length(x1 - nr.origin);
+            f3 camDir = mk3(dot(normalize(cc.cameraU), nr.dir), dot(normalize(cc.cameraV), nr.dir), dot(normalize(cc.cameraW), nr.dir));
+            if (camDir.z > 0.001f && dev_visible(C, nr))
+            {
+                float lw = length(cc.cameraW);
+                f2 film = mk2(lensLocal.x + lw * (camDir.x / camDir.z), lensLocal.y + lw * (camDir.y / camDir.z));
+                f2 ndc = mk2(film.x / length(cc.cameraU), film.y / length(cc.cameraV));
+                f2 nfp = mk2((0.5f * ndc.x + 0.5f) * (float)C.W, (-0.5f * ndc.y + 0.5f) * (float)C.H);
+                if (valid_float(C, nfp)) target = (uint32_t)f_floor(nfp.y) * C.W + (uint32_t)f_floor(nfp.x);
+            }
+        }
+    }
+    targets[ci] = target;
+    if (target != kInvalidIndex) atomicAdd(&counts[target], 1u);
+}
+
+// MultiReprojectTemporalSamples.rt.slang:65-168 (P partitions; targets/counts hold P planes of N)
+__global__ void __launch_bounds__(256) k_multi_reproject(DevCtx C, ResPlanes prev, RecPlanes prevRec,
+                                                         uint32_t* __restrict__ targets, uint32_t* __restrict__ counts)
+{
+    uint32_t ci = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t N = C.W * C.H;
+    if (ci >= N) return;
+    const uint32_t P = C.numTimePartitions;
+    for (uint32_t i = 0; i < P; i++) targets[(size_t)i * N + ci] = kInvalidIndex;
+    f3 integrand = load_integrand(prev, ci);
+    if (all_eq0(integrand)) return;
+    const uint4* p = prevRec.p + ci;
+    uint4 q1 = __ldg(p + prevRec.stride), q2 = __ldg(p + 2 * prevRec.stride);
+    float time = u2f(q1.x);
+    HitInfo firstHit; firstHit.w[0] = q2.x; firstHit.w[1] = q2.y; firstHit.w[2] = q2.z; firstHit.w[3] = q2.w;
+    if (!hit_valid(firstHit)) return;
+    float fractionalTime = time / C.camera.shutterSpeed;
+    float timePartitions = C.camera.shutterSpeed / (float)P;
+    f3 x1 = dev_sd(C, firstHit, mk3(0.f)).posW;
+    for (uint32_t i = 0; i < P; i++)
+    {
+        float newTime = (fractionalTime + (float)i) * timePartitions;
+        CameraData cc; dev_orient(C, cc, newTime);
+        f3 rayDir = x1 - cc.posW;
+        f3 nd = normalize(rayDir);
+        float d = dot(nd, normalize(cc.cameraW));
+        if (d <= 0.001f) continue;
+        if (!dev_visible(C, mk_ray(cc.posW, rayDir, 0.001f, 0.999f))) continue;
+        float tanFovY = cc.focalLength == 0.f ? 0.f : cc.frameHeight / cc.focalLength;
+        d *= tanFovY;
+        f2 offset = mk2(dot(nd, normalize(cc.cameraU)), -dot(nd, normalize(cc.cameraV)));
+        f2 ndc = mk2(0.5f + offset.x / (d * cc.aspectRatio), 0.5f + offset.y / d);
+        f2 nfp = mk2(ndc.x * (float)C.W, ndc.y * (float)C.H);
+        if (!valid_float(C, nfp)) continue;
+        uint32_t t = (uint32_t)f_floor(nfp.y) * C.W + (uint32_t)f_floor(nfp.x);
+        targets[(size_t)i * N + ci] = t;
+        atomicAdd(&counts[(size_t)i * N + t], 1u);
+    }
+}
+
+// ============================================================ cell lists (canonical order)
+// Exclusive scan of the per-cell counts: 1024 threads x 4 items per block, block sums scanned
+// by one block, then added back.  Replaces the atomic offset allocation of
+// SortReprojectedReservoirs.cs.slang:56-73 with a deterministic prefix sum.
+constexpr int kScanThreads = 1024;
+constexpr int kScanItems = 4;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* smem, uint32_t& total)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t x = v;
+    for (int o = 1; o < 32; o <<= 1)
+    {
+        uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) smem[warp] = x;
+    __syncthreads();
+    if (warp == 0)
+    {
+        uint32_t s = (lane < (int)(blockDim.x >> 5)) ? smem[lane] : 0u;
+        for (int o = 1; o < 32; o <<= 1)
+        {
+            uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= o) s += y;
+        }
+        smem[lane] = s;
+    }
+    __syncthreads();
+    uint32_t warpPrefix = warp > 0 ? smem[warp - 1] : 0u;
+    total = smem[(blockDim.x >> 5) - 1];
+    __syncthreads();
+    return warpPrefix + x - v;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_tiles(const uint32_t* __restrict__ in, uint32_t* __restrict__ out,
+                                                             uint32_t* __restrict__ tileSums, uint32_t n)
+{
+    __shared__ uint32_t smem[32];
+    size_t base = (size_t)blockIdx.x * kScanTile + (size_t)threadIdx.x * kScanItems;
+    uint32_t v[kScanItems];
+    uint32_t sum = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; k++)
+    {
+        v[k] = (base + k < n) ? in[base + k] : 0u;
+        sum += v[k];
+    }
+    uint32_t total;
+    uint32_t pre = block_exclusive_scan(sum, smem, total);
+#pragma unroll
+    for (int k = 0; k < kScanItems; k++)
+    {
+        if (base + k < n) out[base + k] = pre;
+        pre += v[k];
+    }
+    if (threadIdx.x == 0) tileSums[blockIdx.x] = total;
+}
+
+// One block scans the tile sums (up to kScanTile tiles = 16.7M cells) and writes the grand total.
+__global__ void __launch_bounds__(kScanThreads) k_scan_tile_sums(uint32_t* __restrict__ tileSums, uint32_t numTiles, uint32_t* __restrict__ totalOut)
+{
+    __shared__ uint32_t smem[32];
+    size_t base = (size_t)threadIdx.x * kScanItems;
+    uint32_t v[kScanItems];
+    uint32_t sum = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; k++)
+    {
+        v[k] = (base + k < numTiles) ? tileSums[base + k] : 0u;
+        sum += v[k];
+    }
+    uint32_t total;
+    uint32_t pre = block_exclusive_scan(sum, smem, total);
+#pragma unroll
+    for (int k = 0; k < kScanItems; k++)
+    {
+        if (base + k < numTiles) tileSums[base + k] = pre;
+        pre += v[k];
+    }
+    if (threadIdx.x == 0 && totalOut) *totalOut = total;
+}
+
+__global__ void __launch_bounds__(256) k_scan_add(uint32_t* __restrict__ out, const uint32_t* __restrict__ tileSums, uint32_t n)
+{
+    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out[i] += tileSums[i / kScanTile];
+}
+
+// Places each splat at offset[target] + arrival rank (order within a cell is fixed up by k_rank_cells).
+__global__ void __launch_bounds__(256) k_fill(const uint32_t* __restrict__ targets, const uint32_t* __restrict__ offsets,
+                                              uint32_t* __restrict__ cursor, uint32_t* __restrict__ unsorted, uint32_t n)
+{
+    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    uint32_t t = targets[s];
+    if (t == kInvalidIndex) return;
+    uint32_t slot = offsets[t] + atomicAdd(&cursor[t], 1u);
+    unsorted[slot] = s;
+}
+
+// Canonical in-cell order: each splat's final slot is offset + (number of splats of the same
+// cell with a smaller source index).  Source indices are distinct, so the ranks are a permutation.
+__global__ void __launch_bounds__(256) k_rank_cells(const uint32_t* __restrict__ targets, const uint32_t* __restrict__ offsets,
+                                                    const uint32_t* __restrict__ counts, const uint32_t* __restrict__ unsorted,
+                                                    uint32_t* __restrict__ sorted, uint32_t n)
+{
+    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    uint32_t t = targets[s];
+    if (t == kInvalidIndex) return;
+    uint32_t off = offsets[t], cnt = counts[t];
+    uint32_t rank = 0;
+    for (uint32_t j = 0; j < cnt; j++) rank += (__ldg(&unsorted[off + j]) < s) ? 1u : 0u;
+    sorted[off + rank] = s;
+}
+
+// ============================================================ backup gather (collect)
+// CollectTemporalSamples.cs.slang:70-257
+__device__ __forceinline__ f2 prev_pixel_from_mvec(const DevCtx& C, const float2* mvec, uint32_t x, uint32_t y)
+{
+    float2 m = __ldg(&mvec[y * C.W + x]);
+    f2 mv = mk2(m.x, m.y);
+    mv = (length(mv) < 1e-06f) ? mk2(0.f, 0.f) : mv;
+    return mk2((float)x + mv.x * (float)C.W, (float)y + mv.y * (float)C.H);
+}
+
+__global__ void __launch_bounds__(128) k_collect(DevCtx C, const float2* __restrict__ mvec, ResPlanes prev, RecPlanes prevRec,
+                                                 ResPlanes inter, RecPlanes interRec, float2* __restrict__ floatingCoords,
+                                                 const Shifted* __restrict__ shiftedPaths)
+{
+    uint32_t ci = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ci >= C.W * C.H) return;
+    uint32_t x = ci % C.W, y = ci / C.W;
+    const bool useConf = C.useConfTemporal != 0;
+    SampleGen sg = sg_create(x, y, pass_seed(C, 2), C.sgKind);
+    f2 prevPixel = prev_pixel_from_mvec(C, mvec, x, y);
+    Res dst = res_default();
+    Recon dstR = recon_default();
+    f2 dstFC = mk2(-1.f, -1.f);
+    if (valid_float(C, prevPixel))
+    {
+        int tlx = (int)f_floor(prevPixel.x), tly = (int)f_floor(prevPixel.y);
+        f2 frac = mk2(f_saturate(prevPixel.x - (float)tlx), f_saturate(prevPixel.y - (float)tly));
+        if (C.gatherOption == 0u) // Fast
+        {
+            dstFC = prevPixel;
+            float totalConfidence = 0.f;
+            for (int ox = 0; ox < 2; ox++)
+                for (int oy = 0; oy < 2; oy++)
+                {
+                    int nx = tlx + ox, ny = tly + oy;
+                    if (!valid_int(C, nx, ny)) continue;
+                    uint32_t ni = (uint32_t)ny * C.W + (uint32_t)nx;
+                    Res nr = load_res(prev, ni);
+                    f2 rel = mk2((float)ox + nr.subPixel.x - frac.x, (float)oy + nr.subPixel.y - frac.y);
+                    float bw = f_lerp((float)(1 - ox), (float)ox, frac.x) * f_lerp((float)(1 - oy), (float)oy, frac.y);
+                    totalConfidence += bw * (useConf ? nr.confidence : 1.f);
+                    if (rel.x >= 0.f && rel.x < 1.f && rel.y >= 0.f && rel.y < 1.f)
+                    {
+                        nr.subPixel = rel;
+                        bool sel = res_add_sample(dst, sg, 1.f, nr.integrand, 1.f, nr);
+                        if (sel) dstR = load_rec(prevRec, ni);
+                    }
+                }
+            dst.confidence = totalConfidence;
+        }
+        else if (C.gatherOption == 1u) // Clamped
+        {
+            float rx = f_round(prevPixel.x), ry = f_round(prevPixel.y);
+            dstFC = mk2(rx, ry);
+            if (valid_int(C, (int)rx, (int)ry))
+            {
+                uint32_t pi = (uint32_t)ry * C.W + (uint32_t)rx;
+                dst = load_res(prev, pi);
+                dstR = load_rec(prevRec, pi);
+            }
+        }
+        else // Robust
+        {
+            dstFC = prevPixel;
+            float totalConfidence = 0.f;
+            for (int ox = 0; ox < 2; ox++)
+                for (int oy = 0; oy < 2; oy++)
+                {
+                    int nx = tlx + ox, ny = tly + oy;
+                    if (!valid_int(C, nx, ny)) continue;
+                    uint32_t ni = (uint32_t)ny * C.W + (uint32_t)nx;
+                    Res nr = load_res(prev, ni);
+                    Recon nrd = load_rec(prevRec, ni);
+                    f2 rel = mk2((float)ox + nr.subPixel.x - frac.x, (float)oy + nr.subPixel.y - frac.y);
+                    float bw = f_lerp((float)(1 - ox), (float)ox, frac.x) * f_lerp((float)(1 - oy), (float)oy, frac.y);
+                    totalConfidence += bw * (useConf ? nr.confidence : 1.f);
+                    int rox = 0, roy = 0;
+                    if (rel.x < 0.f) rox += 1;
+                    if (rel.x >= 1.f) rox -= 1;
+                    if (rel.y < 0.f) roy += 1;
+                    if (rel.y >= 1.f) roy -= 1;
+                    rel = mk2(rel.x + (float)rox, rel.y + (float)roy);
+                    rox += 1; roy += 1;
+                    uint32_t offsetIndex = (uint32_t)(rox + 3 * roy);
+                    bool noShiftNeeded = (offsetIndex == 4);
+                    offsetIndex = (offsetIndex > 4) ? offsetIndex - 1 : offsetIndex;
+                    Shifted sp;
+                    if (noShiftNeeded)
+                    {
+                        sp.primaryHit = nrd.firstHit;
+                        sp.fractionalPixel = mk2((float)nx + nr.subPixel.x, (float)ny + nr.subPixel.y);
+                        sp.lensSample = nrd.lensSample;
+                        sp.firstRayDir = -nrd.firstWi;
+                        sp.subPixelJacobian = nrd.subPixelJacobian;
+                        sp.lensVertexJacobian = nrd.lensVertexJacobian;
+                        sp.secondaryPathJacobian = nrd.secondaryPathJacobian;
+                        sp.radiance = nr.integrand;
+                    }
+                    else sp = shiftedPaths[8 * (size_t)ni + offsetIndex];
+                    float shiftedJacobian = noShiftNeeded ? 1.f : sp.secondaryPathJacobian / nrd.secondaryPathJacobian;
+                    float pHatSource = luminance(nr.integrand);
+                    float sourceWeight = bw * pHatSource * (useConf ? nr.confidence : 1.f);
+                    float totalPHat = sourceWeight;
+                    for (int tx = 0; tx < 2; ++tx)
+                        for (int ty = 0; ty < 2; ++ty)
+                        {
+                            int px = tlx + tx, py = tly + ty;
+                            if (!valid_int(C, px, py)) continue;
+                            int dx = tx - ox, dy = ty - oy;
+                            if (dx == 0 && dy == 0) continue;
+                            float tbw = f_lerp((float)(1 - tx), (float)tx, frac.x) * f_lerp((float)(1 - ty), (float)ty, frac.y);
+                            uint32_t tIdx = (uint32_t)((dx + 1) + 3 * (dy + 1));
+                            tIdx = (tIdx > 4) ? tIdx - 1 : tIdx;
+                            const Shifted& tp = shiftedPaths[8 * (size_t)ni + tIdx];
+                            float tPHat = luminance(tp.radiance);
+                            float tJac = tp.secondaryPathJacobian / nrd.secondaryPathJacobian;
+                            float tConf = useConf ? load_confidence(prev, (uint32_t)py * C.W + (uint32_t)px) : 1.f;
+                            totalPHat += tbw * tPHat * tJac * tConf;
+                        }
+                    float misWeight = (totalPHat > 0.f) ? sourceWeight / totalPHat : 0.f;
+                    nr.subPixel = rel;
+                    recon_update(nrd, sp);
+                    nrd.subPixel = rel;
+                    float lum = luminance(sp.radiance);
+                    bool sel = res_add_sample(dst, sg, misWeight, mk3(lum), shiftedJacobian, nr);
+                    if (sel) dstR = nrd;
+                }
+            dst.confidence = totalConfidence;
+        }
+        if (f_isnan(dst.totalWeight))
+        {
+            dst.integrand = mk3(0.f);
+            dst.totalWeight = 0.f;
+            dstR.subPixelJacobian = 1.f;
+            dstR.lensVertexJacobian = 1.f;
+            dstR.secondaryPathJacobian = 1.f;
+            dstR.pathLength = 0;
+        }
+    }
+    store_res(inter, ci, dst);
+    store_rec(interRec, ci, dstR);
+    floatingCoords[ci] = make_float2(dstFC.x, dstFC.y);
+}
+
+// RobustReuseOptimization.rt.slang:63-89
+__global__ void __launch_bounds__(128) k_robust(DevCtx C, ResPlanes prev, RecPlanes prevRec, Shifted* __restrict__ shiftedPaths)
+{
+    uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= C.W * C.H) return;
+    uint32_t x = idx % C.W, y = idx / C.W;
+    const int kOff[8][2] = {{-1, -1}, {0, -1}, {1, -1}, {-1, 0}, {1, 0}, {-1, 1}, {0, 1}, {1, 1}};
+    SampleGen sg = sg_create(x, y, pass_seed(C, 1), C.sgKind);
+    Res pr = load_res(prev, idx);
+    Recon rd = load_rec(prevRec, idx);
+    for (int k = 0; k < 8; k++)
+    {
+        int nx = (int)x + kOff[k][0], ny = (int)y + kOff[k][1];
+        bool neighborIsValid = valid_float(C, mk2((float)nx, (float)ny));
+        bool canShift = any_gt0(pr.integrand);
+        shiftedPaths[8 * (size_t)idx + k] = (neighborIsValid && canShift)
+            ? dev_gather_lens_copy(C, sg, rd, rd.time + C.cm.artificialFrameTime, mk2((float)nx + pr.subPixel.x, (float)ny + pr.subPixel.y), rd.lensSample)
+            : shifted_default();
+    }
+}
+
+// ============================================================ temporal resampling
+__device__ __forceinline__ float bilinear_confidence(const DevCtx& C, const float2* mvec, const ResPlanes& prev,
+                                                     uint32_t x, uint32_t y, float newConfidence, bool useConf)
+{
+    f2 prevPixel = prev_pixel_from_mvec(C, mvec, x, y);
+    int tlx = (int)f_floor(prevPixel.x), tly = (int)f_floor(prevPixel.y);
+    f2 frac = mk2(f_saturate(prevPixel.x - (float)tlx), f_saturate(prevPixel.y - (float)tly));
+    for (int ox = 0; ox < 2; ox++)
+        for (int oy = 0; oy < 2; oy++)
+        {
+            int nx = tlx + ox, ny = tly + oy;
+            if (!valid_int(C, nx, ny)) continue;
+            float bw = f_lerp((float)(1 - ox), (float)ox, frac.x) * f_lerp((float)(1 - oy), (float)oy, frac.y);
+            newConfidence += bw * (useConf ? load_confidence(prev, (uint32_t)ny * C.W + (uint32_t)nx) : 1.f);
+        }
+    return f_min(kConfidenceCap, newConfidence);
+}
+
+__device__ __forceinline__ void write_color(float4* color, uint32_t i, const Res& r)
+{
+    if (!color) return;
+    f3 c = r.integrand * res_ucw(r); // ResolveReSTIR.cs.slang:45-63
+    color[i] = make_float4(c.x, c.y, c.z, 1.f);
+}
+
+// ScatterTemporalResampling.rt.slang:65-174
+__global__ void __launch_bounds__(128) k_scatter_resample(DevCtx C, const float2* __restrict__ mvec, ResPlanes prev, RecPlanes prevRec,
+                                                          ResPlanes curr, RecPlanes currRec, const uint32_t* __restrict__ counts,
+                                                          const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ sorted,
+                                                          float4* __restrict__ color)
+{
+    uint32_t ri = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ri >= C.W * C.H) return;
+    uint32_t x = ri % C.W, y = ri / C.W;
+    const bool useConf = C.useConfTemporal != 0;
+    SampleGen sg = sg_create(x, y, pass_seed(C, 5), C.sgKind);
+    Res dst = res_default();
+    Recon dstR = recon_default();
+    Res cr = load_res_rw(curr, ri);
+    Recon crd = load_rec_rw(currRec, ri);
+    float currSampleMIS = 1.f;
+    if (any_gt0(cr.integrand))
+    {
+        float m1 = luminance(cr.integrand) * (useConf ? cr.confidence : 1.f);
+        Shifted sc = dev_scatter_shift(C, sg, crd, crd.time + C.cm.artificialFrameTime, crd.firstHit, crd.lensSample, false);
+        float sj = jac_scatter(sc, crd);
+        float m2 = luminance(sc.radiance) * sj;
+        m2 = f_isnan(m2) ? 0.f : m2;
+        int spx = (int)f_floor(sc.fractionalPixel.x), spy = (int)f_floor(sc.fractionalPixel.y);
+        if (valid_int(C, spx, spy)) m2 *= useConf ? load_confidence(prev, (uint32_t)spy * C.W + (uint32_t)spx) : 1.f;
+        else m2 = 0.f;
+        currSampleMIS = (m1 + m2 == 0.f) ? 0.f : m1 / (m1 + m2);
+    }
+    if (res_add_sample(dst, sg, currSampleMIS, cr.integrand, 1.f, cr)) dstR = crd;
+    float newConfidence = dst.confidence;
+    uint32_t n = counts[ri], off = offsets[ri];
+    for (uint32_t i = 0; i < n; i++)
+    {
+        uint32_t si = __ldg(&sorted[off + i]);
+        Res pr = load_res(prev, si);
+        float prevSampleMIS = 0.f;
+        f3 prevPHat = mk3(0.f);
+        float sj = 1.f;
+        Recon prd = load_rec(prevRec, si);
+        if (any_gt0(pr.integrand))
+        {
+            Shifted sp = dev_scatter_shift(C, sg, prd, prd.time, prd.firstHit, prd.lensSample, false);
+            sj = jac_scatter(sp, prd);
+            float m1 = luminance(sp.radiance) * sj * (useConf ? cr.confidence : 1.f);
+            prevPHat = f_isnan(m1) ? mk3(0.f) : sp.radiance;
+            sj = f_isnan(m1) ? 1.f : sj;
+            recon_update(prd, sp);
+            pr.subPixel = prd.subPixel;
+            float m2 = luminance(pr.integrand) * (useConf ? pr.confidence : 1.f);
+            prevSampleMIS = ((m1 + m2) == 0.f) ? 0.f : m2 / (m1 + m2);
+        }
+        if (res_add_sample(dst, sg, prevSampleMIS, prevPHat, sj, pr)) dstR = prd;
+    }
+    dst.confidence = bilinear_confidence(C, mvec, prev, x, y, newConfidence, useConf);
+    store_res(curr, ri, dst);
+    store_rec(currRec, ri, dstR);
+    write_color(color, ri, dst);
+}
+
+// ScatterBackupTemporalResampling.rt.slang:69-283.  With the Clamped gather the backup
+// reservoir is read straight from the previous frame at round(prevPixel) (the collect pass
+// is fused in); otherwise it comes from the collect pass's intermediate buffers.
+template <bool FusedClamped>
+__device__ __forceinline__ void scatter_backup_body(const DevCtx& C, const float2* __restrict__ mvec, ResPlanes prev, RecPlanes prevRec,
+                                                    ResPlanes curr, RecPlanes currRec, ResPlanes inter, RecPlanes interRec,
+                                                    const float2* __restrict__ floatingCoords, const uint32_t* __restrict__ counts,
+                                                    const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ sorted,
+                                                    float4* __restrict__ color)
+{
+    uint32_t ri = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ri >= C.W * C.H) return;
+    uint32_t x = ri % C.W, y = ri / C.W;
+    const bool useConf = C.useConfTemporal != 0;
+    const bool balance = C.scatterBackupMIS == 0u;
+    SampleGen sg = sg_create(x, y, pass_seed(C, 6), C.sgKind);
+    Res dst = res_default();
+    Recon dstR = recon_default();
+    Res cr = load_res_rw(curr, ri);
+    Recon crd = load_rec_rw(currRec, ri);
+    Res br;
+    Recon brd;
+    f2 floatingCoord;
+    if (FusedClamped)
+    {
+        // CollectTemporalSamples.cs.slang:84-99, 143-156
+        br = res_default();
+        brd = recon_default();
+        f2 prevPixel = prev_pixel_from_mvec(C, mvec, x, y);
+        floatingCoord = mk2(-1.f, -1.f);
+        if (valid_float(C, prevPixel))
+        {
+            float rx = f_round(prevPixel.x), ry = f_round(prevPixel.y);
+            floatingCoord = mk2(rx, ry);
+            if (valid_int(C, (int)rx, (int)ry))
+            {
+                uint32_t pi = (uint32_t)ry * C.W + (uint32_t)rx;
+                br = load_res(prev, pi);
+                brd = load_rec(prevRec, pi);
+            }
+            if (f_isnan(br.totalWeight))
+            {
+                br.integrand = mk3(0.f); br.totalWeight = 0.f;
+                brd.subPixelJacobian = 1.f; brd.lensVertexJacobian = 1.f; brd.secondaryPathJacobian = 1.f; brd.pathLength = 0;
+            }
+        }
+    }
+    else
+    {
+        br = load_res(inter, ri);
+        brd = load_rec(interRec, ri);
+        float2 fc = __ldg(&floatingCoords[ri]);
+        floatingCoord = mk2(fc.x, fc.y);
+    }
+    const float misScale = balance ? 1.f : 0.5f;
+    {
+        float currSampleMIS = 1.f;
+        if (any_gt0(cr.integrand))
+        {
+            float m1 = luminance(cr.integrand) * (useConf ? cr.confidence : 1.f);
+            Shifted sc = dev_scatter_shift(C, sg, crd, crd.time + C.cm.artificialFrameTime, crd.firstHit, crd.lensSample, false);
+            float scj = jac_scatter(sc, crd);
+            float m2 = luminance(sc.radiance) * scj;
+            m2 = f_isnan(m2) ? 0.f : m2;
+            int spx = (int)f_floor(sc.fractionalPixel.x), spy = (int)f_floor(sc.fractionalPixel.y);
+            if (valid_int(C, spx, spy)) m2 *= 0.5f * (useConf ? load_confidence(prev, (uint32_t)spy * C.W + (uint32_t)spx) : 1.f);
+            else m2 = 0.f;
+            float m3 = 0.f;
+            if (valid_float(C, floatingCoord))
+            {
+                Shifted gc = dev_gather_lens_copy(C, sg, crd, crd.time + C.cm.artificialFrameTime, floatingCoord + cr.subPixel, crd.lensSample);
+                float gj = gc.secondaryPathJacobian / crd.secondaryPathJacobian;
+                m3 = luminance(gc.radiance) * gj * 0.5f * (useConf ? br.confidence : 1.f);
+            }
+            m3 = f_isnan(m3) ? 0.f : m3;
+            if (balance) currSampleMIS = (m1 + m2 + m3 == 0.f) ? 0.f : m1 / (m1 + m2 + m3);
+            else currSampleMIS = 0.5f * (((m1 + m2 == 0.f) ? 0.f : 0.5f * m1 / (0.5f * m1 + m2)) +
+                                         ((m1 + m3 == 0.f) ? 0.f : 0.5f * m1 / (0.5f * m1 + m3)));
+        }
+        if (res_add_sample(dst, sg, currSampleMIS, cr.integrand, 1.f, cr)) dstR = crd;
+    }
+    {
+        float backupSampleMIS = 0.f;
+        f3 backupPHat = mk3(0.f);
+        float sj = 1.f;
+        if (any_gt0(br.integrand))
+        {
+            Shifted sb = dev_gather_lens_copy(C, sg, brd, brd.time, mk2((float)x + br.subPixel.x, (float)y + br.subPixel.y), brd.lensSample);
+            sj = sb.secondaryPathJacobian / brd.secondaryPathJacobian;
+            float m1 = luminance(sb.radiance) * sj * (useConf ? cr.confidence : 1.f);
+            backupPHat = f_isnan(m1) ? mk3(0.f) : sb.radiance;
+            sj = f_isnan(m1) ? 1.f : sj;
+            m1 = f_isnan(m1) ? 0.f : m1;
+            recon_update(brd, sb);
+            float m2 = 0.f;
+            if (balance)
+            {
+                Shifted ss = dev_scatter_shift(C, sg, brd, brd.time + C.cm.artificialFrameTime, brd.firstHit, brd.lensSample, false);
+                float scj = jac_scatter(ss, brd);
+                m2 = luminance(ss.radiance) * scj * sj;
+                m2 = f_isnan(m2) ? 0.f : m2;
+                int spx = (int)f_floor(ss.fractionalPixel.x), spy = (int)f_floor(ss.fractionalPixel.y);
+                if (valid_int(C, spx, spy)) m2 *= 0.5f * (useConf ? load_confidence(prev, (uint32_t)spy * C.W + (uint32_t)spx) : 1.f);
+                else m2 = 0.f;
+            }
+            float m3 = luminance(br.integrand) * 0.5f * (useConf ? br.confidence : 1.f);
+            backupSampleMIS = misScale * ((m1 + m2 + m3 == 0.f) ? 0.f : m3 / (misScale * m1 + m2 + m3));
+        }
+        if (res_add_sample(dst, sg, backupSampleMIS, backupPHat, sj, br)) dstR = brd;
+    }
+    float newConfidence = dst.confidence;
+    uint32_t n = counts[ri], off = offsets[ri];
+    for (uint32_t i = 0; i < n; i++)
+    {
+        uint32_t si = __ldg(&sorted[off + i]);
+        Res pr = load_res(prev, si);
+        float prevSampleMIS = 0.f;
+        f3 prevPHat = mk3(0.f);
+        float scj = 1.f;
+        Recon prd = load_rec(prevRec, si);
+        if (any_gt0(pr.integrand))
+        {
+            Shifted sp = dev_scatter_shift(C, sg, prd, prd.time, prd.firstHit, prd.lensSample, true);
+            scj = jac_scatter(sp, prd);
+            float m1 = luminance(sp.radiance) * scj * (useConf ? cr.confidence : 1.f);
+            m1 = f_isnan(m1) ? 0.f : m1;
+            prevPHat = sp.radiance; // the NaN test above already cleared m1 (ScatterBackupTemporalResampling.rt.slang:224-226)
+            recon_update(prd, sp);
+            pr.subPixel = prd.subPixel;
+            float m2 = luminance(pr.integrand) * 0.5f * (useConf ? pr.confidence : 1.f);
+            float m3 = 0.f;
+            if (balance)
+            {
+                f2 fp = floatingCoord + pr.subPixel;
+                if (valid_float(C, fp))
+                {
+                    Shifted gp = dev_gather_lens_copy(C, sg, prd, prd.time + C.cm.artificialFrameTime, fp, prd.lensSample);
+                    float gj = gp.secondaryPathJacobian / prd.secondaryPathJacobian;
+                    m3 = luminance(gp.radiance) * gj * scj * 0.5f * (useConf ? br.confidence : 1.f);
+                }
+                m3 = f_isnan(m3) ? 0.f : m3;
+            }
+            prevSampleMIS = misScale * ((m1 + m2 + m3 == 0.f) ? 0.f : m2 / (misScale * m1 + m2 + m3));
+        }
+        if (res_add_sample(dst, sg, prevSampleMIS, prevPHat, scj, pr)) dstR = prd;
+    }
+    dst.confidence = bilinear_confidence(C, mvec, prev, x, y, newConfidence, useConf);
+    store_res(curr, ri, dst);
+    store_rec(currRec, ri, dstR);
+    write_color(color, ri, dst);
+}
+__global__ void __launch_bounds__(128) k_scatter_backup_resample_clamped(DevCtx C, const float2* __restrict__ mvec, ResPlanes prev, RecPlanes prevRec,
+                                                                         ResPlanes curr, RecPlanes currRec, const uint32_t* __restrict__ counts,
+                                                                         const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ sorted,
+                                                                         float4* __restrict__ color)
+{
+    scatter_backup_body<true>(C, mvec, prev, prevRec, curr, currRec, prev, prevRec, nullptr, counts, offsets, sorted, color);
+}
+__global__ void __launch_bounds__(128) k_scatter_backup_resample(DevCtx C, const float2* __restrict__ mvec, ResPlanes prev, RecPlanes prevRec,
+                                                                 ResPlanes curr, RecPlanes currRec, ResPlanes inter, RecPlanes interRec,
+                                                                 const float2* __restrict__ floatingCoords, const uint32_t* __restrict__ counts,
+                                                                 const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ sorted,
+                                                                 float4* __restrict__ color)
+{
+    scatter_backup_body<false>(C, mvec, prev, prevRec, curr, currRec, inter, interRec, floatingCoords, counts, offsets, sorted, color);
+}
+
+// Depth-of-field shift probabilities of a pixel (ShiftMapping.slang:43-80; GatherTemporalResampling.rt.slang:75-96)
+__device__ __forceinline__ f2 pixel_dof_probs(const DevCtx& C, const uint4* vbuffer, uint32_t i)
+{
+    if (!(C.camera.apertureRadius > 0.f)) return mk2(1.f, 0.f);
+    uint4 q = __ldg(&vbuffer[i]);
+    HitInfo h; h.w[0] = q.x; h.w[1] = q.y; h.w[2] = q.z; h.w[3] = q.w;
+    const CameraData& cam = C.camera;
+    float normalizedFilm = length(cam.cameraU / (float)C.W + cam.cameraV / (float)C.H);
+    float coc;
+    if (hit_valid(h))
+    {
+        f3 x1 = dev_sd(C, h, mk3(0.f)).posW;
+        f3 camDir = normalize(cam.cameraW);
+        float camZ = dot(x1 - cam.posW, camDir);
+        float filmZ = camZ - length(cam.cameraW);
+        float filmRadius = f_abs(cam.apertureRadius / camZ * filmZ);
+        coc = filmRadius / normalizedFilm;
+    }
+    else coc = cam.apertureRadius / normalizedFilm;
+    float gamma = 0.2f + 6.2f / (coc - 5.6f);
+    gamma = (coc <= 0.2f) ? 1.f : f_clamp(gamma, 0.2f, 1.f);
+    return mk2(gamma, 1.f - gamma);
+}
+
+// GatherTemporalResampling.rt.slang:68-235
+__global__ void __launch_bounds__(128) k_gather_resample(DevCtx C, const uint4* __restrict__ vbuffer, ResPlanes curr, RecPlanes currRec,
+                                                         ResPlanes inter, RecPlanes interRec, const float2* __restrict__ floatingCoords,
+                                                         float4* __restrict__ color)
+{
+    uint32_t ri = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ri >= C.W * C.H) return;
+    uint32_t x = ri % C.W, y = ri / C.W;
+    const bool useConf = C.useConfTemporal != 0;
+    SampleGen sg = sg_create(x, y, pass_seed(C, 3), C.sgKind);
+    const bool hasDoF = C.camera.apertureRadius > 0.f;
+    f2 probs = pixel_dof_probs(C, vbuffer, ri);
+    const bool doLensCopy = probs.x > 0.f;
+    const bool doPrimaryReconnect = probs.y > 0.f;
+    Res dst = res_default();
+    Recon dstR = recon_default();
+    float2 fcv = __ldg(&floatingCoords[ri]);
+    f2 floatingCoord = mk2(fcv.x, fcv.y);
+    Res currIn = load_res_rw(curr, ri);
+    Recon currInR = load_rec_rw(currRec, ri);
+    for (int stage = 0; stage < 2; stage++)
+    {
+        bool lens = stage == 0;
+        if (lens && !doLensCopy) continue;
+        if (!lens && !(hasDoF && doPrimaryReconnect)) continue;
+        float prob = lens ? probs.x : probs.y;
+        Res pr = load_res(inter, ri);
+        Recon prd = load_rec(interRec, ri);
+        Res cr = (lens || !doLensCopy) ? currIn : dst;
+        Recon crd = (lens || !doLensCopy) ? currInR : dstR;
+        if (!lens) { dst = res_default(); dstR = recon_default(); }
+        float currSampleMIS = 0.f;
+        f3 currPHat = mk3(0.f);
+        if (any_gt0(cr.integrand))
+        {
+            float m1 = luminance(cr.integrand) * (useConf ? cr.confidence : 1.f);
+            currPHat = cr.integrand;
+            Shifted sc = lens ? dev_gather_lens_copy(C, sg, crd, crd.time + C.cm.artificialFrameTime, floatingCoord + cr.subPixel, crd.lensSample)
+                              : dev_gather_primary_reconnect(C, sg, crd, crd.time + C.cm.artificialFrameTime, floatingCoord + cr.subPixel, crd.firstHit);
+            float sj = lens ? sc.secondaryPathJacobian / crd.secondaryPathJacobian
+                            : (sc.lensVertexJacobian * sc.secondaryPathJacobian) / (crd.lensVertexJacobian * crd.secondaryPathJacobian);
+            float m2 = luminance(sc.radiance) * sj * (useConf ? pr.confidence : 1.f) * prob;
+            m2 = f_isnan(m2) ? 0.f : m2;
+            currSampleMIS = (m1 + m2 == 0.f) ? 0.f : m1 / (m1 + m2);
+        }
+        if (res_add_sample(dst, sg, currSampleMIS, currPHat, 1.f, cr)) dstR = crd;
+        float prevSampleMIS = 0.f;
+        f3 prevPHat = mk3(0.f);
+        float sj = 1.f;
+        if (any_gt0(pr.integrand))
+        {
+            f2 fp = mk2((float)x + pr.subPixel.x, (float)y + pr.subPixel.y);
+            Shifted sp = lens ? dev_gather_lens_copy(C, sg, prd, prd.time, fp, prd.lensSample)
+                              : dev_gather_primary_reconnect(C, sg, prd, prd.time, fp, prd.firstHit);
+            sj = lens ? sp.secondaryPathJacobian / prd.secondaryPathJacobian
+                      : (sp.lensVertexJacobian * sp.secondaryPathJacobian) / (prd.lensVertexJacobian * prd.secondaryPathJacobian);
+            float m1 = luminance(sp.radiance) * sj * (useConf ? cr.confidence : 1.f);
+            prevPHat = f_isnan(m1) ? mk3(0.f) : sp.radiance;
+            sj = f_isnan(m1) ? 1.f : sj;
+            m1 = f_isnan(m1) ? 0.f : m1;
+            recon_update(prd, sp);
+            float m2 = luminance(pr.integrand) * (useConf ? pr.confidence : 1.f) * prob;
+            prevSampleMIS = ((m1 + m2) == 0.f) ? 0.f : m2 / (m1 + m2);
+        }
+        if (res_add_sample(dst, sg, prevSampleMIS, prevPHat, sj, pr)) dstR = prd;
+    }
+    store_res(curr, ri, dst);
+    store_rec(currRec, ri, dstR);
+    write_color(color, ri, dst);
+}
+
+// MultiScatterTemporalResampling.rt.slang:65-186
+__global__ void __launch_bounds__(128) k_multi_scatter_resample(DevCtx C, const float2* __restrict__ mvec, ResPlanes prev, RecPlanes prevRec,
+                                                                ResPlanes curr, RecPlanes currRec, const uint32_t* __restrict__ counts,
+                                                                const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ sortedAll,
+                                                                float4* __restrict__ color)
+{
+    uint32_t ri = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t N = C.W * C.H;
+    if (ri >= N) return;
+    uint32_t x = ri % C.W, y = ri / C.W;
+    const bool useConf = C.useConfTemporal != 0;
+    const uint32_t P = C.numTimePartitions;
+    SampleGen sg = sg_create(x, y, pass_seed(C, 5), C.sgKind);
+    Res dst = res_default();
+    Recon dstR = recon_default();
+    float timePartitions = C.camera.shutterSpeed / (float)P;
+    float jacobianScale = 1.f / (float)P;
+    Res cr = load_res_rw(curr, ri);
+    Recon crd = load_rec_rw(currRec, ri);
+    float currSampleMIS = 1.f;
+    if (any_gt0(cr.integrand))
+    {
+        float m1 = luminance(cr.integrand) * (useConf ? cr.confidence : 1.f);
+        float fractionalTime = (crd.time - f_floor(crd.time / timePartitions) * timePartitions) / timePartitions;
+        float shiftedTime = fractionalTime * C.camera.shutterSpeed;
+        Shifted sc = dev_scatter_shift(C, sg, crd, shiftedTime + C.cm.artificialFrameTime, crd.firstHit, crd.lensSample, false);
+        float sj = jac_scatter(sc, crd);
+        float m2 = luminance(sc.radiance) * sj;
+        m2 = f_isnan(m2) ? 0.f : m2;
+        int spx = (int)f_floor(sc.fractionalPixel.x), spy = (int)f_floor(sc.fractionalPixel.y);
+        if (valid_int(C, spx, spy)) m2 *= useConf ? load_confidence(prev, (uint32_t)spy * C.W + (uint32_t)spx) : 1.f;
+        else m2 = 0.f;
+        currSampleMIS = (m1 + m2 == 0.f) ? 0.f : m1 / (m1 + m2);
+    }
+    if (res_add_sample(dst, sg, currSampleMIS, cr.integrand, 1.f, cr)) dstR = crd;
+    float newConfidence = dst.confidence;
+    for (uint32_t j = 0; j < P; j++)
+    {
+        uint32_t n = counts[(size_t)j * N + ri], off = offsets[(size_t)j * N + ri];
+        const uint32_t* sorted = sortedAll + (size_t)j * N; // partition j's lists start at j * N
+        for (uint32_t i = 0; i < n; i++)
+        {
+            uint32_t si = __ldg(&sorted[off + i]);
+            Res pr = load_res(prev, si);
+            Recon prd = load_rec(prevRec, si);
+            f3 prevPHat = mk3(0.f);
+            float sj = 1.f;
+            float prevMIS = 0.f;
+            if (any_gt0(pr.integrand))
+            {
+                float fractionalTime = prd.time / C.camera.shutterSpeed;
+                float newTime = (fractionalTime + (float)j) * timePartitions;
+                Shifted sp = dev_scatter_shift(C, sg, prd, newTime, prd.firstHit, prd.lensSample, false);
+                sj = jac_scatter(sp, prd);
+                float m1 = luminance(sp.radiance) * sj * (useConf ? cr.confidence : 1.f);
+                prevPHat = f_isnan(m1) ? mk3(0.f) : sp.radiance;
+                sj = f_isnan(m1) ? 1.f : sj;
+                recon_update(prd, sp);
+                prd.time = newTime;
+                pr.subPixel = prd.subPixel;
+                float m2 = luminance(pr.integrand) * (useConf ? pr.confidence : 1.f);
+                prevMIS = ((m1 + m2) == 0.f) ? 0.f : m2 / (m1 + m2);
+            }
+            if (res_add_sample(dst, sg, prevMIS, prevPHat, sj * jacobianScale, pr)) dstR = prd;
+        }
+    }
+    dst.confidence = bilinear_confidence(C, mvec, prev, x, y, newConfidence, useConf);
+    store_res(curr, ri, dst);
+    store_rec(currRec, ri, dstR);
+    write_color(color, ri, dst);
+}
+
+// ============================================================ spatial resampling
+// SpatialResampling.rt.slang:67-185 (one iteration: src -> dst)
+__global__ void __launch_bounds__(128) k_spatial(DevCtx C, uint32_t iteration, const uint4* __restrict__ vbuffer, const float2* __restrict__ neighborOffsets,
+                                                 ResPlanes src, RecPlanes srcRec, ResPlanes dstP, RecPlanes dstRec, float4* __restrict__ color)
+{
+    uint32_t ri = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ri >= C.W * C.H) return;
+    uint32_t x = ri % C.W, y = ri / C.W;
+    const bool useConf = C.useConfSpatial != 0;
+    const uint32_t neighborCount = C.neighborCount;
+    const uint32_t kSpatialNeighborSamples = 8192;
+    SampleGen sg = sg_create(x, y, C.useFixedSeed ? C.fixedSeed + 7 : kNumRenderPasses * (C.frameCount + C.seed) + 1337u * iteration + 7u, C.sgKind);
+    f2 probs = pixel_dof_probs(C, vbuffer, ri);
+    const uint32_t numLensCopy = (uint32_t)f_round(probs.x * (float)neighborCount);
+    Res cent = load_res(src, ri);
+    Recon centR = load_rec(srcRec, ri);
+    float centralSampleMIS = 1.f;
+    float centralWeight = luminance(cent.integrand) / (float)neighborCount * (useConf ? cent.confidence : 1.f);
+    Res dst = res_default();
+    Recon dstR = recon_default();
+    int validNeighbors = 0;
+    uint32_t startIdx = (uint32_t)(sampleNext1D(sg) * (float)kSpatialNeighborSamples);
+    for (uint32_t i = 0; i < neighborCount; i++)
+    {
+        bool lensCopy = (i < numLensCopy);
+        float2 off = __ldg(&neighborOffsets[(startIdx + i) % kSpatialNeighborSamples]);
+        int nx = (int)f_round((float)x + C.spatialGatherRadius * off.x);
+        int ny = (int)f_round((float)y + C.spatialGatherRadius * off.y);
+        if (!valid_int(C, nx, ny)) continue;
+        validNeighbors += 1;
+        uint32_t ni = (uint32_t)ny * C.W + (uint32_t)nx;
+        Res nr = load_res(src, ni);
+        Recon nrd = load_rec(srcRec, ni);
+        float m1 = 0.f;
+        if (any_gt0(cent.integrand))
+        {
+            f2 fp = mk2((float)nx + cent.subPixel.x, (float)ny + cent.subPixel.y);
+            Shifted sc = lensCopy ? dev_gather_lens_copy(C, sg, centR, centR.time, fp, centR.lensSample)
+                                  : dev_gather_primary_reconnect(C, sg, centR, centR.time, fp, centR.firstHit);
+            float sj = (lensCopy ? 1.f : (sc.lensVertexJacobian / centR.lensVertexJacobian)) * (sc.secondaryPathJacobian / centR.secondaryPathJacobian);
+            m1 = luminance(sc.radiance) * sj * (useConf ? nr.confidence : 1.f);
+            m1 = f_isnan(m1) ? 0.f : m1;
+        }
+        centralSampleMIS += 1.f;
+        centralSampleMIS -= (m1 + centralWeight > 0.f) ? m1 / (m1 + centralWeight) : 0.f;
+        float neighborSampleMIS = 0.f;
+        f3 neighborPHat = mk3(0.f);
+        float sj = 1.f;
+        if (any_gt0(nr.integrand))
+        {
+            f2 fp = mk2((float)x + nr.subPixel.x, (float)y + nr.subPixel.y);
+            Shifted sn = lensCopy ? dev_gather_lens_copy(C, sg, nrd, nrd.time, fp, nrd.lensSample)
+                                  : dev_gather_primary_reconnect(C, sg, nrd, nrd.time, fp, nrd.firstHit);
+            sj = (lensCopy ? 1.f : (sn.lensVertexJacobian / nrd.lensVertexJacobian)) * (sn.secondaryPathJacobian / nrd.secondaryPathJacobian);
+            float nw = luminance(sn.radiance) * sj * (useConf ? cent.confidence : 1.f);
+            neighborPHat = f_isnan(nw) ? mk3(0.f) : sn.radiance;
+            sj = f_isnan(nw) ? 1.f : sj;
+            nw = f_isnan(nw) ? 0.f : nw / (float)neighborCount;
+            recon_update(nrd, sn);
+            float m2 = luminance(nr.integrand) * (useConf ? nr.confidence : 1.f);
+            neighborSampleMIS = (m2 + nw > 0.f) ? m2 / (nw + m2) : 0.f;
+        }
+        if (res_add_sample(dst, sg, neighborSampleMIS, neighborPHat, sj, nr)) dstR = nrd;
+    }
+    if (res_add_sample(dst, sg, centralSampleMIS, cent.integrand, 1.f, cent)) dstR = centR;
+    dst.totalWeight /= (float)(validNeighbors + 1);
+    store_res(dstP, ri, dst);
+    store_rec(dstRec, ri, dstR);
+    write_color(color, ri, dst);
+}
+
+// ResolveReSTIR.cs.slang:45-63 (used when no resampling kernel wrote the colour)
+__global__ void __launch_bounds__(256) k_resolve(uint32_t n, ResPlanes curr, float4* __restrict__ color)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Res r = load_res(curr, i);
+    write_color(color, i, r);
+}
+
+} // namespace rs

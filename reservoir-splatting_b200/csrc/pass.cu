@@ -1,0 +1,734 @@
+// Host side of the B200 Reservoir Splatting pass behind the C ABI of
+// include/rs_b200.h: option parsing and validation, scene upload and LBVH build,
+// per-frame orchestration (ReservoirSplatting::execute, ReservoirSplatting.cpp:399-509),
+// buffer ping-pong (endFrame, :1648-1680) and the parity/checkpoint views.
+//
+// All device work of rs_execute is issued on the caller's stream with no host
+// synchronisation and no allocation once the frame size and options are stable,
+// so a frame can be captured into a CUDA graph after the first call.
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+#include <memory>
+#include "../../include/rs_b200.h"
+#include "kernels.h"
+#include "bvh_build.h"
+#include "core/scene_prep.h"
+
+using namespace rs;
+
+static thread_local std::string g_lastError;
+
+static rs_status fail(rs_status s, const std::string& msg)
+{
+    g_lastError = msg;
+    return s;
+}
+
+#define RS_CUDA(call)                                                                               \
+    do {                                                                                            \
+        cudaError_t e_ = (call);                                                                    \
+        if (e_ != cudaSuccess)                                                                      \
+            return fail(e_ == cudaErrorMemoryAllocation ? RS_OOM : RS_CUDA_ERROR,                   \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));                      \
+    } while (0)
+
+namespace {
+
+template <typename T>
+struct DevBuf
+{
+    T* p = nullptr;
+    size_t n = 0;
+    ~DevBuf() { release(); }
+    void release() { if (p) cudaFree(p); p = nullptr; n = 0; }
+    cudaError_t ensure(size_t count)
+    {
+        if (count <= n && p) return cudaSuccess;
+        release();
+        if (count == 0) return cudaSuccess;
+        cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+        if (e == cudaSuccess) n = count;
+        return e;
+    }
+};
+
+struct ReservoirSet
+{
+    DevBuf<float4> a, b;     // reservoir planes
+    DevBuf<uint4> rec;       // 7 reconnection planes
+    size_t N = 0;
+    cudaError_t ensure(size_t n)
+    {
+        N = n;
+        cudaError_t e;
+        if ((e = a.ensure(n)) != cudaSuccess) return e;
+        if ((e = b.ensure(n)) != cudaSuccess) return e;
+        return rec.ensure(7 * n);
+    }
+    ResPlanes res() const { return ResPlanes{a.p, b.p}; }
+    RecPlanes recp() const { return RecPlanes{rec.p, N}; }
+};
+
+} // namespace
+
+struct rs_pass
+{
+    rs_options opt;
+    // scene
+    PreparedScene scene;
+    DevBuf<float4> dTri, dNodes;
+    DevBuf<MaterialData> dMaterials;
+    DevBuf<LightTriangle> dLights;
+    DevBuf<u2> dAlias;
+    uint32_t bvhRoot = 0;
+    bool hasScene = false;
+    // frame state
+    uint32_t W = 0, H = 0;
+    uint32_t frameCount = 0, seed = 0;
+    bool frozen = false, swapped = false;
+    uint32_t K = 2, prevK = 0;
+    CameraManager cm;
+    CameraData camera, prevCamera;
+    bool havePrevCamera = false;
+    // buffers
+    ReservoirSet sets[3];
+    int currIdx = 0, prevIdx = 1, tempIdx = 2;
+    ReservoirSet inter, cand;
+    DevBuf<float2> mvec, floatingCoords, neighborOffsets;
+    DevBuf<uint4> vbuffer;
+    DevBuf<uint32_t> targets, counts, offsets, cursor, unsortedSplats, sortedSplats, tileSums, total;
+    DevBuf<Shifted> shiftedPaths;
+    DevBuf<float4> scratchColor;
+    DevBuf<uint32_t> fault;
+    uint32_t* hostFault = nullptr;
+    bool keepCandidates = false;
+    bool lastFusedCollect = false;
+    cudaStream_t lastStream = 0;
+    uint32_t launches = 0;
+    // stage timing
+    bool timing = false;
+    std::vector<std::string> stageNames;
+    std::vector<cudaEvent_t> events;
+    std::vector<float> stageMs;
+
+    ~rs_pass()
+    {
+        for (auto e : events) cudaEventDestroy(e);
+        if (hostFault) cudaFreeHost(hostFault);
+    }
+};
+
+// ------------------------------------------------------------------ options
+extern "C" RS_API void rs_default_options(rs_options* o)
+{
+    // ReservoirSplatting.h:124-184 defaults
+    memset(o, 0, sizeof(*o));
+    o->samplesPerPixel = 1;
+    o->maxSurfaceBounces = 9; o->maxDiffuseBounces = 9; o->maxSpecularBounces = 9; o->maxTransmissionBounces = 9;
+    o->sampleGenerator = RS_SG_TINY_UNIFORM;
+    o->useFixedSeed = 0; o->fixedSeed = 1;
+    o->useRussianRoulette = 1;
+    o->misHeuristic = RS_MIS_HEURISTIC_BALANCE;
+    o->misPowerExponent = 2.f;
+    o->disableCaustics = 0;
+    o->specularRoughnessThreshold = 0.25f;
+    o->enableTemporalResampling = 1;
+    o->enableSpatialResampling = 1;
+    o->temporalReuse = RS_GATHER_ONLY;
+    o->scatterBackupMISOption = RS_MIS_BALANCE;
+    o->gatherOption = RS_GATHER_FAST;
+    o->numTimePartitions = 2;
+    o->useConfidenceWeightsTemporally = 1;
+    o->numSpatialIterations = 1;
+    o->spatialGatherRadius = 30.f;
+    o->neighborCount = 1;
+    o->useConfidenceWeightsSpatially = 1;
+    o->artificialFrameTime = 1.f / 60.f;
+    o->frameWidth = 1920; o->frameHeight = 1080;
+}
+
+// validateOptions (ReservoirSplatting.cpp:263-301): out-of-range values are rejected here
+// (the reference clamps with a warning; a C caller gets RS_INVALID_ARG and the reason).
+static rs_status validate(const rs_options* o)
+{
+    if (!o) return fail(RS_INVALID_ARG, "options is NULL");
+    if (o->samplesPerPixel < 1 || o->samplesPerPixel > 16) return fail(RS_INVALID_ARG, "samplesPerPixel must be in [1, 16]");
+    if (o->maxSurfaceBounces > 254 || o->maxDiffuseBounces > 254 || o->maxSpecularBounces > 254 || o->maxTransmissionBounces > 254)
+        return fail(RS_INVALID_ARG, "bounce limits must be <= 254");
+    if (o->frameWidth == 0 || o->frameHeight == 0 || o->frameWidth > 4096 || o->frameHeight > 4096)
+        return fail(RS_INVALID_ARG, "Frame dimensions up to 4096 pixels width/height are supported");
+    if (o->sampleGenerator != RS_SG_TINY_UNIFORM && o->sampleGenerator != RS_SG_PCG32) return fail(RS_INVALID_ARG, "unknown sampleGenerator");
+    if (o->misHeuristic > 1) return fail(RS_INVALID_ARG, "misHeuristic must be Balance or PowerTwo");
+    if (o->temporalReuse > 3) return fail(RS_INVALID_ARG, "unknown temporalReuse");
+    if (o->gatherOption > 2) return fail(RS_INVALID_ARG, "unknown gatherOption");
+    if (o->scatterBackupMISOption > 1) return fail(RS_INVALID_ARG, "unknown scatterBackupMISOption");
+    if (o->numTimePartitions < 1 || o->numTimePartitions > 8) return fail(RS_INVALID_ARG, "numTimePartitions must be in [1, 8]");
+    if (o->enableSpatialResampling && (o->neighborCount < 1 || o->numSpatialIterations < 1)) return fail(RS_INVALID_ARG, "spatial reuse needs neighborCount and numSpatialIterations >= 1");
+    if (!(o->artificialFrameTime > 0.f)) return fail(RS_INVALID_ARG, "artificialFrameTime must be > 0");
+    if (o->specularRoughnessThreshold < 0.f || o->specularRoughnessThreshold > 1.f) return fail(RS_INVALID_ARG, "specularRoughnessThreshold must be in [0, 1]");
+    return RS_OK;
+}
+
+static rs_status allocate(rs_pass* p)
+{
+    const size_t N = (size_t)p->opt.frameWidth * p->opt.frameHeight;
+    const size_t P = p->opt.temporalReuse == RS_MULTI_SCATTER ? p->opt.numTimePartitions : 1;
+    p->W = p->opt.frameWidth; p->H = p->opt.frameHeight;
+    for (auto& s : p->sets) RS_CUDA(s.ensure(N));
+    const bool needInter = p->opt.temporalReuse == RS_GATHER_ONLY || p->opt.temporalReuse == RS_SCATTER_BACKUP;
+    if (needInter) RS_CUDA(p->inter.ensure(N));
+    RS_CUDA(p->mvec.ensure(N));
+    RS_CUDA(p->floatingCoords.ensure(N));
+    RS_CUDA(p->vbuffer.ensure(N));
+    RS_CUDA(p->targets.ensure(P * N));
+    RS_CUDA(p->counts.ensure(P * N));
+    RS_CUDA(p->offsets.ensure(P * N));
+    RS_CUDA(p->cursor.ensure(P * N));
+    RS_CUDA(p->unsortedSplats.ensure(P * N));
+    RS_CUDA(p->sortedSplats.ensure(P * N));
+    RS_CUDA(p->tileSums.ensure((N + kScanTileElems - 1) / kScanTileElems + 1));
+    RS_CUDA(p->total.ensure(8));
+    if (p->opt.gatherOption == RS_GATHER_ROBUST && needInter) RS_CUDA(p->shiftedPaths.ensure(8 * N));
+    RS_CUDA(p->fault.ensure(1));
+    if (!p->hostFault) RS_CUDA(cudaMallocHost(&p->hostFault, sizeof(uint32_t)));
+    if (!p->neighborOffsets.p)
+    {
+        // createNeighborOffsetTexture (ReservoirSplatting.cpp:1072-1097), decoded as RG8Snorm
+        const uint32_t sampleCount = 8192;
+        std::vector<int8_t> off(sampleCount * 2);
+        const int R = 254;
+        const float phi2 = 1.f / 1.3247179572447f;
+        float u = 0.5f, v = 0.5f;
+        for (uint32_t index = 0; index < sampleCount * 2;)
+        {
+            u += phi2;
+            v += phi2 * phi2;
+            if (u >= 1.f) u -= 1.f;
+            if (v >= 1.f) v -= 1.f;
+            float rSq = (u - 0.5f) * (u - 0.5f) + (v - 0.5f) * (v - 0.5f);
+            if (rSq > 0.25f) continue;
+            off[index++] = (int8_t)((u - 0.5f) * (float)R);
+            off[index++] = (int8_t)((v - 0.5f) * (float)R);
+        }
+        std::vector<float2> dec(sampleCount);
+        for (uint32_t i = 0; i < sampleCount; i++)
+        {
+            float a = (float)off[2 * i] / 127.f, b = (float)off[2 * i + 1] / 127.f;
+            dec[i] = make_float2(a < -1.f ? -1.f : a, b < -1.f ? -1.f : b);
+        }
+        RS_CUDA(p->neighborOffsets.ensure(sampleCount));
+        RS_CUDA(cudaMemcpy(p->neighborOffsets.p, dec.data(), sampleCount * sizeof(float2), cudaMemcpyHostToDevice));
+    }
+    return RS_OK;
+}
+
+extern "C" RS_API rs_status rs_create(const rs_options* opts, rs_pass** out)
+{
+    if (!out) return fail(RS_INVALID_ARG, "out is NULL");
+    rs_status s = validate(opts);
+    if (s != RS_OK) return s;
+    std::unique_ptr<rs_pass> p(new rs_pass());
+    p->opt = *opts;
+    s = allocate(p.get());
+    if (s != RS_OK) return s;
+    *out = p.release();
+    return RS_OK;
+}
+
+extern "C" RS_API rs_status rs_destroy(rs_pass* p)
+{
+    if (!p) return fail(RS_INVALID_ARG, "pass is NULL");
+    cudaDeviceSynchronize();
+    delete p;
+    return RS_OK;
+}
+
+extern "C" RS_API rs_status rs_set_options(rs_pass* p, const rs_options* opts)
+{
+    if (!p) return fail(RS_INVALID_ARG, "pass is NULL");
+    rs_status s = validate(opts);
+    if (s != RS_OK) return s;
+    bool resized = opts->frameWidth != p->opt.frameWidth || opts->frameHeight != p->opt.frameHeight;
+    p->opt = *opts;
+    s = allocate(p);
+    if (s != RS_OK) return s;
+    if (resized) p->frameCount = 0;
+    return RS_OK;
+}
+
+extern "C" RS_API rs_status rs_set_scene(rs_pass* p, const rs_scene_desc* sd)
+{
+    if (!p || !sd) return fail(RS_INVALID_ARG, "pass or scene is NULL");
+    if (sd->numTriangles > 0 && (!sd->positions || !sd->materialIds)) return fail(RS_INVALID_ARG, "scene arrays are NULL");
+    if (sd->numMaterials == 0 || !sd->materials) return fail(RS_INVALID_ARG, "scene has no materials");
+    if (sd->numTriangles >= kLeafBit) return fail(RS_INVALID_ARG, "too many triangles");
+    static_assert(sizeof(rs_material) == sizeof(MaterialData), "material layout");
+    if (!prepare_scene(sd->numTriangles, sd->positions, sd->materialIds, sd->numMaterials,
+                       reinterpret_cast<const MaterialData*>(sd->materials), p->scene))
+        return fail(RS_INVALID_ARG, "material id out of range");
+    const uint32_t n = sd->numTriangles;
+    RS_CUDA(cudaDeviceSynchronize());
+    RS_CUDA(p->dTri.ensure(3ull * (n ? n : 1)));
+    RS_CUDA(p->dMaterials.ensure(sd->numMaterials));
+    RS_CUDA(p->dLights.ensure(p->scene.lights.size() ? p->scene.lights.size() : 1));
+    RS_CUDA(p->dAlias.ensure(p->scene.alias.size() ? p->scene.alias.size() : 1));
+    RS_CUDA(p->dNodes.ensure(4ull * (n > 1 ? n - 1 : 1)));
+    if (n) RS_CUDA(cudaMemcpy(p->dTri.p, p->scene.tri.data(), 48ull * n, cudaMemcpyHostToDevice));
+    RS_CUDA(cudaMemcpy(p->dMaterials.p, p->scene.materials.data(), sizeof(MaterialData) * sd->numMaterials, cudaMemcpyHostToDevice));
+    if (!p->scene.lights.empty())
+    {
+        RS_CUDA(cudaMemcpy(p->dLights.p, p->scene.lights.data(), sizeof(LightTriangle) * p->scene.lights.size(), cudaMemcpyHostToDevice));
+        RS_CUDA(cudaMemcpy(p->dAlias.p, p->scene.alias.data(), sizeof(u2) * p->scene.alias.size(), cudaMemcpyHostToDevice));
+    }
+    cudaStream_t s;
+    RS_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    cudaError_t e = build_lbvh(p->dTri.p, n, p->dNodes.p, &p->bvhRoot, s);
+    cudaStreamDestroy(s);
+    if (e != cudaSuccess) return fail(RS_CUDA_ERROR, std::string("LBVH build: ") + cudaGetErrorString(e));
+    p->hasScene = true;
+    p->frameCount = 0; // setScene resets the frame count (ReservoirSplatting.cpp:380)
+    return RS_OK;
+}
+
+static CameraData to_camera(const rs_camera& c)
+{
+    CameraData d;
+    d.posW = mk3(c.position[0], c.position[1], c.position[2]);
+    d.target = mk3(c.target[0], c.target[1], c.target[2]);
+    d.up = mk3(c.up[0], c.up[1], c.up[2]);
+    d.focalLength = c.focalLength; d.frameHeight = c.frameHeight; d.aspectRatio = c.aspectRatio;
+    d.focalDistance = c.focalDistance; d.apertureRadius = c.apertureRadius; d.shutterSpeed = c.shutterSpeed;
+    d.nearZ = c.nearZ; d.farZ = c.farZ;
+    camera_update_basis(d);
+    return d;
+}
+
+static void stage(rs_pass* p, const char* name, cudaStream_t s)
+{
+    if (!p->timing) return;
+    size_t k = p->stageNames.size();
+    p->stageNames.push_back(name);
+    if (p->events.size() < k + 2)
+    {
+        while (p->events.size() < k + 2)
+        {
+            cudaEvent_t e;
+            cudaEventCreate(&e);
+            p->events.push_back(e);
+        }
+    }
+    cudaEventRecord(p->events[k], s);
+}
+
+extern "C" RS_API rs_status rs_execute(rs_pass* p, const rs_frame_desc* f, void* streamPtr)
+{
+    if (!p || !f) return fail(RS_INVALID_ARG, "pass or frame is NULL");
+    if (!p->hasScene) return fail(RS_NOT_READY, "no scene set");
+    if (!f->color && !f->colorHost) return fail(RS_INVALID_ARG, "no colour output");
+    cudaStream_t s = (cudaStream_t)streamPtr;
+    p->lastStream = s;
+    p->launches = 0;
+    p->stageNames.clear();
+    const uint32_t W = p->W, H = p->H;
+    const uint32_t N = W * H;
+    const rs_options& o = p->opt;
+
+    // beginFrame (ReservoirSplatting.cpp:1550-1646)
+    p->seed = o.useFixedSeed ? o.fixedSeed : p->seed + 1;
+    p->camera = to_camera(f->camera);
+    uint32_t K = 1u + (uint32_t)ceilf(p->camera.shutterSpeed / o.artificialFrameTime) + 1u;
+    if (K > kMaxCameraKeyframes) K = kMaxCameraKeyframes;
+    bool keyframesChanged = K != p->prevK;
+    p->prevK = K;
+    p->K = K;
+    bool shouldReset = f->sceneShouldReset != 0;
+    // prepareCameraManager (:1359-1388)
+    p->cm.artificialFrameTime = o.artificialFrameTime;
+    p->cm.keyframes = K;
+    if (p->frameCount == 0 || shouldReset || keyframesChanged)
+        for (uint32_t i = 0; i < K; i++) { p->cm.positions[i] = p->camera.posW; p->cm.targets[i] = p->camera.target; }
+    else { p->cm.positions[p->frameCount % K] = p->camera.posW; p->cm.targets[p->frameCount % K] = p->camera.target; }
+
+    DevCtx C;
+    memset(&C, 0, sizeof(C));
+    C.bvh.nodes = p->dNodes.p;
+    C.bvh.tri = p->dTri.p;
+    C.bvh.root = p->bvhRoot;
+    C.bvh.numTris = (uint32_t)(p->scene.tri.size() / 3);
+    C.materials = p->dMaterials.p;
+    C.lights.tris = p->dLights.p;
+    C.lights.aliasTable = p->dAlias.p;
+    C.lights.count = (uint32_t)p->scene.lights.size();
+    C.lights.invWeightsSum = p->scene.invWeightsSum;
+    C.camera = p->camera;
+    C.prevCamera = p->havePrevCamera ? p->prevCamera : p->camera;
+    C.cm = p->cm;
+    C.W = W; C.H = H;
+    C.frameCount = p->frameCount; C.seed = p->seed;
+    C.useFixedSeed = o.useFixedSeed; C.fixedSeed = o.fixedSeed;
+    C.sgKind = o.sampleGenerator;
+    C.spp = o.samplesPerPixel;
+    C.maxSurfaceBounces = o.maxSurfaceBounces; C.maxDiffuseBounces = o.maxDiffuseBounces;
+    C.maxSpecularBounces = o.maxSpecularBounces; C.maxTransmissionBounces = o.maxTransmissionBounces;
+    C.useRussianRoulette = o.useRussianRoulette; C.misHeuristic = o.misHeuristic; C.disableCaustics = o.disableCaustics;
+    C.specularRoughnessThreshold = o.specularRoughnessThreshold;
+    C.useConfTemporal = o.useConfidenceWeightsTemporally; C.useConfSpatial = o.useConfidenceWeightsSpatially;
+    C.gatherOption = o.gatherOption; C.scatterBackupMIS = o.scatterBackupMISOption; C.numTimePartitions = o.numTimePartitions;
+    C.neighborCount = o.neighborCount; C.spatialGatherRadius = o.spatialGatherRadius;
+    C.fault = p->fault.p;
+
+    ReservoirSet& curr = p->sets[p->currIdx];
+    ReservoirSet& prev = p->sets[p->prevIdx];
+    float4* colorDev = reinterpret_cast<float4*>(f->color);
+    if (!colorDev)
+    {
+        RS_CUDA(p->scratchColor.ensure(N)); // allocated on the first host-output frame only
+        colorDev = p->scratchColor.p;
+    }
+    auto grid = [](uint32_t n, uint32_t b) { return dim3((n + b - 1) / b); };
+    RS_CUDA(cudaMemsetAsync(p->fault.p, 0, sizeof(uint32_t), s));
+
+    // producer side: primary hits + motion vectors (VBufferRT)
+    stage(p, "vbuffer", s);
+    k_vbuffer<<<grid(N, 256), 256, 0, s>>>(C, p->vbuffer.p, p->mvec.p); p->launches++;
+    const float2* mvec = p->mvec.p;
+    if (f->mvec) mvec = reinterpret_cast<const float2*>(f->mvec);
+
+    stage(p, "initialCandidates", s);
+    k_candidates<<<grid(N, 128), 128, 0, s>>>(C, curr.res(), curr.recp()); p->launches++;
+    if (p->keepCandidates)
+    {
+        RS_CUDA(p->cand.ensure(N));
+        RS_CUDA(cudaMemcpyAsync(p->cand.a.p, curr.a.p, N * 16ull, cudaMemcpyDeviceToDevice, s));
+        RS_CUDA(cudaMemcpyAsync(p->cand.b.p, curr.b.p, N * 16ull, cudaMemcpyDeviceToDevice, s));
+        RS_CUDA(cudaMemcpyAsync(p->cand.rec.p, curr.rec.p, 7ull * N * 16ull, cudaMemcpyDeviceToDevice, s));
+    }
+
+    shouldReset = shouldReset || p->frameCount == 0;
+    const bool temporal = o.enableTemporalResampling && !shouldReset;
+    const bool spatial = o.enableSpatialResampling != 0;
+    bool colorWritten = false;
+    p->lastFusedCollect = false;
+    const uint32_t numTiles = (N + kScanTileElems - 1) / kScanTileElems;
+
+    auto buildCells = [&](uint32_t* tg, uint32_t* cn, uint32_t* of, uint32_t* cu, uint32_t* un, uint32_t* so) {
+        k_scan_tiles<<<numTiles, 1024, 0, s>>>(cn, of, p->tileSums.p, N);
+        k_scan_tile_sums<<<1, 1024, 0, s>>>(p->tileSums.p, numTiles, p->total.p);
+        k_scan_add<<<grid(N, 256), 256, 0, s>>>(of, p->tileSums.p, N);
+        k_fill<<<grid(N, 256), 256, 0, s>>>(tg, of, cu, un, N);
+        k_rank_cells<<<grid(N, 256), 256, 0, s>>>(tg, of, cn, un, so, N);
+        p->launches += 5;
+    };
+
+    float4* temporalColor = spatial ? nullptr : colorDev;
+    if (temporal)
+    {
+        switch (o.temporalReuse)
+        {
+        case RS_GATHER_ONLY:
+            if (o.gatherOption == RS_GATHER_ROBUST)
+            {
+                stage(p, "robustReuse", s);
+                k_robust<<<grid(N, 128), 128, 0, s>>>(C, prev.res(), prev.recp(), p->shiftedPaths.p); p->launches++;
+            }
+            stage(p, "collect", s);
+            k_collect<<<grid(N, 128), 128, 0, s>>>(C, mvec, prev.res(), prev.recp(), p->inter.res(), p->inter.recp(), p->floatingCoords.p, p->shiftedPaths.p); p->launches++;
+            stage(p, "gatherResample", s);
+            k_gather_resample<<<grid(N, 128), 128, 0, s>>>(C, p->vbuffer.p, curr.res(), curr.recp(), p->inter.res(), p->inter.recp(), p->floatingCoords.p, temporalColor); p->launches++;
+            break;
+        case RS_SCATTER_ONLY:
+            stage(p, "reproject", s);
+            RS_CUDA(cudaMemsetAsync(p->counts.p, 0, N * 4ull, s));
+            RS_CUDA(cudaMemsetAsync(p->cursor.p, 0, N * 4ull, s));
+            k_reproject<<<grid(N, 256), 256, 0, s>>>(C, prev.res(), prev.recp(), p->targets.p, p->counts.p); p->launches++;
+            stage(p, "sortCells", s);
+            buildCells(p->targets.p, p->counts.p, p->offsets.p, p->cursor.p, p->unsortedSplats.p, p->sortedSplats.p);
+            stage(p, "scatterResample", s);
+            k_scatter_resample<<<grid(N, 128), 128, 0, s>>>(C, mvec, prev.res(), prev.recp(), curr.res(), curr.recp(), p->counts.p, p->offsets.p, p->sortedSplats.p, temporalColor); p->launches++;
+            break;
+        case RS_SCATTER_BACKUP:
+        {
+            const bool fused = o.gatherOption == RS_GATHER_CLAMPED;
+            p->lastFusedCollect = fused;
+            if (!fused)
+            {
+                if (o.gatherOption == RS_GATHER_ROBUST)
+                {
+                    stage(p, "robustReuse", s);
+                    k_robust<<<grid(N, 128), 128, 0, s>>>(C, prev.res(), prev.recp(), p->shiftedPaths.p); p->launches++;
+                }
+                stage(p, "collect", s);
+                k_collect<<<grid(N, 128), 128, 0, s>>>(C, mvec, prev.res(), prev.recp(), p->inter.res(), p->inter.recp(), p->floatingCoords.p, p->shiftedPaths.p); p->launches++;
+            }
+            stage(p, "reproject", s);
+            RS_CUDA(cudaMemsetAsync(p->counts.p, 0, N * 4ull, s));
+            RS_CUDA(cudaMemsetAsync(p->cursor.p, 0, N * 4ull, s));
+            k_reproject<<<grid(N, 256), 256, 0, s>>>(C, prev.res(), prev.recp(), p->targets.p, p->counts.p); p->launches++;
+            stage(p, "sortCells", s);
+            buildCells(p->targets.p, p->counts.p, p->offsets.p, p->cursor.p, p->unsortedSplats.p, p->sortedSplats.p);
+            stage(p, "scatterBackupResample", s);
+            if (fused)
+                k_scatter_backup_resample_clamped<<<grid(N, 128), 128, 0, s>>>(C, mvec, prev.res(), prev.recp(), curr.res(), curr.recp(),
+                                                                               p->counts.p, p->offsets.p, p->sortedSplats.p, temporalColor);
+            else
+                k_scatter_backup_resample<<<grid(N, 128), 128, 0, s>>>(C, mvec, prev.res(), prev.recp(), curr.res(), curr.recp(), p->inter.res(),
+                                                                       p->inter.recp(), p->floatingCoords.p, p->counts.p, p->offsets.p,
+                                                                       p->sortedSplats.p, temporalColor);
+            p->launches++;
+            break;
+        }
+        case RS_MULTI_SCATTER:
+        {
+            const uint32_t P = o.numTimePartitions;
+            stage(p, "multiReproject", s);
+            RS_CUDA(cudaMemsetAsync(p->counts.p, 0, (size_t)P * N * 4ull, s));
+            RS_CUDA(cudaMemsetAsync(p->cursor.p, 0, (size_t)P * N * 4ull, s));
+            k_multi_reproject<<<grid(N, 256), 256, 0, s>>>(C, prev.res(), prev.recp(), p->targets.p, p->counts.p); p->launches++;
+            stage(p, "multiSortCells", s);
+            for (uint32_t j = 0; j < P; j++)
+            {
+                size_t b = (size_t)j * N;
+                buildCells(p->targets.p + b, p->counts.p + b, p->offsets.p + b, p->cursor.p + b, p->unsortedSplats.p + b, p->sortedSplats.p + b);
+            }
+            stage(p, "multiScatterResample", s);
+            k_multi_scatter_resample<<<grid(N, 128), 128, 0, s>>>(C, mvec, prev.res(), prev.recp(), curr.res(), curr.recp(), p->counts.p, p->offsets.p, p->sortedSplats.p, temporalColor); p->launches++;
+            break;
+        }
+        }
+        colorWritten = !spatial;
+    }
+    if (spatial)
+    {
+        // spatialResampling (ReservoirSplatting.cpp:1994-2020): ping-pong with the prev (or, when
+        // frozen, the temp) buffer
+        int& swapIdx = p->frozen ? p->tempIdx : p->prevIdx;
+        for (uint32_t i = 0; i < o.numSpatialIterations; i++)
+        {
+            std::swap(p->currIdx, swapIdx);
+            ReservoirSet& src = p->sets[swapIdx];
+            ReservoirSet& dst = p->sets[p->currIdx];
+            stage(p, "spatialResample", s);
+            k_spatial<<<grid(N, 128), 128, 0, s>>>(C, i, p->vbuffer.p, p->neighborOffsets.p, src.res(), src.recp(), dst.res(), dst.recp(),
+                                                  i + 1 == o.numSpatialIterations ? colorDev : nullptr);
+            p->launches++;
+        }
+        colorWritten = true;
+    }
+    if (!colorWritten)
+    {
+        stage(p, "resolve", s);
+        k_resolve<<<grid(N, 256), 256, 0, s>>>(N, p->sets[p->currIdx].res(), colorDev); p->launches++;
+    }
+    stage(p, "end", s);
+    RS_CUDA(cudaGetLastError());
+    RS_CUDA(cudaMemcpyAsync(p->hostFault, p->fault.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    if (f->colorHost)
+    {
+        RS_CUDA(cudaMemcpyAsync(f->colorHost, colorDev, N * 16ull, cudaMemcpyDeviceToHost, s));
+        RS_CUDA(cudaStreamSynchronize(s));
+    }
+    // endFrame
+    p->swapped = !p->frozen;
+    if (!p->frozen)
+    {
+        p->frameCount++;
+        std::swap(p->currIdx, p->prevIdx);
+    }
+    p->prevCamera = p->camera;
+    p->havePrevCamera = true;
+    if (f->colorHost && *p->hostFault) return fail(RS_DEVICE_FAULT, "device status word set: BVH traversal stack overflow");
+    return RS_OK;
+}
+
+extern "C" RS_API rs_status rs_reset(rs_pass* p)
+{
+    if (!p) return fail(RS_INVALID_ARG, "pass is NULL");
+    p->frameCount = 0;
+    return RS_OK;
+}
+
+extern "C" RS_API rs_status rs_set_seed(rs_pass* p, uint32_t useFixedSeed, uint32_t fixedSeed)
+{
+    if (!p) return fail(RS_INVALID_ARG, "pass is NULL");
+    p->opt.useFixedSeed = useFixedSeed ? 1u : 0u;
+    p->opt.fixedSeed = fixedSeed;
+    return RS_OK;
+}
+
+extern "C" RS_API rs_status rs_freeze(rs_pass* p, uint32_t frozen)
+{
+    if (!p) return fail(RS_INVALID_ARG, "pass is NULL");
+    p->frozen = frozen != 0;
+    return RS_OK;
+}
+
+// ------------------------------------------------------------------ buffer views
+static rs_status copy_out(rs_pass* p, const void* src, size_t need, void* dst, size_t* bytes)
+{
+    if (!dst) { *bytes = need; return RS_OK; }
+    if (*bytes < need) { *bytes = need; return fail(RS_INVALID_ARG, "destination too small"); }
+    RS_CUDA(cudaStreamSynchronize(p->lastStream));
+    RS_CUDA(cudaMemcpy(dst, src, need, cudaMemcpyDeviceToHost));
+    *bytes = need;
+    return RS_OK;
+}
+
+static rs_status export_res(rs_pass* p, const ReservoirSet& s, void* dst, size_t* bytes)
+{
+    const size_t N = (size_t)p->W * p->H;
+    if (!dst) { *bytes = N * 32; return RS_OK; }
+    if (*bytes < N * 32) { *bytes = N * 32; return fail(RS_INVALID_ARG, "destination too small"); }
+    std::vector<float4> a(N), b(N);
+    RS_CUDA(cudaStreamSynchronize(p->lastStream));
+    RS_CUDA(cudaMemcpy(a.data(), s.a.p, N * 16, cudaMemcpyDeviceToHost));
+    RS_CUDA(cudaMemcpy(b.data(), s.b.p, N * 16, cudaMemcpyDeviceToHost));
+    float* o = (float*)dst;
+    for (size_t i = 0; i < N; i++)
+    {
+        o[8 * i + 0] = a[i].x; o[8 * i + 1] = a[i].y; o[8 * i + 2] = a[i].z; o[8 * i + 3] = a[i].w;
+        o[8 * i + 4] = b[i].x; o[8 * i + 5] = b[i].y; o[8 * i + 6] = b[i].z; o[8 * i + 7] = 0.f;
+    }
+    *bytes = N * 32;
+    return RS_OK;
+}
+
+static rs_status export_rec(rs_pass* p, const ReservoirSet& s, void* dst, size_t* bytes)
+{
+    const size_t N = (size_t)p->W * p->H;
+    if (!dst) { *bytes = N * 112; return RS_OK; }
+    if (*bytes < N * 112) { *bytes = N * 112; return fail(RS_INVALID_ARG, "destination too small"); }
+    std::vector<uint4> planes(7 * N);
+    RS_CUDA(cudaStreamSynchronize(p->lastStream));
+    RS_CUDA(cudaMemcpy(planes.data(), s.rec.p, 7 * N * 16, cudaMemcpyDeviceToHost));
+    uint32_t* o = (uint32_t*)dst;
+    for (size_t i = 0; i < N; i++)
+        for (int k = 0; k < 7; k++)
+        {
+            const uint4& q = planes[k * N + i];
+            o[28 * i + 4 * k + 0] = q.x; o[28 * i + 4 * k + 1] = q.y; o[28 * i + 4 * k + 2] = q.z; o[28 * i + 4 * k + 3] = q.w;
+        }
+    *bytes = N * 112;
+    return RS_OK;
+}
+
+extern "C" RS_API rs_status rs_get_buffer(rs_pass* p, rs_buffer_id id, void* dst, size_t* bytes)
+{
+    if (!p || !bytes) return fail(RS_INVALID_ARG, "pass or bytes is NULL");
+    const size_t N = (size_t)p->W * p->H;
+    const ReservoirSet& last = p->sets[p->swapped ? p->prevIdx : p->currIdx];
+    const ReservoirSet& other = p->sets[p->swapped ? p->currIdx : p->prevIdx];
+    switch (id)
+    {
+    case RS_BUF_CURR_RESERVOIRS: return export_res(p, last, dst, bytes);
+    case RS_BUF_CURR_RECONNECTION: return export_rec(p, last, dst, bytes);
+    case RS_BUF_PREV_RESERVOIRS: return export_res(p, other, dst, bytes);
+    case RS_BUF_PREV_RECONNECTION: return export_rec(p, other, dst, bytes);
+    case RS_BUF_CANDIDATE_RESERVOIRS:
+        if (!p->cand.a.p) return fail(RS_INVALID_ARG, "candidate snapshots are off (keep-candidates option)");
+        return export_res(p, p->cand, dst, bytes);
+    case RS_BUF_CANDIDATE_RECONNECTION:
+        if (!p->cand.a.p) return fail(RS_INVALID_ARG, "candidate snapshots are off (keep-candidates option)");
+        return export_rec(p, p->cand, dst, bytes);
+    case RS_BUF_BACKUP_RESERVOIRS:
+        if (!p->inter.a.p || p->lastFusedCollect) return fail(RS_INVALID_ARG, "no backup buffer in this mode");
+        return export_res(p, p->inter, dst, bytes);
+    case RS_BUF_BACKUP_RECONNECTION:
+        if (!p->inter.a.p || p->lastFusedCollect) return fail(RS_INVALID_ARG, "no backup buffer in this mode");
+        return export_rec(p, p->inter, dst, bytes);
+    case RS_BUF_CELL_COUNTERS: return copy_out(p, p->counts.p, N * 4, dst, bytes);
+    case RS_BUF_CELL_OFFSETS: return copy_out(p, p->offsets.p, N * 4, dst, bytes);
+    case RS_BUF_SPLAT_TARGETS: return copy_out(p, p->targets.p, N * 4, dst, bytes);
+    case RS_BUF_SORTED_SPLATS:
+    {
+        uint32_t total = 0;
+        RS_CUDA(cudaStreamSynchronize(p->lastStream));
+        // the number of splats is the sum of the counts
+        std::vector<uint32_t> c(N);
+        RS_CUDA(cudaMemcpy(c.data(), p->counts.p, N * 4, cudaMemcpyDeviceToHost));
+        for (uint32_t v : c) total += v;
+        return copy_out(p, p->sortedSplats.p, (size_t)total * 4, dst, bytes);
+    }
+    case RS_BUF_FLOATING_COORDS: return copy_out(p, p->floatingCoords.p, N * 8, dst, bytes);
+    case RS_BUF_MVEC: return copy_out(p, p->mvec.p, N * 8, dst, bytes);
+    case RS_BUF_VBUFFER: return copy_out(p, p->vbuffer.p, N * 16, dst, bytes);
+    default: return fail(RS_INVALID_ARG, "unknown buffer id");
+    }
+}
+
+extern "C" RS_API rs_status rs_set_buffer(rs_pass* p, rs_buffer_id id, const void* src, size_t bytes)
+{
+    if (!p || !src) return fail(RS_INVALID_ARG, "pass or src is NULL");
+    const size_t N = (size_t)p->W * p->H;
+    bool curr = id == RS_BUF_CURR_RESERVOIRS || id == RS_BUF_CURR_RECONNECTION;
+    ReservoirSet& s = p->sets[(curr == p->swapped) ? p->prevIdx : p->currIdx];
+    RS_CUDA(cudaDeviceSynchronize());
+    if (id == RS_BUF_CURR_RESERVOIRS || id == RS_BUF_PREV_RESERVOIRS)
+    {
+        if (bytes != N * 32) return fail(RS_INVALID_ARG, "reservoir buffer size mismatch");
+        const float* in = (const float*)src;
+        std::vector<float4> a(N), b(N);
+        for (size_t i = 0; i < N; i++)
+        {
+            a[i] = make_float4(in[8 * i], in[8 * i + 1], in[8 * i + 2], in[8 * i + 3]);
+            b[i] = make_float4(in[8 * i + 4], in[8 * i + 5], in[8 * i + 6], 0.f);
+        }
+        RS_CUDA(cudaMemcpy(s.a.p, a.data(), N * 16, cudaMemcpyHostToDevice));
+        RS_CUDA(cudaMemcpy(s.b.p, b.data(), N * 16, cudaMemcpyHostToDevice));
+        return RS_OK;
+    }
+    if (id == RS_BUF_CURR_RECONNECTION || id == RS_BUF_PREV_RECONNECTION)
+    {
+        if (bytes != N * 112) return fail(RS_INVALID_ARG, "reconnection buffer size mismatch");
+        const uint32_t* in = (const uint32_t*)src;
+        std::vector<uint4> planes(7 * N);
+        for (size_t i = 0; i < N; i++)
+            for (int k = 0; k < 7; k++)
+                planes[k * N + i] = make_uint4(in[28 * i + 4 * k], in[28 * i + 4 * k + 1], in[28 * i + 4 * k + 2], in[28 * i + 4 * k + 3]);
+        RS_CUDA(cudaMemcpy(s.rec.p, planes.data(), 7 * N * 16, cudaMemcpyHostToDevice));
+        return RS_OK;
+    }
+    return fail(RS_INVALID_ARG, "buffer cannot be restored");
+}
+
+extern "C" RS_API rs_status rs_enable_stage_timing(rs_pass* p, uint32_t enable)
+{
+    if (!p) return fail(RS_INVALID_ARG, "pass is NULL");
+    p->timing = enable != 0;
+    return RS_OK;
+}
+
+extern "C" RS_API rs_status rs_get_stage_times(rs_pass* p, float* ms, uint32_t* count, char* names, size_t namesBytes)
+{
+    if (!p || !count) return fail(RS_INVALID_ARG, "pass or count is NULL");
+    if (!p->timing || p->stageNames.size() < 2) { *count = 0; return RS_OK; }
+    RS_CUDA(cudaStreamSynchronize(p->lastStream));
+    uint32_t n = (uint32_t)p->stageNames.size() - 1;
+    if (ms)
+        for (uint32_t i = 0; i < n && i < *count; i++) cudaEventElapsedTime(&ms[i], p->events[i], p->events[i + 1]);
+    if (names)
+    {
+        size_t off = 0;
+        for (uint32_t i = 0; i < n; i++)
+        {
+            size_t l = p->stageNames[i].size() + 1;
+            if (off + l > namesBytes) break;
+            memcpy(names + off, p->stageNames[i].c_str(), l);
+            off += l;
+        }
+    }
+    *count = n;
+    return RS_OK;
+}
+
+extern "C" RS_API uint32_t rs_last_launch_count(rs_pass* p) { return p ? p->launches : 0u; }
+extern "C" RS_API const char* rs_last_error_string(void) { return g_lastError.c_str(); }
+
+// Test hook (not part of the public header): keep a copy of the candidate reservoirs each frame.
+extern "C" RS_API rs_status rs_debug_keep_candidates(rs_pass* p, uint32_t keep)
+{
+    if (!p) return fail(RS_INVALID_ARG, "pass is NULL");
+    p->keepCandidates = keep != 0;
+    return RS_OK;
+}
