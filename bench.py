@@ -1,0 +1,306 @@
+"""Benchmark of the Reservoir Splatting per-frame path (one step = one rendered frame).
+
+Workload: the seeded terrain + icospheres scene (512 x 512 fBm heightfield, 500
+icospheres at subdivision 4, 64 emissive triangles: 3.08M triangles flattened),
+1920 x 1080, ScatterBackup with the Clamped gather and Balance MIS, path length 4
+(maxSurfaceBounces = 2), spatial reuse on (the reference default), camera orbiting
+0.5 degrees per frame.  `value` is frames/s on the device (whole job over N GPUs,
+replicas: each rank renders its own instance); `e2e` is the same through the public
+API with the colour image copied to pinned host memory every frame.
+
+--impl reference times the reference algorithm's CPU restatement (oracle/) on all
+host cores on a bounded sample (a 1/16-area crop-resolution render of the same
+scene and camera path), scaled to 1080p frames/s.  The reference's own GPU path is
+Slang on D3D12/Vulkan and cannot run on this machine.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+PKG_DIR = ROOT / "reservoir-splatting_b200"
+W_FULL, H_FULL = 1920, 1080
+PROPS = {"temporalReuse": "ScatterBackup", "gatherOption": "Clamped", "scatterBackupMISOption": "Balance",
+         "maxSurfaceBounces": 2, "enableSpatialResampling": True}
+SCENE_ARGS = dict(seed=1, grid=512, spheres=500, subdiv=4, lights=64)
+METRIC = "1080p frames/s (ScatterBackup, matched MSE); batched vs plain; bwd/fwd ratio"
+
+
+def _package():
+    if "reservoir_splatting_b200" in sys.modules:
+        return sys.modules["reservoir_splatting_b200"]
+    spec = importlib.util.spec_from_file_location("reservoir_splatting_b200", PKG_DIR / "__init__.py",
+                                                  submodule_search_locations=[str(PKG_DIR)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["reservoir_splatting_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def _peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = Path(os.environ.get("RS_CLOCKS_CSV", "/tmp/rs_clocks_%d.csv" % os.getpid()))
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if not self.path.exists():
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def build_scene(scale: float = 1.0):
+    _package()
+    import reservoir_splatting_b200.scenes as S
+    return S.terrain_spheres(**SCENE_ARGS)
+
+
+def camera(frame, w, h):
+    _package()
+    import reservoir_splatting_b200.scenes as S
+    return S.orbit_camera(frame, w, h)
+
+
+def dominant_kernel_bytes(stage: str, W: int, H: int) -> float:
+    """Algorithmic HBM bytes of one launch of a stage (the per-pixel figures are derived in DESIGN.md)."""
+    N = W * H
+    R, C = 32, 112  # reservoir and reconnection record bytes
+    per_pixel = {
+        "initialCandidates": R + C + 3 * 48,                # write res+rec, read the primary triangle
+        "scatterBackupResample": (3 + 1) * (R + C) + 32 + 3 * 48,
+        "spatialResample": 2 * (R + C) + (R + C) + 16 + 16,
+        "reproject": 4 + 16 + 8 + 48 + 4 + 4,
+        "vbuffer": 16 + 8 + 48,
+        "sortCells": 4 * 6,
+    }.get(stage, R + C)
+    return float(per_pixel * N)
+
+
+def run_ours(args):
+    import torch
+    rs = _package()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    scene = build_scene()
+    W, H = W_FULL, H_FULL
+    p = rs.ReservoirSplatting(PROPS, W, H)
+    p.set_scene(scene)
+    stream = torch.cuda.Stream()
+    color = torch.empty((H, W, 4), dtype=torch.float32, device=dev)
+    frame = 0
+
+    def step(color_ptr=None, color_host=None):
+        nonlocal frame
+        p.execute(camera(frame + 97 * rank, W, H), color_ptr=color_ptr, color_host=color_host, stream=stream.cuda_stream)
+        frame += 1
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step(color.data_ptr())
+    torch.cuda.synchronize()
+    launches = 0
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        with torch.cuda.stream(stream):
+            start.record(stream)
+            for _ in range(args.steps):
+                step(color.data_ptr())
+                launches += p.last_launch_count()
+            stop.record(stream)
+        torch.cuda.synchronize()
+    ms = start.elapsed_time(stop)
+    clocks = clk.summary()
+    t = torch.tensor([ms], device=dev)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.barrier()
+    ms_max = float(t.item())
+    value = world * args.steps / (ms_max / 1e3)
+
+    # per-stage device times on the launching stream (CUDA events inside the pass)
+    p.enable_stage_timing(True)
+    stage_ms = {}
+    with torch.cuda.stream(stream):
+        for _ in range(3):
+            step(color.data_ptr())
+            for k, v in p.stage_times().items():
+                stage_ms[k] = stage_ms.get(k, 0.0) + v / 3.0
+    p.enable_stage_timing(False)
+    torch.cuda.synchronize()
+
+    # end to end through the public API: colour copied to pinned host memory every frame
+    host = torch.empty((H, W, 4), dtype=torch.float32, pin_memory=True)
+    host_np = host.numpy()
+    e2e_steps = max(3, min(args.steps, 10))
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for _ in range(e2e_steps):
+            step(None, host_np)
+        e1.record(stream)
+    torch.cuda.synchronize()
+    te = torch.tensor([e0.elapsed_time(e1)], device=dev)
+    if dist:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = world * e2e_steps / (float(te.item()) / 1e3)
+
+    peak, peak_kind = _peaks()
+    dom = max(stage_ms, key=stage_ms.get) if stage_ms else "initialCandidates"
+    dom_ms = stage_ms.get(dom, ms / args.steps)
+    achieved = dominant_kernel_bytes(dom, W, H) / (dom_ms / 1e3) / 1e9
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 5), "traffic": None, "peak_source": peak_kind,
+                "stage_ms": {k: round(v, 4) for k, v in stage_ms.items()}}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": "frames/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
+            "config": {"workload": "terrain512+500 icospheres(subdiv4)+64 emissive tris = %d tris, 1920x1080, ScatterBackup/Clamped/Balance, "
+                                   "path length 4, spatial reuse on, orbit 0.5 deg/frame" % scene.num_triangles,
+                       "resolution": [W, H], "triangles": scene.num_triangles, "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "per-frame working set (3 x 144 B/pixel reservoir sets + 348 MB BVH) exceeds the 126 MB L2"},
+            "e2e": {"value": round(e2e_value, 3), "unit": "frames/s", "h2d_bytes_per_step": int(C_frame_bytes()),
+                    "d2h_bytes_per_step": int(W * H * 16)},
+            "gpu_launches": int(launches),
+            "roofline": roofline,
+            "clocks": clocks,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(args, quiet=True)
+        print(json.dumps(line), flush=True)
+    p.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+def C_frame_bytes():
+    import ctypes
+    rs = _package()
+    return ctypes.sizeof(rs.abi.RsFrameDesc)
+
+
+def cpu_baseline(args, quiet=False):
+    """The oracle on all host cores on a 480 x 270 render (1/16 of the 1080p pixels) of the same
+    scene and camera path; the frame time is scaled by 16 to 1080p frames/s."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    threads = os.cpu_count() or 1
+    O.set_threads(threads)
+    scene = build_scene()
+    w, h = W_FULL // 4, H_FULL // 4
+    p = O.OraclePass(PROPS, w, h)
+    t0 = time.time()
+    p.set_scene(scene)
+    setup = time.time() - t0
+    p.execute(camera(0, w, h))  # frame 0 (no temporal history)
+    frames = max(1, args.cpu_frames)
+    t0 = time.time()
+    for f in range(1, 1 + frames):
+        p.execute(camera(f, w, h))
+    dt = (time.time() - t0) / frames
+    scale = (W_FULL * H_FULL) / (w * h)
+    return {"value": round(1.0 / (dt * scale), 5), "unit": "frames/s", "cores": threads, "kind": "port",
+            "sample": f"{frames} temporal frame(s) at {w}x{h} (1/{scale:.0f} of 1080p), scaled by {scale:.0f}; scene setup {setup:.1f}s excluded"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    cb = cpu_baseline(args)
+    line = {"metric": METRIC, "value": cb["value"], "unit": "frames/s", "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "impl": "reference",
+            "dtype": "f32", "data": "synthetic (seeded procedural scene)",
+            "config": {"workload": "terrain512+500 icospheres(subdiv4)+64 emissive tris, 1920x1080, ScatterBackup/Clamped/Balance, path length 4, spatial reuse on"},
+            "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "reference GPU path is Slang on D3D12/Vulkan DXR: unavailable on this box; timed: the CPU restatement of its algorithm"}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-frames", type=int, default=1)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,5 +1,5 @@
 // LBVH construction on the GPU (Karras 2012, "Maximizing parallelism in the
-// construction of BVHs, octrees, and k-d trees"): 30-bit Morton codes of the
+// construction of BVHs, octrees, and k-d trees"): 63-bit Morton codes (21 bits per axis) of the
 // triangle centroids, a key/index sort, one thread per internal node to find its
 // range and split, and a bottom-up box pass with per-node arrival counters.
 // Built once per rs_set_scene; the per-frame path only traverses it.
@@ -8,12 +8,15 @@
 
 namespace rs {
 
-__device__ __forceinline__ uint32_t expand_bits10(uint32_t v)
+// Spreads the low 21 bits of v so that two zero bits separate consecutive bits.
+__device__ __forceinline__ uint64_t expand_bits21(uint64_t v)
 {
-    v = (v * 0x00010001u) & 0xFF0000FFu;
-    v = (v * 0x00000101u) & 0x0F00F00Fu;
-    v = (v * 0x00000011u) & 0xC30C30C3u;
-    v = (v * 0x00000005u) & 0x49249249u;
+    v &= 0x1fffffull;
+    v = (v | (v << 32)) & 0x1f00000000ffffull;
+    v = (v | (v << 16)) & 0x1f0000ff0000ffull;
+    v = (v | (v << 8)) & 0x100f00f00f00f00full;
+    v = (v | (v << 4)) & 0x10c30c30c30c30c3ull;
+    v = (v | (v << 2)) & 0x1249249249249249ull;
     return v;
 }
 
@@ -54,7 +57,7 @@ __global__ void k_centroid_bounds(const float4* __restrict__ tri, uint32_t n, ui
 }
 
 __global__ void k_morton(const float4* __restrict__ tri, uint32_t n, const uint32_t* __restrict__ bounds,
-                         uint32_t* __restrict__ keys, uint32_t* __restrict__ vals)
+                         uint64_t* __restrict__ keys, uint32_t* __restrict__ vals)
 {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -67,23 +70,24 @@ __global__ void k_morton(const float4* __restrict__ tri, uint32_t n, const uint3
     }
     float4 a = tri[3 * i], b = tri[3 * i + 1], c = tri[3 * i + 2];
     float cx = (a.x + b.x + c.x) * (1.f / 3.f), cy = (a.y + b.y + c.y) * (1.f / 3.f), cz = (a.z + b.z + c.z) * (1.f / 3.f);
-    uint32_t qx = (uint32_t)fminf(fmaxf((cx - lo[0]) / ext[0] * 1024.f, 0.f), 1023.f);
-    uint32_t qy = (uint32_t)fminf(fmaxf((cy - lo[1]) / ext[1] * 1024.f, 0.f), 1023.f);
-    uint32_t qz = (uint32_t)fminf(fmaxf((cz - lo[2]) / ext[2] * 1024.f, 0.f), 1023.f);
-    keys[i] = (expand_bits10(qx) << 2) | (expand_bits10(qy) << 1) | expand_bits10(qz);
+    const float Q = 2097152.f; // 2^21 cells per axis: 63-bit keys
+    uint64_t qx = (uint64_t)fminf(fmaxf((cx - lo[0]) / ext[0] * Q, 0.f), Q - 1.f);
+    uint64_t qy = (uint64_t)fminf(fmaxf((cy - lo[1]) / ext[1] * Q, 0.f), Q - 1.f);
+    uint64_t qz = (uint64_t)fminf(fmaxf((cz - lo[2]) / ext[2] * Q, 0.f), Q - 1.f);
+    keys[i] = (expand_bits21(qx) << 2) | (expand_bits21(qy) << 1) | expand_bits21(qz);
     vals[i] = i;
 }
 
 // Common-prefix length of sorted keys i and j (index bits break ties between equal keys).
-__device__ __forceinline__ int delta(const uint32_t* keys, int n, int i, int j)
+__device__ __forceinline__ int delta(const uint64_t* keys, int n, int i, int j)
 {
     if (j < 0 || j >= n) return -1;
-    uint32_t a = keys[i], b = keys[j];
-    if (a == b) return 32 + __clz((uint32_t)i ^ (uint32_t)j);
-    return __clz(a ^ b);
+    uint64_t a = keys[i], b = keys[j];
+    if (a == b) return 64 + __clz((uint32_t)i ^ (uint32_t)j);
+    return __clzll((long long)(a ^ b));
 }
 
-__global__ void k_karras(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ prim, int n,
+__global__ void k_karras(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ prim, int n,
                          float4* __restrict__ nodes, uint32_t* __restrict__ parent, uint32_t* __restrict__ leafParent)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -168,13 +172,14 @@ cudaError_t build_lbvh(const float4* dTri, uint32_t n, float4* dNodes, uint32_t*
     if (n == 0) { *rootOut = 0; return cudaSuccess; }
     if (n == 1) { *rootOut = kLeafBit | 0u; return cudaSuccess; }
     cudaError_t e;
-    uint32_t *keys = nullptr, *vals = nullptr, *keys2 = nullptr, *vals2 = nullptr, *bounds = nullptr;
+    uint64_t *keys = nullptr, *keys2 = nullptr;
+    uint32_t *vals = nullptr, *vals2 = nullptr, *bounds = nullptr;
     uint32_t *parent = nullptr, *leafParent = nullptr, *arrivals = nullptr;
     void* temp = nullptr;
     size_t tempBytes = 0;
 #define RS_TRY(x) do { e = (x); if (e != cudaSuccess) goto done; } while (0)
-    RS_TRY(cudaMalloc(&keys, n * 4ull)); RS_TRY(cudaMalloc(&vals, n * 4ull));
-    RS_TRY(cudaMalloc(&keys2, n * 4ull)); RS_TRY(cudaMalloc(&vals2, n * 4ull));
+    RS_TRY(cudaMalloc(&keys, n * 8ull)); RS_TRY(cudaMalloc(&vals, n * 4ull));
+    RS_TRY(cudaMalloc(&keys2, n * 8ull)); RS_TRY(cudaMalloc(&vals2, n * 4ull));
     RS_TRY(cudaMalloc(&bounds, 6 * 4ull));
     RS_TRY(cudaMalloc(&parent, n * 4ull)); RS_TRY(cudaMalloc(&leafParent, n * 4ull)); RS_TRY(cudaMalloc(&arrivals, n * 4ull));
     {
@@ -182,9 +187,9 @@ cudaError_t build_lbvh(const float4* dTri, uint32_t n, float4* dNodes, uint32_t*
         RS_TRY(cudaMemcpyAsync(bounds, init, sizeof(init), cudaMemcpyHostToDevice, s));
         k_centroid_bounds<<<592, 256, 0, s>>>(dTri, n, bounds);
         k_morton<<<(n + 255) / 256, 256, 0, s>>>(dTri, n, bounds, keys, vals);
-        RS_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tempBytes, keys, keys2, vals, vals2, (int)n, 0, 30, s));
+        RS_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tempBytes, keys, keys2, vals, vals2, (int)n, 0, 63, s));
         RS_TRY(cudaMalloc(&temp, tempBytes));
-        RS_TRY(cub::DeviceRadixSort::SortPairs(temp, tempBytes, keys, keys2, vals, vals2, (int)n, 0, 30, s));
+        RS_TRY(cub::DeviceRadixSort::SortPairs(temp, tempBytes, keys, keys2, vals, vals2, (int)n, 0, 63, s));
         RS_TRY(cudaMemsetAsync(dNodes, 0, 64ull * (n - 1), s));
         k_karras<<<(n - 1 + 255) / 256, 256, 0, s>>>(keys2, vals2, (int)n, dNodes, parent, leafParent);
         RS_TRY(cudaMemsetAsync(arrivals, 0, n * 4ull, s));

@@ -552,7 +552,7 @@ __global__ void __launch_bounds__(256) k_fill(const uint32_t* __restrict__ targe
 // cell with a smaller source index).  Source indices are distinct, so the ranks are a permutation.
 __global__ void __launch_bounds__(256) k_rank_cells(const uint32_t* __restrict__ targets, const uint32_t* __restrict__ offsets,
                                                     const uint32_t* __restrict__ counts, const uint32_t* __restrict__ unsorted,
-                                                    uint32_t* __restrict__ sorted, uint32_t n)
+                                                    uint32_t* __restrict__ sorted, uint32_t* __restrict__ sortedCell, uint32_t n)
 {
     uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n) return;
@@ -562,6 +562,7 @@ __global__ void __launch_bounds__(256) k_rank_cells(const uint32_t* __restrict__
     uint32_t rank = 0;
     for (uint32_t j = 0; j < cnt; j++) rank += (__ldg(&unsorted[off + j]) < s) ? 1u : 0u;
     sorted[off + rank] = s;
+    if (sortedCell) sortedCell[off + rank] = t;
 }
 
 // ============================================================ backup gather (collect)
@@ -813,197 +814,6 @@ __global__ void __launch_bounds__(128) k_scatter_resample(DevCtx C, const float2
     write_color(color, ri, dst);
 }
 
-// ScatterBackupTemporalResampling.rt.slang:69-283.  With the Clamped gather the backup
-// reservoir is read straight from the previous frame at round(prevPixel) (the collect pass
-// is fused in); otherwise it comes from the collect pass's intermediate buffers.
-template <bool FusedClamped>
-__device__ __forceinline__ void scatter_backup_body(const DevCtx& C, const float2* __restrict__ mvec, ResPlanes prev, RecPlanes prevRec,
-                                                    ResPlanes curr, RecPlanes currRec, ResPlanes inter, RecPlanes interRec,
-                                                    const float2* __restrict__ floatingCoords, const uint32_t* __restrict__ counts,
-                                                    const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ sorted,
-                                                    float4* __restrict__ color)
-{
-    uint32_t ri = blockIdx.x * blockDim.x + threadIdx.x;
-    if (ri >= C.W * C.H) return;
-    uint32_t x = ri % C.W, y = ri / C.W;
-    const bool useConf = C.useConfTemporal != 0;
-    const bool balance = C.scatterBackupMIS == 0u;
-    SampleGen sg = sg_create(x, y, pass_seed(C, 6), C.sgKind);
-    Res dst = res_default();
-    Recon dstR = recon_default();
-    Res cr = load_res_rw(curr, ri);
-    Recon crd = load_rec_rw(currRec, ri);
-    Res br;
-    Recon brd;
-    f2 floatingCoord;
-    if (FusedClamped)
-    {
-        // CollectTemporalSamples.cs.slang:84-99, 143-156
-        br = res_default();
-        brd = recon_default();
-        f2 prevPixel = prev_pixel_from_mvec(C, mvec, x, y);
-        floatingCoord = mk2(-1.f, -1.f);
-        if (valid_float(C, prevPixel))
-        {
-            float rx = f_round(prevPixel.x), ry = f_round(prevPixel.y);
-            floatingCoord = mk2(rx, ry);
-            if (valid_int(C, (int)rx, (int)ry))
-            {
-                uint32_t pi = (uint32_t)ry * C.W + (uint32_t)rx;
-                br = load_res(prev, pi);
-                brd = load_rec(prevRec, pi);
-            }
-            if (f_isnan(br.totalWeight))
-            {
-                br.integrand = mk3(0.f); br.totalWeight = 0.f;
-                brd.subPixelJacobian = 1.f; brd.lensVertexJacobian = 1.f; brd.secondaryPathJacobian = 1.f; brd.pathLength = 0;
-            }
-        }
-    }
-    else
-    {
-        br = load_res(inter, ri);
-        brd = load_rec(interRec, ri);
-        float2 fc = __ldg(&floatingCoords[ri]);
-        floatingCoord = mk2(fc.x, fc.y);
-    }
-    const float misScale = balance ? 1.f : 0.5f;
-    {
-        float currSampleMIS = 1.f;
-        if (any_gt0(cr.integrand))
-        {
-            float m1 = luminance(cr.integrand) * (useConf ? cr.confidence : 1.f);
-            Shifted sc = dev_scatter_shift(C, sg, crd, crd.time + C.cm.artificialFrameTime, crd.firstHit, crd.lensSample, false);
-            float scj = jac_scatter(sc, crd);
-            float m2 = luminance(sc.radiance) * scj;
-            m2 = f_isnan(m2) ? 0.f : m2;
-            int spx = (int)f_floor(sc.fractionalPixel.x), spy = (int)f_floor(sc.fractionalPixel.y);
-            if (valid_int(C, spx, spy)) m2 *= 0.5f * (useConf ? load_confidence(prev, (uint32_t)spy * C.W + (uint32_t)spx) : 1.f);
-            else m2 = 0.f;
-            float m3 = 0.f;
-            if (valid_float(C, floatingCoord))
-            {
-                Shifted gc = dev_gather_lens_copy(C, sg, crd, crd.time + C.cm.artificialFrameTime, floatingCoord + cr.subPixel, crd.lensSample);
-                float gj = gc.secondaryPathJacobian / crd.secondaryPathJacobian;
-                m3 = luminance(gc.radiance) * gj * 0.5f * (useConf ? br.confidence : 1.f);
-            }
-            m3 = f_isnan(m3) ? 0.f : m3;
-            if (balance) currSampleMIS = (m1 + m2 + m3 == 0.f) ? 0.f : m1 / (m1 + m2 + m3);
-            else currSampleMIS = 0.5f * (((m1 + m2 == 0.f) ? 0.f : 0.5f * m1 / (0.5f * m1 + m2)) +
-                                         ((m1 + m3 == 0.f) ? 0.f : 0.5f * m1 / (0.5f * m1 + m3)));
-        }
-        if (res_add_sample(dst, sg, currSampleMIS, cr.integrand, 1.f, cr)) dstR = crd;
-    }
-    {
-        float backupSampleMIS = 0.f;
-        f3 backupPHat = mk3(0.f);
-        float sj = 1.f;
-        if (any_gt0(br.integrand))
-        {
-            Shifted sb = dev_gather_lens_copy(C, sg, brd, brd.time, mk2((float)x + br.subPixel.x, (float)y + br.subPixel.y), brd.lensSample);
-            sj = sb.secondaryPathJacobian / brd.secondaryPathJacobian;
-            float m1 = luminance(sb.radiance) * sj * (useConf ? cr.confidence : 1.f);
-            backupPHat = f_isnan(m1) ? mk3(0.f) : sb.radiance;
-            sj = f_isnan(m1) ? 1.f : sj;
-            m1 = f_isnan(m1) ? 0.f : m1;
-            recon_update(brd, sb);
-            float m2 = 0.f;
-            if (balance)
-            {
-                Shifted ss = dev_scatter_shift(C, sg, brd, brd.time + C.cm.artificialFrameTime, brd.firstHit, brd.lensSample, false);
-                float scj = jac_scatter(ss, brd);
-                m2 = luminance(ss.radiance) * scj * sj;
-                m2 = f_isnan(m2) ? 0.f : m2;
-                int spx = (int)f_floor(ss.fractionalPixel.x), spy = (int)f_floor(ss.fractionalPixel.y);
-                if (valid_int(C, spx, spy)) m2 *= 0.5f * (useConf ? load_confidence(prev, (uint32_t)spy * C.W + (uint32_t)spx) : 1.f);
-                else m2 = 0.f;
-            }
-            float m3 = luminance(br.integrand) * 0.5f * (useConf ? br.confidence : 1.f);
-            backupSampleMIS = misScale * ((m1 + m2 + m3 == 0.f) ? 0.f : m3 / (misScale * m1 + m2 + m3));
-        }
-        if (res_add_sample(dst, sg, backupSampleMIS, backupPHat, sj, br)) dstR = brd;
-    }
-    float newConfidence = dst.confidence;
-    uint32_t n = counts[ri], off = offsets[ri];
-    for (uint32_t i = 0; i < n; i++)
-    {
-        uint32_t si = __ldg(&sorted[off + i]);
-        Res pr = load_res(prev, si);
-        float prevSampleMIS = 0.f;
-        f3 prevPHat = mk3(0.f);
-        float scj = 1.f;
-        Recon prd = load_rec(prevRec, si);
-        if (any_gt0(pr.integrand))
-        {
-            Shifted sp = dev_scatter_shift(C, sg, prd, prd.time, prd.firstHit, prd.lensSample, true);
-            scj = jac_scatter(sp, prd);
-            float m1 = luminance(sp.radiance) * scj * (useConf ? cr.confidence : 1.f);
-            m1 = f_isnan(m1) ? 0.f : m1;
-            prevPHat = sp.radiance; // the NaN test above already cleared m1 (ScatterBackupTemporalResampling.rt.slang:224-226)
-            recon_update(prd, sp);
-            pr.subPixel = prd.subPixel;
-            float m2 = luminance(pr.integrand) * 0.5f * (useConf ? pr.confidence : 1.f);
-            float m3 = 0.f;
-            if (balance)
-            {
-                f2 fp = floatingCoord + pr.subPixel;
-                if (valid_float(C, fp))
-                {
-                    Shifted gp = dev_gather_lens_copy(C, sg, prd, prd.time + C.cm.artificialFrameTime, fp, prd.lensSample);
-                    float gj = gp.secondaryPathJacobian / prd.secondaryPathJacobian;
-                    m3 = luminance(gp.radiance) * gj * scj * 0.5f * (useConf ? br.confidence : 1.f);
-                }
-                m3 = f_isnan(m3) ? 0.f : m3;
-            }
-            prevSampleMIS = misScale * ((m1 + m2 + m3 == 0.f) ? 0.f : m2 / (misScale * m1 + m2 + m3));
-        }
-        if (res_add_sample(dst, sg, prevSampleMIS, prevPHat, scj, pr)) dstR = prd;
-    }
-    dst.confidence = bilinear_confidence(C, mvec, prev, x, y, newConfidence, useConf);
-    store_res(curr, ri, dst);
-    store_rec(currRec, ri, dstR);
-    write_color(color, ri, dst);
-}
-__global__ void __launch_bounds__(128) k_scatter_backup_resample_clamped(DevCtx C, const float2* __restrict__ mvec, ResPlanes prev, RecPlanes prevRec,
-                                                                         ResPlanes curr, RecPlanes currRec, const uint32_t* __restrict__ counts,
-                                                                         const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ sorted,
-                                                                         float4* __restrict__ color)
-{
-    scatter_backup_body<true>(C, mvec, prev, prevRec, curr, currRec, prev, prevRec, nullptr, counts, offsets, sorted, color);
-}
-__global__ void __launch_bounds__(128) k_scatter_backup_resample(DevCtx C, const float2* __restrict__ mvec, ResPlanes prev, RecPlanes prevRec,
-                                                                 ResPlanes curr, RecPlanes currRec, ResPlanes inter, RecPlanes interRec,
-                                                                 const float2* __restrict__ floatingCoords, const uint32_t* __restrict__ counts,
-                                                                 const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ sorted,
-                                                                 float4* __restrict__ color)
-{
-    scatter_backup_body<false>(C, mvec, prev, prevRec, curr, currRec, inter, interRec, floatingCoords, counts, offsets, sorted, color);
-}
-
-// Depth-of-field shift probabilities of a pixel (ShiftMapping.slang:43-80; GatherTemporalResampling.rt.slang:75-96)
-__device__ __forceinline__ f2 pixel_dof_probs(const DevCtx& C, const uint4* vbuffer, uint32_t i)
-{
-    if (!(C.camera.apertureRadius > 0.f)) return mk2(1.f, 0.f);
-    uint4 q = __ldg(&vbuffer[i]);
-    HitInfo h; h.w[0] = q.x; h.w[1] = q.y; h.w[2] = q.z; h.w[3] = q.w;
-    const CameraData& cam = C.camera;
-    float normalizedFilm = length(cam.cameraU / (float)C.W + cam.cameraV / (float)C.H);
-    float coc;
-    if (hit_valid(h))
-    {
-        f3 x1 = dev_sd(C, h, mk3(0.f)).posW;
-        f3 camDir = normalize(cam.cameraW);
-        float camZ = dot(x1 - cam.posW, camDir);
-        float filmZ = camZ - length(cam.cameraW);
-        float filmRadius = f_abs(cam.apertureRadius / camZ * filmZ);
-        coc = filmRadius / normalizedFilm;
-    }
-    else coc = cam.apertureRadius / normalizedFilm;
-    float gamma = 0.2f + 6.2f / (coc - 5.6f);
-    gamma = (coc <= 0.2f) ? 1.f : f_clamp(gamma, 0.2f, 1.f);
-    return mk2(gamma, 1.f - gamma);
-}
-
 // GatherTemporalResampling.rt.slang:68-235
 __global__ void __launch_bounds__(128) k_gather_resample(DevCtx C, const uint4* __restrict__ vbuffer, ResPlanes curr, RecPlanes currRec,
                                                          ResPlanes inter, RecPlanes interRec, const float2* __restrict__ floatingCoords,
@@ -1144,77 +954,6 @@ __global__ void __launch_bounds__(128) k_multi_scatter_resample(DevCtx C, const 
     dst.confidence = bilinear_confidence(C, mvec, prev, x, y, newConfidence, useConf);
     store_res(curr, ri, dst);
     store_rec(currRec, ri, dstR);
-    write_color(color, ri, dst);
-}
-
-// ============================================================ spatial resampling
-// SpatialResampling.rt.slang:67-185 (one iteration: src -> dst)
-__global__ void __launch_bounds__(128) k_spatial(DevCtx C, uint32_t iteration, const uint4* __restrict__ vbuffer, const float2* __restrict__ neighborOffsets,
-                                                 ResPlanes src, RecPlanes srcRec, ResPlanes dstP, RecPlanes dstRec, float4* __restrict__ color)
-{
-    uint32_t ri = blockIdx.x * blockDim.x + threadIdx.x;
-    if (ri >= C.W * C.H) return;
-    uint32_t x = ri % C.W, y = ri / C.W;
-    const bool useConf = C.useConfSpatial != 0;
-    const uint32_t neighborCount = C.neighborCount;
-    const uint32_t kSpatialNeighborSamples = 8192;
-    SampleGen sg = sg_create(x, y, C.useFixedSeed ? C.fixedSeed + 7 : kNumRenderPasses * (C.frameCount + C.seed) + 1337u * iteration + 7u, C.sgKind);
-    f2 probs = pixel_dof_probs(C, vbuffer, ri);
-    const uint32_t numLensCopy = (uint32_t)f_round(probs.x * (float)neighborCount);
-    Res cent = load_res(src, ri);
-    Recon centR = load_rec(srcRec, ri);
-    float centralSampleMIS = 1.f;
-    float centralWeight = luminance(cent.integrand) / (float)neighborCount * (useConf ? cent.confidence : 1.f);
-    Res dst = res_default();
-    Recon dstR = recon_default();
-    int validNeighbors = 0;
-    uint32_t startIdx = (uint32_t)(sampleNext1D(sg) * (float)kSpatialNeighborSamples);
-    for (uint32_t i = 0; i < neighborCount; i++)
-    {
-        bool lensCopy = (i < numLensCopy);
-        float2 off = __ldg(&neighborOffsets[(startIdx + i) % kSpatialNeighborSamples]);
-        int nx = (int)f_round((float)x + C.spatialGatherRadius * off.x);
-        int ny = (int)f_round((float)y + C.spatialGatherRadius * off.y);
-        if (!valid_int(C, nx, ny)) continue;
-        validNeighbors += 1;
-        uint32_t ni = (uint32_t)ny * C.W + (uint32_t)nx;
-        Res nr = load_res(src, ni);
-        Recon nrd = load_rec(srcRec, ni);
-        float m1 = 0.f;
-        if (any_gt0(cent.integrand))
-        {
-            f2 fp = mk2((float)nx + cent.subPixel.x, (float)ny + cent.subPixel.y);
-            Shifted sc = lensCopy ? dev_gather_lens_copy(C, sg, centR, centR.time, fp, centR.lensSample)
-                                  : dev_gather_primary_reconnect(C, sg, centR, centR.time, fp, centR.firstHit);
-            float sj = (lensCopy ? 1.f : (sc.lensVertexJacobian / centR.lensVertexJacobian)) * (sc.secondaryPathJacobian / centR.secondaryPathJacobian);
-            m1 = luminance(sc.radiance) * sj * (useConf ? nr.confidence : 1.f);
-            m1 = f_isnan(m1) ? 0.f : m1;
-        }
-        centralSampleMIS += 1.f;
-        centralSampleMIS -= (m1 + centralWeight > 0.f) ? m1 / (m1 + centralWeight) : 0.f;
-        float neighborSampleMIS = 0.f;
-        f3 neighborPHat = mk3(0.f);
-        float sj = 1.f;
-        if (any_gt0(nr.integrand))
-        {
-            f2 fp = mk2((float)x + nr.subPixel.x, (float)y + nr.subPixel.y);
-            Shifted sn = lensCopy ? dev_gather_lens_copy(C, sg, nrd, nrd.time, fp, nrd.lensSample)
-                                  : dev_gather_primary_reconnect(C, sg, nrd, nrd.time, fp, nrd.firstHit);
-            sj = (lensCopy ? 1.f : (sn.lensVertexJacobian / nrd.lensVertexJacobian)) * (sn.secondaryPathJacobian / nrd.secondaryPathJacobian);
-            float nw = luminance(sn.radiance) * sj * (useConf ? cent.confidence : 1.f);
-            neighborPHat = f_isnan(nw) ? mk3(0.f) : sn.radiance;
-            sj = f_isnan(nw) ? 1.f : sj;
-            nw = f_isnan(nw) ? 0.f : nw / (float)neighborCount;
-            recon_update(nrd, sn);
-            float m2 = luminance(nr.integrand) * (useConf ? nr.confidence : 1.f);
-            neighborSampleMIS = (m2 + nw > 0.f) ? m2 / (nw + m2) : 0.f;
-        }
-        if (res_add_sample(dst, sg, neighborSampleMIS, neighborPHat, sj, nr)) dstR = nrd;
-    }
-    if (res_add_sample(dst, sg, centralSampleMIS, cent.integrand, 1.f, cent)) dstR = centR;
-    dst.totalWeight /= (float)(validNeighbors + 1);
-    store_res(dstP, ri, dst);
-    store_rec(dstRec, ri, dstR);
     write_color(color, ri, dst);
 }
 

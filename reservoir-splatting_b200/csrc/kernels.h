@@ -13,27 +13,62 @@ __global__ void k_scan_tile_sums(uint32_t* tileSums, uint32_t numTiles, uint32_t
 __global__ void k_scan_add(uint32_t* out, const uint32_t* tileSums, uint32_t n);
 __global__ void k_fill(const uint32_t* targets, const uint32_t* offsets, uint32_t* cursor, uint32_t* unsorted, uint32_t n);
 __global__ void k_rank_cells(const uint32_t* targets, const uint32_t* offsets, const uint32_t* counts, const uint32_t* unsorted,
-                             uint32_t* sorted, uint32_t n);
+                             uint32_t* sorted, uint32_t* sortedCell, uint32_t n);
 __global__ void k_collect(DevCtx C, const float2* mvec, ResPlanes prev, RecPlanes prevRec, ResPlanes inter, RecPlanes interRec,
                           float2* floatingCoords, const Shifted* shiftedPaths);
 __global__ void k_robust(DevCtx C, ResPlanes prev, RecPlanes prevRec, Shifted* shiftedPaths);
 __global__ void k_scatter_resample(DevCtx C, const float2* mvec, ResPlanes prev, RecPlanes prevRec, ResPlanes curr, RecPlanes currRec,
                                    const uint32_t* counts, const uint32_t* offsets, const uint32_t* sorted, float4* color);
-__global__ void k_scatter_backup_resample(DevCtx C, const float2* mvec, ResPlanes prev, RecPlanes prevRec, ResPlanes curr, RecPlanes currRec,
-                                          ResPlanes inter, RecPlanes interRec, const float2* floatingCoords, const uint32_t* counts,
-                                          const uint32_t* offsets, const uint32_t* sorted, float4* color);
-// ScatterBackup with the Clamped gather: the collect pass is fused in (backup read from prev at round(prevPixel)).
-__global__ void k_scatter_backup_resample_clamped(DevCtx C, const float2* mvec, ResPlanes prev, RecPlanes prevRec, ResPlanes curr,
-                                                  RecPlanes currRec, const uint32_t* counts, const uint32_t* offsets, const uint32_t* sorted,
-                                                  float4* color);
 __global__ void k_gather_resample(DevCtx C, const uint4* vbuffer, ResPlanes curr, RecPlanes currRec, ResPlanes inter, RecPlanes interRec,
                                   const float2* floatingCoords, float4* color);
 __global__ void k_multi_scatter_resample(DevCtx C, const float2* mvec, ResPlanes prev, RecPlanes prevRec, ResPlanes curr, RecPlanes currRec,
                                          const uint32_t* counts, const uint32_t* offsets, const uint32_t* sortedAll, float4* color);
-__global__ void k_spatial(DevCtx C, uint32_t iteration, const uint4* vbuffer, const float2* neighborOffsets, ResPlanes src, RecPlanes srcRec,
-                          ResPlanes dstP, RecPlanes dstRec, float4* color);
 __global__ void k_resolve(uint32_t n, ResPlanes curr, float4* color);
 
 constexpr int kScanTileElems = 4096; // k_scan_tiles: 1024 threads x 4 items
+
+// Stored shift results: five uint4 planes (radiance + jacobians + fractional pixel + primary hit +
+// lens sample + first ray direction), plane k at p + k * stride.
+struct ShiftPlanes { uint4* p; size_t stride; };
+
+// Buffers of the wavefront ScatterBackup resampling (wavefront.cu).
+struct WaveCtx
+{
+    DevCtx C;
+    bool fused;                 // Clamped gather read directly from the previous frame
+    const float2* mvec;
+    ResPlanes curr; RecPlanes currRec;
+    ResPlanes prev; RecPlanes prevRec;
+    ResPlanes inter; RecPlanes interRec;
+    const float2* floatingCoords;
+    const uint32_t* counts; const uint32_t* offsets; const uint32_t* sorted; const uint32_t* sortedCell;
+    const uint32_t* totalSplats;
+    float* m2curr; float* m3curr;
+    ShiftPlanes backupShift; float4* backupTerms; float2* backupM;
+    ShiftPlanes splatShift; float4* splatTerms; float4* splatM;
+};
+
+// Buffers of the wavefront spatial resampling (one iteration).
+struct SpatialCtx
+{
+    DevCtx C;
+    uint32_t iteration;
+    const uint4* vbuffer;
+    const float2* neighborOffsets;
+    ResPlanes src; RecPlanes srcRec;
+    ResPlanes dst; RecPlanes dstRec;
+    float* m1; ShiftPlanes shift; float4* terms; float* nw;
+};
+
+__global__ void k_sb_curr_scatter(WaveCtx K);
+__global__ void k_sb_curr_gather(WaveCtx K);
+__global__ void k_sb_backup_gather(WaveCtx K);
+__global__ void k_sb_backup_scatter(WaveCtx K);
+__global__ void k_sb_splat_scatter(WaveCtx K);
+__global__ void k_sb_splat_gather(WaveCtx K);
+__global__ void k_sb_combine(WaveCtx K, float4* color);
+__global__ void k_sp_central(SpatialCtx S);
+__global__ void k_sp_neighbor(SpatialCtx S);
+__global__ void k_sp_combine(SpatialCtx S, float4* color);
 
 } // namespace rs

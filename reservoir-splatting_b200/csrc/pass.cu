@@ -101,6 +101,12 @@ struct rs_pass
     DevBuf<uint32_t> targets, counts, offsets, cursor, unsortedSplats, sortedSplats, tileSums, total;
     DevBuf<Shifted> shiftedPaths;
     DevBuf<float4> scratchColor;
+    // wavefront ScatterBackup / spatial buffers
+    DevBuf<uint32_t> sortedCell;
+    DevBuf<float> m2curr, m3curr, spM1, spNw;
+    DevBuf<uint4> backupShift, splatShift, spShift;
+    DevBuf<float4> backupTerms, splatTerms, splatM, spTerms;
+    DevBuf<float2> backupM;
     DevBuf<uint32_t> fault;
     uint32_t* hostFault = nullptr;
     bool keepCandidates = false;
@@ -188,6 +194,18 @@ static rs_status allocate(rs_pass* p)
     RS_CUDA(p->cursor.ensure(P * N));
     RS_CUDA(p->unsortedSplats.ensure(P * N));
     RS_CUDA(p->sortedSplats.ensure(P * N));
+    RS_CUDA(p->sortedCell.ensure(P * N));
+    if (p->opt.temporalReuse == RS_SCATTER_BACKUP)
+    {
+        RS_CUDA(p->m2curr.ensure(N)); RS_CUDA(p->m3curr.ensure(N));
+        RS_CUDA(p->backupShift.ensure(5 * N)); RS_CUDA(p->backupTerms.ensure(N)); RS_CUDA(p->backupM.ensure(N));
+        RS_CUDA(p->splatShift.ensure(5 * N)); RS_CUDA(p->splatTerms.ensure(N)); RS_CUDA(p->splatM.ensure(N));
+    }
+    if (p->opt.enableSpatialResampling)
+    {
+        const size_t M = (size_t)p->opt.neighborCount * N;
+        RS_CUDA(p->spM1.ensure(M)); RS_CUDA(p->spNw.ensure(M)); RS_CUDA(p->spShift.ensure(5 * M)); RS_CUDA(p->spTerms.ensure(M));
+    }
     RS_CUDA(p->tileSums.ensure((N + kScanTileElems - 1) / kScanTileElems + 1));
     RS_CUDA(p->total.ensure(8));
     if (p->opt.gatherOption == RS_GATHER_ROBUST && needInter) RS_CUDA(p->shiftedPaths.ensure(8 * N));
@@ -413,12 +431,12 @@ extern "C" RS_API rs_status rs_execute(rs_pass* p, const rs_frame_desc* f, void*
     p->lastFusedCollect = false;
     const uint32_t numTiles = (N + kScanTileElems - 1) / kScanTileElems;
 
-    auto buildCells = [&](uint32_t* tg, uint32_t* cn, uint32_t* of, uint32_t* cu, uint32_t* un, uint32_t* so) {
+    auto buildCells = [&](uint32_t* tg, uint32_t* cn, uint32_t* of, uint32_t* cu, uint32_t* un, uint32_t* so, uint32_t* sc) {
         k_scan_tiles<<<numTiles, 1024, 0, s>>>(cn, of, p->tileSums.p, N);
         k_scan_tile_sums<<<1, 1024, 0, s>>>(p->tileSums.p, numTiles, p->total.p);
         k_scan_add<<<grid(N, 256), 256, 0, s>>>(of, p->tileSums.p, N);
         k_fill<<<grid(N, 256), 256, 0, s>>>(tg, of, cu, un, N);
-        k_rank_cells<<<grid(N, 256), 256, 0, s>>>(tg, of, cn, un, so, N);
+        k_rank_cells<<<grid(N, 256), 256, 0, s>>>(tg, of, cn, un, so, sc, N);
         p->launches += 5;
     };
 
@@ -444,7 +462,7 @@ extern "C" RS_API rs_status rs_execute(rs_pass* p, const rs_frame_desc* f, void*
             RS_CUDA(cudaMemsetAsync(p->cursor.p, 0, N * 4ull, s));
             k_reproject<<<grid(N, 256), 256, 0, s>>>(C, prev.res(), prev.recp(), p->targets.p, p->counts.p); p->launches++;
             stage(p, "sortCells", s);
-            buildCells(p->targets.p, p->counts.p, p->offsets.p, p->cursor.p, p->unsortedSplats.p, p->sortedSplats.p);
+            buildCells(p->targets.p, p->counts.p, p->offsets.p, p->cursor.p, p->unsortedSplats.p, p->sortedSplats.p, nullptr);
             stage(p, "scatterResample", s);
             k_scatter_resample<<<grid(N, 128), 128, 0, s>>>(C, mvec, prev.res(), prev.recp(), curr.res(), curr.recp(), p->counts.p, p->offsets.p, p->sortedSplats.p, temporalColor); p->launches++;
             break;
@@ -467,15 +485,40 @@ extern "C" RS_API rs_status rs_execute(rs_pass* p, const rs_frame_desc* f, void*
             RS_CUDA(cudaMemsetAsync(p->cursor.p, 0, N * 4ull, s));
             k_reproject<<<grid(N, 256), 256, 0, s>>>(C, prev.res(), prev.recp(), p->targets.p, p->counts.p); p->launches++;
             stage(p, "sortCells", s);
-            buildCells(p->targets.p, p->counts.p, p->offsets.p, p->cursor.p, p->unsortedSplats.p, p->sortedSplats.p);
-            stage(p, "scatterBackupResample", s);
-            if (fused)
-                k_scatter_backup_resample_clamped<<<grid(N, 128), 128, 0, s>>>(C, mvec, prev.res(), prev.recp(), curr.res(), curr.recp(),
-                                                                               p->counts.p, p->offsets.p, p->sortedSplats.p, temporalColor);
-            else
-                k_scatter_backup_resample<<<grid(N, 128), 128, 0, s>>>(C, mvec, prev.res(), prev.recp(), curr.res(), curr.recp(), p->inter.res(),
-                                                                       p->inter.recp(), p->floatingCoords.p, p->counts.p, p->offsets.p,
-                                                                       p->sortedSplats.p, temporalColor);
+            buildCells(p->targets.p, p->counts.p, p->offsets.p, p->cursor.p, p->unsortedSplats.p, p->sortedSplats.p, p->sortedCell.p);
+            WaveCtx K;
+            K.C = C;
+            K.fused = fused;
+            K.mvec = mvec;
+            K.curr = curr.res(); K.currRec = curr.recp();
+            K.prev = prev.res(); K.prevRec = prev.recp();
+            K.inter = fused ? prev.res() : p->inter.res(); K.interRec = fused ? prev.recp() : p->inter.recp();
+            K.floatingCoords = p->floatingCoords.p;
+            K.counts = p->counts.p; K.offsets = p->offsets.p; K.sorted = p->sortedSplats.p; K.sortedCell = p->sortedCell.p;
+            K.totalSplats = p->total.p;
+            K.m2curr = p->m2curr.p; K.m3curr = p->m3curr.p;
+            K.backupShift = ShiftPlanes{p->backupShift.p, (size_t)N}; K.backupTerms = p->backupTerms.p; K.backupM = p->backupM.p;
+            K.splatShift = ShiftPlanes{p->splatShift.p, (size_t)N}; K.splatTerms = p->splatTerms.p; K.splatM = p->splatM.p;
+            const bool balance = o.scatterBackupMISOption == RS_MIS_BALANCE;
+            stage(p, "sbCurrScatter", s);
+            k_sb_curr_scatter<<<grid(N, 128), 128, 0, s>>>(K);
+            stage(p, "sbCurrGather", s);
+            k_sb_curr_gather<<<grid(N, 128), 128, 0, s>>>(K);
+            stage(p, "sbBackupGather", s);
+            k_sb_backup_gather<<<grid(N, 128), 128, 0, s>>>(K);
+            stage(p, "sbSplatScatter", s);
+            k_sb_splat_scatter<<<grid(N, 128), 128, 0, s>>>(K);
+            p->launches += 4;
+            if (balance)
+            {
+                stage(p, "sbBackupScatter", s);
+                k_sb_backup_scatter<<<grid(N, 128), 128, 0, s>>>(K);
+                stage(p, "sbSplatGather", s);
+                k_sb_splat_gather<<<grid(N, 128), 128, 0, s>>>(K);
+                p->launches += 2;
+            }
+            stage(p, "sbCombine", s);
+            k_sb_combine<<<grid(N, 128), 128, 0, s>>>(K, temporalColor);
             p->launches++;
             break;
         }
@@ -490,7 +533,7 @@ extern "C" RS_API rs_status rs_execute(rs_pass* p, const rs_frame_desc* f, void*
             for (uint32_t j = 0; j < P; j++)
             {
                 size_t b = (size_t)j * N;
-                buildCells(p->targets.p + b, p->counts.p + b, p->offsets.p + b, p->cursor.p + b, p->unsortedSplats.p + b, p->sortedSplats.p + b);
+                buildCells(p->targets.p + b, p->counts.p + b, p->offsets.p + b, p->cursor.p + b, p->unsortedSplats.p + b, p->sortedSplats.p + b, nullptr);
             }
             stage(p, "multiScatterResample", s);
             k_multi_scatter_resample<<<grid(N, 128), 128, 0, s>>>(C, mvec, prev.res(), prev.recp(), curr.res(), curr.recp(), p->counts.p, p->offsets.p, p->sortedSplats.p, temporalColor); p->launches++;
@@ -509,9 +552,23 @@ extern "C" RS_API rs_status rs_execute(rs_pass* p, const rs_frame_desc* f, void*
             std::swap(p->currIdx, swapIdx);
             ReservoirSet& src = p->sets[swapIdx];
             ReservoirSet& dst = p->sets[p->currIdx];
-            stage(p, "spatialResample", s);
-            k_spatial<<<grid(N, 128), 128, 0, s>>>(C, i, p->vbuffer.p, p->neighborOffsets.p, src.res(), src.recp(), dst.res(), dst.recp(),
-                                                  i + 1 == o.numSpatialIterations ? colorDev : nullptr);
+            SpatialCtx S;
+            S.C = C;
+            S.iteration = i;
+            S.vbuffer = p->vbuffer.p;
+            S.neighborOffsets = p->neighborOffsets.p;
+            S.src = src.res(); S.srcRec = src.recp();
+            S.dst = dst.res(); S.dstRec = dst.recp();
+            S.m1 = p->spM1.p; S.nw = p->spNw.p; S.terms = p->spTerms.p;
+            S.shift = ShiftPlanes{p->spShift.p, (size_t)N * o.neighborCount};
+            const uint32_t M = N * o.neighborCount;
+            stage(p, "spatialCentral", s);
+            k_sp_central<<<grid(M, 128), 128, 0, s>>>(S);
+            stage(p, "spatialNeighbor", s);
+            k_sp_neighbor<<<grid(M, 128), 128, 0, s>>>(S);
+            stage(p, "spatialCombine", s);
+            k_sp_combine<<<grid(N, 128), 128, 0, s>>>(S, i + 1 == o.numSpatialIterations ? colorDev : nullptr);
+            p->launches += 2;
             p->launches++;
         }
         colorWritten = true;

@@ -475,4 +475,28 @@ __device__ __forceinline__ float jac_scatter(const Shifted& s, const Recon& r)
     return (s.subPixelJacobian * s.secondaryPathJacobian) / (r.subPixelJacobian * r.secondaryPathJacobian);
 }
 
+// Depth-of-field shift probabilities of a pixel (ShiftMapping.slang:43-80; GatherTemporalResampling.rt.slang:75-96)
+__device__ __forceinline__ f2 pixel_dof_probs(const DevCtx& C, const uint4* vbuffer, uint32_t i)
+{
+    if (!(C.camera.apertureRadius > 0.f)) return mk2(1.f, 0.f);
+    uint4 q = __ldg(&vbuffer[i]);
+    HitInfo h; h.w[0] = q.x; h.w[1] = q.y; h.w[2] = q.z; h.w[3] = q.w;
+    const CameraData& cam = C.camera;
+    float normalizedFilm = length(cam.cameraU / (float)C.W + cam.cameraV / (float)C.H);
+    float coc;
+    if (hit_valid(h))
+    {
+        f3 x1 = dev_sd(C, h, mk3(0.f)).posW;
+        f3 camDir = normalize(cam.cameraW);
+        float camZ = dot(x1 - cam.posW, camDir);
+        float filmZ = camZ - length(cam.cameraW);
+        float filmRadius = f_abs(cam.apertureRadius / camZ * filmZ);
+        coc = filmRadius / normalizedFilm;
+    }
+    else coc = cam.apertureRadius / normalizedFilm;
+    float gamma = 0.2f + 6.2f / (coc - 5.6f);
+    gamma = (coc <= 0.2f) ? 1.f : f_clamp(gamma, 0.2f, 1.f);
+    return mk2(gamma, 1.f - gamma);
+}
+
 } // namespace rs
