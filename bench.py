@@ -130,6 +130,21 @@ def dominant_kernel_bytes(stage: str, W: int, H: int) -> float:
     return float(per_pixel * N)
 
 
+def rank_frame_offset(rank: int) -> int:
+    """Replicas: each rank renders its own instance (the same scene, its own camera-path phase)."""
+    return 97 * rank
+
+
+def max_over_ranks(value: float, dist=None, device=None) -> float:
+    """The job time is the slowest rank's device time."""
+    if dist is None:
+        return float(value)
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_ours(args):
     import torch
     rs = _package()
@@ -154,7 +169,7 @@ def run_ours(args):
 
     def step(color_ptr=None, color_host=None):
         nonlocal frame
-        p.execute(camera(frame + 97 * rank, W, H), color_ptr=color_ptr, color_host=color_host, stream=stream.cuda_stream)
+        p.execute(camera(frame + rank_frame_offset(rank), W, H), color_ptr=color_ptr, color_host=color_host, stream=stream.cuda_stream)
         frame += 1
 
     with torch.cuda.stream(stream):
@@ -176,11 +191,9 @@ def run_ours(args):
         torch.cuda.synchronize()
     ms = start.elapsed_time(stop)
     clocks = clk.summary()
-    t = torch.tensor([ms], device=dev)
+    ms_max = max_over_ranks(ms, dist, dev)
     if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
         dist.barrier()
-    ms_max = float(t.item())
     value = world * args.steps / (ms_max / 1e3)
 
     # per-stage device times on the launching stream (CUDA events inside the pass)
@@ -208,10 +221,8 @@ def run_ours(args):
             step(None, host_np)
         e1.record(stream)
     torch.cuda.synchronize()
-    te = torch.tensor([e0.elapsed_time(e1)], device=dev)
-    if dist:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * e2e_steps / (float(te.item()) / 1e3)
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), dist, dev)
+    e2e_value = world * e2e_steps / (e2e_ms / 1e3)
 
     peak, peak_kind = _peaks()
     dom = max(stage_ms, key=stage_ms.get) if stage_ms else "initialCandidates"

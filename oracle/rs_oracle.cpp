@@ -2044,3 +2044,61 @@ __attribute__((visibility("default"))) int ro_set_buffer(ro_pass* r, int id, con
 __attribute__((visibility("default"))) uint32_t ro_frame_count(ro_pass* r) { return r->p.frameCount; }
 
 } // extern "C"
+
+// ------------------------------------------------------------------ test hooks (known-answer tests)
+extern "C" {
+
+// First n 32-bit outputs of the per-pixel stream of `kind` (0 TinyUniform, 2 PCG32).
+__attribute__((visibility("default"))) void ro_test_rng(uint32_t kind, uint32_t px, uint32_t py, uint32_t seed, uint32_t n, uint32_t* out)
+{
+    SampleGen sg = sg_create(px, py, seed, kind);
+    for (uint32_t i = 0; i < n; i++) out[i] = sg_next(sg);
+}
+__attribute__((visibility("default"))) void ro_test_tea(uint32_t v0, uint32_t v1, uint32_t* out)
+{
+    tea16(v0, v1);
+    out[0] = v0; out[1] = v1;
+}
+__attribute__((visibility("default"))) uint32_t ro_test_interleave(uint32_t x, uint32_t y) { return interleave_32bit(x, y); }
+
+// kind: 0 sin, 1 cos, 2 tan, 3 atan, 4 acos
+__attribute__((visibility("default"))) void ro_test_fmath(int kind, const float* x, float* y, uint32_t n)
+{
+    for (uint32_t i = 0; i < n; i++)
+    {
+        float v = x[i];
+        switch (kind)
+        {
+        case 0: y[i] = f_sin(v); break;
+        case 1: y[i] = f_cos(v); break;
+        case 2: y[i] = f_tan(v); break;
+        case 3: y[i] = f_atan(v); break;
+        default: y[i] = f_acos(v); break;
+        }
+    }
+}
+__attribute__((visibility("default"))) void ro_test_f16(const float* x, uint16_t* h, float* back, uint32_t n)
+{
+    for (uint32_t i = 0; i < n; i++) { h[i] = f32_to_f16(x[i]); back[i] = f16_to_f32(h[i]); }
+}
+// Alias table of `weights`; writes the packed table (2 words per entry) and returns the weight sum.
+__attribute__((visibility("default"))) double ro_test_alias(const float* w, uint32_t n, uint32_t* table)
+{
+    std::vector<float> weights(w, w + n);
+    std::vector<u2> t;
+    double sum;
+    build_alias_table(weights, t, sum);
+    for (uint32_t i = 0; i < n; i++) { table[2 * i] = t[i].x; table[2 * i + 1] = t[i].y; }
+    return sum;
+}
+// Closest hit of one ray against the oracle's BVH of a triangle soup (prim = -1 on a miss).
+__attribute__((visibility("default"))) int ro_test_closest(ro_pass* r, const float* ray, float* tuv)
+{
+    Ray q = mk_ray(mk3(ray[0], ray[1], ray[2]), mk3(ray[3], ray[4], ray[5]), ray[6], ray[7]);
+    HitInfo h; float t;
+    if (!r->p.bvh.closest(q, h, t)) return -1;
+    tuv[0] = t; f2 b = hit_bary(h); tuv[1] = b.x; tuv[2] = b.y;
+    return (int)hit_prim(h);
+}
+
+} // extern "C"

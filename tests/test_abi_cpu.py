@@ -1,0 +1,92 @@
+"""The C ABI library loads without a GPU, exports every symbol include/rs_b200.h declares, and
+its host-side option handling follows the reference pass (no device work is started here)."""
+import ctypes as C
+import re
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parent.parent
+HEADER = ROOT / "include" / "rs_b200.h"
+
+
+def declared_symbols():
+    text = HEADER.read_text()
+    return sorted(set(re.findall(r"RS_API\s+[\w\s\*]+?\b(rs_\w+)\s*\(", text)))
+
+
+def test_header_declares_the_pass_interface():
+    syms = declared_symbols()
+    for name in ("rs_create", "rs_destroy", "rs_set_options", "rs_set_scene", "rs_execute", "rs_reset",
+                 "rs_set_seed", "rs_freeze", "rs_get_buffer", "rs_set_buffer", "rs_last_error_string"):
+        assert name in syms
+
+
+def test_library_exports_every_declared_symbol(rs):
+    lib = rs.load_library()
+    missing = [s for s in declared_symbols() if not hasattr(lib, s)]
+    assert not missing, missing
+
+
+def test_default_options_match_reference_defaults(rs):
+    lib = rs.load_library()
+    o = rs.abi.RsOptions()
+    lib.rs_default_options(C.byref(o))
+    ref = rs.abi.default_options(1920, 1080)
+    for name, _ in rs.abi.RsOptions._fields_:
+        assert getattr(o, name) == pytest.approx(getattr(ref, name)), name
+    # ReservoirSplatting.h:124-184
+    assert o.samplesPerPixel == 1 and o.maxSurfaceBounces == 9 and o.temporalReuse == 0 and o.gatherOption == 0
+    assert o.enableSpatialResampling == 1 and o.neighborCount == 1 and o.spatialGatherRadius == 30.0
+    assert o.numTimePartitions == 2 and o.artificialFrameTime == pytest.approx(1 / 60)
+
+
+def test_properties_parse_like_the_render_graph_script(rs):
+    # scripts/ReservoirSplatting.py:13-21
+    props = {"samplesPerPixel": 1, "enableTemporalResampling": True, "enableSpatialResampling": True,
+             "temporalReuse": "ScatterOnly", "numTimePartitions": 2, "hybridMISOption": "Balance", "gatherOption": "Fast"}
+    o = rs.abi.options_from_properties(props, 640, 480)
+    assert o.temporalReuse == 1 and o.scatterBackupMISOption == 0 and o.gatherOption == 0
+    o = rs.abi.options_from_properties({"maxSurfaceBounces": 3}, 64, 64)
+    assert (o.maxDiffuseBounces, o.maxSpecularBounces, o.maxTransmissionBounces) == (3, 3, 3)
+    o = rs.abi.options_from_properties({"maxDiffuseBounces": 4, "maxSpecularBounces": 2}, 64, 64)
+    assert o.maxSurfaceBounces == 9  # max of the per-type limits (the transmission default is 9)
+    o = rs.abi.options_from_properties({"fixedSeed": 7}, 64, 64)
+    assert o.useFixedSeed == 1 and o.fixedSeed == 7
+    with pytest.raises(KeyError):
+        rs.abi.options_from_properties({"noSuchKey": 1}, 64, 64)
+    with pytest.raises(ValueError):
+        rs.abi.options_from_properties({"temporalReuse": "Sideways"}, 64, 64)
+
+
+@pytest.mark.parametrize("bad", [{"samplesPerPixel": 0}, {"samplesPerPixel": 17}, {"numTimePartitions": 9},
+                                 {"maxDiffuseBounces": 300}, {"specularRoughnessThreshold": 2.0}])
+def test_invalid_options_are_rejected_before_any_device_work(rs, bad):
+    lib = rs.load_library()
+    o = rs.abi.options_from_properties(bad, 64, 64)
+    h = C.c_void_p()
+    st = lib.rs_create(C.byref(o), C.byref(h))
+    assert st == rs.abi.RS_INVALID_ARG
+    assert lib.rs_last_error_string()
+
+
+def test_oversized_frame_is_rejected(rs):
+    lib = rs.load_library()
+    o = rs.abi.options_from_properties({}, 4097, 16)
+    h = C.c_void_p()
+    assert lib.rs_create(C.byref(o), C.byref(h)) == rs.abi.RS_INVALID_ARG
+    assert b"4096" in lib.rs_last_error_string()
+
+
+def test_null_arguments_return_errors(rs):
+    lib = rs.load_library()
+    assert lib.rs_destroy(None) == rs.abi.RS_INVALID_ARG
+    assert lib.rs_execute(None, None, None) == rs.abi.RS_INVALID_ARG
+    assert lib.rs_last_launch_count(None) == 0
+
+
+def test_missing_library_fails_loudly(rs, tmp_path, monkeypatch):
+    monkeypatch.setattr(rs, "_lib", None)
+    monkeypatch.setattr(rs, "LIB_PATH", tmp_path / "librs_b200.so")
+    with pytest.raises(RuntimeError, match="CUDA library missing"):
+        rs.ReservoirSplatting({}, 16, 16)
