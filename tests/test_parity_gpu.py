@@ -104,3 +104,45 @@ def test_terrain_scene_scatter_backup(rs, oracle_mod, scenes):
     props = {"temporalReuse": "ScatterBackup", "gatherOption": "Clamped", "maxSurfaceBounces": 2}
     cam = lambda f, w, h: scenes.orbit_camera(f, w, h, radius=30.0, height_above=12.0)
     run_pair(rs, oracle_mod, sc, cam, props, frames=4, width=96, height=64)
+
+
+@pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
+@pytest.mark.parametrize("props", [{"temporalReuse": "ScatterBackup", "gatherOption": "Clamped"},
+                                   {"temporalReuse": "GatherOnly", "gatherOption": "Robust"}],
+                         ids=["ScatterBackup", "GatherOnly-Robust"])
+def test_bit_exact_against_oracle(rs, oracle_mod, scenes, props):
+    """Host and device evaluate the same float expressions without contraction, so the CUDA pass
+    reproduces the oracle bit for bit (the 1e-4 tolerance elsewhere is the contract, not the need)."""
+    props = dict(props, maxSurfaceBounces=2, enableSpatialResampling=True)
+    gpu = rs.ReservoirSplatting(props, 48, 40)
+    ora = oracle_mod.OraclePass(props, 48, 40)
+    sc = scenes.cornell_box(1)
+    gpu.set_scene(sc)
+    ora.set_scene(sc)
+    for f in range(4):
+        cam = scenes.cornell_camera(f, 48, 40)
+        a, b = gpu.render(cam), ora.execute(cam)
+        assert P.bit_mismatch_fraction(a, b) == 0.0, f"frame {f}"
+        np.testing.assert_array_equal(gpu.get_buffer("curr_reservoirs").view(np.uint32), ora.get_buffer("curr_reservoirs").view(np.uint32))
+        np.testing.assert_array_equal(gpu.get_buffer("curr_reconnection"), ora.get_buffer("curr_reconnection"))
+    gpu.close()
+
+
+@pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
+@pytest.mark.parametrize("name", ["cornell_scatteronly", "cornell_scatterbackup"])
+def test_gpu_matches_committed_golden(rs, scenes, name):
+    import sys
+    from pathlib import Path
+    golden = Path(__file__).resolve().parent / "golden"
+    sys.path.insert(0, str(golden))
+    import make_golden
+    ref = np.load(golden / f"{name}.npz")
+    size = make_golden.GOLDEN_SIZE
+    gpu = rs.ReservoirSplatting(make_golden.GOLDEN_RUNS[name], size, size)
+    gpu.set_scene(scenes.cornell_box(0))
+    for f in range(make_golden.GOLDEN_FRAMES):
+        img = gpu.render(scenes.cornell_camera(f, size, size))
+    P.assert_close("color", img, ref["color"])
+    P.compare_reservoirs("reservoirs", gpu.get_buffer("curr_reservoirs"), ref["reservoirs"])
+    P.compare_recon("reconnection", gpu.get_buffer("curr_reconnection"), ref["reconnection"])
+    gpu.close()
