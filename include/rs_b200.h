@@ -186,6 +186,18 @@ RS_API rs_status rs_get_stage_times(rs_pass* pass, float* ms, uint32_t* count, c
 RS_API uint32_t rs_last_launch_count(rs_pass* pass);
 RS_API const char* rs_last_error_string(void);
 
+/* Batched instances (no reference counterpart: the reference renders one pass per render graph).
+ * rs_batch_execute renders one frame of every member with one CUDA graph launch on `cudaStream`;
+ * the members' stage chains are graph branches that run concurrently.  frames[i] belongs to
+ * passes[i] and must carry a device colour buffer; graphs are cached per set of colour buffers and
+ * per buffer-parity pattern, so keep the buffers stable across frames.  The call returns after the
+ * launch; the previous batch frame is awaited before a member's context is rewritten. */
+typedef struct rs_batch rs_batch;
+RS_API rs_status rs_batch_create(rs_pass* const* passes, uint32_t count, rs_batch** out);
+RS_API rs_status rs_batch_execute(rs_batch* batch, const rs_frame_desc* frames, void* cudaStream);
+RS_API rs_status rs_batch_destroy(rs_batch* batch);
+RS_API uint32_t rs_batch_launch_count(rs_batch* batch);
+
 #ifdef __cplusplus
 }
 #endif

@@ -56,9 +56,14 @@ def load_library():
     lib.rs_last_launch_count.restype = C.c_uint32
     lib.rs_last_error_string.restype = C.c_char_p
     lib.rs_debug_keep_candidates.argtypes = [C.c_void_p, C.c_uint32]
+    lib.rs_batch_create.argtypes = [C.POINTER(C.c_void_p), C.c_uint32, C.POINTER(C.c_void_p)]
+    lib.rs_batch_execute.argtypes = [C.c_void_p, C.POINTER(abi.RsFrameDesc), C.c_void_p]
+    lib.rs_batch_destroy.argtypes = [C.c_void_p]
+    lib.rs_batch_launch_count.argtypes = [C.c_void_p]
+    lib.rs_batch_launch_count.restype = C.c_uint32
     for name in ("rs_create", "rs_destroy", "rs_set_options", "rs_set_scene", "rs_execute", "rs_reset", "rs_set_seed",
                  "rs_freeze", "rs_get_buffer", "rs_set_buffer", "rs_enable_stage_timing", "rs_get_stage_times",
-                 "rs_debug_keep_candidates"):
+                 "rs_debug_keep_candidates", "rs_batch_create", "rs_batch_execute", "rs_batch_destroy"):
         getattr(lib, name).restype = C.c_int
     _lib = lib
     return lib
@@ -181,6 +186,40 @@ class ReservoirSplatting:
 
     def last_launch_count(self) -> int:
         return int(self._lib.rs_last_launch_count(self._h))
+
+
+class Batch:
+    """Renders one frame of several passes with one CUDA graph launch (rs_batch_execute)."""
+
+    def __init__(self, passes):
+        self._lib = load_library()
+        self.passes = list(passes)
+        arr = (C.c_void_p * len(self.passes))(*[p._h.value for p in self.passes])
+        h = C.c_void_p()
+        _check(self._lib.rs_batch_create(arr, len(self.passes), C.byref(h)))
+        self._h = h
+
+    def execute(self, cameras, color_ptrs, stream: int = 0, should_reset: bool = False):
+        frames = (abi.RsFrameDesc * len(self.passes))()
+        for f, cam, ptr in zip(frames, cameras, color_ptrs):
+            f.camera = abi.camera_struct(cam)
+            f.color = ptr
+            f.sceneShouldReset = 1 if should_reset else 0
+        _check(self._lib.rs_batch_execute(self._h, frames, C.c_void_p(stream)))
+
+    def launch_count(self) -> int:
+        return int(self._lib.rs_batch_launch_count(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.rs_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def createPass(name: str, props: dict | None = None, width: int = 1920, height: int = 1080) -> ReservoirSplatting:

@@ -8,12 +8,23 @@
 
 namespace rs {
 
+// Per-pass frame constants, one slot per live pass (kMaxPassSlots), indexed by a kernel argument.
+// Reads with a warp-uniform slot are served by the constant cache; the host updates a slot with a
+// stream-ordered copy (a memcpy node inside a captured graph).
+__constant__ DevCtx c_ctx[kMaxPassSlots];
+
+cudaError_t upload_ctx(uint32_t slot, const DevCtx* hostPinned, cudaStream_t s)
+{
+    return cudaMemcpyToSymbolAsync(c_ctx, hostPinned, sizeof(DevCtx), slot * sizeof(DevCtx), cudaMemcpyHostToDevice, s);
+}
+
 // ============================================================ primary hits + motion vectors
 // VBufferRT.slang:71-150 (samplePattern Center, pinhole): hit of the pixel-centre ray of the
 // frame's camera and mvec = prevScreen - (pixel + 0.5) / dim, prevScreen being the film
 // projection of the hit point through the previous frame's camera.
-__global__ void __launch_bounds__(256) k_vbuffer(DevCtx C, uint4* __restrict__ vbuffer, float2* __restrict__ mvec)
+__global__ void __launch_bounds__(256) k_vbuffer(uint32_t slot, uint4* __restrict__ vbuffer, float2* __restrict__ mvec)
 {
+    const DevCtx& C = c_ctx[slot];
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= C.W * C.H) return;
     uint32_t x = i % C.W, y = i / C.W;
@@ -290,8 +301,9 @@ __device__ void handle_hit(const DevCtx& C, PState& path)
 }
 
 // InitialCandidates.cs.slang:80-141 + addCandidateReservoir (:52-75)
-__global__ void __launch_bounds__(128) k_candidates(DevCtx C, ResPlanes curr, RecPlanes currRec)
+__global__ void __launch_bounds__(128) k_candidates(uint32_t slot, ResPlanes curr, RecPlanes currRec)
 {
+    const DevCtx& C = c_ctx[slot];
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= C.W * C.H) return;
     uint32_t x = i % C.W, y = i / C.W;
@@ -365,9 +377,10 @@ __global__ void __launch_bounds__(128) k_candidates(DevCtx C, ResPlanes curr, Re
 // ============================================================ forward reprojection (splat)
 // ReprojectTemporalSamples.rt.slang:64-175.  Writes the destination cell of every source pixel
 // and counts splats per cell; the cell lists are built by k_fill / k_rank_cells.
-__global__ void __launch_bounds__(256) k_reproject(DevCtx C, ResPlanes prev, RecPlanes prevRec,
+__global__ void __launch_bounds__(256) k_reproject(uint32_t slot, ResPlanes prev, RecPlanes prevRec,
                                                    uint32_t* __restrict__ targets, uint32_t* __restrict__ counts)
 {
+    const DevCtx& C = c_ctx[slot];
     uint32_t ci = blockIdx.x * blockDim.x + threadIdx.x;
     if (ci >= C.W * C.H) return;
     uint32_t target = kInvalidIndex;
@@ -406,9 +419,10 @@ __global__ void __launch_bounds__(256) k_reproject(DevCtx C, ResPlanes prev, Rec
 }
 
 // MultiReprojectTemporalSamples.rt.slang:65-168 (P partitions; targets/counts hold P planes of N)
-__global__ void __launch_bounds__(256) k_multi_reproject(DevCtx C, ResPlanes prev, RecPlanes prevRec,
+__global__ void __launch_bounds__(256) k_multi_reproject(uint32_t slot, ResPlanes prev, RecPlanes prevRec,
                                                          uint32_t* __restrict__ targets, uint32_t* __restrict__ counts)
 {
+    const DevCtx& C = c_ctx[slot];
     uint32_t ci = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t N = C.W * C.H;
     if (ci >= N) return;
@@ -575,10 +589,11 @@ __device__ __forceinline__ f2 prev_pixel_from_mvec(const DevCtx& C, const float2
     return mk2((float)x + mv.x * (float)C.W, (float)y + mv.y * (float)C.H);
 }
 
-__global__ void __launch_bounds__(128) k_collect(DevCtx C, const float2* __restrict__ mvec, ResPlanes prev, RecPlanes prevRec,
+__global__ void __launch_bounds__(128) k_collect(uint32_t slot, const float2* __restrict__ mvec, ResPlanes prev, RecPlanes prevRec,
                                                  ResPlanes inter, RecPlanes interRec, float2* __restrict__ floatingCoords,
                                                  const Shifted* __restrict__ shiftedPaths)
 {
+    const DevCtx& C = c_ctx[slot];
     uint32_t ci = blockIdx.x * blockDim.x + threadIdx.x;
     if (ci >= C.W * C.H) return;
     uint32_t x = ci % C.W, y = ci / C.W;
@@ -710,8 +725,9 @@ __global__ void __launch_bounds__(128) k_collect(DevCtx C, const float2* __restr
 }
 
 // RobustReuseOptimization.rt.slang:63-89
-__global__ void __launch_bounds__(128) k_robust(DevCtx C, ResPlanes prev, RecPlanes prevRec, Shifted* __restrict__ shiftedPaths)
+__global__ void __launch_bounds__(128) k_robust(uint32_t slot, ResPlanes prev, RecPlanes prevRec, Shifted* __restrict__ shiftedPaths)
 {
+    const DevCtx& C = c_ctx[slot];
     uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= C.W * C.H) return;
     uint32_t x = idx % C.W, y = idx / C.W;
@@ -756,11 +772,12 @@ __device__ __forceinline__ void write_color(float4* color, uint32_t i, const Res
 }
 
 // ScatterTemporalResampling.rt.slang:65-174
-__global__ void __launch_bounds__(128) k_scatter_resample(DevCtx C, const float2* __restrict__ mvec, ResPlanes prev, RecPlanes prevRec,
+__global__ void __launch_bounds__(128) k_scatter_resample(uint32_t slot, const float2* __restrict__ mvec, ResPlanes prev, RecPlanes prevRec,
                                                           ResPlanes curr, RecPlanes currRec, const uint32_t* __restrict__ counts,
                                                           const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ sorted,
                                                           float4* __restrict__ color)
 {
+    const DevCtx& C = c_ctx[slot];
     uint32_t ri = blockIdx.x * blockDim.x + threadIdx.x;
     if (ri >= C.W * C.H) return;
     uint32_t x = ri % C.W, y = ri / C.W;
@@ -815,10 +832,11 @@ __global__ void __launch_bounds__(128) k_scatter_resample(DevCtx C, const float2
 }
 
 // GatherTemporalResampling.rt.slang:68-235
-__global__ void __launch_bounds__(128) k_gather_resample(DevCtx C, const uint4* __restrict__ vbuffer, ResPlanes curr, RecPlanes currRec,
+__global__ void __launch_bounds__(128) k_gather_resample(uint32_t slot, const uint4* __restrict__ vbuffer, ResPlanes curr, RecPlanes currRec,
                                                          ResPlanes inter, RecPlanes interRec, const float2* __restrict__ floatingCoords,
                                                          float4* __restrict__ color)
 {
+    const DevCtx& C = c_ctx[slot];
     uint32_t ri = blockIdx.x * blockDim.x + threadIdx.x;
     if (ri >= C.W * C.H) return;
     uint32_t x = ri % C.W, y = ri / C.W;
@@ -886,11 +904,12 @@ __global__ void __launch_bounds__(128) k_gather_resample(DevCtx C, const uint4* 
 }
 
 // MultiScatterTemporalResampling.rt.slang:65-186
-__global__ void __launch_bounds__(128) k_multi_scatter_resample(DevCtx C, const float2* __restrict__ mvec, ResPlanes prev, RecPlanes prevRec,
+__global__ void __launch_bounds__(128) k_multi_scatter_resample(uint32_t slot, const float2* __restrict__ mvec, ResPlanes prev, RecPlanes prevRec,
                                                                 ResPlanes curr, RecPlanes currRec, const uint32_t* __restrict__ counts,
                                                                 const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ sortedAll,
                                                                 float4* __restrict__ color)
 {
+    const DevCtx& C = c_ctx[slot];
     uint32_t ri = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t N = C.W * C.H;
     if (ri >= N) return;
@@ -967,3 +986,6 @@ __global__ void __launch_bounds__(256) k_resolve(uint32_t n, ResPlanes curr, flo
 }
 
 } // namespace rs
+
+// The wavefront kernels share the constant context table, so they live in this translation unit.
+#include "wavefront.cuh"

@@ -4,26 +4,29 @@
 
 namespace rs {
 
-__global__ void k_vbuffer(DevCtx C, uint4* vbuffer, float2* mvec);
-__global__ void k_candidates(DevCtx C, ResPlanes curr, RecPlanes currRec);
-__global__ void k_reproject(DevCtx C, ResPlanes prev, RecPlanes prevRec, uint32_t* targets, uint32_t* counts);
-__global__ void k_multi_reproject(DevCtx C, ResPlanes prev, RecPlanes prevRec, uint32_t* targets, uint32_t* counts);
+__global__ void k_vbuffer(uint32_t slot, uint4* vbuffer, float2* mvec);
+__global__ void k_candidates(uint32_t slot, ResPlanes curr, RecPlanes currRec);
+__global__ void k_reproject(uint32_t slot, ResPlanes prev, RecPlanes prevRec, uint32_t* targets, uint32_t* counts);
+__global__ void k_multi_reproject(uint32_t slot, ResPlanes prev, RecPlanes prevRec, uint32_t* targets, uint32_t* counts);
 __global__ void k_scan_tiles(const uint32_t* in, uint32_t* out, uint32_t* tileSums, uint32_t n);
 __global__ void k_scan_tile_sums(uint32_t* tileSums, uint32_t numTiles, uint32_t* totalOut);
 __global__ void k_scan_add(uint32_t* out, const uint32_t* tileSums, uint32_t n);
 __global__ void k_fill(const uint32_t* targets, const uint32_t* offsets, uint32_t* cursor, uint32_t* unsorted, uint32_t n);
 __global__ void k_rank_cells(const uint32_t* targets, const uint32_t* offsets, const uint32_t* counts, const uint32_t* unsorted,
                              uint32_t* sorted, uint32_t* sortedCell, uint32_t n);
-__global__ void k_collect(DevCtx C, const float2* mvec, ResPlanes prev, RecPlanes prevRec, ResPlanes inter, RecPlanes interRec,
+__global__ void k_collect(uint32_t slot, const float2* mvec, ResPlanes prev, RecPlanes prevRec, ResPlanes inter, RecPlanes interRec,
                           float2* floatingCoords, const Shifted* shiftedPaths);
-__global__ void k_robust(DevCtx C, ResPlanes prev, RecPlanes prevRec, Shifted* shiftedPaths);
-__global__ void k_scatter_resample(DevCtx C, const float2* mvec, ResPlanes prev, RecPlanes prevRec, ResPlanes curr, RecPlanes currRec,
+__global__ void k_robust(uint32_t slot, ResPlanes prev, RecPlanes prevRec, Shifted* shiftedPaths);
+__global__ void k_scatter_resample(uint32_t slot, const float2* mvec, ResPlanes prev, RecPlanes prevRec, ResPlanes curr, RecPlanes currRec,
                                    const uint32_t* counts, const uint32_t* offsets, const uint32_t* sorted, float4* color);
-__global__ void k_gather_resample(DevCtx C, const uint4* vbuffer, ResPlanes curr, RecPlanes currRec, ResPlanes inter, RecPlanes interRec,
+__global__ void k_gather_resample(uint32_t slot, const uint4* vbuffer, ResPlanes curr, RecPlanes currRec, ResPlanes inter, RecPlanes interRec,
                                   const float2* floatingCoords, float4* color);
-__global__ void k_multi_scatter_resample(DevCtx C, const float2* mvec, ResPlanes prev, RecPlanes prevRec, ResPlanes curr, RecPlanes currRec,
+__global__ void k_multi_scatter_resample(uint32_t slot, const float2* mvec, ResPlanes prev, RecPlanes prevRec, ResPlanes curr, RecPlanes currRec,
                                          const uint32_t* counts, const uint32_t* offsets, const uint32_t* sortedAll, float4* color);
 __global__ void k_resolve(uint32_t n, ResPlanes curr, float4* color);
+
+constexpr uint32_t kMaxPassSlots = 64; // passes alive at once (size of the constant context table)
+cudaError_t upload_ctx(uint32_t slot, const DevCtx* hostPinned, cudaStream_t s);
 
 constexpr int kScanTileElems = 4096; // k_scan_tiles: 1024 threads x 4 items
 
@@ -34,7 +37,6 @@ struct ShiftPlanes { uint4* p; size_t stride; };
 // Buffers of the wavefront ScatterBackup resampling (wavefront.cu).
 struct WaveCtx
 {
-    DevCtx C;
     bool fused;                 // Clamped gather read directly from the previous frame
     const float2* mvec;
     ResPlanes curr; RecPlanes currRec;
@@ -51,7 +53,6 @@ struct WaveCtx
 // Buffers of the wavefront spatial resampling (one iteration).
 struct SpatialCtx
 {
-    DevCtx C;
     uint32_t iteration;
     const uint4* vbuffer;
     const float2* neighborOffsets;
@@ -60,15 +61,15 @@ struct SpatialCtx
     float* m1; ShiftPlanes shift; float4* terms; float* nw;
 };
 
-__global__ void k_sb_curr_scatter(WaveCtx K);
-__global__ void k_sb_curr_gather(WaveCtx K);
-__global__ void k_sb_backup_gather(WaveCtx K);
-__global__ void k_sb_backup_scatter(WaveCtx K);
-__global__ void k_sb_splat_scatter(WaveCtx K);
-__global__ void k_sb_splat_gather(WaveCtx K);
-__global__ void k_sb_combine(WaveCtx K, float4* color);
-__global__ void k_sp_central(SpatialCtx S);
-__global__ void k_sp_neighbor(SpatialCtx S);
-__global__ void k_sp_combine(SpatialCtx S, float4* color);
+__global__ void k_sb_curr_scatter(uint32_t slot, WaveCtx K);
+__global__ void k_sb_curr_gather(uint32_t slot, WaveCtx K);
+__global__ void k_sb_backup_gather(uint32_t slot, WaveCtx K);
+__global__ void k_sb_backup_scatter(uint32_t slot, WaveCtx K);
+__global__ void k_sb_splat_scatter(uint32_t slot, WaveCtx K);
+__global__ void k_sb_splat_gather(uint32_t slot, WaveCtx K);
+__global__ void k_sb_combine(uint32_t slot, WaveCtx K, float4* color);
+__global__ void k_sp_central(uint32_t slot, SpatialCtx S);
+__global__ void k_sp_neighbor(uint32_t slot, SpatialCtx S);
+__global__ void k_sp_combine(uint32_t slot, SpatialCtx S, float4* color);
 
 } // namespace rs

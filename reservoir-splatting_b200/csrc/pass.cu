@@ -11,6 +11,7 @@
 #include <string>
 #include <vector>
 #include <memory>
+#include <mutex>
 #include "../../include/rs_b200.h"
 #include "kernels.h"
 #include "bvh_build.h"
@@ -73,6 +74,22 @@ struct ReservoirSet
 
 } // namespace
 
+static std::mutex g_slotMutex;
+static bool g_slotUsed[kMaxPassSlots] = {};
+
+static uint32_t acquire_slot()
+{
+    std::lock_guard<std::mutex> lock(g_slotMutex);
+    for (uint32_t i = 0; i < kMaxPassSlots; i++)
+        if (!g_slotUsed[i]) { g_slotUsed[i] = true; return i; }
+    return kMaxPassSlots;
+}
+static void release_slot(uint32_t s)
+{
+    std::lock_guard<std::mutex> lock(g_slotMutex);
+    if (s < kMaxPassSlots) g_slotUsed[s] = false;
+}
+
 struct rs_pass
 {
     rs_options opt;
@@ -109,6 +126,14 @@ struct rs_pass
     DevBuf<float2> backupM;
     DevBuf<uint32_t> fault;
     uint32_t* hostFault = nullptr;
+    uint32_t slot = kMaxPassSlots;  // this pass's entry of the constant context table
+    DevCtx* hostCtx = nullptr;      // staging copy of the frame's context (begin_frame)
+    static constexpr int kRing = 8;
+    DevCtx* ringCtx = nullptr;      // pinned upload sources for rs_execute, reused round-robin
+    cudaEvent_t ringEv[kRing] = {};
+    int ringNext = 0;
+    DevCtx* graphCtx = nullptr;     // pinned upload source read by a replayed batch graph
+    bool frameShouldReset = false;
     bool keepCandidates = false;
     bool lastFusedCollect = false;
     cudaStream_t lastStream = 0;
@@ -122,7 +147,12 @@ struct rs_pass
     ~rs_pass()
     {
         for (auto e : events) cudaEventDestroy(e);
+        for (auto e : ringEv) if (e) cudaEventDestroy(e);
         if (hostFault) cudaFreeHost(hostFault);
+        if (hostCtx) cudaFreeHost(hostCtx);
+        if (ringCtx) cudaFreeHost(ringCtx);
+        if (graphCtx) cudaFreeHost(graphCtx);
+        release_slot(slot);
     }
 };
 
@@ -211,6 +241,13 @@ static rs_status allocate(rs_pass* p)
     if (p->opt.gatherOption == RS_GATHER_ROBUST && needInter) RS_CUDA(p->shiftedPaths.ensure(8 * N));
     RS_CUDA(p->fault.ensure(1));
     if (!p->hostFault) RS_CUDA(cudaMallocHost(&p->hostFault, sizeof(uint32_t)));
+    if (!p->hostCtx) RS_CUDA(cudaMallocHost(&p->hostCtx, sizeof(DevCtx)));
+    if (!p->ringCtx)
+    {
+        RS_CUDA(cudaMallocHost(&p->ringCtx, sizeof(DevCtx) * rs_pass::kRing));
+        for (auto& e : p->ringEv) RS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    if (!p->graphCtx) RS_CUDA(cudaMallocHost(&p->graphCtx, sizeof(DevCtx)));
     if (!p->neighborOffsets.p)
     {
         // createNeighborOffsetTexture (ReservoirSplatting.cpp:1072-1097), decoded as RG8Snorm
@@ -248,6 +285,8 @@ extern "C" RS_API rs_status rs_create(const rs_options* opts, rs_pass** out)
     rs_status s = validate(opts);
     if (s != RS_OK) return s;
     std::unique_ptr<rs_pass> p(new rs_pass());
+    p->slot = acquire_slot();
+    if (p->slot >= kMaxPassSlots) return fail(RS_INVALID_ARG, "at most 64 passes can exist at once");
     p->opt = *opts;
     s = allocate(p.get());
     if (s != RS_OK) return s;
@@ -340,20 +379,11 @@ static void stage(rs_pass* p, const char* name, cudaStream_t s)
     cudaEventRecord(p->events[k], s);
 }
 
-extern "C" RS_API rs_status rs_execute(rs_pass* p, const rs_frame_desc* f, void* streamPtr)
+// beginFrame (ReservoirSplatting.cpp:1550-1646) and prepareCameraManager (:1359-1388): host-side
+// frame state and the device context of the frame (written to p->hostCtx).
+static void begin_frame(rs_pass* p, const rs_frame_desc* f)
 {
-    if (!p || !f) return fail(RS_INVALID_ARG, "pass or frame is NULL");
-    if (!p->hasScene) return fail(RS_NOT_READY, "no scene set");
-    if (!f->color && !f->colorHost) return fail(RS_INVALID_ARG, "no colour output");
-    cudaStream_t s = (cudaStream_t)streamPtr;
-    p->lastStream = s;
-    p->launches = 0;
-    p->stageNames.clear();
-    const uint32_t W = p->W, H = p->H;
-    const uint32_t N = W * H;
     const rs_options& o = p->opt;
-
-    // beginFrame (ReservoirSplatting.cpp:1550-1646)
     p->seed = o.useFixedSeed ? o.fixedSeed : p->seed + 1;
     p->camera = to_camera(f->camera);
     uint32_t K = 1u + (uint32_t)ceilf(p->camera.shutterSpeed / o.artificialFrameTime) + 1u;
@@ -361,15 +391,14 @@ extern "C" RS_API rs_status rs_execute(rs_pass* p, const rs_frame_desc* f, void*
     bool keyframesChanged = K != p->prevK;
     p->prevK = K;
     p->K = K;
-    bool shouldReset = f->sceneShouldReset != 0;
-    // prepareCameraManager (:1359-1388)
+    p->frameShouldReset = f->sceneShouldReset != 0;
     p->cm.artificialFrameTime = o.artificialFrameTime;
     p->cm.keyframes = K;
-    if (p->frameCount == 0 || shouldReset || keyframesChanged)
+    if (p->frameCount == 0 || p->frameShouldReset || keyframesChanged)
         for (uint32_t i = 0; i < K; i++) { p->cm.positions[i] = p->camera.posW; p->cm.targets[i] = p->camera.target; }
     else { p->cm.positions[p->frameCount % K] = p->camera.posW; p->cm.targets[p->frameCount % K] = p->camera.target; }
 
-    DevCtx C;
+    DevCtx& C = *p->hostCtx;
     memset(&C, 0, sizeof(C));
     C.bvh.nodes = p->dNodes.p;
     C.bvh.tri = p->dTri.p;
@@ -383,7 +412,7 @@ extern "C" RS_API rs_status rs_execute(rs_pass* p, const rs_frame_desc* f, void*
     C.camera = p->camera;
     C.prevCamera = p->havePrevCamera ? p->prevCamera : p->camera;
     C.cm = p->cm;
-    C.W = W; C.H = H;
+    C.W = p->W; C.H = p->H;
     C.frameCount = p->frameCount; C.seed = p->seed;
     C.useFixedSeed = o.useFixedSeed; C.fixedSeed = o.fixedSeed;
     C.sgKind = o.sampleGenerator;
@@ -396,23 +425,63 @@ extern "C" RS_API rs_status rs_execute(rs_pass* p, const rs_frame_desc* f, void*
     C.gatherOption = o.gatherOption; C.scatterBackupMIS = o.scatterBackupMISOption; C.numTimePartitions = o.numTimePartitions;
     C.neighborCount = o.neighborCount; C.spatialGatherRadius = o.spatialGatherRadius;
     C.fault = p->fault.p;
+}
 
+// The spatial ping-pong of spatialResampling (ReservoirSplatting.cpp:2002-2018) on the host-side indices.
+static void apply_spatial_swaps(rs_pass* p)
+{
+    if (!p->opt.enableSpatialResampling) return;
+    int& swapIdx = p->frozen ? p->tempIdx : p->prevIdx;
+    for (uint32_t i = 0; i < p->opt.numSpatialIterations; i++) std::swap(p->currIdx, swapIdx);
+}
+
+// endFrame (ReservoirSplatting.cpp:1648-1680)
+static void end_frame(rs_pass* p)
+{
+    apply_spatial_swaps(p);
+    p->swapped = !p->frozen;
+    if (!p->frozen)
+    {
+        p->frameCount++;
+        std::swap(p->currIdx, p->prevIdx);
+    }
+    p->prevCamera = p->camera;
+    p->havePrevCamera = true;
+}
+
+// Issues the frame's device work on `s`.  The frame context goes to the pass's constant-memory
+// slot by a stream-ordered copy from pinned memory: in graph mode from p->graphCtx (a replayed graph
+// reads the context current at replay time), otherwise from a ring entry that is not reused until
+// its copy has run.
+static rs_status enqueue_frame(rs_pass* p, cudaStream_t s, float4* colorDev, const float2* mvecIn, bool graphMode)
+{
+    const uint32_t W = p->W, H = p->H;
+    const uint32_t N = W * H;
+    const rs_options& o = p->opt;
+    if (graphMode)
+    {
+        RS_CUDA(upload_ctx(p->slot, p->graphCtx, s));
+    }
+    else
+    {
+        const int k = p->ringNext;
+        p->ringNext = (k + 1) % rs_pass::kRing;
+        RS_CUDA(cudaEventSynchronize(p->ringEv[k])); // the copy issued kRing frames ago has run
+        p->ringCtx[k] = *p->hostCtx;
+        RS_CUDA(upload_ctx(p->slot, &p->ringCtx[k], s));
+        RS_CUDA(cudaEventRecord(p->ringEv[k], s));
+    }
+    const uint32_t C = p->slot;
+    bool shouldReset = p->frameShouldReset;
     ReservoirSet& curr = p->sets[p->currIdx];
     ReservoirSet& prev = p->sets[p->prevIdx];
-    float4* colorDev = reinterpret_cast<float4*>(f->color);
-    if (!colorDev)
-    {
-        RS_CUDA(p->scratchColor.ensure(N)); // allocated on the first host-output frame only
-        colorDev = p->scratchColor.p;
-    }
     auto grid = [](uint32_t n, uint32_t b) { return dim3((n + b - 1) / b); };
     RS_CUDA(cudaMemsetAsync(p->fault.p, 0, sizeof(uint32_t), s));
 
     // producer side: primary hits + motion vectors (VBufferRT)
     stage(p, "vbuffer", s);
     k_vbuffer<<<grid(N, 256), 256, 0, s>>>(C, p->vbuffer.p, p->mvec.p); p->launches++;
-    const float2* mvec = p->mvec.p;
-    if (f->mvec) mvec = reinterpret_cast<const float2*>(f->mvec);
+    const float2* mvec = mvecIn ? mvecIn : p->mvec.p;
 
     stage(p, "initialCandidates", s);
     k_candidates<<<grid(N, 128), 128, 0, s>>>(C, curr.res(), curr.recp()); p->launches++;
@@ -487,7 +556,6 @@ extern "C" RS_API rs_status rs_execute(rs_pass* p, const rs_frame_desc* f, void*
             stage(p, "sortCells", s);
             buildCells(p->targets.p, p->counts.p, p->offsets.p, p->cursor.p, p->unsortedSplats.p, p->sortedSplats.p, p->sortedCell.p);
             WaveCtx K;
-            K.C = C;
             K.fused = fused;
             K.mvec = mvec;
             K.curr = curr.res(); K.currRec = curr.recp();
@@ -501,24 +569,24 @@ extern "C" RS_API rs_status rs_execute(rs_pass* p, const rs_frame_desc* f, void*
             K.splatShift = ShiftPlanes{p->splatShift.p, (size_t)N}; K.splatTerms = p->splatTerms.p; K.splatM = p->splatM.p;
             const bool balance = o.scatterBackupMISOption == RS_MIS_BALANCE;
             stage(p, "sbCurrScatter", s);
-            k_sb_curr_scatter<<<grid(N, 128), 128, 0, s>>>(K);
+            k_sb_curr_scatter<<<grid(N, 128), 128, 0, s>>>(C, K);
             stage(p, "sbCurrGather", s);
-            k_sb_curr_gather<<<grid(N, 128), 128, 0, s>>>(K);
+            k_sb_curr_gather<<<grid(N, 128), 128, 0, s>>>(C, K);
             stage(p, "sbBackupGather", s);
-            k_sb_backup_gather<<<grid(N, 128), 128, 0, s>>>(K);
+            k_sb_backup_gather<<<grid(N, 128), 128, 0, s>>>(C, K);
             stage(p, "sbSplatScatter", s);
-            k_sb_splat_scatter<<<grid(N, 128), 128, 0, s>>>(K);
+            k_sb_splat_scatter<<<grid(N, 128), 128, 0, s>>>(C, K);
             p->launches += 4;
             if (balance)
             {
                 stage(p, "sbBackupScatter", s);
-                k_sb_backup_scatter<<<grid(N, 128), 128, 0, s>>>(K);
+                k_sb_backup_scatter<<<grid(N, 128), 128, 0, s>>>(C, K);
                 stage(p, "sbSplatGather", s);
-                k_sb_splat_gather<<<grid(N, 128), 128, 0, s>>>(K);
+                k_sb_splat_gather<<<grid(N, 128), 128, 0, s>>>(C, K);
                 p->launches += 2;
             }
             stage(p, "sbCombine", s);
-            k_sb_combine<<<grid(N, 128), 128, 0, s>>>(K, temporalColor);
+            k_sb_combine<<<grid(N, 128), 128, 0, s>>>(C, K, temporalColor);
             p->launches++;
             break;
         }
@@ -546,14 +614,16 @@ extern "C" RS_API rs_status rs_execute(rs_pass* p, const rs_frame_desc* f, void*
     {
         // spatialResampling (ReservoirSplatting.cpp:1994-2020): ping-pong with the prev (or, when
         // frozen, the temp) buffer
-        int& swapIdx = p->frozen ? p->tempIdx : p->prevIdx;
+        // (on local indices: the host-side transition is apply_spatial_swaps, run for every frame
+        // whether this function issued the work or a replayed graph did)
+        int cur = p->currIdx, prv = p->prevIdx, tmp = p->tempIdx;
+        int& swapIdx = p->frozen ? tmp : prv;
         for (uint32_t i = 0; i < o.numSpatialIterations; i++)
         {
-            std::swap(p->currIdx, swapIdx);
+            std::swap(cur, swapIdx);
             ReservoirSet& src = p->sets[swapIdx];
-            ReservoirSet& dst = p->sets[p->currIdx];
+            ReservoirSet& dst = p->sets[cur];
             SpatialCtx S;
-            S.C = C;
             S.iteration = i;
             S.vbuffer = p->vbuffer.p;
             S.neighborOffsets = p->neighborOffsets.p;
@@ -563,11 +633,11 @@ extern "C" RS_API rs_status rs_execute(rs_pass* p, const rs_frame_desc* f, void*
             S.shift = ShiftPlanes{p->spShift.p, (size_t)N * o.neighborCount};
             const uint32_t M = N * o.neighborCount;
             stage(p, "spatialCentral", s);
-            k_sp_central<<<grid(M, 128), 128, 0, s>>>(S);
+            k_sp_central<<<grid(M, 128), 128, 0, s>>>(C, S);
             stage(p, "spatialNeighbor", s);
-            k_sp_neighbor<<<grid(M, 128), 128, 0, s>>>(S);
+            k_sp_neighbor<<<grid(M, 128), 128, 0, s>>>(C, S);
             stage(p, "spatialCombine", s);
-            k_sp_combine<<<grid(N, 128), 128, 0, s>>>(S, i + 1 == o.numSpatialIterations ? colorDev : nullptr);
+            k_sp_combine<<<grid(N, 128), 128, 0, s>>>(C, S, i + 1 == o.numSpatialIterations ? colorDev : nullptr);
             p->launches += 2;
             p->launches++;
         }
@@ -581,20 +651,34 @@ extern "C" RS_API rs_status rs_execute(rs_pass* p, const rs_frame_desc* f, void*
     stage(p, "end", s);
     RS_CUDA(cudaGetLastError());
     RS_CUDA(cudaMemcpyAsync(p->hostFault, p->fault.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    return RS_OK;
+}
+
+extern "C" RS_API rs_status rs_execute(rs_pass* p, const rs_frame_desc* f, void* streamPtr)
+{
+    if (!p || !f) return fail(RS_INVALID_ARG, "pass or frame is NULL");
+    if (!p->hasScene) return fail(RS_NOT_READY, "no scene set");
+    if (!f->color && !f->colorHost) return fail(RS_INVALID_ARG, "no colour output");
+    cudaStream_t s = (cudaStream_t)streamPtr;
+    p->lastStream = s;
+    p->launches = 0;
+    p->stageNames.clear();
+    const size_t N = (size_t)p->W * p->H;
+    float4* colorDev = reinterpret_cast<float4*>(f->color);
+    if (!colorDev)
+    {
+        RS_CUDA(p->scratchColor.ensure(N)); // allocated on the first host-output frame only
+        colorDev = p->scratchColor.p;
+    }
+    begin_frame(p, f);
+    rs_status st = enqueue_frame(p, s, colorDev, reinterpret_cast<const float2*>(f->mvec), false);
+    if (st != RS_OK) return st;
     if (f->colorHost)
     {
         RS_CUDA(cudaMemcpyAsync(f->colorHost, colorDev, N * 16ull, cudaMemcpyDeviceToHost, s));
         RS_CUDA(cudaStreamSynchronize(s));
     }
-    // endFrame
-    p->swapped = !p->frozen;
-    if (!p->frozen)
-    {
-        p->frameCount++;
-        std::swap(p->currIdx, p->prevIdx);
-    }
-    p->prevCamera = p->camera;
-    p->havePrevCamera = true;
+    end_frame(p);
     if (f->colorHost && *p->hostFault) return fail(RS_DEVICE_FAULT, "device status word set: BVH traversal stack overflow");
     return RS_OK;
 }
@@ -788,4 +872,133 @@ extern "C" RS_API rs_status rs_debug_keep_candidates(rs_pass* p, uint32_t keep)
     if (!p) return fail(RS_INVALID_ARG, "pass is NULL");
     p->keepCandidates = keep != 0;
     return RS_OK;
+}
+
+// ------------------------------------------------------------------ batched instances
+// A batch renders one frame of every member pass with a single CUDA graph launch.  The graph
+// forks one branch per instance from the caller's stream (the instances' stage chains run
+// concurrently and fill the GPU when single instances are small) and joins them at the end.
+// Kernels read each instance's context from device memory, copied from the pinned host context
+// by a node of the graph, so one graph is replayed every frame; a graph is captured per
+// buffer-parity pattern of the members (at most two when spatial reuse is off).
+struct rs_batch
+{
+    std::vector<rs_pass*> passes;
+    std::vector<cudaStream_t> branch;
+    std::vector<cudaEvent_t> joins;
+    cudaEvent_t fork = nullptr, done = nullptr;
+    cudaStream_t capture = nullptr;
+    bool inFlight = false;
+    struct Cached { std::vector<uint32_t> key; std::vector<void*> colors; cudaGraphExec_t exec; };
+    std::vector<Cached> graphs;
+    uint32_t lastLaunches = 0;
+    ~rs_batch()
+    {
+        if (done) cudaEventSynchronize(done);
+        for (auto& g : graphs) cudaGraphExecDestroy(g.exec);
+        for (auto e : joins) cudaEventDestroy(e);
+        for (auto s : branch) cudaStreamDestroy(s);
+        if (fork) cudaEventDestroy(fork);
+        if (done) cudaEventDestroy(done);
+        if (capture) cudaStreamDestroy(capture);
+    }
+};
+
+extern "C" RS_API rs_status rs_batch_create(rs_pass* const* passes, uint32_t count, rs_batch** out)
+{
+    if (!passes || !out || count == 0 || count > 64) return fail(RS_INVALID_ARG, "a batch holds 1 to 64 passes");
+    std::unique_ptr<rs_batch> b(new rs_batch());
+    for (uint32_t i = 0; i < count; i++)
+    {
+        if (!passes[i] || !passes[i]->hasScene) return fail(RS_INVALID_ARG, "every batch member needs a scene");
+        b->passes.push_back(passes[i]);
+        cudaStream_t s;
+        cudaEvent_t e;
+        RS_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        RS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        b->branch.push_back(s);
+        b->joins.push_back(e);
+    }
+    RS_CUDA(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+    RS_CUDA(cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming));
+    RS_CUDA(cudaStreamCreateWithFlags(&b->capture, cudaStreamNonBlocking));
+    *out = b.release();
+    return RS_OK;
+}
+
+extern "C" RS_API rs_status rs_batch_destroy(rs_batch* b)
+{
+    if (!b) return fail(RS_INVALID_ARG, "batch is NULL");
+    delete b;
+    return RS_OK;
+}
+
+// frames[i] is the frame of passes[i]; each frames[i].color must be a device buffer (graphs keep
+// the pointers; a new set of pointers captures a new graph).
+extern "C" RS_API rs_status rs_batch_execute(rs_batch* b, const rs_frame_desc* frames, void* streamPtr)
+{
+    if (!b || !frames) return fail(RS_INVALID_ARG, "batch or frames is NULL");
+    cudaStream_t s = (cudaStream_t)streamPtr;
+    const size_t n = b->passes.size();
+    for (size_t i = 0; i < n; i++)
+        if (!frames[i].color) return fail(RS_INVALID_ARG, "batched frames need device colour buffers");
+    // the previous replay reads the pinned host contexts; wait for it before rewriting them
+    if (b->inFlight) RS_CUDA(cudaEventSynchronize(b->done));
+    std::vector<uint32_t> key(n);
+    std::vector<void*> colors(n);
+    for (size_t i = 0; i < n; i++)
+    {
+        rs_pass* p = b->passes[i];
+        begin_frame(p, &frames[i]);
+        *p->graphCtx = *p->hostCtx;
+        p->lastStream = s;
+        p->stageNames.clear();
+        colors[i] = frames[i].color;
+        // the graph depends on the ping-pong buffers in use and on whether temporal stages run
+        key[i] = (uint32_t)p->currIdx * 3u + (uint32_t)p->prevIdx + 9u * (p->frameCount == 0 || frames[i].sceneShouldReset ? 1u : 0u);
+    }
+    cudaGraphExec_t exec = nullptr;
+    for (auto& g : b->graphs)
+        if (g.key == key && g.colors == colors) { exec = g.exec; break; }
+    if (!exec)
+    {
+        cudaStream_t cs = b->capture; // capture never executes; the caller's stream may be the legacy default
+        RS_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+        cudaEventRecord(b->fork, cs);
+        uint32_t launches = 0;
+        rs_status st = RS_OK;
+        for (size_t i = 0; i < n && st == RS_OK; i++)
+        {
+            rs_pass* p = b->passes[i];
+            cudaStreamWaitEvent(b->branch[i], b->fork, 0);
+            bool timing = p->timing;
+            p->timing = false;
+            p->launches = 0;
+            st = enqueue_frame(p, b->branch[i], reinterpret_cast<float4*>(frames[i].color), nullptr, true);
+            p->timing = timing;
+            launches += p->launches;
+            cudaEventRecord(b->joins[i], b->branch[i]);
+            cudaStreamWaitEvent(cs, b->joins[i], 0);
+        }
+        cudaGraph_t graph = nullptr;
+        cudaError_t e = cudaStreamEndCapture(cs, &graph);
+        if (st != RS_OK) { if (graph) cudaGraphDestroy(graph); return st; }
+        if (e != cudaSuccess) return fail(RS_CUDA_ERROR, std::string("graph capture: ") + cudaGetErrorString(e));
+        e = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) return fail(RS_CUDA_ERROR, std::string("graph instantiate: ") + cudaGetErrorString(e));
+        b->graphs.push_back({key, colors, exec});
+        b->lastLaunches = launches;
+    }
+    RS_CUDA(cudaGraphLaunch(exec, s));
+    RS_CUDA(cudaEventRecord(b->done, s));
+    b->inFlight = true;
+    for (size_t i = 0; i < n; i++) end_frame(b->passes[i]);
+    return RS_OK;
+}
+
+extern "C" RS_API uint32_t rs_batch_launch_count(rs_batch* b)
+{
+    if (!b) return 0u;
+    return b->lastLaunches;
 }

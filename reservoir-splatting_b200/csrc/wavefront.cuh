@@ -11,6 +11,7 @@
 // kernel that replays the reference's resampling order (and its generator draws)
 // on the stored results with no ray queries.  Results are identical to the
 // single-kernel form; only the schedule changes.
+#pragma once
 #include "kernels.h"
 
 namespace rs {
@@ -59,9 +60,8 @@ __device__ __forceinline__ uint32_t clamped_backup(const DevCtx& C, const float2
     return (uint32_t)ry * C.W + (uint32_t)rx;
 }
 
-__device__ __forceinline__ void backup_of(const WaveCtx& K, uint32_t ri, uint32_t x, uint32_t y, Res& br, uint32_t& bi, f2& fc)
+__device__ __forceinline__ void backup_of(const DevCtx& C, const WaveCtx& K, uint32_t ri, uint32_t x, uint32_t y, Res& br, uint32_t& bi, f2& fc)
 {
-    const DevCtx& C = K.C;
     if (K.fused)
     {
         bi = clamped_backup(C, K.mvec, x, y, fc);
@@ -91,9 +91,9 @@ __device__ __forceinline__ Recon backup_rec(const WaveCtx& K, uint32_t bi)
 }
 
 // ---- stage 1: current sample -> previous domain by reprojection (ScatterBackup...:96-114)
-__global__ void __launch_bounds__(128) k_sb_curr_scatter(WaveCtx K)
+__global__ void __launch_bounds__(128) k_sb_curr_scatter(uint32_t slot, WaveCtx K)
 {
-    const DevCtx& C = K.C;
+    const DevCtx& C = c_ctx[slot];
     uint32_t ri = blockIdx.x * blockDim.x + threadIdx.x;
     if (ri >= C.W * C.H) return;
     f3 integrand = load_integrand(K.curr, ri);
@@ -111,16 +111,16 @@ __global__ void __launch_bounds__(128) k_sb_curr_scatter(WaveCtx K)
 }
 
 // ---- stage 1: current sample -> previous domain by the gather shift (:116-129)
-__global__ void __launch_bounds__(128) k_sb_curr_gather(WaveCtx K)
+__global__ void __launch_bounds__(128) k_sb_curr_gather(uint32_t slot, WaveCtx K)
 {
-    const DevCtx& C = K.C;
+    const DevCtx& C = c_ctx[slot];
     uint32_t ri = blockIdx.x * blockDim.x + threadIdx.x;
     if (ri >= C.W * C.H) return;
     Res cr = load_res_rw(K.curr, ri);
     if (!any_gt0(cr.integrand)) return;
     uint32_t x = ri % C.W, y = ri / C.W;
     Res br; uint32_t bi; f2 fc;
-    backup_of(K, ri, x, y, br, bi, fc);
+    backup_of(C, K, ri, x, y, br, bi, fc);
     float m3 = 0.f;
     if (valid_float(C, fc))
     {
@@ -135,14 +135,14 @@ __global__ void __launch_bounds__(128) k_sb_curr_gather(WaveCtx K)
 }
 
 // ---- stage 1: backup sample -> current domain (:156-166)
-__global__ void __launch_bounds__(128) k_sb_backup_gather(WaveCtx K)
+__global__ void __launch_bounds__(128) k_sb_backup_gather(uint32_t slot, WaveCtx K)
 {
-    const DevCtx& C = K.C;
+    const DevCtx& C = c_ctx[slot];
     uint32_t ri = blockIdx.x * blockDim.x + threadIdx.x;
     if (ri >= C.W * C.H) return;
     uint32_t x = ri % C.W, y = ri / C.W;
     Res br; uint32_t bi; f2 fc;
-    backup_of(K, ri, x, y, br, bi, fc);
+    backup_of(C, K, ri, x, y, br, bi, fc);
     if (!any_gt0(br.integrand)) return;
     Recon brd = backup_rec(K, bi);
     SampleGen dummy = {0, C.sgKind};
@@ -159,14 +159,14 @@ __global__ void __launch_bounds__(128) k_sb_backup_gather(WaveCtx K)
 }
 
 // ---- stage 2 (Balance): updated backup -> previous domain by reprojection (:171-189)
-__global__ void __launch_bounds__(128) k_sb_backup_scatter(WaveCtx K)
+__global__ void __launch_bounds__(128) k_sb_backup_scatter(uint32_t slot, WaveCtx K)
 {
-    const DevCtx& C = K.C;
+    const DevCtx& C = c_ctx[slot];
     uint32_t ri = blockIdx.x * blockDim.x + threadIdx.x;
     if (ri >= C.W * C.H) return;
     uint32_t x = ri % C.W, y = ri / C.W;
     Res br; uint32_t bi; f2 fc;
-    backup_of(K, ri, x, y, br, bi, fc);
+    backup_of(C, K, ri, x, y, br, bi, fc);
     if (!any_gt0(br.integrand)) return;
     Recon brd = backup_rec(K, bi);
     Shifted sb = load_shift(K.backupShift, ri);
@@ -184,9 +184,9 @@ __global__ void __launch_bounds__(128) k_sb_backup_scatter(WaveCtx K)
 }
 
 // ---- stage 1: splatted previous sample -> current domain (:218-235), one thread per splat
-__global__ void __launch_bounds__(128) k_sb_splat_scatter(WaveCtx K)
+__global__ void __launch_bounds__(128) k_sb_splat_scatter(uint32_t slot, WaveCtx K)
 {
-    const DevCtx& C = K.C;
+    const DevCtx& C = c_ctx[slot];
     uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= *K.totalSplats) return;
     uint32_t si = __ldg(&K.sorted[j]);
@@ -207,9 +207,9 @@ __global__ void __launch_bounds__(128) k_sb_splat_scatter(WaveCtx K)
 }
 
 // ---- stage 2 (Balance): updated splat -> previous domain by the gather shift (:237-253)
-__global__ void __launch_bounds__(128) k_sb_splat_gather(WaveCtx K)
+__global__ void __launch_bounds__(128) k_sb_splat_gather(uint32_t slot, WaveCtx K)
 {
-    const DevCtx& C = K.C;
+    const DevCtx& C = c_ctx[slot];
     uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= *K.totalSplats) return;
     uint32_t si = __ldg(&K.sorted[j]);
@@ -218,7 +218,7 @@ __global__ void __launch_bounds__(128) k_sb_splat_gather(WaveCtx K)
     uint32_t cell = __ldg(&K.sortedCell[j]);
     uint32_t x = cell % C.W, y = cell / C.W;
     Res br; uint32_t bi; f2 fc;
-    backup_of(K, cell, x, y, br, bi, fc);
+    backup_of(C, K, cell, x, y, br, bi, fc);
     float4 sm = __ldg(&K.splatM[j]);
     f2 fp = fc + mk2(sm.z, sm.w);
     float m3 = 0.f;
@@ -238,9 +238,9 @@ __global__ void __launch_bounds__(128) k_sb_splat_gather(WaveCtx K)
 }
 
 // ---- combine: the GRIS order of ScatterBackupTemporalResampling.rt.slang:91-283 on stored shifts
-__global__ void __launch_bounds__(128) k_sb_combine(WaveCtx K, float4* __restrict__ color)
+__global__ void __launch_bounds__(128) k_sb_combine(uint32_t slot, WaveCtx K, float4* __restrict__ color)
 {
-    const DevCtx& C = K.C;
+    const DevCtx& C = c_ctx[slot];
     uint32_t ri = blockIdx.x * blockDim.x + threadIdx.x;
     if (ri >= C.W * C.H) return;
     uint32_t x = ri % C.W, y = ri / C.W;
@@ -251,7 +251,7 @@ __global__ void __launch_bounds__(128) k_sb_combine(WaveCtx K, float4* __restric
     Res dst = res_default();
     Res cr = load_res_rw(K.curr, ri);
     Res br; uint32_t bi; f2 fc;
-    backup_of(K, ri, x, y, br, bi, fc);
+    backup_of(C, K, ri, x, y, br, bi, fc);
     enum { kSelNone = 0, kSelCurr = 1, kSelBackup = 2, kSelSplat = 3 };
     uint32_t sel = kSelNone, selIndex = 0;
     {
@@ -366,9 +366,9 @@ __device__ __forceinline__ bool spatial_neighbor(const DevCtx& C, uint32_t itera
     return valid_int(C, nx, ny);
 }
 
-__global__ void __launch_bounds__(128) k_sp_central(SpatialCtx S)
+__global__ void __launch_bounds__(128) k_sp_central(uint32_t slot, SpatialCtx S)
 {
-    const DevCtx& C = S.C;
+    const DevCtx& C = c_ctx[slot];
     uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t N = C.W * C.H;
     if (t >= N * C.neighborCount) return;
@@ -395,9 +395,9 @@ __global__ void __launch_bounds__(128) k_sp_central(SpatialCtx S)
     S.m1[t] = m1;
 }
 
-__global__ void __launch_bounds__(128) k_sp_neighbor(SpatialCtx S)
+__global__ void __launch_bounds__(128) k_sp_neighbor(uint32_t slot, SpatialCtx S)
 {
-    const DevCtx& C = S.C;
+    const DevCtx& C = c_ctx[slot];
     uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t N = C.W * C.H;
     if (t >= N * C.neighborCount) return;
@@ -425,9 +425,9 @@ __global__ void __launch_bounds__(128) k_sp_neighbor(SpatialCtx S)
     S.nw[t] = nw;
 }
 
-__global__ void __launch_bounds__(128) k_sp_combine(SpatialCtx S, float4* __restrict__ color)
+__global__ void __launch_bounds__(128) k_sp_combine(uint32_t slot, SpatialCtx S, float4* __restrict__ color)
 {
-    const DevCtx& C = S.C;
+    const DevCtx& C = c_ctx[slot];
     uint32_t ri = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t N = C.W * C.H;
     if (ri >= N) return;
