@@ -231,6 +231,7 @@ def run_ours(args):
     roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 5), "traffic": None, "peak_source": peak_kind,
                 "stage_ms": {k: round(v, 4) for k, v in stage_ms.items()}}
+    p.close()
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "frames/s", "n_gpus": world, "steps": args.steps,
@@ -246,12 +247,82 @@ def run_ours(args):
             "roofline": roofline,
             "clocks": clocks,
         }
+        if world == 1 and not args.no_batched:
+            line["batched"] = run_batched(args, torch, rs, stream, dev)
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(args, quiet=True)
         print(json.dumps(line), flush=True)
-    p.close()
     if dist:
         dist.destroy_process_group()
+
+
+BATCH_RESOLUTIONS = [(320, 240), (640, 480), (1280, 720), (1920, 1080)]
+
+
+def batch_instances(count: int, seed: int = 11):
+    """Seeded batched workload: resolutions uniform over BATCH_RESOLUTIONS, 10k-500k triangles each
+    from the same generator (terrain grid and sphere count scaled to the triangle target)."""
+    _package()
+    import reservoir_splatting_b200.scenes as S
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        w, h = BATCH_RESOLUTIONS[int(rng.integers(0, len(BATCH_RESOLUTIONS)))]
+        target = int(rng.uniform(10_000, 500_000))
+        grid = max(8, int((0.6 * target / 2) ** 0.5))
+        spheres = max(1, int(0.4 * target / 1280))
+        sc = S.terrain_spheres(seed=1000 + i, grid=grid, spheres=spheres, subdiv=3, lights=16)
+        out.append((sc, w, h, i))
+    return out
+
+
+def run_batched(args, torch, rs, stream, dev):
+    """Plain (each instance's frame launched on its own, back to back) vs batched (one CUDA-graph
+    launch per frame for all instances); device time over the same frames."""
+    insts = batch_instances(args.batch_instances)
+    plain = [rs.ReservoirSplatting(PROPS, w, h) for _, w, h, _ in insts]
+    for (sc, _, _, _), a in zip(insts, plain):
+        a.set_scene(sc)
+    batched = plain  # the same passes render both ways (halves the memory of the 64 instances)
+    outs = [torch.empty((h, w, 4), dtype=torch.float32, device=dev) for _, w, h, _ in insts]
+    batch = rs.Batch(batched)
+    cams = lambda f: [camera(f + 13 * i, w, h) for _, w, h, i in insts]
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+
+    def time_frames(fn, first, frames):
+        a, b = ev(), ev()
+        a.record(stream)
+        for f in range(first, first + frames):
+            fn(f)
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b)
+
+    def plain_frame(f):
+        for p, c, o in zip(plain, cams(f), outs):
+            p.execute(c, color_ptr=o.data_ptr(), stream=stream.cuda_stream)
+
+    def batch_frame(f):
+        batch.execute(cams(f), [o.data_ptr() for o in outs], stream=stream.cuda_stream)
+
+    with torch.cuda.stream(stream):
+        time_frames(plain_frame, 0, args.batch_warmup)
+        time_frames(batch_frame, 0, args.batch_warmup)
+        ms_plain = time_frames(plain_frame, args.batch_warmup, args.batch_frames)
+        ms_batch = time_frames(batch_frame, args.batch_warmup, args.batch_frames)
+    n = len(insts)
+    pixels = sum(w * h for _, w, h, _ in insts)
+    tris = [sc.num_triangles for sc, _, _, _ in insts]
+    res = {"instances": n, "frames": args.batch_frames, "pixels_per_batch_frame": pixels,
+           "triangles_min": min(tris), "triangles_max": max(tris),
+           "plain_instance_frames_per_s": round(n * args.batch_frames / (ms_plain / 1e3), 3),
+           "batched_instance_frames_per_s": round(n * args.batch_frames / (ms_batch / 1e3), 3),
+           "speedup": round(ms_plain / ms_batch, 4), "graph_launch_kernels": batch.launch_count(),
+           "how": "plain: rs_execute per instance back to back on one stream; batched: rs_batch_execute (one CUDA graph, per-instance branches)"}
+    batch.close()
+    for p in plain:
+        p.close()
+    return res
 
 
 def C_frame_bytes():
@@ -306,6 +377,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-frames", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--batch-instances", type=int, default=64)
+    ap.add_argument("--batch-frames", type=int, default=4)
+    ap.add_argument("--batch-warmup", type=int, default=2)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
