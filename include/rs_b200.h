@@ -198,6 +198,33 @@ RS_API rs_status rs_batch_execute(rs_batch* batch, const rs_frame_desc* frames, 
 RS_API rs_status rs_batch_destroy(rs_batch* batch);
 RS_API uint32_t rs_batch_launch_count(rs_batch* batch);
 
+/* Allocation-free cell-list build.  This call has no counterpart in the reference.
+ *
+ * It exists for callers that cannot allocate device memory when they run: a host that hands
+ * out all device memory from its own fixed pool, an allocator-free real-time loop, or a plug-in
+ * invoked while its host captures a CUDA graph.  The rs_pass calls allocate their buffers on the
+ * first frame at a given size; this call never calls cudaMalloc, cudaFree or any other
+ * allocating routine.  Its temporaries live in a 16 MiB array compiled into the library, which
+ * every GPU that loads the library holds until the process exits.
+ *
+ * Input:  targets[numSplats], device memory: the cell of each splat, or any value >= numCells
+ *         (0xFFFFFFFF, say) for a splat that lands in no cell.
+ * Output: counts[numCells] (splats per cell), offsets[numCells] (exclusive prefix sum of the
+ *         counts) and sorted[numSplats] (splat indices grouped by cell, ascending within a cell;
+ *         the first sum(counts) entries are written), all device memory on the current device.
+ * These are the lists rs_execute builds for the temporal scatter, in the same order.
+ *
+ * Limits: 1 <= numCells <= RS_CELL_LISTS_STATIC_MAX and numSplats <= RS_CELL_LISTS_STATIC_MAX
+ * (2^21, enough for a 1920x1080 frame); larger sizes return RS_INVALID_ARG before any device work.
+ * The first call on a device looks up the array's device address (cudaGetSymbolAddress with that
+ * device current); make that first call before any stream capture begins.  Work is enqueued on
+ * `cudaStream` and the call returns without waiting.  All calls on a device share the one array:
+ * calls whose work overlaps on the GPU (other streams, other host threads) race and corrupt each
+ * other's lists, so order them on one stream or with events. */
+#define RS_CELL_LISTS_STATIC_MAX (1u << 21)
+RS_API rs_status rs_build_cell_lists_static(const uint32_t* targets, uint32_t numSplats, uint32_t numCells,
+                                            uint32_t* counts, uint32_t* offsets, uint32_t* sorted, void* cudaStream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -61,9 +61,11 @@ def load_library():
     lib.rs_batch_destroy.argtypes = [C.c_void_p]
     lib.rs_batch_launch_count.argtypes = [C.c_void_p]
     lib.rs_batch_launch_count.restype = C.c_uint32
+    lib.rs_build_cell_lists_static.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     for name in ("rs_create", "rs_destroy", "rs_set_options", "rs_set_scene", "rs_execute", "rs_reset", "rs_set_seed",
                  "rs_freeze", "rs_get_buffer", "rs_set_buffer", "rs_enable_stage_timing", "rs_get_stage_times",
-                 "rs_debug_keep_candidates", "rs_batch_create", "rs_batch_execute", "rs_batch_destroy"):
+                 "rs_debug_keep_candidates", "rs_batch_create", "rs_batch_execute", "rs_batch_destroy",
+                 "rs_build_cell_lists_static"):
         getattr(lib, name).restype = C.c_int
     _lib = lib
     return lib

@@ -27,6 +27,9 @@ static rs_status fail(rs_status s, const std::string& msg)
     return s;
 }
 
+// Lets entry points defined in other files report through rs_last_error_string().
+namespace rs { void set_last_error(const std::string& msg) { g_lastError = msg; } }
+
 #define RS_CUDA(call)                                                                               \
     do {                                                                                            \
         cudaError_t e_ = (call);                                                                    \
