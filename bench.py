@@ -275,6 +275,8 @@ def run_ours(args):
         }
         if world == 1 and not args.no_batched:
             line["batched"] = run_batched(args, torch, rs, stream, dev)
+        if world == 1 and not args.no_adjoint:
+            line["adjoint"] = run_adjoint(args, torch, rs, stream)
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(args, quiet=True)
         print(json.dumps(line), flush=True)
@@ -351,6 +353,70 @@ def run_batched(args, torch, rs, stream, dev):
     return res
 
 
+ADJ_RES = 512
+ADJ_FRAMES = 8
+ADJ_PROPS = {"temporalReuse": "ScatterBackup", "gatherOption": "Clamped", "scatterBackupMISOption": "Balance",
+             "maxSurfaceBounces": 1, "enableSpatialResampling": True}
+
+
+def run_adjoint(args, torch, rs, stream):
+    """Differentiation workload: 512 x 512, the seeded 199k-triangle scene with 32 metal-rough
+    materials and 8 emitters, ScatterBackup over 8 frames of a translating camera, L2 loss against a
+    target rendered with parameters perturbed by N(0, 0.05).  Forward = the 8 frames plus one
+    reservoir checkpoint per frame; backward = rs_backward for each frame (path replay).  Device
+    time of each, CUDA events on the launching stream, after one untimed sequence."""
+    import reservoir_splatting_b200.scenes as S
+    import reservoir_splatting_b200.adjoint as adj
+    sc = S.inverse_scene()
+    renderer = adj.Renderer(sc, ADJ_PROPS, ADJ_RES, ADJ_RES)
+    cams = [S.translate_camera(f, ADJ_RES, ADJ_RES) for f in range(ADJ_FRAMES)]
+    theta = renderer.params()
+    rng = np.random.default_rng(7)
+    pert = theta.clone()
+    pert[:, :7] += torch.from_numpy(rng.normal(0.0, 0.05, (len(pert), 7)).astype(np.float32))
+    emissive = theta[:, 4:7].amax(1) > 0
+    pert[~emissive, 4:7] = 0.0
+    pert[emissive, :4] = theta[emissive, :4]
+    pert[:, :3] = pert[:, :3].clamp(0.0, 1.0)
+    pert[:, 3] = pert[:, 3].clamp(0.1, 1.0)
+    pert[:, 7] = theta[:, 7]
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        renderer.apply(pert)
+        target, _ = renderer.render(cams, keep_checkpoints=False)
+        renderer.apply(theta)
+        fwd_ms = bwd_ms = 0.0
+        reps = max(1, args.adjoint_reps)
+        for rep in range(reps + 1):
+            a, b, c = ev(), ev(), ev()
+            a.record(stream)
+            images, ckpts = renderer.render(cams)
+            b.record(stream)
+            gimg = 2.0 * (images - target)
+            gimg[..., 3] = 0.0
+            b2 = ev()
+            b2.record(stream)
+            grad = renderer.backward(gimg, ckpts)
+            c.record(stream)
+            torch.cuda.synchronize()
+            if rep > 0:  # the first sequence is the warm-up
+                fwd_ms += a.elapsed_time(b)
+                bwd_ms += b2.elapsed_time(c)
+        stats = renderer.pass_.backward_stats()
+        loss = float(((images - target)[..., :3] ** 2).sum().item())
+    fwd = fwd_ms / reps / ADJ_FRAMES
+    bwd = bwd_ms / reps / ADJ_FRAMES
+    renderer.pass_.close()
+    return {"resolution": [ADJ_RES, ADJ_RES], "frames": ADJ_FRAMES, "triangles": sc.num_triangles,
+            "materials": int(sc.info["materials"]), "emitters": int(sc.info["emitters"]),
+            "params": int(sc.info["materials"]) * 4 + int(sc.info["emitters"]) * 3,
+            "fwd_ms_per_frame": round(fwd, 4), "bwd_ms_per_frame": round(bwd, 4), "bwd_over_fwd": round(bwd / fwd, 4),
+            "loss": loss, "grad_norm": float(grad.norm().item()),
+            "replayed_paths": int(stats[0]), "paths_too_long": int(stats[1]), "emitter_not_found": int(stats[2]),
+            "how": "fwd: rs_execute x 8 frames + rs_checkpoint (144 B/pixel) per frame; bwd: rs_backward per frame "
+                   "from its checkpoint; the gradient check against FP64 central differences is in the tests"}
+
+
 def C_frame_bytes():
     import ctypes
     rs = _package()
@@ -407,6 +473,8 @@ def main():
     ap.add_argument("--batch-instances", type=int, default=64)
     ap.add_argument("--batch-frames", type=int, default=4)
     ap.add_argument("--batch-warmup", type=int, default=2)
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--adjoint-reps", type=int, default=3)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

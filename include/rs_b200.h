@@ -136,7 +136,7 @@ typedef struct rs_frame_desc {
     uint32_t sceneShouldReset;           /* Scene::shouldReset(): restart the temporal history */
 } rs_frame_desc;
 
-/* Buffers readable with rs_get_buffer (canonical host layouts, see DESIGN.md):
+/* Buffers readable with rs_get_buffer (canonical host layouts):
  *   reservoirs      8 floats / pixel: integrand.xyz, totalWeight, subPixel.xy, confidence, 0
  *   reconnection    28 words / pixel (layout in rs_get_buffer's documentation)
  *   cellCounters    uint32 / pixel        cellOffsets  uint32 / pixel
@@ -197,6 +197,29 @@ RS_API rs_status rs_batch_create(rs_pass* const* passes, uint32_t count, rs_batc
 RS_API rs_status rs_batch_execute(rs_batch* batch, const rs_frame_desc* frames, void* cudaStream);
 RS_API rs_status rs_batch_destroy(rs_batch* batch);
 RS_API uint32_t rs_batch_launch_count(rs_batch* batch);
+
+/* Path-replay adjoint (no reference counterpart: the reference pass renders forward only).
+ *
+ * A pixel's colour is f(y) * W, y being the path its final reservoir selected.  rs_backward holds
+ * each pixel's y, W, sampling densities and MIS weights at their rendered values and
+ * differentiates f(y) with respect to every material's baseColor (per channel), roughness and
+ * emissive radiance (per channel).  E[df(y)/dtheta * W] is the derivative of the pixel integral, so
+ * the gradient is unbiased.  Only the final reservoirs of a frame are needed: rs_checkpoint copies
+ * them (rs_checkpoint_bytes = 144 bytes per pixel) and rs_backward recomputes the rest.  Paths must
+ * have at most three vertices (maxSurfaceBounces <= 1); metallic and ior are not differentiated.
+ *
+ *   rs_set_materials   replace material parameters in place (same count; geometry and BVH stay)
+ *   rs_checkpoint      copy the last frame's final reservoirs to caller device memory
+ *   rs_backward        gradMaterials[m * 8 + k] += d loss / d (baseColor.xyz, roughness, emissive.xyz, -)
+ *                      for d loss / d colour `gradColor` (device float4 per pixel); checkpoint NULL
+ *                      means the last frame; the materials must be those the frame used
+ *   rs_backward_stats  read and clear {paths replayed, paths too long, emitter not found, value mismatch} */
+RS_API rs_status rs_set_materials(rs_pass* pass, const rs_material* materials, uint32_t count);
+RS_API rs_status rs_checkpoint_bytes(rs_pass* pass, size_t* bytes);
+RS_API rs_status rs_checkpoint(rs_pass* pass, void* dstDevice, void* cudaStream);
+RS_API rs_status rs_backward(rs_pass* pass, const void* checkpointDevice, const float* gradColor, float* gradMaterials,
+                             void* cudaStream);
+RS_API rs_status rs_backward_stats(rs_pass* pass, uint64_t* stats4);
 
 /* Allocation-free cell-list build.  This call has no counterpart in the reference.
  *

@@ -70,6 +70,11 @@ def load():
     lib.ro_set_buffer.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]
     lib.ro_frame_count.argtypes = [C.c_void_p]
     lib.ro_frame_count.restype = C.c_uint32
+    lib.ro_set_materials.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32]
+    lib.ro_backward.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.ro_replay_loss.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32]
+    lib.ro_replay_loss.restype = C.c_double
+    lib.ro_test_bsdf_grad.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]
     _lib = lib
     return lib
 
@@ -139,3 +144,38 @@ class OraclePass:
         st = self._lib.ro_set_buffer(self._h, self._abi.BUF[name], data.ctypes.data, data.nbytes)
         if st != 0:
             raise RuntimeError(f"oracle set_buffer failed: {st}")
+
+    # ---- path-replay adjoint (checker of rs_backward)
+    def set_materials(self, materials: np.ndarray):
+        m = np.ascontiguousarray(materials, np.float32)
+        st = self._lib.ro_set_materials(self._h, m.ctypes.data, len(m))
+        if st != 0:
+            raise RuntimeError(f"oracle set_materials failed: {st}")
+
+    def backward(self, grad_color: np.ndarray, num_materials: int):
+        """Analytic replay gradient of the last frame: (num_materials x 8 float64, stats[4])."""
+        g = np.ascontiguousarray(grad_color, np.float32).reshape(-1, 4)
+        out = np.zeros((num_materials, 8), np.float64)
+        stats = np.zeros(4, np.uint64)
+        st = self._lib.ro_backward(self._h, g.ctypes.data, out.ctypes.data, stats.ctypes.data)
+        if st != 0:
+            raise RuntimeError(f"oracle backward failed: {st}")
+        return out, stats
+
+    def replay_loss(self, target: np.ndarray, params: np.ndarray) -> float:
+        """FP64 replay loss of the last frame at `params` (materials x 8 float64: baseColor.xyz,
+        roughness, emissive.xyz, metallic); the detached terms stay at the pass's materials."""
+        t = np.ascontiguousarray(target, np.float32).reshape(-1, 4)
+        q = np.ascontiguousarray(params, np.float64)
+        return float(self._lib.ro_replay_loss(self._h, t.ctypes.data, q.ctypes.data, len(q)))
+
+
+def bsdf_grad(material, wi, wo, lobe_mask: int = 0):
+    """(value, dBase, dRough) in FP32 and the FP64 value, for the BSDF derivative check."""
+    lib = load()
+    m = np.asarray(material, np.float32)
+    a, b = np.asarray(wi, np.float32), np.asarray(wo, np.float32)
+    out = np.zeros(9, np.float32)
+    vd = np.zeros(3, np.float64)
+    lib.ro_test_bsdf_grad(m.ctypes.data, a.ctypes.data, b.ctypes.data, lobe_mask, out.ctypes.data, vd.ctypes.data)
+    return out[0:3], out[3:6], out[6:9], vd

@@ -28,11 +28,14 @@
 #include <algorithm>
 #include <vector>
 #include <memory>
+#include <array>
 #include <omp.h>
 
 #include "../include/rs_b200.h"
 #include "../reservoir-splatting_b200/csrc/core/camera.h"
 #include "../reservoir-splatting_b200/csrc/core/scene_prep.h"
+#include "../reservoir-splatting_b200/csrc/core/material_grad.h"
+#include <cmath>
 
 using namespace rs;
 
@@ -1936,12 +1939,280 @@ static void import_recon(ReconnectionData& r, const uint32_t* o)
     r.irradiance = mk3(u2f(o[24]), u2f(o[25]), u2f(o[26]));
 }
 
+// ================================================= path-replay adjoint (no reference counterpart)
+// The resolved colour of a pixel is f(y) * W (ResolveReSTIR.cs.slang:45-63).  The adjoint holds the
+// frame's selected path y, its contribution weight W, the sampling densities and the MIS weights at
+// their values for the pass's materials, and differentiates f(y) with respect to each material's
+// baseColor and roughness (BSDF factors at x1 and x2) and emitted radiance (the Le the path carries).
+// f(y) is the reconnection-shift evaluation of the record at its own primary hit
+// (handleReconnectionHit / pathReconnectionShift above) without the visibility ray, which does not
+// depend on materials.  Paths longer than three vertices carry suffix radiance from materials that
+// the record does not name; they are counted and skipped.
+struct ReplayVertex
+{
+    uint32_t material = kInvalidIndex;
+    f3 wi = mk3(0.f), wo = mk3(0.f); // local frame
+    bool valid = false;               // hemisphere test and minimum cosine
+    bool diffuseOn = false, specularOn = false;
+    BsdfGrad g;                       // value and derivatives at the pass's materials
+};
+struct Replay
+{
+    uint32_t L = 0;
+    float W = 0.f;                    // contribution weight of the pixel's reservoir
+    float s = 0.f;                    // detached factor: MIS weight over the sampling densities
+    f3 Le = mk3(0.f);                 // emitted radiance the path carries
+    uint32_t emitter = kInvalidIndex; // material that emits Le, when the replay finds it
+    uint32_t nv = 0;                  // BSDF vertices on the path (0, 1 or 2)
+    ReplayVertex v[2];
+    f3 value = mk3(0.f);              // replayed f(y)
+    f3 k = mk3(1.f);                  // integrand / value per channel (detached; 1 where value is 0)
+};
+enum { kStatReplayed = 0, kStatTooLong = 1, kStatNoEmitter = 2, kStatValueMismatch = 3 };
+
+static ReplayVertex replay_vertex(const Pass& p, const ShadingData& sd, uint32_t lobeMask, f3 wo)
+{
+    ReplayVertex v;
+    BsdfData d = p.instance(sd);
+    v.material = sd.materialID;
+    v.wi = sd_to_local(sd, sd.V);
+    v.wo = sd_to_local(sd, wo);
+    v.valid = valid_hemisphere(sd, v.wi, v.wo, wo) && f_min(v.wi.z, v.wo.z) >= kMinCosTheta;
+    StandardBSDF b = make_bsdf(v.wi, d, lobeMask);
+    uint32_t mask = lobeMask == 0 ? 0xfu : lobeMask;
+    v.diffuseOn = b.pDiffuseReflection > 0.f && (mask & 0x1u);
+    v.specularOn = b.pSpecularReflection > 0.f && (mask & 0x4u) && b.alpha != 0.f;
+    v.g = mi_eval_grad(sd, d, lobeMask, wo);
+    return v;
+}
+
+// The material whose front-face emission is the radiance the path carries.
+static uint32_t emitter_of(const Pass& p, const ShadingData& sd, f3 Le)
+{
+    f3 e = p.instance(sd).emission;
+    if (!any_gt0(e)) return kInvalidIndex;
+    const float a[3] = {e.x, e.y, e.z}, b[3] = {Le.x, Le.y, Le.z};
+    for (int c = 0; c < 3; c++)
+        if (f_abs(a[c] - b[c]) > 1e-5f * f_max(f_abs(a[c]), 1e-30f)) return kInvalidIndex;
+    return sd.materialID;
+}
+
+static bool replay_pixel(const Pass& p, const PathReservoir& r, const ReconnectionData& rd, Replay& out, uint64_t* stats)
+{
+    out = Replay();
+    out.W = r.computeUCW();
+    if (!(out.W > 0.f) || rd.pathLength == 0) return false;
+    if (rd.pathLength > 3) { stats[kStatTooLong]++; return false; }
+    out.L = rd.pathLength;
+    out.Le = rd.irradiance;
+    ShadingData sd1 = p.loadSD(rd.firstHit, -rd.firstWi);
+    if (rd.pathLength == 1)
+    {
+        out.s = 1.f;
+        out.emitter = emitter_of(p, sd1, rd.irradiance);
+    }
+    else
+    {
+        BsdfData d1 = p.instance(sd1);
+        f3 origin = sd_ray_origin(sd1, !rd.transmissionEvent);
+        ShadingData sec = p.loadSD(rd.secondHit, mk3(0.f));
+        f3 off = sec.posW - sd1.posW;
+        float jac = f_abs(dot(sec.faceN, -normalize(off))) / dot(off, off);
+        f3 dir = normalize(sec.posW - origin);
+        uint32_t mask1 = 1u << rd.firstBSDFComponentType;
+        float lobePdf = mi_pdf(sd1, d1, mask1, dir), totalPdf = mi_pdf(sd1, d1, 0u, dir);
+        if (rd.pathLength == 2)
+        {
+            float lightPdf = rd.lightPdf / jac;
+            if (rd.lightIsNEE)
+            {
+                out.v[0] = replay_vertex(p, sd1, 0u, dir);
+                if (!any_gt0(out.v[0].g.value) || totalPdf == 0.f) return false;
+                out.s = p.mis(lightPdf, totalPdf) / lightPdf;
+            }
+            else
+            {
+                out.v[0] = replay_vertex(p, sd1, mask1, dir);
+                if (!any_gt0(out.v[0].g.value) || lobePdf == 0.f) return false;
+                out.s = p.mis(totalPdf, lightPdf) / lobePdf;
+            }
+            out.nv = 1;
+            out.emitter = emitter_of(p, p.loadSD(rd.secondHit, dir), rd.irradiance);
+        }
+        else
+        {
+            out.v[0] = replay_vertex(p, sd1, mask1, dir);
+            if (!any_gt0(out.v[0].g.value) || lobePdf == 0.f) return false;
+            ShadingData sd2 = p.loadSD(rd.secondHit, dir);
+            BsdfData d2 = p.instance(sd2);
+            uint32_t mask2 = 1u << rd.secondBSDFComponentType;
+            float lsp = mi_pdf(sd2, d2, mask2, rd.secondWo), tp = mi_pdf(sd2, d2, 0xFu, rd.secondWo);
+            if (!any_gt0(mi_eval(sd2, d2, 0xFu, rd.secondWo))) return false;
+            if (rd.lightIsNEE)
+            {
+                out.v[1] = replay_vertex(p, sd2, 0xFu, rd.secondWo);
+                out.s = (1.f / lobePdf) * (p.mis(rd.lightPdf, tp) / rd.lightPdf);
+            }
+            else
+            {
+                if (!(lsp > 0.f)) return false;
+                out.v[1] = replay_vertex(p, sd2, mask2, rd.secondWo);
+                out.s = (1.f / lobePdf) * (p.mis(tp, rd.lightPdf) / lsp);
+            }
+            out.nv = 2;
+            f3 o2 = computeRayOrigin(sd2.posW, dot(sd2.faceN, rd.secondWo) >= 0.f ? sd2.faceN : -sd2.faceN);
+            HitInfo h; float t;
+            if (p.bvh.closest(mk_ray(o2, rd.secondWo, 0.f, kRayTMax), h, t))
+                out.emitter = emitter_of(p, p.loadSD(h, rd.secondWo), rd.irradiance);
+        }
+    }
+    f3 B = out.nv == 2 ? out.v[1].g.value : mk3(1.f);
+    f3 A = out.nv >= 1 ? out.v[0].g.value : mk3(1.f);
+    out.value = A * B * out.Le * out.s;
+    // The differentiated function is k * W * s * A(theta) * B(theta) * Le(theta) with k fixed, so that
+    // at the pass's materials it equals the resolved colour integrand * W exactly (the replay and the
+    // path tracer place ray origins slightly differently, which moves f(y) by ~1e-5 relative).
+    out.k = mk3(out.value.x != 0.f ? r.integrand.x / out.value.x : 1.f, out.value.y != 0.f ? r.integrand.y / out.value.y : 1.f,
+                out.value.z != 0.f ? r.integrand.z / out.value.z : 1.f);
+    stats[kStatReplayed]++;
+    if (out.emitter == kInvalidIndex) stats[kStatNoEmitter]++;
+    f3 diff = out.value - r.integrand;
+    if (f_abs(diff.x) + f_abs(diff.y) + f_abs(diff.z) > 1e-3f * (f_abs(r.integrand.x) + f_abs(r.integrand.y) + f_abs(r.integrand.z)))
+        stats[kStatValueMismatch]++;
+    return true;
+}
+
+// d loss / d parameters of one pixel, given d loss / d colour (analytic, FP32 per pixel).
+static void replay_accumulate(const Replay& q, f3 gradColor, double* grad)
+{
+    f3 g = gradColor * q.W * q.k;
+    f3 A = q.nv >= 1 ? q.v[0].g.value : mk3(1.f);
+    f3 B = q.nv == 2 ? q.v[1].g.value : mk3(1.f);
+    if (q.emitter != kInvalidIndex)
+    {
+        f3 dLe = g * A * B * q.s;
+        double* e = grad + (size_t)q.emitter * kGradStride + kGradEmissive;
+        e[0] += dLe.x; e[1] += dLe.y; e[2] += dLe.z;
+    }
+    for (uint32_t k = 0; k < q.nv; k++)
+    {
+        const ReplayVertex& v = q.v[k];
+        f3 other = (k == 0) ? B : A;
+        f3 common = g * other * q.Le * q.s;
+        f3 dB = common * v.g.dBase;
+        f3 dR = common * v.g.dRough;
+        double* m = grad + (size_t)v.material * kGradStride;
+        m[kGradBase + 0] += dB.x; m[kGradBase + 1] += dB.y; m[kGradBase + 2] += dB.z;
+        m[kGradRough] += (double)dR.x + (double)dR.y + (double)dR.z;
+    }
+}
+
+// FP64 value of one BSDF factor of the replay at material parameters `m` (the gates and the
+// local directions stay those of the pass's materials).
+// FP64 material parameters of the replay: baseColor.xyz, roughness, emissive.xyz, metallic.
+struct ParamsFp64 { double v[kGradStride]; };
+
+static void replay_vertex_fp64(const ReplayVertex& v, const ParamsFp64& q, float ior, double out[3])
+{
+    out[0] = out[1] = out[2] = 0.0;
+    if (!v.valid) return;
+    const double wi[3] = {v.wi.x, v.wi.y, v.wi.z}, wo[3] = {v.wo.x, v.wo.y, v.wo.z};
+    double h[3] = {wi[0] + wo[0], wi[1] + wo[1], wi[2] + wo[2]};
+    double hl = std::sqrt(h[0] * h[0] + h[1] * h[1] + h[2] * h[2]);
+    for (double& x : h) x /= hl;
+    const double r = q.v[kGradRough], metal = q.v[7];
+    const double kPiD = 3.14159265358979323846;
+    if (v.diffuseOn)
+    {
+        double woDotH = wo[0] * h[0] + wo[1] * h[1] + wo[2] * h[2];
+        double E = 1.0 + r * (1.0 / 1.51 - 1.0);
+        double fd90 = 0.5 * r + 2.0 * woDotH * woDotH * r;
+        double Pi = std::pow(std::max(1.0 - wi[2], 0.0), 5.0), Po = std::pow(std::max(1.0 - wo[2], 0.0), 5.0);
+        double S = (1.0 + (fd90 - 1.0) * Pi) * (1.0 + (fd90 - 1.0) * Po) * E / kPiD * wo[2];
+        for (int c = 0; c < 3; c++) out[c] += q.v[kGradBase + c] * (1.0 - metal) * S;
+    }
+    if (v.specularOn)
+    {
+        double alpha = std::max(r * r, (double)kMinGGXAlpha), a2 = alpha * alpha;
+        double c = h[2];
+        double dd = c * c * (a2 - 1.0) + 1.0;
+        double D = a2 / (dd * dd * kPiD);
+        auto lambda = [&](double cs) { double t2 = std::max(1.0 - cs * cs, 0.0) / (cs * cs); return 0.5 * (std::sqrt(1.0 + a2 * t2) - 1.0); };
+        double G = 1.0 / (1.0 + lambda(wi[2]) + lambda(wo[2]));
+        double wiDotH = wi[0] * h[0] + wi[1] * h[1] + wi[2] * h[2];
+        double P = std::pow(std::max(1.0 - wiDotH, 0.0), 5.0);
+        double f = (double)((ior - 1.f) / (ior + 1.f));
+        double F0 = f * f;
+        for (int k = 0; k < 3; k++)
+        {
+            double spec = F0 + (q.v[kGradBase + k] - F0) * metal;
+            out[k] += (spec + (1.0 - spec) * P) * D * G * 0.25 / wi[2];
+        }
+    }
+}
+
+static ParamsFp64 params_of(const MaterialData& m)
+{
+    ParamsFp64 q;
+    for (int c = 0; c < 3; c++) { q.v[kGradBase + c] = m.baseColor[c]; q.v[kGradEmissive + c] = m.emissive[c]; }
+    q.v[kGradRough] = m.roughness;
+    q.v[7] = m.metallic;
+    return q;
+}
+
+// The FP64 replay: f(theta) = integrand * W * prod_k factor_k(theta) / factor_k(theta0), so that
+// it equals the resolved colour at the pass's materials theta0 and moves with the FP64 factors.
+static void replay_fp64(const Replay& q, const ParamsFp64* params, const MaterialData* mats, const f3& integrand, double out[3])
+{
+    double A[3] = {1.0, 1.0, 1.0}, B[3] = {1.0, 1.0, 1.0}, A0[3] = {1.0, 1.0, 1.0}, B0[3] = {1.0, 1.0, 1.0};
+    if (q.nv >= 1)
+    {
+        const uint32_t m = q.v[0].material;
+        replay_vertex_fp64(q.v[0], params[m], mats[m].ior, A);
+        replay_vertex_fp64(q.v[0], params_of(mats[m]), mats[m].ior, A0);
+    }
+    if (q.nv == 2)
+    {
+        const uint32_t m = q.v[1].material;
+        replay_vertex_fp64(q.v[1], params[m], mats[m].ior, B);
+        replay_vertex_fp64(q.v[1], params_of(mats[m]), mats[m].ior, B0);
+    }
+    double Le[3] = {q.Le.x, q.Le.y, q.Le.z}, Le0[3] = {q.Le.x, q.Le.y, q.Le.z};
+    if (q.emitter != kInvalidIndex)
+        for (int c = 0; c < 3; c++) { Le[c] = params[q.emitter].v[kGradEmissive + c]; Le0[c] = mats[q.emitter].emissive[c]; }
+    const double I[3] = {integrand.x, integrand.y, integrand.z};
+    for (int c = 0; c < 3; c++)
+    {
+        double den = A0[c] * B0[c] * Le0[c];
+        out[c] = den != 0.0 ? I[c] * (double)q.W * (A[c] * B[c] * Le[c] / den) : 0.0;
+    }
+}
+
+static double replay_loss_fp64(const Replay& q, const ParamsFp64* params, const MaterialData* mats, const f3& integrand,
+                               const float* target)
+{
+    double v[3];
+    replay_fp64(q, params, mats, integrand, v);
+    double loss = 0.0;
+    for (int c = 0; c < 3; c++)
+    {
+        double e = v[c] - (double)target[c];
+        loss += e * e;
+    }
+    return loss;
+}
+
 } // namespace oracle
 
 // ------------------------------------------------------------------ C API (ctypes)
 extern "C" {
 
-struct ro_pass { oracle::Pass p; };
+struct ro_pass
+{
+    oracle::Pass p;
+    std::vector<float> positions;      // the scene's triangle soup, kept for material updates
+    std::vector<uint32_t> materialIds;
+};
 
 __attribute__((visibility("default"))) ro_pass* ro_create(const rs_options* opt)
 {
@@ -1959,6 +2230,8 @@ __attribute__((visibility("default"))) int ro_set_scene(ro_pass* r, const rs_sce
     oracle::Pass& p = r->p;
     if (!prepare_scene(s->numTriangles, s->positions, s->materialIds, s->numMaterials, reinterpret_cast<const MaterialData*>(s->materials), p.scene))
         return RS_INVALID_ARG;
+    r->positions.assign(s->positions, s->positions + 9 * (size_t)s->numTriangles);
+    r->materialIds.assign(s->materialIds, s->materialIds + s->numTriangles);
     p.bvh.build(p.scene.tri, s->numTriangles);
     p.lv.tris = p.scene.lights.data();
     p.lv.aliasTable = p.scene.alias.data();
@@ -1975,7 +2248,12 @@ __attribute__((visibility("default"))) int ro_execute(ro_pass* r, const rs_frame
 }
 
 __attribute__((visibility("default"))) int ro_freeze(ro_pass* r, int frozen) { r->p.frozen = frozen != 0; return RS_OK; }
-__attribute__((visibility("default"))) int ro_reset(ro_pass* r) { r->p.frameCount = 0; return RS_OK; }
+// ReservoirSplatting::reset (ReservoirSplatting.cpp:813-820)
+__attribute__((visibility("default"))) int ro_reset(ro_pass* r)
+{
+    if (!r->p.frozen) { r->p.frameCount = 0; r->p.seed = 0; }
+    return RS_OK;
+}
 
 // Same buffer ids and canonical layouts as rs_get_buffer.
 __attribute__((visibility("default"))) long ro_get_buffer(ro_pass* r, int id, void* dst, size_t cap)
@@ -2043,6 +2321,81 @@ __attribute__((visibility("default"))) int ro_set_buffer(ro_pass* r, int id, con
 
 __attribute__((visibility("default"))) uint32_t ro_frame_count(ro_pass* r) { return r->p.frameCount; }
 
+// Replaces the material parameters (same count) and rebuilds the light collection; the geometry
+// and its BVH stay.
+__attribute__((visibility("default"))) int ro_set_materials(ro_pass* r, const rs_material* mats, uint32_t count)
+{
+    oracle::Pass& p = r->p;
+    if (!p.hasScene || count != p.scene.materials.size()) return RS_INVALID_ARG;
+    if (!prepare_scene((uint32_t)r->materialIds.size(), r->positions.data(), r->materialIds.data(), count,
+                       reinterpret_cast<const MaterialData*>(mats), p.scene))
+        return RS_INVALID_ARG;
+    p.lv.tris = p.scene.lights.data();
+    p.lv.aliasTable = p.scene.alias.data();
+    p.lv.count = (uint32_t)p.scene.lights.size();
+    p.lv.invWeightsSum = p.scene.invWeightsSum;
+    return RS_OK;
+}
+
+// Analytic path-replay gradient of the last frame: adds d loss / d material parameters (count x 8
+// doubles: baseColor.xyz, roughness, emissive.xyz, 0) given d loss / d colour (float4 per pixel).
+// stats: replayed paths, paths longer than three vertices, paths without an identified emitter,
+// replays whose value differs from the reservoir's integrand by more than 1e-3.
+__attribute__((visibility("default"))) int ro_backward(ro_pass* r, const float* gradColor, double* gradOut, uint64_t* stats)
+{
+    oracle::Pass& p = r->p;
+    if (!p.hasScene) return RS_NOT_READY;
+    const auto& res = p.swapped ? p.prev : p.curr;
+    const auto& rec = p.swapped ? p.prevR : p.currR;
+    const size_t N = (size_t)p.W * p.H, M = p.scene.materials.size() * kGradStride;
+    int T = omp_get_max_threads();
+    std::vector<std::vector<double>> part(T, std::vector<double>(M, 0.0));
+    std::vector<std::array<uint64_t, 4>> st(T, std::array<uint64_t, 4>{0, 0, 0, 0});
+#pragma omp parallel for schedule(dynamic, 256)
+    for (long i = 0; i < (long)N; i++)
+    {
+        int t = omp_get_thread_num();
+        oracle::Replay q;
+        if (!oracle::replay_pixel(p, res[i], rec[i], q, st[t].data())) continue;
+        oracle::replay_accumulate(q, mk3(gradColor[4 * i], gradColor[4 * i + 1], gradColor[4 * i + 2]), part[t].data());
+    }
+    for (int t = 0; t < T; t++)
+    {
+        for (size_t k = 0; k < M; k++) gradOut[k] += part[t][k];
+        if (stats) for (int k = 0; k < 4; k++) stats[k] += st[t][k];
+    }
+    return RS_OK;
+}
+
+// FP64 replay loss of the last frame, sum over pixels and channels of (f(y) W - target)^2, with the
+// differentiated parameters taken from `params` (count x 8 doubles: baseColor.xyz, roughness,
+// emissive.xyz, metallic) and everything detached taken from the pass's materials.
+__attribute__((visibility("default"))) double ro_replay_loss(ro_pass* r, const float* target, const double* params, uint32_t count)
+{
+    oracle::Pass& p = r->p;
+    if (!p.hasScene || count != p.scene.materials.size()) return -1.0;
+    const auto& res = p.swapped ? p.prev : p.curr;
+    const auto& rec = p.swapped ? p.prevR : p.currR;
+    const oracle::ParamsFp64* q64 = reinterpret_cast<const oracle::ParamsFp64*>(params);
+    const MaterialData* m = p.scene.materials.data();
+    const size_t N = (size_t)p.W * p.H;
+    double loss = 0.0;
+#pragma omp parallel for schedule(dynamic, 256) reduction(+ : loss)
+    for (long i = 0; i < (long)N; i++)
+    {
+        uint64_t st[4] = {0, 0, 0, 0};
+        oracle::Replay q;
+        const float* t = target + 4 * i;
+        if (!oracle::replay_pixel(p, res[i], rec[i], q, st))
+        {
+            loss += (double)t[0] * t[0] + (double)t[1] * t[1] + (double)t[2] * t[2];
+            continue;
+        }
+        loss += oracle::replay_loss_fp64(q, q64, m, res[i].integrand, t);
+    }
+    return loss;
+}
+
 } // extern "C"
 
 // ------------------------------------------------------------------ test hooks (known-answer tests)
@@ -2091,6 +2444,42 @@ __attribute__((visibility("default"))) double ro_test_alias(const float* w, uint
     for (uint32_t i = 0; i < n; i++) { table[2 * i] = t[i].x; table[2 * i + 1] = t[i].y; }
     return sum;
 }
+// BSDF derivative check: material = (baseColor.xyz, roughness, metallic, ior), directions in the
+// local frame (normal +z).  out = value.xyz, dBase.xyz, dRough.xyz (FP32 analytic); valueFp64 = the
+// FP64 value at the same parameters (for central differences).
+__attribute__((visibility("default"))) void ro_test_bsdf_grad(const float* mat, const float* wi, const float* wo, uint32_t lobeMask,
+                                                             float* out, double* valueFp64)
+{
+    MaterialData m;
+    memset(&m, 0, sizeof(m));
+    m.baseColor[0] = mat[0]; m.baseColor[1] = mat[1]; m.baseColor[2] = mat[2];
+    m.roughness = mat[3]; m.metallic = mat[4]; m.ior = mat[5];
+    ShadingData sd;
+    memset(&sd, 0, sizeof(sd));
+    sd.N = mk3(0.f, 0.f, 1.f); sd.T = mk3(1.f, 0.f, 0.f); sd.B = mk3(0.f, 1.f, 0.f); sd.faceN = sd.N;
+    sd.V = mk3(wi[0], wi[1], wi[2]);
+    sd.frontFacing = true;
+    f3 w = mk3(wo[0], wo[1], wo[2]);
+    BsdfData d = setup_material(m, true);
+    BsdfGrad g = mi_eval_grad(sd, d, lobeMask, w);
+    const f3 v[3] = {g.value, g.dBase, g.dRough};
+    for (int k = 0; k < 3; k++) { out[3 * k] = v[k].x; out[3 * k + 1] = v[k].y; out[3 * k + 2] = v[k].z; }
+    oracle::ParamsFp64 q64;
+    for (int k = 0; k < 8; k++) q64.v[k] = 0.0;
+    for (int k = 0; k < 3; k++) q64.v[kGradBase + k] = mat[k];
+    q64.v[kGradRough] = mat[3];
+    q64.v[7] = mat[4];
+    oracle::ReplayVertex rv;
+    f3 wil = sd_to_local(sd, sd.V), wol = sd_to_local(sd, w);
+    rv.wi = wil; rv.wo = wol;
+    rv.valid = valid_hemisphere(sd, wil, wol, w) && f_min(wil.z, wol.z) >= kMinCosTheta;
+    StandardBSDF b = make_bsdf(wil, d, lobeMask);
+    uint32_t mask = lobeMask == 0 ? 0xfu : lobeMask;
+    rv.diffuseOn = b.pDiffuseReflection > 0.f && (mask & 0x1u);
+    rv.specularOn = b.pSpecularReflection > 0.f && (mask & 0x4u) && b.alpha != 0.f;
+    oracle::replay_vertex_fp64(rv, q64, m.ior, valueFp64);
+}
+
 // Closest hit of one ray against the oracle's BVH of a triangle soup (prim = -1 on a miss).
 __attribute__((visibility("default"))) int ro_test_closest(ro_pass* r, const float* ray, float* tuv)
 {

@@ -61,11 +61,17 @@ def load_library():
     lib.rs_batch_destroy.argtypes = [C.c_void_p]
     lib.rs_batch_launch_count.argtypes = [C.c_void_p]
     lib.rs_batch_launch_count.restype = C.c_uint32
+    lib.rs_set_materials.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32]
+    lib.rs_checkpoint_bytes.argtypes = [C.c_void_p, C.POINTER(C.c_size_t)]
+    lib.rs_checkpoint.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.rs_backward.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.rs_backward_stats.argtypes = [C.c_void_p, C.c_void_p]
     lib.rs_build_cell_lists_static.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     for name in ("rs_create", "rs_destroy", "rs_set_options", "rs_set_scene", "rs_execute", "rs_reset", "rs_set_seed",
                  "rs_freeze", "rs_get_buffer", "rs_set_buffer", "rs_enable_stage_timing", "rs_get_stage_times",
                  "rs_debug_keep_candidates", "rs_batch_create", "rs_batch_execute", "rs_batch_destroy",
-                 "rs_build_cell_lists_static"):
+                 "rs_build_cell_lists_static", "rs_set_materials", "rs_checkpoint_bytes", "rs_checkpoint", "rs_backward",
+                 "rs_backward_stats"):
         getattr(lib, name).restype = C.c_int
     _lib = lib
     return lib
@@ -188,6 +194,32 @@ class ReservoirSplatting:
 
     def last_launch_count(self) -> int:
         return int(self._lib.rs_last_launch_count(self._h))
+
+    # ---- path-replay adjoint (no reference counterpart)
+    def set_materials(self, materials: np.ndarray):
+        """Replaces the scene's material records (n x 16 float32, the rs_material layout)."""
+        m = np.ascontiguousarray(materials, np.float32)
+        _check(self._lib.rs_set_materials(self._h, m.ctypes.data, len(m)))
+
+    def checkpoint_bytes(self) -> int:
+        n = C.c_size_t(0)
+        _check(self._lib.rs_checkpoint_bytes(self._h, C.byref(n)))
+        return int(n.value)
+
+    def checkpoint(self, dst_ptr: int, stream: int = 0):
+        """Copies the last frame's final reservoirs to device memory at dst_ptr."""
+        _check(self._lib.rs_checkpoint(self._h, C.c_void_p(dst_ptr), C.c_void_p(stream)))
+
+    def backward(self, grad_color_ptr: int, grad_materials_ptr: int, checkpoint_ptr: int | None = None, stream: int = 0):
+        """gradMaterials (device, n x 8 float32) += d loss / d parameters for d loss / d colour."""
+        _check(self._lib.rs_backward(self._h, C.c_void_p(checkpoint_ptr) if checkpoint_ptr else None,
+                                     C.c_void_p(grad_color_ptr), C.c_void_p(grad_materials_ptr), C.c_void_p(stream)))
+
+    def backward_stats(self) -> np.ndarray:
+        """Counters since the last read: replayed, too long, emitter not found, value mismatch."""
+        out = np.zeros(4, np.uint64)
+        _check(self._lib.rs_backward_stats(self._h, out.ctypes.data))
+        return out
 
 
 class Batch:

@@ -987,5 +987,7 @@ __global__ void __launch_bounds__(256) k_resolve(uint32_t n, ResPlanes curr, flo
 
 } // namespace rs
 
-// The wavefront kernels share the constant context table, so they live in this translation unit.
+// The wavefront kernels and the adjoint share the constant context table, so they live in this
+// translation unit.
 #include "wavefront.cuh"
+#include "adjoint.cuh"

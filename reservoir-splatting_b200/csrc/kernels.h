@@ -1,6 +1,7 @@
 // Kernel declarations of the Reservoir Splatting pass (definitions in kernels.cu).
 #pragma once
 #include "pass_device.cuh"
+#include "core/material_grad.h"
 
 namespace rs {
 
@@ -24,6 +25,12 @@ __global__ void k_gather_resample(uint32_t slot, const uint4* vbuffer, ResPlanes
 __global__ void k_multi_scatter_resample(uint32_t slot, const float2* mvec, ResPlanes prev, RecPlanes prevRec, ResPlanes curr, RecPlanes currRec,
                                          const uint32_t* counts, const uint32_t* offsets, const uint32_t* sortedAll, float4* color);
 __global__ void k_resolve(uint32_t n, ResPlanes curr, float4* color);
+
+__global__ void k_backward(uint32_t slot, ResPlanes res, RecPlanes rec, const float4* gradColor, double* acc, uint32_t numMaterials,
+                           unsigned long long* stats);
+__global__ void k_grad_flush(const double* acc, float* grad, uint32_t n);
+constexpr uint32_t kAdjointThreads = 128;        // k_backward block size
+constexpr uint32_t kAdjointSharedDoubles = 6016; // k_backward stages numMaterials x 8 sums in shared memory up to this (47 KB)
 
 constexpr uint32_t kMaxPassSlots = 64; // passes alive at once (size of the constant context table)
 cudaError_t upload_ctx(uint32_t slot, const DevCtx* hostPinned, cudaStream_t s);

@@ -6,6 +6,7 @@
 // All device work of rs_execute is issued on the caller's stream with no host
 // synchronisation and no allocation once the frame size and options are stable,
 // so a frame can be captured into a CUDA graph after the first call.
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -129,6 +130,9 @@ struct rs_pass
     DevBuf<float2> backupM;
     DevBuf<uint32_t> fault;
     uint32_t* hostFault = nullptr;
+    DevBuf<unsigned long long> adjStats; // rs_backward counters (replayed, too long, no emitter, value mismatch)
+    DevBuf<double> adjAcc;               // rs_backward FP64 sums, numMaterials x 8
+    bool haveFrameCtx = false;           // hostCtx holds a frame's context (set by begin_frame)
     uint32_t slot = kMaxPassSlots;  // this pass's entry of the constant context table
     DevCtx* hostCtx = nullptr;      // staging copy of the frame's context (begin_frame)
     static constexpr int kRing = 8;
@@ -428,6 +432,7 @@ static void begin_frame(rs_pass* p, const rs_frame_desc* f)
     C.gatherOption = o.gatherOption; C.scatterBackupMIS = o.scatterBackupMISOption; C.numTimePartitions = o.numTimePartitions;
     C.neighborCount = o.neighborCount; C.spatialGatherRadius = o.spatialGatherRadius;
     C.fault = p->fault.p;
+    p->haveFrameCtx = true;
 }
 
 // The spatial ping-pong of spatialResampling (ReservoirSplatting.cpp:2002-2018) on the host-side indices.
@@ -686,10 +691,15 @@ extern "C" RS_API rs_status rs_execute(rs_pass* p, const rs_frame_desc* f, void*
     return RS_OK;
 }
 
+// reset() (ReservoirSplatting.cpp:813-820): frame count and seed restart unless the scene is frozen.
 extern "C" RS_API rs_status rs_reset(rs_pass* p)
 {
     if (!p) return fail(RS_INVALID_ARG, "pass is NULL");
-    p->frameCount = 0;
+    if (!p->frozen)
+    {
+        p->frameCount = 0;
+        p->seed = 0;
+    }
     return RS_OK;
 }
 
@@ -834,6 +844,137 @@ extern "C" RS_API rs_status rs_set_buffer(rs_pass* p, rs_buffer_id id, const voi
         return RS_OK;
     }
     return fail(RS_INVALID_ARG, "buffer cannot be restored");
+}
+
+// ------------------------------------------------------------------ path-replay adjoint
+// (no reference counterpart; the kernel and its estimator are described in adjoint.cuh)
+
+// Replaces the material parameters in place.  The triangle records keep their positions, so the
+// BVH stays; the light collection and its alias table are rebuilt for the new emission.
+extern "C" RS_API rs_status rs_set_materials(rs_pass* p, const rs_material* materials, uint32_t count)
+{
+    if (!p || !materials) return fail(RS_INVALID_ARG, "pass or materials is NULL");
+    if (!p->hasScene) return fail(RS_NOT_READY, "rs_set_materials needs a scene");
+    if (count != p->scene.materials.size()) return fail(RS_INVALID_ARG, "material count differs from the scene's");
+    const size_t n = p->scene.tri.size() / 3;
+    std::vector<float> pos(9 * n);
+    std::vector<uint32_t> ids(n);
+    for (size_t t = 0; t < n; t++)
+    {
+        for (int v = 0; v < 3; v++)
+        {
+            const f4& q = p->scene.tri[3 * t + v];
+            pos[9 * t + 3 * v + 0] = q.x; pos[9 * t + 3 * v + 1] = q.y; pos[9 * t + 3 * v + 2] = q.z;
+        }
+        ids[t] = f2u(p->scene.tri[3 * t].w);
+    }
+    PreparedScene ps;
+    if (!prepare_scene((uint32_t)n, pos.data(), ids.data(), count, reinterpret_cast<const MaterialData*>(materials), ps))
+        return fail(RS_INVALID_ARG, "material id out of range");
+    RS_CUDA(cudaDeviceSynchronize());
+    RS_CUDA(p->dLights.ensure(ps.lights.size() ? ps.lights.size() : 1));
+    RS_CUDA(p->dAlias.ensure(ps.alias.size() ? ps.alias.size() : 1));
+    if (n) RS_CUDA(cudaMemcpy(p->dTri.p, ps.tri.data(), 48ull * n, cudaMemcpyHostToDevice));
+    RS_CUDA(cudaMemcpy(p->dMaterials.p, ps.materials.data(), sizeof(MaterialData) * count, cudaMemcpyHostToDevice));
+    if (!ps.lights.empty())
+    {
+        RS_CUDA(cudaMemcpy(p->dLights.p, ps.lights.data(), sizeof(LightTriangle) * ps.lights.size(), cudaMemcpyHostToDevice));
+        RS_CUDA(cudaMemcpy(p->dAlias.p, ps.alias.data(), sizeof(u2) * ps.alias.size(), cudaMemcpyHostToDevice));
+    }
+    p->scene = std::move(ps);
+    return RS_OK;
+}
+
+extern "C" RS_API rs_status rs_checkpoint_bytes(rs_pass* p, size_t* bytes)
+{
+    if (!p || !bytes) return fail(RS_INVALID_ARG, "pass or bytes is NULL");
+    *bytes = (size_t)p->W * p->H * 144ull;
+    return RS_OK;
+}
+
+// Copies the last frame's final reservoirs into `dst` (device memory, rs_checkpoint_bytes):
+// reservoir plane a, plane b, then the seven reconnection planes, N entries of 16 bytes each.
+extern "C" RS_API rs_status rs_checkpoint(rs_pass* p, void* dst, void* streamPtr)
+{
+    if (!p || !dst) return fail(RS_INVALID_ARG, "pass or destination is NULL");
+    if (!p->haveFrameCtx) return fail(RS_NOT_READY, "no frame has been rendered");
+    cudaStream_t s = static_cast<cudaStream_t>(streamPtr);
+    const size_t N = (size_t)p->W * p->H;
+    const ReservoirSet& last = p->sets[p->swapped ? p->prevIdx : p->currIdx];
+    char* d = static_cast<char*>(dst);
+    RS_CUDA(cudaMemcpyAsync(d, last.a.p, N * 16, cudaMemcpyDeviceToDevice, s));
+    RS_CUDA(cudaMemcpyAsync(d + N * 16, last.b.p, N * 16, cudaMemcpyDeviceToDevice, s));
+    RS_CUDA(cudaMemcpyAsync(d + N * 32, last.rec.p, N * 112, cudaMemcpyDeviceToDevice, s));
+    return RS_OK;
+}
+
+// Adds d loss / d material parameters to gradMaterials (device, numMaterials x 8 floats in the
+// order baseColor.xyz, roughness, emissive.xyz, metallic; the metallic slot is not differentiated)
+// for d loss / d colour `gradColor` (device float4 per pixel) of the frame whose reservoirs are in
+// `checkpoint` (rs_checkpoint layout), or of the last frame when checkpoint is NULL.  The
+// materials must be those the frame was rendered with.
+extern "C" RS_API rs_status rs_backward(rs_pass* p, const void* checkpoint, const float* gradColor, float* gradMaterials, void* streamPtr)
+{
+    if (!p || !gradColor || !gradMaterials) return fail(RS_INVALID_ARG, "pass, gradColor or gradMaterials is NULL");
+    if (!p->hasScene || !p->haveFrameCtx) return fail(RS_NOT_READY, "rs_backward needs a rendered frame");
+    if (p->opt.maxSurfaceBounces > 1)
+        return fail(RS_INVALID_ARG, "rs_backward replays paths of at most three vertices: set maxSurfaceBounces <= 1");
+    cudaStream_t s = static_cast<cudaStream_t>(streamPtr);
+    const size_t N = (size_t)p->W * p->H;
+    if (!p->adjStats.p)
+    {
+        RS_CUDA(p->adjStats.ensure(4));
+        RS_CUDA(cudaMemset(p->adjStats.p, 0, 4 * sizeof(unsigned long long)));
+    }
+    ResPlanes res;
+    RecPlanes rec;
+    if (checkpoint)
+    {
+        char* c = const_cast<char*>(static_cast<const char*>(checkpoint));
+        res = ResPlanes{reinterpret_cast<float4*>(c), reinterpret_cast<float4*>(c + N * 16)};
+        rec = RecPlanes{reinterpret_cast<uint4*>(c + N * 32), N};
+    }
+    else
+    {
+        const ReservoirSet& last = p->sets[p->swapped ? p->prevIdx : p->currIdx];
+        res = last.res();
+        rec = last.recp();
+    }
+    const int k = p->ringNext;
+    p->ringNext = (k + 1) % rs_pass::kRing;
+    RS_CUDA(cudaEventSynchronize(p->ringEv[k]));
+    p->ringCtx[k] = *p->hostCtx;
+    RS_CUDA(upload_ctx(p->slot, &p->ringCtx[k], s));
+    RS_CUDA(cudaEventRecord(p->ringEv[k], s));
+    const uint32_t numMaterials = (uint32_t)p->scene.materials.size();
+    const uint32_t M = numMaterials * kGradStride;
+    RS_CUDA(p->adjAcc.ensure(M));
+    RS_CUDA(cudaMemsetAsync(p->adjAcc.p, 0, M * sizeof(double), s));
+    const size_t smem = M <= kAdjointSharedDoubles ? M * sizeof(double) : 0;
+    const uint32_t blocks = (uint32_t)std::min<size_t>((N + kAdjointThreads - 1) / kAdjointThreads, 148ull * 8ull);
+    k_backward<<<blocks, kAdjointThreads, smem, s>>>(p->slot, res, rec, reinterpret_cast<const float4*>(gradColor), p->adjAcc.p,
+                                                     numMaterials, p->adjStats.p);
+    k_grad_flush<<<(M + 255) / 256, 256, 0, s>>>(p->adjAcc.p, gradMaterials, M);
+    RS_CUDA(cudaGetLastError());
+    p->lastStream = s;
+    p->launches = 2;
+    return RS_OK;
+}
+
+// Reads and clears the counters of rs_backward since the last read: paths replayed, paths longer
+// than three vertices (skipped), paths whose emitter the replay could not identify (no emission
+// gradient), replays that differ from the stored integrand by more than 1e-3 relative.
+extern "C" RS_API rs_status rs_backward_stats(rs_pass* p, uint64_t* out)
+{
+    if (!p || !out) return fail(RS_INVALID_ARG, "pass or out is NULL");
+    for (int i = 0; i < 4; i++) out[i] = 0;
+    if (!p->adjStats.p) return RS_OK;
+    unsigned long long h[4];
+    RS_CUDA(cudaStreamSynchronize(p->lastStream));
+    RS_CUDA(cudaMemcpy(h, p->adjStats.p, sizeof(h), cudaMemcpyDeviceToHost));
+    RS_CUDA(cudaMemset(p->adjStats.p, 0, sizeof(h)));
+    for (int i = 0; i < 4; i++) out[i] = h[i];
+    return RS_OK;
 }
 
 extern "C" RS_API rs_status rs_enable_stage_timing(rs_pass* p, uint32_t enable)

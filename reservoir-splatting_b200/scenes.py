@@ -220,6 +220,51 @@ def terrain_spheres(seed: int = 1, grid: int = 512, spheres: int = 500, subdiv: 
     return Scene(pos, np.concatenate(mids), np.stack(mats).astype(np.float32), "terrain_spheres", info)
 
 
+def inverse_scene(seed: int = 5, grid: int = 300, spheres: int = 16, subdiv: int = 3, materials: int = 32,
+                  emitters: int = 8, extent: float = 60.0, height: float = 6.0) -> Scene:
+    """Scene for differentiation: fBm terrain + icospheres sharing `materials` metal-rough materials
+    (albedo U[0.2, 0.9] per channel, roughness U[0.1, 0.8], half of them with metallic U[0, 1]) and
+    `emitters` emissive quads, each with its own material (radiance U[5, 50] per channel).
+    The defaults give 199,298 triangles."""
+    rng = np.random.default_rng(seed)
+    hmap = _fbm(grid, rng) * height
+    xs = np.linspace(-extent / 2, extent / 2, grid)
+    X, Z = np.meshgrid(xs, xs)
+    P = np.stack([X, hmap, Z], -1)
+    a, b, c, d = P[:-1, :-1], P[:-1, 1:], P[1:, 1:], P[1:, :-1]
+    t1 = np.stack([a, c, b], 2).reshape(-1, 9)
+    t2 = np.stack([a, d, c], 2).reshape(-1, 9)
+    terrain = np.concatenate([t1, t2]).astype(np.float32)
+    mats = []
+    for m in range(materials):
+        metallic = float(rng.uniform(0.0, 1.0)) if m % 2 else 0.0
+        mats.append(material(tuple(rng.uniform(0.2, 0.9, 3)), roughness=float(rng.uniform(0.1, 0.8)), metallic=metallic))
+    # terrain in bands of the first four materials, spheres over the rest
+    band = np.clip(((terrain[:, 0] + extent / 2) / extent * 4).astype(np.int64), 0, 3)
+    blocks, mids = [terrain], [band.astype(np.uint32)]
+    ico = _icosphere(subdiv)
+    for s in range(spheres):
+        r = rng.uniform(0.8, 3.0)
+        px, pz = rng.uniform(-0.4 * extent, 0.4 * extent, 2)
+        gi = int((px + extent / 2) / extent * (grid - 1))
+        gj = int((pz + extent / 2) / extent * (grid - 1))
+        py = hmap[min(max(gj, 0), grid - 1), min(max(gi, 0), grid - 1)] + r * 0.8
+        tri = (ico * r + np.array([px, py, pz])).reshape(-1, 9).astype(np.float32)
+        blocks.append(tri)
+        mids.append(np.full(len(tri), 4 + s % (materials - 4), np.uint32))
+    for e in range(emitters):
+        cx, cz = rng.uniform(-0.4 * extent, 0.4 * extent, 2)
+        cy = height + rng.uniform(6.0, 14.0)
+        s = rng.uniform(1.5, 3.5)
+        p0, p1, p2, p3 = (cx - s, cy, cz - s), (cx + s, cy, cz - s), (cx + s, cy, cz + s), (cx - s, cy, cz + s)
+        blocks.append(np.array([p0 + p1 + p2, p0 + p2 + p3], np.float32))  # normals point down
+        mats.append(material((0.0, 0.0, 0.0), emissive=tuple(rng.uniform(5.0, 50.0, 3)), double_sided=False))
+        mids.append(np.full(2, len(mats) - 1, np.uint32))
+    pos = np.concatenate(blocks).astype(np.float32)
+    info = {"triangles": int(len(pos)), "materials": materials, "emitters": emitters}
+    return Scene(pos, np.concatenate(mids), np.stack(mats).astype(np.float32), "inverse_scene", info)
+
+
 def orbit_camera(frame: int, width: int, height: int, degrees_per_frame: float = 0.5, radius: float = 60.0,
                  height_above: float = 22.0, fov_y_deg: float = 45.0) -> Camera:
     """Camera orbiting the scene centre at `degrees_per_frame`."""

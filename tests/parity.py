@@ -1,6 +1,6 @@
 """Comparison helpers for the CUDA-vs-oracle parity tests.
 
-Contract: splat targets, surviving splats, in-cell order and
+Parity contract: splat targets, surviving splats, in-cell order and
 selected-reservoir data (hits, path lengths, flags) are bit-exact; radiance, W and
 the other float fields agree within REL_TOL relative error.
 """

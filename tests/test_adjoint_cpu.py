@@ -1,0 +1,123 @@
+"""Path-replay adjoint on the CPU: the BSDF derivatives and the oracle's analytic replay gradient
+against FP64 central differences.
+
+The differentiated function is the replay estimator of the pass (selections, contribution weights,
+sampling densities and MIS weights held at the rendered values; BSDF factors and emitted radiance
+re-evaluated), written out in FP64 by the oracle.  Central differences use h = 1e-3 and h = 5e-4
+combined by Richardson extrapolation: a plain h = 1e-3 difference has an O(h^2) truncation error
+near 1e-3 on the roughness of sharp GGX lobes, the size of the tolerance itself.
+"""
+import numpy as np
+import pytest
+
+GRAD_TOL = 1e-3  # relative error of a gradient against FP64 central differences
+
+
+def _cd(f, x, h):
+    return (f(x + h) - f(x - h)) / (2 * h)
+
+
+def _richardson(f, x, h=1e-3):
+    return (4 * _cd(f, x, h / 2) - _cd(f, x, h)) / 3
+
+
+def test_bsdf_derivatives_match_fp64_differences(oracle_mod):
+    rng = np.random.default_rng(0)
+    worst = 0.0
+    for _ in range(300):
+        mat = np.array([*rng.uniform(0.05, 0.95, 3), rng.uniform(0.12, 0.95), rng.choice([0.0, 0.3, 1.0]), 1.5])
+
+        def unit():
+            v = rng.normal(size=3)
+            v[2] = abs(v[2]) + 0.1
+            return v / np.linalg.norm(v)
+
+        wi, wo = unit(), unit()
+        mask = int(rng.choice([0, 1, 4, 0xF]))
+        value, d_base, d_rough, value64 = oracle_mod.bsdf_grad(mat, wi, wo, mask)
+        scale = max(np.abs(value64).max(), 1e-9)
+        assert np.abs(value - value64).max() <= 1e-5 * scale
+
+        def val(k):
+            def f(x):
+                m = mat.copy()
+                m[k] = x
+                return oracle_mod.bsdf_grad(m, wi, wo, mask)[3]
+            return f
+
+        fd_base = np.array([_richardson(val(c), mat[c])[c] for c in range(3)])
+        fd_rough = _richardson(val(3), mat[3])
+        err = max(np.abs(fd_base - d_base).max() / max(np.abs(fd_base).max(), 1e-9),
+                  np.abs(fd_rough - d_rough).max() / max(np.abs(fd_rough).max(), 1e-3 * scale))
+        worst = max(worst, err)
+    assert worst < GRAD_TOL, worst
+
+
+def _replay_check(oracle_mod, scene, camera_fn, width, height, frames, props, perturb_seed=1):
+    """Analytic oracle gradient vs FP64 Richardson differences of the replay L2 loss against a
+    target rendered with perturbed parameters; returns (max error / max |grad|, stats)."""
+    mats = np.array(scene.materials, np.float32).reshape(len(scene.materials), -1)
+    emissive = mats[:, 4:7].max(1) > 0
+    rng = np.random.default_rng(perturb_seed)
+    pert = mats.copy()
+    pert[~emissive, :3] = np.clip(pert[~emissive, :3] + rng.normal(0, 0.05, (int((~emissive).sum()), 3)), 0.0, 1.0)
+    pert[~emissive, 3] = np.clip(pert[~emissive, 3] + rng.normal(0, 0.05, int((~emissive).sum())), 0.1, 1.0)
+    pert[emissive, 4:7] *= 1.0 + rng.normal(0, 0.05, (int(emissive.sum()), 3))
+    tgt = oracle_mod.OraclePass(props, width, height)
+    tgt.set_scene(scene)
+    tgt.set_materials(pert)
+    ora = oracle_mod.OraclePass(props, width, height)
+    ora.set_scene(scene)
+    P0 = mats[:, :8].astype(np.float64)
+    params = [(m, k) for m in range(len(mats)) for k in (range(4, 7) if emissive[m] else range(4))]
+    G = np.zeros((len(mats), 8))
+    FD = np.zeros((len(mats), 8))
+    stats = np.zeros(4, np.uint64)
+    for f in range(frames):
+        cam = camera_fn(f, width, height)
+        target = tgt.execute(cam)
+        img = ora.execute(cam)
+        g, st = ora.backward(2.0 * (img - target), len(mats))
+        G += g
+        stats += st
+        for m, k in params:
+            def loss(x):
+                q = P0.copy()
+                q[m, k] = x
+                return ora.replay_loss(target, q)
+            FD[m, k] += _richardson(loss, P0[m, k])
+    return np.abs(G - FD).max() / np.abs(FD).max(), stats, G, FD
+
+
+@pytest.mark.parametrize("case", ["cornell", "inverse_scene"])
+def test_oracle_replay_gradient_matches_fp64_differences(oracle_mod, scenes, case):
+    props = {"temporalReuse": "ScatterBackup", "gatherOption": "Clamped", "maxSurfaceBounces": 1,
+             "enableSpatialResampling": True}
+    if case == "cornell":
+        err, stats, G, FD = _replay_check(oracle_mod, scenes.cornell_box(0), scenes.cornell_camera, 32, 32, 3, props)
+    else:
+        sc = scenes.inverse_scene(grid=64, spheres=6, subdiv=2)
+        err, stats, G, FD = _replay_check(oracle_mod, sc, scenes.translate_camera, 40, 40, 3, props)
+    assert stats[0] > 0 and stats[1] == 0
+    assert err < GRAD_TOL, err
+    big = np.abs(FD) > 1e-2 * np.abs(FD).max()
+    assert (np.abs(G - FD)[big] / np.abs(FD)[big]).max() < GRAD_TOL
+
+
+def test_set_materials_equals_a_fresh_scene(oracle_mod, scenes):
+    """Replacing the materials in place renders exactly what a scene built with them renders."""
+    props = {"temporalReuse": "ScatterBackup", "maxSurfaceBounces": 1}
+    sc = scenes.cornell_box(0)
+    mats = np.array(sc.materials, np.float32).reshape(len(sc.materials), -1).copy()
+    mats[0, :3] = (0.3, 0.6, 0.2)
+    mats[3, 4:7] = (9.0, 14.0, 6.0)
+    a = oracle_mod.OraclePass(props, 24, 24)
+    a.set_scene(sc)
+    a.set_materials(mats)
+    sc2 = scenes.cornell_box(0)
+    sc2.materials[:] = mats
+    b = oracle_mod.OraclePass(props, 24, 24)
+    b.set_scene(sc2)
+    for f in range(2):
+        cam = scenes.cornell_camera(f, 24, 24)
+        np.testing.assert_array_equal(a.execute(cam), b.execute(cam))

@@ -1,0 +1,161 @@
+"""rs_backward (CUDA, through the C ABI) against the oracle's replay gradient and FP64 differences,
+and the torch.autograd layer over it.
+
+The forward passes are bit-exact between GPU and oracle, so both differentiate the same selected
+paths.  The GPU sums per-pixel terms in FP32 with atomics in arbitrary order; the oracle sums them
+in FP64.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+GRAD_TOL = 1e-3    # against FP64 central differences (Richardson, h = 1e-3 and 5e-4)
+ORACLE_TOL = 1e-4  # against the oracle's analytic gradient, relative to the largest component
+
+
+def _cuda_ok():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+PROPS = {"temporalReuse": "ScatterBackup", "gatherOption": "Clamped", "maxSurfaceBounces": 1,
+         "enableSpatialResampling": True}
+
+
+def _setup(rs, oracle_mod, scenes, width=64, height=64):
+    sc = scenes.inverse_scene(grid=80, spheres=8, subdiv=2)
+    gpu = rs.ReservoirSplatting(PROPS, width, height)
+    gpu.set_scene(sc)
+    ora = oracle_mod.OraclePass(PROPS, width, height)
+    ora.set_scene(sc)
+    mats = np.array(sc.materials, np.float32).reshape(len(sc.materials), -1)
+    return sc, gpu, ora, mats
+
+
+def _richardson(f, x, h=1e-3):
+    cd = lambda hh: (f(x + hh) - f(x - hh)) / (2 * hh)
+    return (4 * cd(h / 2) - cd(h)) / 3
+
+
+@pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
+def test_backward_matches_oracle_and_fp64_differences(rs, oracle_mod, scenes):
+    import torch
+    W = H = 64
+    sc, gpu, ora, mats = _setup(rs, oracle_mod, scenes, W, H)
+    rng = np.random.default_rng(2)
+    n = len(mats)
+    G = torch.zeros((n, 8), dtype=torch.float32, device="cuda")
+    O = np.zeros((n, 8))
+    FD = np.zeros((n, 8))
+    P0 = mats[:, :8].astype(np.float64)
+    emissive = mats[:, 4:7].max(1) > 0
+    params = [(m, k) for m in range(n) for k in (range(4, 7) if emissive[m] else range(4))]
+    stats = np.zeros(4, np.uint64)
+    for f in range(3):
+        cam = scenes.translate_camera(f, W, H)
+        img = gpu.render(cam)
+        np.testing.assert_array_equal(img, ora.execute(cam))
+        target = (img * rng.uniform(0.9, 1.1, img.shape)).astype(np.float32)
+        gc = (2.0 * (img - target)).astype(np.float32)
+        gpu.backward(torch.from_numpy(gc).cuda().data_ptr(), G.data_ptr())
+        torch.cuda.synchronize()
+        stats += gpu.backward_stats()
+        O += ora.backward(gc, n)[0]
+        for m, k in params:
+            def loss(x):
+                q = P0.copy()
+                q[m, k] = x
+                return ora.replay_loss(target, q)
+            FD[m, k] += _richardson(loss, P0[m, k])
+    g = G.cpu().numpy().astype(np.float64)
+    assert stats[0] > 0 and stats[1] == 0
+    assert np.abs(g - O).max() <= ORACLE_TOL * np.abs(O).max()
+    assert np.abs(g - FD).max() <= GRAD_TOL * np.abs(FD).max()
+    big = np.abs(FD) > 1e-2 * np.abs(FD).max()
+    assert (np.abs(g - FD)[big] / np.abs(FD)[big]).max() < GRAD_TOL
+    gpu.close()
+
+
+@pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
+def test_checkpoint_replays_an_earlier_frame(rs, scenes):
+    """Backward from a checkpoint taken at frame f equals backward run right after frame f."""
+    import torch
+    W = H = 48
+    sc = scenes.inverse_scene(grid=64, spheres=6, subdiv=2)
+    p = rs.ReservoirSplatting(PROPS, W, H)
+    p.set_scene(sc)
+    n = len(sc.materials)
+    gc = torch.rand((H, W, 4), device="cuda")
+    p.render(scenes.translate_camera(0, W, H))
+    ck = torch.empty(p.checkpoint_bytes(), dtype=torch.uint8, device="cuda")
+    p.checkpoint(ck.data_ptr())
+    direct = torch.zeros((n, 8), device="cuda")
+    p.backward(gc.data_ptr(), direct.data_ptr())
+    p.render(scenes.translate_camera(1, W, H))
+    later = torch.zeros((n, 8), device="cuda")
+    p.backward(gc.data_ptr(), later.data_ptr(), checkpoint_ptr=ck.data_ptr())
+    torch.cuda.synchronize()
+    scale = direct.abs().max().item()
+    assert scale > 0
+    assert (direct - later).abs().max().item() <= 1e-5 * scale
+    p.close()
+
+
+@pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
+def test_set_materials_renders_like_the_oracle(rs, oracle_mod, scenes):
+    W = H = 40
+    sc, gpu, ora, mats = _setup(rs, oracle_mod, scenes, W, H)
+    new = mats.copy()
+    new[:32, :3] = np.clip(new[:32, :3] * 0.8 + 0.1, 0, 1)
+    new[32:, 4:7] *= 1.3
+    gpu.set_materials(new)
+    ora.set_materials(new)
+    for f in range(3):
+        cam = scenes.translate_camera(f, W, H)
+        np.testing.assert_array_equal(gpu.render(cam), ora.execute(cam))
+    gpu.close()
+
+
+@pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
+def test_backward_rejects_paths_longer_than_three_vertices(rs, scenes):
+    import torch
+    p = rs.ReservoirSplatting(dict(PROPS, maxSurfaceBounces=2), 16, 16)
+    p.set_scene(scenes.cornell_box(0))
+    p.render(scenes.cornell_camera(0, 16, 16))
+    g = torch.zeros((16, 16, 4), device="cuda")
+    out = torch.zeros((len(scenes.cornell_box(0).materials), 8), device="cuda")
+    with pytest.raises(rs.RsError, match="maxSurfaceBounces"):
+        p.backward(g.data_ptr(), out.data_ptr())
+    p.close()
+
+
+@pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
+def test_autograd_l2_loss_matches_direct_backward(rs, scenes):
+    """torch autograd over render_sequence gives the summed rs_backward gradient of the L2 loss."""
+    import torch
+    import reservoir_splatting_b200.adjoint as adj
+    W = H = 48
+    sc = scenes.inverse_scene(grid=64, spheres=6, subdiv=2)
+    renderer = adj.Renderer(sc, PROPS, W, H)
+    cams = [scenes.translate_camera(f, W, H) for f in range(3)]
+    theta = renderer.params().clone()
+    target, _ = renderer.render(cams, keep_checkpoints=False)
+    target = target * 1.05
+    p = theta.clone().requires_grad_(True)
+    images = adj.render_sequence(p, renderer, cams)
+    loss = ((images - target)[..., :3] ** 2).sum()
+    loss.backward()
+    # direct: the same frames, rs_backward with d loss / d image = 2 (image - target)
+    imgs, ckpts = renderer.render(cams)
+    torch.testing.assert_close(imgs, images.detach(), rtol=0, atol=0)
+    gimg = 2.0 * (imgs - target)
+    gimg[..., 3] = 0.0
+    direct = renderer.backward(gimg, ckpts).cpu()
+    scale = direct.abs().max().item()
+    assert scale > 0
+    assert (p.grad - direct).abs().max().item() <= 1e-5 * scale
+    assert torch.all(p.grad[:, 7] == 0)

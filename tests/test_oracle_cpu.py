@@ -129,3 +129,28 @@ def test_resampled_estimate_is_unbiased(oracle_mod, scenes):
     a = np.mean([im[..., :3].mean() for im in plain])
     b = np.mean([im[..., :3].mean() for im in restir[4:]])
     assert b == pytest.approx(a, rel=0.06)
+
+
+def test_reset_restarts_frame_count_and_seed(oracle_mod, scenes):
+    """reset() (ReservoirSplatting.cpp:813-820) zeroes the frame count and the seed unless the scene
+    is frozen, so a sequence rendered after a reset repeats exactly."""
+    props = {"temporalReuse": "ScatterBackup", "maxSurfaceBounces": 1, "enableSpatialResampling": True}
+    ora = oracle_mod.OraclePass(props, 24, 24)
+    ora.set_scene(scenes.cornell_box(0))
+    cams = [scenes.cornell_camera(f, 24, 24) for f in range(3)]
+
+    def sequence():
+        ora.reset()
+        return [ora.execute(c, should_reset=(f == 0)) for f, c in enumerate(cams)]
+
+    a, b = sequence(), sequence()
+    for x, y in zip(a, b):
+        np.testing.assert_array_equal(x, y)
+    count = lambda: ora._lib.ro_frame_count(ora._h)
+    assert count() == 3
+    ora.freeze(True)
+    ora.reset()  # ignored while frozen
+    assert count() == 3
+    ora.freeze(False)
+    ora.reset()
+    assert count() == 0
