@@ -198,6 +198,13 @@ RS_API rs_status rs_batch_execute(rs_batch* batch, const rs_frame_desc* frames, 
 RS_API rs_status rs_batch_destroy(rs_batch* batch);
 RS_API uint32_t rs_batch_launch_count(rs_batch* batch);
 
+/* Ray-query diagnostics (no reference counterpart).  rs_debug_trace_rays: closest hits of n host
+ * rays (8 floats each: origin.xyz, direction.xyz, tMin, tMax) against the pass's BVH: prim[n] (-1 on
+ * a miss), tuv[3n], counts[2n] = nodes visited and triangles tested.  rs_debug_bvh_shape: {nodes,
+ * depth, internal children, leaf children, leaf triangles, surface-area cost}.  Both synchronise. */
+RS_API rs_status rs_debug_trace_rays(rs_pass* pass, const float* rays, uint32_t n, int32_t* prim, float* tuv, uint32_t* counts);
+RS_API rs_status rs_debug_bvh_shape(rs_pass* pass, double* out6);
+
 /* Path-replay adjoint (no reference counterpart: the reference pass renders forward only).
  *
  * A pixel's colour is f(y) * W, y being the path its final reservoir selected.  rs_backward holds

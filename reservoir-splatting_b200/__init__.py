@@ -66,12 +66,14 @@ def load_library():
     lib.rs_checkpoint.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
     lib.rs_backward.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     lib.rs_backward_stats.argtypes = [C.c_void_p, C.c_void_p]
+    lib.rs_debug_trace_rays.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.rs_debug_bvh_shape.argtypes = [C.c_void_p, C.c_void_p]
     lib.rs_build_cell_lists_static.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     for name in ("rs_create", "rs_destroy", "rs_set_options", "rs_set_scene", "rs_execute", "rs_reset", "rs_set_seed",
                  "rs_freeze", "rs_get_buffer", "rs_set_buffer", "rs_enable_stage_timing", "rs_get_stage_times",
                  "rs_debug_keep_candidates", "rs_batch_create", "rs_batch_execute", "rs_batch_destroy",
                  "rs_build_cell_lists_static", "rs_set_materials", "rs_checkpoint_bytes", "rs_checkpoint", "rs_backward",
-                 "rs_backward_stats"):
+                 "rs_backward_stats", "rs_debug_trace_rays", "rs_debug_bvh_shape"):
         getattr(lib, name).restype = C.c_int
     _lib = lib
     return lib
@@ -214,6 +216,22 @@ class ReservoirSplatting:
         """gradMaterials (device, n x 8 float32) += d loss / d parameters for d loss / d colour."""
         _check(self._lib.rs_backward(self._h, C.c_void_p(checkpoint_ptr) if checkpoint_ptr else None,
                                      C.c_void_p(grad_color_ptr), C.c_void_p(grad_materials_ptr), C.c_void_p(stream)))
+
+    # ---- ray-query diagnostics
+    def trace_rays(self, rays: np.ndarray):
+        """Closest hits of rays (n x 8 float32: origin, direction, tMin, tMax): prim, tuv, counts."""
+        r = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+        n = len(r)
+        prim = np.empty(n, np.int32)
+        tuv = np.empty((n, 3), np.float32)
+        counts = np.empty((n, 2), np.uint32)
+        _check(self._lib.rs_debug_trace_rays(self._h, r.ctypes.data, n, prim.ctypes.data, tuv.ctypes.data, counts.ctypes.data))
+        return prim, tuv, counts
+
+    def bvh_shape(self) -> dict:
+        out = np.zeros(6, np.float64)
+        _check(self._lib.rs_debug_bvh_shape(self._h, out.ctypes.data))
+        return dict(zip(["nodes", "depth", "internal_children", "leaf_children", "leaf_triangles", "sah_cost"], out.tolist()))
 
     def backward_stats(self) -> np.ndarray:
         """Counters since the last read: replayed, too long, emitter not found, value mismatch."""

@@ -1,40 +1,120 @@
-// Linear BVH over the triangle soup and its stack traversal: the ray-query
-// layer that replaces the reference's hardware acceleration structure
-// (SceneRayQuery::traceRay / traceVisibilityRay, Scene/RaytracingInline.slang:86-362).
+// The ray-query layer that replaces the reference's hardware acceleration structure
+// (SceneRayQuery::traceRay / traceVisibilityRay, Scene/RaytracingInline.slang:86-362): two trees
+// over the same triangles, each serving the query it traverses fastest.
 //
-// Node layout (64 B, one 4 x float4 record per internal node):
-//   [0] = left child box lo.xyz,  left child index (uint bits)
-//   [1] = left child box hi.xyz,  right child index (uint bits)
-//   [2] = right child box lo.xyz, unused
-//   [3] = right child box hi.xyz, unused
-// A child index with bit 31 set is a leaf holding the triangle index in bits 0-30.
-// Boxes are padded outward by a relative 1e-6 so a box test can only prune, never
-// reject a triangle the exact intersection test accepts; the closest hit is the
-// (t, triangle index) minimum over all triangles and does not depend on the tree.
+// Closest hit: the binary LBVH, 64 bytes per internal node (four float4):
+//   [0] left child box lo.xyz, left child reference   [1] left child box hi.xyz, right child reference
+//   [2] right child box lo.xyz                         [3] right child box hi.xyz
+// A reference with kLeafBit set is a single-triangle leaf (its position in the leaf-order array).
+// The traversal visits the nearer child first and keeps the farther one on a stack.
+//
+// Visibility (any hit): the 4-wide tree collapsed from it, 112 bytes per node (seven float4),
+// children's boxes as structure of arrays:
+//   [0] lo.x of children 0-3   [1] hi.x   [2] lo.y   [3] hi.y   [4] lo.z   [5] hi.z
+//   [6] child references (uint bits): an internal child's node index; a leaf
+//       kLeafBit | first << 2 | (count - 1), count 1..4 triangles from leaf triangle `first`;
+//       an empty slot kInvalidIndex with the box (+inf, -inf), which no ray enters.
+// Leaf triangles are the scene's triangles in leaf order as (p0, scene index), (p1 - p0), (p2 - p0)
+// (the edges the intersection test forms anyway).
+//
+// Child boxes are padded outward by a relative 1e-6 of their coordinates and a box counts as hit
+// when its entry distance is within 2e-6 |exit distance| of the exit, so a box test only prunes
+// triangles the exact intersection test rejects: the slab distances are off by a few ulp of the
+// box coordinate (inside the padding) and of t (inside the slack).  A zero direction component
+// uses 1/d = +-1e20 in the 4-wide test, so its products stay finite and NaN-free.
+// The closest hit is the (t, scene index) minimum over all triangles and does not depend on the
+// tree; shading reads the scene-order triangle array.
 #pragma once
 #include "core/material.h"
 
 namespace rs {
 
 constexpr uint32_t kLeafBit = 0x80000000u;
-constexpr int kTraversalStack = 64;
+constexpr uint32_t kMaxBvhTriangles = 1u << 29; // leaf references keep `first` in 29 bits
+constexpr int kTraversalStack = 64;             // pending subtrees per ray
 
 struct BvhView
 {
-    const float4* nodes;
-    const float4* tri;      // 3 float4 per triangle (see geom.h TriangleView)
-    uint32_t root;          // kLeafBit | tri when the scene has one triangle
+    const float4* binNodes; // binary nodes, four float4 each
+    uint32_t binRoot;       // 0, or kLeafBit | 0 for a scene of one triangle
+    const float4* nodes;    // 4-wide nodes, seven float4 each; the root is node 0
+    const float4* leafTri;  // leaf-order triangles, three float4 each
+    const float4* tri;      // scene-order triangles (geom.h layout), for shading
     uint32_t numTris;
 };
 
-__device__ __forceinline__ bool slab_interval(float lo, float hi, float o, float inv, float& t0, float& t1)
+// A ray as values: the traversal keeps it in registers (a reference into local or constant
+// memory could alias the traversal stack and force reloads).
+struct RayQ
+{
+    float ox, oy, oz, dx, dy, dz;
+    float ix, iy, iz; // 1/d, a zero component as +-1e20 (keeps the sign, no inf * 0)
+    float ox_ix, oy_iy, oz_iz;
+    float tMin, tMax;
+    uint32_t nearX, farX, nearY, farY, nearZ, farZ; // node float4 holding each axis' entry / exit planes
+};
+
+__device__ __forceinline__ float safe_inv(float d) { return fabsf(d) > 1e-20f ? 1.f / d : copysignf(1e20f, d); }
+
+__device__ __forceinline__ RayQ make_rayq(const Ray& r)
+{
+    RayQ q;
+    q.ox = r.origin.x; q.oy = r.origin.y; q.oz = r.origin.z;
+    q.dx = r.dir.x; q.dy = r.dir.y; q.dz = r.dir.z;
+    q.ix = safe_inv(r.dir.x); q.iy = safe_inv(r.dir.y); q.iz = safe_inv(r.dir.z);
+    q.ox_ix = q.ox * q.ix; q.oy_iy = q.oy * q.iy; q.oz_iz = q.oz * q.iz;
+    q.tMin = r.tMin; q.tMax = r.tMax;
+    const uint32_t sx = q.ix < 0.f ? 1u : 0u, sy = q.iy < 0.f ? 1u : 0u, sz = q.iz < 0.f ? 1u : 0u;
+    q.nearX = sx; q.farX = 1u - sx; q.nearY = 2u + sy; q.farY = 3u - sy; q.nearZ = 4u + sz; q.farZ = 5u - sz;
+    return q;
+}
+
+__device__ __forceinline__ float max3f(float a, float b, float c)
+{
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+__device__ __forceinline__ float min3f(float a, float b, float c)
+{
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+
+// Entry distance into a child box given its entry planes (nx, ny, nz) and exit planes (fx, fy, fz)
+// along the ray's direction, or kMissKey when the box is not entered before tmax.  With 1/d's
+// sign the entry plane of each slab is known, so one fma per plane and two 3-way min / max give
+// the interval (the same interval as min / max over both planes).
+constexpr float kMissKey = 3e38f;
+__device__ __forceinline__ float child_entry(float nx, float fx, float ny, float fy, float nz, float fz, const RayQ& r, float tmax)
+{
+    const float t0 = max3f(__fmaf_rn(nx, r.ix, -r.ox_ix), __fmaf_rn(ny, r.iy, -r.oy_iy), fmaxf(__fmaf_rn(nz, r.iz, -r.oz_iz), 0.f));
+    const float t1 = min3f(__fmaf_rn(fx, r.ix, -r.ox_ix), __fmaf_rn(fy, r.iy, -r.oy_iy), fminf(__fmaf_rn(fz, r.iz, -r.oz_iz), tmax));
+    return t0 <= __fmaf_rn(2e-6f, fabsf(t1), t1) ? t0 : kMissKey;
+}
+
+__device__ __forceinline__ bool leaf_tri_test(const float4* __restrict__ leafTri, uint32_t k, const RayQ& r, float& t, float& u, float& v,
+                                              uint32_t& prim)
+{
+    const float4 a = __ldg(&leafTri[3 * (size_t)k + 0]);
+    const float4 b = __ldg(&leafTri[3 * (size_t)k + 1]);
+    const float4 c = __ldg(&leafTri[3 * (size_t)k + 2]);
+    prim = __float_as_uint(a.w);
+    return intersect_triangle_e(mk3(r.ox, r.oy, r.oz), mk3(r.dx, r.dy, r.dz), mk3(a.x, a.y, a.z), mk3(b.x, b.y, b.z), mk3(c.x, c.y, c.z),
+                                r.tMin, r.tMax, t, u, v);
+}
+
+struct TraceHit { uint32_t prim; float t, u, v; };
+
+// Binary-node box test in the plain slab form (as the build's boxes were padded for).
+__device__ __forceinline__ void slab_interval(float lo, float hi, float o, float inv, float& t0, float& t1)
 {
     float a = (lo - o) * inv, b = (hi - o) * inv;
     if (a != a) a = -3e38f; // (0 * inf): origin on the slab plane, direction parallel
     if (b != b) b = 3e38f;
     t0 = fmaxf(t0, fminf(a, b));
     t1 = fminf(t1, fmaxf(a, b));
-    return true;
 }
 
 __device__ __forceinline__ bool box_hit(float4 lo, float4 hi, f3 o, f3 inv, float tmax, float& tEntry)
@@ -47,50 +127,49 @@ __device__ __forceinline__ bool box_hit(float4 lo, float4 hi, f3 o, f3 inv, floa
     return t0 <= t1 + 2e-6f * fabsf(t1);
 }
 
-__device__ __forceinline__ bool tri_test(const BvhView& bv, uint32_t prim, const Ray& r, float& t, float& u, float& v)
+// Closest hit on (tMin, tMax) over the binary tree; ties on t go to the lower scene triangle index;
+// prim is kInvalidIndex on a miss.  kCount adds the nodes visited and triangles tested to
+// counts[0..1].  *overflow is set when the stack would overflow (the subtree is skipped and the
+// caller reports a device fault).
+template <bool kCount>
+__device__ __forceinline__ TraceHit trace_closest_bin(const BvhView& bv, const Ray& r, uint32_t* overflow, uint32_t* counts = nullptr)
 {
-    float4 a = __ldg(&bv.tri[3 * prim + 0]);
-    float4 b = __ldg(&bv.tri[3 * prim + 1]);
-    float4 c = __ldg(&bv.tri[3 * prim + 2]);
-    return intersect_triangle(r.origin, r.dir, mk3(a.x, a.y, a.z), mk3(b.x, b.y, b.z), mk3(c.x, c.y, c.z), r.tMin, r.tMax, t, u, v);
-}
-
-// Closest hit on (tMin, tMax); ties on t go to the lower triangle index.
-// Returns false on a miss.  *overflow is set when the stack would overflow (the
-// remaining subtree is skipped, the caller reports a device fault).
-__device__ inline bool trace_closest(const BvhView& bv, const Ray& r, HitInfo& hit, float& tHit, uint32_t* overflow)
-{
-    if (bv.numTris == 0) return false;
-    f3 inv = mk3(1.f / r.dir.x, 1.f / r.dir.y, 1.f / r.dir.z);
-    float best = r.tMax;
-    uint32_t bestPrim = kInvalidIndex;
-    float bu = 0.f, bv_ = 0.f;
+    const f3 inv = mk3(1.f / r.dir.x, 1.f / r.dir.y, 1.f / r.dir.z);
+    TraceHit best;
+    best.prim = kInvalidIndex; best.t = r.tMax; best.u = 0.f; best.v = 0.f;
     uint32_t stack[kTraversalStack];
     int sp = 0;
-    uint32_t node = bv.root;
+    uint32_t node = bv.binRoot;
     while (true)
     {
         if (node & kLeafBit)
         {
-            uint32_t prim = node & ~kLeafBit;
+            const uint32_t k = node & ~kLeafBit;
+            const float4 a = __ldg(&bv.leafTri[3 * (size_t)k + 0]);
+            const float4 b = __ldg(&bv.leafTri[3 * (size_t)k + 1]);
+            const float4 c = __ldg(&bv.leafTri[3 * (size_t)k + 2]);
+            const uint32_t prim = __float_as_uint(a.w);
             float t, u, v;
-            if (tri_test(bv, prim, r, t, u, v) && (t < best || (t == best && prim < bestPrim)))
+            if (kCount) counts[1]++;
+            if (intersect_triangle_e(r.origin, r.dir, mk3(a.x, a.y, a.z), mk3(b.x, b.y, b.z), mk3(c.x, c.y, c.z), r.tMin, r.tMax, t, u, v) &&
+                (t < best.t || (t == best.t && prim < best.prim)))
             {
-                best = t; bestPrim = prim; bu = u; bv_ = v;
+                best.t = t; best.prim = prim; best.u = u; best.v = v;
             }
             if (sp == 0) break;
             node = stack[--sp];
             continue;
         }
-        const float4* n = bv.nodes + 4 * (size_t)node;
-        float4 l0 = __ldg(n + 0), l1 = __ldg(n + 1), r0 = __ldg(n + 2), r1 = __ldg(n + 3);
+        if (kCount) counts[0]++;
+        const float4* n = bv.binNodes + 4 * (size_t)node;
+        const float4 l0 = __ldg(n + 0), l1 = __ldg(n + 1), r0 = __ldg(n + 2), r1 = __ldg(n + 3);
         float tl, tr;
-        bool hl = box_hit(l0, l1, r.origin, inv, best, tl);
-        bool hr = box_hit(r0, r1, r.origin, inv, best, tr);
-        uint32_t cl = __float_as_uint(l0.w), cr = __float_as_uint(l1.w);
+        const bool hl = box_hit(l0, l1, r.origin, inv, best.t, tl);
+        const bool hr = box_hit(r0, r1, r.origin, inv, best.t, tr);
+        const uint32_t cl = __float_as_uint(l0.w), cr = __float_as_uint(l1.w);
         if (hl && hr)
         {
-            uint32_t nearC = tl <= tr ? cl : cr, farC = tl <= tr ? cr : cl;
+            const uint32_t nearC = tl <= tr ? cl : cr, farC = tl <= tr ? cr : cl;
             if (sp < kTraversalStack) stack[sp++] = farC;
             else *overflow = 1u;
             node = nearC;
@@ -103,51 +182,73 @@ __device__ inline bool trace_closest(const BvhView& bv, const Ray& r, HitInfo& h
             node = stack[--sp];
         }
     }
-    if (bestPrim == kInvalidIndex) return false;
-    hit = hit_tri(bestPrim, bu, bv_);
-    tHit = best;
-    return true;
+    return best;
 }
 
 // True when no triangle is hit on (tMin, tMax).
-__device__ inline bool trace_visible(const BvhView& bv, const Ray& r, uint32_t* overflow)
+static __device__ __noinline__ bool trace_visible_q(const float4* __restrict__ nodes, const float4* __restrict__ leafTri, RayQ r,
+                                                    uint32_t* overflow)
 {
-    if (bv.numTris == 0) return true;
-    f3 inv = mk3(1.f / r.dir.x, 1.f / r.dir.y, 1.f / r.dir.z);
     uint32_t stack[kTraversalStack];
     int sp = 0;
-    uint32_t node = bv.root;
+    uint32_t node = 0;
     while (true)
     {
-        if (node & kLeafBit)
+        const float4* n = nodes + 7 * (size_t)node;
+        const float4 nx = __ldg(n + r.nearX), fx = __ldg(n + r.farX), ny = __ldg(n + r.nearY), fy = __ldg(n + r.farY);
+        const float4 nz = __ldg(n + r.nearZ), fz = __ldg(n + r.farZ);
+        const uint4 rf = __ldg(reinterpret_cast<const uint4*>(n + 6));
+        const bool h[4] = {child_entry(nx.x, fx.x, ny.x, fy.x, nz.x, fz.x, r, r.tMax) != kMissKey,
+                           child_entry(nx.y, fx.y, ny.y, fy.y, nz.y, fz.y, r, r.tMax) != kMissKey,
+                           child_entry(nx.z, fx.z, ny.z, fy.z, nz.z, fz.z, r, r.tMax) != kMissKey,
+                           child_entry(nx.w, fx.w, ny.w, fy.w, nz.w, fz.w, r, r.tMax) != kMissKey};
+        const uint32_t c4[4] = {rf.x, rf.y, rf.z, rf.w};
+        uint32_t next = kInvalidIndex;
+#pragma unroll
+        for (int c = 0; c < 4; c++)
         {
-            float t, u, v;
-            if (tri_test(bv, node & ~kLeafBit, r, t, u, v)) return false;
-            if (sp == 0) break;
-            node = stack[--sp];
-            continue;
+            if (!h[c] || c4[c] == kInvalidIndex) continue;
+            if (c4[c] & kLeafBit)
+            {
+                const uint32_t first = (c4[c] & ~kLeafBit) >> 2, count = (c4[c] & 3u) + 1u;
+                for (uint32_t j = 0; j < count; j++)
+                {
+                    float t, u, v;
+                    uint32_t prim;
+                    if (leaf_tri_test(leafTri, first + j, r, t, u, v, prim)) return false;
+                }
+            }
+            else
+            {
+                if (next != kInvalidIndex)
+                {
+                    if (sp < kTraversalStack) stack[sp++] = next;
+                    else *overflow = 1u;
+                }
+                next = c4[c];
+            }
         }
-        const float4* n = bv.nodes + 4 * (size_t)node;
-        float4 l0 = __ldg(n + 0), l1 = __ldg(n + 1), r0 = __ldg(n + 2), r1 = __ldg(n + 3);
-        float tl, tr;
-        bool hl = box_hit(l0, l1, r.origin, inv, r.tMax, tl);
-        bool hr = box_hit(r0, r1, r.origin, inv, r.tMax, tr);
-        uint32_t cl = __float_as_uint(l0.w), cr = __float_as_uint(l1.w);
-        if (hl && hr)
-        {
-            if (sp < kTraversalStack) stack[sp++] = cr;
-            else *overflow = 1u;
-            node = cl;
-        }
-        else if (hl) node = cl;
-        else if (hr) node = cr;
-        else
-        {
-            if (sp == 0) break;
-            node = stack[--sp];
-        }
+        if (next != kInvalidIndex) { node = next; continue; }
+        if (sp == 0) break;
+        node = stack[--sp];
     }
     return true;
+}
+
+__device__ __forceinline__ bool trace_closest(const BvhView& bv, const Ray& r, HitInfo& hit, float& tHit, uint32_t* overflow)
+{
+    if (bv.numTris == 0) return false;
+    const TraceHit h = trace_closest_bin<false>(bv, r, overflow);
+    if (h.prim == kInvalidIndex) return false;
+    hit = hit_tri(h.prim, h.u, h.v);
+    tHit = h.t;
+    return true;
+}
+
+__device__ __forceinline__ bool trace_visible(const BvhView& bv, const Ray& r, uint32_t* overflow)
+{
+    if (bv.numTris == 0) return true;
+    return trace_visible_q(bv.nodes, bv.leafTri, make_rayq(r), overflow);
 }
 
 } // namespace rs

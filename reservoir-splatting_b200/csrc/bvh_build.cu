@@ -1,8 +1,14 @@
-// LBVH construction on the GPU (Karras 2012, "Maximizing parallelism in the
-// construction of BVHs, octrees, and k-d trees"): 63-bit Morton codes (21 bits per axis) of the
-// triangle centroids, a key/index sort, one thread per internal node to find its
-// range and split, and a bottom-up box pass with per-node arrival counters.
-// Built once per rs_set_scene; the per-frame path only traverses it.
+// BVH construction on the GPU, once per rs_set_scene.
+//
+// 1. LBVH (Karras 2012, "Maximizing parallelism in the construction of BVHs, octrees, and k-d
+//    trees"): 63-bit Morton codes (21 bits per axis) of the triangle centroids, a key/index radix
+//    sort, the triangles gathered in key order, one thread per internal node to find its range and
+//    split, and a bottom-up box pass with per-node arrival counters.
+// 2. Collapse of the binary tree (kept for closest-hit queries) into the 4-wide tree of bvh.cuh, top down, one thread per node
+//    and one launch per level: a node takes its binary node's two children and repeatedly opens
+//    the child of largest surface area that holds more than four triangles, up to four children;
+//    children of at most four triangles become leaves, which are ranges of the key-ordered
+//    triangles (the leaf-order array).
 #include <cub/device/device_radix_sort.cuh>
 #include "bvh_build.h"
 
@@ -87,8 +93,23 @@ __device__ __forceinline__ int delta(const uint64_t* keys, int n, int i, int j)
     return __clzll((long long)(a ^ b));
 }
 
-__global__ void k_karras(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ prim, int n,
-                         float4* __restrict__ nodes, uint32_t* __restrict__ parent, uint32_t* __restrict__ leafParent)
+// Triangles in key order; the third record keeps the scene index in w.
+__global__ void k_gather_sorted(const float4* __restrict__ tri, const uint32_t* __restrict__ order, uint32_t n, float4* __restrict__ sorted)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t t = order[i];
+    sorted[3 * (size_t)i + 0] = tri[3 * (size_t)t + 0];
+    sorted[3 * (size_t)i + 1] = tri[3 * (size_t)t + 1];
+    float4 c = tri[3 * (size_t)t + 2];
+    c.w = __uint_as_float(t);
+    sorted[3 * (size_t)i + 2] = c;
+}
+
+// Binary node i: children in nodes[4i].w / nodes[4i+1].w (kLeafBit | sorted position for a leaf),
+// its sorted range in range[i].
+__global__ void k_karras(const uint64_t* __restrict__ keys, int n, float4* __restrict__ nodes, uint2* __restrict__ range,
+                         uint32_t* __restrict__ parent, uint32_t* __restrict__ leafParent)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n - 1) return;
@@ -110,17 +131,18 @@ __global__ void k_karras(const uint64_t* __restrict__ keys, const uint32_t* __re
     }
     int gamma = i + s * d + (d < 0 ? -1 : 0);
     int lo = i < j ? i : j, hi = i < j ? j : i;
-    uint32_t left = (lo == gamma) ? (kLeafBit | prim[gamma]) : (uint32_t)gamma;
-    uint32_t right = (hi == gamma + 1) ? (kLeafBit | prim[gamma + 1]) : (uint32_t)(gamma + 1);
+    uint32_t left = (lo == gamma) ? (kLeafBit | (uint32_t)gamma) : (uint32_t)gamma;
+    uint32_t right = (hi == gamma + 1) ? (kLeafBit | (uint32_t)(gamma + 1)) : (uint32_t)(gamma + 1);
     nodes[4 * (size_t)i + 0].w = __uint_as_float(left);
     nodes[4 * (size_t)i + 1].w = __uint_as_float(right);
+    range[i] = make_uint2((uint32_t)lo, (uint32_t)hi);
     if (lo == gamma) leafParent[gamma] = (uint32_t)i; else parent[gamma] = (uint32_t)i;
     if (hi == gamma + 1) leafParent[gamma + 1] = (uint32_t)i; else parent[gamma + 1] = (uint32_t)i;
 }
 
 __device__ __forceinline__ void tri_box(const float4* tri, uint32_t p, float lo[3], float hi[3])
 {
-    float4 a = tri[3 * p], b = tri[3 * p + 1], c = tri[3 * p + 2];
+    float4 a = tri[3 * (size_t)p], b = tri[3 * (size_t)p + 1], c = tri[3 * (size_t)p + 2];
     lo[0] = fminf(a.x, fminf(b.x, c.x)); hi[0] = fmaxf(a.x, fmaxf(b.x, c.x));
     lo[1] = fminf(a.y, fminf(b.y, c.y)); hi[1] = fmaxf(a.y, fmaxf(b.y, c.y));
     lo[2] = fminf(a.z, fminf(b.z, c.z)); hi[2] = fmaxf(a.z, fmaxf(b.z, c.z));
@@ -167,21 +189,158 @@ __global__ void k_refit(const float4* __restrict__ tri, int n, float4* nodes, co
     }
 }
 
-cudaError_t build_lbvh(const float4* dTri, uint32_t n, float4* dNodes, uint32_t* rootOut, cudaStream_t s)
+// ------------------------------------------------------------------ collapse to the 4-wide tree
+struct WideChild
 {
-    if (n == 0) { *rootOut = 0; return cudaSuccess; }
-    if (n == 1) { *rootOut = kLeafBit | 0u; return cudaSuccess; }
+    uint32_t ref;          // binary reference (kLeafBit | sorted position, or internal node)
+    uint32_t first, count; // sorted triangle range
+    float lo[3], hi[3];
+};
+
+__device__ __forceinline__ float box_area(const WideChild& c)
+{
+    float dx = c.hi[0] - c.lo[0], dy = c.hi[1] - c.lo[1], dz = c.hi[2] - c.lo[2];
+    return dx * dy + dy * dz + dz * dx;
+}
+
+__device__ __forceinline__ WideChild binary_child(const float4* nodes, const uint2* range, uint32_t b, int side)
+{
+    WideChild c;
+    const float4* n = nodes + 4 * (size_t)b;
+    float4 lo = n[2 * side], hi = n[2 * side + 1];
+    c.ref = __float_as_uint(n[side].w);
+    c.lo[0] = lo.x; c.lo[1] = lo.y; c.lo[2] = lo.z;
+    c.hi[0] = hi.x; c.hi[1] = hi.y; c.hi[2] = hi.z;
+    if (c.ref & kLeafBit) { c.first = c.ref & ~kLeafBit; c.count = 1; }
+    else { uint2 r = range[c.ref]; c.first = r.x; c.count = r.y - r.x + 1; }
+    return c;
+}
+
+constexpr uint32_t kWideLeafMax = 1; // triangles per leaf
+
+__device__ __forceinline__ bool is_wide_leaf(const WideChild& c) { return (c.ref & kLeafBit) || c.count <= kWideLeafMax; }
+
+// Writes node w for children c[0..n): internal children get consecutive node indices from
+// childBase (returned through childOf), leaves reference their sorted range.
+__device__ void write_wide_node(float4* wnodes, uint32_t w, const WideChild* c, int n, uint32_t childBase, uint32_t* childOf)
+{
+    float lo[3][4], hi[3][4];
+    uint32_t ref[4];
+    uint32_t nInternal = 0;
+    for (int j = 0; j < 4; j++)
+    {
+        childOf[j] = kInvalidIndex;
+        if (j >= n)
+        {
+            for (int a = 0; a < 3; a++) { lo[a][j] = __int_as_float(0x7f800000); hi[a][j] = __int_as_float(0xff800000); }
+            ref[j] = kInvalidIndex;
+            continue;
+        }
+        for (int a = 0; a < 3; a++) { lo[a][j] = c[j].lo[a]; hi[a][j] = c[j].hi[a]; }
+        if (is_wide_leaf(c[j])) ref[j] = kLeafBit | (c[j].first << 2) | (c[j].count - 1u);
+        else
+        {
+            ref[j] = childBase + nInternal;
+            childOf[j] = childBase + nInternal;
+            nInternal++;
+        }
+    }
+    float4* o = wnodes + 7 * (size_t)w;
+    o[0] = make_float4(lo[0][0], lo[0][1], lo[0][2], lo[0][3]);
+    o[1] = make_float4(hi[0][0], hi[0][1], hi[0][2], hi[0][3]);
+    o[2] = make_float4(lo[1][0], lo[1][1], lo[1][2], lo[1][3]);
+    o[3] = make_float4(hi[1][0], hi[1][1], hi[1][2], hi[1][3]);
+    o[4] = make_float4(lo[2][0], lo[2][1], lo[2][2], lo[2][3]);
+    o[5] = make_float4(hi[2][0], hi[2][1], hi[2][2], hi[2][3]);
+    o[6] = make_float4(__uint_as_float(ref[0]), __uint_as_float(ref[1]), __uint_as_float(ref[2]), __uint_as_float(ref[3]));
+}
+
+// counters: [0] nodes allocated, [1] unused, [2] next-level items, [3] unused
+__global__ void k_collapse(const float4* __restrict__ nodes, const uint2* __restrict__ range, const uint2* __restrict__ qin, uint32_t nin,
+                           uint2* __restrict__ qout, uint32_t* __restrict__ counters, float4* __restrict__ wnodes)
+{
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nin) return;
+    const uint2 item = qin[t]; // (binary internal node, wide node)
+    WideChild c[4];
+    int n = 2;
+    c[0] = binary_child(nodes, range, item.x, 0);
+    c[1] = binary_child(nodes, range, item.x, 1);
+    while (n < 4)
+    {
+        int open = -1;
+        float best = -1.f;
+        for (int j = 0; j < n; j++)
+            if (!is_wide_leaf(c[j]) && box_area(c[j]) > best) { best = box_area(c[j]); open = j; }
+        if (open < 0) break;
+        const uint32_t b = c[open].ref;
+        c[open] = binary_child(nodes, range, b, 0);
+        c[n++] = binary_child(nodes, range, b, 1);
+    }
+    uint32_t nInternal = 0;
+    for (int j = 0; j < n; j++)
+        if (!is_wide_leaf(c[j])) nInternal++;
+    const uint32_t childBase = nInternal ? atomicAdd(&counters[0], nInternal) : 0u;
+    uint32_t childOf[4];
+    write_wide_node(wnodes, item.y, c, n, childBase, childOf);
+    for (int j = 0; j < n; j++)
+        if (childOf[j] != kInvalidIndex) qout[atomicAdd(&counters[2], 1u)] = make_uint2(c[j].ref, childOf[j]);
+}
+
+// A scene of one triangle: one node with one leaf.
+__global__ void k_single_leaf(const float4* __restrict__ sorted, float4* __restrict__ wnodes)
+{
+    WideChild c;
+    c.ref = kLeafBit;
+    c.first = 0;
+    c.count = 1;
+    tri_box(sorted, 0, c.lo, c.hi);
+    uint32_t childOf[4];
+    write_wide_node(wnodes, 0, &c, 1, 0, childOf);
+}
+
+// Leaf-order triangles in the traversal form (p0, scene index), (p1 - p0), (p2 - p0).
+__global__ void k_leaf_tris(const float4* __restrict__ sorted, uint32_t n, float4* __restrict__ leafTri)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 a = sorted[3 * (size_t)i], b = sorted[3 * (size_t)i + 1], c = sorted[3 * (size_t)i + 2];
+    leafTri[3 * (size_t)i + 0] = make_float4(a.x, a.y, a.z, c.w);
+    leafTri[3 * (size_t)i + 1] = make_float4(b.x - a.x, b.y - a.y, b.z - a.z, 0.f);
+    leafTri[3 * (size_t)i + 2] = make_float4(c.x - a.x, c.y - a.y, c.z - a.z, 0.f);
+}
+
+void free_wide_bvh(WideBvh* b)
+{
+    if (b->binNodes) cudaFree(b->binNodes);
+    if (b->nodes) cudaFree(b->nodes);
+    if (b->leafTri) cudaFree(b->leafTri);
+    *b = WideBvh();
+}
+
+cudaError_t build_wide_bvh(const float4* dTri, uint32_t n, WideBvh* out, cudaStream_t s)
+{
+    free_wide_bvh(out);
+    if (n == 0) return cudaSuccess;
+    if (n >= kMaxBvhTriangles) return cudaErrorInvalidValue;
     cudaError_t e;
     uint64_t *keys = nullptr, *keys2 = nullptr;
     uint32_t *vals = nullptr, *vals2 = nullptr, *bounds = nullptr;
-    uint32_t *parent = nullptr, *leafParent = nullptr, *arrivals = nullptr;
+    uint32_t *parent = nullptr, *leafParent = nullptr, *arrivals = nullptr, *counters = nullptr;
+    float4 *sorted = nullptr, *nodes = nullptr;
+    uint2 *range = nullptr, *qa = nullptr, *qb = nullptr;
     void* temp = nullptr;
     size_t tempBytes = 0;
+    const uint32_t maxWide = n / kWideLeafMax + 2; // every node but the root holds more than kWideLeafMax triangles
 #define RS_TRY(x) do { e = (x); if (e != cudaSuccess) goto done; } while (0)
+    RS_TRY(cudaMalloc(&out->nodes, 112ull * maxWide));
+    RS_TRY(cudaMalloc(&out->leafTri, 48ull * n));
     RS_TRY(cudaMalloc(&keys, n * 8ull)); RS_TRY(cudaMalloc(&vals, n * 4ull));
     RS_TRY(cudaMalloc(&keys2, n * 8ull)); RS_TRY(cudaMalloc(&vals2, n * 4ull));
     RS_TRY(cudaMalloc(&bounds, 6 * 4ull));
-    RS_TRY(cudaMalloc(&parent, n * 4ull)); RS_TRY(cudaMalloc(&leafParent, n * 4ull)); RS_TRY(cudaMalloc(&arrivals, n * 4ull));
+    RS_TRY(cudaMalloc(&sorted, 48ull * n));
+    RS_TRY(cudaMalloc(&counters, 4 * 4ull));
+    RS_TRY(cudaMemsetAsync(counters, 0, 16, s));
     {
         uint32_t init[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
         RS_TRY(cudaMemcpyAsync(bounds, init, sizeof(init), cudaMemcpyHostToDevice, s));
@@ -190,18 +349,58 @@ cudaError_t build_lbvh(const float4* dTri, uint32_t n, float4* dNodes, uint32_t*
         RS_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tempBytes, keys, keys2, vals, vals2, (int)n, 0, 63, s));
         RS_TRY(cudaMalloc(&temp, tempBytes));
         RS_TRY(cub::DeviceRadixSort::SortPairs(temp, tempBytes, keys, keys2, vals, vals2, (int)n, 0, 63, s));
-        RS_TRY(cudaMemsetAsync(dNodes, 0, 64ull * (n - 1), s));
-        k_karras<<<(n - 1 + 255) / 256, 256, 0, s>>>(keys2, vals2, (int)n, dNodes, parent, leafParent);
-        RS_TRY(cudaMemsetAsync(arrivals, 0, n * 4ull, s));
-        k_refit<<<(n + 255) / 256, 256, 0, s>>>(dTri, (int)n, dNodes, parent, leafParent, arrivals);
+        k_gather_sorted<<<(n + 255) / 256, 256, 0, s>>>(dTri, vals2, n, sorted);
+        uint32_t levels = 0, numWide = 1;
+        if (n == 1)
+        {
+            k_single_leaf<<<1, 1, 0, s>>>(sorted, out->nodes);
+            levels = 1;
+        }
+        else
+        {
+            RS_TRY(cudaMalloc(&nodes, 64ull * (n - 1)));
+            RS_TRY(cudaMalloc(&range, 8ull * (n - 1)));
+            RS_TRY(cudaMalloc(&parent, n * 4ull)); RS_TRY(cudaMalloc(&leafParent, n * 4ull)); RS_TRY(cudaMalloc(&arrivals, n * 4ull));
+            RS_TRY(cudaMalloc(&qa, 8ull * maxWide)); RS_TRY(cudaMalloc(&qb, 8ull * maxWide));
+            RS_TRY(cudaMemsetAsync(nodes, 0, 64ull * (n - 1), s));
+            k_karras<<<(n - 1 + 255) / 256, 256, 0, s>>>(keys2, (int)n, nodes, range, parent, leafParent);
+            RS_TRY(cudaMemsetAsync(arrivals, 0, n * 4ull, s));
+            k_refit<<<(n + 255) / 256, 256, 0, s>>>(sorted, (int)n, nodes, parent, leafParent, arrivals);
+            const uint2 root = make_uint2(0u, 0u);
+            const uint32_t one = 1u;
+            RS_TRY(cudaMemcpyAsync(qa, &root, sizeof(root), cudaMemcpyHostToDevice, s));
+            RS_TRY(cudaMemcpyAsync(counters, &one, 4, cudaMemcpyHostToDevice, s)); // node 0 is the root
+            uint32_t nin = 1;
+            while (nin > 0)
+            {
+                RS_TRY(cudaMemsetAsync(counters + 2, 0, 4, s));
+                k_collapse<<<(nin + 127) / 128, 128, 0, s>>>(nodes, range, qa, nin, qb, counters, out->nodes);
+                RS_TRY(cudaGetLastError());
+                RS_TRY(cudaMemcpyAsync(&nin, counters + 2, 4, cudaMemcpyDeviceToHost, s));
+                RS_TRY(cudaStreamSynchronize(s));
+                std::swap(qa, qb);
+                levels++;
+            }
+        }
+        k_leaf_tris<<<(n + 255) / 256, 256, 0, s>>>(sorted, n, out->leafTri);
+        uint32_t host[4];
+        RS_TRY(cudaMemcpyAsync(host, counters, 16, cudaMemcpyDeviceToHost, s));
         RS_TRY(cudaGetLastError());
         RS_TRY(cudaStreamSynchronize(s));
-        *rootOut = 0;
+        numWide = n == 1 ? 1u : host[0];
+        if (numWide > maxWide) { e = cudaErrorUnknown; goto done; }
+        out->numNodes = numWide;
+        out->depth = levels;
+        out->binNodes = nodes; // the binary tree stays for closest-hit queries
+        out->binRoot = n == 1 ? kLeafBit : 0u;
+        nodes = nullptr;
     }
 done:
 #undef RS_TRY
-    cudaFree(keys); cudaFree(vals); cudaFree(keys2); cudaFree(vals2); cudaFree(bounds);
-    cudaFree(parent); cudaFree(leafParent); cudaFree(arrivals); cudaFree(temp);
+    cudaFree(keys); cudaFree(vals); cudaFree(keys2); cudaFree(vals2); cudaFree(bounds); cudaFree(sorted); cudaFree(counters);
+    cudaFree(nodes); cudaFree(range); cudaFree(parent); cudaFree(leafParent); cudaFree(arrivals); cudaFree(qa); cudaFree(qb);
+    cudaFree(temp);
+    if (e != cudaSuccess) free_wide_bvh(out);
     return e;
 }
 

@@ -1,10 +1,30 @@
-// GPU LBVH build entry point (see bvh_build.cu).
+// GPU BVH build entry point (see bvh_build.cu).
 #pragma once
 #include <cuda_runtime.h>
 #include "bvh.cuh"
 
 namespace rs {
-// dNodes must hold 4 float4 per internal node (n - 1 nodes).  *rootOut receives the
-// root child index (0, or a leaf when n == 1).  Synchronises `s` before returning.
-cudaError_t build_lbvh(const float4* dTri, uint32_t n, float4* dNodes, uint32_t* rootOut, cudaStream_t s);
+
+// The two trees of bvh.cuh and their leaf-order triangle array (device memory owned by the caller
+// after a successful build; release with free_wide_bvh).
+struct WideBvh
+{
+    float4* binNodes = nullptr; // binary tree (closest hit)
+    uint32_t binRoot = 0;
+    float4* nodes = nullptr;    // 4-wide tree (visibility)
+    float4* leafTri = nullptr;
+    uint32_t numNodes = 0;
+    uint32_t depth = 0; // levels of nodes
+};
+
+// Builds the tree over n triangles (dTri: three float4 per triangle, geom.h layout); replaces
+// *out.  Synchronises `s`.  n must be below kMaxBvhTriangles.
+cudaError_t build_wide_bvh(const float4* dTri, uint32_t n, WideBvh* out, cudaStream_t s);
+void free_wide_bvh(WideBvh* b);
+
+// Diagnostics (bvh_debug.cu): rays are 8 floats (origin, direction, tMin, tMax); counts get the
+// nodes visited and triangles tested per ray.
+__global__ void k_debug_trace(BvhView bv, const float* rays, uint32_t n, int32_t* prim, float* tuv, uint32_t* counts, uint32_t* overflow);
+void wide_bvh_shape(const WideBvh& b, double* out);
+
 }

@@ -62,10 +62,9 @@ struct TriangleView
 
 // Moller-Trumbore, no culling.  Returns true and (t, u, v) when
 // tMin < t < tMax and the barycentrics lie in the triangle.
-RS_HD bool intersect_triangle(f3 o, f3 d, f3 p0, f3 p1, f3 p2, float tMin, float tMax, float& t, float& u, float& v)
+// The test with the edges e1 = p1 - p0, e2 = p2 - p0 already formed (same result bit for bit).
+RS_HD bool intersect_triangle_e(f3 o, f3 d, f3 p0, f3 e1, f3 e2, float tMin, float tMax, float& t, float& u, float& v)
 {
-    f3 e1 = p1 - p0;
-    f3 e2 = p2 - p0;
     f3 pv = cross(d, e2);
     float det = dot(e1, pv);
     if (det == 0.f) return false;
@@ -78,6 +77,10 @@ RS_HD bool intersect_triangle(f3 o, f3 d, f3 p0, f3 p1, f3 p2, float tMin, float
     if (!(v >= 0.f && u + v <= 1.f)) return false;
     t = dot(e2, qv) * inv;
     return t > tMin && t < tMax;
+}
+RS_HD bool intersect_triangle(f3 o, f3 d, f3 p0, f3 p1, f3 p2, float tMin, float tMax, float& t, float& u, float& v)
+{
+    return intersect_triangle_e(o, d, p0, p1 - p0, p2 - p0, tMin, tMax, t, u, v);
 }
 
 // GeometryHelpers.slang:54-68 (integer ulp offset away from the surface).

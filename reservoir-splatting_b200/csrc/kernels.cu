@@ -301,7 +301,7 @@ __device__ void handle_hit(const DevCtx& C, PState& path)
 }
 
 // InitialCandidates.cs.slang:80-141 + addCandidateReservoir (:52-75)
-__global__ void __launch_bounds__(128) k_candidates(uint32_t slot, ResPlanes curr, RecPlanes currRec)
+__global__ void __launch_bounds__(128, 3) k_candidates(uint32_t slot, ResPlanes curr, RecPlanes currRec)
 {
     const DevCtx& C = c_ctx[slot];
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;

@@ -99,11 +99,11 @@ struct rs_pass
     rs_options opt;
     // scene
     PreparedScene scene;
-    DevBuf<float4> dTri, dNodes;
+    DevBuf<float4> dTri;
+    WideBvh bvh;
     DevBuf<MaterialData> dMaterials;
     DevBuf<LightTriangle> dLights;
     DevBuf<u2> dAlias;
-    uint32_t bvhRoot = 0;
     bool hasScene = false;
     // frame state
     uint32_t W = 0, H = 0;
@@ -159,6 +159,7 @@ struct rs_pass
         if (hostCtx) cudaFreeHost(hostCtx);
         if (ringCtx) cudaFreeHost(ringCtx);
         if (graphCtx) cudaFreeHost(graphCtx);
+        free_wide_bvh(&bvh);
         release_slot(slot);
     }
 };
@@ -327,7 +328,7 @@ extern "C" RS_API rs_status rs_set_scene(rs_pass* p, const rs_scene_desc* sd)
     if (!p || !sd) return fail(RS_INVALID_ARG, "pass or scene is NULL");
     if (sd->numTriangles > 0 && (!sd->positions || !sd->materialIds)) return fail(RS_INVALID_ARG, "scene arrays are NULL");
     if (sd->numMaterials == 0 || !sd->materials) return fail(RS_INVALID_ARG, "scene has no materials");
-    if (sd->numTriangles >= kLeafBit) return fail(RS_INVALID_ARG, "too many triangles");
+    if (sd->numTriangles >= kMaxBvhTriangles) return fail(RS_INVALID_ARG, "too many triangles (limit 2^29)");
     static_assert(sizeof(rs_material) == sizeof(MaterialData), "material layout");
     if (!prepare_scene(sd->numTriangles, sd->positions, sd->materialIds, sd->numMaterials,
                        reinterpret_cast<const MaterialData*>(sd->materials), p->scene))
@@ -338,7 +339,6 @@ extern "C" RS_API rs_status rs_set_scene(rs_pass* p, const rs_scene_desc* sd)
     RS_CUDA(p->dMaterials.ensure(sd->numMaterials));
     RS_CUDA(p->dLights.ensure(p->scene.lights.size() ? p->scene.lights.size() : 1));
     RS_CUDA(p->dAlias.ensure(p->scene.alias.size() ? p->scene.alias.size() : 1));
-    RS_CUDA(p->dNodes.ensure(4ull * (n > 1 ? n - 1 : 1)));
     if (n) RS_CUDA(cudaMemcpy(p->dTri.p, p->scene.tri.data(), 48ull * n, cudaMemcpyHostToDevice));
     RS_CUDA(cudaMemcpy(p->dMaterials.p, p->scene.materials.data(), sizeof(MaterialData) * sd->numMaterials, cudaMemcpyHostToDevice));
     if (!p->scene.lights.empty())
@@ -348,9 +348,9 @@ extern "C" RS_API rs_status rs_set_scene(rs_pass* p, const rs_scene_desc* sd)
     }
     cudaStream_t s;
     RS_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-    cudaError_t e = build_lbvh(p->dTri.p, n, p->dNodes.p, &p->bvhRoot, s);
+    cudaError_t e = build_wide_bvh(p->dTri.p, n, &p->bvh, s);
     cudaStreamDestroy(s);
-    if (e != cudaSuccess) return fail(RS_CUDA_ERROR, std::string("LBVH build: ") + cudaGetErrorString(e));
+    if (e != cudaSuccess) return fail(RS_CUDA_ERROR, std::string("BVH build: ") + cudaGetErrorString(e));
     p->hasScene = true;
     p->frameCount = 0; // setScene resets the frame count (ReservoirSplatting.cpp:380)
     return RS_OK;
@@ -407,9 +407,11 @@ static void begin_frame(rs_pass* p, const rs_frame_desc* f)
 
     DevCtx& C = *p->hostCtx;
     memset(&C, 0, sizeof(C));
-    C.bvh.nodes = p->dNodes.p;
+    C.bvh.binNodes = p->bvh.binNodes;
+    C.bvh.binRoot = p->bvh.binRoot;
+    C.bvh.nodes = p->bvh.nodes;
+    C.bvh.leafTri = p->bvh.leafTri;
     C.bvh.tri = p->dTri.p;
-    C.bvh.root = p->bvhRoot;
     C.bvh.numTris = (uint32_t)(p->scene.tri.size() / 3);
     C.materials = p->dMaterials.p;
     C.lights.tris = p->dLights.p;
@@ -974,6 +976,45 @@ extern "C" RS_API rs_status rs_backward_stats(rs_pass* p, uint64_t* out)
     RS_CUDA(cudaMemcpy(h, p->adjStats.p, sizeof(h), cudaMemcpyDeviceToHost));
     RS_CUDA(cudaMemset(p->adjStats.p, 0, sizeof(h)));
     for (int i = 0; i < 4; i++) out[i] = h[i];
+    return RS_OK;
+}
+
+// ------------------------------------------------------------------ ray-query diagnostics
+// Closest hits of n host rays (8 floats each: origin, direction, tMin, tMax) against the pass's
+// tree: prim (-1 on a miss), t/u/v, and per ray the nodes visited and triangles tested.
+extern "C" RS_API rs_status rs_debug_trace_rays(rs_pass* p, const float* rays, uint32_t n, int32_t* prim, float* tuv, uint32_t* counts)
+{
+    if (!p || !rays || !prim || !tuv || !counts) return fail(RS_INVALID_ARG, "NULL argument");
+    if (!p->hasScene) return fail(RS_NOT_READY, "no scene");
+    if (n == 0) return RS_OK;
+    DevBuf<float> dr;
+    DevBuf<int32_t> dp;
+    DevBuf<float> dt;
+    DevBuf<uint32_t> dc, dof;
+    RS_CUDA(dr.ensure(8ull * n)); RS_CUDA(dp.ensure(n)); RS_CUDA(dt.ensure(3ull * n)); RS_CUDA(dc.ensure(2ull * n)); RS_CUDA(dof.ensure(1));
+    RS_CUDA(cudaMemcpy(dr.p, rays, 32ull * n, cudaMemcpyHostToDevice));
+    RS_CUDA(cudaMemset(dof.p, 0, 4));
+    BvhView bv;
+    bv.binNodes = p->bvh.binNodes; bv.binRoot = p->bvh.binRoot; bv.nodes = p->bvh.nodes; bv.leafTri = p->bvh.leafTri;
+    bv.tri = p->dTri.p; bv.numTris = (uint32_t)(p->scene.tri.size() / 3);
+    k_debug_trace<<<(n + 127) / 128, 128>>>(bv, dr.p, n, dp.p, dt.p, dc.p, dof.p);
+    RS_CUDA(cudaGetLastError());
+    RS_CUDA(cudaDeviceSynchronize());
+    uint32_t of = 0;
+    RS_CUDA(cudaMemcpy(&of, dof.p, 4, cudaMemcpyDeviceToHost));
+    if (of) return fail(RS_DEVICE_FAULT, "traversal stack overflow");
+    RS_CUDA(cudaMemcpy(prim, dp.p, 4ull * n, cudaMemcpyDeviceToHost));
+    RS_CUDA(cudaMemcpy(tuv, dt.p, 12ull * n, cudaMemcpyDeviceToHost));
+    RS_CUDA(cudaMemcpy(counts, dc.p, 8ull * n, cudaMemcpyDeviceToHost));
+    return RS_OK;
+}
+
+// Shape of the pass's tree: {nodes, depth, internal children, leaf children, leaf triangles,
+// surface-area cost per root-box ray (node visits + triangle tests)}.
+extern "C" RS_API rs_status rs_debug_bvh_shape(rs_pass* p, double* out6)
+{
+    if (!p || !out6) return fail(RS_INVALID_ARG, "NULL argument");
+    wide_bvh_shape(p->bvh, out6);
     return RS_OK;
 }
 
