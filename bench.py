@@ -248,6 +248,11 @@ def run_ours(args):
     e2e_ms = max_over_ranks(e0.elapsed_time(e1), dist, dev)
     e2e_value = world * e2e_steps / (e2e_ms / 1e3)
 
+    quality = None
+    if rank == 0 and not args.no_quality:
+        with torch.cuda.stream(stream):
+            quality = measure_quality(args, torch, rs, scene, camera(frame - 1 + rank_frame_offset(rank), W, H), host_np, W, H, stream)
+
     peak, peak_kind = _peaks()
     traffic = measured_traffic()
     dom = max(stage_ms, key=stage_ms.get) if stage_ms else "initialCandidates"
@@ -273,6 +278,8 @@ def run_ours(args):
             "roofline": roofline,
             "clocks": clocks,
         }
+        if quality is not None:
+            line["quality"] = quality
         if world == 1 and not args.no_batched:
             line["batched"] = run_batched(args, torch, rs, stream, dev)
         if world == 1 and not args.no_adjoint:
@@ -282,6 +289,39 @@ def run_ours(args):
         print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
+
+
+def measure_quality(args, torch, rs, scene, cam, image, W, H, stream):
+    """Error of the last rendered frame against an FP64 ground truth of the same camera.
+
+    The ground truth accumulates, in FP64 on the device, `gt_spp` frames of the pass with temporal
+    and spatial reuse off: each such frame is the initial-candidate estimate alone, an unbiased
+    one-path-per-pixel estimate, with its own seed.  Its first frame is also reported as the
+    one-path path-tracing baseline.  The ground truth's own noise (variance of the mean) is about
+    mse_1spp / gt_spp and is reported beside the numbers."""
+    props = dict(PROPS, enableTemporalResampling=False, enableSpatialResampling=False)
+    gt_pass = rs.ReservoirSplatting(props, W, H)
+    gt_pass.set_scene(scene)
+    col = torch.empty((H, W, 4), dtype=torch.float32, device="cuda")
+    acc = torch.zeros((H, W, 3), dtype=torch.float64, device="cuda")
+    one = None
+    for k in range(args.gt_spp):
+        gt_pass.execute(cam, color_ptr=col.data_ptr(), stream=stream.cuda_stream)
+        acc += col[..., :3].double()
+        if k == 0:
+            one = col[..., :3].double().clone()
+    torch.cuda.synchronize()
+    gt = acc / args.gt_spp
+    img = torch.from_numpy(image[..., :3]).cuda().double()
+    mse = float(((img - gt) ** 2).mean())
+    mse1 = float(((one - gt) ** 2).mean())
+    rel = lambda a: float((((a - gt) ** 2) / (gt ** 2 + 1e-2)).mean())
+    gt_pass.close()
+    return {"mse_vs_fp64_gt": mse, "relmse_vs_fp64_gt": rel(img), "mse_1spp_path_tracing": mse1, "relmse_1spp_path_tracing": rel(one),
+            "mse_ratio_1spp_over_restir": round(mse1 / mse, 3) if mse > 0 else None, "gt_spp": args.gt_spp,
+            "gt_noise_mse_estimate": mse1 / args.gt_spp, "gt_mean_radiance": float(gt.mean()),
+            "how": "last timed-configuration frame vs the FP64 mean of gt_spp independent candidate-only frames at the same camera "
+                   "(batched and plain passes run the same kernels per instance and give bit-identical images)"}
 
 
 BATCH_RESOLUTIONS = [(320, 240), (640, 480), (1280, 720), (1920, 1080)]
@@ -474,6 +514,8 @@ def main():
     ap.add_argument("--batch-frames", type=int, default=4)
     ap.add_argument("--batch-warmup", type=int, default=2)
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-quality", action="store_true")
+    ap.add_argument("--gt-spp", type=int, default=512)
     ap.add_argument("--adjoint-reps", type=int, default=3)
     args = ap.parse_args()
     if args.impl == "reference":
