@@ -198,6 +198,15 @@ RS_API rs_status rs_batch_execute(rs_batch* batch, const rs_frame_desc* frames, 
 RS_API rs_status rs_batch_destroy(rs_batch* batch);
 RS_API uint32_t rs_batch_launch_count(rs_batch* batch);
 
+/* Moving geometry (Falcor's animated-scene update, done by the caller).  rs_update_geometry moves
+ * every triangle to `positions` (9 floats per triangle, the scene's count; host memory, or device
+ * memory of the current device when onDevice != 0) for the next rs_execute: the previous positions
+ * give that frame's motion vectors (Scene::getPrevPosW, VBufferRT.slang:84), both BVHs are refitted
+ * in place (the topology of rs_set_scene stays; rebuild with rs_set_scene after large changes) and
+ * light records follow their triangles, with the power sampler's weights of the last
+ * rs_set_scene / rs_set_materials.  Call it at most once per frame; stream-ordered on cudaStream. */
+RS_API rs_status rs_update_geometry(rs_pass* pass, const float* positions, uint32_t numTriangles, uint32_t onDevice, void* cudaStream);
+
 /* Ray-query diagnostics (no reference counterpart).  rs_debug_trace_rays: closest hits of n host
  * rays (8 floats each: origin.xyz, direction.xyz, tMin, tMax) against the pass's BVH: prim[n] (-1 on
  * a miss), tuv[3n], counts[2n] = nodes visited and triangles tested.  rs_debug_bvh_shape: {nodes,

@@ -71,6 +71,7 @@ def load():
     lib.ro_frame_count.argtypes = [C.c_void_p]
     lib.ro_frame_count.restype = C.c_uint32
     lib.ro_set_materials.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32]
+    lib.ro_update_geometry.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32]
     lib.ro_backward.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     lib.ro_replay_loss.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32]
     lib.ro_replay_loss.restype = C.c_double
@@ -144,6 +145,13 @@ class OraclePass:
         st = self._lib.ro_set_buffer(self._h, self._abi.BUF[name], data.ctypes.data, data.nbytes)
         if st != 0:
             raise RuntimeError(f"oracle set_buffer failed: {st}")
+
+    def update_geometry(self, positions: np.ndarray):
+        """Moves the triangles (n x 9 float32) for the next frame."""
+        q = np.ascontiguousarray(positions, np.float32).reshape(-1, 9)
+        st = self._lib.ro_update_geometry(self._h, q.ctypes.data, len(q))
+        if st != 0:
+            raise RuntimeError(f"oracle update_geometry failed: {st}")
 
     # ---- path-replay adjoint (checker of rs_backward)
     def set_materials(self, materials: np.ndarray):

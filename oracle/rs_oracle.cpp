@@ -378,6 +378,8 @@ struct Pass
     std::vector<std::vector<uint32_t>> mCellCounters, mCellOffsets, mSorted;
     std::vector<ShiftedPathData> shiftedPaths;
     std::vector<f2> neighborOffsets;  // RG8Snorm decoded
+    std::vector<f4> prevTri;          // the previous frame's triangles, after a geometry update
+    bool geometryMoved = false;       // positions changed since the last frame
 
     // ---- options
     uint32_t maxSurface() const { return opt.maxSurfaceBounces; }
@@ -1074,7 +1076,8 @@ struct Pass
                 if (bvh.closest(mk_ray(camera.posW, dir, 0.f, kRayTMax), h, t))
                 {
                     vbuffer[idx] = h;
-                    f3 prevPosW = loadSD(h, dir).posW;
+                    // Scene::getPrevPosW (VBufferRT.slang:84): the hit on the previous frame's geometry
+                    f3 prevPosW = hit_position(geometryMoved ? prevTri.data() : scene.tri.data(), h);
                     f3 d = prevPosW - pc.posW;
                     f3 camRay = mk3(dot(normalize(pc.cameraU), d), dot(normalize(pc.cameraV), d), dot(normalize(pc.cameraW), d));
                     float lw = length(pc.cameraW);
@@ -1901,6 +1904,7 @@ struct Pass
         }
         prevFrameCamera = camera;
         havePrevFrameCamera = true;
+        geometryMoved = false;
         return RS_OK;
     }
 };
@@ -2320,6 +2324,31 @@ __attribute__((visibility("default"))) int ro_set_buffer(ro_pass* r, int id, con
 }
 
 __attribute__((visibility("default"))) uint32_t ro_frame_count(ro_pass* r) { return r->p.frameCount; }
+
+// Moves the scene's triangles (same count; materials stay) for the next frame: the previous
+// positions are kept for that frame's motion vectors, the BVH is rebuilt and the light records
+// take their triangles' new vertices (their flux, and the power sampler, stay).
+__attribute__((visibility("default"))) int ro_update_geometry(ro_pass* r, const float* positions, uint32_t numTriangles)
+{
+    oracle::Pass& p = r->p;
+    if (!p.hasScene || numTriangles != r->materialIds.size()) return RS_INVALID_ARG;
+    p.prevTri = p.scene.tri;
+    for (size_t t = 0; t < numTriangles; t++)
+        for (int v = 0; v < 3; v++)
+        {
+            f4& q = p.scene.tri[3 * t + v];
+            q.x = positions[9 * t + 3 * v + 0]; q.y = positions[9 * t + 3 * v + 1]; q.z = positions[9 * t + 3 * v + 2];
+        }
+    r->positions.assign(positions, positions + 9 * (size_t)numTriangles);
+    for (LightTriangle& L : p.scene.lights)
+    {
+        const f4* q = &p.scene.tri[3 * (size_t)L.sceneTri];
+        light_set_vertices(L, f4xyz(q[0]), f4xyz(q[1]), f4xyz(q[2]));
+    }
+    p.bvh.build(p.scene.tri, numTriangles);
+    p.geometryMoved = true;
+    return RS_OK;
+}
 
 // Replaces the material parameters (same count) and rebuilds the light collection; the geometry
 // and its BVH stay.

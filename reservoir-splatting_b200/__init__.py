@@ -66,6 +66,7 @@ def load_library():
     lib.rs_checkpoint.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
     lib.rs_backward.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     lib.rs_backward_stats.argtypes = [C.c_void_p, C.c_void_p]
+    lib.rs_update_geometry.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p]
     lib.rs_debug_trace_rays.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]
     lib.rs_debug_bvh_shape.argtypes = [C.c_void_p, C.c_void_p]
     lib.rs_build_cell_lists_static.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
@@ -73,7 +74,8 @@ def load_library():
                  "rs_freeze", "rs_get_buffer", "rs_set_buffer", "rs_enable_stage_timing", "rs_get_stage_times",
                  "rs_debug_keep_candidates", "rs_batch_create", "rs_batch_execute", "rs_batch_destroy",
                  "rs_build_cell_lists_static", "rs_set_materials", "rs_checkpoint_bytes", "rs_checkpoint", "rs_backward",
-                 "rs_backward_stats", "rs_debug_trace_rays", "rs_debug_bvh_shape"):
+                 "rs_backward_stats", "rs_debug_trace_rays", "rs_debug_bvh_shape",
+                 "rs_update_geometry"):
         getattr(lib, name).restype = C.c_int
     _lib = lib
     return lib
@@ -216,6 +218,17 @@ class ReservoirSplatting:
         """gradMaterials (device, n x 8 float32) += d loss / d parameters for d loss / d colour."""
         _check(self._lib.rs_backward(self._h, C.c_void_p(checkpoint_ptr) if checkpoint_ptr else None,
                                      C.c_void_p(grad_color_ptr), C.c_void_p(grad_materials_ptr), C.c_void_p(stream)))
+
+    # ---- moving geometry
+    def update_geometry(self, positions, stream: int = 0):
+        """Moves the triangles for the next frame: positions is a host array (n x 9 float32) or a
+        CUDA tensor of the same shape."""
+        if hasattr(positions, "data_ptr"):
+            assert positions.is_cuda and positions.dtype.itemsize == 4 and positions.is_contiguous()
+            _check(self._lib.rs_update_geometry(self._h, C.c_void_p(positions.data_ptr()), positions.numel() // 9, 1, C.c_void_p(stream)))
+        else:
+            q = np.ascontiguousarray(positions, np.float32).reshape(-1, 9)
+            _check(self._lib.rs_update_geometry(self._h, q.ctypes.data, len(q), 0, C.c_void_p(stream)))
 
     # ---- ray-query diagnostics
     def trace_rays(self, rays: np.ndarray):

@@ -153,9 +153,16 @@ __device__ __forceinline__ void tri_box(const float4* tri, uint32_t p, float lo[
     }
 }
 
-__device__ __forceinline__ void child_box(const float4* tri, const float4* nodes, uint32_t c, float lo[3], float hi[3])
+// Padded box of the triangle at leaf position p: tri is key ordered when leafTri is null, else scene
+// ordered and reached through the scene index leafTri keeps.
+__device__ __forceinline__ void leaf_box(const float4* tri, const float4* leafTri, uint32_t p, float lo[3], float hi[3])
 {
-    if (c & kLeafBit) { tri_box(tri, c & ~kLeafBit, lo, hi); return; }
+    tri_box(tri, leafTri ? __float_as_uint(leafTri[3 * (size_t)p].w) : p, lo, hi);
+}
+
+__device__ __forceinline__ void child_box(const float4* tri, const float4* leafTri, const float4* nodes, uint32_t c, float lo[3], float hi[3])
+{
+    if (c & kLeafBit) { leaf_box(tri, leafTri, c & ~kLeafBit, lo, hi); return; }
     const volatile float4* n = nodes + 4 * (size_t)c;
     float l0x = n[0].x, l0y = n[0].y, l0z = n[0].z, l1x = n[1].x, l1y = n[1].y, l1z = n[1].z;
     float r0x = n[2].x, r0y = n[2].y, r0z = n[2].z, r1x = n[3].x, r1y = n[3].y, r1z = n[3].z;
@@ -163,8 +170,8 @@ __device__ __forceinline__ void child_box(const float4* tri, const float4* nodes
     hi[0] = fmaxf(l1x, r1x); hi[1] = fmaxf(l1y, r1y); hi[2] = fmaxf(l1z, r1z);
 }
 
-__global__ void k_refit(const float4* __restrict__ tri, int n, float4* nodes, const uint32_t* __restrict__ parent,
-                        const uint32_t* __restrict__ leafParent, uint32_t* arrivals)
+__global__ void k_refit(const float4* __restrict__ tri, const float4* __restrict__ leafTri, int n, float4* nodes,
+                        const uint32_t* __restrict__ parent, const uint32_t* __restrict__ leafParent, uint32_t* arrivals)
 {
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
@@ -177,8 +184,8 @@ __global__ void k_refit(const float4* __restrict__ tri, int n, float4* nodes, co
         uint32_t cl = __float_as_uint(((volatile float4*)nodes)[4 * (size_t)node + 0].w);
         uint32_t cr = __float_as_uint(((volatile float4*)nodes)[4 * (size_t)node + 1].w);
         float llo[3], lhi[3], rlo[3], rhi[3];
-        child_box(tri, nodes, cl, llo, lhi);
-        child_box(tri, nodes, cr, rlo, rhi);
+        child_box(tri, leafTri, nodes, cl, llo, lhi);
+        child_box(tri, leafTri, nodes, cr, rlo, rhi);
         volatile float4* o = (volatile float4*)(nodes + 4 * (size_t)node);
         o[0].x = llo[0]; o[0].y = llo[1]; o[0].z = llo[2];
         o[1].x = lhi[0]; o[1].y = lhi[1]; o[1].z = lhi[2];
@@ -222,10 +229,10 @@ __device__ __forceinline__ bool is_wide_leaf(const WideChild& c) { return (c.ref
 
 // Writes node w for children c[0..n): internal children get consecutive node indices from
 // childBase (returned through childOf), leaves reference their sorted range.
-__device__ void write_wide_node(float4* wnodes, uint32_t w, const WideChild* c, int n, uint32_t childBase, uint32_t* childOf)
+__device__ void write_wide_node(float4* wnodes, uint4* binRef, uint32_t w, const WideChild* c, int n, uint32_t childBase, uint32_t* childOf)
 {
     float lo[3][4], hi[3][4];
-    uint32_t ref[4];
+    uint32_t ref[4], src[4];
     uint32_t nInternal = 0;
     for (int j = 0; j < 4; j++)
     {
@@ -234,8 +241,10 @@ __device__ void write_wide_node(float4* wnodes, uint32_t w, const WideChild* c, 
         {
             for (int a = 0; a < 3; a++) { lo[a][j] = __int_as_float(0x7f800000); hi[a][j] = __int_as_float(0xff800000); }
             ref[j] = kInvalidIndex;
+            src[j] = kInvalidIndex;
             continue;
         }
+        src[j] = c[j].ref;
         for (int a = 0; a < 3; a++) { lo[a][j] = c[j].lo[a]; hi[a][j] = c[j].hi[a]; }
         if (is_wide_leaf(c[j])) ref[j] = kLeafBit | (c[j].first << 2) | (c[j].count - 1u);
         else
@@ -253,11 +262,12 @@ __device__ void write_wide_node(float4* wnodes, uint32_t w, const WideChild* c, 
     o[4] = make_float4(lo[2][0], lo[2][1], lo[2][2], lo[2][3]);
     o[5] = make_float4(hi[2][0], hi[2][1], hi[2][2], hi[2][3]);
     o[6] = make_float4(__uint_as_float(ref[0]), __uint_as_float(ref[1]), __uint_as_float(ref[2]), __uint_as_float(ref[3]));
+    binRef[w] = make_uint4(src[0], src[1], src[2], src[3]);
 }
 
 // counters: [0] nodes allocated, [1] unused, [2] next-level items, [3] unused
 __global__ void k_collapse(const float4* __restrict__ nodes, const uint2* __restrict__ range, const uint2* __restrict__ qin, uint32_t nin,
-                           uint2* __restrict__ qout, uint32_t* __restrict__ counters, float4* __restrict__ wnodes)
+                           uint2* __restrict__ qout, uint32_t* __restrict__ counters, float4* __restrict__ wnodes, uint4* __restrict__ binRef)
 {
     uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nin) return;
@@ -282,13 +292,13 @@ __global__ void k_collapse(const float4* __restrict__ nodes, const uint2* __rest
         if (!is_wide_leaf(c[j])) nInternal++;
     const uint32_t childBase = nInternal ? atomicAdd(&counters[0], nInternal) : 0u;
     uint32_t childOf[4];
-    write_wide_node(wnodes, item.y, c, n, childBase, childOf);
+    write_wide_node(wnodes, binRef, item.y, c, n, childBase, childOf);
     for (int j = 0; j < n; j++)
         if (childOf[j] != kInvalidIndex) qout[atomicAdd(&counters[2], 1u)] = make_uint2(c[j].ref, childOf[j]);
 }
 
 // A scene of one triangle: one node with one leaf.
-__global__ void k_single_leaf(const float4* __restrict__ sorted, float4* __restrict__ wnodes)
+__global__ void k_single_leaf(const float4* __restrict__ sorted, float4* __restrict__ wnodes, uint4* __restrict__ binRef)
 {
     WideChild c;
     c.ref = kLeafBit;
@@ -296,7 +306,7 @@ __global__ void k_single_leaf(const float4* __restrict__ sorted, float4* __restr
     c.count = 1;
     tri_box(sorted, 0, c.lo, c.hi);
     uint32_t childOf[4];
-    write_wide_node(wnodes, 0, &c, 1, 0, childOf);
+    write_wide_node(wnodes, binRef, 0, &c, 1, 0, childOf);
 }
 
 // Leaf-order triangles in the traversal form (p0, scene index), (p1 - p0), (p2 - p0).
@@ -310,8 +320,77 @@ __global__ void k_leaf_tris(const float4* __restrict__ sorted, uint32_t n, float
     leafTri[3 * (size_t)i + 2] = make_float4(c.x - a.x, c.y - a.y, c.z - a.z, 0.f);
 }
 
+// ------------------------------------------------------------------ refit to moved triangles
+// Leaf triangles from the scene-order triangles through the scene index each one keeps.
+__global__ void k_refit_leaf_tris(const float4* __restrict__ tri, uint32_t n, float4* __restrict__ leafTri)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t t = __float_as_uint(leafTri[3 * (size_t)i].w);
+    const float4 a = tri[3 * (size_t)t], b = tri[3 * (size_t)t + 1], c = tri[3 * (size_t)t + 2];
+    leafTri[3 * (size_t)i + 0] = make_float4(a.x, a.y, a.z, __uint_as_float(t));
+    leafTri[3 * (size_t)i + 1] = make_float4(b.x - a.x, b.y - a.y, b.z - a.z, 0.f);
+    leafTri[3 * (size_t)i + 2] = make_float4(c.x - a.x, c.y - a.y, c.z - a.z, 0.f);
+}
+
+// Box of a binary reference: a leaf's padded triangle box, or the union of an internal node's children.
+__device__ __forceinline__ void binary_ref_box(const float4* tri, const float4* leafTri, const float4* nodes, uint32_t ref, float lo[3], float hi[3])
+{
+    if (ref & kLeafBit) { leaf_box(tri, leafTri, ref & ~kLeafBit, lo, hi); return; }
+    const float4* n = nodes + 4 * (size_t)ref;
+    lo[0] = fminf(n[0].x, n[2].x); lo[1] = fminf(n[0].y, n[2].y); lo[2] = fminf(n[0].z, n[2].z);
+    hi[0] = fmaxf(n[1].x, n[3].x); hi[1] = fmaxf(n[1].y, n[3].y); hi[2] = fmaxf(n[1].z, n[3].z);
+}
+
+__global__ void k_refit_wide(const float4* __restrict__ tri, const float4* __restrict__ leafTri, const float4* __restrict__ nodes,
+                             const uint4* __restrict__ binRef, uint32_t numWide, float4* __restrict__ wnodes)
+{
+    uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= numWide) return;
+    const uint4 src4 = binRef[w];
+    const uint32_t src[4] = {src4.x, src4.y, src4.z, src4.w};
+    float4* o = wnodes + 7 * (size_t)w;
+    float lo[3][4], hi[3][4];
+    for (int j = 0; j < 4; j++)
+    {
+        if (src[j] == kInvalidIndex)
+        {
+            for (int a = 0; a < 3; a++) { lo[a][j] = __int_as_float(0x7f800000); hi[a][j] = __int_as_float(0xff800000); }
+            continue;
+        }
+        float l[3], h[3];
+        binary_ref_box(tri, leafTri, nodes, src[j], l, h);
+        for (int a = 0; a < 3; a++) { lo[a][j] = l[a]; hi[a][j] = h[a]; }
+    }
+    o[0] = make_float4(lo[0][0], lo[0][1], lo[0][2], lo[0][3]);
+    o[1] = make_float4(hi[0][0], hi[0][1], hi[0][2], hi[0][3]);
+    o[2] = make_float4(lo[1][0], lo[1][1], lo[1][2], lo[1][3]);
+    o[3] = make_float4(hi[1][0], hi[1][1], hi[1][2], hi[1][3]);
+    o[4] = make_float4(lo[2][0], lo[2][1], lo[2][2], lo[2][3]);
+    o[5] = make_float4(hi[2][0], hi[2][1], hi[2][2], hi[2][3]);
+}
+
+cudaError_t refit_wide_bvh(const float4* dTri, WideBvh* b, cudaStream_t s)
+{
+    const uint32_t n = b->numTris;
+    if (n == 0) return cudaSuccess;
+    k_refit_leaf_tris<<<(n + 255) / 256, 256, 0, s>>>(dTri, n, b->leafTri);
+    if (n > 1)
+    {
+        cudaError_t e = cudaMemsetAsync(b->arrivals, 0, n * 4ull, s);
+        if (e != cudaSuccess) return e;
+        k_refit<<<(n + 255) / 256, 256, 0, s>>>(dTri, b->leafTri, (int)n, b->binNodes, b->parent, b->leafParent, b->arrivals);
+    }
+    k_refit_wide<<<(b->numNodes + 127) / 128, 128, 0, s>>>(dTri, b->leafTri, b->binNodes, b->binRef, b->numNodes, b->nodes);
+    return cudaGetLastError();
+}
+
 void free_wide_bvh(WideBvh* b)
 {
+    if (b->parent) cudaFree(b->parent);
+    if (b->leafParent) cudaFree(b->leafParent);
+    if (b->arrivals) cudaFree(b->arrivals);
+    if (b->binRef) cudaFree(b->binRef);
     if (b->binNodes) cudaFree(b->binNodes);
     if (b->nodes) cudaFree(b->nodes);
     if (b->leafTri) cudaFree(b->leafTri);
@@ -334,6 +413,7 @@ cudaError_t build_wide_bvh(const float4* dTri, uint32_t n, WideBvh* out, cudaStr
     const uint32_t maxWide = n / kWideLeafMax + 2; // every node but the root holds more than kWideLeafMax triangles
 #define RS_TRY(x) do { e = (x); if (e != cudaSuccess) goto done; } while (0)
     RS_TRY(cudaMalloc(&out->nodes, 112ull * maxWide));
+    RS_TRY(cudaMalloc(&out->binRef, 16ull * maxWide));
     RS_TRY(cudaMalloc(&out->leafTri, 48ull * n));
     RS_TRY(cudaMalloc(&keys, n * 8ull)); RS_TRY(cudaMalloc(&vals, n * 4ull));
     RS_TRY(cudaMalloc(&keys2, n * 8ull)); RS_TRY(cudaMalloc(&vals2, n * 4ull));
@@ -353,7 +433,7 @@ cudaError_t build_wide_bvh(const float4* dTri, uint32_t n, WideBvh* out, cudaStr
         uint32_t levels = 0, numWide = 1;
         if (n == 1)
         {
-            k_single_leaf<<<1, 1, 0, s>>>(sorted, out->nodes);
+            k_single_leaf<<<1, 1, 0, s>>>(sorted, out->nodes, out->binRef);
             levels = 1;
         }
         else
@@ -365,7 +445,7 @@ cudaError_t build_wide_bvh(const float4* dTri, uint32_t n, WideBvh* out, cudaStr
             RS_TRY(cudaMemsetAsync(nodes, 0, 64ull * (n - 1), s));
             k_karras<<<(n - 1 + 255) / 256, 256, 0, s>>>(keys2, (int)n, nodes, range, parent, leafParent);
             RS_TRY(cudaMemsetAsync(arrivals, 0, n * 4ull, s));
-            k_refit<<<(n + 255) / 256, 256, 0, s>>>(sorted, (int)n, nodes, parent, leafParent, arrivals);
+            k_refit<<<(n + 255) / 256, 256, 0, s>>>(sorted, nullptr, (int)n, nodes, parent, leafParent, arrivals);
             const uint2 root = make_uint2(0u, 0u);
             const uint32_t one = 1u;
             RS_TRY(cudaMemcpyAsync(qa, &root, sizeof(root), cudaMemcpyHostToDevice, s));
@@ -374,7 +454,7 @@ cudaError_t build_wide_bvh(const float4* dTri, uint32_t n, WideBvh* out, cudaStr
             while (nin > 0)
             {
                 RS_TRY(cudaMemsetAsync(counters + 2, 0, 4, s));
-                k_collapse<<<(nin + 127) / 128, 128, 0, s>>>(nodes, range, qa, nin, qb, counters, out->nodes);
+                k_collapse<<<(nin + 127) / 128, 128, 0, s>>>(nodes, range, qa, nin, qb, counters, out->nodes, out->binRef);
                 RS_TRY(cudaGetLastError());
                 RS_TRY(cudaMemcpyAsync(&nin, counters + 2, 4, cudaMemcpyDeviceToHost, s));
                 RS_TRY(cudaStreamSynchronize(s));
@@ -393,7 +473,9 @@ cudaError_t build_wide_bvh(const float4* dTri, uint32_t n, WideBvh* out, cudaStr
         out->depth = levels;
         out->binNodes = nodes; // the binary tree stays for closest-hit queries
         out->binRoot = n == 1 ? kLeafBit : 0u;
-        nodes = nullptr;
+        out->numTris = n;
+        out->parent = parent; out->leafParent = leafParent; out->arrivals = arrivals; // kept for refits
+        nodes = nullptr; parent = nullptr; leafParent = nullptr; arrivals = nullptr;
     }
 done:
 #undef RS_TRY

@@ -22,6 +22,25 @@ struct alignas(16) LightTriangle
     float Le[3]; float pad;
 };
 
+// Geometry of a light record from its triangle's current vertices (LightCollection.cpp /
+// BuildTriangleList.cs.slang:62: normal = N / |N|, area = |N| / 2 with N = (p1 - p0) x (p2 - p0)).
+// The flux, and so the power sampler's selection weights, stay those of the last scene or
+// material update; selection and its pdf both read them, so the estimator stays consistent.
+RS_HD void light_set_vertices(LightTriangle& L, f3 p0, f3 p1, f3 p2)
+{
+    f3 N = cross(p1 - p0, p2 - p0);
+    float len = length(N);
+    L.p0[0] = p0.x; L.p0[1] = p0.y; L.p0[2] = p0.z;
+    L.p1[0] = p1.x; L.p1[1] = p1.y; L.p1[2] = p1.z;
+    L.p2[0] = p2.x; L.p2[1] = p2.y; L.p2[2] = p2.z;
+    L.area = 0.5f * len;
+    if (len > 0.f)
+    {
+        f3 n = N / len;
+        L.normal[0] = n.x; L.normal[1] = n.y; L.normal[2] = n.z;
+    }
+}
+
 struct LightView
 {
     const LightTriangle* tris;

@@ -83,6 +83,20 @@ RS_HD BsdfData setup_material(const MaterialData& m, bool frontFacing)
 }
 
 // loadShadingData (LoadShadingData.slang:134-142) for a triangle hit of the soup.
+// World position of a triangle hit with the arithmetic of load_shading_data (used with the
+// previous frame's triangles for motion vectors: Scene::getPrevPosW, VBufferRT.slang:84).
+RS_HD f3 hit_position(const f4* tri, const HitInfo& hit)
+{
+    uint32_t prim = hit_prim(hit);
+    f3 p0 = f4xyz(tri[3 * prim + 0]), p1 = f4xyz(tri[3 * prim + 1]), p2 = f4xyz(tri[3 * prim + 2]);
+    f2 bc = hit_bary(hit);
+    float b0 = 1.f - bc.x - bc.y;
+    f3 pos = p0 * b0;
+    pos += p1 * bc.x;
+    pos += p2 * bc.y;
+    return pos;
+}
+
 RS_HD ShadingData load_shading_data(const f4* tri, const MaterialData* mtl, const HitInfo& hit, f3 rayDir)
 {
     ShadingData sd;

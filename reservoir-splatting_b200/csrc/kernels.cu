@@ -37,7 +37,8 @@ __global__ void __launch_bounds__(256) k_vbuffer(uint32_t slot, uint4* __restric
     if (trace_closest(C.bvh, mk_ray(cam.posW, dir, 0.f, kRayTMax), h, t, C.fault))
     {
         vbuffer[i] = make_uint4(h.w[0], h.w[1], h.w[2], h.w[3]);
-        f3 prevPosW = dev_sd(C, h, dir).posW;
+        // Scene::getPrevPosW (VBufferRT.slang:84): the hit on the previous frame's geometry
+        f3 prevPosW = hit_position(reinterpret_cast<const f4*>(C.prevTri), h);
         f3 d = prevPosW - pc.posW;
         f3 camRay = mk3(dot(normalize(pc.cameraU), d), dot(normalize(pc.cameraV), d), dot(normalize(pc.cameraW), d));
         float lw = length(pc.cameraW);

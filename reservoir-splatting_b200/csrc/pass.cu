@@ -101,6 +101,10 @@ struct rs_pass
     PreparedScene scene;
     DevBuf<float4> dTri;
     WideBvh bvh;
+    DevBuf<float4> dPrevTri;    // triangles of the previous frame after rs_update_geometry
+    DevBuf<float> dPosStage;    // host positions staged for rs_update_geometry
+    bool geometryMoved = false; // rs_update_geometry since the last frame
+    bool hostTriStale = false;  // scene.tri positions behind the device copy
     DevBuf<MaterialData> dMaterials;
     DevBuf<LightTriangle> dLights;
     DevBuf<u2> dAlias;
@@ -352,6 +356,8 @@ extern "C" RS_API rs_status rs_set_scene(rs_pass* p, const rs_scene_desc* sd)
     cudaStreamDestroy(s);
     if (e != cudaSuccess) return fail(RS_CUDA_ERROR, std::string("BVH build: ") + cudaGetErrorString(e));
     p->hasScene = true;
+    p->hostTriStale = false;
+    p->geometryMoved = false;
     p->frameCount = 0; // setScene resets the frame count (ReservoirSplatting.cpp:380)
     return RS_OK;
 }
@@ -412,6 +418,7 @@ static void begin_frame(rs_pass* p, const rs_frame_desc* f)
     C.bvh.nodes = p->bvh.nodes;
     C.bvh.leafTri = p->bvh.leafTri;
     C.bvh.tri = p->dTri.p;
+    C.prevTri = p->geometryMoved ? p->dPrevTri.p : p->dTri.p;
     C.bvh.numTris = (uint32_t)(p->scene.tri.size() / 3);
     C.materials = p->dMaterials.p;
     C.lights.tris = p->dLights.p;
@@ -457,6 +464,7 @@ static void end_frame(rs_pass* p)
     }
     p->prevCamera = p->camera;
     p->havePrevCamera = true;
+    p->geometryMoved = false;
 }
 
 // Issues the frame's device work on `s`.  The frame context goes to the pass's constant-memory
@@ -848,6 +856,62 @@ extern "C" RS_API rs_status rs_set_buffer(rs_pass* p, rs_buffer_id id, const voi
     return fail(RS_INVALID_ARG, "buffer cannot be restored");
 }
 
+// ------------------------------------------------------------------ moving geometry
+// Moves every triangle to `positions` (x, y, z of p0, p1, p2 per triangle; host memory, or device
+// memory of the current device when onDevice is set) for the next frame (Falcor's animated scene
+// update).  The previous positions serve that frame's motion vectors (Scene::getPrevPosW,
+// VBufferRT.slang:84); reprojection and shifts read the new positions through the hit records
+// (ReprojectTemporalSamples.rt.slang:104).  Both trees are refitted in place (same topology), and
+// the light records take their triangles' new vertices with the flux of the last scene or material
+// update.  Stream-ordered on `cudaStream`.
+__global__ void k_set_positions(float4* __restrict__ tri, const float* __restrict__ pos, uint32_t n)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= 3u * n) return;
+    float4 q = tri[i];
+    q.x = pos[3 * (size_t)i]; q.y = pos[3 * (size_t)i + 1]; q.z = pos[3 * (size_t)i + 2];
+    tri[i] = q;
+}
+
+__global__ void k_update_lights(LightTriangle* __restrict__ lights, uint32_t count, const float4* __restrict__ tri)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    LightTriangle L = lights[i];
+    const float4* q = tri + 3 * (size_t)L.sceneTri;
+    light_set_vertices(L, mk3(q[0].x, q[0].y, q[0].z), mk3(q[1].x, q[1].y, q[1].z), mk3(q[2].x, q[2].y, q[2].z));
+    lights[i] = L;
+}
+
+extern "C" RS_API rs_status rs_update_geometry(rs_pass* p, const float* positions, uint32_t numTriangles, uint32_t onDevice, void* streamPtr)
+{
+    if (!p || !positions) return fail(RS_INVALID_ARG, "pass or positions is NULL");
+    if (!p->hasScene) return fail(RS_NOT_READY, "rs_update_geometry needs a scene");
+    const uint32_t n = (uint32_t)(p->scene.tri.size() / 3);
+    if (numTriangles != n) return fail(RS_INVALID_ARG, "triangle count differs from the scene's");
+    if (n == 0) return RS_OK;
+    cudaStream_t s = static_cast<cudaStream_t>(streamPtr);
+    RS_CUDA(p->dPrevTri.ensure(3ull * n));
+    const float* src = positions;
+    if (!onDevice)
+    {
+        RS_CUDA(p->dPosStage.ensure(9ull * n));
+        RS_CUDA(cudaMemcpyAsync(p->dPosStage.p, positions, 36ull * n, cudaMemcpyHostToDevice, s));
+        src = p->dPosStage.p;
+    }
+    RS_CUDA(cudaMemcpyAsync(p->dPrevTri.p, p->dTri.p, 48ull * n, cudaMemcpyDeviceToDevice, s));
+    k_set_positions<<<(3 * n + 255) / 256, 256, 0, s>>>(p->dTri.p, src, n);
+    const uint32_t nl = (uint32_t)p->scene.lights.size();
+    if (nl) k_update_lights<<<(nl + 127) / 128, 128, 0, s>>>(p->dLights.p, nl, p->dTri.p);
+    RS_CUDA(cudaGetLastError());
+    cudaError_t e = refit_wide_bvh(p->dTri.p, &p->bvh, s);
+    if (e != cudaSuccess) return fail(RS_CUDA_ERROR, std::string("BVH refit: ") + cudaGetErrorString(e));
+    p->hostTriStale = true; // rs_set_materials reads the positions back before it rebuilds the lights
+    p->geometryMoved = true;
+    p->lastStream = s;
+    return RS_OK;
+}
+
 // ------------------------------------------------------------------ path-replay adjoint
 // (no reference counterpart; the kernel and its estimator are described in adjoint.cuh)
 
@@ -859,6 +923,12 @@ extern "C" RS_API rs_status rs_set_materials(rs_pass* p, const rs_material* mate
     if (!p->hasScene) return fail(RS_NOT_READY, "rs_set_materials needs a scene");
     if (count != p->scene.materials.size()) return fail(RS_INVALID_ARG, "material count differs from the scene's");
     const size_t n = p->scene.tri.size() / 3;
+    if (p->hostTriStale && n)
+    {
+        RS_CUDA(cudaDeviceSynchronize());
+        RS_CUDA(cudaMemcpy(p->scene.tri.data(), p->dTri.p, 48ull * n, cudaMemcpyDeviceToHost));
+        p->hostTriStale = false;
+    }
     std::vector<float> pos(9 * n);
     std::vector<uint32_t> ids(n);
     for (size_t t = 0; t < n; t++)

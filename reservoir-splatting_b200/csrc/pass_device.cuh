@@ -18,6 +18,7 @@ constexpr float kConfidenceCap = 20.f;   // Reservoir.slang:75
 struct DevCtx
 {
     BvhView bvh;
+    const float4* prevTri; // the previous frame's triangles (scene order; bvh.tri when nothing moved)
     const MaterialData* materials;
     LightView lights;
     CameraData camera;      // gScene.camera of this frame

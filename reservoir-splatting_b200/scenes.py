@@ -220,6 +220,37 @@ def terrain_spheres(seed: int = 1, grid: int = 512, spheres: int = 500, subdiv: 
     return Scene(pos, np.concatenate(mids), np.stack(mats).astype(np.float32), "terrain_spheres", info)
 
 
+class SphereMotion:
+    """Linear motion of some of terrain_spheres' icospheres: sphere s moves by velocity[s] per frame
+    (uniform direction in the ground plane, speed U[0, max_speed]).  positions(frame) gives the
+    scene's triangle soup (n x 9 float32) at that frame, for ReservoirSplatting.update_geometry."""
+
+    def __init__(self, scene: Scene, moving: int = 200, max_speed: float = 0.05, seed: int = 0):
+        info = scene.info
+        self.base = np.ascontiguousarray(scene.positions, np.float32).reshape(-1, 9).copy()
+        first = info["terrain_triangles"]
+        per = info["sphere_triangles_each"]
+        rng = np.random.default_rng(seed)
+        moving = min(moving, info["spheres"])
+        self.spheres = np.sort(rng.choice(info["spheres"], moving, replace=False))
+        ang = rng.uniform(0.0, 2.0 * math.pi, moving)
+        speed = rng.uniform(0.0, max_speed, moving)
+        self.velocity = np.stack([speed * np.cos(ang), np.zeros(moving), speed * np.sin(ang)], 1).astype(np.float32)
+        self.ranges = [(first + int(k) * per, per) for k in self.spheres]
+        self.tri_velocity = np.zeros((len(self.base), 3), np.float32)
+        for (a, n), v in zip(self.ranges, self.velocity):
+            self.tri_velocity[a:a + n] = v
+
+    def positions(self, frame: int) -> np.ndarray:
+        return self.base + np.tile(self.tri_velocity * np.float32(frame), (1, 3))
+
+
+def motion_blur_scene(seed: int = 3, grid: int = 800, spheres: int = 500, subdiv: int = 4, lights: int = 64):
+    """terrain_spheres scaled to about 4M triangles (800 x 800 heightfield: 1.28M, 500 icospheres at
+    subdivision 4: 2.56M, 64 emissive triangles)."""
+    return terrain_spheres(seed=seed, grid=grid, spheres=spheres, subdiv=subdiv, lights=lights)
+
+
 def inverse_scene(seed: int = 5, grid: int = 300, spheres: int = 16, subdiv: int = 3, materials: int = 32,
                   emitters: int = 8, extent: float = 60.0, height: float = 6.0) -> Scene:
     """Scene for differentiation: fBm terrain + icospheres sharing `materials` metal-rough materials

@@ -146,3 +146,34 @@ def test_gpu_matches_committed_golden(rs, scenes, name):
     P.compare_reservoirs("reservoirs", gpu.get_buffer("curr_reservoirs"), ref["reservoirs"])
     P.compare_recon("reconnection", gpu.get_buffer("curr_reconnection"), ref["reconnection"])
     gpu.close()
+
+
+@pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
+@pytest.mark.parametrize("mode", ["ScatterBackup", "MultiScatter"])
+def test_moving_spheres(rs, oracle_mod, scenes, mode):
+    """Spheres moving linearly each frame (rs_update_geometry: refitted trees, previous-frame motion
+    vectors) against the oracle, which rebuilds its own tree every frame."""
+    sc = scenes.terrain_spheres(seed=5, grid=40, spheres=10, subdiv=2, lights=6, extent=30.0, height=3.0)
+    motion = scenes.SphereMotion(sc, moving=6, max_speed=0.3, seed=2)
+    props = {"temporalReuse": mode, "gatherOption": "Clamped", "maxSurfaceBounces": 2, "numTimePartitions": 4,
+             "artificialFrameTime": 1.0 / 48.0, "enableSpatialResampling": True}
+    W, H = 80, 56
+    gpu = rs.ReservoirSplatting(props, W, H)
+    ora = oracle_mod.OraclePass(props, W, H)
+    gpu.set_scene(sc)
+    ora.set_scene(sc)
+    for f in range(5):
+        cam = scenes.orbit_camera(f, W, H, radius=24.0, height_above=9.0)
+        cam.shutter_speed = 1.0 / 24.0 if mode == "MultiScatter" else 0.0
+        cam.aperture_radius = 0.02
+        if f > 0:
+            pos = motion.positions(f)
+            gpu.update_geometry(pos)
+            ora.update_geometry(pos)
+        img_g = gpu.render(cam)
+        img_o = ora.execute(cam)
+        P.assert_equal(f"frame{f}.vbuffer", gpu.get_buffer("vbuffer"), ora.get_buffer("vbuffer"))
+        P.assert_equal(f"frame{f}.mvec", gpu.get_buffer("mvec").view(np.uint32), ora.get_buffer("mvec").view(np.uint32))
+        P.compare_reservoirs(f"frame{f}.reservoirs", gpu.get_buffer("curr_reservoirs"), ora.get_buffer("curr_reservoirs"))
+        P.assert_close(f"frame{f}.color", img_g, img_o)
+    gpu.close()
