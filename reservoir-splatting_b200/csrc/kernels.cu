@@ -71,7 +71,8 @@ struct PState
     Recon rec;           // path.reconnection
     float candTotalWeight; // path.reservoir (CandidateReservoir)
     f3 candIntegrand;
-    Recon candRec;       // path.reservoir.selectedReconnection
+    Recon candRec;       // path.reservoir.selectedReconnection (several samples per pixel)
+    bool anySelected;    // a candidate was selected (one sample per pixel: its record is in the output)
 };
 enum : uint32_t { kPActive = 1u, kPHit = 2u, kPSpecular = 8u, kPDelta = 16u, kPLightUpper = 64u, kPLightLower = 128u };
 
@@ -104,7 +105,11 @@ __device__ __forceinline__ void next_hit(const DevCtx& C, PState& p) // PathTrac
 }
 
 // handleHit (PathTracer.slang:783-1168)
-__device__ void handle_hit(const DevCtx& C, PState& path)
+// kDirect (one sample per pixel): a selected candidate's record is written straight to the
+// output planes (outRec, pixel pix) instead of being carried in the path state; the output is the
+// same, and ~28 registers of long-lived state are freed.
+template <bool kDirect>
+__device__ void handle_hit(const DevCtx& C, PState& path, const RecPlanes& outRec, uint32_t pix)
 {
     const bool isPrimaryHit = path.vertex == 1;
     ShadingData sd = dev_sd(C, path.hit, path.dir);
@@ -156,14 +161,16 @@ __device__ void handle_hit(const DevCtx& C, PState& path)
         bool selected = cand_add_vertex(path, 1.f, path.earlyThroughput * path.thp * d.emission * misWeight);
         if (selected)
         {
-            path.candRec = path.rec;
-            path.candRec.pathLength = path.vertex;
-            path.candRec.lightIsNEE = false;
-            path.candRec.lightIsDistant = false;
-            path.candRec.lightPdf = lightPdf;
-            if (path.vertex == 2) path.candRec.lightPdf *= geometryFactor;
-            if (path.vertex == 2 || path.vertex == 3) path.candRec.irradiance = d.emission;
-            else path.candRec.irradiance = path.thp * d.emission * misWeight;
+            Recon sel = path.rec;
+            sel.pathLength = path.vertex;
+            sel.lightIsNEE = false;
+            sel.lightIsDistant = false;
+            sel.lightPdf = lightPdf;
+            if (path.vertex == 2) sel.lightPdf *= geometryFactor;
+            if (path.vertex == 2 || path.vertex == 3) sel.irradiance = d.emission;
+            else sel.irradiance = path.thp * d.emission * misWeight;
+            if (kDirect) { store_rec(outRec, pix, sel); path.anySelected = true; }
+            else path.candRec = sel;
         }
     }
 
@@ -222,27 +229,29 @@ __device__ void handle_hit(const DevCtx& C, PState& path)
                 bool selected = cand_add_vertex(path, 1.f, path.earlyThroughput * path.thp * weight * lsLi * misWeight);
                 if (selected)
                 {
-                    path.candRec = path.rec;
-                    path.candRec.pathLength = path.vertex + 1;
-                    path.candRec.lightIsNEE = true;
-                    path.candRec.irradiance = Le;
-                    if (path.vertex == 1) path.candRec.transmissionEvent = dot(sd.faceN, sd.V) * dot(sd.faceN, lsDir) < 0.f;
-                    path.candRec.lightIsDistant = false;
+                    Recon sel = path.rec;
+                    sel.pathLength = path.vertex + 1;
+                    sel.lightIsNEE = true;
+                    sel.irradiance = Le;
+                    if (path.vertex == 1) sel.transmissionEvent = dot(sd.faceN, sd.V) * dot(sd.faceN, lsDir) < 0.f;
+                    sel.lightIsDistant = false;
                     if (path.vertex == 1)
                     {
-                        path.candRec.secondHit = hit_tri(C.lights.tris[tls.triangleIndex].sceneTri, tls.uv.x, tls.uv.y);
-                        path.candRec.secondaryPathJacobian = lsPdf * tls.geometryTerm;
-                        path.candRec.lightPdf = lsPdf * tls.geometryTerm;
+                        sel.secondHit = hit_tri(C.lights.tris[tls.triangleIndex].sceneTri, tls.uv.x, tls.uv.y);
+                        sel.secondaryPathJacobian = lsPdf * tls.geometryTerm;
+                        sel.lightPdf = lsPdf * tls.geometryTerm;
                     }
                     else if (path.vertex == 2)
                     {
-                        path.candRec.secondWo = lsDir;
-                        path.candRec.lightPdf = lsPdf;
+                        sel.secondWo = lsDir;
+                        sel.lightPdf = lsPdf;
                     }
                     else
                     {
-                        path.candRec.irradiance = path.thp * Lr;
+                        sel.irradiance = path.thp * Lr;
                     }
+                    if (kDirect) { store_rec(outRec, pix, sel); path.anySelected = true; }
+                    else path.candRec = sel;
                 }
             }
         }
@@ -302,13 +311,11 @@ __device__ void handle_hit(const DevCtx& C, PState& path)
 }
 
 // InitialCandidates.cs.slang:80-141 + addCandidateReservoir (:52-75)
-__global__ void __launch_bounds__(128, 3) k_candidates(uint32_t slot, ResPlanes curr, RecPlanes currRec)
+template <bool kDirect>
+__device__ __forceinline__ void candidates_pixel(const DevCtx& C, uint32_t i, const ResPlanes& curr, const RecPlanes& currRec)
 {
-    const DevCtx& C = c_ctx[slot];
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= C.W * C.H) return;
     uint32_t x = i % C.W, y = i / C.W;
-    const uint32_t spp = C.spp;
+    const uint32_t spp = kDirect ? 1u : C.spp;
     for (uint32_t sIdx = 0; sIdx < spp; sIdx++)
     {
         PState path;
@@ -323,7 +330,8 @@ __global__ void __launch_bounds__(128, 3) k_candidates(uint32_t slot, ResPlanes 
         path.rec = recon_default();
         path.candTotalWeight = 0.f;
         path.candIntegrand = mk3(0.f);
-        path.candRec = recon_default();
+        if (!kDirect) path.candRec = recon_default();
+        path.anySelected = false;
         path.sg = sg_create(x, y, C.useFixedSeed ? C.fixedSeed + 0 : kNumRenderPasses * (C.frameCount + C.seed) + 0, C.sgKind);
         CameraData cam = C.camera;
         path.rec.time = sampleNext1D(path.sg) * cam.shutterSpeed;
@@ -344,11 +352,11 @@ __global__ void __launch_bounds__(128, 3) k_candidates(uint32_t slot, ResPlanes 
         next_hit(C, path);
         if (path.flags & kPHit)
         {
-            handle_hit(C, path);
+            handle_hit<kDirect>(C, path, currRec, i);
             while (path.flags & kPActive)
             {
                 next_hit(C, path);
-                if (path.flags & kPHit) handle_hit(C, path);
+                if (path.flags & kPHit) handle_hit<kDirect>(C, path, currRec, i);
                 else
                 {
                     // handleMiss (:1433-1524) without an environment map
@@ -370,9 +378,34 @@ __global__ void __launch_bounds__(128, 3) k_candidates(uint32_t slot, ResPlanes 
         ex.subPixel = selected ? path.rec.subPixel : ex.subPixel;
         ex.confidence = 1.f;
         store_res(curr, i, ex);
-        Recon exr = isFirstSample ? recon_default() : load_rec_rw(currRec, i);
-        store_rec(currRec, i, selected ? path.candRec : exr);
+        if (kDirect)
+        {
+            // the output holds the last selected candidate's record when one was selected
+            if (!(selected && path.anySelected)) store_rec(currRec, i, recon_default());
+        }
+        else
+        {
+            Recon exr = isFirstSample ? recon_default() : load_rec_rw(currRec, i);
+            store_rec(currRec, i, selected ? path.candRec : exr);
+        }
     }
+}
+
+__global__ void __launch_bounds__(128, 3) k_candidates(uint32_t slot, ResPlanes curr, RecPlanes currRec)
+{
+    const DevCtx& C = c_ctx[slot];
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= C.W * C.H) return;
+    candidates_pixel<false>(C, i, curr, currRec);
+}
+
+// One sample per pixel (the reference default): records go straight to the output planes.
+__global__ void __launch_bounds__(128, 4) k_candidates_direct(uint32_t slot, ResPlanes curr, RecPlanes currRec)
+{
+    const DevCtx& C = c_ctx[slot];
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= C.W * C.H) return;
+    candidates_pixel<true>(C, i, curr, currRec);
 }
 
 // ============================================================ forward reprojection (splat)

@@ -7,6 +7,7 @@ namespace rs {
 
 __global__ void k_vbuffer(uint32_t slot, uint4* vbuffer, float2* mvec);
 __global__ void k_candidates(uint32_t slot, ResPlanes curr, RecPlanes currRec);
+__global__ void k_candidates_direct(uint32_t slot, ResPlanes curr, RecPlanes currRec);
 __global__ void k_reproject(uint32_t slot, ResPlanes prev, RecPlanes prevRec, uint32_t* targets, uint32_t* counts);
 __global__ void k_multi_reproject(uint32_t slot, ResPlanes prev, RecPlanes prevRec, uint32_t* targets, uint32_t* counts);
 __global__ void k_scan_tiles(const uint32_t* in, uint32_t* out, uint32_t* tileSums, uint32_t n);

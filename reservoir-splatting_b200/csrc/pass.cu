@@ -502,7 +502,9 @@ static rs_status enqueue_frame(rs_pass* p, cudaStream_t s, float4* colorDev, con
     const float2* mvec = mvecIn ? mvecIn : p->mvec.p;
 
     stage(p, "initialCandidates", s);
-    k_candidates<<<grid(N, 128), 128, 0, s>>>(C, curr.res(), curr.recp()); p->launches++;
+    if (o.samplesPerPixel == 1) k_candidates_direct<<<grid(N, 128), 128, 0, s>>>(C, curr.res(), curr.recp());
+    else k_candidates<<<grid(N, 128), 128, 0, s>>>(C, curr.res(), curr.recp());
+    p->launches++;
     if (p->keepCandidates)
     {
         RS_CUDA(p->cand.ensure(N));
