@@ -411,7 +411,7 @@ __global__ void __launch_bounds__(128, 4) k_candidates_direct(uint32_t slot, Res
 // ============================================================ forward reprojection (splat)
 // ReprojectTemporalSamples.rt.slang:64-175.  Writes the destination cell of every source pixel
 // and counts splats per cell; the cell lists are built by k_fill / k_rank_cells.
-__global__ void __launch_bounds__(256) k_reproject(uint32_t slot, ResPlanes prev, RecPlanes prevRec,
+__global__ void __launch_bounds__(256, 4) k_reproject(uint32_t slot, ResPlanes prev, RecPlanes prevRec,
                                                    uint32_t* __restrict__ targets, uint32_t* __restrict__ counts)
 {
     const DevCtx& C = c_ctx[slot];

@@ -91,7 +91,7 @@ __device__ __forceinline__ Recon backup_rec(const WaveCtx& K, uint32_t bi)
 }
 
 // ---- stage 1: current sample -> previous domain by reprojection (ScatterBackup...:96-114)
-__global__ void __launch_bounds__(128) k_sb_curr_scatter(uint32_t slot, WaveCtx K)
+__global__ void __launch_bounds__(128, 8) k_sb_curr_scatter(uint32_t slot, WaveCtx K)
 {
     const DevCtx& C = c_ctx[slot];
     uint32_t ri = blockIdx.x * blockDim.x + threadIdx.x;
@@ -111,7 +111,7 @@ __global__ void __launch_bounds__(128) k_sb_curr_scatter(uint32_t slot, WaveCtx 
 }
 
 // ---- stage 1: current sample -> previous domain by the gather shift (:116-129)
-__global__ void __launch_bounds__(128) k_sb_curr_gather(uint32_t slot, WaveCtx K)
+__global__ void __launch_bounds__(128, 8) k_sb_curr_gather(uint32_t slot, WaveCtx K)
 {
     const DevCtx& C = c_ctx[slot];
     uint32_t ri = blockIdx.x * blockDim.x + threadIdx.x;
@@ -135,7 +135,7 @@ __global__ void __launch_bounds__(128) k_sb_curr_gather(uint32_t slot, WaveCtx K
 }
 
 // ---- stage 1: backup sample -> current domain (:156-166)
-__global__ void __launch_bounds__(128) k_sb_backup_gather(uint32_t slot, WaveCtx K)
+__global__ void __launch_bounds__(128, 8) k_sb_backup_gather(uint32_t slot, WaveCtx K)
 {
     const DevCtx& C = c_ctx[slot];
     uint32_t ri = blockIdx.x * blockDim.x + threadIdx.x;
@@ -159,7 +159,7 @@ __global__ void __launch_bounds__(128) k_sb_backup_gather(uint32_t slot, WaveCtx
 }
 
 // ---- stage 2 (Balance): updated backup -> previous domain by reprojection (:171-189)
-__global__ void __launch_bounds__(128) k_sb_backup_scatter(uint32_t slot, WaveCtx K)
+__global__ void __launch_bounds__(128, 8) k_sb_backup_scatter(uint32_t slot, WaveCtx K)
 {
     const DevCtx& C = c_ctx[slot];
     uint32_t ri = blockIdx.x * blockDim.x + threadIdx.x;
@@ -184,7 +184,7 @@ __global__ void __launch_bounds__(128) k_sb_backup_scatter(uint32_t slot, WaveCt
 }
 
 // ---- stage 1: splatted previous sample -> current domain (:218-235), one thread per splat
-__global__ void __launch_bounds__(128) k_sb_splat_scatter(uint32_t slot, WaveCtx K)
+__global__ void __launch_bounds__(128, 7) k_sb_splat_scatter(uint32_t slot, WaveCtx K)
 {
     const DevCtx& C = c_ctx[slot];
     uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -207,7 +207,7 @@ __global__ void __launch_bounds__(128) k_sb_splat_scatter(uint32_t slot, WaveCtx
 }
 
 // ---- stage 2 (Balance): updated splat -> previous domain by the gather shift (:237-253)
-__global__ void __launch_bounds__(128) k_sb_splat_gather(uint32_t slot, WaveCtx K)
+__global__ void __launch_bounds__(128, 8) k_sb_splat_gather(uint32_t slot, WaveCtx K)
 {
     const DevCtx& C = c_ctx[slot];
     uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -366,7 +366,7 @@ __device__ __forceinline__ bool spatial_neighbor(const DevCtx& C, uint32_t itera
     return valid_int(C, nx, ny);
 }
 
-__global__ void __launch_bounds__(128) k_sp_central(uint32_t slot, SpatialCtx S)
+__global__ void __launch_bounds__(128, 7) k_sp_central(uint32_t slot, SpatialCtx S)
 {
     const DevCtx& C = c_ctx[slot];
     uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -395,7 +395,7 @@ __global__ void __launch_bounds__(128) k_sp_central(uint32_t slot, SpatialCtx S)
     S.m1[t] = m1;
 }
 
-__global__ void __launch_bounds__(128) k_sp_neighbor(uint32_t slot, SpatialCtx S)
+__global__ void __launch_bounds__(128, 6) k_sp_neighbor(uint32_t slot, SpatialCtx S)
 {
     const DevCtx& C = c_ctx[slot];
     uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
