@@ -1,15 +1,17 @@
 // BVH construction on the GPU, once per rs_set_scene.
 //
-// 1. LBVH (Karras 2012, "Maximizing parallelism in the construction of BVHs, octrees, and k-d
-//    trees"): 63-bit Morton codes (21 bits per axis) of the triangle centroids, a key/index radix
-//    sort, the triangles gathered in key order, one thread per internal node to find its range and
-//    split, and a bottom-up box pass with per-node arrival counters.
+// 1. Binary tree: 63-bit Morton codes (21 bits per axis) of the triangle centroids, a key/index
+//    radix sort, the triangles gathered in key order, then PLOC clustering of the ordered leaves
+//    (below).  k_karras (Karras 2012, "Maximizing parallelism in the construction of BVHs, octrees,
+//    and k-d trees") is the LBVH alternative; k_refit is the bottom-up box pass with per-node
+//    arrival counters that refits either tree after geometry moves.
 // 2. Collapse of the binary tree (kept for closest-hit queries) into the 4-wide tree of bvh.cuh, top down, one thread per node
 //    and one launch per level: a node takes its binary node's two children and repeatedly opens
 //    the child of largest surface area that holds more than four triangles, up to four children;
 //    children of at most four triangles become leaves, which are ranges of the key-ordered
 //    triangles (the leaf-order array).
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 #include "bvh_build.h"
 
 namespace rs {
@@ -194,6 +196,91 @@ __global__ void k_refit(const float4* __restrict__ tri, const float4* __restrict
         if (node == 0) return;
         node = parent[node];
     }
+}
+
+// ------------------------------------------------------------------ PLOC (binary tree)
+// Parallel locally-ordered clustering (Meister & Bittner 2018): the key-ordered leaves start as
+// clusters; each round every cluster finds, among the kPlocRadius clusters on either side, the
+// one whose merged box has the smallest surface area; mutual nearest neighbours merge into a new
+// node; the clusters are compacted in order.  Node indices come from prefix sums of the merges,
+// counting down from n - 2, so the numbering is deterministic and the last merge is the root, node 0.
+constexpr int kPlocRadius = 24;
+
+struct ClusterBox { float4 lo, hi; }; // lo.w = reference bits (kLeafBit | leaf, or node), hi.w = triangle count
+
+__global__ void k_ploc_init(const float4* __restrict__ sorted, uint32_t n, ClusterBox* __restrict__ cl)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float lo[3], hi[3];
+    tri_box(sorted, i, lo, hi);
+    cl[i].lo = make_float4(lo[0], lo[1], lo[2], __uint_as_float(kLeafBit | i));
+    cl[i].hi = make_float4(hi[0], hi[1], hi[2], __uint_as_float(1u));
+}
+
+__device__ __forceinline__ float union_area(const ClusterBox& a, const ClusterBox& b)
+{
+    float dx = fmaxf(a.hi.x, b.hi.x) - fminf(a.lo.x, b.lo.x);
+    float dy = fmaxf(a.hi.y, b.hi.y) - fminf(a.lo.y, b.lo.y);
+    float dz = fmaxf(a.hi.z, b.hi.z) - fminf(a.lo.z, b.lo.z);
+    return dx * dy + dy * dz + dz * dx;
+}
+
+// Nearest neighbour of every cluster within the window; ties go to the lower index.
+__global__ void k_ploc_nn(const ClusterBox* __restrict__ cl, uint32_t c, uint32_t* __restrict__ nn)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c) return;
+    const ClusterBox me = cl[i];
+    const uint32_t lo = i > (uint32_t)kPlocRadius ? i - kPlocRadius : 0u;
+    const uint32_t hi = i + kPlocRadius < c - 1 ? i + kPlocRadius : c - 1;
+    float best = 3e38f;
+    uint32_t arg = i == 0 ? 1u : i - 1;
+    for (uint32_t j = lo; j <= hi; j++)
+    {
+        if (j == i) continue;
+        const float a = union_area(me, cl[j]);
+        if (a < best) { best = a; arg = j; }
+    }
+    nn[i] = arg;
+}
+
+// merge[i]: i is the lower partner of a mutual pair (it creates the node); keep[i]: i survives the
+// round (everything but the upper partner of a mutual pair).
+__global__ void k_ploc_flags(const uint32_t* __restrict__ nn, uint32_t c, uint32_t* __restrict__ merge, uint32_t* __restrict__ keep)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c) return;
+    const uint32_t j = nn[i];
+    const bool mutual = nn[j] == i;
+    merge[i] = (mutual && i < j) ? 1u : 0u;
+    keep[i] = (mutual && i > j) ? 0u : 1u;
+}
+
+__global__ void k_ploc_merge(const ClusterBox* __restrict__ cl, uint32_t c, const uint32_t* __restrict__ nn, const uint32_t* __restrict__ merge,
+                             const uint32_t* __restrict__ mergeOff, const uint32_t* __restrict__ keep, const uint32_t* __restrict__ keepOff,
+                             uint32_t top, ClusterBox* __restrict__ out, float4* __restrict__ nodes, uint2* __restrict__ range,
+                             uint32_t* __restrict__ parent, uint32_t* __restrict__ leafParent)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c || !keep[i]) return;
+    ClusterBox a = cl[i];
+    if (merge[i])
+    {
+        const ClusterBox b = cl[nn[i]];
+        const uint32_t node = top - mergeOff[i];
+        const uint32_t ra = __float_as_uint(a.lo.w), rb = __float_as_uint(b.lo.w);
+        float4* o = nodes + 4 * (size_t)node;
+        o[0] = a.lo; o[1] = make_float4(a.hi.x, a.hi.y, a.hi.z, __uint_as_float(rb));
+        o[2] = make_float4(b.lo.x, b.lo.y, b.lo.z, 0.f); o[3] = make_float4(b.hi.x, b.hi.y, b.hi.z, 0.f);
+        const uint32_t count = __float_as_uint(a.hi.w) + __float_as_uint(b.hi.w);
+        range[node] = make_uint2(0u, count - 1u); // only the triangle count is used for internal nodes
+        if (ra & kLeafBit) leafParent[ra & ~kLeafBit] = node; else parent[ra] = node;
+        if (rb & kLeafBit) leafParent[rb & ~kLeafBit] = node; else parent[rb] = node;
+        a.lo = make_float4(fminf(a.lo.x, b.lo.x), fminf(a.lo.y, b.lo.y), fminf(a.lo.z, b.lo.z), __uint_as_float(node));
+        a.hi = make_float4(fmaxf(a.hi.x, b.hi.x), fmaxf(a.hi.y, b.hi.y), fmaxf(a.hi.z, b.hi.z), __uint_as_float(count));
+    }
+    out[keepOff[i]] = a;
 }
 
 // ------------------------------------------------------------------ collapse to the 4-wide tree
@@ -443,9 +530,43 @@ cudaError_t build_wide_bvh(const float4* dTri, uint32_t n, WideBvh* out, cudaStr
             RS_TRY(cudaMalloc(&parent, n * 4ull)); RS_TRY(cudaMalloc(&leafParent, n * 4ull)); RS_TRY(cudaMalloc(&arrivals, n * 4ull));
             RS_TRY(cudaMalloc(&qa, 8ull * maxWide)); RS_TRY(cudaMalloc(&qb, 8ull * maxWide));
             RS_TRY(cudaMemsetAsync(nodes, 0, 64ull * (n - 1), s));
-            k_karras<<<(n - 1 + 255) / 256, 256, 0, s>>>(keys2, (int)n, nodes, range, parent, leafParent);
-            RS_TRY(cudaMemsetAsync(arrivals, 0, n * 4ull, s));
-            k_refit<<<(n + 255) / 256, 256, 0, s>>>(sorted, nullptr, (int)n, nodes, parent, leafParent, arrivals);
+            {
+                // PLOC over the key-ordered leaves (node 0 = root); the binary tree the rest uses
+                ClusterBox *ca = nullptr, *cb = nullptr;
+                uint32_t *nn = nullptr, *mflag = nullptr, *kflag = nullptr, *moff = nullptr, *koff = nullptr;
+                void* stemp = nullptr;
+                size_t stempBytes = 0;
+                RS_TRY(cudaMalloc(&ca, 32ull * n)); RS_TRY(cudaMalloc(&cb, 32ull * n));
+                RS_TRY(cudaMalloc(&nn, 4ull * n)); RS_TRY(cudaMalloc(&mflag, 4ull * n)); RS_TRY(cudaMalloc(&kflag, 4ull * n));
+                RS_TRY(cudaMalloc(&moff, 4ull * n)); RS_TRY(cudaMalloc(&koff, 4ull * n));
+                RS_TRY(cub::DeviceScan::ExclusiveSum(nullptr, stempBytes, mflag, moff, (int)n, s));
+                RS_TRY(cudaMalloc(&stemp, stempBytes));
+                k_ploc_init<<<(n + 255) / 256, 256, 0, s>>>(sorted, n, ca);
+                uint32_t c = n, top = n - 2;
+                while (c > 1 && e == cudaSuccess)
+                {
+                    k_ploc_nn<<<(c + 127) / 128, 128, 0, s>>>(ca, c, nn);
+                    k_ploc_flags<<<(c + 255) / 256, 256, 0, s>>>(nn, c, mflag, kflag);
+                    e = cub::DeviceScan::ExclusiveSum(stemp, stempBytes, mflag, moff, (int)c, s);
+                    if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(stemp, stempBytes, kflag, koff, (int)c, s);
+                    uint32_t tail[4] = {0, 0, 0, 0};
+                    if (e == cudaSuccess) e = cudaMemcpyAsync(&tail[0], moff + c - 1, 4, cudaMemcpyDeviceToHost, s);
+                    if (e == cudaSuccess) e = cudaMemcpyAsync(&tail[1], mflag + c - 1, 4, cudaMemcpyDeviceToHost, s);
+                    if (e == cudaSuccess) e = cudaMemcpyAsync(&tail[2], koff + c - 1, 4, cudaMemcpyDeviceToHost, s);
+                    if (e == cudaSuccess) e = cudaMemcpyAsync(&tail[3], kflag + c - 1, 4, cudaMemcpyDeviceToHost, s);
+                    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+                    if (e != cudaSuccess) break;
+                    const uint32_t merges = tail[0] + tail[1], kept = tail[2] + tail[3];
+                    if (merges == 0 || kept + merges != c) { e = cudaErrorUnknown; break; } // a round always merges the globally closest pair
+                    k_ploc_merge<<<(c + 255) / 256, 256, 0, s>>>(ca, c, nn, mflag, moff, kflag, koff, top, cb, nodes, range, parent, leafParent);
+                    e = cudaGetLastError();
+                    top -= merges;
+                    c = kept;
+                    std::swap(ca, cb);
+                }
+                cudaFree(ca); cudaFree(cb); cudaFree(nn); cudaFree(mflag); cudaFree(kflag); cudaFree(moff); cudaFree(koff); cudaFree(stemp);
+                if (e != cudaSuccess) goto done;
+            }
             const uint2 root = make_uint2(0u, 0u);
             const uint32_t one = 1u;
             RS_TRY(cudaMemcpyAsync(qa, &root, sizeof(root), cudaMemcpyHostToDevice, s));
