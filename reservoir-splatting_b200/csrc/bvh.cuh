@@ -2,7 +2,8 @@
 // (SceneRayQuery::traceRay / traceVisibilityRay, Scene/RaytracingInline.slang:86-362): two trees
 // over the same triangles, each serving the query it traverses fastest.
 //
-// Closest hit: the binary LBVH, 64 bytes per internal node (four float4):
+// Closest hit: the binary tree (PLOC clustering of the Morton-ordered leaves), 64 bytes per
+// internal node (four float4):
 //   [0] left child box lo.xyz, left child reference   [1] left child box hi.xyz, right child reference
 //   [2] right child box lo.xyz                         [3] right child box hi.xyz
 // A reference with kLeafBit set is a single-triangle leaf (its position in the leaf-order array).
@@ -21,7 +22,7 @@
 // when its entry distance is within 2e-6 |exit distance| of the exit, so a box test only prunes
 // triangles the exact intersection test rejects: the slab distances are off by a few ulp of the
 // box coordinate (inside the padding) and of t (inside the slack).  A zero direction component
-// uses 1/d = +-1e20 in the 4-wide test, so its products stay finite and NaN-free.
+// uses 1/d = +-1e20, so the products stay finite and NaN-free.
 // The closest hit is the (t, scene index) minimum over all triangles and does not depend on the
 // tree; shading reads the scene-order triangle array.
 #pragma once
@@ -107,24 +108,17 @@ __device__ __forceinline__ bool leaf_tri_test(const float4* __restrict__ leafTri
 
 struct TraceHit { uint32_t prim; float t, u, v; };
 
-// Binary-node box test in the plain slab form (as the build's boxes were padded for).
-__device__ __forceinline__ void slab_interval(float lo, float hi, float o, float inv, float& t0, float& t1)
+// Binary-node box test: slab distances t = box * (1/d) - o * (1/d) by fma, entry as the 3-way
+// max of the near planes (and 0), exit as the 3-way min of the far planes (and tmax).
+__device__ __forceinline__ bool box_hit(float4 lo, float4 hi, const RayQ& r, float tmax, float& tEntry)
 {
-    float a = (lo - o) * inv, b = (hi - o) * inv;
-    if (a != a) a = -3e38f; // (0 * inf): origin on the slab plane, direction parallel
-    if (b != b) b = 3e38f;
-    t0 = fmaxf(t0, fminf(a, b));
-    t1 = fminf(t1, fmaxf(a, b));
-}
-
-__device__ __forceinline__ bool box_hit(float4 lo, float4 hi, f3 o, f3 inv, float tmax, float& tEntry)
-{
-    float t0 = 0.f, t1 = tmax;
-    slab_interval(lo.x, hi.x, o.x, inv.x, t0, t1);
-    slab_interval(lo.y, hi.y, o.y, inv.y, t0, t1);
-    slab_interval(lo.z, hi.z, o.z, inv.z, t0, t1);
+    const float ax = __fmaf_rn(lo.x, r.ix, -r.ox_ix), bx = __fmaf_rn(hi.x, r.ix, -r.ox_ix);
+    const float ay = __fmaf_rn(lo.y, r.iy, -r.oy_iy), by = __fmaf_rn(hi.y, r.iy, -r.oy_iy);
+    const float az = __fmaf_rn(lo.z, r.iz, -r.oz_iz), bz = __fmaf_rn(hi.z, r.iz, -r.oz_iz);
+    const float t0 = max3f(fminf(ax, bx), fminf(ay, by), fmaxf(fminf(az, bz), 0.f));
+    const float t1 = min3f(fmaxf(ax, bx), fmaxf(ay, by), fminf(fmaxf(az, bz), tmax));
     tEntry = t0;
-    return t0 <= t1 + 2e-6f * fabsf(t1);
+    return t0 <= __fmaf_rn(2e-6f, fabsf(t1), t1);
 }
 
 // Closest hit on (tMin, tMax) over the binary tree; ties on t go to the lower scene triangle index;
@@ -134,7 +128,7 @@ __device__ __forceinline__ bool box_hit(float4 lo, float4 hi, f3 o, f3 inv, floa
 template <bool kCount>
 __device__ __forceinline__ TraceHit trace_closest_bin(const BvhView& bv, const Ray& r, uint32_t* overflow, uint32_t* counts = nullptr)
 {
-    const f3 inv = mk3(1.f / r.dir.x, 1.f / r.dir.y, 1.f / r.dir.z);
+    const RayQ q = make_rayq(r);
     TraceHit best;
     best.prim = kInvalidIndex; best.t = r.tMax; best.u = 0.f; best.v = 0.f;
     uint32_t stack[kTraversalStack];
@@ -164,8 +158,8 @@ __device__ __forceinline__ TraceHit trace_closest_bin(const BvhView& bv, const R
         const float4* n = bv.binNodes + 4 * (size_t)node;
         const float4 l0 = __ldg(n + 0), l1 = __ldg(n + 1), r0 = __ldg(n + 2), r1 = __ldg(n + 3);
         float tl, tr;
-        const bool hl = box_hit(l0, l1, r.origin, inv, best.t, tl);
-        const bool hr = box_hit(r0, r1, r.origin, inv, best.t, tr);
+        const bool hl = box_hit(l0, l1, q, best.t, tl);
+        const bool hr = box_hit(r0, r1, q, best.t, tr);
         const uint32_t cl = __float_as_uint(l0.w), cr = __float_as_uint(l1.w);
         if (hl && hr)
         {
