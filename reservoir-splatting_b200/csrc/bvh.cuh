@@ -239,6 +239,13 @@ __device__ __forceinline__ bool trace_closest(const BvhView& bv, const Ray& r, H
     return true;
 }
 
+// The closest-hit traversal as a call: one copy in kernels with several ray sites and many live
+// values around them (the path tracer), where inlining it raises register pressure.
+static __device__ __noinline__ TraceHit trace_closest_call(BvhView bv, Ray r, uint32_t* overflow)
+{
+    return trace_closest_bin<false>(bv, r, overflow);
+}
+
 __device__ __forceinline__ bool trace_visible(const BvhView& bv, const Ray& r, uint32_t* overflow)
 {
     if (bv.numTris == 0) return true;

@@ -100,7 +100,8 @@ __device__ __forceinline__ void next_hit(const DevCtx& C, PState& p) // PathTrac
 {
     p.vertex += 1;
     HitInfo h; float t;
-    if (trace_closest(C.bvh, mk_ray(p.origin, p.dir, 0.f, kRayTMax), h, t, C.fault)) { p.hit = h; p.flags |= kPHit; }
+    const TraceHit th = C.bvh.numTris ? trace_closest_call(C.bvh, mk_ray(p.origin, p.dir, 0.f, kRayTMax), C.fault) : TraceHit{kInvalidIndex, 0.f, 0.f, 0.f};
+    if (th.prim != kInvalidIndex) { h = hit_tri(th.prim, th.u, th.v); t = th.t; p.hit = h; p.flags |= kPHit; }
     else p.flags &= ~kPHit;
 }
 

@@ -346,9 +346,9 @@ __device__ inline Shifted dev_gather_lens_copy(const DevCtx& C, SampleGen sg, co
     path.thp = mk3(1.f);
     path.dir = cr.dir;
     path.active = true;
-    float tHit;
-    bool isHit = trace_closest(C.bvh, mk_ray(cr.origin, cr.dir, 0.f, kRayTMax), path.hit, tHit, C.fault);
-    if (!isHit) path.hit = hit_none();
+    const TraceHit th = C.bvh.numTris ? trace_closest_call(C.bvh, mk_ray(cr.origin, cr.dir, 0.f, kRayTMax), C.fault) : TraceHit{kInvalidIndex, 0.f, 0.f, 0.f};
+    const bool isHit = th.prim != kInvalidIndex;
+    path.hit = isHit ? hit_tri(th.prim, th.u, th.v) : hit_none();
     path.origin = camera_lens_point_scaled(cam, lensSample);
     f3 camDir = normalize(cam.cameraW);
     Shifted sp = shifted_default();
