@@ -128,7 +128,7 @@ STAGE_BYTES_PER_PIXEL = {
     "reproject": 16 + 8 + 16 + T + 4 + 4,
     "sortCells": 4 * 8,
 }
-STAGE_KERNEL = {"initialCandidates": "k_candidates", "sbCombine": "k_sb_combine", "sbBackupScatter": "k_sb_backup_scatter",
+STAGE_KERNEL = {"initialCandidates": "k_candidates_direct", "sbCombine": "k_sb_combine", "sbBackupScatter": "k_sb_backup_scatter",
                 "spatialNeighbor": "k_sp_neighbor", "sortCells": "k_rank_cells"}
 
 
