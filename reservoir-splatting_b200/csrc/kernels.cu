@@ -25,8 +25,8 @@ cudaError_t upload_ctx(uint32_t slot, const DevCtx* hostPinned, cudaStream_t s)
 __global__ void __launch_bounds__(256) k_vbuffer(uint32_t slot, uint4* __restrict__ vbuffer, float2* __restrict__ mvec)
 {
     const DevCtx& C = c_ctx[slot];
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= C.W * C.H) return;
+    uint32_t i;
+    if (!tiled_pixel(C.W, C.H, i)) return;
     uint32_t x = i % C.W, y = i / C.W;
     const CameraData& cam = C.camera;
     const CameraData& pc = C.prevCamera;
@@ -404,8 +404,8 @@ __global__ void __launch_bounds__(128, 3) k_candidates(uint32_t slot, ResPlanes 
 __global__ void __launch_bounds__(128, 4) k_candidates_direct(uint32_t slot, ResPlanes curr, RecPlanes currRec)
 {
     const DevCtx& C = c_ctx[slot];
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= C.W * C.H) return;
+    uint32_t i;
+    if (!tiled_pixel(C.W, C.H, i)) return;
     candidates_pixel<true>(C, i, curr, currRec);
 }
 
@@ -416,8 +416,8 @@ __global__ void __launch_bounds__(256, 4) k_reproject(uint32_t slot, ResPlanes p
                                                    uint32_t* __restrict__ targets, uint32_t* __restrict__ counts)
 {
     const DevCtx& C = c_ctx[slot];
-    uint32_t ci = blockIdx.x * blockDim.x + threadIdx.x;
-    if (ci >= C.W * C.H) return;
+    uint32_t ci;
+    if (!tiled_pixel(C.W, C.H, ci)) return;
     uint32_t target = kInvalidIndex;
     f3 integrand = load_integrand(prev, ci);
     if (!all_eq0(integrand))

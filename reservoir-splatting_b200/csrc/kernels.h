@@ -33,6 +33,13 @@ __global__ void k_grad_flush(const double* acc, float* grad, uint32_t n);
 constexpr uint32_t kAdjointThreads = 128;        // k_backward block size
 constexpr uint32_t kAdjointSharedDoubles = 6016; // k_backward stages numMaterials x 8 sums in shared memory up to this (47 KB)
 
+// Blocks of `threads` (a multiple of 64) covering a W x H image for tiled_pixel.
+inline uint32_t tiled_blocks(uint32_t W, uint32_t H, uint32_t threads)
+{
+    const uint32_t rows = (threads / 32u) * 2u;
+    return ((W + 15u) / 16u) * ((H + rows - 1u) / rows);
+}
+
 constexpr uint32_t kMaxPassSlots = 64; // passes alive at once (size of the constant context table)
 cudaError_t upload_ctx(uint32_t slot, const DevCtx* hostPinned, cudaStream_t s);
 

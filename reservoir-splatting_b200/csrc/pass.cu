@@ -498,11 +498,11 @@ static rs_status enqueue_frame(rs_pass* p, cudaStream_t s, float4* colorDev, con
 
     // producer side: primary hits + motion vectors (VBufferRT)
     stage(p, "vbuffer", s);
-    k_vbuffer<<<grid(N, 256), 256, 0, s>>>(C, p->vbuffer.p, p->mvec.p); p->launches++;
+    k_vbuffer<<<tiled_blocks(W, H, 256), 256, 0, s>>>(C, p->vbuffer.p, p->mvec.p); p->launches++;
     const float2* mvec = mvecIn ? mvecIn : p->mvec.p;
 
     stage(p, "initialCandidates", s);
-    if (o.samplesPerPixel == 1) k_candidates_direct<<<grid(N, 128), 128, 0, s>>>(C, curr.res(), curr.recp());
+    if (o.samplesPerPixel == 1) k_candidates_direct<<<tiled_blocks(W, H, 128), 128, 0, s>>>(C, curr.res(), curr.recp());
     else k_candidates<<<grid(N, 128), 128, 0, s>>>(C, curr.res(), curr.recp());
     p->launches++;
     if (p->keepCandidates)
@@ -549,7 +549,7 @@ static rs_status enqueue_frame(rs_pass* p, cudaStream_t s, float4* colorDev, con
             stage(p, "reproject", s);
             RS_CUDA(cudaMemsetAsync(p->counts.p, 0, N * 4ull, s));
             RS_CUDA(cudaMemsetAsync(p->cursor.p, 0, N * 4ull, s));
-            k_reproject<<<grid(N, 256), 256, 0, s>>>(C, prev.res(), prev.recp(), p->targets.p, p->counts.p); p->launches++;
+            k_reproject<<<tiled_blocks(W, H, 256), 256, 0, s>>>(C, prev.res(), prev.recp(), p->targets.p, p->counts.p); p->launches++;
             stage(p, "sortCells", s);
             buildCells(p->targets.p, p->counts.p, p->offsets.p, p->cursor.p, p->unsortedSplats.p, p->sortedSplats.p, nullptr);
             stage(p, "scatterResample", s);
@@ -572,7 +572,7 @@ static rs_status enqueue_frame(rs_pass* p, cudaStream_t s, float4* colorDev, con
             stage(p, "reproject", s);
             RS_CUDA(cudaMemsetAsync(p->counts.p, 0, N * 4ull, s));
             RS_CUDA(cudaMemsetAsync(p->cursor.p, 0, N * 4ull, s));
-            k_reproject<<<grid(N, 256), 256, 0, s>>>(C, prev.res(), prev.recp(), p->targets.p, p->counts.p); p->launches++;
+            k_reproject<<<tiled_blocks(W, H, 256), 256, 0, s>>>(C, prev.res(), prev.recp(), p->targets.p, p->counts.p); p->launches++;
             stage(p, "sortCells", s);
             buildCells(p->targets.p, p->counts.p, p->offsets.p, p->cursor.p, p->unsortedSplats.p, p->sortedSplats.p, p->sortedCell.p);
             WaveCtx K;
@@ -589,24 +589,24 @@ static rs_status enqueue_frame(rs_pass* p, cudaStream_t s, float4* colorDev, con
             K.splatShift = ShiftPlanes{p->splatShift.p, (size_t)N}; K.splatTerms = p->splatTerms.p; K.splatM = p->splatM.p;
             const bool balance = o.scatterBackupMISOption == RS_MIS_BALANCE;
             stage(p, "sbCurrScatter", s);
-            k_sb_curr_scatter<<<grid(N, 128), 128, 0, s>>>(C, K);
+            k_sb_curr_scatter<<<tiled_blocks(W, H, 128), 128, 0, s>>>(C, K);
             stage(p, "sbCurrGather", s);
-            k_sb_curr_gather<<<grid(N, 128), 128, 0, s>>>(C, K);
+            k_sb_curr_gather<<<tiled_blocks(W, H, 128), 128, 0, s>>>(C, K);
             stage(p, "sbBackupGather", s);
-            k_sb_backup_gather<<<grid(N, 128), 128, 0, s>>>(C, K);
+            k_sb_backup_gather<<<tiled_blocks(W, H, 128), 128, 0, s>>>(C, K);
             stage(p, "sbSplatScatter", s);
             k_sb_splat_scatter<<<grid(N, 128), 128, 0, s>>>(C, K);
             p->launches += 4;
             if (balance)
             {
                 stage(p, "sbBackupScatter", s);
-                k_sb_backup_scatter<<<grid(N, 128), 128, 0, s>>>(C, K);
+                k_sb_backup_scatter<<<tiled_blocks(W, H, 128), 128, 0, s>>>(C, K);
                 stage(p, "sbSplatGather", s);
                 k_sb_splat_gather<<<grid(N, 128), 128, 0, s>>>(C, K);
                 p->launches += 2;
             }
             stage(p, "sbCombine", s);
-            k_sb_combine<<<grid(N, 128), 128, 0, s>>>(C, K, temporalColor);
+            k_sb_combine<<<tiled_blocks(W, H, 128), 128, 0, s>>>(C, K, temporalColor);
             p->launches++;
             break;
         }
@@ -653,11 +653,11 @@ static rs_status enqueue_frame(rs_pass* p, cudaStream_t s, float4* colorDev, con
             S.shift = ShiftPlanes{p->spShift.p, (size_t)N * o.neighborCount};
             const uint32_t M = N * o.neighborCount;
             stage(p, "spatialCentral", s);
-            k_sp_central<<<grid(M, 128), 128, 0, s>>>(C, S);
+            k_sp_central<<<dim3(tiled_blocks(W, H, 128), o.neighborCount), 128, 0, s>>>(C, S);
             stage(p, "spatialNeighbor", s);
-            k_sp_neighbor<<<grid(M, 128), 128, 0, s>>>(C, S);
+            k_sp_neighbor<<<dim3(tiled_blocks(W, H, 128), o.neighborCount), 128, 0, s>>>(C, S);
             stage(p, "spatialCombine", s);
-            k_sp_combine<<<grid(N, 128), 128, 0, s>>>(C, S, i + 1 == o.numSpatialIterations ? colorDev : nullptr);
+            k_sp_combine<<<tiled_blocks(W, H, 128), 128, 0, s>>>(C, S, i + 1 == o.numSpatialIterations ? colorDev : nullptr);
             p->launches += 2;
             p->launches++;
         }

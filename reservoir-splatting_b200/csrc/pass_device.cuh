@@ -46,6 +46,23 @@ __device__ __forceinline__ uint32_t pass_seed(const DevCtx& C, uint32_t k)
 __device__ __forceinline__ bool valid_float(const DevCtx& C, f2 p) { return p.x >= 0.f && p.y >= 0.f && p.x < (float)C.W && p.y < (float)C.H; }
 __device__ __forceinline__ bool valid_int(const DevCtx& C, int x, int y) { return x >= 0 && y >= 0 && x < (int)C.W && y < (int)C.H; }
 
+// Pixel of this thread when each warp covers an 8 x 4 pixel tile and the warps of a block sit two
+// tiles wide (a 128-thread block covers 16 x 8 pixels): a warp's primary rays leave from a compact
+// patch, so their traversals share more nodes and cache lines than a 32 x 1 row.  Launch with
+// tiled_blocks().  False for threads past the image edge.
+__device__ __forceinline__ bool tiled_pixel(uint32_t W, uint32_t H, uint32_t& i)
+{
+    const uint32_t rowsPerBlock = (blockDim.x >> 5) * 2u;
+    const uint32_t tilesX = (W + 15u) / 16u;
+    const uint32_t bx = blockIdx.x % tilesX, by = blockIdx.x / tilesX;
+    const uint32_t w = threadIdx.x >> 5, l = threadIdx.x & 31u;
+    const uint32_t x = bx * 16u + (w & 1u) * 8u + (l & 7u);
+    const uint32_t y = by * rowsPerBlock + (w >> 1) * 4u + (l >> 3);
+    if (x >= W || y >= H) return false;
+    i = y * W + x;
+    return true;
+}
+
 __device__ __forceinline__ bool dev_visible(const DevCtx& C, const Ray& r) { return trace_visible(C.bvh, r, C.fault); }
 __device__ __forceinline__ ShadingData dev_sd(const DevCtx& C, const HitInfo& h, f3 rayDir)
 {

@@ -94,8 +94,8 @@ __device__ __forceinline__ Recon backup_rec(const WaveCtx& K, uint32_t bi)
 __global__ void __launch_bounds__(128, 8) k_sb_curr_scatter(uint32_t slot, WaveCtx K)
 {
     const DevCtx& C = c_ctx[slot];
-    uint32_t ri = blockIdx.x * blockDim.x + threadIdx.x;
-    if (ri >= C.W * C.H) return;
+    uint32_t ri;
+    if (!tiled_pixel(C.W, C.H, ri)) return;
     f3 integrand = load_integrand(K.curr, ri);
     if (!any_gt0(integrand)) return;
     Recon crd = load_rec_rw(K.currRec, ri);
@@ -114,8 +114,8 @@ __global__ void __launch_bounds__(128, 8) k_sb_curr_scatter(uint32_t slot, WaveC
 __global__ void __launch_bounds__(128, 8) k_sb_curr_gather(uint32_t slot, WaveCtx K)
 {
     const DevCtx& C = c_ctx[slot];
-    uint32_t ri = blockIdx.x * blockDim.x + threadIdx.x;
-    if (ri >= C.W * C.H) return;
+    uint32_t ri;
+    if (!tiled_pixel(C.W, C.H, ri)) return;
     Res cr = load_res_rw(K.curr, ri);
     if (!any_gt0(cr.integrand)) return;
     uint32_t x = ri % C.W, y = ri / C.W;
@@ -138,8 +138,8 @@ __global__ void __launch_bounds__(128, 8) k_sb_curr_gather(uint32_t slot, WaveCt
 __global__ void __launch_bounds__(128, 8) k_sb_backup_gather(uint32_t slot, WaveCtx K)
 {
     const DevCtx& C = c_ctx[slot];
-    uint32_t ri = blockIdx.x * blockDim.x + threadIdx.x;
-    if (ri >= C.W * C.H) return;
+    uint32_t ri;
+    if (!tiled_pixel(C.W, C.H, ri)) return;
     uint32_t x = ri % C.W, y = ri / C.W;
     Res br; uint32_t bi; f2 fc;
     backup_of(C, K, ri, x, y, br, bi, fc);
@@ -162,8 +162,8 @@ __global__ void __launch_bounds__(128, 8) k_sb_backup_gather(uint32_t slot, Wave
 __global__ void __launch_bounds__(128, 8) k_sb_backup_scatter(uint32_t slot, WaveCtx K)
 {
     const DevCtx& C = c_ctx[slot];
-    uint32_t ri = blockIdx.x * blockDim.x + threadIdx.x;
-    if (ri >= C.W * C.H) return;
+    uint32_t ri;
+    if (!tiled_pixel(C.W, C.H, ri)) return;
     uint32_t x = ri % C.W, y = ri / C.W;
     Res br; uint32_t bi; f2 fc;
     backup_of(C, K, ri, x, y, br, bi, fc);
@@ -241,8 +241,8 @@ __global__ void __launch_bounds__(128, 8) k_sb_splat_gather(uint32_t slot, WaveC
 __global__ void __launch_bounds__(128) k_sb_combine(uint32_t slot, WaveCtx K, float4* __restrict__ color)
 {
     const DevCtx& C = c_ctx[slot];
-    uint32_t ri = blockIdx.x * blockDim.x + threadIdx.x;
-    if (ri >= C.W * C.H) return;
+    uint32_t ri;
+    if (!tiled_pixel(C.W, C.H, ri)) return;
     uint32_t x = ri % C.W, y = ri / C.W;
     const bool useConf = C.useConfTemporal != 0;
     const bool balance = C.scatterBackupMIS == 0u;
@@ -369,10 +369,11 @@ __device__ __forceinline__ bool spatial_neighbor(const DevCtx& C, uint32_t itera
 __global__ void __launch_bounds__(128, 7) k_sp_central(uint32_t slot, SpatialCtx S)
 {
     const DevCtx& C = c_ctx[slot];
-    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    // blockIdx.y: the neighbour; blockIdx.x / threadIdx.x: the pixel (tiled)
     const uint32_t N = C.W * C.H;
-    if (t >= N * C.neighborCount) return;
-    uint32_t i = t / N, ri = t % N;
+    uint32_t ri;
+    if (blockIdx.y >= C.neighborCount || !tiled_pixel(C.W, C.H, ri)) return;
+    const uint32_t i = blockIdx.y, t = i * N + ri;
     uint32_t x = ri % C.W, y = ri / C.W;
     int nx, ny;
     if (!spatial_neighbor(C, S.iteration, S.neighborOffsets, x, y, i, nx, ny)) return;
@@ -398,10 +399,11 @@ __global__ void __launch_bounds__(128, 7) k_sp_central(uint32_t slot, SpatialCtx
 __global__ void __launch_bounds__(128, 6) k_sp_neighbor(uint32_t slot, SpatialCtx S)
 {
     const DevCtx& C = c_ctx[slot];
-    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    // blockIdx.y: the neighbour; blockIdx.x / threadIdx.x: the pixel (tiled)
     const uint32_t N = C.W * C.H;
-    if (t >= N * C.neighborCount) return;
-    uint32_t i = t / N, ri = t % N;
+    uint32_t ri;
+    if (blockIdx.y >= C.neighborCount || !tiled_pixel(C.W, C.H, ri)) return;
+    const uint32_t i = blockIdx.y, t = i * N + ri;
     uint32_t x = ri % C.W, y = ri / C.W;
     int nx, ny;
     if (!spatial_neighbor(C, S.iteration, S.neighborOffsets, x, y, i, nx, ny)) return;
@@ -428,9 +430,9 @@ __global__ void __launch_bounds__(128, 6) k_sp_neighbor(uint32_t slot, SpatialCt
 __global__ void __launch_bounds__(128) k_sp_combine(uint32_t slot, SpatialCtx S, float4* __restrict__ color)
 {
     const DevCtx& C = c_ctx[slot];
-    uint32_t ri = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t ri;
     const uint32_t N = C.W * C.H;
-    if (ri >= N) return;
+    if (!tiled_pixel(C.W, C.H, ri)) return;
     uint32_t x = ri % C.W, y = ri / C.W;
     const bool useConf = C.useConfSpatial != 0;
     const uint32_t neighborCount = C.neighborCount;
