@@ -458,9 +458,9 @@ __global__ void __launch_bounds__(256) k_multi_reproject(uint32_t slot, ResPlane
                                                          uint32_t* __restrict__ targets, uint32_t* __restrict__ counts)
 {
     const DevCtx& C = c_ctx[slot];
-    uint32_t ci = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t ci;
     const uint32_t N = C.W * C.H;
-    if (ci >= N) return;
+    if (!tiled_pixel(C.W, C.H, ci)) return;
     const uint32_t P = C.numTimePartitions;
     for (uint32_t i = 0; i < P; i++) targets[(size_t)i * N + ci] = kInvalidIndex;
     f3 integrand = load_integrand(prev, ci);
@@ -624,13 +624,13 @@ __device__ __forceinline__ f2 prev_pixel_from_mvec(const DevCtx& C, const float2
     return mk2((float)x + mv.x * (float)C.W, (float)y + mv.y * (float)C.H);
 }
 
-__global__ void __launch_bounds__(128) k_collect(uint32_t slot, const float2* __restrict__ mvec, ResPlanes prev, RecPlanes prevRec,
+__global__ void __launch_bounds__(128, 4) k_collect(uint32_t slot, const float2* __restrict__ mvec, ResPlanes prev, RecPlanes prevRec,
                                                  ResPlanes inter, RecPlanes interRec, float2* __restrict__ floatingCoords,
                                                  const Shifted* __restrict__ shiftedPaths)
 {
     const DevCtx& C = c_ctx[slot];
-    uint32_t ci = blockIdx.x * blockDim.x + threadIdx.x;
-    if (ci >= C.W * C.H) return;
+    uint32_t ci;
+    if (!tiled_pixel(C.W, C.H, ci)) return;
     uint32_t x = ci % C.W, y = ci / C.W;
     const bool useConf = C.useConfTemporal != 0;
     SampleGen sg = sg_create(x, y, pass_seed(C, 2), C.sgKind);
@@ -760,11 +760,11 @@ __global__ void __launch_bounds__(128) k_collect(uint32_t slot, const float2* __
 }
 
 // RobustReuseOptimization.rt.slang:63-89
-__global__ void __launch_bounds__(128) k_robust(uint32_t slot, ResPlanes prev, RecPlanes prevRec, Shifted* __restrict__ shiftedPaths)
+__global__ void __launch_bounds__(128, 4) k_robust(uint32_t slot, ResPlanes prev, RecPlanes prevRec, Shifted* __restrict__ shiftedPaths)
 {
     const DevCtx& C = c_ctx[slot];
-    uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= C.W * C.H) return;
+    uint32_t idx;
+    if (!tiled_pixel(C.W, C.H, idx)) return;
     uint32_t x = idx % C.W, y = idx / C.W;
     const int kOff[8][2] = {{-1, -1}, {0, -1}, {1, -1}, {-1, 0}, {1, 0}, {-1, 1}, {0, 1}, {1, 1}};
     SampleGen sg = sg_create(x, y, pass_seed(C, 1), C.sgKind);
@@ -807,14 +807,14 @@ __device__ __forceinline__ void write_color(float4* color, uint32_t i, const Res
 }
 
 // ScatterTemporalResampling.rt.slang:65-174
-__global__ void __launch_bounds__(128) k_scatter_resample(uint32_t slot, const float2* __restrict__ mvec, ResPlanes prev, RecPlanes prevRec,
+__global__ void __launch_bounds__(128, 3) k_scatter_resample(uint32_t slot, const float2* __restrict__ mvec, ResPlanes prev, RecPlanes prevRec,
                                                           ResPlanes curr, RecPlanes currRec, const uint32_t* __restrict__ counts,
                                                           const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ sorted,
                                                           float4* __restrict__ color)
 {
     const DevCtx& C = c_ctx[slot];
-    uint32_t ri = blockIdx.x * blockDim.x + threadIdx.x;
-    if (ri >= C.W * C.H) return;
+    uint32_t ri;
+    if (!tiled_pixel(C.W, C.H, ri)) return;
     uint32_t x = ri % C.W, y = ri / C.W;
     const bool useConf = C.useConfTemporal != 0;
     SampleGen sg = sg_create(x, y, pass_seed(C, 5), C.sgKind);
@@ -867,13 +867,13 @@ __global__ void __launch_bounds__(128) k_scatter_resample(uint32_t slot, const f
 }
 
 // GatherTemporalResampling.rt.slang:68-235
-__global__ void __launch_bounds__(128) k_gather_resample(uint32_t slot, const uint4* __restrict__ vbuffer, ResPlanes curr, RecPlanes currRec,
+__global__ void __launch_bounds__(128, 3) k_gather_resample(uint32_t slot, const uint4* __restrict__ vbuffer, ResPlanes curr, RecPlanes currRec,
                                                          ResPlanes inter, RecPlanes interRec, const float2* __restrict__ floatingCoords,
                                                          float4* __restrict__ color)
 {
     const DevCtx& C = c_ctx[slot];
-    uint32_t ri = blockIdx.x * blockDim.x + threadIdx.x;
-    if (ri >= C.W * C.H) return;
+    uint32_t ri;
+    if (!tiled_pixel(C.W, C.H, ri)) return;
     uint32_t x = ri % C.W, y = ri / C.W;
     const bool useConf = C.useConfTemporal != 0;
     SampleGen sg = sg_create(x, y, pass_seed(C, 3), C.sgKind);
@@ -933,79 +933,6 @@ __global__ void __launch_bounds__(128) k_gather_resample(uint32_t slot, const ui
         }
         if (res_add_sample(dst, sg, prevSampleMIS, prevPHat, sj, pr)) dstR = prd;
     }
-    store_res(curr, ri, dst);
-    store_rec(currRec, ri, dstR);
-    write_color(color, ri, dst);
-}
-
-// MultiScatterTemporalResampling.rt.slang:65-186
-__global__ void __launch_bounds__(128) k_multi_scatter_resample(uint32_t slot, const float2* __restrict__ mvec, ResPlanes prev, RecPlanes prevRec,
-                                                                ResPlanes curr, RecPlanes currRec, const uint32_t* __restrict__ counts,
-                                                                const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ sortedAll,
-                                                                float4* __restrict__ color)
-{
-    const DevCtx& C = c_ctx[slot];
-    uint32_t ri = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t N = C.W * C.H;
-    if (ri >= N) return;
-    uint32_t x = ri % C.W, y = ri / C.W;
-    const bool useConf = C.useConfTemporal != 0;
-    const uint32_t P = C.numTimePartitions;
-    SampleGen sg = sg_create(x, y, pass_seed(C, 5), C.sgKind);
-    Res dst = res_default();
-    Recon dstR = recon_default();
-    float timePartitions = C.camera.shutterSpeed / (float)P;
-    float jacobianScale = 1.f / (float)P;
-    Res cr = load_res_rw(curr, ri);
-    Recon crd = load_rec_rw(currRec, ri);
-    float currSampleMIS = 1.f;
-    if (any_gt0(cr.integrand))
-    {
-        float m1 = luminance(cr.integrand) * (useConf ? cr.confidence : 1.f);
-        float fractionalTime = (crd.time - f_floor(crd.time / timePartitions) * timePartitions) / timePartitions;
-        float shiftedTime = fractionalTime * C.camera.shutterSpeed;
-        Shifted sc = dev_scatter_shift(C, sg, crd, shiftedTime + C.cm.artificialFrameTime, crd.firstHit, crd.lensSample, false);
-        float sj = jac_scatter(sc, crd);
-        float m2 = luminance(sc.radiance) * sj;
-        m2 = f_isnan(m2) ? 0.f : m2;
-        int spx = (int)f_floor(sc.fractionalPixel.x), spy = (int)f_floor(sc.fractionalPixel.y);
-        if (valid_int(C, spx, spy)) m2 *= useConf ? load_confidence(prev, (uint32_t)spy * C.W + (uint32_t)spx) : 1.f;
-        else m2 = 0.f;
-        currSampleMIS = (m1 + m2 == 0.f) ? 0.f : m1 / (m1 + m2);
-    }
-    if (res_add_sample(dst, sg, currSampleMIS, cr.integrand, 1.f, cr)) dstR = crd;
-    float newConfidence = dst.confidence;
-    for (uint32_t j = 0; j < P; j++)
-    {
-        uint32_t n = counts[(size_t)j * N + ri], off = offsets[(size_t)j * N + ri];
-        const uint32_t* sorted = sortedAll + (size_t)j * N; // partition j's lists start at j * N
-        for (uint32_t i = 0; i < n; i++)
-        {
-            uint32_t si = __ldg(&sorted[off + i]);
-            Res pr = load_res(prev, si);
-            Recon prd = load_rec(prevRec, si);
-            f3 prevPHat = mk3(0.f);
-            float sj = 1.f;
-            float prevMIS = 0.f;
-            if (any_gt0(pr.integrand))
-            {
-                float fractionalTime = prd.time / C.camera.shutterSpeed;
-                float newTime = (fractionalTime + (float)j) * timePartitions;
-                Shifted sp = dev_scatter_shift(C, sg, prd, newTime, prd.firstHit, prd.lensSample, false);
-                sj = jac_scatter(sp, prd);
-                float m1 = luminance(sp.radiance) * sj * (useConf ? cr.confidence : 1.f);
-                prevPHat = f_isnan(m1) ? mk3(0.f) : sp.radiance;
-                sj = f_isnan(m1) ? 1.f : sj;
-                recon_update(prd, sp);
-                prd.time = newTime;
-                pr.subPixel = prd.subPixel;
-                float m2 = luminance(pr.integrand) * (useConf ? pr.confidence : 1.f);
-                prevMIS = ((m1 + m2) == 0.f) ? 0.f : m2 / (m1 + m2);
-            }
-            if (res_add_sample(dst, sg, prevMIS, prevPHat, sj * jacobianScale, pr)) dstR = prd;
-        }
-    }
-    dst.confidence = bilinear_confidence(C, mvec, prev, x, y, newConfidence, useConf);
     store_res(curr, ri, dst);
     store_rec(currRec, ri, dstR);
     write_color(color, ri, dst);

@@ -23,8 +23,6 @@ __global__ void k_scatter_resample(uint32_t slot, const float2* mvec, ResPlanes 
                                    const uint32_t* counts, const uint32_t* offsets, const uint32_t* sorted, float4* color);
 __global__ void k_gather_resample(uint32_t slot, const uint4* vbuffer, ResPlanes curr, RecPlanes currRec, ResPlanes inter, RecPlanes interRec,
                                   const float2* floatingCoords, float4* color);
-__global__ void k_multi_scatter_resample(uint32_t slot, const float2* mvec, ResPlanes prev, RecPlanes prevRec, ResPlanes curr, RecPlanes currRec,
-                                         const uint32_t* counts, const uint32_t* offsets, const uint32_t* sortedAll, float4* color);
 __global__ void k_resolve(uint32_t n, ResPlanes curr, float4* color);
 
 __global__ void k_backward(uint32_t slot, ResPlanes res, RecPlanes rec, const float4* gradColor, double* acc, uint32_t numMaterials,
@@ -64,6 +62,24 @@ struct WaveCtx
     ShiftPlanes backupShift; float4* backupTerms; float2* backupM;
     ShiftPlanes splatShift; float4* splatTerms; float4* splatM;
 };
+
+// Buffers of the wavefront MultiSplatting resampling: P partitions' cell lists (partition j at j * N)
+// and, per splat position, its stored shift and terms.
+struct MultiCtx
+{
+    const float2* mvec;
+    ResPlanes curr; RecPlanes currRec;
+    ResPlanes prev; RecPlanes prevRec;
+    const uint32_t* counts; const uint32_t* offsets; const uint32_t* sorted; const uint32_t* sortedCell;
+    const uint32_t* totals;        // splats per partition
+    float* currMIS;                // per pixel: the current sample's MIS weight
+    ShiftPlanes shift;             // per splat position (stride P * N)
+    float4* terms;                 // per splat: prevPHat.xyz, Jacobian
+    float4* misSub;                // per splat: prevMIS, shifted sub-pixel.xy, 0
+};
+__global__ void k_ms_curr(uint32_t slot, MultiCtx M);
+__global__ void k_ms_splat(uint32_t slot, MultiCtx M);
+__global__ void k_ms_combine(uint32_t slot, MultiCtx M, float4* color);
 
 // Buffers of the wavefront spatial resampling (one iteration).
 struct SpatialCtx

@@ -132,6 +132,9 @@ struct rs_pass
     DevBuf<uint4> backupShift, splatShift, spShift;
     DevBuf<float4> backupTerms, splatTerms, splatM, spTerms;
     DevBuf<float2> backupM;
+    DevBuf<float> msCurr;                 // wavefront MultiSplatting buffers
+    DevBuf<uint4> msShift;
+    DevBuf<float4> msTerms, msMisSub;
     DevBuf<uint32_t> fault;
     uint32_t* hostFault = nullptr;
     DevBuf<unsigned long long> adjStats; // rs_backward counters (replayed, too long, no emitter, value mismatch)
@@ -242,6 +245,11 @@ static rs_status allocate(rs_pass* p)
         RS_CUDA(p->m2curr.ensure(N)); RS_CUDA(p->m3curr.ensure(N));
         RS_CUDA(p->backupShift.ensure(5 * N)); RS_CUDA(p->backupTerms.ensure(N)); RS_CUDA(p->backupM.ensure(N));
         RS_CUDA(p->splatShift.ensure(5 * N)); RS_CUDA(p->splatTerms.ensure(N)); RS_CUDA(p->splatM.ensure(N));
+    }
+    if (p->opt.temporalReuse == RS_MULTI_SCATTER)
+    {
+        RS_CUDA(p->msCurr.ensure(N));
+        RS_CUDA(p->msShift.ensure(5 * P * N)); RS_CUDA(p->msTerms.ensure(P * N)); RS_CUDA(p->msMisSub.ensure(P * N));
     }
     if (p->opt.enableSpatialResampling)
     {
@@ -520,9 +528,9 @@ static rs_status enqueue_frame(rs_pass* p, cudaStream_t s, float4* colorDev, con
     p->lastFusedCollect = false;
     const uint32_t numTiles = (N + kScanTileElems - 1) / kScanTileElems;
 
-    auto buildCells = [&](uint32_t* tg, uint32_t* cn, uint32_t* of, uint32_t* cu, uint32_t* un, uint32_t* so, uint32_t* sc) {
+    auto buildCells = [&](uint32_t* tg, uint32_t* cn, uint32_t* of, uint32_t* cu, uint32_t* un, uint32_t* so, uint32_t* sc, uint32_t* tot) {
         k_scan_tiles<<<numTiles, 1024, 0, s>>>(cn, of, p->tileSums.p, N);
-        k_scan_tile_sums<<<1, 1024, 0, s>>>(p->tileSums.p, numTiles, p->total.p);
+        k_scan_tile_sums<<<1, 1024, 0, s>>>(p->tileSums.p, numTiles, tot);
         k_scan_add<<<grid(N, 256), 256, 0, s>>>(of, p->tileSums.p, N);
         k_fill<<<grid(N, 256), 256, 0, s>>>(tg, of, cu, un, N);
         k_rank_cells<<<grid(N, 256), 256, 0, s>>>(tg, of, cn, un, so, sc, N);
@@ -538,12 +546,12 @@ static rs_status enqueue_frame(rs_pass* p, cudaStream_t s, float4* colorDev, con
             if (o.gatherOption == RS_GATHER_ROBUST)
             {
                 stage(p, "robustReuse", s);
-                k_robust<<<grid(N, 128), 128, 0, s>>>(C, prev.res(), prev.recp(), p->shiftedPaths.p); p->launches++;
+                k_robust<<<tiled_blocks(W, H, 128), 128, 0, s>>>(C, prev.res(), prev.recp(), p->shiftedPaths.p); p->launches++;
             }
             stage(p, "collect", s);
-            k_collect<<<grid(N, 128), 128, 0, s>>>(C, mvec, prev.res(), prev.recp(), p->inter.res(), p->inter.recp(), p->floatingCoords.p, p->shiftedPaths.p); p->launches++;
+            k_collect<<<tiled_blocks(W, H, 128), 128, 0, s>>>(C, mvec, prev.res(), prev.recp(), p->inter.res(), p->inter.recp(), p->floatingCoords.p, p->shiftedPaths.p); p->launches++;
             stage(p, "gatherResample", s);
-            k_gather_resample<<<grid(N, 128), 128, 0, s>>>(C, p->vbuffer.p, curr.res(), curr.recp(), p->inter.res(), p->inter.recp(), p->floatingCoords.p, temporalColor); p->launches++;
+            k_gather_resample<<<tiled_blocks(W, H, 128), 128, 0, s>>>(C, p->vbuffer.p, curr.res(), curr.recp(), p->inter.res(), p->inter.recp(), p->floatingCoords.p, temporalColor); p->launches++;
             break;
         case RS_SCATTER_ONLY:
             stage(p, "reproject", s);
@@ -551,9 +559,9 @@ static rs_status enqueue_frame(rs_pass* p, cudaStream_t s, float4* colorDev, con
             RS_CUDA(cudaMemsetAsync(p->cursor.p, 0, N * 4ull, s));
             k_reproject<<<tiled_blocks(W, H, 256), 256, 0, s>>>(C, prev.res(), prev.recp(), p->targets.p, p->counts.p); p->launches++;
             stage(p, "sortCells", s);
-            buildCells(p->targets.p, p->counts.p, p->offsets.p, p->cursor.p, p->unsortedSplats.p, p->sortedSplats.p, nullptr);
+            buildCells(p->targets.p, p->counts.p, p->offsets.p, p->cursor.p, p->unsortedSplats.p, p->sortedSplats.p, nullptr, p->total.p);
             stage(p, "scatterResample", s);
-            k_scatter_resample<<<grid(N, 128), 128, 0, s>>>(C, mvec, prev.res(), prev.recp(), curr.res(), curr.recp(), p->counts.p, p->offsets.p, p->sortedSplats.p, temporalColor); p->launches++;
+            k_scatter_resample<<<tiled_blocks(W, H, 128), 128, 0, s>>>(C, mvec, prev.res(), prev.recp(), curr.res(), curr.recp(), p->counts.p, p->offsets.p, p->sortedSplats.p, temporalColor); p->launches++;
             break;
         case RS_SCATTER_BACKUP:
         {
@@ -564,17 +572,17 @@ static rs_status enqueue_frame(rs_pass* p, cudaStream_t s, float4* colorDev, con
                 if (o.gatherOption == RS_GATHER_ROBUST)
                 {
                     stage(p, "robustReuse", s);
-                    k_robust<<<grid(N, 128), 128, 0, s>>>(C, prev.res(), prev.recp(), p->shiftedPaths.p); p->launches++;
+                    k_robust<<<tiled_blocks(W, H, 128), 128, 0, s>>>(C, prev.res(), prev.recp(), p->shiftedPaths.p); p->launches++;
                 }
                 stage(p, "collect", s);
-                k_collect<<<grid(N, 128), 128, 0, s>>>(C, mvec, prev.res(), prev.recp(), p->inter.res(), p->inter.recp(), p->floatingCoords.p, p->shiftedPaths.p); p->launches++;
+                k_collect<<<tiled_blocks(W, H, 128), 128, 0, s>>>(C, mvec, prev.res(), prev.recp(), p->inter.res(), p->inter.recp(), p->floatingCoords.p, p->shiftedPaths.p); p->launches++;
             }
             stage(p, "reproject", s);
             RS_CUDA(cudaMemsetAsync(p->counts.p, 0, N * 4ull, s));
             RS_CUDA(cudaMemsetAsync(p->cursor.p, 0, N * 4ull, s));
             k_reproject<<<tiled_blocks(W, H, 256), 256, 0, s>>>(C, prev.res(), prev.recp(), p->targets.p, p->counts.p); p->launches++;
             stage(p, "sortCells", s);
-            buildCells(p->targets.p, p->counts.p, p->offsets.p, p->cursor.p, p->unsortedSplats.p, p->sortedSplats.p, p->sortedCell.p);
+            buildCells(p->targets.p, p->counts.p, p->offsets.p, p->cursor.p, p->unsortedSplats.p, p->sortedSplats.p, p->sortedCell.p, p->total.p);
             WaveCtx K;
             K.fused = fused;
             K.mvec = mvec;
@@ -616,15 +624,24 @@ static rs_status enqueue_frame(rs_pass* p, cudaStream_t s, float4* colorDev, con
             stage(p, "multiReproject", s);
             RS_CUDA(cudaMemsetAsync(p->counts.p, 0, (size_t)P * N * 4ull, s));
             RS_CUDA(cudaMemsetAsync(p->cursor.p, 0, (size_t)P * N * 4ull, s));
-            k_multi_reproject<<<grid(N, 256), 256, 0, s>>>(C, prev.res(), prev.recp(), p->targets.p, p->counts.p); p->launches++;
+            k_multi_reproject<<<tiled_blocks(W, H, 256), 256, 0, s>>>(C, prev.res(), prev.recp(), p->targets.p, p->counts.p); p->launches++;
             stage(p, "multiSortCells", s);
             for (uint32_t j = 0; j < P; j++)
             {
                 size_t b = (size_t)j * N;
-                buildCells(p->targets.p + b, p->counts.p + b, p->offsets.p + b, p->cursor.p + b, p->unsortedSplats.p + b, p->sortedSplats.p + b, nullptr);
+                buildCells(p->targets.p + b, p->counts.p + b, p->offsets.p + b, p->cursor.p + b, p->unsortedSplats.p + b, p->sortedSplats.p + b,
+                           p->sortedCell.p + b, p->total.p + j);
             }
             stage(p, "multiScatterResample", s);
-            k_multi_scatter_resample<<<grid(N, 128), 128, 0, s>>>(C, mvec, prev.res(), prev.recp(), curr.res(), curr.recp(), p->counts.p, p->offsets.p, p->sortedSplats.p, temporalColor); p->launches++;
+            MultiCtx M;
+            M.mvec = mvec; M.curr = curr.res(); M.currRec = curr.recp(); M.prev = prev.res(); M.prevRec = prev.recp();
+            M.counts = p->counts.p; M.offsets = p->offsets.p; M.sorted = p->sortedSplats.p; M.sortedCell = p->sortedCell.p;
+            M.totals = p->total.p; M.currMIS = p->msCurr.p;
+            M.shift = ShiftPlanes{p->msShift.p, (size_t)P * N}; M.terms = p->msTerms.p; M.misSub = p->msMisSub.p;
+            k_ms_curr<<<tiled_blocks(W, H, 128), 128, 0, s>>>(C, M);
+            k_ms_splat<<<grid(P * N, 128), 128, 0, s>>>(C, M);
+            k_ms_combine<<<tiled_blocks(W, H, 128), 128, 0, s>>>(C, M, temporalColor);
+            p->launches += 3;
             break;
         }
         }

@@ -493,4 +493,134 @@ __global__ void __launch_bounds__(128) k_sp_combine(uint32_t slot, SpatialCtx S,
     }
 }
 
+
+// ============================================================ MultiSplatting, wavefront form
+// MultiScatterTemporalResampling.rt.slang:65-186 split like the ScatterBackup resampling: the shift
+// mappings never use the generator's values, so the current sample's shift (k_ms_curr) and every
+// splat's shift into its time partition (k_ms_splat, one thread per splat) run first and store their
+// results; k_ms_combine replays the reference's resampling order and generator draws on them and
+// rebuilds only the selected record.
+
+// The current sample's scatter shift for its MIS weight (:96-117).
+__global__ void __launch_bounds__(128, 8) k_ms_curr(uint32_t slot, MultiCtx M)
+{
+    const DevCtx& C = c_ctx[slot];
+    uint32_t ri;
+    if (!tiled_pixel(C.W, C.H, ri)) return;
+    const bool useConf = C.useConfTemporal != 0;
+    const uint32_t P = C.numTimePartitions;
+    float timePartitions = C.camera.shutterSpeed / (float)P;
+    Res cr = load_res(M.curr, ri);
+    float currSampleMIS = 1.f;
+    if (any_gt0(cr.integrand))
+    {
+        Recon crd = load_rec(M.currRec, ri);
+        float m1 = luminance(cr.integrand) * (useConf ? cr.confidence : 1.f);
+        float fractionalTime = (crd.time - f_floor(crd.time / timePartitions) * timePartitions) / timePartitions;
+        float shiftedTime = fractionalTime * C.camera.shutterSpeed;
+        SampleGen dummy = {0, C.sgKind};
+        Shifted sc = dev_scatter_shift(C, dummy, crd, shiftedTime + C.cm.artificialFrameTime, crd.firstHit, crd.lensSample, false);
+        float sj = jac_scatter(sc, crd);
+        float m2 = luminance(sc.radiance) * sj;
+        m2 = f_isnan(m2) ? 0.f : m2;
+        int spx = (int)f_floor(sc.fractionalPixel.x), spy = (int)f_floor(sc.fractionalPixel.y);
+        if (valid_int(C, spx, spy)) m2 *= useConf ? load_confidence(M.prev, (uint32_t)spy * C.W + (uint32_t)spx) : 1.f;
+        else m2 = 0.f;
+        currSampleMIS = (m1 + m2 == 0.f) ? 0.f : m1 / (m1 + m2);
+    }
+    M.currMIS[ri] = currSampleMIS;
+}
+
+// One splat of partition j (sorted position g = j * N + k) shifted to its partition's time (:124-160).
+__global__ void __launch_bounds__(128, 8) k_ms_splat(uint32_t slot, MultiCtx M)
+{
+    const DevCtx& C = c_ctx[slot];
+    const uint32_t N = C.W * C.H, P = C.numTimePartitions;
+    uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= P * N) return;
+    const uint32_t j = g / N, k = g - j * N;
+    if (k >= __ldg(&M.totals[j])) return;
+    const bool useConf = C.useConfTemporal != 0;
+    float timePartitions = C.camera.shutterSpeed / (float)P;
+    const uint32_t si = __ldg(&M.sorted[g]), cell = __ldg(&M.sortedCell[g]);
+    Res pr = load_res(M.prev, si);
+    f3 prevPHat = mk3(0.f);
+    float sj = 1.f, prevMIS = 0.f;
+    f2 sub = pr.subPixel;
+    if (any_gt0(pr.integrand))
+    {
+        Recon prd = load_rec(M.prevRec, si);
+        float fractionalTime = prd.time / C.camera.shutterSpeed;
+        float newTime = (fractionalTime + (float)j) * timePartitions;
+        SampleGen dummy = {0, C.sgKind};
+        Shifted sp = dev_scatter_shift(C, dummy, prd, newTime, prd.firstHit, prd.lensSample, false);
+        store_shift(M.shift, g, sp);
+        sj = jac_scatter(sp, prd);
+        float m1 = luminance(sp.radiance) * sj * (useConf ? load_confidence(M.curr, cell) : 1.f);
+        prevPHat = f_isnan(m1) ? mk3(0.f) : sp.radiance;
+        sj = f_isnan(m1) ? 1.f : sj;
+        sub = sp.fractionalPixel - floor2(sp.fractionalPixel); // the record update's sub-pixel
+        float m2 = luminance(pr.integrand) * (useConf ? pr.confidence : 1.f);
+        prevMIS = ((m1 + m2) == 0.f) ? 0.f : m2 / (m1 + m2);
+    }
+    M.terms[g] = make_float4(prevPHat.x, prevPHat.y, prevPHat.z, sj);
+    M.misSub[g] = make_float4(prevMIS, sub.x, sub.y, 0.f);
+}
+
+// The resampling of :90-186 in the reference's order (current sample, then partitions 0..P-1 and
+// each cell's splats in sorted order) on the stored terms.
+__global__ void __launch_bounds__(128) k_ms_combine(uint32_t slot, MultiCtx M, float4* __restrict__ color)
+{
+    const DevCtx& C = c_ctx[slot];
+    uint32_t ri;
+    if (!tiled_pixel(C.W, C.H, ri)) return;
+    const uint32_t N = C.W * C.H;
+    uint32_t x = ri % C.W, y = ri / C.W;
+    const bool useConf = C.useConfTemporal != 0;
+    const uint32_t P = C.numTimePartitions;
+    SampleGen sg = sg_create(x, y, pass_seed(C, 5), C.sgKind);
+    Res dst = res_default();
+    float jacobianScale = 1.f / (float)P;
+    float timePartitions = C.camera.shutterSpeed / (float)P;
+    Res cr = load_res_rw(M.curr, ri);
+    bool selCurr = false, selZero = false;
+    uint32_t selG = kInvalidIndex, selJ = 0;
+    if (res_add_sample(dst, sg, M.currMIS[ri], cr.integrand, 1.f, cr)) selCurr = true;
+    float newConfidence = dst.confidence;
+    for (uint32_t j = 0; j < P; j++)
+    {
+        uint32_t n = __ldg(&M.counts[(size_t)j * N + ri]), off = __ldg(&M.offsets[(size_t)j * N + ri]);
+        for (uint32_t i = 0; i < n; i++)
+        {
+            const uint32_t g = j * N + off + i;
+            const uint32_t si = __ldg(&M.sorted[g]);
+            Res pr = load_res(M.prev, si);
+            const float4 t = __ldg(&M.terms[g]), m = __ldg(&M.misSub[g]);
+            const bool live = any_gt0(pr.integrand);
+            if (live) pr.subPixel = mk2(m.y, m.z);
+            if (res_add_sample(dst, sg, m.x, mk3(t.x, t.y, t.z), t.w * jacobianScale, pr))
+            {
+                selCurr = false; selG = g; selJ = j; selZero = !live;
+            }
+        }
+    }
+    dst.confidence = bilinear_confidence(C, M.mvec, M.prev, x, y, newConfidence, useConf);
+    store_res(M.curr, ri, dst);
+    Recon dstR = recon_default();
+    if (selCurr) dstR = load_rec_rw(M.currRec, ri);
+    else if (selG != kInvalidIndex)
+    {
+        dstR = load_rec(M.prevRec, __ldg(&M.sorted[selG]));
+        if (!selZero)
+        {
+            float fractionalTime = dstR.time / C.camera.shutterSpeed;
+            float newTime = (fractionalTime + (float)selJ) * timePartitions;
+            recon_update(dstR, load_shift(M.shift, selG));
+            dstR.time = newTime;
+        }
+    }
+    store_rec(M.currRec, ri, dstR);
+    write_color(color, ri, dst);
+}
+
 } // namespace rs
