@@ -760,25 +760,25 @@ __global__ void __launch_bounds__(128, 4) k_collect(uint32_t slot, const float2*
 }
 
 // RobustReuseOptimization.rt.slang:63-89
-__global__ void __launch_bounds__(128, 4) k_robust(uint32_t slot, ResPlanes prev, RecPlanes prevRec, Shifted* __restrict__ shiftedPaths)
+// One thread per (pixel, neighbour): the eight lens-copy shifts are independent (the generator
+// goes to the shift by value and is never advanced), so blockIdx.y is the neighbour k.
+__global__ void __launch_bounds__(128, 8) k_robust(uint32_t slot, ResPlanes prev, RecPlanes prevRec, Shifted* __restrict__ shiftedPaths)
 {
     const DevCtx& C = c_ctx[slot];
     uint32_t idx;
     if (!tiled_pixel(C.W, C.H, idx)) return;
+    const int k = (int)blockIdx.y;
     uint32_t x = idx % C.W, y = idx / C.W;
     const int kOff[8][2] = {{-1, -1}, {0, -1}, {1, -1}, {-1, 0}, {1, 0}, {-1, 1}, {0, 1}, {1, 1}};
     SampleGen sg = sg_create(x, y, pass_seed(C, 1), C.sgKind);
     Res pr = load_res(prev, idx);
+    int nx = (int)x + kOff[k][0], ny = (int)y + kOff[k][1];
+    bool neighborIsValid = valid_float(C, mk2((float)nx, (float)ny));
+    bool canShift = any_gt0(pr.integrand);
+    if (!(neighborIsValid && canShift)) { shiftedPaths[8 * (size_t)idx + k] = shifted_default(); return; }
     Recon rd = load_rec(prevRec, idx);
-    for (int k = 0; k < 8; k++)
-    {
-        int nx = (int)x + kOff[k][0], ny = (int)y + kOff[k][1];
-        bool neighborIsValid = valid_float(C, mk2((float)nx, (float)ny));
-        bool canShift = any_gt0(pr.integrand);
-        shiftedPaths[8 * (size_t)idx + k] = (neighborIsValid && canShift)
-            ? dev_gather_lens_copy(C, sg, rd, rd.time + C.cm.artificialFrameTime, mk2((float)nx + pr.subPixel.x, (float)ny + pr.subPixel.y), rd.lensSample)
-            : shifted_default();
-    }
+    shiftedPaths[8 * (size_t)idx + k] =
+        dev_gather_lens_copy(C, sg, rd, rd.time + C.cm.artificialFrameTime, mk2((float)nx + pr.subPixel.x, (float)ny + pr.subPixel.y), rd.lensSample);
 }
 
 // ============================================================ temporal resampling

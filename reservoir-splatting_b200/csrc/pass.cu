@@ -546,7 +546,7 @@ static rs_status enqueue_frame(rs_pass* p, cudaStream_t s, float4* colorDev, con
             if (o.gatherOption == RS_GATHER_ROBUST)
             {
                 stage(p, "robustReuse", s);
-                k_robust<<<tiled_blocks(W, H, 128), 128, 0, s>>>(C, prev.res(), prev.recp(), p->shiftedPaths.p); p->launches++;
+                k_robust<<<dim3(tiled_blocks(W, H, 128), 8), 128, 0, s>>>(C, prev.res(), prev.recp(), p->shiftedPaths.p); p->launches++;
             }
             stage(p, "collect", s);
             k_collect<<<tiled_blocks(W, H, 128), 128, 0, s>>>(C, mvec, prev.res(), prev.recp(), p->inter.res(), p->inter.recp(), p->floatingCoords.p, p->shiftedPaths.p); p->launches++;
@@ -572,7 +572,7 @@ static rs_status enqueue_frame(rs_pass* p, cudaStream_t s, float4* colorDev, con
                 if (o.gatherOption == RS_GATHER_ROBUST)
                 {
                     stage(p, "robustReuse", s);
-                    k_robust<<<tiled_blocks(W, H, 128), 128, 0, s>>>(C, prev.res(), prev.recp(), p->shiftedPaths.p); p->launches++;
+                    k_robust<<<dim3(tiled_blocks(W, H, 128), 8), 128, 0, s>>>(C, prev.res(), prev.recp(), p->shiftedPaths.p); p->launches++;
                 }
                 stage(p, "collect", s);
                 k_collect<<<tiled_blocks(W, H, 128), 128, 0, s>>>(C, mvec, prev.res(), prev.recp(), p->inter.res(), p->inter.recp(), p->floatingCoords.p, p->shiftedPaths.p); p->launches++;
