@@ -141,7 +141,7 @@ struct Bvh
     // Closest hit on (tMin, tMax); ties on t go to the lower triangle index.
     bool closest(const Ray& r, HitInfo& hit, float& tHit) const
     {
-        if (nodes.empty()) return false;
+        if (nodes.empty() || ray_has_nan(r)) return false;
         f3 invd = mk3(1.f / r.dir.x, 1.f / r.dir.y, 1.f / r.dir.z);
         float best = r.tMax; uint32_t bestPrim = kInvalidIndex; float bu = 0, bv = 0;
         uint32_t stack[128]; int sp = 0; stack[sp++] = 0;
@@ -172,7 +172,7 @@ struct Bvh
     // True when nothing is hit on (tMin, tMax).
     bool visible(const Ray& r) const
     {
-        if (nodes.empty()) return true;
+        if (nodes.empty() || ray_has_nan(r)) return true;
         f3 invd = mk3(1.f / r.dir.x, 1.f / r.dir.y, 1.f / r.dir.z);
         uint32_t stack[128]; int sp = 0; stack[sp++] = 0;
         while (sp)

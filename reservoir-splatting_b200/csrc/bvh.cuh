@@ -128,9 +128,10 @@ __device__ __forceinline__ bool box_hit(float4 lo, float4 hi, const RayQ& r, flo
 template <bool kCount>
 __device__ __forceinline__ TraceHit trace_closest_bin(const BvhView& bv, const Ray& r, uint32_t* overflow, uint32_t* counts = nullptr)
 {
-    const RayQ q = make_rayq(r);
     TraceHit best;
     best.prim = kInvalidIndex; best.t = r.tMax; best.u = 0.f; best.v = 0.f;
+    if (ray_has_nan(r)) return best;
+    const RayQ q = make_rayq(r);
     uint32_t stack[kTraversalStack];
     int sp = 0;
     uint32_t node = bv.binRoot;
@@ -248,7 +249,7 @@ static __device__ __noinline__ TraceHit trace_closest_call(BvhView bv, Ray r, ui
 
 __device__ __forceinline__ bool trace_visible(const BvhView& bv, const Ray& r, uint32_t* overflow)
 {
-    if (bv.numTris == 0) return true;
+    if (bv.numTris == 0 || ray_has_nan(r)) return true;
     return trace_visible_q(bv.nodes, bv.leafTri, make_rayq(r), overflow);
 }
 

@@ -78,6 +78,15 @@ RS_HD bool intersect_triangle_e(f3 o, f3 d, f3 p0, f3 e1, f3 e2, float tMin, flo
     t = dot(e2, qv) * inv;
     return t > tMin && t < tMax;
 }
+// A ray with a NaN in its origin, direction or interval hits no triangle (every comparison in
+// intersect_triangle_e fails on NaN) while min/max slab tests accept every box for it, so
+// traversals return a miss for it before visiting any node: the result of a full traversal,
+// without its cost (a NaN camera time makes such rays).
+RS_HD bool ray_has_nan(const Ray& r)
+{
+    return !(r.origin.x == r.origin.x && r.origin.y == r.origin.y && r.origin.z == r.origin.z && r.dir.x == r.dir.x &&
+             r.dir.y == r.dir.y && r.dir.z == r.dir.z && r.tMin == r.tMin && r.tMax == r.tMax);
+}
 RS_HD bool intersect_triangle(f3 o, f3 d, f3 p0, f3 p1, f3 p2, float tMin, float tMax, float& t, float& u, float& v)
 {
     return intersect_triangle_e(o, d, p0, p1 - p0, p2 - p0, tMin, tMax, t, u, v);

@@ -426,6 +426,44 @@ RS_HD float mi_pdf(const ShadingData& sd, const BsdfData& d, uint32_t lobeMask, 
     StandardBSDF b = make_bsdf(wiLocal, d, lobeMask);
     return bsdf_pdf_local(b, wiLocal, woLocal);
 }
+// mi_eval and mi_pdf for the single lobe 1 << comp (comp < 4) and for all lobes (mask 0 or 0xF) in
+// one pass.  The per-lobe values do not depend on the mask (make_bsdf changes alpha only for mask
+// 5, which no single lobe has), so they are computed once and summed in the order of
+// bsdf_eval_local / bsdf_pdf_local: every result has the bits of the four separate calls.
+struct BsdfPair
+{
+    f3 lobeBsdf;
+    float lobePdf;
+    f3 totalBsdf;
+    float totalPdf;
+};
+RS_HD BsdfPair mi_eval_pair(const ShadingData& sd, const BsdfData& d, uint32_t comp, f3 wo)
+{
+    BsdfPair r;
+    r.lobeBsdf = mk3(0.f); r.totalBsdf = mk3(0.f);
+    r.lobePdf = 0.f; r.totalPdf = 0.f;
+    f3 wiLocal = sd_to_local(sd, sd.V);
+    f3 woLocal = sd_to_local(sd, wo);
+    if (!valid_hemisphere(sd, wiLocal, woLocal, wo)) return r;
+    const uint32_t mask = 1u << comp;
+    StandardBSDF b = make_bsdf(wiLocal, d, mask);
+    if (b.pDiffuseReflection > 0.f)
+    {
+        const f3 v = diffuse_eval(b, wiLocal, woLocal);
+        const float p = b.pDiffuseReflection * diffuse_pdf(wiLocal, woLocal);
+        r.totalBsdf += v; r.totalPdf += p;
+        if (mask & 0x1u) { r.lobeBsdf += v; r.lobePdf += p; }
+    }
+    if (b.pSpecularReflection > 0.f)
+    {
+        const f3 v = specular_eval(b, wiLocal, woLocal);
+        const float p = b.pSpecularReflection * specular_pdf(b, wiLocal, woLocal);
+        r.totalBsdf += v; r.totalPdf += p;
+        if (mask & 0x4u) { r.lobeBsdf += v; r.lobePdf += p; }
+    }
+    return r;
+}
+
 struct BSDFSample
 {
     f3 wo;

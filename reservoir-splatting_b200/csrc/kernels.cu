@@ -221,9 +221,10 @@ __device__ void handle_hit(const DevCtx& C, PState& path, const RecPlanes& outRe
         if (validSample)
         {
             f3 Le = lsLi * lsPdf;
-            float scatterPdf = mi_pdf(sd, d, 0u, lsDir);
+            const BsdfPair bp = mi_eval_pair(sd, d, 0u, lsDir); // all lobes: the pair's total
+            float scatterPdf = bp.totalPdf;
             float misWeight = dev_mis(C, lsPdf, scatterPdf);
-            f3 weight = mi_eval(sd, d, 0u, lsDir);
+            f3 weight = bp.totalBsdf;
             f3 Lr = weight * misWeight * lsLi;
             if (any_gt0(Lr) && dev_visible(C, mk_ray(lsOrigin, lsDir, 0.f, lsDistance)))
             {
@@ -311,93 +312,97 @@ __device__ void handle_hit(const DevCtx& C, PState& path, const RecPlanes& outRe
     if (!valid) path.flags &= ~kPActive;
 }
 
-// InitialCandidates.cs.slang:80-141 + addCandidateReservoir (:52-75)
+// generatePath (PathTracer.slang:194-221): the path of pixel (x, y) up to its primary ray.
 template <bool kDirect>
-__device__ __forceinline__ void candidates_pixel(const DevCtx& C, uint32_t i, const ResPlanes& curr, const RecPlanes& currRec)
+__device__ __forceinline__ void path_init(const DevCtx& C, uint32_t x, uint32_t y, PState& path)
 {
-    uint32_t x = i % C.W, y = i / C.W;
-    const uint32_t spp = kDirect ? 1u : C.spp;
-    for (uint32_t sIdx = 0; sIdx < spp; sIdx++)
+    path.flags = kPActive;
+    path.vertex = 0;
+    path.bounces = 0;
+    path.thp = mk3(1.f);
+    path.earlyThroughput = mk3(1.f);
+    path.pdf = 0.f; path.totalPdf = 0.f;
+    path.hit = hit_none();
+    path.rec = recon_default();
+    path.candTotalWeight = 0.f;
+    path.candIntegrand = mk3(0.f);
+    if (!kDirect) path.candRec = recon_default();
+    path.anySelected = false;
+    path.sg = sg_create(x, y, C.useFixedSeed ? C.fixedSeed + 0 : kNumRenderPasses * (C.frameCount + C.seed) + 0, C.sgKind);
+    CameraData cam = C.camera;
+    path.rec.time = sampleNext1D(path.sg) * cam.shutterSpeed;
+    path.rec.subPixel.x = sampleNext1D(path.sg);
+    path.rec.subPixel.y = sampleNext1D(path.sg);
+    if (cam.apertureRadius > 0.f)
     {
-        PState path;
-        // generatePath (PathTracer.slang:194-221)
-        path.flags = kPActive;
-        path.vertex = 0;
-        path.bounces = 0;
-        path.thp = mk3(1.f);
-        path.earlyThroughput = mk3(1.f);
-        path.pdf = 0.f; path.totalPdf = 0.f;
-        path.hit = hit_none();
-        path.rec = recon_default();
-        path.candTotalWeight = 0.f;
-        path.candIntegrand = mk3(0.f);
-        if (!kDirect) path.candRec = recon_default();
-        path.anySelected = false;
-        path.sg = sg_create(x, y, C.useFixedSeed ? C.fixedSeed + 0 : kNumRenderPasses * (C.frameCount + C.seed) + 0, C.sgKind);
-        CameraData cam = C.camera;
-        path.rec.time = sampleNext1D(path.sg) * cam.shutterSpeed;
-        path.rec.subPixel.x = sampleNext1D(path.sg);
-        path.rec.subPixel.y = sampleNext1D(path.sg);
-        if (cam.apertureRadius > 0.f)
-        {
-            f2 u; u.x = sampleNext1D(path.sg); u.y = sampleNext1D(path.sg);
-            path.rec.lensSample = sample_disk(u);
-        }
-        else path.rec.lensSample = mk2(0.f, 0.f);
-        orient_camera(C.cm, cam, C.frameCount, path.rec.time);
-        Ray r = camera_ray_thinlens(cam, C.W, C.H, mk2((float)x + path.rec.subPixel.x, (float)y + path.rec.subPixel.y), path.rec.lensSample);
-        path.origin = r.origin;
-        path.dir = r.dir;
-        path.prevHitPos = camera_lens_point(cam, path.rec.lensSample);
+        f2 u; u.x = sampleNext1D(path.sg); u.y = sampleNext1D(path.sg);
+        path.rec.lensSample = sample_disk(u);
+    }
+    else path.rec.lensSample = mk2(0.f, 0.f);
+    orient_camera(C.cm, cam, C.frameCount, path.rec.time);
+    Ray r = camera_ray_thinlens(cam, C.W, C.H, mk2((float)x + path.rec.subPixel.x, (float)y + path.rec.subPixel.y), path.rec.lensSample);
+    path.origin = r.origin;
+    path.dir = r.dir;
+    path.prevHitPos = camera_lens_point(cam, path.rec.lensSample);
+}
 
-        next_hit(C, path);
-        if (path.flags & kPHit)
-        {
-            handle_hit<kDirect>(C, path, currRec, i);
-            while (path.flags & kPActive)
-            {
-                next_hit(C, path);
-                if (path.flags & kPHit) handle_hit<kDirect>(C, path, currRec, i);
-                else
-                {
-                    // handleMiss (:1433-1524) without an environment map
-                    if (path.vertex == 2) path.rec.secondaryPathJacobian = path.pdf * 1.f;
-                    else if (path.vertex == 3) path.rec.secondaryPathJacobian *= path.pdf;
-                    path.flags &= ~kPActive;
-                }
-            }
-        }
-        // addCandidateReservoir
-        const bool isFirstSample = (sIdx == spp - 1) || spp == 1;
-        Res ex = isFirstSample ? res_default() : load_res_rw(curr, i);
-        float weight = (1.f / (float)spp) * path.candTotalWeight;
-        ex.totalWeight = ex.totalWeight + weight;
-        ex.confidence = f_min(ex.confidence + 1.f, kConfidenceCap);
-        float rng = sampleNext1D(path.sg);
-        bool selected = (rng * ex.totalWeight < weight);
-        ex.integrand = selected ? path.candIntegrand : ex.integrand;
-        ex.subPixel = selected ? path.rec.subPixel : ex.subPixel;
-        ex.confidence = 1.f;
-        store_res(curr, i, ex);
-        if (kDirect)
-        {
-            // the output holds the last selected candidate's record when one was selected
-            if (!(selected && path.anySelected)) store_rec(currRec, i, recon_default());
-        }
-        else
-        {
-            Recon exr = isFirstSample ? recon_default() : load_rec_rw(currRec, i);
-            store_rec(currRec, i, selected ? path.candRec : exr);
-        }
+// One vertex of the tracePath loop (InitialCandidates.cs.slang:80-141): the next closest hit, then
+// handleHit, or handleMiss (PathTracer.slang:1433-1524, no environment map) which ends the path.
+template <bool kDirect>
+__device__ __forceinline__ void path_step(const DevCtx& C, PState& path, const RecPlanes& currRec, uint32_t i)
+{
+    next_hit(C, path);
+    if (path.flags & kPHit) handle_hit<kDirect>(C, path, currRec, i);
+    else
+    {
+        if (path.vertex == 2) path.rec.secondaryPathJacobian = path.pdf * 1.f;
+        else if (path.vertex == 3) path.rec.secondaryPathJacobian *= path.pdf;
+        path.flags &= ~kPActive;
     }
 }
 
+// addCandidateReservoir (InitialCandidates.cs.slang:52-75) of sample sIdx of spp.
+template <bool kDirect>
+__device__ __forceinline__ void path_finish(PState& path, uint32_t sIdx, uint32_t spp, const ResPlanes& curr, const RecPlanes& currRec, uint32_t i)
+{
+    const bool isFirstSample = (sIdx == spp - 1) || spp == 1;
+    Res ex = isFirstSample ? res_default() : load_res_rw(curr, i);
+    float weight = (1.f / (float)spp) * path.candTotalWeight;
+    ex.totalWeight = ex.totalWeight + weight;
+    ex.confidence = f_min(ex.confidence + 1.f, kConfidenceCap);
+    float rng = sampleNext1D(path.sg);
+    bool selected = (rng * ex.totalWeight < weight);
+    ex.integrand = selected ? path.candIntegrand : ex.integrand;
+    ex.subPixel = selected ? path.rec.subPixel : ex.subPixel;
+    ex.confidence = 1.f;
+    store_res(curr, i, ex);
+    if (kDirect)
+    {
+        // the output holds the last selected candidate's record when one was selected
+        if (!(selected && path.anySelected)) store_rec(currRec, i, recon_default());
+    }
+    else
+    {
+        Recon exr = isFirstSample ? recon_default() : load_rec_rw(currRec, i);
+        store_rec(currRec, i, selected ? path.candRec : exr);
+    }
+}
+
+// InitialCandidates.cs.slang:80-141, several samples per pixel: one thread runs the pixel's paths.
 __global__ void __launch_bounds__(128, 3) k_candidates(uint32_t slot, ResPlanes curr, RecPlanes currRec)
 {
     const DevCtx& C = c_ctx[slot];
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= C.W * C.H) return;
-    candidates_pixel<false>(C, i, curr, currRec);
+    const uint32_t x = i % C.W, y = i / C.W;
+    for (uint32_t sIdx = 0; sIdx < C.spp; sIdx++)
+    {
+        PState path;
+        path_init<false>(C, x, y, path);
+        do path_step<false>(C, path, currRec, i);
+        while (path.flags & kPActive);
+        path_finish<false>(path, sIdx, C.spp, curr, currRec, i);
+    }
 }
 
 // One sample per pixel (the reference default): records go straight to the output planes.
@@ -406,7 +411,11 @@ __global__ void __launch_bounds__(128, 4) k_candidates_direct(uint32_t slot, Res
     const DevCtx& C = c_ctx[slot];
     uint32_t i;
     if (!tiled_pixel(C.W, C.H, i)) return;
-    candidates_pixel<true>(C, i, curr, currRec);
+    PState path;
+    path_init<true>(C, i % C.W, i / C.W, path);
+    do path_step<true>(C, path, currRec, i);
+    while (path.flags & kPActive);
+    path_finish<true>(path, 0, 1, curr, currRec, i);
 }
 
 // ============================================================ forward reprojection (splat)

@@ -271,11 +271,9 @@ __device__ inline void dev_reconnection_hit(const DevCtx& C, ShiftPath& path, co
     }
     else nextDir = hit_as_direction(rd.secondHit);
 
-    uint32_t lobeMask = 1u << rd.firstComp;
-    f3 lobeScatterBsdf = mi_eval(sd, d, lobeMask, nextDir);
-    float lobeScatterPdf = mi_pdf(sd, d, lobeMask, nextDir);
-    f3 totalScatterBsdf = mi_eval(sd, d, 0u, nextDir);
-    float totalScatterPdf = mi_pdf(sd, d, 0u, nextDir);
+    const BsdfPair bp = mi_eval_pair(sd, d, rd.firstComp, nextDir);
+    const f3 lobeScatterBsdf = bp.lobeBsdf, totalScatterBsdf = bp.totalBsdf;
+    const float lobeScatterPdf = bp.lobePdf, totalScatterPdf = bp.totalPdf;
     path.dir = nextDir;
 
     if (rd.pathLength == 2)
@@ -320,11 +318,9 @@ __device__ inline f3 dev_path_reconnection_shift(const DevCtx& C, const Recon& r
     if (rd.pathLength == 2) return 1.f * path.thp * rd.irradiance; // the x2 BSDF terms are not used for length 2
     ShadingData secondSd = dev_sd(C, rd.secondHit, path.dir);
     BsdfData d = dev_instance(C, secondSd);
-    uint32_t lobeMask = 1u << rd.secondComp;
-    f3 lobeSpecificBsdf = mi_eval(secondSd, d, lobeMask, rd.secondWo);
-    float lobeSpecificPdf = mi_pdf(secondSd, d, lobeMask, rd.secondWo);
-    f3 totalBsdf = mi_eval(secondSd, d, 0xFu, rd.secondWo);
-    float totalPdf = mi_pdf(secondSd, d, 0xFu, rd.secondWo);
+    const BsdfPair bp = mi_eval_pair(secondSd, d, rd.secondComp, rd.secondWo);
+    const f3 lobeSpecificBsdf = bp.lobeBsdf, totalBsdf = bp.totalBsdf;
+    const float lobeSpecificPdf = bp.lobePdf, totalPdf = bp.totalPdf;
     if (rd.pathLength > 2 && !any_gt0(totalBsdf)) return mk3(0.f);
     float misWeight = 1.f;
     if (rd.pathLength == 3)

@@ -75,3 +75,28 @@ def test_closest_hits_match_the_oracle_tree(rs, oracle_mod, scenes, which):
     shape = p.bvh_shape()
     assert shape["leaf_triangles"] == sc.num_triangles
     p.close()
+
+
+@pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
+def test_nan_rays_miss_without_traversal(rs, oracle_mod, scenes):
+    """A NaN in the origin, direction or interval (a NaN camera time makes such rays) hits nothing
+    and visits no node, on the GPU and in the oracle alike."""
+    sc = scenes.terrain_spheres(seed=9, grid=64, spheres=20, subdiv=2, lights=8, extent=30.0, height=3.0)
+    p = rs.ReservoirSplatting({"maxSurfaceBounces": 1}, 16, 16)
+    p.set_scene(sc)
+    ora = oracle_mod.OraclePass({"maxSurfaceBounces": 1}, 16, 16)
+    ora.set_scene(sc)
+    lib = oracle_mod.load()
+    lib.ro_test_closest.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.ro_test_closest.restype = C.c_int
+    base = np.array([0.0, 10.0, 0.0, 0.0, -1.0, 0.0, 0.0, 1e30], np.float32)  # straight down onto the terrain
+    rays = np.tile(base, (9, 1))
+    for k in range(8):
+        rays[k + 1, k] = np.nan
+    prim, tuv, counts = p.trace_rays(rays)
+    assert prim[0] >= 0 and counts[0, 0] > 0
+    assert (prim[1:] == -1).all() and (counts[1:] == 0).all()
+    for i in range(1, len(rays)):
+        tv = np.zeros(3, np.float32)
+        assert lib.ro_test_closest(ora._h, np.ascontiguousarray(rays[i]).ctypes.data, tv.ctypes.data) == -1
+    p.close()
