@@ -98,16 +98,24 @@ RS_HD void recalculate_camera_vectors(CameraData& c, f3 forward)
     c.cameraV = c.cameraV * vlen;
 }
 
-// CameraManager::orientCamera: camera at `time` seconds before the current frame.
-RS_HD void orient_camera(const CameraManager& cm, CameraData& c, uint32_t frameCount, float time)
+// The keyframe pair and interpolation weight of CameraManager::orientCamera at `time`.
+RS_HD void camera_keyframes_at(const CameraManager& cm, uint32_t frameCount, float time, int& first, int& second, float& t)
 {
     const int K = (int)cm.keyframes;
     int currIndex = (int)(frameCount % cm.keyframes);
     int frameIndex = (int)f_floor(time / cm.artificialFrameTime);
-    int firstCameraIndex = (currIndex - frameIndex - 1 + K) % K;
-    if (firstCameraIndex < 0) firstCameraIndex += K; // times outside [0, shutter + frame time] stay in the ring
-    int secondCameraIndex = (firstCameraIndex + 1 + K) % K;
-    float t = (time - (float)frameIndex * cm.artificialFrameTime) / cm.artificialFrameTime;
+    first = (currIndex - frameIndex - 1 + K) % K;
+    if (first < 0) first += K; // times outside [0, shutter + frame time] stay in the ring
+    second = (first + 1 + K) % K;
+    t = (time - (float)frameIndex * cm.artificialFrameTime) / cm.artificialFrameTime;
+}
+
+// CameraManager::orientCamera: camera at `time` seconds before the current frame.
+RS_HD void orient_camera(const CameraManager& cm, CameraData& c, uint32_t frameCount, float time)
+{
+    int firstCameraIndex, secondCameraIndex;
+    float t;
+    camera_keyframes_at(cm, frameCount, time, firstCameraIndex, secondCameraIndex, t);
     f3 firstPos = cm.positions[firstCameraIndex], firstTarget = cm.targets[firstCameraIndex];
     f3 secondPos = cm.positions[secondCameraIndex], secondTarget = cm.targets[secondCameraIndex];
     c.up = mk3(0.f, 1.f, 0.f);
@@ -116,6 +124,52 @@ RS_HD void orient_camera(const CameraManager& cm, CameraData& c, uint32_t frameC
     f3 secondForward = normalize(secondTarget - secondPos);
     f3 interpolatedForward = angular_lerp(firstForward, secondForward, t);
     recalculate_camera_vectors(c, interpolatedForward);
+}
+
+// The parts of orient_camera that depend only on the frame (its keyframes and camera): each
+// keyframe's forward direction, the angular_lerp axis and angle of each keyframe pair
+// (i, i + 1 mod K), and the film extents of recalculate_camera_vectors.  camera_table_* compute
+// them with orient_camera's own operations, so orient_camera_table returns orient_camera's bits
+// while evaluating per call only what depends on the time.
+struct CameraTable
+{
+    f3 forward[kMaxCameraKeyframes];
+    f3 pairAxis[kMaxCameraKeyframes];
+    float pairAngle[kMaxCameraKeyframes];
+    float ulen, vlen;
+};
+RS_HD f3 camera_table_forward(const CameraManager& cm, int i) { return normalize(cm.targets[i] - cm.positions[i]); }
+// Pair (i, i + 1 mod K) from the forwards: angular_lerp(prev = forward[i], curr = forward[i + 1]).
+RS_HD void camera_table_pair(const CameraManager& cm, const f3* forward, int i, f3& axis, float& angle)
+{
+    const int K = (int)cm.keyframes;
+    const f3 prevForward = forward[i], currForward = forward[(i + 1 + K) % K];
+    axis = normalize(cross(currForward, prevForward));
+    angle = f_acos(dot(currForward, prevForward));
+}
+RS_HD void camera_table_extents(const CameraData& c, float& ulen, float& vlen)
+{
+    float fovY = camera_fovY(c);
+    ulen = c.focalDistance * f_tan(fovY * 0.5f) * c.aspectRatio;
+    vlen = c.focalDistance * f_tan(fovY * 0.5f);
+}
+// orient_camera(cm, c, frameCount, time) for c = the frame's camera, from its table.
+RS_HD void orient_camera_table(const CameraManager& cm, const CameraTable& T, CameraData& c, uint32_t frameCount, float time)
+{
+    int first, second;
+    float t;
+    camera_keyframes_at(cm, frameCount, time, first, second, t);
+    c.up = mk3(0.f, 1.f, 0.f);
+    c.posW = lerp(cm.positions[second], cm.positions[first], t);
+    const f3 currForward = T.forward[second];
+    const float angle = T.pairAngle[first];
+    f3 forward = currForward;
+    if (!(angle < 0.001f)) forward = rotate_vector(currForward, rotate_angle_axis(angle * t, T.pairAxis[first]));
+    c.cameraW = forward * c.focalDistance;
+    c.cameraU = normalize(cross(c.cameraW, c.up));
+    c.cameraV = normalize(cross(c.cameraU, c.cameraW));
+    c.cameraU = c.cameraU * T.ulen;
+    c.cameraV = c.cameraV * T.vlen;
 }
 
 // Camera::computeRayThinlensSubPixelRandom

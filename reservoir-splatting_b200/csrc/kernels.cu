@@ -54,6 +54,24 @@ __global__ void __launch_bounds__(256) k_vbuffer(uint32_t slot, uint4* __restric
     }
 }
 
+// ============================================================ camera table
+// The frame constants of orient_camera (CameraTable) for the context of `slot`; one block of
+// kMaxCameraKeyframes threads, launched after the context upload of the frame.
+__global__ void __launch_bounds__(kMaxCameraKeyframes) k_camera_table(uint32_t slot, CameraTable* __restrict__ table)
+{
+    const DevCtx& C = c_ctx[slot];
+    __shared__ f3 forward[kMaxCameraKeyframes];
+    const int i = (int)threadIdx.x, K = (int)C.cm.keyframes;
+    if (i < K) forward[i] = camera_table_forward(C.cm, i);
+    __syncthreads();
+    if (i < K)
+    {
+        table->forward[i] = forward[i];
+        camera_table_pair(C.cm, forward, i, table->pairAxis[i], table->pairAngle[i]);
+    }
+    if (i == 0) camera_table_extents(C.camera, table->ulen, table->vlen);
+}
+
 // ============================================================ initial candidates
 // Path state of the candidate tracer (PathStates.slang:85-219, the fields the pass uses).
 struct PState
@@ -339,7 +357,7 @@ __device__ __forceinline__ void path_init(const DevCtx& C, uint32_t x, uint32_t 
         path.rec.lensSample = sample_disk(u);
     }
     else path.rec.lensSample = mk2(0.f, 0.f);
-    orient_camera(C.cm, cam, C.frameCount, path.rec.time);
+    orient_camera_table(C.cm, *C.camTable, cam, C.frameCount, path.rec.time);
     Ray r = camera_ray_thinlens(cam, C.W, C.H, mk2((float)x + path.rec.subPixel.x, (float)y + path.rec.subPixel.y), path.rec.lensSample);
     path.origin = r.origin;
     path.dir = r.dir;

@@ -137,6 +137,7 @@ struct rs_pass
     DevBuf<float4> msTerms, msMisSub;
     DevBuf<uint32_t> fault;
     uint32_t* hostFault = nullptr;
+    DevBuf<CameraTable> camTable;
     DevBuf<unsigned long long> adjStats; // rs_backward counters (replayed, too long, no emitter, value mismatch)
     DevBuf<double> adjAcc;               // rs_backward FP64 sums, numMaterials x 8
     bool haveFrameCtx = false;           // hostCtx holds a frame's context (set by begin_frame)
@@ -260,6 +261,7 @@ static rs_status allocate(rs_pass* p)
     RS_CUDA(p->total.ensure(8));
     if (p->opt.gatherOption == RS_GATHER_ROBUST && needInter) RS_CUDA(p->shiftedPaths.ensure(8 * N));
     RS_CUDA(p->fault.ensure(1));
+    RS_CUDA(p->camTable.ensure(1));
     if (!p->hostFault) RS_CUDA(cudaMallocHost(&p->hostFault, sizeof(uint32_t)));
     if (!p->hostCtx) RS_CUDA(cudaMallocHost(&p->hostCtx, sizeof(DevCtx)));
     if (!p->ringCtx)
@@ -436,6 +438,7 @@ static void begin_frame(rs_pass* p, const rs_frame_desc* f)
     C.camera = p->camera;
     C.prevCamera = p->havePrevCamera ? p->prevCamera : p->camera;
     C.cm = p->cm;
+    C.camTable = p->camTable.p;
     C.W = p->W; C.H = p->H;
     C.frameCount = p->frameCount; C.seed = p->seed;
     C.useFixedSeed = o.useFixedSeed; C.fixedSeed = o.fixedSeed;
@@ -503,6 +506,7 @@ static rs_status enqueue_frame(rs_pass* p, cudaStream_t s, float4* colorDev, con
     ReservoirSet& prev = p->sets[p->prevIdx];
     auto grid = [](uint32_t n, uint32_t b) { return dim3((n + b - 1) / b); };
     RS_CUDA(cudaMemsetAsync(p->fault.p, 0, sizeof(uint32_t), s));
+    k_camera_table<<<1, kMaxCameraKeyframes, 0, s>>>(C, p->camTable.p); p->launches++;
 
     // producer side: primary hits + motion vectors (VBufferRT)
     stage(p, "vbuffer", s);

@@ -24,6 +24,7 @@ struct DevCtx
     CameraData camera;      // gScene.camera of this frame
     CameraData prevCamera;  // previous frame's camera (motion vectors)
     CameraManager cm;
+    const CameraTable* camTable; // frame constants of orient_camera (k_camera_table)
     uint32_t W, H;
     uint32_t frameCount, seed;
     uint32_t useFixedSeed, fixedSeed;
@@ -85,7 +86,7 @@ __device__ __forceinline__ float dev_mis(const DevCtx& C, float p0, float p1) //
 __device__ __forceinline__ void dev_orient(const DevCtx& C, CameraData& c, float t)
 {
     c = C.camera;
-    orient_camera(C.cm, c, C.frameCount, t);
+    orient_camera_table(C.cm, *C.camTable, c, C.frameCount, t);
 }
 
 // ------------------------------------------------------------ records
