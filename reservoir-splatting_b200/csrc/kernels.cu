@@ -114,11 +114,13 @@ __device__ __forceinline__ bool cand_add_vertex(PState& p, float sampleMIS, f3 s
     return selected;
 }
 
-__device__ __forceinline__ void next_hit(const DevCtx& C, PState& p) // PathTracer.slang:278-299
+// `hint`: a closest-hit traversal hint (trace_closest_bin), the pixel's primary hit for the camera ray.
+__device__ __forceinline__ void next_hit(const DevCtx& C, PState& p, uint32_t hint) // PathTracer.slang:278-299
 {
     p.vertex += 1;
     HitInfo h; float t;
-    const TraceHit th = C.bvh.numTris ? trace_closest_call(C.bvh, mk_ray(p.origin, p.dir, 0.f, kRayTMax), C.fault) : TraceHit{kInvalidIndex, 0.f, 0.f, 0.f};
+    const TraceHit th = C.bvh.numTris ? trace_closest_call(C.bvh, mk_ray(p.origin, p.dir, 0.f, kRayTMax), C.fault, hint)
+                                      : TraceHit{kInvalidIndex, 0.f, 0.f, 0.f};
     if (th.prim != kInvalidIndex) { h = hit_tri(th.prim, th.u, th.v); t = th.t; p.hit = h; p.flags |= kPHit; }
     else p.flags &= ~kPHit;
 }
@@ -369,7 +371,7 @@ __device__ __forceinline__ void path_init(const DevCtx& C, uint32_t x, uint32_t 
 template <bool kDirect>
 __device__ __forceinline__ void path_step(const DevCtx& C, PState& path, const RecPlanes& currRec, uint32_t i)
 {
-    next_hit(C, path);
+    next_hit(C, path, path.vertex == 0 ? pixel_hint(C, i) : kInvalidIndex);
     if (path.flags & kPHit) handle_hit<kDirect>(C, path, currRec, i);
     else
     {

@@ -138,6 +138,12 @@ struct rs_pass
     DevBuf<uint32_t> fault;
     uint32_t* hostFault = nullptr;
     DevBuf<CameraTable> camTable;
+    // side streams for independent kernels of a frame (fork/join through events on the frame's
+    // stream, so the frame stays one ordered unit for the caller and for graph capture)
+    static constexpr int kSide = 3;
+    cudaStream_t side[kSide] = {};
+    cudaEvent_t forkEv = nullptr;
+    cudaEvent_t joinEv[kSide] = {};
     DevBuf<unsigned long long> adjStats; // rs_backward counters (replayed, too long, no emitter, value mismatch)
     DevBuf<double> adjAcc;               // rs_backward FP64 sums, numMaterials x 8
     bool haveFrameCtx = false;           // hostCtx holds a frame's context (set by begin_frame)
@@ -163,6 +169,9 @@ struct rs_pass
     {
         for (auto e : events) cudaEventDestroy(e);
         for (auto e : ringEv) if (e) cudaEventDestroy(e);
+        for (auto e : joinEv) if (e) cudaEventDestroy(e);
+        for (auto q : side) if (q) cudaStreamDestroy(q);
+        if (forkEv) cudaEventDestroy(forkEv);
         if (hostFault) cudaFreeHost(hostFault);
         if (hostCtx) cudaFreeHost(hostCtx);
         if (ringCtx) cudaFreeHost(ringCtx);
@@ -262,6 +271,15 @@ static rs_status allocate(rs_pass* p)
     if (p->opt.gatherOption == RS_GATHER_ROBUST && needInter) RS_CUDA(p->shiftedPaths.ensure(8 * N));
     RS_CUDA(p->fault.ensure(1));
     RS_CUDA(p->camTable.ensure(1));
+    if (!p->forkEv)
+    {
+        RS_CUDA(cudaEventCreateWithFlags(&p->forkEv, cudaEventDisableTiming));
+        for (int i = 0; i < rs_pass::kSide; i++)
+        {
+            RS_CUDA(cudaStreamCreateWithFlags(&p->side[i], cudaStreamNonBlocking));
+            RS_CUDA(cudaEventCreateWithFlags(&p->joinEv[i], cudaEventDisableTiming));
+        }
+    }
     if (!p->hostFault) RS_CUDA(cudaMallocHost(&p->hostFault, sizeof(uint32_t)));
     if (!p->hostCtx) RS_CUDA(cudaMallocHost(&p->hostCtx, sizeof(DevCtx)));
     if (!p->ringCtx)
@@ -385,6 +403,27 @@ static CameraData to_camera(const rs_camera& c)
     return d;
 }
 
+// Streams for n independent launch chains after the work queued on s: s itself and n - 1 side
+// streams that wait for it.  With stage timing on, every chain runs on s in order.
+static void fork_streams(rs_pass* p, cudaStream_t s, int n, cudaStream_t* out)
+{
+    out[0] = s;
+    for (int i = 1; i < n; i++) out[i] = p->timing ? s : p->side[i - 1];
+    if (p->timing || n < 2) return;
+    cudaEventRecord(p->forkEv, s);
+    for (int i = 1; i < n; i++) cudaStreamWaitEvent(p->side[i - 1], p->forkEv, 0);
+}
+// s waits for the side streams of fork_streams(p, s, n, ...).
+static void join_streams(rs_pass* p, cudaStream_t s, int n)
+{
+    if (p->timing) return;
+    for (int i = 1; i < n; i++)
+    {
+        cudaEventRecord(p->joinEv[i - 1], p->side[i - 1]);
+        cudaStreamWaitEvent(s, p->joinEv[i - 1], 0);
+    }
+}
+
 static void stage(rs_pass* p, const char* name, cudaStream_t s)
 {
     if (!p->timing) return;
@@ -439,6 +478,7 @@ static void begin_frame(rs_pass* p, const rs_frame_desc* f)
     C.prevCamera = p->havePrevCamera ? p->prevCamera : p->camera;
     C.cm = p->cm;
     C.camTable = p->camTable.p;
+    C.vbuffer = p->vbuffer.p;
     C.W = p->W; C.H = p->H;
     C.frameCount = p->frameCount; C.seed = p->seed;
     C.useFixedSeed = o.useFixedSeed; C.fixedSeed = o.fixedSeed;
@@ -600,23 +640,28 @@ static rs_status enqueue_frame(rs_pass* p, cudaStream_t s, float4* colorDev, con
             K.backupShift = ShiftPlanes{p->backupShift.p, (size_t)N}; K.backupTerms = p->backupTerms.p; K.backupM = p->backupM.p;
             K.splatShift = ShiftPlanes{p->splatShift.p, (size_t)N}; K.splatTerms = p->splatTerms.p; K.splatM = p->splatM.p;
             const bool balance = o.scatterBackupMISOption == RS_MIS_BALANCE;
-            stage(p, "sbCurrScatter", s);
-            k_sb_curr_scatter<<<tiled_blocks(W, H, 128), 128, 0, s>>>(C, K);
-            stage(p, "sbCurrGather", s);
-            k_sb_curr_gather<<<tiled_blocks(W, H, 128), 128, 0, s>>>(C, K);
-            stage(p, "sbBackupGather", s);
-            k_sb_backup_gather<<<tiled_blocks(W, H, 128), 128, 0, s>>>(C, K);
-            stage(p, "sbSplatScatter", s);
-            k_sb_splat_scatter<<<grid(N, 128), 128, 0, s>>>(C, K);
+            // four independent chains: current -> previous by scatter and by gather, backup
+            // gather (-> scatter), splat scatter (-> gather); the combine reads all of them
+            cudaStream_t q[4];
+            fork_streams(p, s, 4, q);
+            stage(p, "sbCurrScatter", q[0]);
+            k_sb_curr_scatter<<<tiled_blocks(W, H, 128), 128, 0, q[0]>>>(C, K);
+            stage(p, "sbCurrGather", q[1]);
+            k_sb_curr_gather<<<tiled_blocks(W, H, 128), 128, 0, q[1]>>>(C, K);
+            stage(p, "sbBackupGather", q[2]);
+            k_sb_backup_gather<<<tiled_blocks(W, H, 128), 128, 0, q[2]>>>(C, K);
+            stage(p, "sbSplatScatter", q[3]);
+            k_sb_splat_scatter<<<grid(N, 128), 128, 0, q[3]>>>(C, K);
             p->launches += 4;
             if (balance)
             {
-                stage(p, "sbBackupScatter", s);
-                k_sb_backup_scatter<<<tiled_blocks(W, H, 128), 128, 0, s>>>(C, K);
-                stage(p, "sbSplatGather", s);
-                k_sb_splat_gather<<<grid(N, 128), 128, 0, s>>>(C, K);
+                stage(p, "sbBackupScatter", q[2]);
+                k_sb_backup_scatter<<<tiled_blocks(W, H, 128), 128, 0, q[2]>>>(C, K);
+                stage(p, "sbSplatGather", q[3]);
+                k_sb_splat_gather<<<grid(N, 128), 128, 0, q[3]>>>(C, K);
                 p->launches += 2;
             }
+            join_streams(p, s, 4);
             stage(p, "sbCombine", s);
             k_sb_combine<<<tiled_blocks(W, H, 128), 128, 0, s>>>(C, K, temporalColor);
             p->launches++;
@@ -673,10 +718,13 @@ static rs_status enqueue_frame(rs_pass* p, cudaStream_t s, float4* colorDev, con
             S.m1 = p->spM1.p; S.nw = p->spNw.p; S.terms = p->spTerms.p;
             S.shift = ShiftPlanes{p->spShift.p, (size_t)N * o.neighborCount};
             const uint32_t M = N * o.neighborCount;
-            stage(p, "spatialCentral", s);
-            k_sp_central<<<dim3(tiled_blocks(W, H, 128), o.neighborCount), 128, 0, s>>>(C, S);
-            stage(p, "spatialNeighbor", s);
-            k_sp_neighbor<<<dim3(tiled_blocks(W, H, 128), o.neighborCount), 128, 0, s>>>(C, S);
+            cudaStream_t q[2];
+            fork_streams(p, s, 2, q); // the two shift directions are independent
+            stage(p, "spatialCentral", q[0]);
+            k_sp_central<<<dim3(tiled_blocks(W, H, 128), o.neighborCount), 128, 0, q[0]>>>(C, S);
+            stage(p, "spatialNeighbor", q[1]);
+            k_sp_neighbor<<<dim3(tiled_blocks(W, H, 128), o.neighborCount), 128, 0, q[1]>>>(C, S);
+            join_streams(p, s, 2);
             stage(p, "spatialCombine", s);
             k_sp_combine<<<tiled_blocks(W, H, 128), 128, 0, s>>>(C, S, i + 1 == o.numSpatialIterations ? colorDev : nullptr);
             p->launches += 2;
@@ -1075,22 +1123,28 @@ extern "C" RS_API rs_status rs_backward_stats(rs_pass* p, uint64_t* out)
 // ------------------------------------------------------------------ ray-query diagnostics
 // Closest hits of n host rays (8 floats each: origin, direction, tMin, tMax) against the pass's
 // tree: prim (-1 on a miss), t/u/v, and per ray the nodes visited and triangles tested.
-extern "C" RS_API rs_status rs_debug_trace_rays(rs_pass* p, const float* rays, uint32_t n, int32_t* prim, float* tuv, uint32_t* counts)
+extern "C" RS_API rs_status rs_debug_trace_rays(rs_pass* p, const float* rays, const int32_t* hints, uint32_t n, int32_t* prim, float* tuv,
+                                               uint32_t* counts)
 {
     if (!p || !rays || !prim || !tuv || !counts) return fail(RS_INVALID_ARG, "NULL argument");
     if (!p->hasScene) return fail(RS_NOT_READY, "no scene");
     if (n == 0) return RS_OK;
     DevBuf<float> dr;
-    DevBuf<int32_t> dp;
+    DevBuf<int32_t> dp, dh;
     DevBuf<float> dt;
     DevBuf<uint32_t> dc, dof;
     RS_CUDA(dr.ensure(8ull * n)); RS_CUDA(dp.ensure(n)); RS_CUDA(dt.ensure(3ull * n)); RS_CUDA(dc.ensure(2ull * n)); RS_CUDA(dof.ensure(1));
     RS_CUDA(cudaMemcpy(dr.p, rays, 32ull * n, cudaMemcpyHostToDevice));
+    if (hints)
+    {
+        RS_CUDA(dh.ensure(n));
+        RS_CUDA(cudaMemcpy(dh.p, hints, 4ull * n, cudaMemcpyHostToDevice));
+    }
     RS_CUDA(cudaMemset(dof.p, 0, 4));
     BvhView bv;
     bv.binNodes = p->bvh.binNodes; bv.binRoot = p->bvh.binRoot; bv.nodes = p->bvh.nodes; bv.leafTri = p->bvh.leafTri;
     bv.tri = p->dTri.p; bv.numTris = (uint32_t)(p->scene.tri.size() / 3);
-    k_debug_trace<<<(n + 127) / 128, 128>>>(bv, dr.p, n, dp.p, dt.p, dc.p, dof.p);
+    k_debug_trace<<<(n + 127) / 128, 128>>>(bv, dr.p, hints ? dh.p : nullptr, n, dp.p, dt.p, dc.p, dof.p);
     RS_CUDA(cudaGetLastError());
     RS_CUDA(cudaDeviceSynchronize());
     uint32_t of = 0;
