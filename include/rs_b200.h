@@ -209,13 +209,9 @@ RS_API rs_status rs_update_geometry(rs_pass* pass, const float* positions, uint3
 
 /* Ray-query diagnostics (no reference counterpart).  rs_debug_trace_rays: closest hits of n host
  * rays (8 floats each: origin.xyz, direction.xyz, tMin, tMax) against the pass's BVH: prim[n] (-1 on
- * a miss), tuv[3n], counts[2n] = nodes visited and triangles tested.  hints (NULL, or n scene
- * triangle indices, -1 for none) are the traversal hints the pass gives rays through a pixel (its
- * primary hit): tested first, they bound the search and never change a result.
- * rs_debug_bvh_shape: {nodes, depth, internal children, leaf children, leaf triangles, surface-area
- * cost}.  Both synchronise. */
-RS_API rs_status rs_debug_trace_rays(rs_pass* pass, const float* rays, const int32_t* hints, uint32_t n, int32_t* prim, float* tuv,
-                                     uint32_t* counts);
+ * a miss), tuv[3n], counts[2n] = nodes visited and triangles tested.  rs_debug_bvh_shape: {nodes,
+ * depth, internal children, leaf children, leaf triangles, surface-area cost}.  Both synchronise. */
+RS_API rs_status rs_debug_trace_rays(rs_pass* pass, const float* rays, uint32_t n, int32_t* prim, float* tuv, uint32_t* counts);
 RS_API rs_status rs_debug_bvh_shape(rs_pass* pass, double* out6);
 
 /* Path-replay adjoint (no reference counterpart: the reference pass renders forward only).

@@ -67,7 +67,7 @@ def load_library():
     lib.rs_backward.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     lib.rs_backward_stats.argtypes = [C.c_void_p, C.c_void_p]
     lib.rs_update_geometry.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p]
-    lib.rs_debug_trace_rays.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.rs_debug_trace_rays.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]
     lib.rs_debug_bvh_shape.argtypes = [C.c_void_p, C.c_void_p]
     lib.rs_build_cell_lists_static.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     for name in ("rs_create", "rs_destroy", "rs_set_options", "rs_set_scene", "rs_execute", "rs_reset", "rs_set_seed",
@@ -231,17 +231,14 @@ class ReservoirSplatting:
             _check(self._lib.rs_update_geometry(self._h, q.ctypes.data, len(q), 0, C.c_void_p(stream)))
 
     # ---- ray-query diagnostics
-    def trace_rays(self, rays: np.ndarray, hints=None):
-        """Closest hits of rays (n x 8 float32: origin, direction, tMin, tMax): prim, tuv, counts.
-        hints: optional n scene triangle indices (-1 for none) tested first as traversal bounds."""
+    def trace_rays(self, rays: np.ndarray):
+        """Closest hits of rays (n x 8 float32: origin, direction, tMin, tMax): prim, tuv, counts."""
         r = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
         n = len(r)
-        h = None if hints is None else np.ascontiguousarray(hints, np.int32).reshape(n)
         prim = np.empty(n, np.int32)
         tuv = np.empty((n, 3), np.float32)
         counts = np.empty((n, 2), np.uint32)
-        _check(self._lib.rs_debug_trace_rays(self._h, r.ctypes.data, None if h is None else h.ctypes.data, n, prim.ctypes.data,
-                                             tuv.ctypes.data, counts.ctypes.data))
+        _check(self._lib.rs_debug_trace_rays(self._h, r.ctypes.data, n, prim.ctypes.data, tuv.ctypes.data, counts.ctypes.data))
         return prim, tuv, counts
 
     def bvh_shape(self) -> dict:

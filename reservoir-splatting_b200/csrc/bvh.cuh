@@ -125,32 +125,12 @@ __device__ __forceinline__ bool box_hit(float4 lo, float4 hi, const RayQ& r, flo
 // prim is kInvalidIndex on a miss.  kCount adds the nodes visited and triangles tested to
 // counts[0..1].  *overflow is set when the stack would overflow (the subtree is skipped and the
 // caller reports a device fault).
-//
-// `hint` (a scene triangle index or kInvalidIndex) is tested first: a hit on it is a valid upper
-// bound on the closest t, so the walk starts with a tighter interval.  Box tests accept every box
-// whose entry is at or below the current best t and the (t, index) minimum is kept, so the result
-// is the same for any hint; a good hint (the pixel's primary hit for a ray through that pixel)
-// only prunes nodes.
 template <bool kCount>
-__device__ __forceinline__ TraceHit trace_closest_bin(const BvhView& bv, const Ray& r, uint32_t* overflow, uint32_t* counts = nullptr,
-                                                      uint32_t hint = kInvalidIndex)
+__device__ __forceinline__ TraceHit trace_closest_bin(const BvhView& bv, const Ray& r, uint32_t* overflow, uint32_t* counts = nullptr)
 {
     TraceHit best;
     best.prim = kInvalidIndex; best.t = r.tMax; best.u = 0.f; best.v = 0.f;
     if (ray_has_nan(r)) return best;
-    if (hint < bv.numTris)
-    {
-        // scene-order vertices: the edges p1 - p0, p2 - p0 are the leaf's stored e1, e2 bit for bit
-        const float4 a = __ldg(&bv.tri[3 * (size_t)hint + 0]);
-        const float4 b = __ldg(&bv.tri[3 * (size_t)hint + 1]);
-        const float4 c = __ldg(&bv.tri[3 * (size_t)hint + 2]);
-        float t, u, v;
-        if (kCount) counts[1]++;
-        if (intersect_triangle(r.origin, r.dir, mk3(a.x, a.y, a.z), mk3(b.x, b.y, b.z), mk3(c.x, c.y, c.z), r.tMin, r.tMax, t, u, v))
-        {
-            best.t = t; best.prim = hint; best.u = u; best.v = v;
-        }
-    }
     const RayQ q = make_rayq(r);
     uint32_t stack[kTraversalStack];
     int sp = 0;
@@ -262,9 +242,9 @@ __device__ __forceinline__ bool trace_closest(const BvhView& bv, const Ray& r, H
 
 // The closest-hit traversal as a call: one copy in kernels with several ray sites and many live
 // values around them (the path tracer), where inlining it raises register pressure.
-static __device__ __noinline__ TraceHit trace_closest_call(BvhView bv, Ray r, uint32_t* overflow, uint32_t hint = kInvalidIndex)
+static __device__ __noinline__ TraceHit trace_closest_call(BvhView bv, Ray r, uint32_t* overflow)
 {
-    return trace_closest_bin<false>(bv, r, overflow, nullptr, hint);
+    return trace_closest_bin<false>(bv, r, overflow);
 }
 
 __device__ __forceinline__ bool trace_visible(const BvhView& bv, const Ray& r, uint32_t* overflow)

@@ -35,8 +35,7 @@ cudaError_t refit_wide_bvh(const float4* dTri, WideBvh* b, cudaStream_t s);
 
 // Diagnostics (bvh_debug.cu): rays are 8 floats (origin, direction, tMin, tMax); counts get the
 // nodes visited and triangles tested per ray.
-__global__ void k_debug_trace(BvhView bv, const float* rays, const int32_t* hints, uint32_t n, int32_t* prim, float* tuv, uint32_t* counts,
-                              uint32_t* overflow);
+__global__ void k_debug_trace(BvhView bv, const float* rays, uint32_t n, int32_t* prim, float* tuv, uint32_t* counts, uint32_t* overflow);
 void wide_bvh_shape(const WideBvh& b, double* out);
 
 }

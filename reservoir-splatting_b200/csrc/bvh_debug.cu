@@ -6,8 +6,8 @@
 
 namespace rs {
 
-__global__ void k_debug_trace(BvhView bv, const float* __restrict__ rays, const int32_t* __restrict__ hints, uint32_t n, int32_t* __restrict__ prim,
-                              float* __restrict__ tuv, uint32_t* __restrict__ counts, uint32_t* overflow)
+__global__ void k_debug_trace(BvhView bv, const float* __restrict__ rays, uint32_t n, int32_t* __restrict__ prim, float* __restrict__ tuv,
+                              uint32_t* __restrict__ counts, uint32_t* overflow)
 {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -16,7 +16,7 @@ __global__ void k_debug_trace(BvhView bv, const float* __restrict__ rays, const 
     uint32_t c[2] = {0u, 0u};
     TraceHit h;
     if (bv.numTris == 0) { h.prim = kInvalidIndex; h.t = 0.f; h.u = 0.f; h.v = 0.f; }
-    else h = trace_closest_bin<true>(bv, r, overflow, c, hints && hints[i] >= 0 ? (uint32_t)hints[i] : kInvalidIndex);
+    else h = trace_closest_bin<true>(bv, r, overflow, c);
     prim[i] = h.prim == kInvalidIndex ? -1 : (int32_t)h.prim;
     tuv[3 * i] = h.t; tuv[3 * i + 1] = h.u; tuv[3 * i + 2] = h.v;
     counts[2 * i] = c[0];

@@ -114,13 +114,11 @@ __device__ __forceinline__ bool cand_add_vertex(PState& p, float sampleMIS, f3 s
     return selected;
 }
 
-// `hint`: a closest-hit traversal hint (trace_closest_bin), the pixel's primary hit for the camera ray.
-__device__ __forceinline__ void next_hit(const DevCtx& C, PState& p, uint32_t hint) // PathTracer.slang:278-299
+__device__ __forceinline__ void next_hit(const DevCtx& C, PState& p) // PathTracer.slang:278-299
 {
     p.vertex += 1;
     HitInfo h; float t;
-    const TraceHit th = C.bvh.numTris ? trace_closest_call(C.bvh, mk_ray(p.origin, p.dir, 0.f, kRayTMax), C.fault, hint)
-                                      : TraceHit{kInvalidIndex, 0.f, 0.f, 0.f};
+    const TraceHit th = C.bvh.numTris ? trace_closest_call(C.bvh, mk_ray(p.origin, p.dir, 0.f, kRayTMax), C.fault) : TraceHit{kInvalidIndex, 0.f, 0.f, 0.f};
     if (th.prim != kInvalidIndex) { h = hit_tri(th.prim, th.u, th.v); t = th.t; p.hit = h; p.flags |= kPHit; }
     else p.flags &= ~kPHit;
 }
@@ -371,7 +369,7 @@ __device__ __forceinline__ void path_init(const DevCtx& C, uint32_t x, uint32_t 
 template <bool kDirect>
 __device__ __forceinline__ void path_step(const DevCtx& C, PState& path, const RecPlanes& currRec, uint32_t i)
 {
-    next_hit(C, path, path.vertex == 0 ? pixel_hint(C, i) : kInvalidIndex);
+    next_hit(C, path);
     if (path.flags & kPHit) handle_hit<kDirect>(C, path, currRec, i);
     else
     {
@@ -426,7 +424,7 @@ __global__ void __launch_bounds__(128, 3) k_candidates(uint32_t slot, ResPlanes 
 }
 
 // One sample per pixel (the reference default): records go straight to the output planes.
-__global__ void __launch_bounds__(128, 4) k_candidates_direct(uint32_t slot, ResPlanes curr, RecPlanes currRec)
+__global__ void __launch_bounds__(128, 8) k_candidates_direct(uint32_t slot, ResPlanes curr, RecPlanes currRec)
 {
     const DevCtx& C = c_ctx[slot];
     uint32_t i;
@@ -791,7 +789,7 @@ __global__ void __launch_bounds__(128, 4) k_collect(uint32_t slot, const float2*
 // RobustReuseOptimization.rt.slang:63-89
 // One thread per (pixel, neighbour): the eight lens-copy shifts are independent (the generator
 // goes to the shift by value and is never advanced), so blockIdx.y is the neighbour k.
-__global__ void __launch_bounds__(128, 8) k_robust(uint32_t slot, ResPlanes prev, RecPlanes prevRec, Shifted* __restrict__ shiftedPaths)
+__global__ void __launch_bounds__(128, 10) k_robust(uint32_t slot, ResPlanes prev, RecPlanes prevRec, Shifted* __restrict__ shiftedPaths)
 {
     const DevCtx& C = c_ctx[slot];
     uint32_t idx;
@@ -836,7 +834,7 @@ __device__ __forceinline__ void write_color(float4* color, uint32_t i, const Res
 }
 
 // ScatterTemporalResampling.rt.slang:65-174
-__global__ void __launch_bounds__(128, 3) k_scatter_resample(uint32_t slot, const float2* __restrict__ mvec, ResPlanes prev, RecPlanes prevRec,
+__global__ void __launch_bounds__(128, 6) k_scatter_resample(uint32_t slot, const float2* __restrict__ mvec, ResPlanes prev, RecPlanes prevRec,
                                                           ResPlanes curr, RecPlanes currRec, const uint32_t* __restrict__ counts,
                                                           const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ sorted,
                                                           float4* __restrict__ color)
@@ -896,7 +894,7 @@ __global__ void __launch_bounds__(128, 3) k_scatter_resample(uint32_t slot, cons
 }
 
 // GatherTemporalResampling.rt.slang:68-235
-__global__ void __launch_bounds__(128, 3) k_gather_resample(uint32_t slot, const uint4* __restrict__ vbuffer, ResPlanes curr, RecPlanes currRec,
+__global__ void __launch_bounds__(128, 6) k_gather_resample(uint32_t slot, const uint4* __restrict__ vbuffer, ResPlanes curr, RecPlanes currRec,
                                                          ResPlanes inter, RecPlanes interRec, const float2* __restrict__ floatingCoords,
                                                          float4* __restrict__ color)
 {

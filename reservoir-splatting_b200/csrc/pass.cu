@@ -478,7 +478,6 @@ static void begin_frame(rs_pass* p, const rs_frame_desc* f)
     C.prevCamera = p->havePrevCamera ? p->prevCamera : p->camera;
     C.cm = p->cm;
     C.camTable = p->camTable.p;
-    C.vbuffer = p->vbuffer.p;
     C.W = p->W; C.H = p->H;
     C.frameCount = p->frameCount; C.seed = p->seed;
     C.useFixedSeed = o.useFixedSeed; C.fixedSeed = o.fixedSeed;
@@ -1123,28 +1122,22 @@ extern "C" RS_API rs_status rs_backward_stats(rs_pass* p, uint64_t* out)
 // ------------------------------------------------------------------ ray-query diagnostics
 // Closest hits of n host rays (8 floats each: origin, direction, tMin, tMax) against the pass's
 // tree: prim (-1 on a miss), t/u/v, and per ray the nodes visited and triangles tested.
-extern "C" RS_API rs_status rs_debug_trace_rays(rs_pass* p, const float* rays, const int32_t* hints, uint32_t n, int32_t* prim, float* tuv,
-                                               uint32_t* counts)
+extern "C" RS_API rs_status rs_debug_trace_rays(rs_pass* p, const float* rays, uint32_t n, int32_t* prim, float* tuv, uint32_t* counts)
 {
     if (!p || !rays || !prim || !tuv || !counts) return fail(RS_INVALID_ARG, "NULL argument");
     if (!p->hasScene) return fail(RS_NOT_READY, "no scene");
     if (n == 0) return RS_OK;
     DevBuf<float> dr;
-    DevBuf<int32_t> dp, dh;
+    DevBuf<int32_t> dp;
     DevBuf<float> dt;
     DevBuf<uint32_t> dc, dof;
     RS_CUDA(dr.ensure(8ull * n)); RS_CUDA(dp.ensure(n)); RS_CUDA(dt.ensure(3ull * n)); RS_CUDA(dc.ensure(2ull * n)); RS_CUDA(dof.ensure(1));
     RS_CUDA(cudaMemcpy(dr.p, rays, 32ull * n, cudaMemcpyHostToDevice));
-    if (hints)
-    {
-        RS_CUDA(dh.ensure(n));
-        RS_CUDA(cudaMemcpy(dh.p, hints, 4ull * n, cudaMemcpyHostToDevice));
-    }
     RS_CUDA(cudaMemset(dof.p, 0, 4));
     BvhView bv;
     bv.binNodes = p->bvh.binNodes; bv.binRoot = p->bvh.binRoot; bv.nodes = p->bvh.nodes; bv.leafTri = p->bvh.leafTri;
     bv.tri = p->dTri.p; bv.numTris = (uint32_t)(p->scene.tri.size() / 3);
-    k_debug_trace<<<(n + 127) / 128, 128>>>(bv, dr.p, hints ? dh.p : nullptr, n, dp.p, dt.p, dc.p, dof.p);
+    k_debug_trace<<<(n + 127) / 128, 128>>>(bv, dr.p, n, dp.p, dt.p, dc.p, dof.p);
     RS_CUDA(cudaGetLastError());
     RS_CUDA(cudaDeviceSynchronize());
     uint32_t of = 0;

@@ -25,7 +25,6 @@ struct DevCtx
     CameraData prevCamera;  // previous frame's camera (motion vectors)
     CameraManager cm;
     const CameraTable* camTable; // frame constants of orient_camera (k_camera_table)
-    const uint4* vbuffer;        // this frame's primary hits (k_vbuffer), traversal hints
     uint32_t W, H;
     uint32_t frameCount, seed;
     uint32_t useFixedSeed, fixedSeed;
@@ -63,14 +62,6 @@ __device__ __forceinline__ bool tiled_pixel(uint32_t W, uint32_t H, uint32_t& i)
     if (x >= W || y >= H) return false;
     i = y * W + x;
     return true;
-}
-
-// The pixel's primary-hit triangle from the vbuffer (kInvalidIndex on a miss): a closest-hit
-// traversal hint for rays through that pixel (trace_closest_bin).
-__device__ __forceinline__ uint32_t pixel_hint(const DevCtx& C, uint32_t pix)
-{
-    const uint4 v = __ldg(&C.vbuffer[pix]);
-    return v.x == kHitTriangle ? v.y : kInvalidIndex;
 }
 
 __device__ __forceinline__ bool dev_visible(const DevCtx& C, const Ray& r) { return trace_visible(C.bvh, r, C.fault); }
@@ -369,10 +360,7 @@ __device__ inline Shifted dev_gather_lens_copy(const DevCtx& C, SampleGen sg, co
     path.thp = mk3(1.f);
     path.dir = cr.dir;
     path.active = true;
-    // fractionalPixel passed valid_float: its pixel is in the image
-    const uint32_t hint = pixel_hint(C, (uint32_t)f_floor(fractionalPixel.y) * C.W + (uint32_t)f_floor(fractionalPixel.x));
-    const TraceHit th = C.bvh.numTris ? trace_closest_call(C.bvh, mk_ray(cr.origin, cr.dir, 0.f, kRayTMax), C.fault, hint)
-                                      : TraceHit{kInvalidIndex, 0.f, 0.f, 0.f};
+    const TraceHit th = C.bvh.numTris ? trace_closest_call(C.bvh, mk_ray(cr.origin, cr.dir, 0.f, kRayTMax), C.fault) : TraceHit{kInvalidIndex, 0.f, 0.f, 0.f};
     const bool isHit = th.prim != kInvalidIndex;
     path.hit = isHit ? hit_tri(th.prim, th.u, th.v) : hit_none();
     path.origin = camera_lens_point_scaled(cam, lensSample);

@@ -111,7 +111,7 @@ __global__ void __launch_bounds__(128, 8) k_sb_curr_scatter(uint32_t slot, WaveC
 }
 
 // ---- stage 1: current sample -> previous domain by the gather shift (:116-129)
-__global__ void __launch_bounds__(128, 8) k_sb_curr_gather(uint32_t slot, WaveCtx K)
+__global__ void __launch_bounds__(128, 10) k_sb_curr_gather(uint32_t slot, WaveCtx K)
 {
     const DevCtx& C = c_ctx[slot];
     uint32_t ri;
@@ -184,7 +184,7 @@ __global__ void __launch_bounds__(128, 8) k_sb_backup_scatter(uint32_t slot, Wav
 }
 
 // ---- stage 1: splatted previous sample -> current domain (:218-235), one thread per splat
-__global__ void __launch_bounds__(128, 7) k_sb_splat_scatter(uint32_t slot, WaveCtx K)
+__global__ void __launch_bounds__(128, 10) k_sb_splat_scatter(uint32_t slot, WaveCtx K)
 {
     const DevCtx& C = c_ctx[slot];
     uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -366,7 +366,7 @@ __device__ __forceinline__ bool spatial_neighbor(const DevCtx& C, uint32_t itera
     return valid_int(C, nx, ny);
 }
 
-__global__ void __launch_bounds__(128, 7) k_sp_central(uint32_t slot, SpatialCtx S)
+__global__ void __launch_bounds__(128, 10) k_sp_central(uint32_t slot, SpatialCtx S)
 {
     const DevCtx& C = c_ctx[slot];
     // blockIdx.y: the neighbour; blockIdx.x / threadIdx.x: the pixel (tiled)
@@ -396,7 +396,7 @@ __global__ void __launch_bounds__(128, 7) k_sp_central(uint32_t slot, SpatialCtx
     S.m1[t] = m1;
 }
 
-__global__ void __launch_bounds__(128, 6) k_sp_neighbor(uint32_t slot, SpatialCtx S)
+__global__ void __launch_bounds__(128, 9) k_sp_neighbor(uint32_t slot, SpatialCtx S)
 {
     const DevCtx& C = c_ctx[slot];
     // blockIdx.y: the neighbour; blockIdx.x / threadIdx.x: the pixel (tiled)

@@ -100,37 +100,3 @@ def test_nan_rays_miss_without_traversal(rs, oracle_mod, scenes):
         tv = np.zeros(3, np.float32)
         assert lib.ro_test_closest(ora._h, np.ascontiguousarray(rays[i]).ctypes.data, tv.ctypes.data) == -1
     p.close()
-
-
-@pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
-def test_traversal_hints_never_change_a_hit(rs, scenes):
-    """The pass hints closest-hit traversals with the pixel's primary hit (tested first, its t bounds
-    the walk).  Any hint must give the same triangle and t, u, v bits as no hint: the true closest
-    triangle, a triangle the ray hits farther away, a random triangle, an out-of-range index.  The
-    true closest hint visits no more nodes in total."""
-    sc = scenes.terrain_spheres(seed=9, grid=64, spheres=20, subdiv=2, lights=8, extent=30.0, height=3.0)
-    p = rs.ReservoirSplatting({"maxSurfaceBounces": 1}, 16, 16)
-    p.set_scene(sc)
-    rng = np.random.default_rng(5)
-    rays = _rays(sc, rng, 4000)
-    prim0, tuv0, counts0 = p.trace_rays(rays)
-    hit = prim0 >= 0
-    assert hit.sum() > len(rays) // 4
-    # a farther hit on the same line: the closest hit of the ray restarted just past the first one
-    far = rays.copy()
-    far[hit, 6] = tuv0[hit, 0] * np.float32(1.0001) + np.float32(1e-3)
-    prim_far, _, _ = p.trace_rays(far)
-    n = sc.num_triangles
-    variants = {
-        "closest": np.where(hit, prim0, -1),
-        "farther": np.where(hit & (prim_far >= 0), prim_far, -1),
-        "random": rng.integers(0, n, len(rays)).astype(np.int32),
-        "out_of_range": np.full(len(rays), n + 7, np.int32),
-    }
-    for name, hints in variants.items():
-        prim, tuv, counts = p.trace_rays(rays, hints)
-        np.testing.assert_array_equal(prim, prim0, err_msg=name)
-        np.testing.assert_array_equal(tuv[hit], tuv0[hit], err_msg=name)
-        if name == "closest":
-            assert counts[:, 0].sum() <= counts0[:, 0].sum()
-    p.close()
