@@ -213,6 +213,11 @@ RS_API rs_status rs_update_geometry(rs_pass* pass, const float* positions, uint3
  * depth, internal children, leaf children, leaf triangles, surface-area cost}.  Both synchronise. */
 RS_API rs_status rs_debug_trace_rays(rs_pass* pass, const float* rays, uint32_t n, int32_t* prim, float* tuv, uint32_t* counts);
 RS_API rs_status rs_debug_bvh_shape(rs_pass* pass, double* out6);
+/* Ray-query counts per stage of the last frame rendered with stage timing on (no reference
+ * counterpart): rays[2i], rays[2i+1] = closest-hit and visibility queries of stage i, in the order of
+ * rs_get_stage_times; *count = stages.  Only a library built with -DRS_RAY_STATS counts (build.py
+ * build_ray_stats, raystats.py); the default library reports *count = 0.  Synchronises. */
+RS_API rs_status rs_debug_stage_rays(rs_pass* pass, uint64_t* rays, uint32_t* count);
 
 /* Path-replay adjoint (no reference counterpart: the reference pass renders forward only).
  *

@@ -52,6 +52,7 @@ def load_library():
     lib.rs_set_buffer.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]
     lib.rs_enable_stage_timing.argtypes = [C.c_void_p, C.c_uint32]
     lib.rs_get_stage_times.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_uint32), C.c_char_p, C.c_size_t]
+    lib.rs_debug_stage_rays.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_uint32)]
     lib.rs_last_launch_count.argtypes = [C.c_void_p]
     lib.rs_last_launch_count.restype = C.c_uint32
     lib.rs_last_error_string.restype = C.c_char_p
@@ -74,7 +75,7 @@ def load_library():
                  "rs_freeze", "rs_get_buffer", "rs_set_buffer", "rs_enable_stage_timing", "rs_get_stage_times",
                  "rs_debug_keep_candidates", "rs_batch_create", "rs_batch_execute", "rs_batch_destroy",
                  "rs_build_cell_lists_static", "rs_set_materials", "rs_checkpoint_bytes", "rs_checkpoint", "rs_backward",
-                 "rs_backward_stats", "rs_debug_trace_rays", "rs_debug_bvh_shape",
+                 "rs_backward_stats", "rs_debug_trace_rays", "rs_debug_bvh_shape", "rs_debug_stage_rays",
                  "rs_update_geometry"):
         getattr(lib, name).restype = C.c_int
     _lib = lib
@@ -184,6 +185,15 @@ class ReservoirSplatting:
 
     def enable_stage_timing(self, enable: bool = True):
         _check(self._lib.rs_enable_stage_timing(self._h, 1 if enable else 0))
+
+    def stage_rays(self) -> dict:
+        """{stage: (closest-hit queries, visibility queries)} of the last stage-timed frame; empty unless
+        the library was built with ray counting (build.py build_ray_stats)."""
+        cnt = C.c_uint32(64)
+        rays = np.zeros(128, np.uint64)
+        _check(self._lib.rs_debug_stage_rays(self._h, rays.ctypes.data, C.byref(cnt)))
+        names = list(self.stage_times().keys())
+        return {names[i]: (int(rays[2 * i]), int(rays[2 * i + 1])) for i in range(min(cnt.value, len(names)))}
 
     def stage_times(self) -> dict:
         cnt = C.c_uint32(64)

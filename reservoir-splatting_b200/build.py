@@ -32,15 +32,24 @@ def _deps():
         sorted((CSRC / "core").glob("*.h")) + [PKG.parent / "include" / "rs_b200.h"]
 
 
-def build(force: bool = False, verbose: bool = False) -> Path:
-    if not force and LIB.exists() and LIB.stat().st_mtime >= max(p.stat().st_mtime for p in _deps()):
-        return LIB
-    LIB.parent.mkdir(exist_ok=True)
-    cmd = [nvcc()] + ARCH + FLAGS + ["-o", str(LIB)] + [str(CSRC / s) for s in SOURCES]
+def build(force: bool = False, verbose: bool = False, lib: Path = LIB, defines=()) -> Path:
+    if not force and lib.exists() and lib.stat().st_mtime >= max(p.stat().st_mtime for p in _deps()):
+        return lib
+    lib.parent.mkdir(exist_ok=True)
+    cmd = [nvcc()] + ARCH + FLAGS + [f"-D{d}" for d in defines] + ["-o", str(lib)] + [str(CSRC / s) for s in SOURCES]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True, cwd=str(CSRC))
-    return LIB
+    return lib
+
+
+# The same library with ray-query counters (RS_RAY_STATS): for workload measurement only, the
+# counting atomics and per-stage synchronisation make it slower.
+LIB_RAY_STATS = PKG / "lib" / "librs_b200_raystats.so"
+
+
+def build_ray_stats(force: bool = False, verbose: bool = False) -> Path:
+    return build(force, verbose, LIB_RAY_STATS, ("RS_RAY_STATS",))
 
 
 if __name__ == "__main__":

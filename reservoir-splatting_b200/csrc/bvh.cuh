@@ -230,8 +230,22 @@ static __device__ __noinline__ bool trace_visible_q(const float4* __restrict__ n
     return true;
 }
 
+#ifdef RS_RAY_STATS
+// Ray counting for workload measurement (a build with -DRS_RAY_STATS only): closest-hit and
+// visibility queries, one warp-aggregated atomic per call site and warp.
+static __device__ unsigned long long g_rayStats[2];
+__device__ __forceinline__ void count_ray(int kind)
+{
+    const unsigned m = __activemask();
+    if ((threadIdx.x & 31u) == (unsigned)(__ffs(m) - 1)) atomicAdd(&g_rayStats[kind], (unsigned long long)__popc(m));
+}
+#else
+__device__ __forceinline__ void count_ray(int) {}
+#endif
+
 __device__ __forceinline__ bool trace_closest(const BvhView& bv, const Ray& r, HitInfo& hit, float& tHit, uint32_t* overflow)
 {
+    count_ray(0);
     if (bv.numTris == 0) return false;
     const TraceHit h = trace_closest_bin<false>(bv, r, overflow);
     if (h.prim == kInvalidIndex) return false;
@@ -244,11 +258,13 @@ __device__ __forceinline__ bool trace_closest(const BvhView& bv, const Ray& r, H
 // values around them (the path tracer), where inlining it raises register pressure.
 static __device__ __noinline__ TraceHit trace_closest_call(BvhView bv, Ray r, uint32_t* overflow)
 {
+    count_ray(0);
     return trace_closest_bin<false>(bv, r, overflow);
 }
 
 __device__ __forceinline__ bool trace_visible(const BvhView& bv, const Ray& r, uint32_t* overflow)
 {
+    count_ray(1);
     if (bv.numTris == 0 || ray_has_nan(r)) return true;
     return trace_visible_q(bv.nodes, bv.leafTri, make_rayq(r), overflow);
 }

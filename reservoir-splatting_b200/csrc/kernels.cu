@@ -54,6 +54,21 @@ __global__ void __launch_bounds__(256) k_vbuffer(uint32_t slot, uint4* __restric
     }
 }
 
+#ifdef RS_RAY_STATS
+// Closest-hit and visibility queries counted by the frame kernels since the last call (reset).
+cudaError_t ray_stats_take(unsigned long long out[2], cudaStream_t s)
+{
+    cudaError_t e = cudaMemcpyFromSymbolAsync(out, g_rayStats, 2 * sizeof(unsigned long long), 0, cudaMemcpyDeviceToHost, s);
+    if (e != cudaSuccess) return e;
+    e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return e;
+    const unsigned long long zero[2] = {0ull, 0ull};
+    e = cudaMemcpyToSymbolAsync(g_rayStats, zero, sizeof(zero), 0, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return e;
+    return cudaStreamSynchronize(s);
+}
+#endif
+
 // ============================================================ camera table
 // The frame constants of orient_camera (CameraTable) for the context of `slot`; one block of
 // kMaxCameraKeyframes threads, launched after the context upload of the frame.

@@ -7,6 +7,9 @@ namespace rs {
 
 __global__ void k_vbuffer(uint32_t slot, uint4* vbuffer, float2* mvec);
 __global__ void k_camera_table(uint32_t slot, CameraTable* table);
+#ifdef RS_RAY_STATS
+cudaError_t ray_stats_take(unsigned long long out[2], cudaStream_t s);
+#endif
 __global__ void k_candidates(uint32_t slot, ResPlanes curr, RecPlanes currRec);
 __global__ void k_candidates_direct(uint32_t slot, ResPlanes curr, RecPlanes currRec);
 __global__ void k_reproject(uint32_t slot, ResPlanes prev, RecPlanes prevRec, uint32_t* targets, uint32_t* counts);

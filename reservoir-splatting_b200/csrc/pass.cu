@@ -164,6 +164,9 @@ struct rs_pass
     std::vector<std::string> stageNames;
     std::vector<cudaEvent_t> events;
     std::vector<float> stageMs;
+#ifdef RS_RAY_STATS
+    std::vector<unsigned long long> stageRays; // closest, visibility per stage (RS_RAY_STATS builds)
+#endif
 
     ~rs_pass()
     {
@@ -428,6 +431,12 @@ static void stage(rs_pass* p, const char* name, cudaStream_t s)
 {
     if (!p->timing) return;
     size_t k = p->stageNames.size();
+#ifdef RS_RAY_STATS
+    // rays of the stage that ends here (stage timing runs every launch on s in order)
+    unsigned long long r[2] = {0ull, 0ull};
+    ray_stats_take(r, s);
+    if (k > 0) { p->stageRays.push_back(r[0]); p->stageRays.push_back(r[1]); }
+#endif
     p->stageNames.push_back(name);
     if (p->events.size() < k + 2)
     {
@@ -751,6 +760,9 @@ extern "C" RS_API rs_status rs_execute(rs_pass* p, const rs_frame_desc* f, void*
     p->lastStream = s;
     p->launches = 0;
     p->stageNames.clear();
+#ifdef RS_RAY_STATS
+    p->stageRays.clear();
+#endif
     const size_t N = (size_t)p->W * p->H;
     float4* colorDev = reinterpret_cast<float4*>(f->color);
     if (!colorDev)
@@ -1185,6 +1197,22 @@ extern "C" RS_API rs_status rs_get_stage_times(rs_pass* p, float* ms, uint32_t* 
         }
     }
     *count = n;
+    return RS_OK;
+}
+
+extern "C" RS_API rs_status rs_debug_stage_rays(rs_pass* p, uint64_t* rays, uint32_t* count)
+{
+    if (!p || !count) return fail(RS_INVALID_ARG, "pass or count is NULL");
+#ifdef RS_RAY_STATS
+    if (!p->timing || p->stageNames.size() < 2) { *count = 0; return RS_OK; }
+    RS_CUDA(cudaStreamSynchronize(p->lastStream));
+    const uint32_t n = (uint32_t)std::min(p->stageNames.size() - 1, p->stageRays.size() / 2);
+    if (rays)
+        for (uint32_t i = 0; i < n && i < *count; i++) { rays[2 * i] = p->stageRays[2 * i]; rays[2 * i + 1] = p->stageRays[2 * i + 1]; }
+    *count = n;
+#else
+    *count = 0;
+#endif
     return RS_OK;
 }
 
