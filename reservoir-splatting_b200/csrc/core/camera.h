@@ -137,6 +137,10 @@ struct CameraTable
     f3 pairAxis[kMaxCameraKeyframes];
     float pairAngle[kMaxCameraKeyframes];
     float ulen, vlen;
+    // the oriented camera at the two times most queries use (the current frame, 0, and the
+    // previous one, the artificial frame time, when the shutter is closed)
+    float time[2];
+    CameraData at[2];
 };
 RS_HD f3 camera_table_forward(const CameraManager& cm, int i) { return normalize(cm.targets[i] - cm.positions[i]); }
 // Pair (i, i + 1 mod K) from the forwards: angular_lerp(prev = forward[i], curr = forward[i + 1]).

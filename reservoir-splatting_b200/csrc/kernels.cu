@@ -85,6 +85,15 @@ __global__ void __launch_bounds__(kMaxCameraKeyframes) k_camera_table(uint32_t s
         camera_table_pair(C.cm, forward, i, table->pairAxis[i], table->pairAngle[i]);
     }
     if (i == 0) camera_table_extents(C.camera, table->ulen, table->vlen);
+    __syncthreads();
+    if (i < 2)
+    {
+        const float t = i == 0 ? 0.f : C.cm.artificialFrameTime;
+        CameraData c = C.camera;
+        orient_camera_table(C.cm, *table, c, C.frameCount, t);
+        table->time[i] = t;
+        table->at[i] = c;
+    }
 }
 
 // ============================================================ initial candidates
@@ -372,7 +381,7 @@ __device__ __forceinline__ void path_init(const DevCtx& C, uint32_t x, uint32_t 
         path.rec.lensSample = sample_disk(u);
     }
     else path.rec.lensSample = mk2(0.f, 0.f);
-    orient_camera_table(C.cm, *C.camTable, cam, C.frameCount, path.rec.time);
+    dev_orient(C, cam, path.rec.time);
     Ray r = camera_ray_thinlens(cam, C.W, C.H, mk2((float)x + path.rec.subPixel.x, (float)y + path.rec.subPixel.y), path.rec.lensSample);
     path.origin = r.origin;
     path.dir = r.dir;

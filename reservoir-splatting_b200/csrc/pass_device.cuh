@@ -85,8 +85,13 @@ __device__ __forceinline__ float dev_mis(const DevCtx& C, float p0, float p1) //
 }
 __device__ __forceinline__ void dev_orient(const DevCtx& C, CameraData& c, float t)
 {
+    // the memoised cameras of the table, for times with the same bits (orientation is a function of
+    // the time alone within a frame)
+    const CameraTable& T = *C.camTable;
+    if (f2u(t) == f2u(T.time[0])) { c = T.at[0]; return; }
+    if (f2u(t) == f2u(T.time[1])) { c = T.at[1]; return; }
     c = C.camera;
-    orient_camera_table(C.cm, *C.camTable, c, C.frameCount, t);
+    orient_camera_table(C.cm, T, c, C.frameCount, t);
 }
 
 // ------------------------------------------------------------ records
