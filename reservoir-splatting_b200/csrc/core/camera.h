@@ -24,7 +24,17 @@ struct CameraData
     float apertureRadius;
     float shutterSpeed;
     float nearZ, farZ;
+    // derived from cameraU/V/W by camera_set_derived (normalize / length of each), kept with them
+    // by every function that sets the basis
+    f3 unitU, unitV, unitW;
+    float lenU, lenV, lenW;
 };
+
+RS_HD void camera_set_derived(CameraData& c)
+{
+    c.unitU = normalize(c.cameraU); c.unitV = normalize(c.cameraV); c.unitW = normalize(c.cameraW);
+    c.lenU = length(c.cameraU); c.lenV = length(c.cameraV); c.lenW = length(c.cameraW);
+}
 
 RS_HD float camera_fovY(const CameraData& c)
 {
@@ -42,6 +52,7 @@ RS_HD void camera_update_basis(CameraData& c)
     c.cameraU = c.cameraU * ulen;
     const float vlen = c.focalDistance * f_tan(fovY * 0.5f);
     c.cameraV = c.cameraV * vlen;
+    camera_set_derived(c);
 }
 
 struct CameraManager
@@ -96,6 +107,7 @@ RS_HD void recalculate_camera_vectors(CameraData& c, f3 forward)
     float vlen = c.focalDistance * f_tan(fovY * 0.5f);
     c.cameraU = c.cameraU * ulen;
     c.cameraV = c.cameraV * vlen;
+    camera_set_derived(c);
 }
 
 // The keyframe pair and interpolation weight of CameraManager::orientCamera at `time`.
@@ -174,6 +186,7 @@ RS_HD void orient_camera_table(const CameraManager& cm, const CameraTable& T, Ca
     c.cameraV = normalize(cross(c.cameraU, c.cameraW));
     c.cameraU = c.cameraU * T.ulen;
     c.cameraV = c.cameraV * T.vlen;
+    camera_set_derived(c);
 }
 
 // Camera::computeRayThinlensSubPixelRandom
@@ -188,9 +201,9 @@ RS_HD Ray camera_ray_thinlens(const CameraData& c, uint32_t W, uint32_t H, f2 fr
     ray.origin = c.posW;
     ray.dir = c.cameraU * ndc.x + c.cameraV * ndc.y + c.cameraW;
     f3 rayTarget = ray.origin + ray.dir;
-    ray.origin += (normalize(c.cameraU) * lensSample.x + normalize(c.cameraV) * lensSample.y) * c.apertureRadius;
+    ray.origin += (c.unitU * lensSample.x + c.unitV * lensSample.y) * c.apertureRadius;
     ray.dir = normalize(rayTarget - ray.origin);
-    float invCos = 1.f / dot(normalize(c.cameraW), ray.dir);
+    float invCos = 1.f / dot(c.unitW, ray.dir);
     ray.tMin = c.nearZ * invCos;
     ray.tMax = c.farZ * invCos;
     return ray;
@@ -200,7 +213,7 @@ RS_HD Ray camera_ray_thinlens(const CameraData& c, uint32_t W, uint32_t H, f2 fr
 // (PathTracer.slang:218-220, 817-819).
 RS_HD f3 camera_lens_point(const CameraData& c, f2 lensSample)
 {
-    return c.posW + (normalize(c.cameraU) * lensSample.x + normalize(c.cameraV) * lensSample.y) * c.apertureRadius;
+    return c.posW + (c.unitU * lensSample.x + c.unitV * lensSample.y) * c.apertureRadius;
 }
 
 // Lens point written as posW + ((aperture * lens.x) * U^ + (aperture * lens.y) * V^)
@@ -208,7 +221,7 @@ RS_HD f3 camera_lens_point(const CameraData& c, f2 lensSample)
 RS_HD f3 camera_lens_point_scaled(const CameraData& c, f2 lensSample)
 {
     float lx = c.apertureRadius * lensSample.x, ly = c.apertureRadius * lensSample.y;
-    return c.posW + (normalize(c.cameraU) * lx + normalize(c.cameraV) * ly);
+    return c.posW + (c.unitU * lx + c.unitV * ly);
 }
 
 } // namespace rs

@@ -40,10 +40,10 @@ __global__ void __launch_bounds__(256) k_vbuffer(uint32_t slot, uint4* __restric
         // Scene::getPrevPosW (VBufferRT.slang:84): the hit on the previous frame's geometry
         f3 prevPosW = hit_position(reinterpret_cast<const f4*>(C.prevTri), h);
         f3 d = prevPosW - pc.posW;
-        f3 camRay = mk3(dot(normalize(pc.cameraU), d), dot(normalize(pc.cameraV), d), dot(normalize(pc.cameraW), d));
-        float lw = length(pc.cameraW);
+        f3 camRay = mk3(dot(pc.unitU, d), dot(pc.unitV, d), dot(pc.unitW, d));
+        float lw = pc.lenW;
         f2 film = mk2(lw * (camRay.x / camRay.z), lw * (camRay.y / camRay.z));
-        f2 pndc = mk2(film.x / length(pc.cameraU), film.y / length(pc.cameraV));
+        f2 pndc = mk2(film.x / pc.lenU, film.y / pc.lenV);
         f2 prevCrd = mk2(0.5f * pndc.x + 0.5f, -0.5f * pndc.y + 0.5f);
         mvec[i] = make_float2(prevCrd.x - p.x, prevCrd.y - p.y);
     }
@@ -169,11 +169,11 @@ __device__ void handle_hit(const DevCtx& C, PState& path, const RecPlanes& outRe
         float dist = length(sd.posW - x0);
         float distSquared = dist * dist;
         float cosNormal = dot(-path.dir, sd.faceN);
-        float cosSensor = dot(normalize(cam.cameraW), path.dir);
+        float cosSensor = dot(cam.unitW, path.dir);
         path.rec.subPixelJacobian = f_abs(cosNormal / distSquared) / f_abs(f_pow3(cosSensor));
-        f3 camDir = normalize(cam.cameraW);
+        f3 camDir = cam.unitW;
         float camZ = dot(sd.posW - cam.posW, camDir);
-        float d0 = (length(cam.cameraW) / f_abs(camZ) * dist);
+        float d0 = (cam.lenW / f_abs(camZ) * dist);
         float d1 = dist - d0;
         path.rec.lensVertexJacobian = (d0 * d0) / (d1 * d1) * (f_abs(dot(-path.dir, sd.faceN))) / (f_abs(dot(-path.dir, camDir)));
     }
@@ -482,19 +482,19 @@ __global__ void __launch_bounds__(256, 4) k_reproject(uint32_t slot, ResPlanes p
         {
             CameraData cc; dev_orient(C, cc, time);
             f2 lensLocal = mk2(cc.apertureRadius * lensSample.x, cc.apertureRadius * lensSample.y);
-            f3 lensWorld = normalize(cc.cameraU) * lensLocal.x + normalize(cc.cameraV) * lensLocal.y;
+            f3 lensWorld = cc.unitU * lensLocal.x + cc.unitV * lensLocal.y;
             Ray nr;
             nr.origin = cc.posW + lensWorld;
             f3 x1 = dev_sd(C, firstHit, mk3(0.f)).posW;
             nr.dir = normalize(x1 - nr.origin);
             nr.tMin = 0.001f * length(x1 - nr.origin);
             nr.tMax = 0.999f * length(x1 - nr.origin);
-            f3 camDir = mk3(dot(normalize(cc.cameraU), nr.dir), dot(normalize(cc.cameraV), nr.dir), dot(normalize(cc.cameraW), nr.dir));
+            f3 camDir = mk3(dot(cc.unitU, nr.dir), dot(cc.unitV, nr.dir), dot(cc.unitW, nr.dir));
             if (camDir.z > 0.001f && dev_visible(C, nr))
             {
-                float lw = length(cc.cameraW);
+                float lw = cc.lenW;
                 f2 film = mk2(lensLocal.x + lw * (camDir.x / camDir.z), lensLocal.y + lw * (camDir.y / camDir.z));
-                f2 ndc = mk2(film.x / length(cc.cameraU), film.y / length(cc.cameraV));
+                f2 ndc = mk2(film.x / cc.lenU, film.y / cc.lenV);
                 f2 nfp = mk2((0.5f * ndc.x + 0.5f) * (float)C.W, (-0.5f * ndc.y + 0.5f) * (float)C.H);
                 if (valid_float(C, nfp)) target = (uint32_t)f_floor(nfp.y) * C.W + (uint32_t)f_floor(nfp.x);
             }
@@ -530,12 +530,12 @@ __global__ void __launch_bounds__(256) k_multi_reproject(uint32_t slot, ResPlane
         CameraData cc; dev_orient(C, cc, newTime);
         f3 rayDir = x1 - cc.posW;
         f3 nd = normalize(rayDir);
-        float d = dot(nd, normalize(cc.cameraW));
+        float d = dot(nd, cc.unitW);
         if (d <= 0.001f) continue;
         if (!dev_visible(C, mk_ray(cc.posW, rayDir, 0.001f, 0.999f))) continue;
         float tanFovY = cc.focalLength == 0.f ? 0.f : cc.frameHeight / cc.focalLength;
         d *= tanFovY;
-        f2 offset = mk2(dot(nd, normalize(cc.cameraU)), -dot(nd, normalize(cc.cameraV)));
+        f2 offset = mk2(dot(nd, cc.unitU), -dot(nd, cc.unitV));
         f2 ndc = mk2(0.5f + offset.x / (d * cc.aspectRatio), 0.5f + offset.y / d);
         f2 nfp = mk2(ndc.x * (float)C.W, ndc.y * (float)C.H);
         if (!valid_float(C, nfp)) continue;

@@ -369,7 +369,7 @@ __device__ inline Shifted dev_gather_lens_copy(const DevCtx& C, SampleGen sg, co
     const bool isHit = th.prim != kInvalidIndex;
     path.hit = isHit ? hit_tri(th.prim, th.u, th.v) : hit_none();
     path.origin = camera_lens_point_scaled(cam, lensSample);
-    f3 camDir = normalize(cam.cameraW);
+    f3 camDir = cam.unitW;
     Shifted sp = shifted_default();
     sp.primaryHit = path.hit;
     sp.firstRayDir = path.dir;
@@ -385,7 +385,7 @@ __device__ inline Shifted dev_gather_lens_copy(const DevCtx& C, SampleGen sg, co
         float cosSensor = dot(camDir, path.dir);
         sp.subPixelJacobian = f_abs(cosNormal / distSquared) / f_abs(f_pow3(cosSensor));
         float camZ = dot(x1 - cam.posW, camDir);
-        float d0 = (length(cam.cameraW) / f_abs(camZ) * dist);
+        float d0 = (cam.lenW / f_abs(camZ) * dist);
         float d1 = dist - d0;
         sp.lensVertexJacobian = (d0 * d0) / (d1 * d1) * f_abs(cosNormal) / f_abs(cosSensor);
     }
@@ -409,14 +409,14 @@ __device__ inline Shifted dev_gather_primary_reconnect(const DevCtx& C, SampleGe
     ShadingData sd = dev_sd(C, primaryHit, mk3(0.f));
     f3 x1 = sd.posW, n = sd.faceN;
     path.dir = normalize(x1 - filmWorld);
-    f3 camDir = normalize(cam.cameraW);
+    f3 camDir = cam.unitW;
     float camZ = dot(x1 - cam.posW, camDir);
     float rayT = camZ / dot(path.dir, camDir);
     path.origin = x1 - path.dir * rayT;
     path.dir = normalize(x1 - path.origin);
     f3 lensOffsetWorld = path.origin - cam.posW;
-    f2 lensLocalNormalized = mk2(dot(lensOffsetWorld, normalize(cam.cameraU)) / cam.apertureRadius,
-                                 dot(lensOffsetWorld, normalize(cam.cameraV)) / cam.apertureRadius);
+    f2 lensLocalNormalized = mk2(dot(lensOffsetWorld, cam.unitU) / cam.apertureRadius,
+                                 dot(lensOffsetWorld, cam.unitV) / cam.apertureRadius);
     if (length(lensLocalNormalized) > 1.f) return shifted_default();
     float dist = length(x1 - path.origin);
     if (!dev_visible(C, mk_ray(path.origin, path.dir, 0.001f * dist, 0.999f * dist))) return shifted_default();
@@ -433,7 +433,7 @@ __device__ inline Shifted dev_gather_primary_reconnect(const DevCtx& C, SampleGe
         float cosNormal = dot(path.dir, n);
         float cosSensor = dot(camDir, path.dir);
         sp.subPixelJacobian = f_abs(cosNormal / distSquared) / f_abs(f_pow3(cosSensor));
-        float d0 = (length(cam.cameraW) / f_abs(camZ) * rayT);
+        float d0 = (cam.lenW / f_abs(camZ) * rayT);
         float d1 = rayT - d0;
         sp.lensVertexJacobian = (d0 * d0) / (d1 * d1) * (f_abs(cosNormal)) / (f_abs(cosSensor));
     }
@@ -449,8 +449,8 @@ __device__ inline Shifted dev_scatter_shift(const DevCtx& C, SampleGen sg, const
     if (hitEnvMap || !hit_valid(primaryHit)) return shifted_default();
     CameraData cam; dev_orient(C, cam, time);
     f2 lensLocal = mk2(cam.apertureRadius * lensSample.x, cam.apertureRadius * lensSample.y);
-    f3 camU = normalize(cam.cameraU);
-    f3 camV = normalize(cam.cameraV);
+    f3 camU = cam.unitU;
+    f3 camV = cam.unitV;
     ShiftPath path;
     path.thp = mk3(1.f);
     path.active = true;
@@ -458,12 +458,12 @@ __device__ inline Shifted dev_scatter_shift(const DevCtx& C, SampleGen sg, const
     ShadingData firstSd = dev_sd(C, primaryHit, mk3(0.f));
     f3 x1 = firstSd.posW, n = firstSd.faceN;
     path.dir = normalize(x1 - path.origin);
-    f3 camDir = normalize(cam.cameraW);
+    f3 camDir = cam.unitW;
     f3 camRay = mk3(dot(camU, path.dir), dot(camV, path.dir), dot(camDir, path.dir));
     if (camRay.z <= 0.001f) return shifted_default();
-    float lw = length(cam.cameraW);
+    float lw = cam.lenW;
     f2 film = mk2(lensLocal.x + lw * (camRay.x / camRay.z), lensLocal.y + lw * (camRay.y / camRay.z));
-    f2 ndc = mk2(film.x / length(cam.cameraU), film.y / length(cam.cameraV));
+    f2 ndc = mk2(film.x / cam.lenU, film.y / cam.lenV);
     f2 nfp = mk2((0.5f * ndc.x + 0.5f) * (float)C.W, (-0.5f * ndc.y + 0.5f) * (float)C.H);
     if (!valid_float(C, nfp)) return shifted_default();
     float dist = length(x1 - path.origin);
@@ -478,10 +478,10 @@ __device__ inline Shifted dev_scatter_shift(const DevCtx& C, SampleGen sg, const
     {
         float distSquared = dist * dist;
         float cosNormal = dot(-path.dir, n);
-        float cosSensor = dot(normalize(cam.cameraW), path.dir);
+        float cosSensor = dot(cam.unitW, path.dir);
         sp.subPixelJacobian = f_abs(cosNormal / distSquared) / f_abs(f_pow3(cosSensor));
         float camZ = dot(x1 - cam.posW, camDir);
-        float d0 = (length(cam.cameraW) / f_abs(camZ) * dist);
+        float d0 = (cam.lenW / f_abs(camZ) * dist);
         float d1 = dist - d0;
         sp.lensVertexJacobian = (d0 * d0) / (d1 * d1) * f_abs(cosNormal) / f_abs(cosSensor);
     }
@@ -507,9 +507,9 @@ __device__ __forceinline__ f2 pixel_dof_probs(const DevCtx& C, const uint4* vbuf
     if (hit_valid(h))
     {
         f3 x1 = dev_sd(C, h, mk3(0.f)).posW;
-        f3 camDir = normalize(cam.cameraW);
+        f3 camDir = cam.unitW;
         float camZ = dot(x1 - cam.posW, camDir);
-        float filmZ = camZ - length(cam.cameraW);
+        float filmZ = camZ - cam.lenW;
         float filmRadius = f_abs(cam.apertureRadius / camZ * filmZ);
         coc = filmRadius / normalizedFilm;
     }

@@ -52,6 +52,13 @@ int main(int argc, char** argv)
             orient_camera_table(cm, T, b, frame, time);
             const float* pa = &a.posW.x; const float* pb = &b.posW.x;
             for (int j = 0; j < 18; j++) { checked++; if (bits(pa[j]) != bits(pb[j])) mismatched++; }
+            // the derived unit vectors and lengths, and that they are those of the basis
+            const float* da = &a.unitU.x; const float* db = &b.unitU.x;
+            for (int j = 0; j < 12; j++) { checked++; if (bits(da[j]) != bits(db[j])) mismatched++; }
+            CameraData r = b;
+            camera_set_derived(r);
+            const float* dr = &r.unitU.x;
+            for (int j = 0; j < 12; j++) { checked++; if (bits(dr[j]) != bits(db[j])) mismatched++; }
         }
     }
     printf("%ld %ld\n", checked, mismatched);
@@ -75,5 +82,5 @@ def harness(tmp_path_factory):
 def test_table_orientation_has_orient_camera_bits(harness, seed):
     out = subprocess.run([str(harness), str(seed)], check=True, capture_output=True, text=True).stdout.split()
     checked, mismatched = int(out[0]), int(out[1])
-    assert checked == 200 * 400 * 18
+    assert checked == 200 * 400 * (18 + 24)
     assert mismatched == 0
