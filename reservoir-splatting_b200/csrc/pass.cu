@@ -556,23 +556,8 @@ static rs_status enqueue_frame(rs_pass* p, cudaStream_t s, float4* colorDev, con
     RS_CUDA(cudaMemsetAsync(p->fault.p, 0, sizeof(uint32_t), s));
     k_camera_table<<<1, kMaxCameraKeyframes, 0, s>>>(C, p->camTable.p); p->launches++;
 
-    // producer side: primary hits + motion vectors (VBufferRT)
-    stage(p, "vbuffer", s);
-    k_vbuffer<<<tiled_blocks(W, H, 256), 256, 0, s>>>(C, p->vbuffer.p, p->mvec.p); p->launches++;
     const float2* mvec = mvecIn ? mvecIn : p->mvec.p;
-
-    stage(p, "initialCandidates", s);
-    if (o.samplesPerPixel == 1) k_candidates_direct<<<tiled_blocks(W, H, 128), 128, 0, s>>>(C, curr.res(), curr.recp());
-    else k_candidates<<<grid(N, 128), 128, 0, s>>>(C, curr.res(), curr.recp());
-    p->launches++;
-    if (p->keepCandidates)
-    {
-        RS_CUDA(p->cand.ensure(N));
-        RS_CUDA(cudaMemcpyAsync(p->cand.a.p, curr.a.p, N * 16ull, cudaMemcpyDeviceToDevice, s));
-        RS_CUDA(cudaMemcpyAsync(p->cand.b.p, curr.b.p, N * 16ull, cudaMemcpyDeviceToDevice, s));
-        RS_CUDA(cudaMemcpyAsync(p->cand.rec.p, curr.rec.p, 7ull * N * 16ull, cudaMemcpyDeviceToDevice, s));
-    }
-
+    if (p->keepCandidates) RS_CUDA(p->cand.ensure(N));
     shouldReset = shouldReset || p->frameCount == 0;
     const bool temporal = o.enableTemporalResampling && !shouldReset;
     const bool spatial = o.enableSpatialResampling != 0;
@@ -580,14 +565,69 @@ static rs_status enqueue_frame(rs_pass* p, cudaStream_t s, float4* colorDev, con
     p->lastFusedCollect = false;
     const uint32_t numTiles = (N + kScanTileElems - 1) / kScanTileElems;
 
-    auto buildCells = [&](uint32_t* tg, uint32_t* cn, uint32_t* of, uint32_t* cu, uint32_t* un, uint32_t* so, uint32_t* sc, uint32_t* tot) {
-        k_scan_tiles<<<numTiles, 1024, 0, s>>>(cn, of, p->tileSums.p, N);
-        k_scan_tile_sums<<<1, 1024, 0, s>>>(p->tileSums.p, numTiles, tot);
-        k_scan_add<<<grid(N, 256), 256, 0, s>>>(of, p->tileSums.p, N);
-        k_fill<<<grid(N, 256), 256, 0, s>>>(tg, of, cu, un, N);
-        k_rank_cells<<<grid(N, 256), 256, 0, s>>>(tg, of, cn, un, so, sc, N);
+    auto buildCells = [&](cudaStream_t q, uint32_t* tg, uint32_t* cn, uint32_t* of, uint32_t* cu, uint32_t* un, uint32_t* so, uint32_t* sc,
+                          uint32_t* tot) {
+        k_scan_tiles<<<numTiles, 1024, 0, q>>>(cn, of, p->tileSums.p, N);
+        k_scan_tile_sums<<<1, 1024, 0, q>>>(p->tileSums.p, numTiles, tot);
+        k_scan_add<<<grid(N, 256), 256, 0, q>>>(of, p->tileSums.p, N);
+        k_fill<<<grid(N, 256), 256, 0, q>>>(tg, of, cu, un, N);
+        k_rank_cells<<<grid(N, 256), 256, 0, q>>>(tg, of, cn, un, so, sc, N);
         p->launches += 5;
     };
+
+    // Three independent chains: the primary hits and motion vectors (VBufferRT); the candidate path
+    // tracer (current reservoirs); and the temporal work that reads only the previous frame (robust
+    // neighbour shifts, reprojection of the previous samples and their cell lists).  They join
+    // before the first kernel that reads two of them.
+    cudaStream_t q[3];
+    fork_streams(p, s, 3, q);
+    stage(p, "vbuffer", q[0]);
+    k_vbuffer<<<tiled_blocks(W, H, 256), 256, 0, q[0]>>>(C, p->vbuffer.p, p->mvec.p); p->launches++;
+    stage(p, "initialCandidates", q[1]);
+    if (o.samplesPerPixel == 1) k_candidates_direct<<<tiled_blocks(W, H, 128), 128, 0, q[1]>>>(C, curr.res(), curr.recp());
+    else k_candidates<<<grid(N, 128), 128, 0, q[1]>>>(C, curr.res(), curr.recp());
+    p->launches++;
+    if (p->keepCandidates)
+    {
+        RS_CUDA(cudaMemcpyAsync(p->cand.a.p, curr.a.p, N * 16ull, cudaMemcpyDeviceToDevice, q[1]));
+        RS_CUDA(cudaMemcpyAsync(p->cand.b.p, curr.b.p, N * 16ull, cudaMemcpyDeviceToDevice, q[1]));
+        RS_CUDA(cudaMemcpyAsync(p->cand.rec.p, curr.rec.p, 7ull * N * 16ull, cudaMemcpyDeviceToDevice, q[1]));
+    }
+    if (temporal)
+    {
+        const bool robust = o.gatherOption == RS_GATHER_ROBUST && (o.temporalReuse == RS_GATHER_ONLY || o.temporalReuse == RS_SCATTER_BACKUP);
+        if (robust)
+        {
+            stage(p, "robustReuse", q[2]);
+            k_robust<<<dim3(tiled_blocks(W, H, 128), 8), 128, 0, q[2]>>>(C, prev.res(), prev.recp(), p->shiftedPaths.p); p->launches++;
+        }
+        if (o.temporalReuse == RS_SCATTER_ONLY || o.temporalReuse == RS_SCATTER_BACKUP)
+        {
+            stage(p, "reproject", q[2]);
+            RS_CUDA(cudaMemsetAsync(p->counts.p, 0, N * 4ull, q[2]));
+            RS_CUDA(cudaMemsetAsync(p->cursor.p, 0, N * 4ull, q[2]));
+            k_reproject<<<tiled_blocks(W, H, 256), 256, 0, q[2]>>>(C, prev.res(), prev.recp(), p->targets.p, p->counts.p); p->launches++;
+            stage(p, "sortCells", q[2]);
+            buildCells(q[2], p->targets.p, p->counts.p, p->offsets.p, p->cursor.p, p->unsortedSplats.p, p->sortedSplats.p,
+                       o.temporalReuse == RS_SCATTER_BACKUP ? p->sortedCell.p : nullptr, p->total.p);
+        }
+        else if (o.temporalReuse == RS_MULTI_SCATTER)
+        {
+            const uint32_t P = o.numTimePartitions;
+            stage(p, "multiReproject", q[2]);
+            RS_CUDA(cudaMemsetAsync(p->counts.p, 0, (size_t)P * N * 4ull, q[2]));
+            RS_CUDA(cudaMemsetAsync(p->cursor.p, 0, (size_t)P * N * 4ull, q[2]));
+            k_multi_reproject<<<tiled_blocks(W, H, 256), 256, 0, q[2]>>>(C, prev.res(), prev.recp(), p->targets.p, p->counts.p); p->launches++;
+            stage(p, "multiSortCells", q[2]);
+            for (uint32_t j = 0; j < P; j++)
+            {
+                size_t b = (size_t)j * N;
+                buildCells(q[2], p->targets.p + b, p->counts.p + b, p->offsets.p + b, p->cursor.p + b, p->unsortedSplats.p + b,
+                           p->sortedSplats.p + b, p->sortedCell.p + b, p->total.p + j);
+            }
+        }
+    }
+    join_streams(p, s, 3);
 
     float4* temporalColor = spatial ? nullptr : colorDev;
     if (temporal)
@@ -595,23 +635,12 @@ static rs_status enqueue_frame(rs_pass* p, cudaStream_t s, float4* colorDev, con
         switch (o.temporalReuse)
         {
         case RS_GATHER_ONLY:
-            if (o.gatherOption == RS_GATHER_ROBUST)
-            {
-                stage(p, "robustReuse", s);
-                k_robust<<<dim3(tiled_blocks(W, H, 128), 8), 128, 0, s>>>(C, prev.res(), prev.recp(), p->shiftedPaths.p); p->launches++;
-            }
             stage(p, "collect", s);
             k_collect<<<tiled_blocks(W, H, 128), 128, 0, s>>>(C, mvec, prev.res(), prev.recp(), p->inter.res(), p->inter.recp(), p->floatingCoords.p, p->shiftedPaths.p); p->launches++;
             stage(p, "gatherResample", s);
             k_gather_resample<<<tiled_blocks(W, H, 128), 128, 0, s>>>(C, p->vbuffer.p, curr.res(), curr.recp(), p->inter.res(), p->inter.recp(), p->floatingCoords.p, temporalColor); p->launches++;
             break;
         case RS_SCATTER_ONLY:
-            stage(p, "reproject", s);
-            RS_CUDA(cudaMemsetAsync(p->counts.p, 0, N * 4ull, s));
-            RS_CUDA(cudaMemsetAsync(p->cursor.p, 0, N * 4ull, s));
-            k_reproject<<<tiled_blocks(W, H, 256), 256, 0, s>>>(C, prev.res(), prev.recp(), p->targets.p, p->counts.p); p->launches++;
-            stage(p, "sortCells", s);
-            buildCells(p->targets.p, p->counts.p, p->offsets.p, p->cursor.p, p->unsortedSplats.p, p->sortedSplats.p, nullptr, p->total.p);
             stage(p, "scatterResample", s);
             k_scatter_resample<<<tiled_blocks(W, H, 128), 128, 0, s>>>(C, mvec, prev.res(), prev.recp(), curr.res(), curr.recp(), p->counts.p, p->offsets.p, p->sortedSplats.p, temporalColor); p->launches++;
             break;
@@ -621,20 +650,9 @@ static rs_status enqueue_frame(rs_pass* p, cudaStream_t s, float4* colorDev, con
             p->lastFusedCollect = fused;
             if (!fused)
             {
-                if (o.gatherOption == RS_GATHER_ROBUST)
-                {
-                    stage(p, "robustReuse", s);
-                    k_robust<<<dim3(tiled_blocks(W, H, 128), 8), 128, 0, s>>>(C, prev.res(), prev.recp(), p->shiftedPaths.p); p->launches++;
-                }
                 stage(p, "collect", s);
                 k_collect<<<tiled_blocks(W, H, 128), 128, 0, s>>>(C, mvec, prev.res(), prev.recp(), p->inter.res(), p->inter.recp(), p->floatingCoords.p, p->shiftedPaths.p); p->launches++;
             }
-            stage(p, "reproject", s);
-            RS_CUDA(cudaMemsetAsync(p->counts.p, 0, N * 4ull, s));
-            RS_CUDA(cudaMemsetAsync(p->cursor.p, 0, N * 4ull, s));
-            k_reproject<<<tiled_blocks(W, H, 256), 256, 0, s>>>(C, prev.res(), prev.recp(), p->targets.p, p->counts.p); p->launches++;
-            stage(p, "sortCells", s);
-            buildCells(p->targets.p, p->counts.p, p->offsets.p, p->cursor.p, p->unsortedSplats.p, p->sortedSplats.p, p->sortedCell.p, p->total.p);
             WaveCtx K;
             K.fused = fused;
             K.mvec = mvec;
@@ -678,17 +696,6 @@ static rs_status enqueue_frame(rs_pass* p, cudaStream_t s, float4* colorDev, con
         case RS_MULTI_SCATTER:
         {
             const uint32_t P = o.numTimePartitions;
-            stage(p, "multiReproject", s);
-            RS_CUDA(cudaMemsetAsync(p->counts.p, 0, (size_t)P * N * 4ull, s));
-            RS_CUDA(cudaMemsetAsync(p->cursor.p, 0, (size_t)P * N * 4ull, s));
-            k_multi_reproject<<<tiled_blocks(W, H, 256), 256, 0, s>>>(C, prev.res(), prev.recp(), p->targets.p, p->counts.p); p->launches++;
-            stage(p, "multiSortCells", s);
-            for (uint32_t j = 0; j < P; j++)
-            {
-                size_t b = (size_t)j * N;
-                buildCells(p->targets.p + b, p->counts.p + b, p->offsets.p + b, p->cursor.p + b, p->unsortedSplats.p + b, p->sortedSplats.p + b,
-                           p->sortedCell.p + b, p->total.p + j);
-            }
             stage(p, "multiScatterResample", s);
             MultiCtx M;
             M.mvec = mvec; M.curr = curr.res(); M.currRec = curr.recp(); M.prev = prev.res(); M.prevRec = prev.recp();
