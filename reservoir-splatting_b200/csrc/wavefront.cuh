@@ -111,7 +111,7 @@ __global__ void __launch_bounds__(128, 8) k_sb_curr_scatter(uint32_t slot, WaveC
 }
 
 // ---- stage 1: current sample -> previous domain by the gather shift (:116-129)
-__global__ void __launch_bounds__(128, 10) k_sb_curr_gather(uint32_t slot, WaveCtx K)
+__global__ void __launch_bounds__(128, 9) k_sb_curr_gather(uint32_t slot, WaveCtx K)
 {
     const DevCtx& C = c_ctx[slot];
     uint32_t ri;
@@ -135,7 +135,7 @@ __global__ void __launch_bounds__(128, 10) k_sb_curr_gather(uint32_t slot, WaveC
 }
 
 // ---- stage 1: backup sample -> current domain (:156-166)
-__global__ void __launch_bounds__(128, 8) k_sb_backup_gather(uint32_t slot, WaveCtx K)
+__global__ void __launch_bounds__(128, 9) k_sb_backup_gather(uint32_t slot, WaveCtx K)
 {
     const DevCtx& C = c_ctx[slot];
     uint32_t ri;
@@ -184,7 +184,7 @@ __global__ void __launch_bounds__(128, 8) k_sb_backup_scatter(uint32_t slot, Wav
 }
 
 // ---- stage 1: splatted previous sample -> current domain (:218-235), one thread per splat
-__global__ void __launch_bounds__(128, 10) k_sb_splat_scatter(uint32_t slot, WaveCtx K)
+__global__ void __launch_bounds__(128, 9) k_sb_splat_scatter(uint32_t slot, WaveCtx K)
 {
     const DevCtx& C = c_ctx[slot];
     uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -207,7 +207,7 @@ __global__ void __launch_bounds__(128, 10) k_sb_splat_scatter(uint32_t slot, Wav
 }
 
 // ---- stage 2 (Balance): updated splat -> previous domain by the gather shift (:237-253)
-__global__ void __launch_bounds__(128, 8) k_sb_splat_gather(uint32_t slot, WaveCtx K)
+__global__ void __launch_bounds__(128, 9) k_sb_splat_gather(uint32_t slot, WaveCtx K)
 {
     const DevCtx& C = c_ctx[slot];
     uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
