@@ -242,6 +242,39 @@ RS_API rs_status rs_backward(rs_pass* pass, const void* checkpointDevice, const 
                              void* cudaStream);
 RS_API rs_status rs_backward_stats(rs_pass* pass, uint64_t* stats4);
 
+/* Frame output: the ToneMapper pass followed by the FrameDumper pass's 8-bit sRGB conversion
+ * (RenderPasses/ToneMapper/ToneMapping.ps.slang:45-173, ToneMapper.cpp:538-550,
+ * FrameDumper.cpp:80-90,151-158).  rs_tonemap reads width*height float4 colours (device memory,
+ * e.g. rs_frame_desc.color) and writes width*height RGBA8 texels (device memory, R in the low
+ * byte): auto exposure (key 0.042 over the mean log2 luminance, from the image itself), the
+ * exposure scale 2^exposureCompensation (times filmSpeed/100 / (shutter * fNumber^2) without auto
+ * exposure), the operator, the optional clamp, then sRGB encoding to 8 bits; alpha is stored
+ * linearly.  With autoExposure, workspaceDev is device memory of rs_tonemap_workspace_bytes().
+ * White balance is not implemented.  Work is enqueued on `cudaStream`; nothing is allocated. */
+typedef enum rs_tonemap_operator {
+    RS_TONEMAP_LINEAR = 0,
+    RS_TONEMAP_REINHARD = 1,
+    RS_TONEMAP_REINHARD_MODIFIED = 2,
+    RS_TONEMAP_HEJI_HABLE_ALU = 3,
+    RS_TONEMAP_HABLE_UC2 = 4,
+    RS_TONEMAP_ACES = 5
+} rs_tonemap_operator;
+
+typedef struct rs_tonemap_options {
+    uint32_t op;                /* rs_tonemap_operator (ToneMapperOperator) */
+    float exposureCompensation; /* EV steps */
+    uint32_t autoExposure;
+    float filmSpeed, fNumber, shutter; /* manual exposure (shutter = reciprocal seconds) */
+    uint32_t clamp;
+    float whiteMaxLuminance;    /* ReinhardModified */
+    float whiteScale;           /* HableUc2 */
+} rs_tonemap_options;
+
+RS_API void rs_tonemap_default_options(rs_tonemap_options* options);
+RS_API size_t rs_tonemap_workspace_bytes(void);
+RS_API rs_status rs_tonemap(const void* colorDev, uint32_t width, uint32_t height, const rs_tonemap_options* options, void* rgba8Dev,
+                            void* workspaceDev, void* cudaStream);
+
 /* Allocation-free cell-list build.  This call has no counterpart in the reference.
  *
  * It exists for callers that cannot allocate device memory when they run: a host that hands

@@ -60,6 +60,15 @@ class RsFrameDesc(C.Structure):
                 ("colorHost", C.c_void_p), ("sceneShouldReset", C.c_uint32)]
 
 
+TONEMAP_OPERATOR = {"Linear": 0, "Reinhard": 1, "ReinhardModified": 2, "HejiHableAlu": 3, "HableUc2": 4, "Aces": 5}
+
+
+class RsTonemapOptions(C.Structure):
+    _fields_ = [("op", C.c_uint32), ("exposureCompensation", C.c_float), ("autoExposure", C.c_uint32), ("filmSpeed", C.c_float),
+                ("fNumber", C.c_float), ("shutter", C.c_float), ("clamp", C.c_uint32), ("whiteMaxLuminance", C.c_float),
+                ("whiteScale", C.c_float)]
+
+
 def default_options(width: int = 1920, height: int = 1080) -> RsOptions:
     """ReservoirSplatting.h:124-184 defaults (the C library's rs_default_options, restated for CPU-only use)."""
     o = RsOptions()

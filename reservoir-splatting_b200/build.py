@@ -14,7 +14,7 @@ from pathlib import Path
 PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 LIB = PKG / "lib" / "librs_b200.so"
-SOURCES = ["kernels.cu", "pass.cu", "bvh_build.cu", "bvh_debug.cu", "cells_static.cu"]
+SOURCES = ["kernels.cu", "pass.cu", "bvh_build.cu", "bvh_debug.cu", "cells_static.cu", "frame_output.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-fmad=false", "-prec-div=true", "-prec-sqrt=true",
          "-Xcompiler", "-fPIC,-ffp-contract=off,-fvisibility=hidden", "-shared"]
