@@ -91,15 +91,20 @@ typedef struct rs_options {
     uint32_t frameHeight;                /* <= 4096 */
 } rs_options;
 
-/* StandardMaterial metal-rough parameters; 64 bytes.  flags bit 0 = double sided. */
+/* StandardMaterial parameters; 64 bytes.  flags bit 0 = double sided; bit 1 = the spec-gloss
+ * shading model (ShadingModel::SpecGloss, StandardMaterial.slang:88-94, what Falcor's OBJ import
+ * makes): baseColor is the diffuse colour, specular[3] the specular colour, `roughness` holds the
+ * glossiness and metallic is derived; without bit 1 the model is metal-rough and specular[] is
+ * unused. */
 typedef struct rs_material {
     float baseColor[3];
-    float roughness;
+    float roughness;                     /* glossiness with the spec-gloss model */
     float emissive[3];                   /* radiance, emissive factor included */
-    float metallic;
+    float metallic;                      /* metal-rough only */
     float ior;
     uint32_t flags;
-    float reserved[6];
+    float specular[3];                   /* spec-gloss only */
+    float reserved[3];
 } rs_material;
 
 /* Flattened world-space triangle soup (the ray-traced geometry of a Falcor scene). */

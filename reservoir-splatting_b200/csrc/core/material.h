@@ -41,11 +41,12 @@ enum LobeType : uint32_t
 constexpr float kMinCosTheta = 1e-6f;   // IBSDF.slang:35
 constexpr float kMinGGXAlpha = 0.0064f; // StandardBSDF.slang:52
 
-enum MaterialFlags : uint32_t { kMtlDoubleSided = 1u };
+enum MaterialFlags : uint32_t { kMtlDoubleSided = 1u, kMtlSpecGloss = 2u };
 
-// One material: 16 floats.  baseColor/roughness/metallic/ior are the
-// StandardMaterial metal-rough parameters; emissive already includes
-// the emissive factor.
+// One material: 16 floats.  Metal-rough (StandardMaterial's default shading model): baseColor,
+// roughness, metallic, ior.  Spec-gloss (kMtlSpecGloss, the model Falcor's OBJ import uses):
+// baseColor is the diffuse colour, specular the specular colour and `roughness` holds the
+// glossiness.  emissive already includes the emissive factor.
 struct alignas(16) MaterialData
 {
     float baseColor[3];
@@ -54,7 +55,8 @@ struct alignas(16) MaterialData
     float metallic;
     float ior;
     uint32_t flags;
-    float pad[6];
+    float specular[3];
+    float pad[3];
 };
 
 // Material instance parameters (StandardMaterial.slang:48-115, opaque subset).
@@ -67,17 +69,41 @@ struct BsdfData
     f3 emission;
 };
 
+// The metallic factor of a spec-gloss material (ShadingUtils.slang:57-71): the metallic m for which
+// the UE4 metal-rough conversion with specular level 0.5 (F0 = 0.04) gives the two colours'
+// luminances, the root of 0.04 m^2 + (s + d - 0.08) m + (0.04 - s) = 0; 0 without specular.  Like
+// the reference it can return a negative value or NaN for colour pairs no metallic produces.
+RS_HD float spec_gloss_metallic(f3 diffuse, f3 specular)
+{
+    const float d = luminance(diffuse), s = luminance(specular);
+    if (s == 0.f) return 0.f;
+    const float b = s + d - 0.08f;
+    const float c = 0.04f - s;
+    const float root = f_sqrt(b * b - 0.16f * c);
+    return (root - b) * 12.5f;
+}
+
 RS_HD BsdfData setup_material(const MaterialData& m, bool frontFacing)
 {
     BsdfData d;
-    float f = (m.ior - 1.f) / (m.ior + 1.f);
-    float F0 = f * f;
     f3 baseColor = mk3(m.baseColor[0], m.baseColor[1], m.baseColor[2]);
-    float metallic = m.metallic;
-    d.diffuse = lerp(baseColor, mk3(0.f), metallic);
-    d.specular = lerp(mk3(F0), baseColor, metallic);
-    d.roughness = m.roughness;
-    d.metallic = metallic;
+    if (m.flags & kMtlSpecGloss)
+    {
+        d.diffuse = baseColor;
+        d.specular = mk3(m.specular[0], m.specular[1], m.specular[2]);
+        d.roughness = 1.f - m.roughness; // the stored glossiness
+        d.metallic = spec_gloss_metallic(d.diffuse, d.specular);
+    }
+    else
+    {
+        float f = (m.ior - 1.f) / (m.ior + 1.f);
+        float F0 = f * f;
+        float metallic = m.metallic;
+        d.diffuse = lerp(baseColor, mk3(0.f), metallic);
+        d.specular = lerp(mk3(F0), baseColor, metallic);
+        d.roughness = m.roughness;
+        d.metallic = metallic;
+    }
     d.emission = frontFacing ? mk3(m.emissive[0], m.emissive[1], m.emissive[2]) : mk3(0.f);
     return d;
 }

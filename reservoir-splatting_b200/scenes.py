@@ -25,9 +25,11 @@ import numpy as np
 
 MATERIAL_FLOATS = 16
 DOUBLE_SIDED = 1
+SPEC_GLOSS = 2
 
 
 def material(base=(0.73, 0.73, 0.73), roughness=1.0, emissive=(0.0, 0.0, 0.0), metallic=0.0, ior=1.5, double_sided=True):
+    """Metal-rough StandardMaterial parameters in the rs_material layout."""
     m = np.zeros(MATERIAL_FLOATS, np.float32)
     m[0:3] = base
     m[3] = roughness
@@ -35,6 +37,20 @@ def material(base=(0.73, 0.73, 0.73), roughness=1.0, emissive=(0.0, 0.0, 0.0), m
     m[7] = metallic
     m[8] = ior
     m[9] = np.frombuffer(np.uint32(DOUBLE_SIDED if double_sided else 0).tobytes(), np.float32)[0]
+    return m
+
+
+def spec_gloss_material(diffuse=(0.73, 0.73, 0.73), specular=(0.0, 0.0, 0.0), glossiness=0.0, emissive=(0.0, 0.0, 0.0), ior=1.5,
+                        double_sided=False):
+    """Spec-gloss StandardMaterial parameters (ShadingModel::SpecGloss): the roughness slot holds the
+    glossiness, metallic is derived from the two colours when the material is shaded."""
+    m = np.zeros(MATERIAL_FLOATS, np.float32)
+    m[0:3] = diffuse
+    m[3] = glossiness
+    m[4:7] = emissive
+    m[8] = ior
+    m[9] = np.frombuffer(np.uint32(SPEC_GLOSS | (DOUBLE_SIDED if double_sided else 0)).tobytes(), np.float32)[0]
+    m[10:13] = specular
     return m
 
 

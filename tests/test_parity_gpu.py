@@ -107,6 +107,33 @@ def test_terrain_scene_scatter_backup(rs, oracle_mod, scenes):
 
 
 @pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
+@pytest.mark.parametrize("mode", ["ScatterBackup", "GatherOnly"])
+def test_imported_obj_spec_gloss_scene(rs, oracle_mod, scenes, tmp_path, mode):
+    """A Cornell box written as OBJ + MTL and imported with the Assimp importer's OBJ mapping:
+    spec-gloss materials (diffuse, specular colour, glossiness from the Phong exponent, derived
+    metallic), shaded the same on the GPU and in the oracle.  The adjoint rejects the scene."""
+    import torch
+    import reservoir_splatting_b200.importers as I
+    sc = scenes.cornell_box(0)
+    I.save_obj(sc, tmp_path / "cb.obj", ["white", "red", "green", "light"],
+               {"white": {"Kd": (0.7, 0.7, 0.7), "Ks": (0.05, 0.05, 0.05), "Ns": 30.0},
+                "red": {"Kd": (0.6, 0.05, 0.05), "Ks": (0.3, 0.3, 0.3), "Ns": 400.0},
+                "green": {"Kd": (0.1, 0.4, 0.1), "Ks": (0.02, 0.02, 0.02), "Ns": 5.0},
+                "light": {"Kd": (0, 0, 0), "Ke": (17, 12, 4)}})
+    imported = I.load_obj(tmp_path / "cb.obj")
+    props = {"temporalReuse": mode, "gatherOption": "Clamped", "maxSurfaceBounces": 2, "enableSpatialResampling": True}
+    run_pair(rs, oracle_mod, imported, scenes.cornell_camera, props, frames=4)
+    p = rs.ReservoirSplatting(dict(props, maxSurfaceBounces=1), W, H)
+    p.set_scene(imported)
+    p.render(scenes.cornell_camera(0, W, H))
+    g = torch.zeros((H, W, 4), device="cuda")
+    gm = torch.zeros((len(imported.materials), 8), device="cuda")
+    with pytest.raises(rs.RsError, match="spec-gloss"):
+        p.backward(g.data_ptr(), gm.data_ptr())
+    p.close()
+
+
+@pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
 @pytest.mark.parametrize("props", [{"temporalReuse": "ScatterBackup", "gatherOption": "Clamped"},
                                    {"temporalReuse": "GatherOnly", "gatherOption": "Robust"}],
                          ids=["ScatterBackup", "GatherOnly-Robust"])
