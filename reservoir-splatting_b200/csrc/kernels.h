@@ -81,6 +81,9 @@ struct MultiCtx
     float4* terms;                 // per splat: prevPHat.xyz, Jacobian
     float4* misSub;                // per splat: prevMIS, shifted sub-pixel.xy, 0
 };
+__global__ void k_go_curr(uint32_t slot, WaveCtx K);
+__global__ void k_go_prev(uint32_t slot, WaveCtx K);
+__global__ void k_go_combine(uint32_t slot, WaveCtx K, float4* color);
 __global__ void k_ms_curr(uint32_t slot, MultiCtx M);
 __global__ void k_ms_splat(uint32_t slot, MultiCtx M);
 __global__ void k_ms_combine(uint32_t slot, MultiCtx M, float4* color);

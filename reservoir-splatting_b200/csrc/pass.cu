@@ -253,6 +253,11 @@ static rs_status allocate(rs_pass* p)
     RS_CUDA(p->unsortedSplats.ensure(P * N));
     RS_CUDA(p->sortedSplats.ensure(P * N));
     RS_CUDA(p->sortedCell.ensure(P * N));
+    if (p->opt.temporalReuse == RS_GATHER_ONLY)
+    {
+        RS_CUDA(p->m2curr.ensure(N));
+        RS_CUDA(p->backupShift.ensure(5 * N)); RS_CUDA(p->backupTerms.ensure(N)); RS_CUDA(p->backupM.ensure(N));
+    }
     if (p->opt.temporalReuse == RS_SCATTER_BACKUP)
     {
         RS_CUDA(p->m2curr.ensure(N)); RS_CUDA(p->m3curr.ensure(N));
@@ -637,6 +642,28 @@ static rs_status enqueue_frame(rs_pass* p, cudaStream_t s, float4* colorDev, con
         case RS_GATHER_ONLY:
             stage(p, "collect", s);
             k_collect<<<tiled_blocks(W, H, 128), 128, 0, s>>>(C, mvec, prev.res(), prev.recp(), p->inter.res(), p->inter.recp(), p->floatingCoords.p, p->shiftedPaths.p); p->launches++;
+            if (!(p->camera.apertureRadius > 0.f))
+            {
+                // without depth of field only the lens-copy stage runs: two shift kernels on two
+                // streams, then the combine (k_go_*)
+                WaveCtx K = {};
+                K.curr = curr.res(); K.currRec = curr.recp();
+                K.inter = p->inter.res(); K.interRec = p->inter.recp();
+                K.floatingCoords = p->floatingCoords.p;
+                K.m2curr = p->m2curr.p;
+                K.backupShift = ShiftPlanes{p->backupShift.p, (size_t)N}; K.backupTerms = p->backupTerms.p; K.backupM = p->backupM.p;
+                cudaStream_t q[2];
+                fork_streams(p, s, 2, q);
+                stage(p, "gatherCurrShift", q[0]);
+                k_go_curr<<<tiled_blocks(W, H, 128), 128, 0, q[0]>>>(C, K);
+                stage(p, "gatherPrevShift", q[1]);
+                k_go_prev<<<tiled_blocks(W, H, 128), 128, 0, q[1]>>>(C, K);
+                join_streams(p, s, 2);
+                stage(p, "gatherResample", s);
+                k_go_combine<<<tiled_blocks(W, H, 128), 128, 0, s>>>(C, K, temporalColor);
+                p->launches += 3;
+                break;
+            }
             stage(p, "gatherResample", s);
             k_gather_resample<<<tiled_blocks(W, H, 128), 128, 0, s>>>(C, p->vbuffer.p, curr.res(), curr.recp(), p->inter.res(), p->inter.recp(), p->floatingCoords.p, temporalColor); p->launches++;
             break;

@@ -90,6 +90,95 @@ __device__ __forceinline__ Recon backup_rec(const WaveCtx& K, uint32_t bi)
     return r;
 }
 
+// ================================================================ GatherOnly, lens-copy stage
+// GatherTemporalResampling.rt.slang:68-235 without depth of field (the lens-copy stage alone, with
+// probability 1): the current sample's shift into the previous frame and the gathered sample's shift
+// into this pixel are independent kernels (their generator copies are never used), the combine
+// replays the pixel's two resampling draws.  Buffers: m2curr (the current sample's MIS term),
+// backupShift / backupTerms / backupM (the gathered sample's shift, prevPHat and Jacobian, MIS term).
+__global__ void __launch_bounds__(128, 9) k_go_curr(uint32_t slot, WaveCtx K)
+{
+    const DevCtx& C = c_ctx[slot];
+    uint32_t ri;
+    if (!tiled_pixel(C.W, C.H, ri)) return;
+    const Res cr = load_res(K.curr, ri);
+    if (!any_gt0(cr.integrand)) return;
+    const Res pr = load_res(K.inter, ri);
+    const float2 fcv = __ldg(&K.floatingCoords[ri]);
+    const Recon crd = load_rec(K.currRec, ri);
+    SampleGen dummy = {0, C.sgKind};
+    Shifted sc = dev_gather_lens_copy(C, dummy, crd, crd.time + C.cm.artificialFrameTime, mk2(fcv.x, fcv.y) + cr.subPixel, crd.lensSample);
+    float sj = sc.secondaryPathJacobian / crd.secondaryPathJacobian;
+    float m2 = luminance(sc.radiance) * sj * (C.useConfTemporal ? pr.confidence : 1.f) * 1.f;
+    K.m2curr[ri] = f_isnan(m2) ? 0.f : m2;
+}
+
+__global__ void __launch_bounds__(128, 9) k_go_prev(uint32_t slot, WaveCtx K)
+{
+    const DevCtx& C = c_ctx[slot];
+    uint32_t ri;
+    if (!tiled_pixel(C.W, C.H, ri)) return;
+    const Res pr = load_res(K.inter, ri);
+    if (!any_gt0(pr.integrand)) return;
+    const uint32_t x = ri % C.W, y = ri / C.W;
+    const Res cr = load_res(K.curr, ri);
+    const Recon prd = load_rec(K.interRec, ri);
+    SampleGen dummy = {0, C.sgKind};
+    Shifted sp = dev_gather_lens_copy(C, dummy, prd, prd.time, mk2((float)x + pr.subPixel.x, (float)y + pr.subPixel.y), prd.lensSample);
+    store_shift(K.backupShift, ri, sp);
+    float sj = sp.secondaryPathJacobian / prd.secondaryPathJacobian;
+    float m1 = luminance(sp.radiance) * sj * (C.useConfTemporal ? cr.confidence : 1.f);
+    const f3 prevPHat = f_isnan(m1) ? mk3(0.f) : sp.radiance;
+    sj = f_isnan(m1) ? 1.f : sj;
+    m1 = f_isnan(m1) ? 0.f : m1;
+    K.backupTerms[ri] = make_float4(prevPHat.x, prevPHat.y, prevPHat.z, sj);
+    K.backupM[ri] = make_float2(m1, 0.f);
+}
+
+__global__ void __launch_bounds__(128) k_go_combine(uint32_t slot, WaveCtx K, float4* __restrict__ color)
+{
+    const DevCtx& C = c_ctx[slot];
+    uint32_t ri;
+    if (!tiled_pixel(C.W, C.H, ri)) return;
+    const uint32_t x = ri % C.W, y = ri / C.W;
+    const bool useConf = C.useConfTemporal != 0;
+    SampleGen sg = sg_create(x, y, pass_seed(C, 3), C.sgKind);
+    Res dst = res_default();
+    Recon dstR = recon_default();
+    const Res cr = load_res_rw(K.curr, ri);
+    const Res pr = load_res(K.inter, ri);
+    float currSampleMIS = 0.f;
+    f3 currPHat = mk3(0.f);
+    if (any_gt0(cr.integrand))
+    {
+        const float m1 = luminance(cr.integrand) * (useConf ? cr.confidence : 1.f);
+        currPHat = cr.integrand;
+        const float m2 = K.m2curr[ri];
+        currSampleMIS = (m1 + m2 == 0.f) ? 0.f : m1 / (m1 + m2);
+    }
+    if (res_add_sample(dst, sg, currSampleMIS, currPHat, 1.f, cr)) dstR = load_rec_rw(K.currRec, ri);
+    float prevSampleMIS = 0.f;
+    f3 prevPHat = mk3(0.f);
+    float sj = 1.f;
+    if (any_gt0(pr.integrand))
+    {
+        const float4 t = __ldg(&K.backupTerms[ri]);
+        prevPHat = mk3(t.x, t.y, t.z);
+        sj = t.w;
+        const float m1 = __ldg(&K.backupM[ri]).x;
+        const float m2 = luminance(pr.integrand) * (useConf ? pr.confidence : 1.f) * 1.f;
+        prevSampleMIS = ((m1 + m2) == 0.f) ? 0.f : m2 / (m1 + m2);
+    }
+    if (res_add_sample(dst, sg, prevSampleMIS, prevPHat, sj, pr))
+    {
+        dstR = load_rec(K.interRec, ri);
+        recon_update(dstR, load_shift(K.backupShift, ri));
+    }
+    store_res(K.curr, ri, dst);
+    store_rec(K.currRec, ri, dstR);
+    write_color(color, ri, dst);
+}
+
 // ---- stage 1: current sample -> previous domain by reprojection (ScatterBackup...:96-114)
 __global__ void __launch_bounds__(128, 8) k_sb_curr_scatter(uint32_t slot, WaveCtx K)
 {
