@@ -857,65 +857,6 @@ __device__ __forceinline__ void write_color(float4* color, uint32_t i, const Res
     color[i] = make_float4(c.x, c.y, c.z, 1.f);
 }
 
-// ScatterTemporalResampling.rt.slang:65-174
-__global__ void __launch_bounds__(128, 6) k_scatter_resample(uint32_t slot, const float2* __restrict__ mvec, ResPlanes prev, RecPlanes prevRec,
-                                                          ResPlanes curr, RecPlanes currRec, const uint32_t* __restrict__ counts,
-                                                          const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ sorted,
-                                                          float4* __restrict__ color)
-{
-    const DevCtx& C = c_ctx[slot];
-    uint32_t ri;
-    if (!tiled_pixel(C.W, C.H, ri)) return;
-    uint32_t x = ri % C.W, y = ri / C.W;
-    const bool useConf = C.useConfTemporal != 0;
-    SampleGen sg = sg_create(x, y, pass_seed(C, 5), C.sgKind);
-    Res dst = res_default();
-    Recon dstR = recon_default();
-    Res cr = load_res_rw(curr, ri);
-    Recon crd = load_rec_rw(currRec, ri);
-    float currSampleMIS = 1.f;
-    if (any_gt0(cr.integrand))
-    {
-        float m1 = luminance(cr.integrand) * (useConf ? cr.confidence : 1.f);
-        Shifted sc = dev_scatter_shift(C, sg, crd, crd.time + C.cm.artificialFrameTime, crd.firstHit, crd.lensSample, false);
-        float sj = jac_scatter(sc, crd);
-        float m2 = luminance(sc.radiance) * sj;
-        m2 = f_isnan(m2) ? 0.f : m2;
-        int spx = (int)f_floor(sc.fractionalPixel.x), spy = (int)f_floor(sc.fractionalPixel.y);
-        if (valid_int(C, spx, spy)) m2 *= useConf ? load_confidence(prev, (uint32_t)spy * C.W + (uint32_t)spx) : 1.f;
-        else m2 = 0.f;
-        currSampleMIS = (m1 + m2 == 0.f) ? 0.f : m1 / (m1 + m2);
-    }
-    if (res_add_sample(dst, sg, currSampleMIS, cr.integrand, 1.f, cr)) dstR = crd;
-    float newConfidence = dst.confidence;
-    uint32_t n = counts[ri], off = offsets[ri];
-    for (uint32_t i = 0; i < n; i++)
-    {
-        uint32_t si = __ldg(&sorted[off + i]);
-        Res pr = load_res(prev, si);
-        float prevSampleMIS = 0.f;
-        f3 prevPHat = mk3(0.f);
-        float sj = 1.f;
-        Recon prd = load_rec(prevRec, si);
-        if (any_gt0(pr.integrand))
-        {
-            Shifted sp = dev_scatter_shift(C, sg, prd, prd.time, prd.firstHit, prd.lensSample, false);
-            sj = jac_scatter(sp, prd);
-            float m1 = luminance(sp.radiance) * sj * (useConf ? cr.confidence : 1.f);
-            prevPHat = f_isnan(m1) ? mk3(0.f) : sp.radiance;
-            sj = f_isnan(m1) ? 1.f : sj;
-            recon_update(prd, sp);
-            pr.subPixel = prd.subPixel;
-            float m2 = luminance(pr.integrand) * (useConf ? pr.confidence : 1.f);
-            prevSampleMIS = ((m1 + m2) == 0.f) ? 0.f : m2 / (m1 + m2);
-        }
-        if (res_add_sample(dst, sg, prevSampleMIS, prevPHat, sj, pr)) dstR = prd;
-    }
-    dst.confidence = bilinear_confidence(C, mvec, prev, x, y, newConfidence, useConf);
-    store_res(curr, ri, dst);
-    store_rec(currRec, ri, dstR);
-    write_color(color, ri, dst);
-}
 
 // GatherTemporalResampling.rt.slang:68-235
 __global__ void __launch_bounds__(128, 6) k_gather_resample(uint32_t slot, const uint4* __restrict__ vbuffer, ResPlanes curr, RecPlanes currRec,

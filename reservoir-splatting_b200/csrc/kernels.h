@@ -23,8 +23,6 @@ __global__ void k_rank_cells(const uint32_t* targets, const uint32_t* offsets, c
 __global__ void k_collect(uint32_t slot, const float2* mvec, ResPlanes prev, RecPlanes prevRec, ResPlanes inter, RecPlanes interRec,
                           float2* floatingCoords, const Shifted* shiftedPaths);
 __global__ void k_robust(uint32_t slot, ResPlanes prev, RecPlanes prevRec, Shifted* shiftedPaths);
-__global__ void k_scatter_resample(uint32_t slot, const float2* mvec, ResPlanes prev, RecPlanes prevRec, ResPlanes curr, RecPlanes currRec,
-                                   const uint32_t* counts, const uint32_t* offsets, const uint32_t* sorted, float4* color);
 __global__ void k_gather_resample(uint32_t slot, const uint4* vbuffer, ResPlanes curr, RecPlanes currRec, ResPlanes inter, RecPlanes interRec,
                                   const float2* floatingCoords, float4* color);
 __global__ void k_resolve(uint32_t n, ResPlanes curr, float4* color);
@@ -81,6 +79,9 @@ struct MultiCtx
     float4* terms;                 // per splat: prevPHat.xyz, Jacobian
     float4* misSub;                // per splat: prevMIS, shifted sub-pixel.xy, 0
 };
+__global__ void k_so_curr(uint32_t slot, WaveCtx K);
+__global__ void k_so_splat(uint32_t slot, WaveCtx K);
+__global__ void k_so_combine(uint32_t slot, WaveCtx K, float4* color);
 __global__ void k_go_curr(uint32_t slot, WaveCtx K);
 __global__ void k_go_prev(uint32_t slot, WaveCtx K);
 __global__ void k_go_combine(uint32_t slot, WaveCtx K, float4* color);

@@ -253,6 +253,11 @@ static rs_status allocate(rs_pass* p)
     RS_CUDA(p->unsortedSplats.ensure(P * N));
     RS_CUDA(p->sortedSplats.ensure(P * N));
     RS_CUDA(p->sortedCell.ensure(P * N));
+    if (p->opt.temporalReuse == RS_SCATTER_ONLY)
+    {
+        RS_CUDA(p->m2curr.ensure(N));
+        RS_CUDA(p->splatShift.ensure(5 * N)); RS_CUDA(p->splatTerms.ensure(N)); RS_CUDA(p->splatM.ensure(N));
+    }
     if (p->opt.temporalReuse == RS_GATHER_ONLY)
     {
         RS_CUDA(p->m2curr.ensure(N));
@@ -614,7 +619,7 @@ static rs_status enqueue_frame(rs_pass* p, cudaStream_t s, float4* colorDev, con
             k_reproject<<<tiled_blocks(W, H, 256), 256, 0, q[2]>>>(C, prev.res(), prev.recp(), p->targets.p, p->counts.p); p->launches++;
             stage(p, "sortCells", q[2]);
             buildCells(q[2], p->targets.p, p->counts.p, p->offsets.p, p->cursor.p, p->unsortedSplats.p, p->sortedSplats.p,
-                       o.temporalReuse == RS_SCATTER_BACKUP ? p->sortedCell.p : nullptr, p->total.p);
+                       p->sortedCell.p, p->total.p);
         }
         else if (o.temporalReuse == RS_MULTI_SCATTER)
         {
@@ -668,9 +673,28 @@ static rs_status enqueue_frame(rs_pass* p, cudaStream_t s, float4* colorDev, con
             k_gather_resample<<<tiled_blocks(W, H, 128), 128, 0, s>>>(C, p->vbuffer.p, curr.res(), curr.recp(), p->inter.res(), p->inter.recp(), p->floatingCoords.p, temporalColor); p->launches++;
             break;
         case RS_SCATTER_ONLY:
+        {
+            // the current sample's shift and the splats' shifts on two streams, then the combine
+            WaveCtx K = {};
+            K.mvec = mvec;
+            K.curr = curr.res(); K.currRec = curr.recp();
+            K.prev = prev.res(); K.prevRec = prev.recp();
+            K.counts = p->counts.p; K.offsets = p->offsets.p; K.sorted = p->sortedSplats.p; K.sortedCell = p->sortedCell.p;
+            K.totalSplats = p->total.p;
+            K.m2curr = p->m2curr.p;
+            K.splatShift = ShiftPlanes{p->splatShift.p, (size_t)N}; K.splatTerms = p->splatTerms.p; K.splatM = p->splatM.p;
+            cudaStream_t q[2];
+            fork_streams(p, s, 2, q);
+            stage(p, "scatterCurrShift", q[0]);
+            k_so_curr<<<tiled_blocks(W, H, 128), 128, 0, q[0]>>>(C, K);
+            stage(p, "scatterSplatShift", q[1]);
+            k_so_splat<<<grid(N, 128), 128, 0, q[1]>>>(C, K);
+            join_streams(p, s, 2);
             stage(p, "scatterResample", s);
-            k_scatter_resample<<<tiled_blocks(W, H, 128), 128, 0, s>>>(C, mvec, prev.res(), prev.recp(), curr.res(), curr.recp(), p->counts.p, p->offsets.p, p->sortedSplats.p, temporalColor); p->launches++;
+            k_so_combine<<<tiled_blocks(W, H, 128), 128, 0, s>>>(C, K, temporalColor);
+            p->launches += 3;
             break;
+        }
         case RS_SCATTER_BACKUP:
         {
             const bool fused = o.gatherOption == RS_GATHER_CLAMPED;

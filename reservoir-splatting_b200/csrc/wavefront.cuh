@@ -90,6 +90,106 @@ __device__ __forceinline__ Recon backup_rec(const WaveCtx& K, uint32_t bi)
     return r;
 }
 
+// ================================================================ ScatterOnly
+// ScatterTemporalResampling.rt.slang:65-174: the current sample's reprojection shift into the
+// previous frame (k_so_curr) and every splat's reprojection shift into its cell (k_so_splat, one
+// thread per splat of the sorted cell lists) are stored; the combine walks each cell's splats in the
+// canonical order and replays the resampling draws.  Buffers: m2curr, splatShift / splatTerms
+// (prevPHat, Jacobian) / splatM (MIS weight, 0, shifted sub-pixel).
+__global__ void __launch_bounds__(128, 8) k_so_curr(uint32_t slot, WaveCtx K)
+{
+    const DevCtx& C = c_ctx[slot];
+    uint32_t ri;
+    if (!tiled_pixel(C.W, C.H, ri)) return;
+    const f3 integrand = load_integrand(K.curr, ri);
+    if (!any_gt0(integrand)) return;
+    const Recon crd = load_rec(K.currRec, ri);
+    SampleGen dummy = {0, C.sgKind};
+    Shifted sc = dev_scatter_shift(C, dummy, crd, crd.time + C.cm.artificialFrameTime, crd.firstHit, crd.lensSample, false);
+    float sj = jac_scatter(sc, crd);
+    float m2 = luminance(sc.radiance) * sj;
+    m2 = f_isnan(m2) ? 0.f : m2;
+    int spx = (int)f_floor(sc.fractionalPixel.x), spy = (int)f_floor(sc.fractionalPixel.y);
+    if (valid_int(C, spx, spy)) m2 *= C.useConfTemporal ? load_confidence(K.prev, (uint32_t)spy * C.W + (uint32_t)spx) : 1.f;
+    else m2 = 0.f;
+    K.m2curr[ri] = m2;
+}
+
+__global__ void __launch_bounds__(128, 8) k_so_splat(uint32_t slot, WaveCtx K)
+{
+    const DevCtx& C = c_ctx[slot];
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= *K.totalSplats) return;
+    const uint32_t si = __ldg(&K.sorted[j]);
+    const Res pr = load_res(K.prev, si);
+    if (!any_gt0(pr.integrand)) return;
+    const uint32_t cell = __ldg(&K.sortedCell[j]);
+    const Recon prd = load_rec(K.prevRec, si);
+    SampleGen dummy = {0, C.sgKind};
+    Shifted sp = dev_scatter_shift(C, dummy, prd, prd.time, prd.firstHit, prd.lensSample, false);
+    store_shift(K.splatShift, j, sp);
+    float sj = jac_scatter(sp, prd);
+    const float m1 = luminance(sp.radiance) * sj * (C.useConfTemporal ? load_confidence(K.curr, cell) : 1.f);
+    const f3 prevPHat = f_isnan(m1) ? mk3(0.f) : sp.radiance;
+    sj = f_isnan(m1) ? 1.f : sj;
+    const float m2 = luminance(pr.integrand) * (C.useConfTemporal ? pr.confidence : 1.f);
+    const float prevSampleMIS = ((m1 + m2) == 0.f) ? 0.f : m2 / (m1 + m2);
+    const f2 sub = sp.fractionalPixel - floor2(sp.fractionalPixel); // recon_update's sub-pixel
+    K.splatTerms[j] = make_float4(prevPHat.x, prevPHat.y, prevPHat.z, sj);
+    K.splatM[j] = make_float4(prevSampleMIS, 0.f, sub.x, sub.y);
+}
+
+__global__ void __launch_bounds__(128) k_so_combine(uint32_t slot, WaveCtx K, float4* __restrict__ color)
+{
+    const DevCtx& C = c_ctx[slot];
+    uint32_t ri;
+    if (!tiled_pixel(C.W, C.H, ri)) return;
+    const uint32_t x = ri % C.W, y = ri / C.W;
+    const bool useConf = C.useConfTemporal != 0;
+    SampleGen sg = sg_create(x, y, pass_seed(C, 5), C.sgKind);
+    Res dst = res_default();
+    Recon dstR = recon_default();
+    const Res cr = load_res_rw(K.curr, ri);
+    float currSampleMIS = 1.f;
+    if (any_gt0(cr.integrand))
+    {
+        const float m1 = luminance(cr.integrand) * (useConf ? cr.confidence : 1.f);
+        const float m2 = K.m2curr[ri];
+        currSampleMIS = (m1 + m2 == 0.f) ? 0.f : m1 / (m1 + m2);
+    }
+    if (res_add_sample(dst, sg, currSampleMIS, cr.integrand, 1.f, cr)) dstR = load_rec_rw(K.currRec, ri);
+    const float newConfidence = dst.confidence;
+    const uint32_t n = __ldg(&K.counts[ri]), off = __ldg(&K.offsets[ri]);
+    for (uint32_t i = 0; i < n; i++)
+    {
+        const uint32_t j = off + i;
+        const uint32_t si = __ldg(&K.sorted[j]);
+        Res pr = load_res(K.prev, si);
+        float prevSampleMIS = 0.f;
+        f3 prevPHat = mk3(0.f);
+        float sj = 1.f;
+        const bool shifted = any_gt0(pr.integrand);
+        if (shifted)
+        {
+            const float4 t = __ldg(&K.splatTerms[j]);
+            const float4 m = __ldg(&K.splatM[j]);
+            prevPHat = mk3(t.x, t.y, t.z);
+            sj = t.w;
+            prevSampleMIS = m.x;
+            pr.subPixel = mk2(m.z, m.w);
+        }
+        if (res_add_sample(dst, sg, prevSampleMIS, prevPHat, sj, pr))
+        {
+            dstR = load_rec(K.prevRec, si);
+            if (shifted) recon_update(dstR, load_shift(K.splatShift, j));
+        }
+    }
+    dst.confidence = bilinear_confidence(C, K.mvec, K.prev, x, y, newConfidence, useConf);
+    store_res(K.curr, ri, dst);
+    store_rec(K.currRec, ri, dstR);
+    write_color(color, ri, dst);
+}
+
 // ================================================================ GatherOnly, lens-copy stage
 // GatherTemporalResampling.rt.slang:68-235 without depth of field (the lens-copy stage alone, with
 // probability 1): the current sample's shift into the previous frame and the gathered sample's shift
