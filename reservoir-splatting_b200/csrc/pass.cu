@@ -747,14 +747,20 @@ static rs_status enqueue_frame(rs_pass* p, cudaStream_t s, float4* colorDev, con
         case RS_MULTI_SCATTER:
         {
             const uint32_t P = o.numTimePartitions;
-            stage(p, "multiScatterResample", s);
             MultiCtx M;
             M.mvec = mvec; M.curr = curr.res(); M.currRec = curr.recp(); M.prev = prev.res(); M.prevRec = prev.recp();
             M.counts = p->counts.p; M.offsets = p->offsets.p; M.sorted = p->sortedSplats.p; M.sortedCell = p->sortedCell.p;
             M.totals = p->total.p; M.currMIS = p->msCurr.p;
             M.shift = ShiftPlanes{p->msShift.p, (size_t)P * N}; M.terms = p->msTerms.p; M.misSub = p->msMisSub.p;
-            k_ms_curr<<<tiled_blocks(W, H, 128), 128, 0, s>>>(C, M);
-            k_ms_splat<<<grid(P * N, 128), 128, 0, s>>>(C, M);
+            // the current sample's shifts and the splats' shifts on two streams, then the combine
+            cudaStream_t q[2];
+            fork_streams(p, s, 2, q);
+            stage(p, "multiCurrShift", q[0]);
+            k_ms_curr<<<tiled_blocks(W, H, 128), 128, 0, q[0]>>>(C, M);
+            stage(p, "multiSplatShift", q[1]);
+            k_ms_splat<<<grid(P * N, 128), 128, 0, q[1]>>>(C, M);
+            join_streams(p, s, 2);
+            stage(p, "multiScatterResample", s);
             k_ms_combine<<<tiled_blocks(W, H, 128), 128, 0, s>>>(C, M, temporalColor);
             p->launches += 3;
             break;
