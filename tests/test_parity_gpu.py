@@ -78,6 +78,23 @@ def test_cornell_modes(rs, oracle_mod, scenes, name, props, spatial):
     assert img[..., :3].mean() > 0.01
 
 
+ODD_MODES = MODES + [("MultiScatter", {"temporalReuse": "MultiScatter", "numTimePartitions": 3})]
+
+
+@pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
+@pytest.mark.parametrize("name,props", ODD_MODES, ids=[m[0] for m in ODD_MODES])
+@pytest.mark.parametrize("size", [(37, 23), (1, 1)], ids=["37x23", "1x1"])
+def test_odd_image_sizes(rs, oracle_mod, scenes, name, props, size):
+    """Images that are not a multiple of the 8 x 4 warp tile (and a single pixel): the tile-edge
+    guards of every pixel kernel and the bounds of the per-splat kernels, in every temporal mode."""
+    w, h = size
+    props = dict(props, maxSurfaceBounces=2, enableSpatialResampling=True)
+    shutter = 0.04 if name == "MultiScatter" else 0.0
+    report, img = run_pair(rs, oracle_mod, scenes.cornell_box(0), scenes.cornell_camera, props, frames=4, width=w, height=h,
+                           shutter=shutter)
+    assert img.shape == (h, w, 4) and np.isfinite(img).all()
+
+
 @pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
 def test_multiscatter_motion_blur(rs, oracle_mod, scenes):
     props = {"temporalReuse": "MultiScatter", "numTimePartitions": 4, "maxSurfaceBounces": 1, "enableSpatialResampling": False,
