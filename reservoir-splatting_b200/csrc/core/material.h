@@ -507,6 +507,28 @@ RS_HD bool mi_sample(const ShadingData& sd, const BsdfData& d, uint32_t lobeMask
     if (!valid_hemisphere(sd, wiLocal, woLocal, r.wo)) return false;
     return true;
 }
+// mi_sample(sd, d, lobeMask, sg, r) and, in `totalPdf`, mi_pdf(sd, d, 0xF, r.wo) in one pass: the
+// local incident direction and the BSDF parameters are shared (make_bsdf's mask changes alpha only
+// for mask 5, so lobeMask != 5 is required), the sampled direction is brought back to the local
+// frame from its world value as mi_pdf does; every result has the bits of the two calls.  r.wo must
+// hold the caller's value for a failed sample (mi_sample leaves it unchanged then).
+RS_HD bool mi_sample_total_pdf(const ShadingData& sd, const BsdfData& d, uint32_t lobeMask, SampleGen& sg, BSDFSample& r, float& totalPdf)
+{
+    const f3 wiLocal = sd_to_local(sd, sd.V);
+    StandardBSDF b = make_bsdf(wiLocal, d, lobeMask);
+    f3 woLocal;
+    bool ok = bsdf_sample_local(b, wiLocal, woLocal, r.pdf, r.weight, r.lobeType, sg);
+    if (ok)
+    {
+        r.wo = sd_from_local(sd, woLocal);
+        ok = valid_hemisphere(sd, wiLocal, woLocal, r.wo);
+    }
+    const f3 woTotal = sd_to_local(sd, r.wo);
+    b.lobeMask = 0xFu;
+    totalPdf = valid_hemisphere(sd, wiLocal, woTotal, r.wo) ? bsdf_pdf_local(b, wiLocal, woTotal) : 0.f;
+    return ok;
+}
+
 // getLobeTypes for an opaque StandardBSDFData (StandardBSDF.slang:210-232).
 RS_HD uint32_t mi_lobe_types(const BsdfData& d)
 {

@@ -313,7 +313,8 @@ __device__ void handle_hit(const DevCtx& C, PState& path, const RecPlanes& outRe
     // generateScatterRay (:331-382)
     BSDFSample result;
     result.wo = mk3(0.f); result.pdf = 0.f; result.weight = mk3(0.f); result.lobeType = 0;
-    bool valid = mi_sample(sd, d, 1u, path.sg, result);
+    float totalPdf;
+    bool valid = mi_sample_total_pdf(sd, d, 1u, path.sg, result, totalPdf); // and mi_pdf(sd, d, 0xF, result.wo)
     path.pdf = result.pdf;
     uint32_t componentType = 0;
     if (result.lobeType & kLobeDiffuseReflection)
@@ -327,7 +328,7 @@ __device__ void handle_hit(const DevCtx& C, PState& path, const RecPlanes& outRe
     }
     if (path.vertex == 1) path.rec.firstComp = componentType;
     else if (path.vertex == 2) { path.rec.secondComp = componentType; path.rec.secondWo = result.wo; }
-    path.totalPdf = mi_pdf(sd, d, 0xFu, result.wo);
+    path.totalPdf = totalPdf;
     if (valid)
     {
         // generateScatterRay(bs, ...) (:391-471)
