@@ -253,8 +253,11 @@ struct ShiftPath
     bool active;
 };
 
-// handleReconnectionHit (PathTracer.slang:1177-1397)
-__device__ inline void dev_reconnection_hit(const DevCtx& C, ShiftPath& path, const Recon& rd, float& dstJacobian)
+// handleReconnectionHit (PathTracer.slang:1177-1397).  The x1 -> x2 visibility test that ends it is
+// not traced here: when the path is still active its ray is returned in `vis` (an occluded ray
+// deactivates the path, ending the shift with 0), for the caller to trace once nothing else is left
+// to compute.
+__device__ inline void dev_reconnection_hit(const DevCtx& C, ShiftPath& path, const Recon& rd, float& dstJacobian, Ray& vis)
 {
     ShadingData sd = dev_sd(C, path.hit, path.dir);
     BsdfData d = dev_instance(C, sd);
@@ -312,15 +315,22 @@ __device__ inline void dev_reconnection_hit(const DevCtx& C, ShiftPath& path, co
     // PathState), so the caustics test of :1378 never fires here.
     bool valid = any_gt0(path.thp);
     if (!valid) path.active = false;
-    else if (!dev_visible(C, mk_ray(path.origin, path.dir, 0.f, rayLength))) path.active = false;
+    else vis = mk_ray(path.origin, path.dir, 0.f, rayLength);
 }
 
-// pathReconnectionShift (ShiftMapping.slang:430-513)
-__device__ inline f3 dev_path_reconnection_shift(const DevCtx& C, const Recon& rd, ShiftPath& path, float& dstJacobian)
+// pathReconnectionShift (ShiftMapping.slang:430-513) with its visibility test deferred: returns the
+// value for a visible reconnection; `needVis` tells whether the x1 -> x2 ray `vis` has to be traced,
+// and if it is occluded the shift's value is 0 and dstJacobian is `jacobianIfOccluded` (the values
+// the reference returns at its visibility test).
+__device__ inline f3 dev_path_reconnection_shift_deferred(const DevCtx& C, const Recon& rd, ShiftPath& path, float& dstJacobian, Ray& vis,
+                                                         bool& needVis, float& jacobianIfOccluded)
 {
     dstJacobian = 1.f;
-    dev_reconnection_hit(C, path, rd, dstJacobian);
+    needVis = false;
+    dev_reconnection_hit(C, path, rd, dstJacobian, vis);
     if (!path.active) return mk3(0.f);
+    needVis = true;
+    jacobianIfOccluded = dstJacobian;
     if (rd.pathLength == 2) return 1.f * path.thp * rd.irradiance; // the x2 BSDF terms are not used for length 2
     ShadingData secondSd = dev_sd(C, rd.secondHit, path.dir);
     BsdfData d = dev_instance(C, secondSd);
@@ -345,6 +355,17 @@ __device__ inline f3 dev_path_reconnection_shift(const DevCtx& C, const Recon& r
         dstJacobian *= lobeSpecificPdf;
     }
     return misWeight * path.thp * rd.irradiance;
+}
+
+// pathReconnectionShift (ShiftMapping.slang:430-513), the visibility traced after the x2 terms.
+__device__ inline f3 dev_path_reconnection_shift(const DevCtx& C, const Recon& rd, ShiftPath& path, float& dstJacobian)
+{
+    Ray vis;
+    bool needVis;
+    float jacobianIfOccluded;
+    const f3 value = dev_path_reconnection_shift_deferred(C, rd, path, dstJacobian, vis, needVis, jacobianIfOccluded);
+    if (needVis && !dev_visible(C, vis)) { dstJacobian = jacobianIfOccluded; return mk3(0.f); }
+    return value;
 }
 
 __device__ __forceinline__ f3 dev_primary_light(const DevCtx& C, const ShiftPath& path) // PathTracer.slang:1399-1410
@@ -467,7 +488,9 @@ __device__ inline Shifted dev_scatter_shift(const DevCtx& C, SampleGen sg, const
     f2 nfp = mk2((0.5f * ndc.x + 0.5f) * (float)C.W, (-0.5f * ndc.y + 0.5f) * (float)C.H);
     if (!valid_float(C, nfp)) return shifted_default();
     float dist = length(x1 - path.origin);
-    if (!skipVisibilityCheck && !dev_visible(C, mk_ray(path.origin, path.dir, 0.001f, 0.999f * dist))) return shifted_default();
+    // the camera -> x1 test (occluded: the shift fails) and the reconnection's x1 -> x2 test are
+    // traced in that order after the rest of the shift, when only their outcomes are left to apply
+    const Ray camVis = mk_ray(path.origin, path.dir, 0.001f, 0.999f * dist);
     Shifted sp = shifted_default();
     sp.lensSample = lensSample;
     sp.firstRayDir = path.dir;
@@ -485,8 +508,13 @@ __device__ inline Shifted dev_scatter_shift(const DevCtx& C, SampleGen sg, const
         float d1 = dist - d0;
         sp.lensVertexJacobian = (d0 * d0) / (d1 * d1) * f_abs(cosNormal) / f_abs(cosSensor);
     }
-    if (rd.pathLength == 1) { sp.radiance = dev_primary_light(C, path); return sp; }
-    sp.radiance = dev_path_reconnection_shift(C, rd, path, sp.secondaryPathJacobian);
+    Ray vis;
+    bool needVis = false;
+    float jacobianIfOccluded = 0.f;
+    if (rd.pathLength == 1) sp.radiance = dev_primary_light(C, path);
+    else sp.radiance = dev_path_reconnection_shift_deferred(C, rd, path, sp.secondaryPathJacobian, vis, needVis, jacobianIfOccluded);
+    if (!skipVisibilityCheck && !dev_visible(C, camVis)) return shifted_default();
+    if (needVis && !dev_visible(C, vis)) { sp.radiance = mk3(0.f); sp.secondaryPathJacobian = jacobianIfOccluded; }
     return sp;
 }
 
