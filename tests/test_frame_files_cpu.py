@@ -43,3 +43,22 @@ def test_png_decodes_to_the_texels(rs, tmp_path):
 def test_tonemap_options_by_name(rs):
     import reservoir_splatting_b200.abi as abi
     assert abi.TONEMAP_OPERATOR == {"Linear": 0, "Reinhard": 1, "ReinhardModified": 2, "HejiHableAlu": 3, "HableUc2": 4, "Aces": 5}
+
+
+def test_tonemap_rejects_bad_arguments_before_device_work(rs):
+    """rs_tonemap validates its arguments before any device work (callable without a GPU)."""
+    import ctypes as C
+    import reservoir_splatting_b200.frame_output as FO
+    lib = rs.load_library()
+    o = FO.tonemap_options()
+    fake = C.c_void_p(0x1000)  # never dereferenced: every call below fails validation
+    assert lib.rs_tonemap(None, 4, 4, C.byref(o), fake, None, None) == rs.abi.RS_INVALID_ARG
+    assert lib.rs_tonemap(fake, 4, 4, None, fake, None, None) == rs.abi.RS_INVALID_ARG
+    assert lib.rs_tonemap(fake, 4, 4, C.byref(o), None, None, None) == rs.abi.RS_INVALID_ARG
+    bad = FO.tonemap_options(op=6 - 1)
+    bad.op = 6
+    assert lib.rs_tonemap(fake, 4, 4, C.byref(bad), fake, None, None) == rs.abi.RS_INVALID_ARG
+    assert lib.rs_tonemap(fake, 4, 4, C.byref(FO.tonemap_options(fNumber=0.0)), fake, None, None) == rs.abi.RS_INVALID_ARG
+    assert lib.rs_tonemap(fake, 4, 4, C.byref(FO.tonemap_options(autoExposure=1)), fake, None, None) == rs.abi.RS_INVALID_ARG
+    assert lib.rs_tonemap(fake, 0, 4, C.byref(o), fake, None, None) == rs.abi.RS_OK  # nothing to do
+    assert lib.rs_tonemap_workspace_bytes() >= 8
