@@ -280,6 +280,8 @@ def run_ours(args):
         }
         if quality is not None:
             line["quality"] = quality
+        if world == 1 and not args.no_modes:
+            line["modes"] = run_modes(args, torch, rs, scene, stream)
         if world == 1 and not args.no_batched:
             line["batched"] = run_batched(args, torch, rs, stream, dev)
         if world == 1 and not args.no_motion_blur:
@@ -327,6 +329,50 @@ def measure_quality(args, torch, rs, scene, cam, image, W, H, stream):
 
 
 BATCH_RESOLUTIONS = [(320, 240), (640, 480), (1280, 720), (1920, 1080)]
+
+
+MODE_PROPS = {
+    "GatherOnly-Clamped": {"temporalReuse": "GatherOnly", "gatherOption": "Clamped"},
+    "GatherOnly-Robust": {"temporalReuse": "GatherOnly", "gatherOption": "Robust"},
+    "ScatterOnly": {"temporalReuse": "ScatterOnly"},
+    "ScatterBackup-Fast-Pairwise": {"temporalReuse": "ScatterBackup", "gatherOption": "Fast", "scatterBackupMISOption": "Pairwise"},
+    "MultiScatter-P4-shutter-1/24": {"temporalReuse": "MultiScatter", "numTimePartitions": 4, "artificialFrameTime": 1.0 / 48.0},
+}
+MODE_SHUTTER = {"MultiScatter-P4-shutter-1/24": 1.0 / 24.0}
+
+
+def run_modes(args, torch, rs, scene, stream):
+    """The other temporal modes on the benchmark scene and camera path at 1080p (path length 4,
+    spatial reuse on): device frames/s from CUDA events over `args.mode_frames` frames after 4
+    warm-up frames, each mode in its own pass."""
+    W, H = W_FULL, H_FULL
+    color = torch.empty((H, W, 4), dtype=torch.float32, device="cuda")
+    out = {}
+    for name, props in MODE_PROPS.items():
+        p = rs.ReservoirSplatting(dict(props, maxSurfaceBounces=2, enableSpatialResampling=True), W, H)
+        p.set_scene(scene)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+        def cam(f):
+            c = camera(f, W, H)
+            c.shutter_speed = MODE_SHUTTER.get(name, 0.0)
+            return c
+
+        with torch.cuda.stream(stream):
+            for f in range(4):
+                p.execute(cam(f), color_ptr=color.data_ptr(), stream=stream.cuda_stream)
+            a.record(stream)
+            for f in range(4, 4 + args.mode_frames):
+                p.execute(cam(f), color_ptr=color.data_ptr(), stream=stream.cuda_stream)
+            b.record(stream)
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / args.mode_frames
+        out[name] = {"frames_per_s": round(1000.0 / ms, 3), "ms_per_frame": round(ms, 4)}
+        p.close()
+    out["how"] = (f"1920x1080, the benchmark scene and orbit, path length 4, spatial reuse on; {args.mode_frames} frames "
+                  "after 4 warm-up frames per mode, CUDA events on the launching stream; MultiScatter with shutter 1/24 s and "
+                  "artificial frame time 1/48 s on the static scene")
+    return out
 
 
 def batch_instances(count: int, seed: int = 11):
@@ -566,6 +612,8 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-quality", action="store_true")
     ap.add_argument("--no-motion-blur", action="store_true")
+    ap.add_argument("--no-modes", action="store_true")
+    ap.add_argument("--mode-frames", type=int, default=10)
     ap.add_argument("--gt-spp", type=int, default=512)
     ap.add_argument("--adjoint-reps", type=int, default=3)
     args = ap.parse_args()
