@@ -218,6 +218,10 @@ RS_API rs_status rs_update_geometry(rs_pass* pass, const float* positions, uint3
  * depth, internal children, leaf children, leaf triangles, surface-area cost}.  Both synchronise. */
 RS_API rs_status rs_debug_trace_rays(rs_pass* pass, const float* rays, uint32_t n, int32_t* prim, float* tuv, uint32_t* counts);
 RS_API rs_status rs_debug_bvh_shape(rs_pass* pass, double* out6);
+/* Binary-tree builder for the next rs_set_scene (no reference counterpart: the reference traces with
+ * the driver's RT acceleration structures): 0 = PLOC clustering (the default, the better tree),
+ * 1 = LBVH (Karras 2012 radix tree over the same Morton order).  Hits do not depend on it. */
+RS_API rs_status rs_set_bvh_builder(rs_pass* pass, uint32_t builder);
 /* Ray-query counts per stage of the last frame rendered with stage timing on (no reference
  * counterpart): rays[2i], rays[2i+1] = closest-hit and visibility queries of stage i, in the order of
  * rs_get_stage_times; *count = stages.  Only a library built with -DRS_RAY_STATS counts (build.py

@@ -53,6 +53,7 @@ def load_library():
     lib.rs_enable_stage_timing.argtypes = [C.c_void_p, C.c_uint32]
     lib.rs_get_stage_times.argtypes = [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_uint32), C.c_char_p, C.c_size_t]
     lib.rs_debug_stage_rays.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_uint32)]
+    lib.rs_set_bvh_builder.argtypes = [C.c_void_p, C.c_uint32]
     lib.rs_tonemap_default_options.argtypes = [C.POINTER(abi.RsTonemapOptions)]
     lib.rs_tonemap_default_options.restype = None
     lib.rs_tonemap_workspace_bytes.argtypes = []
@@ -81,6 +82,7 @@ def load_library():
                  "rs_debug_keep_candidates", "rs_batch_create", "rs_batch_execute", "rs_batch_destroy",
                  "rs_build_cell_lists_static", "rs_set_materials", "rs_checkpoint_bytes", "rs_checkpoint", "rs_backward",
                  "rs_backward_stats", "rs_debug_trace_rays", "rs_debug_bvh_shape", "rs_debug_stage_rays", "rs_tonemap",
+                 "rs_set_bvh_builder",
                  "rs_update_geometry"):
         getattr(lib, name).restype = C.c_int
     _lib = lib
@@ -255,6 +257,10 @@ class ReservoirSplatting:
         counts = np.empty((n, 2), np.uint32)
         _check(self._lib.rs_debug_trace_rays(self._h, r.ctypes.data, n, prim.ctypes.data, tuv.ctypes.data, counts.ctypes.data))
         return prim, tuv, counts
+
+    def set_bvh_builder(self, builder: str):
+        """Binary-tree builder of the next set_scene: "PLOC" (default) or "LBVH" (Karras radix tree)."""
+        _check(self._lib.rs_set_bvh_builder(self._h, {"PLOC": 0, "LBVH": 1}[builder]))
 
     def bvh_shape(self) -> dict:
         out = np.zeros(6, np.float64)

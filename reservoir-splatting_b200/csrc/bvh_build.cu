@@ -2,9 +2,10 @@
 //
 // 1. Binary tree: 63-bit Morton codes (21 bits per axis) of the triangle centroids, a key/index
 //    radix sort, the triangles gathered in key order, then PLOC clustering of the ordered leaves
-//    (below).  k_karras (Karras 2012, "Maximizing parallelism in the construction of BVHs, octrees,
-//    and k-d trees") is the LBVH alternative; k_refit is the bottom-up box pass with per-node
-//    arrival counters that refits either tree after geometry moves.
+//    (below), or with kBvhLbvh the LBVH of k_karras (Karras 2012, "Maximizing parallelism in the
+//    construction of BVHs, octrees, and k-d trees": the radix tree of the sorted keys) with its boxes
+//    from k_refit, the bottom-up box pass with per-node arrival counters that also refits either
+//    tree after geometry moves.
 // 2. Collapse of the binary tree (kept for closest-hit queries) into the 4-wide tree of bvh.cuh, top down, one thread per node
 //    and one launch per level: a node takes its binary node's two children and repeatedly opens
 //    the child of largest surface area that holds more than four triangles, up to four children;
@@ -484,7 +485,7 @@ void free_wide_bvh(WideBvh* b)
     *b = WideBvh();
 }
 
-cudaError_t build_wide_bvh(const float4* dTri, uint32_t n, WideBvh* out, cudaStream_t s)
+cudaError_t build_wide_bvh(const float4* dTri, uint32_t n, WideBvh* out, cudaStream_t s, BvhBuilder builder)
 {
     free_wide_bvh(out);
     if (n == 0) return cudaSuccess;
@@ -530,6 +531,16 @@ cudaError_t build_wide_bvh(const float4* dTri, uint32_t n, WideBvh* out, cudaStr
             RS_TRY(cudaMalloc(&parent, n * 4ull)); RS_TRY(cudaMalloc(&leafParent, n * 4ull)); RS_TRY(cudaMalloc(&arrivals, n * 4ull));
             RS_TRY(cudaMalloc(&qa, 8ull * maxWide)); RS_TRY(cudaMalloc(&qb, 8ull * maxWide));
             RS_TRY(cudaMemsetAsync(nodes, 0, 64ull * (n - 1), s));
+            k_leaf_tris<<<(n + 255) / 256, 256, 0, s>>>(sorted, n, out->leafTri);
+            if (builder == kBvhLbvh)
+            {
+                // the radix tree of the sorted keys (node 0 = root), then its boxes bottom up
+                k_karras<<<(n - 1 + 255) / 256, 256, 0, s>>>(keys2, (int)n, nodes, range, parent, leafParent);
+                RS_TRY(cudaMemsetAsync(arrivals, 0, n * 4ull, s));
+                k_refit<<<(n + 255) / 256, 256, 0, s>>>(dTri, out->leafTri, (int)n, nodes, parent, leafParent, arrivals);
+                RS_TRY(cudaGetLastError());
+            }
+            else
             {
                 // PLOC over the key-ordered leaves (node 0 = root); the binary tree the rest uses
                 ClusterBox *ca = nullptr, *cb = nullptr;
@@ -583,7 +594,7 @@ cudaError_t build_wide_bvh(const float4* dTri, uint32_t n, WideBvh* out, cudaStr
                 levels++;
             }
         }
-        k_leaf_tris<<<(n + 255) / 256, 256, 0, s>>>(sorted, n, out->leafTri);
+        if (n == 1) k_leaf_tris<<<1, 256, 0, s>>>(sorted, n, out->leafTri);
         uint32_t host[4];
         RS_TRY(cudaMemcpyAsync(host, counters, 16, cudaMemcpyDeviceToHost, s));
         RS_TRY(cudaGetLastError());

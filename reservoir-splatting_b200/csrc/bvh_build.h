@@ -26,7 +26,9 @@ struct WideBvh
 
 // Builds the tree over n triangles (dTri: three float4 per triangle, geom.h layout); replaces
 // *out.  Synchronises `s`.  n must be below kMaxBvhTriangles.
-cudaError_t build_wide_bvh(const float4* dTri, uint32_t n, WideBvh* out, cudaStream_t s);
+// Binary-tree builders: PLOC (the default) or the LBVH of Karras 2012 over the same Morton order.
+enum BvhBuilder : uint32_t { kBvhPloc = 0, kBvhLbvh = 1 };
+cudaError_t build_wide_bvh(const float4* dTri, uint32_t n, WideBvh* out, cudaStream_t s, BvhBuilder builder = kBvhPloc);
 void free_wide_bvh(WideBvh* b);
 
 // Refits both trees to moved triangles (same count and topology): leaf triangles, binary boxes

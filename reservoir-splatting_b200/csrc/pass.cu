@@ -104,6 +104,7 @@ struct rs_pass
     DevBuf<float4> dPrevTri;    // triangles of the previous frame after rs_update_geometry
     DevBuf<float> dPosStage;    // host positions staged for rs_update_geometry
     bool geometryMoved = false; // rs_update_geometry since the last frame
+    BvhBuilder bvhBuilder = kBvhPloc;
     bool hostTriStale = false;  // scene.tri positions behind the device copy
     DevBuf<MaterialData> dMaterials;
     DevBuf<LightTriangle> dLights;
@@ -393,7 +394,7 @@ extern "C" RS_API rs_status rs_set_scene(rs_pass* p, const rs_scene_desc* sd)
     }
     cudaStream_t s;
     RS_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-    cudaError_t e = build_wide_bvh(p->dTri.p, n, &p->bvh, s);
+    cudaError_t e = build_wide_bvh(p->dTri.p, n, &p->bvh, s, p->bvhBuilder);
     cudaStreamDestroy(s);
     if (e != cudaSuccess) return fail(RS_CUDA_ERROR, std::string("BVH build: ") + cudaGetErrorString(e));
     p->hasScene = true;
@@ -1225,6 +1226,15 @@ extern "C" RS_API rs_status rs_debug_trace_rays(rs_pass* p, const float* rays, u
     RS_CUDA(cudaMemcpy(prim, dp.p, 4ull * n, cudaMemcpyDeviceToHost));
     RS_CUDA(cudaMemcpy(tuv, dt.p, 12ull * n, cudaMemcpyDeviceToHost));
     RS_CUDA(cudaMemcpy(counts, dc.p, 8ull * n, cudaMemcpyDeviceToHost));
+    return RS_OK;
+}
+
+// The binary-tree builder of the next rs_set_scene: 0 = PLOC (default), 1 = LBVH (Karras radix tree).
+extern "C" RS_API rs_status rs_set_bvh_builder(rs_pass* p, uint32_t builder)
+{
+    if (!p) return fail(RS_INVALID_ARG, "pass is NULL");
+    if (builder > kBvhLbvh) return fail(RS_INVALID_ARG, "builder must be 0 (PLOC) or 1 (LBVH)");
+    p->bvhBuilder = static_cast<BvhBuilder>(builder);
     return RS_OK;
 }
 

@@ -24,8 +24,9 @@ def _cuda_ok():
 
 
 def run_pair(rs, oracle_mod, scene, camera_fn, props, frames=FRAMES, width=W, height=H, shutter=0.0, aperture=0.0,
-             check_candidates=True):
+             check_candidates=True, builder="PLOC"):
     gpu = rs.ReservoirSplatting(props, width, height)
+    gpu.set_bvh_builder(builder)
     gpu.keep_candidates(True)
     ora = oracle_mod.OraclePass(props, width, height)
     gpu.set_scene(scene)
@@ -116,11 +117,12 @@ def test_pcg32_and_longer_paths(rs, oracle_mod, scenes):
 
 
 @pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
-def test_terrain_scene_scatter_backup(rs, oracle_mod, scenes):
+@pytest.mark.parametrize("builder", ["PLOC", "LBVH"])
+def test_terrain_scene_scatter_backup(rs, oracle_mod, scenes, builder):
     sc = scenes.terrain_spheres(seed=7, grid=48, spheres=12, subdiv=2, lights=8, extent=40.0, height=4.0)
     props = {"temporalReuse": "ScatterBackup", "gatherOption": "Clamped", "maxSurfaceBounces": 2}
     cam = lambda f, w, h: scenes.orbit_camera(f, w, h, radius=30.0, height_above=12.0)
-    run_pair(rs, oracle_mod, sc, cam, props, frames=4, width=96, height=64)
+    run_pair(rs, oracle_mod, sc, cam, props, frames=4, width=96, height=64, builder=builder)
 
 
 @pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
@@ -193,8 +195,8 @@ def test_gpu_matches_committed_golden(rs, scenes, name):
 
 
 @pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
-@pytest.mark.parametrize("mode", ["ScatterBackup", "MultiScatter"])
-def test_moving_spheres(rs, oracle_mod, scenes, mode):
+@pytest.mark.parametrize("mode,builder", [("ScatterBackup", "PLOC"), ("MultiScatter", "PLOC"), ("ScatterBackup", "LBVH")])
+def test_moving_spheres(rs, oracle_mod, scenes, mode, builder):
     """Spheres moving linearly each frame (rs_update_geometry: refitted trees, previous-frame motion
     vectors) against the oracle, which rebuilds its own tree every frame."""
     sc = scenes.terrain_spheres(seed=5, grid=40, spheres=10, subdiv=2, lights=6, extent=30.0, height=3.0)
@@ -203,6 +205,7 @@ def test_moving_spheres(rs, oracle_mod, scenes, mode):
              "artificialFrameTime": 1.0 / 48.0, "enableSpatialResampling": True}
     W, H = 80, 56
     gpu = rs.ReservoirSplatting(props, W, H)
+    gpu.set_bvh_builder(builder)
     ora = oracle_mod.OraclePass(props, W, H)
     gpu.set_scene(sc)
     ora.set_scene(sc)

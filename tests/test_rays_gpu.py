@@ -52,10 +52,12 @@ def _rays(scene, rng, n):
 
 @pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
 @pytest.mark.parametrize("which", ["cornell", "terrain"])
-def test_closest_hits_match_the_oracle_tree(rs, oracle_mod, scenes, which):
+@pytest.mark.parametrize("builder", ["PLOC", "LBVH"])
+def test_closest_hits_match_the_oracle_tree(rs, oracle_mod, scenes, which, builder):
     sc = scenes.cornell_box(0) if which == "cornell" else scenes.terrain_spheres(seed=9, grid=64, spheres=20, subdiv=2, lights=8,
                                                                                    extent=30.0, height=3.0)
     p = rs.ReservoirSplatting({"maxSurfaceBounces": 1}, 16, 16)
+    p.set_bvh_builder(builder)
     p.set_scene(sc)
     ora = oracle_mod.OraclePass({"maxSurfaceBounces": 1}, 16, 16)
     ora.set_scene(sc)
