@@ -9,6 +9,7 @@
  *   rs_create / rs_destroy      registerPlugin + constructor           ReservoirSplatting.cpp:136-175
  *   rs_set_options              setProperties / parseProperties        ReservoirSplatting.cpp:177-261
  *   rs_set_scene                setScene (scene + light collection)    ReservoirSplatting.cpp:378-397
+ *   rs_set_env_map              Scene envMap + EnvMapSampler setup     Scene/Lights/EnvMap.cpp:60-137, Rendering/Lights/EnvMapSampler.cpp:45-113
  *   rs_execute                  execute (one frame)                    ReservoirSplatting.cpp:399-509
  *   rs_reset                    reset()                                ReservoirSplatting.cpp:813-820
  *   rs_set_seed                 Python useFixedSeed / fixedSeed        ReservoirSplatting.cpp:142-156
@@ -163,7 +164,8 @@ typedef enum rs_buffer_id {
     RS_BUF_CANDIDATE_RESERVOIRS = 11,
     RS_BUF_CANDIDATE_RECONNECTION = 12,
     RS_BUF_BACKUP_RESERVOIRS = 13,
-    RS_BUF_BACKUP_RECONNECTION = 14
+    RS_BUF_BACKUP_RECONNECTION = 14,
+    RS_BUF_ENV_IMPORTANCE = 15           /* float, the env map's importance mips 512^2 .. 1 back to back */
 } rs_buffer_id;
 
 typedef struct rs_pass rs_pass;
@@ -173,6 +175,22 @@ RS_API rs_status rs_create(const rs_options* opts, rs_pass** out);
 RS_API rs_status rs_destroy(rs_pass* pass);
 RS_API rs_status rs_set_options(rs_pass* pass, const rs_options* opts);
 RS_API rs_status rs_set_scene(rs_pass* pass, const rs_scene_desc* scene);
+/* Environment map light (Falcor EnvMap + EnvMapSampler).  A lat-long map of width x height RGBA
+ * float texels (host, row-major, row 0 at the top: v = 0 looks along +y), centred on -z and wrapping
+ * clockwise; radiance = bilinear texel value * intensity * tint, looked up after the rotation
+ * (XYZ Euler angles in degrees, EnvMap::setRotation).  The pass builds the 512 x 512 importance map
+ * with its mip chain on the device (64 luminance samples per texel) and samples the map for NEE in
+ * proportion to it; light types are picked with equal probability when the scene also has emissive
+ * triangles.  The light is used when intensity > 0 (Scene::useEnvLight).  NULL or width == 0 removes
+ * it.  Synchronous; the next frame uses the new map. */
+typedef struct rs_env_map {
+    uint32_t width, height;
+    const float* texels;                 /* host, 4 floats per texel (the fourth is ignored) */
+    float intensity;
+    float tint[3];
+    float rotation[3];                   /* degrees */
+} rs_env_map;
+RS_API rs_status rs_set_env_map(rs_pass* pass, const rs_env_map* env);
 RS_API rs_status rs_execute(rs_pass* pass, const rs_frame_desc* frame, void* cudaStream);
 RS_API rs_status rs_reset(rs_pass* pass);
 RS_API rs_status rs_set_seed(rs_pass* pass, uint32_t useFixedSeed, uint32_t fixedSeed);

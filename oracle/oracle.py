@@ -62,6 +62,9 @@ def load():
     lib.ro_set_threads.argtypes = [C.c_int]
     lib.ro_set_threads.restype = C.c_int
     lib.ro_set_scene.argtypes = [C.c_void_p, C.POINTER(a.RsSceneDesc)]
+    lib.ro_set_env_map.argtypes = [C.c_void_p, C.POINTER(a.RsEnvMap)]
+    lib.ro_get_env_importance.argtypes = [C.c_void_p, C.c_void_p]
+    lib.ro_env_debug.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]
     lib.ro_execute.argtypes = [C.c_void_p, C.POINTER(a.RsFrameDesc), C.c_void_p, C.c_void_p]
     lib.ro_freeze.argtypes = [C.c_void_p, C.c_int]
     lib.ro_reset.argtypes = [C.c_void_p]
@@ -108,6 +111,30 @@ class OraclePass:
         st = self._lib.ro_set_scene(self._h, C.byref(desc))
         if st != 0:
             raise RuntimeError(f"oracle set_scene failed: {st}")
+
+    def set_env_map(self, texels, intensity: float = 1.0, tint=(1.0, 1.0, 1.0), rotation=(0.0, 0.0, 0.0)):
+        desc, keep = self._abi.env_map_struct(texels, intensity, tint, rotation)
+        st = self._lib.ro_set_env_map(self._h, C.byref(desc))
+        del keep
+        if st != 0:
+            raise RuntimeError(f"oracle set_env_map failed: {st}")
+
+    def env_importance(self) -> np.ndarray:
+        """The importance mips (512^2 .. 1 texels back to back)."""
+        out = np.empty(349525, np.float32)
+        st = self._lib.ro_get_env_importance(self._h, out.ctypes.data)
+        if st != 0:
+            raise RuntimeError("no env map set")
+        return out
+
+    def env_samples(self, rnd: np.ndarray) -> np.ndarray:
+        """[n, 11]: sampled dir.xyz, pdf, Le.xyz, then evalPdf(dir) and eval(dir).xyz, for rnd [n, 2]."""
+        rnd = np.ascontiguousarray(rnd, np.float32)
+        out = np.empty((len(rnd), 11), np.float32)
+        st = self._lib.ro_env_debug(self._h, rnd.ctypes.data, len(rnd), out.ctypes.data)
+        if st != 0:
+            raise RuntimeError("no env map set")
+        return out
 
     def execute(self, camera, mvec: np.ndarray | None = None, should_reset: bool = False) -> np.ndarray:
         f = self._abi.RsFrameDesc()

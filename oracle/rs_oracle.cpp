@@ -33,6 +33,7 @@
 
 #include "../include/rs_b200.h"
 #include "../reservoir-splatting_b200/csrc/core/camera.h"
+#include "../reservoir-splatting_b200/csrc/core/envmap.h"
 #include "../reservoir-splatting_b200/csrc/core/scene_prep.h"
 #include "../reservoir-splatting_b200/csrc/core/material_grad.h"
 #include <cmath>
@@ -358,6 +359,9 @@ struct Pass
     Bvh bvh;
     bool hasScene = false;
     LightView lv;
+    // environment map (PathTracer.slang kUseEnvLight = env.present): texels and importance mips
+    EnvMapView env = {};
+    std::vector<float> envTexels, envImportance;
 
     uint32_t W = 0, H = 0;
     uint32_t frameCount = 0, seed = 0;
@@ -519,39 +523,56 @@ struct Pass
     struct LightSample
     {
         f3 Li; float pdf; f3 origin; float distance; f3 dir; uint32_t triangleId; f2 barycentrics; float geometryTerm;
+        uint32_t lightType; // 0 env map, 1 emissive (LightType)
     };
 
-    // generateLightSample (:668-701) with only emissive lights in the scene:
-    // p = {0, 1, 0}; the type-selection draw is always taken.
+    // getLightTypeSelectionProbabilities (:606-622): p = {env, emissive, 0} normalised
+    void lightTypeProbabilities(float& pEnv, float& pEmissive) const { light_type_probabilities(env.present != 0, lv.count > 0, pEnv, pEmissive); }
+
+    // generateLightSample (:668-701); the type-selection draw is always taken.
     bool generateLightSample(f3 vpos, f3 vfaceN, bool vfront, bool sampleUpper, bool sampleLower, SampleGen& sg, LightSample& ls) const
     {
         ls = LightSample();
-        float p1 = lv.count > 0 ? 1.f : 0.f;
+        float p[2];
+        lightTypeProbabilities(p[0], p[1]);
         float u = sampleNext1D(sg);
         // selectLightType (:634-656)
-        if (!(u < 0.f))
+        uint32_t lightType = 2;
+        for (uint32_t t = 0; t < 2; t++)
         {
-            u -= 0.f;
-            if (!(u < p1)) return false;
+            if (u < p[t]) { lightType = t; break; }
+            u -= p[t];
         }
-        else return false;
-        float selectionPdf = p1;
-        // generateEmissiveSample (:543-565)
-        TriangleLightSample tls;
-        f3 orientedN = vfront ? vfaceN : -vfaceN;
-        (void)orientedN;
-        if (!sample_emissive_power(lv, vpos, sg, tls)) return false;
-        ls.Li = tls.pdf > 0.f ? tls.Le / tls.pdf : mk3(0.f);
-        ls.pdf = tls.pdf;
-        f3 lightPos = computeRayOrigin(tls.posW, tls.normalW);
-        f3 toL = lightPos - vpos;
-        ls.origin = computeRayOrigin(vpos, dot(vfaceN, toL) >= 0.f ? vfaceN : -vfaceN);
-        f3 toLight = lightPos - ls.origin;
-        ls.distance = length(toLight);
-        ls.dir = normalize(toLight);
-        ls.barycentrics = tls.uv;
-        ls.triangleId = tls.triangleIndex;
-        ls.geometryTerm = tls.geometryTerm;
+        if (lightType == 2) return false;
+        float selectionPdf = p[lightType];
+        ls.lightType = lightType;
+        if (lightType == 0)
+        {
+            // generateEnvMapSample (:516-534)
+            f2 r; r.x = sampleNext1D(sg); r.y = sampleNext1D(sg);
+            f3 Le;
+            env_sample(env, r, ls.dir, ls.pdf, Le);
+            ls.Li = ls.pdf > 0.f ? Le / ls.pdf : mk3(0.f);
+            ls.origin = computeRayOrigin(vpos, dot(vfaceN, ls.dir) >= 0.f ? vfaceN : -vfaceN);
+            ls.distance = kRayTMax;
+        }
+        else
+        {
+            // generateEmissiveSample (:543-565)
+            TriangleLightSample tls;
+            if (!sample_emissive_power(lv, vpos, sg, tls)) return false;
+            ls.Li = tls.pdf > 0.f ? tls.Le / tls.pdf : mk3(0.f);
+            ls.pdf = tls.pdf;
+            f3 lightPos = computeRayOrigin(tls.posW, tls.normalW);
+            f3 toL = lightPos - vpos;
+            ls.origin = computeRayOrigin(vpos, dot(vfaceN, toL) >= 0.f ? vfaceN : -vfaceN);
+            f3 toLight = lightPos - ls.origin;
+            ls.distance = length(toLight);
+            ls.dir = normalize(toLight);
+            ls.barycentrics = tls.uv;
+            ls.triangleId = tls.triangleIndex;
+            ls.geometryTerm = tls.geometryTerm;
+        }
         if (!any_gt0(ls.Li)) return false;
         float NdotL = dot(vfront ? vfaceN : -vfaceN, ls.dir);
         if ((!sampleUpper && NdotL >= -kMinCosTheta) || (!sampleLower && NdotL <= kMinCosTheta)) return false;
@@ -607,7 +628,9 @@ struct Pass
             if (lv.count > 0 && !isPrimaryHit && path.isLightSampled() && isLightSamplable)
             {
                 // upperHemisphere is ignored by the power sampler
-                lightPdf = 1.f * eval_emissive_pdf(lv, path.origin, sd.lightIndex, sd.posW, sd_oriented_face_normal(sd));
+                float pEnv, pEmissive;
+                lightTypeProbabilities(pEnv, pEmissive);
+                lightPdf = pEmissive * eval_emissive_pdf(lv, path.origin, sd.lightIndex, sd.posW, sd_oriented_face_normal(sd));
                 misWeight = mis(path.totalPdf, lightPdf);
             }
             bool selected = path.reservoir.addVertex(path.sg, 1.f, path.reconnection.earlyThroughput * path.thp * d.emission * misWeight);
@@ -660,12 +683,21 @@ struct Pass
                             s.lightIsNEE = true;
                             s.irradiance = Le;
                             if (path.getVertexIndex() == 1) s.transmissionEvent = dot(sd.faceN, sd.V) * dot(sd.faceN, ls.dir) < 0.f;
-                            s.lightIsDistant = false;
+                            s.lightIsDistant = ls.lightType == 0;
                             if (path.getVertexIndex() == 1)
                             {
-                                s.secondHit = hit_tri(lv.tris[ls.triangleId].sceneTri, ls.barycentrics.x, ls.barycentrics.y);
-                                s.secondaryPathJacobian = ls.pdf * ls.geometryTerm;
-                                s.lightPdf = ls.pdf * ls.geometryTerm;
+                                if (ls.lightType == 0)
+                                {
+                                    s.secondHit = hit_direction(ls.dir);
+                                    s.secondaryPathJacobian = ls.pdf;
+                                    s.lightPdf = ls.pdf; // a distant light: no area measure
+                                }
+                                else
+                                {
+                                    s.secondHit = hit_tri(lv.tris[ls.triangleId].sceneTri, ls.barycentrics.x, ls.barycentrics.y);
+                                    s.secondaryPathJacobian = ls.pdf * ls.geometryTerm;
+                                    s.lightPdf = ls.pdf * ls.geometryTerm;
+                                }
                             }
                             else if (path.getVertexIndex() == 2)
                             {
@@ -699,13 +731,69 @@ struct Pass
         if (!valid) path.terminate();
     }
 
-    // handleMiss (:1433-1524) without an environment map
+    // handleMiss (:1433-1524)
     void handleMiss(PathState& path) const
     {
         float prevScatterPdf = path.pdf;
         float geometryFactor = 1.f;
         if (path.getVertexIndex() == 2) path.reconnection.secondaryPathJacobian = prevScatterPdf * geometryFactor;
         else if (path.getVertexIndex() == 3) path.reconnection.secondaryPathJacobian *= prevScatterPdf;
+        const bool isLightSamplable = path.isLightSamplable();
+        bool computeEnv = env.present && (!path.isLightSampled() || !isLightSamplable);
+        if (computeEnv)
+        {
+            float misWeight = 1.f;
+            float lightPdf = 0.f;
+            if (path.isLightSampled() && isLightSamplable)
+            {
+                float pEnv, pEmissive;
+                lightTypeProbabilities(pEnv, pEmissive);
+                lightPdf = pEnv * env_eval_pdf(env, path.dir);
+                misWeight = mis(path.totalPdf, lightPdf);
+            }
+            f3 Le = env_eval(env, path.dir);
+            f3 emitterRadiance = misWeight * Le;
+            bool selected = path.reservoir.addVertex(path.sg, 1.f, path.reconnection.earlyThroughput * path.thp * Le * misWeight);
+            if (selected)
+            {
+                path.reservoir.selectedReconnection = path.reconnection;
+                ReconnectionData& s = path.reservoir.selectedReconnection;
+                s.pathLength = path.getVertexIndex();
+                s.lightIsNEE = false;
+                s.lightIsDistant = true;
+                s.lightPdf = lightPdf;
+                if (path.getVertexIndex() == 2) s.secondHit = hit_direction(path.dir);
+                if (path.getVertexIndex() == 2 || path.getVertexIndex() == 3) s.irradiance = Le;
+                else s.irradiance = path.thp * emitterRadiance;
+            }
+        }
+        path.terminate();
+    }
+
+    // handlePrimaryMiss (:1529-1569)
+    void handlePrimaryMiss(PathState& path) const
+    {
+        if (env.present)
+        {
+            f3 Le = env_eval(env, path.dir);
+            bool selected = path.reservoir.addVertex(path.sg, 1.f, Le);
+            if (selected)
+            {
+                path.reservoir.selectedReconnection = path.reconnection;
+                ReconnectionData& s = path.reservoir.selectedReconnection;
+                s.lightIsDistant = true;
+                CameraData cam; orient(cam, path.time);
+                f3 camDir = normalize(cam.cameraW);
+                float cosSensor = dot(camDir, path.dir);
+                s.subPixelJacobian = 1.f / f_abs(f_pow3(cosSensor));
+                float focalPlaneZ = length(cam.cameraW);
+                float d0 = focalPlaneZ / dot(camDir, path.dir);
+                s.lensVertexJacobian = (d0 * d0) / f_abs(cosSensor);
+                s.firstWi = -path.dir;
+                s.pathLength = 1;
+                s.irradiance = Le;
+            }
+        }
         path.terminate();
     }
 
@@ -779,6 +867,9 @@ struct Pass
     }
 
     // handleReconnectionPrimaryLight (:1399-1410)
+    // handleReconnectionEnvMap (:1412-1416)
+    f3 handleReconnectionEnvMap(const PathState& path) const { return env_reconnection(env, path.dir); }
+
     f3 handleReconnectionPrimaryLight(const PathState& path) const
     {
         ShadingData sd = loadSD(path.hit, path.dir);
@@ -792,6 +883,9 @@ struct Pass
         dstJacobian = 1.f;
         handleReconnectionHit(path, rd, dstJacobian);
         if (!path.isActive()) return mk3(0.f);
+        // Length 2 uses none of the x2 terms (misWeight stays 1); the reference still loads x2's
+        // shading data, which for an environment vertex is a direction, not a hit, so skip it.
+        if (rd.pathLength == 2) return 1.f * path.thp * rd.irradiance;
         ShadingData secondSd = loadSD(rd.secondHit, path.dir);
         BsdfData d = instance(secondSd);
         uint32_t lobeMask = 1u << rd.secondBSDFComponentType;
@@ -854,7 +948,14 @@ struct Pass
         }
         else
         {
-            return ShiftedPathData(); // no environment map: an expected hit that misses fails
+            if (!hitEnvMap) return ShiftedPathData(); // an expected hit that misses fails
+            sp.radiance = handleReconnectionEnvMap(path);
+            float cosSensor = dot(camDir, path.dir);
+            sp.subPixelJacobian = 1.f / f_abs(f_pow3(cosSensor));
+            float focalPlaneZ = length(cam.cameraW);
+            float d0 = focalPlaneZ / dot(camDir, path.dir);
+            sp.lensVertexJacobian = (d0 * d0) / f_abs(cosSensor);
+            return sp;
         }
         if (rd.pathLength == 1)
         {
@@ -879,9 +980,15 @@ struct Pass
         f2 ndc = mk2(2.f * p.x + -1.f, -2.f * p.y + 1.f);
         f3 filmWorld = cam.posW + (cam.cameraU * ndc.x + cam.cameraV * ndc.y + cam.cameraW);
         f3 x1, n;
-        if (hitEnvMap) return ShiftedPathData(); // no environment map
-        if (!hit_valid(primaryHit)) return ShiftedPathData();
+        if (hitEnvMap)
         {
+            path.dir = -rd.firstWi;
+            x1 = filmWorld + path.dir;
+            n = mk3(0.f);
+        }
+        else
+        {
+            if (!hit_valid(primaryHit)) return ShiftedPathData();
             ShadingData sd = loadSD(primaryHit, mk3(0.f));
             x1 = sd.posW;
             path.dir = normalize(x1 - filmWorld);
@@ -891,14 +998,14 @@ struct Pass
         float camZ = dot(x1 - cam.posW, camDir);
         float rayT = camZ / dot(path.dir, camDir);
         path.origin = x1 - path.dir * rayT;
-        path.dir = normalize(x1 - path.origin);
+        path.dir = hitEnvMap ? path.dir : normalize(x1 - path.origin);
         f3 lensOffsetWorld = path.origin - cam.posW;
         f2 lensLocalNormalized = mk2(dot(lensOffsetWorld, normalize(cam.cameraU)) / cam.apertureRadius,
                                      dot(lensOffsetWorld, normalize(cam.cameraV)) / cam.apertureRadius);
         if (length(lensLocalNormalized) > 1.f) return ShiftedPathData();
         float dist = length(x1 - path.origin);
-        float rayMin = 0.001f * dist;
-        float rayMax = 0.999f * dist;
+        float rayMin = hitEnvMap ? 0.001f : 0.001f * dist;
+        float rayMax = hitEnvMap ? kRayTMax : 0.999f * dist;
         if (!traceVisibilityRay(mk_ray(path.origin, path.dir, rayMin, rayMax))) return ShiftedPathData();
         sp.firstRayDir = path.dir;
         sp.fractionalPixel = fractionalPixel;
@@ -907,6 +1014,16 @@ struct Pass
         path.sg = makeSg((uint32_t)fractionalPixel.x, (uint32_t)fractionalPixel.y, f2u(sampleNext1D(sg)));
         path.incrementVertexIndex();
         path.hit = primaryHit; path.setFlag(kHit);
+        if (hitEnvMap)
+        {
+            sp.radiance = handleReconnectionEnvMap(path);
+            float cosSensor = dot(camDir, path.dir);
+            sp.subPixelJacobian = 1.f / f_abs(f_pow3(cosSensor));
+            float focalPlaneZ = length(cam.cameraW);
+            float d0 = focalPlaneZ / dot(camDir, path.dir);
+            sp.lensVertexJacobian = (d0 * d0) / f_abs(dot(camDir, path.dir));
+            return sp;
+        }
         {
             float dist2 = length(x1 - path.origin);
             float distSquared = dist2 * dist2;
@@ -942,9 +1059,10 @@ struct Pass
         f3 lensWorld = camU * lensLocal.x + camV * lensLocal.y;
         path.origin = cam.posW + lensWorld;
         f3 x1 = mk3(0.f), n = mk3(0.f);
-        if (hitEnvMap) return ShiftedPathData(); // no environment map
-        if (!hit_valid(primaryHit)) return ShiftedPathData();
+        if (hitEnvMap) path.dir = -rd.firstWi;
+        else
         {
+            if (!hit_valid(primaryHit)) return ShiftedPathData();
             ShadingData firstSd = loadSD(primaryHit, mk3(0.f));
             x1 = firstSd.posW;
             n = firstSd.faceN;
@@ -959,7 +1077,7 @@ struct Pass
         f2 nfp = mk2((0.5f * ndc.x + 0.5f) * (float)W, (-0.5f * ndc.y + 0.5f) * (float)H);
         if (!validFloat(nfp)) return ShiftedPathData();
         float dist = length(x1 - path.origin);
-        float rayMax = 0.999f * dist;
+        float rayMax = hitEnvMap ? kRayTMax : 0.999f * dist;
         if (!skipVisibilityCheck && !traceVisibilityRay(mk_ray(path.origin, path.dir, 0.001f, rayMax))) return ShiftedPathData();
         sp.lensSample = lensSample;
         sp.firstRayDir = path.dir;
@@ -968,6 +1086,16 @@ struct Pass
         path.sg = makeSg((uint32_t)nfp.x, (uint32_t)nfp.y, f2u(sampleNext1D(sg)));
         path.incrementVertexIndex();
         path.hit = primaryHit; path.setFlag(kHit);
+        if (hitEnvMap)
+        {
+            sp.radiance = handleReconnectionEnvMap(path);
+            float cosSensor = dot(camDir, path.dir);
+            sp.subPixelJacobian = 1.f / f_abs(f_pow3(cosSensor));
+            float focalPlaneZ = length(cam.cameraW);
+            float d0 = focalPlaneZ / dot(camDir, path.dir);
+            sp.lensVertexJacobian = (d0 * d0) / f_abs(cosSensor);
+            return sp;
+        }
         {
             float distSquared = dist * dist;
             float cosNormal = dot(-path.dir, n);
@@ -1043,7 +1171,7 @@ struct Pass
                     }
                     else
                     {
-                        path.terminate(); // handlePrimaryMiss without an environment map
+                        handlePrimaryMiss(path);
                     }
                     // addCandidateReservoir (:52-75)
                     const bool isFirstSample = (path.sampleIdx() == (spp - 1));
@@ -1127,7 +1255,14 @@ struct Pass
                     nr.tMin = 0.001f * length(x1 - nr.origin);
                     nr.tMax = 0.999f * length(x1 - nr.origin);
                 }
-                else continue; // no environment map: an invalid first hit cannot be reprojected
+                else if (rd.lightIsDistant)
+                {
+                    // an environment sample reprojects by its direction (:110-118)
+                    nr.dir = -rd.firstWi;
+                    nr.tMin = 0.001f;
+                    nr.tMax = kRayTMax;
+                }
+                else continue; // an invalid first hit cannot be reprojected
                 f3 camDir = mk3(dot(normalize(currCam.cameraU), nr.dir), dot(normalize(currCam.cameraV), nr.dir), dot(normalize(currCam.cameraW), nr.dir));
                 if (camDir.z <= 0.001f) continue;
                 if (!traceVisibilityRay(nr)) continue;
@@ -1607,6 +1742,11 @@ struct Pass
                         f3 x1 = loadSD(rd.firstHit, mk3(0.f)).posW;
                         rayDir = x1 - cc.posW;
                         rayLength = 0.999f;
+                    }
+                    else if (rd.lightIsDistant)
+                    {
+                        rayDir = -rd.firstWi;
+                        rayLength = kRayTMax;
                     }
                     else continue;
                     f3 nd = normalize(rayDir);
@@ -2228,6 +2368,63 @@ __attribute__((visibility("default"))) ro_pass* ro_create(const rs_options* opt)
 }
 __attribute__((visibility("default"))) void ro_destroy(ro_pass* r) { delete r; }
 __attribute__((visibility("default"))) int ro_set_threads(int n) { if (n > 0) omp_set_num_threads(n); return omp_get_max_threads(); }
+
+// Scene envMap + EnvMapSampler::createImportanceMap (EnvMap.cpp:60-137, EnvMapSampler.cpp:80-113):
+// the texels, the transform, and the importance mips built on the host with the device's
+// per-texel and reduction functions.
+__attribute__((visibility("default"))) int ro_set_env_map(ro_pass* r, const rs_env_map* m)
+{
+    oracle::Pass& p = r->p;
+    EnvMapView v = {};
+    if (m && m->width > 0)
+    {
+        if (!m->texels || m->height == 0) return RS_INVALID_ARG;
+        p.envTexels.assign(m->texels, m->texels + 4 * (size_t)m->width * m->height);
+        p.envImportance.assign(kEnvImportanceTexels, 0.f);
+        v.texels = p.envTexels.data();
+        v.importance = p.envImportance.data();
+        v.w = m->width; v.h = m->height;
+        v.present = m->intensity > 0.f ? 1u : 0u;
+        env_transform(m->rotation, v.toWorld, v.toLocal);
+        for (int k = 0; k < 3; k++) v.scale[k] = m->intensity * m->tint[k];
+        float* imp = p.envImportance.data();
+        #pragma omp parallel for schedule(dynamic, 8)
+        for (int y = 0; y < (int)kEnvImportanceDim; y++)
+            for (uint32_t x = 0; x < kEnvImportanceDim; x++) imp[(size_t)y * kEnvImportanceDim + x] = env_importance_texel(v, x, (uint32_t)y);
+        for (uint32_t mip = 1; mip < kEnvImportanceMips; mip++)
+        {
+            const uint32_t d = kEnvImportanceDim >> mip;
+            for (uint32_t y = 0; y < d; y++)
+                for (uint32_t x = 0; x < d; x++) imp[env_mip_offset(mip) + y * d + x] = env_importance_reduce(imp, mip, x, y);
+        }
+    }
+    p.env = v;
+    return RS_OK;
+}
+
+// Sampler checks: for each of n pairs of uniform numbers, env_sample's direction, pdf and radiance,
+// then env_eval_pdf and env_eval of that direction (9 + 2 floats per sample).
+__attribute__((visibility("default"))) int ro_env_debug(ro_pass* r, const float* rnd, uint32_t n, float* out)
+{
+    const EnvMapView& e = r->p.env;
+    if (!e.importance) return RS_NOT_READY;
+    for (uint32_t i = 0; i < n; i++)
+    {
+        f3 dir, Le; float pdf;
+        env_sample(e, mk2(rnd[2 * i], rnd[2 * i + 1]), dir, pdf, Le);
+        const f3 ev = env_eval(e, dir);
+        const float o[11] = {dir.x, dir.y, dir.z, pdf, Le.x, Le.y, Le.z, env_eval_pdf(e, dir), ev.x, ev.y, ev.z};
+        memcpy(out + 11 * (size_t)i, o, sizeof(o));
+    }
+    return RS_OK;
+}
+
+__attribute__((visibility("default"))) int ro_get_env_importance(ro_pass* r, float* out)
+{
+    if (r->p.envImportance.size() != kEnvImportanceTexels) return RS_NOT_READY;
+    memcpy(out, r->p.envImportance.data(), kEnvImportanceTexels * sizeof(float));
+    return RS_OK;
+}
 
 __attribute__((visibility("default"))) int ro_set_scene(ro_pass* r, const rs_scene_desc* s)
 {

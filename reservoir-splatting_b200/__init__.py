@@ -44,6 +44,7 @@ def load_library():
     lib.rs_destroy.argtypes = [C.c_void_p]
     lib.rs_set_options.argtypes = [C.c_void_p, C.POINTER(abi.RsOptions)]
     lib.rs_set_scene.argtypes = [C.c_void_p, C.POINTER(abi.RsSceneDesc)]
+    lib.rs_set_env_map.argtypes = [C.c_void_p, C.POINTER(abi.RsEnvMap)]
     lib.rs_execute.argtypes = [C.c_void_p, C.POINTER(abi.RsFrameDesc), C.c_void_p]
     lib.rs_reset.argtypes = [C.c_void_p]
     lib.rs_set_seed.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32]
@@ -77,7 +78,7 @@ def load_library():
     lib.rs_debug_trace_rays.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]
     lib.rs_debug_bvh_shape.argtypes = [C.c_void_p, C.c_void_p]
     lib.rs_build_cell_lists_static.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
-    for name in ("rs_create", "rs_destroy", "rs_set_options", "rs_set_scene", "rs_execute", "rs_reset", "rs_set_seed",
+    for name in ("rs_create", "rs_destroy", "rs_set_options", "rs_set_scene", "rs_set_env_map", "rs_execute", "rs_reset", "rs_set_seed",
                  "rs_freeze", "rs_get_buffer", "rs_set_buffer", "rs_enable_stage_timing", "rs_get_stage_times",
                  "rs_debug_keep_candidates", "rs_batch_create", "rs_batch_execute", "rs_batch_destroy",
                  "rs_build_cell_lists_static", "rs_set_materials", "rs_checkpoint_bytes", "rs_checkpoint", "rs_backward",
@@ -126,6 +127,12 @@ class ReservoirSplatting:
     def set_scene(self, scene):
         desc, keep = abi.scene_struct(scene)
         _check(self._lib.rs_set_scene(self._h, C.byref(desc)))
+        del keep
+
+    def set_env_map(self, texels, intensity: float = 1.0, tint=(1.0, 1.0, 1.0), rotation=(0.0, 0.0, 0.0)):
+        """Environment light from a lat-long map float [H, W, 3|4] (None removes it); see rs_set_env_map."""
+        desc, keep = abi.env_map_struct(texels, intensity, tint, rotation)
+        _check(self._lib.rs_set_env_map(self._h, C.byref(desc)))
         del keep
 
     def reset(self):

@@ -24,7 +24,7 @@ BUF = {
     "curr_reservoirs": 0, "curr_reconnection": 1, "prev_reservoirs": 2, "prev_reconnection": 3,
     "cell_counters": 4, "cell_offsets": 5, "sorted_splats": 6, "floating_coords": 7, "mvec": 8, "vbuffer": 9,
     "splat_targets": 10, "candidate_reservoirs": 11, "candidate_reconnection": 12,
-    "backup_reservoirs": 13, "backup_reconnection": 14,
+    "backup_reservoirs": 13, "backup_reconnection": 14, "env_importance": 15,
 }
 
 
@@ -41,6 +41,30 @@ class RsOptions(C.Structure):
         ("useConfidenceWeightsSpatially", C.c_uint32), ("artificialFrameTime", C.c_float), ("frameWidth", C.c_uint32),
         ("frameHeight", C.c_uint32),
     ]
+
+
+class RsEnvMap(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("texels", C.c_void_p), ("intensity", C.c_float),
+                ("tint", C.c_float * 3), ("rotation", C.c_float * 3)]
+
+
+def env_map_struct(texels, intensity=1.0, tint=(1.0, 1.0, 1.0), rotation=(0.0, 0.0, 0.0)) -> tuple[RsEnvMap, np.ndarray | None]:
+    """Descriptor of a lat-long map given as float [H, W, 3] or [H, W, 4] (row 0 at the top), and the
+    RGBA array it points into (keep it alive during the call).  None removes the map."""
+    e = RsEnvMap()
+    if texels is None:
+        return e, None
+    t = np.asarray(texels, np.float32)
+    if t.ndim != 3 or t.shape[2] not in (3, 4):
+        raise ValueError("env map texels must be [H, W, 3] or [H, W, 4]")
+    rgba = np.zeros((t.shape[0], t.shape[1], 4), np.float32)
+    rgba[..., :t.shape[2]] = t
+    rgba = np.ascontiguousarray(rgba)
+    e.width, e.height, e.texels = t.shape[1], t.shape[0], rgba.ctypes.data
+    e.intensity = float(intensity)
+    e.tint[:] = [float(v) for v in tint]
+    e.rotation[:] = [float(v) for v in rotation]
+    return e, rgba
 
 
 class RsSceneDesc(C.Structure):
@@ -170,7 +194,7 @@ BUFFER_LAYOUT = {
     "curr_reservoirs": (np.float32, 8), "prev_reservoirs": (np.float32, 8), "candidate_reservoirs": (np.float32, 8),
     "backup_reservoirs": (np.float32, 8),
     "curr_reconnection": (np.uint32, 28), "prev_reconnection": (np.uint32, 28), "candidate_reconnection": (np.uint32, 28),
-    "backup_reconnection": (np.uint32, 28),
+    "backup_reconnection": (np.uint32, 28), "env_importance": (np.float32, 1),
     "cell_counters": (np.uint32, 1), "cell_offsets": (np.uint32, 1), "sorted_splats": (np.uint32, 1),
     "splat_targets": (np.uint32, 1), "floating_coords": (np.float32, 2), "mvec": (np.float32, 2), "vbuffer": (np.uint32, 4),
 }

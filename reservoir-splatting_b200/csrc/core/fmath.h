@@ -152,6 +152,17 @@ RS_HD float f_acos(float x)
     return kPi - f_atan(s / -x);
 }
 
+// atan2 from atan of the quotient of magnitudes, placed in the quadrant of (x, y): (0, 0) gives 0,
+// x = 0 gives +-pi/2, y = +-0 with x < 0 gives pi.
+RS_HD float f_atan2(float y, float x)
+{
+    if (f_isnan(x) || f_isnan(y)) return x + y;
+    if (x == 0.f) return y > 0.f ? kPiOver2 : (y < 0.f ? -kPiOver2 : 0.f);
+    float a = f_atan(fabsf(y) / fabsf(x));
+    if (x < 0.f) a = kPi - a;
+    return y < 0.f ? -a : a;
+}
+
 // Integer powers written out as products (replaces pow(x, 3) / pow(x, 5)).
 RS_HD float f_pow3(float x) { return x * x * x; }
 RS_HD float f_pow5(float x) { float x2 = x * x; return x2 * x2 * x; }

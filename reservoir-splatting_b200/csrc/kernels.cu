@@ -198,7 +198,7 @@ __device__ void handle_hit(const DevCtx& C, PState& path, const RecPlanes& outRe
         float lightPdf = 0.f;
         if (haveLights && !isPrimaryHit && isLightSampled && isLightSamplable)
         {
-            lightPdf = 1.f * eval_emissive_pdf(C.lights, path.origin, sd.lightIndex, sd.posW, sd_oriented_face_normal(sd));
+            lightPdf = C.pEmissiveLight * eval_emissive_pdf(C.lights, path.origin, sd.lightIndex, sd.posW, sd_oriented_face_normal(sd));
             misWeight = dev_mis(C, path.totalPdf, lightPdf);
         }
         bool selected = cand_add_vertex(path, 1.f, path.earlyThroughput * path.thp * d.emission * misWeight);
@@ -227,15 +227,30 @@ __device__ void handle_hit(const DevCtx& C, PState& path, const RecPlanes& outRe
     {
         bool sampleUpper = (lobeTypes & kLobeNonDeltaReflection) != 0;
         bool sampleLower = (lobeTypes & kLobeNonDeltaTransmission) != 0;
-        // generateLightSample (:668-701) with p = {0, haveLights, 0}: the type-selection draw is always taken.
-        bool validSample = false;
+        // generateLightSample (:668-701): the type-selection draw is always taken, then the env map
+        // (p = pEnvLight) or the emissive triangles (p = pEmissiveLight) are sampled.
+        bool validSample = false, lsEnv = false;
         TriangleLightSample tls;
         f3 lsLi = mk3(0.f), lsOrigin = mk3(0.f), lsDir = mk3(0.f);
-        float lsPdf = 0.f, lsDistance = 0.f;
+        float lsPdf = 0.f, lsDistance = 0.f, selectionPdf = 0.f;
+        bool sampled = false;
         float u = sampleNext1D(path.sg);
-        if (!(u < 0.f) && (u < (haveLights ? 1.f : 0.f)))
+        if (u < C.pEnvLight)
         {
-            const float selectionPdf = 1.f;
+            // generateEnvMapSample (:516-534)
+            selectionPdf = C.pEnvLight;
+            lsEnv = true;
+            f2 r2; r2.x = sampleNext1D(path.sg); r2.y = sampleNext1D(path.sg);
+            f3 envLe;
+            env_sample(*C.env, r2, lsDir, lsPdf, envLe);
+            lsLi = lsPdf > 0.f ? envLe / lsPdf : mk3(0.f);
+            lsOrigin = computeRayOrigin(sd.posW, dot(sd.faceN, lsDir) >= 0.f ? sd.faceN : -sd.faceN);
+            lsDistance = kRayTMax;
+            sampled = any_gt0(lsLi);
+        }
+        else if (u - C.pEnvLight < C.pEmissiveLight)
+        {
+            selectionPdf = C.pEmissiveLight;
             if (sample_emissive_power(C.lights, sd.posW, path.sg, tls))
             {
                 lsLi = tls.pdf > 0.f ? tls.Le / tls.pdf : mk3(0.f);
@@ -246,16 +261,17 @@ __device__ void handle_hit(const DevCtx& C, PState& path, const RecPlanes& outRe
                 f3 toLight = lightPos - lsOrigin;
                 lsDistance = length(toLight);
                 lsDir = normalize(toLight);
-                if (any_gt0(lsLi))
-                {
-                    float NdotL = dot(sd_oriented_face_normal(sd), lsDir);
-                    if (!((!sampleUpper && NdotL >= -kMinCosTheta) || (!sampleLower && NdotL <= kMinCosTheta)))
-                    {
-                        lsPdf *= selectionPdf;
-                        lsLi /= selectionPdf;
-                        validSample = true;
-                    }
-                }
+                sampled = any_gt0(lsLi);
+            }
+        }
+        if (sampled)
+        {
+            float NdotL = dot(sd_oriented_face_normal(sd), lsDir);
+            if (!((!sampleUpper && NdotL >= -kMinCosTheta) || (!sampleLower && NdotL <= kMinCosTheta)))
+            {
+                lsPdf *= selectionPdf;
+                lsLi /= selectionPdf;
+                validSample = true;
             }
         }
         if (sampleUpper) path.flags |= kPLightUpper;
@@ -278,12 +294,21 @@ __device__ void handle_hit(const DevCtx& C, PState& path, const RecPlanes& outRe
                     sel.lightIsNEE = true;
                     sel.irradiance = Le;
                     if (path.vertex == 1) sel.transmissionEvent = dot(sd.faceN, sd.V) * dot(sd.faceN, lsDir) < 0.f;
-                    sel.lightIsDistant = false;
+                    sel.lightIsDistant = lsEnv;
                     if (path.vertex == 1)
                     {
-                        sel.secondHit = hit_tri(C.lights.tris[tls.triangleIndex].sceneTri, tls.uv.x, tls.uv.y);
-                        sel.secondaryPathJacobian = lsPdf * tls.geometryTerm;
-                        sel.lightPdf = lsPdf * tls.geometryTerm;
+                        if (lsEnv)
+                        {
+                            sel.secondHit = hit_direction(lsDir);
+                            sel.secondaryPathJacobian = lsPdf;
+                            sel.lightPdf = lsPdf; // a distant light: no area measure
+                        }
+                        else
+                        {
+                            sel.secondHit = hit_tri(C.lights.tris[tls.triangleIndex].sceneTri, tls.uv.x, tls.uv.y);
+                            sel.secondaryPathJacobian = lsPdf * tls.geometryTerm;
+                            sel.lightPdf = lsPdf * tls.geometryTerm;
+                        }
                     }
                     else if (path.vertex == 2)
                     {
@@ -389,8 +414,74 @@ __device__ __forceinline__ void path_init(const DevCtx& C, uint32_t x, uint32_t 
     path.prevHitPos = camera_lens_point(cam, path.rec.lensSample);
 }
 
+template <bool kDirect>
+__device__ __forceinline__ void select_record(PState& path, const Recon& sel, const RecPlanes& outRec, uint32_t pix)
+{
+    if (kDirect) { store_rec(outRec, pix, sel); path.anySelected = true; }
+    else path.candRec = sel;
+}
+
+// handlePrimaryMiss (PathTracer.slang:1529-1569): the environment seen straight through the pixel.
+// The camera is the one at time 0 (generatePath leaves path.time unset).
+template <bool kDirect>
+__device__ void handle_primary_miss(const DevCtx& C, PState& path, const RecPlanes& outRec, uint32_t pix)
+{
+    const EnvMapView& E = *C.env;
+    if (!E.present) return;
+    const f3 Le = env_eval(E, path.dir);
+    if (cand_add_vertex(path, 1.f, Le))
+    {
+        Recon sel = path.rec;
+        sel.lightIsDistant = true;
+        CameraData cam; dev_orient(C, cam, 0.f);
+        const f3 camDir = cam.unitW;
+        const float cosSensor = dot(camDir, path.dir);
+        sel.subPixelJacobian = 1.f / f_abs(f_pow3(cosSensor));
+        const float d0 = cam.lenW / dot(camDir, path.dir);
+        sel.lensVertexJacobian = (d0 * d0) / f_abs(cosSensor);
+        sel.firstWi = -path.dir;
+        sel.pathLength = 1;
+        sel.irradiance = Le;
+        select_record<kDirect>(path, sel, outRec, pix);
+    }
+}
+
+// handleMiss (PathTracer.slang:1433-1524): a scatter ray that leaves the scene sees the environment
+// unless the previous vertex's light sample already covered it.
+template <bool kDirect>
+__device__ void handle_miss(const DevCtx& C, PState& path, const RecPlanes& outRec, uint32_t pix)
+{
+    if (path.vertex == 2) path.rec.secondaryPathJacobian = path.pdf * 1.f;
+    else if (path.vertex == 3) path.rec.secondaryPathJacobian *= path.pdf;
+    const EnvMapView& E = *C.env;
+    const bool isLightSamplable = !(path.flags & kPDelta);
+    const bool isLightSampled = (path.flags & (kPLightUpper | kPLightLower)) != 0;
+    if (!(E.present && (!isLightSampled || !isLightSamplable))) return;
+    float misWeight = 1.f;
+    float lightPdf = 0.f;
+    if (isLightSampled && isLightSamplable)
+    {
+        lightPdf = C.pEnvLight * env_eval_pdf(E, path.dir);
+        misWeight = dev_mis(C, path.totalPdf, lightPdf);
+    }
+    const f3 Le = env_eval(E, path.dir);
+    const f3 emitterRadiance = misWeight * Le;
+    if (cand_add_vertex(path, 1.f, path.earlyThroughput * path.thp * Le * misWeight))
+    {
+        Recon sel = path.rec;
+        sel.pathLength = path.vertex;
+        sel.lightIsNEE = false;
+        sel.lightIsDistant = true;
+        sel.lightPdf = lightPdf;
+        if (path.vertex == 2) sel.secondHit = hit_direction(path.dir);
+        if (path.vertex == 2 || path.vertex == 3) sel.irradiance = Le;
+        else sel.irradiance = path.thp * emitterRadiance;
+        select_record<kDirect>(path, sel, outRec, pix);
+    }
+}
+
 // One vertex of the tracePath loop (InitialCandidates.cs.slang:80-141): the next closest hit, then
-// handleHit, or handleMiss (PathTracer.slang:1433-1524, no environment map) which ends the path.
+// handleHit, or handlePrimaryMiss / handleMiss, which end the path.
 template <bool kDirect>
 __device__ __forceinline__ void path_step(const DevCtx& C, PState& path, const RecPlanes& currRec, uint32_t i)
 {
@@ -398,8 +489,8 @@ __device__ __forceinline__ void path_step(const DevCtx& C, PState& path, const R
     if (path.flags & kPHit) handle_hit<kDirect>(C, path, currRec, i);
     else
     {
-        if (path.vertex == 2) path.rec.secondaryPathJacobian = path.pdf * 1.f;
-        else if (path.vertex == 3) path.rec.secondaryPathJacobian *= path.pdf;
+        if (path.vertex == 1) handle_primary_miss<kDirect>(C, path, currRec, i);
+        else handle_miss<kDirect>(C, path, currRec, i);
         path.flags &= ~kPActive;
     }
 }
@@ -461,6 +552,24 @@ __global__ void __launch_bounds__(128, 8) k_candidates_direct(uint32_t slot, Res
     path_finish<true>(path, 0, 1, curr, currRec, i);
 }
 
+// ============================================================ environment-map importance
+// EnvMapSamplerSetup.cs.slang:48-76: one thread per texel of the 512 x 512 finest mip.
+__global__ void __launch_bounds__(256) k_env_importance(EnvMapView E, float* __restrict__ importance)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= kEnvImportanceDim * kEnvImportanceDim) return;
+    importance[i] = env_importance_texel(E, i % kEnvImportanceDim, i / kEnvImportanceDim);
+}
+
+// Mip m (>= 1) of the importance map from mip m - 1 (Texture::generateMips: 2 x 2 means).
+__global__ void __launch_bounds__(256) k_env_reduce(float* __restrict__ importance, uint32_t m)
+{
+    const uint32_t d = kEnvImportanceDim >> m;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d * d) return;
+    importance[env_mip_offset(m) + i] = env_importance_reduce(importance, m, i % d, i / d);
+}
+
 // ============================================================ forward reprojection (splat)
 // ReprojectTemporalSamples.rt.slang:64-175.  Writes the destination cell of every source pixel
 // and counts splats per cell; the cell lists are built by k_fill / k_rank_cells.
@@ -479,17 +588,29 @@ __global__ void __launch_bounds__(256, 4) k_reproject(uint32_t slot, ResPlanes p
         f2 lensSample = mk2(u2f(q0.z), u2f(q0.w));
         float time = u2f(q1.x);
         HitInfo firstHit; firstHit.w[0] = q2.x; firstHit.w[1] = q2.y; firstHit.w[2] = q2.z; firstHit.w[3] = q2.w;
-        if (hit_valid(firstHit))
+        const bool valid = hit_valid(firstHit);
+        // an environment sample (no primary hit) reprojects by its direction (:110-118)
+        if (valid || ((q1.y >> 14) & 1u))
         {
             CameraData cc; dev_orient(C, cc, time);
             f2 lensLocal = mk2(cc.apertureRadius * lensSample.x, cc.apertureRadius * lensSample.y);
             f3 lensWorld = cc.unitU * lensLocal.x + cc.unitV * lensLocal.y;
             Ray nr;
             nr.origin = cc.posW + lensWorld;
-            f3 x1 = dev_sd(C, firstHit, mk3(0.f)).posW;
-            nr.dir = normalize(x1 - nr.origin);
-            nr.tMin = 0.001f * length(x1 - nr.origin);
-            nr.tMax = 0.999f * length(x1 - nr.origin);
+            if (valid)
+            {
+                f3 x1 = dev_sd(C, firstHit, mk3(0.f)).posW;
+                nr.dir = normalize(x1 - nr.origin);
+                nr.tMin = 0.001f * length(x1 - nr.origin);
+                nr.tMax = 0.999f * length(x1 - nr.origin);
+            }
+            else
+            {
+                const uint4 q4 = __ldg(p + 4 * prevRec.stride);
+                nr.dir = -mk3(u2f(q4.x), u2f(q4.y), u2f(q4.z));
+                nr.tMin = 0.001f;
+                nr.tMax = kRayTMax;
+            }
             f3 camDir = mk3(dot(cc.unitU, nr.dir), dot(cc.unitV, nr.dir), dot(cc.unitW, nr.dir));
             if (camDir.z > 0.001f && dev_visible(C, nr))
             {
@@ -521,19 +642,28 @@ __global__ void __launch_bounds__(256) k_multi_reproject(uint32_t slot, ResPlane
     uint4 q1 = __ldg(p + prevRec.stride), q2 = __ldg(p + 2 * prevRec.stride);
     float time = u2f(q1.x);
     HitInfo firstHit; firstHit.w[0] = q2.x; firstHit.w[1] = q2.y; firstHit.w[2] = q2.z; firstHit.w[3] = q2.w;
-    if (!hit_valid(firstHit)) return;
+    const bool valid = hit_valid(firstHit);
+    // an environment sample (no primary hit) reprojects by its direction (:108-118)
+    if (!valid && !((q1.y >> 14) & 1u)) return;
     float fractionalTime = time / C.camera.shutterSpeed;
     float timePartitions = C.camera.shutterSpeed / (float)P;
-    f3 x1 = dev_sd(C, firstHit, mk3(0.f)).posW;
+    f3 x1 = mk3(0.f), envDir = mk3(0.f);
+    if (valid) x1 = dev_sd(C, firstHit, mk3(0.f)).posW;
+    else
+    {
+        const uint4 q4 = __ldg(p + 4 * prevRec.stride);
+        envDir = -mk3(u2f(q4.x), u2f(q4.y), u2f(q4.z));
+    }
     for (uint32_t i = 0; i < P; i++)
     {
         float newTime = (fractionalTime + (float)i) * timePartitions;
         CameraData cc; dev_orient(C, cc, newTime);
-        f3 rayDir = x1 - cc.posW;
+        f3 rayDir = valid ? x1 - cc.posW : envDir;
+        const float rayLength = valid ? 0.999f : kRayTMax;
         f3 nd = normalize(rayDir);
         float d = dot(nd, cc.unitW);
         if (d <= 0.001f) continue;
-        if (!dev_visible(C, mk_ray(cc.posW, rayDir, 0.001f, 0.999f))) continue;
+        if (!dev_visible(C, mk_ray(cc.posW, rayDir, 0.001f, rayLength))) continue;
         float tanFovY = cc.focalLength == 0.f ? 0.f : cc.frameHeight / cc.focalLength;
         d *= tanFovY;
         f2 offset = mk2(dot(nd, cc.unitU), -dot(nd, cc.unitV));

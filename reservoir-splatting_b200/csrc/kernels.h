@@ -12,6 +12,8 @@ cudaError_t ray_stats_take(unsigned long long out[2], cudaStream_t s);
 #endif
 __global__ void k_candidates(uint32_t slot, ResPlanes curr, RecPlanes currRec);
 __global__ void k_candidates_direct(uint32_t slot, ResPlanes curr, RecPlanes currRec);
+__global__ void k_env_importance(EnvMapView E, float* importance);
+__global__ void k_env_reduce(float* importance, uint32_t m);
 __global__ void k_reproject(uint32_t slot, ResPlanes prev, RecPlanes prevRec, uint32_t* targets, uint32_t* counts);
 __global__ void k_multi_reproject(uint32_t slot, ResPlanes prev, RecPlanes prevRec, uint32_t* targets, uint32_t* counts);
 __global__ void k_scan_tiles(const uint32_t* in, uint32_t* out, uint32_t* tileSums, uint32_t n);

@@ -8,6 +8,7 @@
 // so a frame can be captured into a CUDA graph after the first call.
 #include <algorithm>
 #include <cstdio>
+#include <cmath>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -110,6 +111,10 @@ struct rs_pass
     DevBuf<LightTriangle> dLights;
     DevBuf<u2> dAlias;
     bool hasScene = false;
+    // environment map: texels, importance mips and the view the kernels read (present = 0 without one)
+    DevBuf<float> envTexels, envImportance;
+    DevBuf<EnvMapView> envView;
+    EnvMapView envHost = {};
     // frame state
     uint32_t W = 0, H = 0;
     uint32_t frameCount = 0, seed = 0;
@@ -344,6 +349,8 @@ extern "C" RS_API rs_status rs_create(const rs_options* opts, rs_pass** out)
     p->opt = *opts;
     s = allocate(p.get());
     if (s != RS_OK) return s;
+    RS_CUDA(p->envView.ensure(1));
+    RS_CUDA(cudaMemcpy(p->envView.p, &p->envHost, sizeof(EnvMapView), cudaMemcpyHostToDevice));
     *out = p.release();
     return RS_OK;
 }
@@ -401,6 +408,44 @@ extern "C" RS_API rs_status rs_set_scene(rs_pass* p, const rs_scene_desc* sd)
     p->hostTriStale = false;
     p->geometryMoved = false;
     p->frameCount = 0; // setScene resets the frame count (ReservoirSplatting.cpp:380)
+    return RS_OK;
+}
+
+extern "C" RS_API rs_status rs_set_env_map(rs_pass* p, const rs_env_map* m)
+{
+    if (!p) return fail(RS_INVALID_ARG, "pass is NULL");
+    EnvMapView v = {};
+    if (m && m->width > 0)
+    {
+        if (!m->texels || m->height == 0) return fail(RS_INVALID_ARG, "env map texels are NULL or its height is 0");
+        if (m->width > 16384 || m->height > 16384) return fail(RS_INVALID_ARG, "env map larger than 16384 x 16384");
+        if (!(m->intensity >= 0.f) || !std::isfinite(m->intensity)) return fail(RS_INVALID_ARG, "env map intensity must be finite and >= 0");
+        for (int k = 0; k < 3; k++)
+            if (!std::isfinite(m->tint[k]) || !std::isfinite(m->rotation[k])) return fail(RS_INVALID_ARG, "env map tint and rotation must be finite");
+        const size_t texels = (size_t)m->width * m->height;
+        RS_CUDA(cudaDeviceSynchronize());
+        RS_CUDA(p->envTexels.ensure(4 * texels));
+        RS_CUDA(p->envImportance.ensure(kEnvImportanceTexels));
+        RS_CUDA(cudaMemcpy(p->envTexels.p, m->texels, 16 * texels, cudaMemcpyHostToDevice));
+        v.texels = p->envTexels.p;
+        v.importance = p->envImportance.p;
+        v.w = m->width; v.h = m->height;
+        v.present = m->intensity > 0.f ? 1u : 0u;
+        env_transform(m->rotation, v.toWorld, v.toLocal);
+        for (int k = 0; k < 3; k++) v.scale[k] = m->intensity * m->tint[k];
+        // the importance map (EnvMapSampler::createImportanceMap), then its mips
+        k_env_importance<<<kEnvImportanceDim * kEnvImportanceDim / 256, 256>>>(v, p->envImportance.p);
+        for (uint32_t mip = 1; mip < kEnvImportanceMips; mip++)
+        {
+            const uint32_t d = kEnvImportanceDim >> mip;
+            k_env_reduce<<<(d * d + 255) / 256, 256>>>(p->envImportance.p, mip);
+        }
+        RS_CUDA(cudaGetLastError());
+        RS_CUDA(cudaDeviceSynchronize());
+    }
+    else RS_CUDA(cudaDeviceSynchronize());
+    p->envHost = v;
+    RS_CUDA(cudaMemcpy(p->envView.p, &p->envHost, sizeof(EnvMapView), cudaMemcpyHostToDevice));
     return RS_OK;
 }
 
@@ -494,6 +539,8 @@ static void begin_frame(rs_pass* p, const rs_frame_desc* f)
     C.lights.aliasTable = p->dAlias.p;
     C.lights.count = (uint32_t)p->scene.lights.size();
     C.lights.invWeightsSum = p->scene.invWeightsSum;
+    C.env = p->envView.p;
+    light_type_probabilities(p->envHost.present != 0, C.lights.count > 0, C.pEnvLight, C.pEmissiveLight);
     C.camera = p->camera;
     C.prevCamera = p->havePrevCamera ? p->prevCamera : p->camera;
     C.cm = p->cm;
@@ -964,6 +1011,9 @@ extern "C" RS_API rs_status rs_get_buffer(rs_pass* p, rs_buffer_id id, void* dst
     case RS_BUF_FLOATING_COORDS: return copy_out(p, p->floatingCoords.p, N * 8, dst, bytes);
     case RS_BUF_MVEC: return copy_out(p, p->mvec.p, N * 8, dst, bytes);
     case RS_BUF_VBUFFER: return copy_out(p, p->vbuffer.p, N * 16, dst, bytes);
+    case RS_BUF_ENV_IMPORTANCE:
+        if (!p->envHost.importance) return fail(RS_NOT_READY, "no env map set");
+        return copy_out(p, p->envImportance.p, kEnvImportanceTexels * 4ull, dst, bytes);
     default: return fail(RS_INVALID_ARG, "unknown buffer id");
     }
 }
@@ -1138,6 +1188,7 @@ extern "C" RS_API rs_status rs_backward(rs_pass* p, const void* checkpoint, cons
     if (!p->hasScene || !p->haveFrameCtx) return fail(RS_NOT_READY, "rs_backward needs a rendered frame");
     if (p->opt.maxSurfaceBounces > 1)
         return fail(RS_INVALID_ARG, "rs_backward replays paths of at most three vertices: set maxSurfaceBounces <= 1");
+    if (p->envHost.present) return fail(RS_INVALID_ARG, "rs_backward differentiates scenes lit by emissive triangles; the pass has an env map");
     for (const MaterialData& m : p->scene.materials)
         if (m.flags & kMtlSpecGloss)
             return fail(RS_INVALID_ARG, "rs_backward differentiates metal-rough materials; the scene has a spec-gloss material");

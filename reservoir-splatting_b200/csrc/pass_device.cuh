@@ -8,6 +8,7 @@
 #include "bvh.cuh"
 #include "core/camera.h"
 #include "core/lights.h"
+#include "core/envmap.h"
 
 namespace rs {
 
@@ -21,6 +22,8 @@ struct DevCtx
     const float4* prevTri; // the previous frame's triangles (scene order; bvh.tri when nothing moved)
     const MaterialData* materials;
     LightView lights;
+    const EnvMapView* env;  // environment map (present = 0 without one), in device memory
+    float pEnvLight, pEmissiveLight; // light-type selection probabilities (PathTracer.slang:606-622)
     CameraData camera;      // gScene.camera of this frame
     CameraData prevCamera;  // previous frame's camera (motion vectors)
     CameraManager cm;
@@ -396,7 +399,17 @@ __device__ inline Shifted dev_gather_lens_copy(const DevCtx& C, SampleGen sg, co
     sp.firstRayDir = path.dir;
     sp.fractionalPixel = fractionalPixel;
     sp.lensSample = lensSample;
-    if (!isHit || hitEnvMap) return shifted_default();
+    if (isHit && hitEnvMap) return shifted_default(); // expected the environment, met geometry
+    if (!isHit)
+    {
+        if (!hitEnvMap) return shifted_default();      // expected geometry, saw the environment
+        sp.radiance = env_reconnection(*C.env, path.dir);
+        float cosSensor = dot(camDir, path.dir);
+        sp.subPixelJacobian = 1.f / f_abs(f_pow3(cosSensor));
+        float d0 = cam.lenW / dot(camDir, path.dir);
+        sp.lensVertexJacobian = (d0 * d0) / f_abs(cosSensor);
+        return sp;
+    }
     {
         ShadingData firstSd = dev_sd(C, path.hit, path.dir);
         f3 x1 = firstSd.posW;
@@ -419,7 +432,7 @@ __device__ inline Shifted dev_gather_lens_copy(const DevCtx& C, SampleGen sg, co
 __device__ inline Shifted dev_gather_primary_reconnect(const DevCtx& C, SampleGen sg, const Recon& rd, float time, f2 fractionalPixel, const HitInfo& primaryHit)
 {
     const bool hitEnvMap = (rd.pathLength == 1 && rd.lightIsDistant);
-    if (hitEnvMap || !hit_valid(primaryHit)) return shifted_default();
+    if (!hitEnvMap && !hit_valid(primaryHit)) return shifted_default();
     CameraData cam; dev_orient(C, cam, time);
     f2 p = mk2(fractionalPixel.x / (float)C.W, fractionalPixel.y / (float)C.H);
     f2 ndc = mk2(2.f * p.x + -1.f, -2.f * p.y + 1.f);
@@ -427,20 +440,31 @@ __device__ inline Shifted dev_gather_primary_reconnect(const DevCtx& C, SampleGe
     ShiftPath path;
     path.thp = mk3(1.f);
     path.active = true;
-    ShadingData sd = dev_sd(C, primaryHit, mk3(0.f));
-    f3 x1 = sd.posW, n = sd.faceN;
-    path.dir = normalize(x1 - filmWorld);
+    f3 x1, n;
+    if (hitEnvMap)
+    {
+        path.dir = -rd.firstWi;
+        x1 = filmWorld + path.dir;
+        n = mk3(0.f);
+    }
+    else
+    {
+        ShadingData sd = dev_sd(C, primaryHit, mk3(0.f));
+        x1 = sd.posW; n = sd.faceN;
+        path.dir = normalize(x1 - filmWorld);
+    }
     f3 camDir = cam.unitW;
     float camZ = dot(x1 - cam.posW, camDir);
     float rayT = camZ / dot(path.dir, camDir);
     path.origin = x1 - path.dir * rayT;
-    path.dir = normalize(x1 - path.origin);
+    if (!hitEnvMap) path.dir = normalize(x1 - path.origin);
     f3 lensOffsetWorld = path.origin - cam.posW;
     f2 lensLocalNormalized = mk2(dot(lensOffsetWorld, cam.unitU) / cam.apertureRadius,
                                  dot(lensOffsetWorld, cam.unitV) / cam.apertureRadius);
     if (length(lensLocalNormalized) > 1.f) return shifted_default();
     float dist = length(x1 - path.origin);
-    if (!dev_visible(C, mk_ray(path.origin, path.dir, 0.001f * dist, 0.999f * dist))) return shifted_default();
+    const float rayMin = hitEnvMap ? 0.001f : 0.001f * dist, rayMax = hitEnvMap ? kRayTMax : 0.999f * dist;
+    if (!dev_visible(C, mk_ray(path.origin, path.dir, rayMin, rayMax))) return shifted_default();
     Shifted sp = shifted_default();
     sp.firstRayDir = path.dir;
     sp.fractionalPixel = fractionalPixel;
@@ -448,6 +472,15 @@ __device__ inline Shifted dev_gather_primary_reconnect(const DevCtx& C, SampleGe
     sp.primaryHit = primaryHit;
     (void)sampleNext1D(sg);
     path.hit = primaryHit;
+    if (hitEnvMap)
+    {
+        sp.radiance = env_reconnection(*C.env, path.dir);
+        float cosSensor = dot(camDir, path.dir);
+        sp.subPixelJacobian = 1.f / f_abs(f_pow3(cosSensor));
+        float d0 = cam.lenW / dot(camDir, path.dir);
+        sp.lensVertexJacobian = (d0 * d0) / f_abs(dot(camDir, path.dir));
+        return sp;
+    }
     {
         float dist2 = length(x1 - path.origin);
         float distSquared = dist2 * dist2;
@@ -467,7 +500,7 @@ __device__ inline Shifted dev_gather_primary_reconnect(const DevCtx& C, SampleGe
 __device__ inline Shifted dev_scatter_shift(const DevCtx& C, SampleGen sg, const Recon& rd, float time, const HitInfo& primaryHit, f2 lensSample, bool skipVisibilityCheck)
 {
     const bool hitEnvMap = (rd.pathLength == 1) && rd.lightIsDistant;
-    if (hitEnvMap || !hit_valid(primaryHit)) return shifted_default();
+    if (!hitEnvMap && !hit_valid(primaryHit)) return shifted_default();
     CameraData cam; dev_orient(C, cam, time);
     f2 lensLocal = mk2(cam.apertureRadius * lensSample.x, cam.apertureRadius * lensSample.y);
     f3 camU = cam.unitU;
@@ -476,9 +509,14 @@ __device__ inline Shifted dev_scatter_shift(const DevCtx& C, SampleGen sg, const
     path.thp = mk3(1.f);
     path.active = true;
     path.origin = cam.posW + (camU * lensLocal.x + camV * lensLocal.y);
-    ShadingData firstSd = dev_sd(C, primaryHit, mk3(0.f));
-    f3 x1 = firstSd.posW, n = firstSd.faceN;
-    path.dir = normalize(x1 - path.origin);
+    f3 x1 = mk3(0.f), n = mk3(0.f);
+    if (hitEnvMap) path.dir = -rd.firstWi;
+    else
+    {
+        ShadingData firstSd = dev_sd(C, primaryHit, mk3(0.f));
+        x1 = firstSd.posW; n = firstSd.faceN;
+        path.dir = normalize(x1 - path.origin);
+    }
     f3 camDir = cam.unitW;
     f3 camRay = mk3(dot(camU, path.dir), dot(camV, path.dir), dot(camDir, path.dir));
     if (camRay.z <= 0.001f) return shifted_default();
@@ -490,7 +528,7 @@ __device__ inline Shifted dev_scatter_shift(const DevCtx& C, SampleGen sg, const
     float dist = length(x1 - path.origin);
     // the camera -> x1 test (occluded: the shift fails) and the reconnection's x1 -> x2 test are
     // traced in that order after the rest of the shift, when only their outcomes are left to apply
-    const Ray camVis = mk_ray(path.origin, path.dir, 0.001f, 0.999f * dist);
+    const Ray camVis = mk_ray(path.origin, path.dir, 0.001f, hitEnvMap ? kRayTMax : 0.999f * dist);
     Shifted sp = shifted_default();
     sp.lensSample = lensSample;
     sp.firstRayDir = path.dir;
@@ -498,6 +536,16 @@ __device__ inline Shifted dev_scatter_shift(const DevCtx& C, SampleGen sg, const
     sp.primaryHit = primaryHit;
     (void)sampleNext1D(sg);
     path.hit = primaryHit;
+    if (hitEnvMap)
+    {
+        sp.radiance = env_reconnection(*C.env, path.dir);
+        float cosSensor = dot(camDir, path.dir);
+        sp.subPixelJacobian = 1.f / f_abs(f_pow3(cosSensor));
+        float d0 = cam.lenW / dot(camDir, path.dir);
+        sp.lensVertexJacobian = (d0 * d0) / f_abs(cosSensor);
+        if (!skipVisibilityCheck && !dev_visible(C, camVis)) return shifted_default();
+        return sp;
+    }
     {
         float distSquared = dist * dist;
         float cosNormal = dot(-path.dir, n);

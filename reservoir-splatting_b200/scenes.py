@@ -325,3 +325,26 @@ def translate_camera(frame: int, width: int, height: int, step: float = 0.05) ->
     f = 0.5 * 24.0 / math.tan(0.5 * math.radians(45.0))
     return Camera((-20.0 + step * frame, 18.0, 40.0), (-20.0 + step * frame, 2.0, 0.0), focal_length=f,
                   aspect_ratio=width / height, far_z=10000.0)
+
+
+def sky_env_map(width: int = 256, height: int = 128, seed: int = 0, sun_dir=(0.4, 0.6, -0.5), sun_radiance: float = 40.0,
+                sun_radius_deg: float = 6.0) -> np.ndarray:
+    """A seeded lat-long sky float32 [height, width, 3] in the layout rs_set_env_map reads (row 0 at
+    the top, u = 0.5 looking along -z): a blue-to-white gradient above the horizon, dim ground below,
+    a bright sun disc around `sun_dir`, and a little seeded per-texel noise so the importance map is
+    not smooth."""
+    rng = np.random.default_rng(seed)
+    v = (np.arange(height, dtype=np.float64) + 0.5) / height
+    u = (np.arange(width, dtype=np.float64) + 0.5) / width
+    theta = np.pi * v[:, None]                     # 0 = up
+    phi = np.pi * (2.0 * u[None, :] - 1.0)
+    d = np.stack([np.sin(theta) * np.sin(phi), np.cos(theta) * np.ones_like(phi), -np.sin(theta) * np.cos(phi)], -1)
+    up = d[..., 1]
+    sky = np.where(up[..., None] > 0, np.array([0.35, 0.55, 1.0]) * (1 - up[..., None]) + np.array([1.0, 1.0, 1.0]) * up[..., None],
+                   np.array([0.18, 0.16, 0.14]))
+    s = np.asarray(sun_dir, np.float64)
+    s = s / np.linalg.norm(s)
+    cosang = np.clip(d @ s, -1.0, 1.0)
+    sun = (cosang > math.cos(math.radians(sun_radius_deg)))[..., None] * sun_radiance * np.array([1.0, 0.9, 0.75])
+    img = sky + sun + rng.uniform(0.0, 0.05, (height, width, 3))
+    return img.astype(np.float32)
