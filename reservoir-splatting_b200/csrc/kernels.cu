@@ -151,7 +151,7 @@ __device__ __forceinline__ void next_hit(const DevCtx& C, PState& p) // PathTrac
 // kDirect (one sample per pixel): a selected candidate's record is written straight to the
 // output planes (outRec, pixel pix) instead of being carried in the path state; the output is the
 // same, and ~28 registers of long-lived state are freed.
-template <bool kDirect>
+template <bool kDirect, bool kEnv>
 __device__ void handle_hit(const DevCtx& C, PState& path, const RecPlanes& outRec, uint32_t pix)
 {
     const bool isPrimaryHit = path.vertex == 1;
@@ -198,7 +198,7 @@ __device__ void handle_hit(const DevCtx& C, PState& path, const RecPlanes& outRe
         float lightPdf = 0.f;
         if (haveLights && !isPrimaryHit && isLightSampled && isLightSamplable)
         {
-            lightPdf = C.pEmissiveLight * eval_emissive_pdf(C.lights, path.origin, sd.lightIndex, sd.posW, sd_oriented_face_normal(sd));
+            lightPdf = (kEnv ? C.pEmissiveLight : 1.f) * eval_emissive_pdf(C.lights, path.origin, sd.lightIndex, sd.posW, sd_oriented_face_normal(sd));
             misWeight = dev_mis(C, path.totalPdf, lightPdf);
         }
         bool selected = cand_add_vertex(path, 1.f, path.earlyThroughput * path.thp * d.emission * misWeight);
@@ -234,23 +234,26 @@ __device__ void handle_hit(const DevCtx& C, PState& path, const RecPlanes& outRe
         f3 lsLi = mk3(0.f), lsOrigin = mk3(0.f), lsDir = mk3(0.f);
         float lsPdf = 0.f, lsDistance = 0.f, selectionPdf = 0.f;
         bool sampled = false;
+        // without an env map p = {0, haveLights, 0} and the emissive sample's selection pdf is 1
+        const float pEnv = kEnv ? C.pEnvLight : 0.f;
+        const float pEmissive = kEnv ? C.pEmissiveLight : (haveLights ? 1.f : 0.f);
         float u = sampleNext1D(path.sg);
-        if (u < C.pEnvLight)
+        if (kEnv && u < pEnv)
         {
             // generateEnvMapSample (:516-534)
-            selectionPdf = C.pEnvLight;
+            selectionPdf = pEnv;
             lsEnv = true;
             f2 r2; r2.x = sampleNext1D(path.sg); r2.y = sampleNext1D(path.sg);
-            f3 envLe;
-            env_sample(*C.env, r2, lsDir, lsPdf, envLe);
-            lsLi = lsPdf > 0.f ? envLe / lsPdf : mk3(0.f);
+            const EnvSample es = dev_env_sample(C.env, r2);
+            lsDir = es.dir; lsPdf = es.pdf;
+            lsLi = lsPdf > 0.f ? es.Le / lsPdf : mk3(0.f);
             lsOrigin = computeRayOrigin(sd.posW, dot(sd.faceN, lsDir) >= 0.f ? sd.faceN : -sd.faceN);
             lsDistance = kRayTMax;
             sampled = any_gt0(lsLi);
         }
-        else if (u - C.pEnvLight < C.pEmissiveLight)
+        else if (u - pEnv < pEmissive)
         {
-            selectionPdf = C.pEmissiveLight;
+            selectionPdf = kEnv ? pEmissive : 1.f;
             if (sample_emissive_power(C.lights, sd.posW, path.sg, tls))
             {
                 lsLi = tls.pdf > 0.f ? tls.Le / tls.pdf : mk3(0.f);
@@ -426,9 +429,8 @@ __device__ __forceinline__ void select_record(PState& path, const Recon& sel, co
 template <bool kDirect>
 __device__ void handle_primary_miss(const DevCtx& C, PState& path, const RecPlanes& outRec, uint32_t pix)
 {
-    const EnvMapView& E = *C.env;
-    if (!E.present) return;
-    const f3 Le = env_eval(E, path.dir);
+    if (!C.env->present) return;
+    const f3 Le = dev_env_eval(C.env, path.dir);
     if (cand_add_vertex(path, 1.f, Le))
     {
         Recon sel = path.rec;
@@ -453,18 +455,17 @@ __device__ void handle_miss(const DevCtx& C, PState& path, const RecPlanes& outR
 {
     if (path.vertex == 2) path.rec.secondaryPathJacobian = path.pdf * 1.f;
     else if (path.vertex == 3) path.rec.secondaryPathJacobian *= path.pdf;
-    const EnvMapView& E = *C.env;
     const bool isLightSamplable = !(path.flags & kPDelta);
     const bool isLightSampled = (path.flags & (kPLightUpper | kPLightLower)) != 0;
-    if (!(E.present && (!isLightSampled || !isLightSamplable))) return;
+    if (!(C.env->present && (!isLightSampled || !isLightSamplable))) return;
     float misWeight = 1.f;
     float lightPdf = 0.f;
     if (isLightSampled && isLightSamplable)
     {
-        lightPdf = C.pEnvLight * env_eval_pdf(E, path.dir);
+        lightPdf = C.pEnvLight * dev_env_eval_pdf(C.env, path.dir);
         misWeight = dev_mis(C, path.totalPdf, lightPdf);
     }
-    const f3 Le = env_eval(E, path.dir);
+    const f3 Le = dev_env_eval(C.env, path.dir);
     const f3 emitterRadiance = misWeight * Le;
     if (cand_add_vertex(path, 1.f, path.earlyThroughput * path.thp * Le * misWeight))
     {
@@ -482,14 +483,19 @@ __device__ void handle_miss(const DevCtx& C, PState& path, const RecPlanes& outR
 
 // One vertex of the tracePath loop (InitialCandidates.cs.slang:80-141): the next closest hit, then
 // handleHit, or handlePrimaryMiss / handleMiss, which end the path.
-template <bool kDirect>
+template <bool kDirect, bool kEnv>
 __device__ __forceinline__ void path_step(const DevCtx& C, PState& path, const RecPlanes& currRec, uint32_t i)
 {
     next_hit(C, path);
-    if (path.flags & kPHit) handle_hit<kDirect>(C, path, currRec, i);
+    if (path.flags & kPHit) handle_hit<kDirect, kEnv>(C, path, currRec, i);
     else
     {
-        if (path.vertex == 1) handle_primary_miss<kDirect>(C, path, currRec, i);
+        if (!kEnv)
+        {
+            if (path.vertex == 2) path.rec.secondaryPathJacobian = path.pdf * 1.f;
+            else if (path.vertex == 3) path.rec.secondaryPathJacobian *= path.pdf;
+        }
+        else if (path.vertex == 1) handle_primary_miss<kDirect>(C, path, currRec, i);
         else handle_miss<kDirect>(C, path, currRec, i);
         path.flags &= ~kPActive;
     }
@@ -523,6 +529,7 @@ __device__ __forceinline__ void path_finish(PState& path, uint32_t sIdx, uint32_
 }
 
 // InitialCandidates.cs.slang:80-141, several samples per pixel: one thread runs the pixel's paths.
+template <bool kEnv>
 __global__ void __launch_bounds__(128, 3) k_candidates(uint32_t slot, ResPlanes curr, RecPlanes currRec)
 {
     const DevCtx& C = c_ctx[slot];
@@ -533,13 +540,14 @@ __global__ void __launch_bounds__(128, 3) k_candidates(uint32_t slot, ResPlanes 
     {
         PState path;
         path_init<false>(C, x, y, path);
-        do path_step<false>(C, path, currRec, i);
+        do path_step<false, kEnv>(C, path, currRec, i);
         while (path.flags & kPActive);
         path_finish<false>(path, sIdx, C.spp, curr, currRec, i);
     }
 }
 
 // One sample per pixel (the reference default): records go straight to the output planes.
+template <bool kEnv>
 __global__ void __launch_bounds__(128, 8) k_candidates_direct(uint32_t slot, ResPlanes curr, RecPlanes currRec)
 {
     const DevCtx& C = c_ctx[slot];
@@ -547,7 +555,7 @@ __global__ void __launch_bounds__(128, 8) k_candidates_direct(uint32_t slot, Res
     if (!tiled_pixel(C.W, C.H, i)) return;
     PState path;
     path_init<true>(C, i % C.W, i / C.W, path);
-    do path_step<true>(C, path, currRec, i);
+    do path_step<true, kEnv>(C, path, currRec, i);
     while (path.flags & kPActive);
     path_finish<true>(path, 0, 1, curr, currRec, i);
 }
@@ -944,6 +952,7 @@ __global__ void __launch_bounds__(128, 4) k_collect(uint32_t slot, const float2*
 // RobustReuseOptimization.rt.slang:63-89
 // One thread per (pixel, neighbour): the eight lens-copy shifts are independent (the generator
 // goes to the shift by value and is never advanced), so blockIdx.y is the neighbour k.
+template <bool kEnv>
 __global__ void __launch_bounds__(128, 10) k_robust(uint32_t slot, ResPlanes prev, RecPlanes prevRec, Shifted* __restrict__ shiftedPaths)
 {
     const DevCtx& C = c_ctx[slot];
@@ -960,7 +969,7 @@ __global__ void __launch_bounds__(128, 10) k_robust(uint32_t slot, ResPlanes pre
     if (!(neighborIsValid && canShift)) { shiftedPaths[8 * (size_t)idx + k] = shifted_default(); return; }
     Recon rd = load_rec(prevRec, idx);
     shiftedPaths[8 * (size_t)idx + k] =
-        dev_gather_lens_copy(C, sg, rd, rd.time + C.cm.artificialFrameTime, mk2((float)nx + pr.subPixel.x, (float)ny + pr.subPixel.y), rd.lensSample);
+        dev_gather_lens_copy<kEnv>(C, sg, rd, rd.time + C.cm.artificialFrameTime, mk2((float)nx + pr.subPixel.x, (float)ny + pr.subPixel.y), rd.lensSample);
 }
 
 // ============================================================ temporal resampling
@@ -990,6 +999,7 @@ __device__ __forceinline__ void write_color(float4* color, uint32_t i, const Res
 
 
 // GatherTemporalResampling.rt.slang:68-235
+template <bool kEnv>
 __global__ void __launch_bounds__(128, 6) k_gather_resample(uint32_t slot, const uint4* __restrict__ vbuffer, ResPlanes curr, RecPlanes currRec,
                                                          ResPlanes inter, RecPlanes interRec, const float2* __restrict__ floatingCoords,
                                                          float4* __restrict__ color)
@@ -1027,8 +1037,8 @@ __global__ void __launch_bounds__(128, 6) k_gather_resample(uint32_t slot, const
         {
             float m1 = luminance(cr.integrand) * (useConf ? cr.confidence : 1.f);
             currPHat = cr.integrand;
-            Shifted sc = lens ? dev_gather_lens_copy(C, sg, crd, crd.time + C.cm.artificialFrameTime, floatingCoord + cr.subPixel, crd.lensSample)
-                              : dev_gather_primary_reconnect(C, sg, crd, crd.time + C.cm.artificialFrameTime, floatingCoord + cr.subPixel, crd.firstHit);
+            Shifted sc = lens ? dev_gather_lens_copy<kEnv>(C, sg, crd, crd.time + C.cm.artificialFrameTime, floatingCoord + cr.subPixel, crd.lensSample)
+                              : dev_gather_primary_reconnect<kEnv>(C, sg, crd, crd.time + C.cm.artificialFrameTime, floatingCoord + cr.subPixel, crd.firstHit);
             float sj = lens ? sc.secondaryPathJacobian / crd.secondaryPathJacobian
                             : (sc.lensVertexJacobian * sc.secondaryPathJacobian) / (crd.lensVertexJacobian * crd.secondaryPathJacobian);
             float m2 = luminance(sc.radiance) * sj * (useConf ? pr.confidence : 1.f) * prob;
@@ -1042,8 +1052,8 @@ __global__ void __launch_bounds__(128, 6) k_gather_resample(uint32_t slot, const
         if (any_gt0(pr.integrand))
         {
             f2 fp = mk2((float)x + pr.subPixel.x, (float)y + pr.subPixel.y);
-            Shifted sp = lens ? dev_gather_lens_copy(C, sg, prd, prd.time, fp, prd.lensSample)
-                              : dev_gather_primary_reconnect(C, sg, prd, prd.time, fp, prd.firstHit);
+            Shifted sp = lens ? dev_gather_lens_copy<kEnv>(C, sg, prd, prd.time, fp, prd.lensSample)
+                              : dev_gather_primary_reconnect<kEnv>(C, sg, prd, prd.time, fp, prd.firstHit);
             sj = lens ? sp.secondaryPathJacobian / prd.secondaryPathJacobian
                       : (sp.lensVertexJacobian * sp.secondaryPathJacobian) / (prd.lensVertexJacobian * prd.secondaryPathJacobian);
             float m1 = luminance(sp.radiance) * sj * (useConf ? cr.confidence : 1.f);
@@ -1076,3 +1086,101 @@ __global__ void __launch_bounds__(256) k_resolve(uint32_t n, ResPlanes curr, flo
 // translation unit.
 #include "wavefront.cuh"
 #include "adjoint.cuh"
+
+namespace rs {
+
+// Launchers of both variants of the kernels that reach an environment-light branch: with
+// env = false the kernel carries none of it (the reference compiles its shaders with USE_ENV_LIGHT
+// 0 or 1 the same way).  They live beside the kernels so each launch finds its device code.
+void launch_k_candidates(bool env, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, ResPlanes curr, RecPlanes currRec)
+{
+    if (env) k_candidates<true><<<grid, block, 0, s>>>(slot, curr, currRec);
+    else k_candidates<false><<<grid, block, 0, s>>>(slot, curr, currRec);
+}
+void launch_k_candidates_direct(bool env, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, ResPlanes curr, RecPlanes currRec)
+{
+    if (env) k_candidates_direct<true><<<grid, block, 0, s>>>(slot, curr, currRec);
+    else k_candidates_direct<false><<<grid, block, 0, s>>>(slot, curr, currRec);
+}
+void launch_k_robust(bool env, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, ResPlanes prev, RecPlanes prevRec, Shifted* __restrict__ shiftedPaths)
+{
+    if (env) k_robust<true><<<grid, block, 0, s>>>(slot, prev, prevRec, shiftedPaths);
+    else k_robust<false><<<grid, block, 0, s>>>(slot, prev, prevRec, shiftedPaths);
+}
+void launch_k_gather_resample(bool env, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, const uint4* __restrict__ vbuffer, ResPlanes curr, RecPlanes currRec, ResPlanes inter, RecPlanes interRec, const float2* __restrict__ floatingCoords, float4* __restrict__ color)
+{
+    if (env) k_gather_resample<true><<<grid, block, 0, s>>>(slot, vbuffer, curr, currRec, inter, interRec, floatingCoords, color);
+    else k_gather_resample<false><<<grid, block, 0, s>>>(slot, vbuffer, curr, currRec, inter, interRec, floatingCoords, color);
+}
+void launch_k_so_curr(bool env, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, WaveCtx K)
+{
+    if (env) k_so_curr<true><<<grid, block, 0, s>>>(slot, K);
+    else k_so_curr<false><<<grid, block, 0, s>>>(slot, K);
+}
+void launch_k_so_splat(bool env, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, WaveCtx K)
+{
+    if (env) k_so_splat<true><<<grid, block, 0, s>>>(slot, K);
+    else k_so_splat<false><<<grid, block, 0, s>>>(slot, K);
+}
+void launch_k_go_curr(bool env, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, WaveCtx K)
+{
+    if (env) k_go_curr<true><<<grid, block, 0, s>>>(slot, K);
+    else k_go_curr<false><<<grid, block, 0, s>>>(slot, K);
+}
+void launch_k_go_prev(bool env, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, WaveCtx K)
+{
+    if (env) k_go_prev<true><<<grid, block, 0, s>>>(slot, K);
+    else k_go_prev<false><<<grid, block, 0, s>>>(slot, K);
+}
+void launch_k_ms_curr(bool env, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, MultiCtx M)
+{
+    if (env) k_ms_curr<true><<<grid, block, 0, s>>>(slot, M);
+    else k_ms_curr<false><<<grid, block, 0, s>>>(slot, M);
+}
+void launch_k_ms_splat(bool env, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, MultiCtx M)
+{
+    if (env) k_ms_splat<true><<<grid, block, 0, s>>>(slot, M);
+    else k_ms_splat<false><<<grid, block, 0, s>>>(slot, M);
+}
+void launch_k_sb_curr_scatter(bool env, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, WaveCtx K)
+{
+    if (env) k_sb_curr_scatter<true><<<grid, block, 0, s>>>(slot, K);
+    else k_sb_curr_scatter<false><<<grid, block, 0, s>>>(slot, K);
+}
+void launch_k_sb_curr_gather(bool env, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, WaveCtx K)
+{
+    if (env) k_sb_curr_gather<true><<<grid, block, 0, s>>>(slot, K);
+    else k_sb_curr_gather<false><<<grid, block, 0, s>>>(slot, K);
+}
+void launch_k_sb_backup_gather(bool env, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, WaveCtx K)
+{
+    if (env) k_sb_backup_gather<true><<<grid, block, 0, s>>>(slot, K);
+    else k_sb_backup_gather<false><<<grid, block, 0, s>>>(slot, K);
+}
+void launch_k_sb_backup_scatter(bool env, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, WaveCtx K)
+{
+    if (env) k_sb_backup_scatter<true><<<grid, block, 0, s>>>(slot, K);
+    else k_sb_backup_scatter<false><<<grid, block, 0, s>>>(slot, K);
+}
+void launch_k_sb_splat_scatter(bool env, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, WaveCtx K)
+{
+    if (env) k_sb_splat_scatter<true><<<grid, block, 0, s>>>(slot, K);
+    else k_sb_splat_scatter<false><<<grid, block, 0, s>>>(slot, K);
+}
+void launch_k_sb_splat_gather(bool env, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, WaveCtx K)
+{
+    if (env) k_sb_splat_gather<true><<<grid, block, 0, s>>>(slot, K);
+    else k_sb_splat_gather<false><<<grid, block, 0, s>>>(slot, K);
+}
+void launch_k_sp_central(bool env, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, SpatialCtx S)
+{
+    if (env) k_sp_central<true><<<grid, block, 0, s>>>(slot, S);
+    else k_sp_central<false><<<grid, block, 0, s>>>(slot, S);
+}
+void launch_k_sp_neighbor(bool env, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, SpatialCtx S)
+{
+    if (env) k_sp_neighbor<true><<<grid, block, 0, s>>>(slot, S);
+    else k_sp_neighbor<false><<<grid, block, 0, s>>>(slot, S);
+}
+
+} // namespace rs

@@ -10,8 +10,6 @@ __global__ void k_camera_table(uint32_t slot, CameraTable* table);
 #ifdef RS_RAY_STATS
 cudaError_t ray_stats_take(unsigned long long out[2], cudaStream_t s);
 #endif
-__global__ void k_candidates(uint32_t slot, ResPlanes curr, RecPlanes currRec);
-__global__ void k_candidates_direct(uint32_t slot, ResPlanes curr, RecPlanes currRec);
 __global__ void k_env_importance(EnvMapView E, float* importance);
 __global__ void k_env_reduce(float* importance, uint32_t m);
 __global__ void k_reproject(uint32_t slot, ResPlanes prev, RecPlanes prevRec, uint32_t* targets, uint32_t* counts);
@@ -24,9 +22,6 @@ __global__ void k_rank_cells(const uint32_t* targets, const uint32_t* offsets, c
                              uint32_t* sorted, uint32_t* sortedCell, uint32_t n);
 __global__ void k_collect(uint32_t slot, const float2* mvec, ResPlanes prev, RecPlanes prevRec, ResPlanes inter, RecPlanes interRec,
                           float2* floatingCoords, const Shifted* shiftedPaths);
-__global__ void k_robust(uint32_t slot, ResPlanes prev, RecPlanes prevRec, Shifted* shiftedPaths);
-__global__ void k_gather_resample(uint32_t slot, const uint4* vbuffer, ResPlanes curr, RecPlanes currRec, ResPlanes inter, RecPlanes interRec,
-                                  const float2* floatingCoords, float4* color);
 __global__ void k_resolve(uint32_t n, ResPlanes curr, float4* color);
 
 __global__ void k_backward(uint32_t slot, ResPlanes res, RecPlanes rec, const float4* gradColor, double* acc, uint32_t numMaterials,
@@ -81,14 +76,8 @@ struct MultiCtx
     float4* terms;                 // per splat: prevPHat.xyz, Jacobian
     float4* misSub;                // per splat: prevMIS, shifted sub-pixel.xy, 0
 };
-__global__ void k_so_curr(uint32_t slot, WaveCtx K);
-__global__ void k_so_splat(uint32_t slot, WaveCtx K);
 __global__ void k_so_combine(uint32_t slot, WaveCtx K, float4* color);
-__global__ void k_go_curr(uint32_t slot, WaveCtx K);
-__global__ void k_go_prev(uint32_t slot, WaveCtx K);
 __global__ void k_go_combine(uint32_t slot, WaveCtx K, float4* color);
-__global__ void k_ms_curr(uint32_t slot, MultiCtx M);
-__global__ void k_ms_splat(uint32_t slot, MultiCtx M);
 __global__ void k_ms_combine(uint32_t slot, MultiCtx M, float4* color);
 
 // Buffers of the wavefront spatial resampling (one iteration).
@@ -102,15 +91,29 @@ struct SpatialCtx
     float* m1; ShiftPlanes shift; float4* terms; float* nw;
 };
 
-__global__ void k_sb_curr_scatter(uint32_t slot, WaveCtx K);
-__global__ void k_sb_curr_gather(uint32_t slot, WaveCtx K);
-__global__ void k_sb_backup_gather(uint32_t slot, WaveCtx K);
-__global__ void k_sb_backup_scatter(uint32_t slot, WaveCtx K);
-__global__ void k_sb_splat_scatter(uint32_t slot, WaveCtx K);
-__global__ void k_sb_splat_gather(uint32_t slot, WaveCtx K);
 __global__ void k_sb_combine(uint32_t slot, WaveCtx K, float4* color);
-__global__ void k_sp_central(uint32_t slot, SpatialCtx S);
-__global__ void k_sp_neighbor(uint32_t slot, SpatialCtx S);
 __global__ void k_sp_combine(uint32_t slot, SpatialCtx S, float4* color);
+
+
+// The kernels that reach an environment-light branch are templates on it (kEnv), defined and
+// launched in kernels.cu: launch one of the two variants (env: the pass has an environment light).
+void launch_k_candidates(bool env, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, ResPlanes curr, RecPlanes currRec);
+void launch_k_candidates_direct(bool env, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, ResPlanes curr, RecPlanes currRec);
+void launch_k_robust(bool env, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, ResPlanes prev, RecPlanes prevRec, Shifted* __restrict__ shiftedPaths);
+void launch_k_gather_resample(bool env, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, const uint4* __restrict__ vbuffer, ResPlanes curr, RecPlanes currRec, ResPlanes inter, RecPlanes interRec, const float2* __restrict__ floatingCoords, float4* __restrict__ color);
+void launch_k_so_curr(bool env, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, WaveCtx K);
+void launch_k_so_splat(bool env, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, WaveCtx K);
+void launch_k_go_curr(bool env, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, WaveCtx K);
+void launch_k_go_prev(bool env, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, WaveCtx K);
+void launch_k_ms_curr(bool env, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, MultiCtx M);
+void launch_k_ms_splat(bool env, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, MultiCtx M);
+void launch_k_sb_curr_scatter(bool env, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, WaveCtx K);
+void launch_k_sb_curr_gather(bool env, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, WaveCtx K);
+void launch_k_sb_backup_gather(bool env, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, WaveCtx K);
+void launch_k_sb_backup_scatter(bool env, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, WaveCtx K);
+void launch_k_sb_splat_scatter(bool env, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, WaveCtx K);
+void launch_k_sb_splat_gather(bool env, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, WaveCtx K);
+void launch_k_sp_central(bool env, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, SpatialCtx S);
+void launch_k_sp_neighbor(bool env, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, SpatialCtx S);
 
 } // namespace rs

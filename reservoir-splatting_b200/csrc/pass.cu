@@ -584,12 +584,17 @@ static void end_frame(rs_pass* p)
     p->geometryMoved = false;
 }
 
+// Launches the variant of an env-dependent kernel for a pass with (env) or without an environment
+// light; the one without carries no env branches.
+#define RS_ENV_LAUNCH(env, kernel, grid, block, stream, ...) launch_##kernel(env, grid, block, stream, __VA_ARGS__)
+
 // Issues the frame's device work on `s`.  The frame context goes to the pass's constant-memory
 // slot by a stream-ordered copy from pinned memory: in graph mode from p->graphCtx (a replayed graph
 // reads the context current at replay time), otherwise from a ring entry that is not reused until
 // its copy has run.
 static rs_status enqueue_frame(rs_pass* p, cudaStream_t s, float4* colorDev, const float2* mvecIn, bool graphMode)
 {
+    const bool env = p->envHost.present != 0; // which variant of the env-dependent kernels runs
     const uint32_t W = p->W, H = p->H;
     const uint32_t N = W * H;
     const rs_options& o = p->opt;
@@ -642,8 +647,8 @@ static rs_status enqueue_frame(rs_pass* p, cudaStream_t s, float4* colorDev, con
     stage(p, "vbuffer", q[0]);
     k_vbuffer<<<tiled_blocks(W, H, 256), 256, 0, q[0]>>>(C, p->vbuffer.p, p->mvec.p); p->launches++;
     stage(p, "initialCandidates", q[1]);
-    if (o.samplesPerPixel == 1) k_candidates_direct<<<tiled_blocks(W, H, 128), 128, 0, q[1]>>>(C, curr.res(), curr.recp());
-    else k_candidates<<<grid(N, 128), 128, 0, q[1]>>>(C, curr.res(), curr.recp());
+    if (o.samplesPerPixel == 1) RS_ENV_LAUNCH(env, k_candidates_direct, tiled_blocks(W, H, 128), 128, q[1], C, curr.res(), curr.recp());
+    else RS_ENV_LAUNCH(env, k_candidates, grid(N, 128), 128, q[1], C, curr.res(), curr.recp());
     p->launches++;
     if (p->keepCandidates)
     {
@@ -657,7 +662,7 @@ static rs_status enqueue_frame(rs_pass* p, cudaStream_t s, float4* colorDev, con
         if (robust)
         {
             stage(p, "robustReuse", q[2]);
-            k_robust<<<dim3(tiled_blocks(W, H, 128), 8), 128, 0, q[2]>>>(C, prev.res(), prev.recp(), p->shiftedPaths.p); p->launches++;
+            RS_ENV_LAUNCH(env, k_robust, dim3(tiled_blocks(W, H, 128), 8), 128, q[2], C, prev.res(), prev.recp(), p->shiftedPaths.p); p->launches++;
         }
         if (o.temporalReuse == RS_SCATTER_ONLY || o.temporalReuse == RS_SCATTER_BACKUP)
         {
@@ -708,9 +713,9 @@ static rs_status enqueue_frame(rs_pass* p, cudaStream_t s, float4* colorDev, con
                 cudaStream_t q[2];
                 fork_streams(p, s, 2, q);
                 stage(p, "gatherCurrShift", q[0]);
-                k_go_curr<<<tiled_blocks(W, H, 128), 128, 0, q[0]>>>(C, K);
+                RS_ENV_LAUNCH(env, k_go_curr, tiled_blocks(W, H, 128), 128, q[0], C, K);
                 stage(p, "gatherPrevShift", q[1]);
-                k_go_prev<<<tiled_blocks(W, H, 128), 128, 0, q[1]>>>(C, K);
+                RS_ENV_LAUNCH(env, k_go_prev, tiled_blocks(W, H, 128), 128, q[1], C, K);
                 join_streams(p, s, 2);
                 stage(p, "gatherResample", s);
                 k_go_combine<<<tiled_blocks(W, H, 128), 128, 0, s>>>(C, K, temporalColor);
@@ -718,7 +723,7 @@ static rs_status enqueue_frame(rs_pass* p, cudaStream_t s, float4* colorDev, con
                 break;
             }
             stage(p, "gatherResample", s);
-            k_gather_resample<<<tiled_blocks(W, H, 128), 128, 0, s>>>(C, p->vbuffer.p, curr.res(), curr.recp(), p->inter.res(), p->inter.recp(), p->floatingCoords.p, temporalColor); p->launches++;
+            RS_ENV_LAUNCH(env, k_gather_resample, tiled_blocks(W, H, 128), 128, s, C, p->vbuffer.p, curr.res(), curr.recp(), p->inter.res(), p->inter.recp(), p->floatingCoords.p, temporalColor); p->launches++;
             break;
         case RS_SCATTER_ONLY:
         {
@@ -734,9 +739,9 @@ static rs_status enqueue_frame(rs_pass* p, cudaStream_t s, float4* colorDev, con
             cudaStream_t q[2];
             fork_streams(p, s, 2, q);
             stage(p, "scatterCurrShift", q[0]);
-            k_so_curr<<<tiled_blocks(W, H, 128), 128, 0, q[0]>>>(C, K);
+            RS_ENV_LAUNCH(env, k_so_curr, tiled_blocks(W, H, 128), 128, q[0], C, K);
             stage(p, "scatterSplatShift", q[1]);
-            k_so_splat<<<grid(N, 128), 128, 0, q[1]>>>(C, K);
+            RS_ENV_LAUNCH(env, k_so_splat, grid(N, 128), 128, q[1], C, K);
             join_streams(p, s, 2);
             stage(p, "scatterResample", s);
             k_so_combine<<<tiled_blocks(W, H, 128), 128, 0, s>>>(C, K, temporalColor);
@@ -770,20 +775,20 @@ static rs_status enqueue_frame(rs_pass* p, cudaStream_t s, float4* colorDev, con
             cudaStream_t q[4];
             fork_streams(p, s, 4, q);
             stage(p, "sbCurrScatter", q[0]);
-            k_sb_curr_scatter<<<tiled_blocks(W, H, 128), 128, 0, q[0]>>>(C, K);
+            RS_ENV_LAUNCH(env, k_sb_curr_scatter, tiled_blocks(W, H, 128), 128, q[0], C, K);
             stage(p, "sbCurrGather", q[1]);
-            k_sb_curr_gather<<<tiled_blocks(W, H, 128), 128, 0, q[1]>>>(C, K);
+            RS_ENV_LAUNCH(env, k_sb_curr_gather, tiled_blocks(W, H, 128), 128, q[1], C, K);
             stage(p, "sbBackupGather", q[2]);
-            k_sb_backup_gather<<<tiled_blocks(W, H, 128), 128, 0, q[2]>>>(C, K);
+            RS_ENV_LAUNCH(env, k_sb_backup_gather, tiled_blocks(W, H, 128), 128, q[2], C, K);
             stage(p, "sbSplatScatter", q[3]);
-            k_sb_splat_scatter<<<grid(N, 128), 128, 0, q[3]>>>(C, K);
+            RS_ENV_LAUNCH(env, k_sb_splat_scatter, grid(N, 128), 128, q[3], C, K);
             p->launches += 4;
             if (balance)
             {
                 stage(p, "sbBackupScatter", q[2]);
-                k_sb_backup_scatter<<<tiled_blocks(W, H, 128), 128, 0, q[2]>>>(C, K);
+                RS_ENV_LAUNCH(env, k_sb_backup_scatter, tiled_blocks(W, H, 128), 128, q[2], C, K);
                 stage(p, "sbSplatGather", q[3]);
-                k_sb_splat_gather<<<grid(N, 128), 128, 0, q[3]>>>(C, K);
+                RS_ENV_LAUNCH(env, k_sb_splat_gather, grid(N, 128), 128, q[3], C, K);
                 p->launches += 2;
             }
             join_streams(p, s, 4);
@@ -804,9 +809,9 @@ static rs_status enqueue_frame(rs_pass* p, cudaStream_t s, float4* colorDev, con
             cudaStream_t q[2];
             fork_streams(p, s, 2, q);
             stage(p, "multiCurrShift", q[0]);
-            k_ms_curr<<<tiled_blocks(W, H, 128), 128, 0, q[0]>>>(C, M);
+            RS_ENV_LAUNCH(env, k_ms_curr, tiled_blocks(W, H, 128), 128, q[0], C, M);
             stage(p, "multiSplatShift", q[1]);
-            k_ms_splat<<<grid(P * N, 128), 128, 0, q[1]>>>(C, M);
+            RS_ENV_LAUNCH(env, k_ms_splat, grid(P * N, 128), 128, q[1], C, M);
             join_streams(p, s, 2);
             stage(p, "multiScatterResample", s);
             k_ms_combine<<<tiled_blocks(W, H, 128), 128, 0, s>>>(C, M, temporalColor);
@@ -841,9 +846,9 @@ static rs_status enqueue_frame(rs_pass* p, cudaStream_t s, float4* colorDev, con
             cudaStream_t q[2];
             fork_streams(p, s, 2, q); // the two shift directions are independent
             stage(p, "spatialCentral", q[0]);
-            k_sp_central<<<dim3(tiled_blocks(W, H, 128), o.neighborCount), 128, 0, q[0]>>>(C, S);
+            RS_ENV_LAUNCH(env, k_sp_central, dim3(tiled_blocks(W, H, 128), o.neighborCount), 128, q[0], C, S);
             stage(p, "spatialNeighbor", q[1]);
-            k_sp_neighbor<<<dim3(tiled_blocks(W, H, 128), o.neighborCount), 128, 0, q[1]>>>(C, S);
+            RS_ENV_LAUNCH(env, k_sp_neighbor, dim3(tiled_blocks(W, H, 128), o.neighborCount), 128, q[1], C, S);
             join_streams(p, s, 2);
             stage(p, "spatialCombine", s);
             k_sp_combine<<<tiled_blocks(W, H, 128), 128, 0, s>>>(C, S, i + 1 == o.numSpatialIterations ? colorDev : nullptr);

@@ -68,6 +68,18 @@ __device__ __forceinline__ bool tiled_pixel(uint32_t W, uint32_t H, uint32_t& i)
 }
 
 __device__ __forceinline__ bool dev_visible(const DevCtx& C, const Ray& r) { return trace_visible(C.bvh, r, C.fault); }
+// The environment light's evaluation, pdf and sampling as calls: the kernels reach them only on
+// misses and env light samples, and inlined they would add their registers to every kernel's
+// triangle work.
+static __device__ __noinline__ f3 dev_env_eval(const EnvMapView* E, f3 dir) { return env_eval(*E, dir); }
+static __device__ __noinline__ float dev_env_eval_pdf(const EnvMapView* E, f3 dir) { return env_eval_pdf(*E, dir); }
+struct EnvSample { f3 dir; float pdf; f3 Le; };
+static __device__ __noinline__ EnvSample dev_env_sample(const EnvMapView* E, f2 rnd)
+{
+    EnvSample r;
+    env_sample(*E, rnd, r.dir, r.pdf, r.Le);
+    return r;
+}
 __device__ __forceinline__ ShadingData dev_sd(const DevCtx& C, const HitInfo& h, f3 rayDir)
 {
     return load_shading_data(reinterpret_cast<const f4*>(C.bvh.tri), C.materials, h, rayDir);
@@ -377,7 +389,82 @@ __device__ __forceinline__ f3 dev_primary_light(const DevCtx& C, const ShiftPath
     return dev_instance(C, sd).emission;
 }
 
+// The shifts' environment branch (ShiftMapping.slang:151-166, 259-269, 383-393): the map seen along
+// `dir` and the Jacobians of a primary vertex at infinity.
+struct EnvPrimary { f3 radiance; float subPixelJacobian, lensVertexJacobian; };
+static __device__ __noinline__ EnvPrimary dev_env_primary(const EnvMapView* E, f3 dir, f3 camDir, float lenW)
+{
+    EnvPrimary e;
+    e.radiance = env_reconnection(*E, dir);
+    const float cosSensor = dot(camDir, dir);
+    e.subPixelJacobian = 1.f / f_abs(f_pow3(cosSensor));
+    const float d0 = lenW / dot(camDir, dir);
+    e.lensVertexJacobian = (d0 * d0) / f_abs(cosSensor);
+    return e;
+}
+
+// gatherPrimaryHitReconnectionShift (ShiftMapping.slang:183-296) of an environment sample (a path
+// of length 1 to a distant light): the film ray along the sample's direction, out of the lens.
+static __device__ __noinline__ Shifted dev_gather_primary_reconnect_env(const DevCtx& C, SampleGen sg, f3 firstWi, float time, f2 fractionalPixel,
+                                                                          HitInfo primaryHit)
+{
+    CameraData cam; dev_orient(C, cam, time);
+    f2 p = mk2(fractionalPixel.x / (float)C.W, fractionalPixel.y / (float)C.H);
+    f2 ndc = mk2(2.f * p.x + -1.f, -2.f * p.y + 1.f);
+    f3 filmWorld = cam.posW + (cam.cameraU * ndc.x + cam.cameraV * ndc.y + cam.cameraW);
+    const f3 dir = -firstWi;
+    const f3 x1 = filmWorld + dir;
+    const f3 camDir = cam.unitW;
+    float camZ = dot(x1 - cam.posW, camDir);
+    float rayT = camZ / dot(dir, camDir);
+    const f3 origin = x1 - dir * rayT;
+    f3 lensOffsetWorld = origin - cam.posW;
+    f2 lensLocalNormalized = mk2(dot(lensOffsetWorld, cam.unitU) / cam.apertureRadius,
+                                 dot(lensOffsetWorld, cam.unitV) / cam.apertureRadius);
+    if (length(lensLocalNormalized) > 1.f) return shifted_default();
+    if (!dev_visible(C, mk_ray(origin, dir, 0.001f, kRayTMax))) return shifted_default();
+    Shifted sp = shifted_default();
+    sp.firstRayDir = dir;
+    sp.fractionalPixel = fractionalPixel;
+    sp.lensSample = lensLocalNormalized;
+    sp.primaryHit = primaryHit;
+    (void)sampleNext1D(sg);
+    const EnvPrimary e = dev_env_primary(C.env, dir, camDir, cam.lenW);
+    sp.radiance = e.radiance; sp.subPixelJacobian = e.subPixelJacobian; sp.lensVertexJacobian = e.lensVertexJacobian;
+    return sp;
+}
+
+// scatterReprojectionShift (ShiftMapping.slang:301-421) of an environment sample: the direction
+// reprojected through the camera at `time`, the camera ray tested to infinity.
+static __device__ __noinline__ Shifted dev_scatter_shift_env(const DevCtx& C, SampleGen sg, f3 firstWi, float time, HitInfo primaryHit, f2 lensSample,
+                                                               bool skipVisibilityCheck)
+{
+    CameraData cam; dev_orient(C, cam, time);
+    f2 lensLocal = mk2(cam.apertureRadius * lensSample.x, cam.apertureRadius * lensSample.y);
+    const f3 origin = cam.posW + (cam.unitU * lensLocal.x + cam.unitV * lensLocal.y);
+    const f3 dir = -firstWi;
+    const f3 camDir = cam.unitW;
+    f3 camRay = mk3(dot(cam.unitU, dir), dot(cam.unitV, dir), dot(camDir, dir));
+    if (camRay.z <= 0.001f) return shifted_default();
+    float lw = cam.lenW;
+    f2 film = mk2(lensLocal.x + lw * (camRay.x / camRay.z), lensLocal.y + lw * (camRay.y / camRay.z));
+    f2 ndc = mk2(film.x / cam.lenU, film.y / cam.lenV);
+    f2 nfp = mk2((0.5f * ndc.x + 0.5f) * (float)C.W, (-0.5f * ndc.y + 0.5f) * (float)C.H);
+    if (!valid_float(C, nfp)) return shifted_default();
+    if (!skipVisibilityCheck && !dev_visible(C, mk_ray(origin, dir, 0.001f, kRayTMax))) return shifted_default();
+    Shifted sp = shifted_default();
+    sp.lensSample = lensSample;
+    sp.firstRayDir = dir;
+    sp.fractionalPixel = nfp;
+    sp.primaryHit = primaryHit;
+    (void)sampleNext1D(sg);
+    const EnvPrimary e = dev_env_primary(C.env, dir, camDir, cam.lenW);
+    sp.radiance = e.radiance; sp.subPixelJacobian = e.subPixelJacobian; sp.lensVertexJacobian = e.lensVertexJacobian;
+    return sp;
+}
+
 // gatherLensVertexCopyShift (ShiftMapping.slang:90-180); `sg` is taken by value.
+template <bool kEnv>
 __device__ inline Shifted dev_gather_lens_copy(const DevCtx& C, SampleGen sg, const Recon& rd, float time, f2 fractionalPixel, f2 lensSample)
 {
     if (!valid_float(C, fractionalPixel)) return shifted_default();
@@ -399,15 +486,13 @@ __device__ inline Shifted dev_gather_lens_copy(const DevCtx& C, SampleGen sg, co
     sp.firstRayDir = path.dir;
     sp.fractionalPixel = fractionalPixel;
     sp.lensSample = lensSample;
-    if (isHit && hitEnvMap) return shifted_default(); // expected the environment, met geometry
-    if (!isHit)
+    if (!kEnv && (!isHit || hitEnvMap)) return shifted_default();
+    if (kEnv && isHit && hitEnvMap) return shifted_default(); // expected the environment, met geometry
+    if (kEnv && !isHit)
     {
         if (!hitEnvMap) return shifted_default();      // expected geometry, saw the environment
-        sp.radiance = env_reconnection(*C.env, path.dir);
-        float cosSensor = dot(camDir, path.dir);
-        sp.subPixelJacobian = 1.f / f_abs(f_pow3(cosSensor));
-        float d0 = cam.lenW / dot(camDir, path.dir);
-        sp.lensVertexJacobian = (d0 * d0) / f_abs(cosSensor);
+        const EnvPrimary e = dev_env_primary(C.env, path.dir, camDir, cam.lenW);
+        sp.radiance = e.radiance; sp.subPixelJacobian = e.subPixelJacobian; sp.lensVertexJacobian = e.lensVertexJacobian;
         return sp;
     }
     {
@@ -429,10 +514,12 @@ __device__ inline Shifted dev_gather_lens_copy(const DevCtx& C, SampleGen sg, co
 }
 
 // gatherPrimaryHitReconnectionShift (ShiftMapping.slang:183-296)
+template <bool kEnv>
 __device__ inline Shifted dev_gather_primary_reconnect(const DevCtx& C, SampleGen sg, const Recon& rd, float time, f2 fractionalPixel, const HitInfo& primaryHit)
 {
     const bool hitEnvMap = (rd.pathLength == 1 && rd.lightIsDistant);
-    if (!hitEnvMap && !hit_valid(primaryHit)) return shifted_default();
+    if (kEnv && hitEnvMap) return dev_gather_primary_reconnect_env(C, sg, rd.firstWi, time, fractionalPixel, primaryHit);
+    if (hitEnvMap || !hit_valid(primaryHit)) return shifted_default();
     CameraData cam; dev_orient(C, cam, time);
     f2 p = mk2(fractionalPixel.x / (float)C.W, fractionalPixel.y / (float)C.H);
     f2 ndc = mk2(2.f * p.x + -1.f, -2.f * p.y + 1.f);
@@ -440,31 +527,20 @@ __device__ inline Shifted dev_gather_primary_reconnect(const DevCtx& C, SampleGe
     ShiftPath path;
     path.thp = mk3(1.f);
     path.active = true;
-    f3 x1, n;
-    if (hitEnvMap)
-    {
-        path.dir = -rd.firstWi;
-        x1 = filmWorld + path.dir;
-        n = mk3(0.f);
-    }
-    else
-    {
-        ShadingData sd = dev_sd(C, primaryHit, mk3(0.f));
-        x1 = sd.posW; n = sd.faceN;
-        path.dir = normalize(x1 - filmWorld);
-    }
+    ShadingData sd = dev_sd(C, primaryHit, mk3(0.f));
+    f3 x1 = sd.posW, n = sd.faceN;
+    path.dir = normalize(x1 - filmWorld);
     f3 camDir = cam.unitW;
     float camZ = dot(x1 - cam.posW, camDir);
     float rayT = camZ / dot(path.dir, camDir);
     path.origin = x1 - path.dir * rayT;
-    if (!hitEnvMap) path.dir = normalize(x1 - path.origin);
+    path.dir = normalize(x1 - path.origin);
     f3 lensOffsetWorld = path.origin - cam.posW;
     f2 lensLocalNormalized = mk2(dot(lensOffsetWorld, cam.unitU) / cam.apertureRadius,
                                  dot(lensOffsetWorld, cam.unitV) / cam.apertureRadius);
     if (length(lensLocalNormalized) > 1.f) return shifted_default();
     float dist = length(x1 - path.origin);
-    const float rayMin = hitEnvMap ? 0.001f : 0.001f * dist, rayMax = hitEnvMap ? kRayTMax : 0.999f * dist;
-    if (!dev_visible(C, mk_ray(path.origin, path.dir, rayMin, rayMax))) return shifted_default();
+    if (!dev_visible(C, mk_ray(path.origin, path.dir, 0.001f * dist, 0.999f * dist))) return shifted_default();
     Shifted sp = shifted_default();
     sp.firstRayDir = path.dir;
     sp.fractionalPixel = fractionalPixel;
@@ -472,15 +548,6 @@ __device__ inline Shifted dev_gather_primary_reconnect(const DevCtx& C, SampleGe
     sp.primaryHit = primaryHit;
     (void)sampleNext1D(sg);
     path.hit = primaryHit;
-    if (hitEnvMap)
-    {
-        sp.radiance = env_reconnection(*C.env, path.dir);
-        float cosSensor = dot(camDir, path.dir);
-        sp.subPixelJacobian = 1.f / f_abs(f_pow3(cosSensor));
-        float d0 = cam.lenW / dot(camDir, path.dir);
-        sp.lensVertexJacobian = (d0 * d0) / f_abs(dot(camDir, path.dir));
-        return sp;
-    }
     {
         float dist2 = length(x1 - path.origin);
         float distSquared = dist2 * dist2;
@@ -497,10 +564,12 @@ __device__ inline Shifted dev_gather_primary_reconnect(const DevCtx& C, SampleGe
 }
 
 // scatterReprojectionShift (ShiftMapping.slang:301-421)
+template <bool kEnv>
 __device__ inline Shifted dev_scatter_shift(const DevCtx& C, SampleGen sg, const Recon& rd, float time, const HitInfo& primaryHit, f2 lensSample, bool skipVisibilityCheck)
 {
     const bool hitEnvMap = (rd.pathLength == 1) && rd.lightIsDistant;
-    if (!hitEnvMap && !hit_valid(primaryHit)) return shifted_default();
+    if (kEnv && hitEnvMap) return dev_scatter_shift_env(C, sg, rd.firstWi, time, primaryHit, lensSample, skipVisibilityCheck);
+    if (hitEnvMap || !hit_valid(primaryHit)) return shifted_default();
     CameraData cam; dev_orient(C, cam, time);
     f2 lensLocal = mk2(cam.apertureRadius * lensSample.x, cam.apertureRadius * lensSample.y);
     f3 camU = cam.unitU;
@@ -509,14 +578,9 @@ __device__ inline Shifted dev_scatter_shift(const DevCtx& C, SampleGen sg, const
     path.thp = mk3(1.f);
     path.active = true;
     path.origin = cam.posW + (camU * lensLocal.x + camV * lensLocal.y);
-    f3 x1 = mk3(0.f), n = mk3(0.f);
-    if (hitEnvMap) path.dir = -rd.firstWi;
-    else
-    {
-        ShadingData firstSd = dev_sd(C, primaryHit, mk3(0.f));
-        x1 = firstSd.posW; n = firstSd.faceN;
-        path.dir = normalize(x1 - path.origin);
-    }
+    ShadingData firstSd = dev_sd(C, primaryHit, mk3(0.f));
+    f3 x1 = firstSd.posW, n = firstSd.faceN;
+    path.dir = normalize(x1 - path.origin);
     f3 camDir = cam.unitW;
     f3 camRay = mk3(dot(camU, path.dir), dot(camV, path.dir), dot(camDir, path.dir));
     if (camRay.z <= 0.001f) return shifted_default();
@@ -528,7 +592,7 @@ __device__ inline Shifted dev_scatter_shift(const DevCtx& C, SampleGen sg, const
     float dist = length(x1 - path.origin);
     // the camera -> x1 test (occluded: the shift fails) and the reconnection's x1 -> x2 test are
     // traced in that order after the rest of the shift, when only their outcomes are left to apply
-    const Ray camVis = mk_ray(path.origin, path.dir, 0.001f, hitEnvMap ? kRayTMax : 0.999f * dist);
+    const Ray camVis = mk_ray(path.origin, path.dir, 0.001f, 0.999f * dist);
     Shifted sp = shifted_default();
     sp.lensSample = lensSample;
     sp.firstRayDir = path.dir;
@@ -536,16 +600,6 @@ __device__ inline Shifted dev_scatter_shift(const DevCtx& C, SampleGen sg, const
     sp.primaryHit = primaryHit;
     (void)sampleNext1D(sg);
     path.hit = primaryHit;
-    if (hitEnvMap)
-    {
-        sp.radiance = env_reconnection(*C.env, path.dir);
-        float cosSensor = dot(camDir, path.dir);
-        sp.subPixelJacobian = 1.f / f_abs(f_pow3(cosSensor));
-        float d0 = cam.lenW / dot(camDir, path.dir);
-        sp.lensVertexJacobian = (d0 * d0) / f_abs(cosSensor);
-        if (!skipVisibilityCheck && !dev_visible(C, camVis)) return shifted_default();
-        return sp;
-    }
     {
         float distSquared = dist * dist;
         float cosNormal = dot(-path.dir, n);

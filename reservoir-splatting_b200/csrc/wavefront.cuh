@@ -96,6 +96,7 @@ __device__ __forceinline__ Recon backup_rec(const WaveCtx& K, uint32_t bi)
 // thread per splat of the sorted cell lists) are stored; the combine walks each cell's splats in the
 // canonical order and replays the resampling draws.  Buffers: m2curr, splatShift / splatTerms
 // (prevPHat, Jacobian) / splatM (MIS weight, 0, shifted sub-pixel).
+template <bool kEnv>
 __global__ void __launch_bounds__(128, 8) k_so_curr(uint32_t slot, WaveCtx K)
 {
     const DevCtx& C = c_ctx[slot];
@@ -105,7 +106,7 @@ __global__ void __launch_bounds__(128, 8) k_so_curr(uint32_t slot, WaveCtx K)
     if (!any_gt0(integrand)) return;
     const Recon crd = load_rec(K.currRec, ri);
     SampleGen dummy = {0, C.sgKind};
-    Shifted sc = dev_scatter_shift(C, dummy, crd, crd.time + C.cm.artificialFrameTime, crd.firstHit, crd.lensSample, false);
+    Shifted sc = dev_scatter_shift<kEnv>(C, dummy, crd, crd.time + C.cm.artificialFrameTime, crd.firstHit, crd.lensSample, false);
     float sj = jac_scatter(sc, crd);
     float m2 = luminance(sc.radiance) * sj;
     m2 = f_isnan(m2) ? 0.f : m2;
@@ -115,6 +116,7 @@ __global__ void __launch_bounds__(128, 8) k_so_curr(uint32_t slot, WaveCtx K)
     K.m2curr[ri] = m2;
 }
 
+template <bool kEnv>
 __global__ void __launch_bounds__(128, 8) k_so_splat(uint32_t slot, WaveCtx K)
 {
     const DevCtx& C = c_ctx[slot];
@@ -126,7 +128,7 @@ __global__ void __launch_bounds__(128, 8) k_so_splat(uint32_t slot, WaveCtx K)
     const uint32_t cell = __ldg(&K.sortedCell[j]);
     const Recon prd = load_rec(K.prevRec, si);
     SampleGen dummy = {0, C.sgKind};
-    Shifted sp = dev_scatter_shift(C, dummy, prd, prd.time, prd.firstHit, prd.lensSample, false);
+    Shifted sp = dev_scatter_shift<kEnv>(C, dummy, prd, prd.time, prd.firstHit, prd.lensSample, false);
     store_shift(K.splatShift, j, sp);
     float sj = jac_scatter(sp, prd);
     const float m1 = luminance(sp.radiance) * sj * (C.useConfTemporal ? load_confidence(K.curr, cell) : 1.f);
@@ -196,6 +198,7 @@ __global__ void __launch_bounds__(128) k_so_combine(uint32_t slot, WaveCtx K, fl
 // into this pixel are independent kernels (their generator copies are never used), the combine
 // replays the pixel's two resampling draws.  Buffers: m2curr (the current sample's MIS term),
 // backupShift / backupTerms / backupM (the gathered sample's shift, prevPHat and Jacobian, MIS term).
+template <bool kEnv>
 __global__ void __launch_bounds__(128, 9) k_go_curr(uint32_t slot, WaveCtx K)
 {
     const DevCtx& C = c_ctx[slot];
@@ -207,12 +210,13 @@ __global__ void __launch_bounds__(128, 9) k_go_curr(uint32_t slot, WaveCtx K)
     const float2 fcv = __ldg(&K.floatingCoords[ri]);
     const Recon crd = load_rec(K.currRec, ri);
     SampleGen dummy = {0, C.sgKind};
-    Shifted sc = dev_gather_lens_copy(C, dummy, crd, crd.time + C.cm.artificialFrameTime, mk2(fcv.x, fcv.y) + cr.subPixel, crd.lensSample);
+    Shifted sc = dev_gather_lens_copy<kEnv>(C, dummy, crd, crd.time + C.cm.artificialFrameTime, mk2(fcv.x, fcv.y) + cr.subPixel, crd.lensSample);
     float sj = sc.secondaryPathJacobian / crd.secondaryPathJacobian;
     float m2 = luminance(sc.radiance) * sj * (C.useConfTemporal ? pr.confidence : 1.f) * 1.f;
     K.m2curr[ri] = f_isnan(m2) ? 0.f : m2;
 }
 
+template <bool kEnv>
 __global__ void __launch_bounds__(128, 9) k_go_prev(uint32_t slot, WaveCtx K)
 {
     const DevCtx& C = c_ctx[slot];
@@ -224,7 +228,7 @@ __global__ void __launch_bounds__(128, 9) k_go_prev(uint32_t slot, WaveCtx K)
     const Res cr = load_res(K.curr, ri);
     const Recon prd = load_rec(K.interRec, ri);
     SampleGen dummy = {0, C.sgKind};
-    Shifted sp = dev_gather_lens_copy(C, dummy, prd, prd.time, mk2((float)x + pr.subPixel.x, (float)y + pr.subPixel.y), prd.lensSample);
+    Shifted sp = dev_gather_lens_copy<kEnv>(C, dummy, prd, prd.time, mk2((float)x + pr.subPixel.x, (float)y + pr.subPixel.y), prd.lensSample);
     store_shift(K.backupShift, ri, sp);
     float sj = sp.secondaryPathJacobian / prd.secondaryPathJacobian;
     float m1 = luminance(sp.radiance) * sj * (C.useConfTemporal ? cr.confidence : 1.f);
@@ -280,6 +284,7 @@ __global__ void __launch_bounds__(128) k_go_combine(uint32_t slot, WaveCtx K, fl
 }
 
 // ---- stage 1: current sample -> previous domain by reprojection (ScatterBackup...:96-114)
+template <bool kEnv>
 __global__ void __launch_bounds__(128, 8) k_sb_curr_scatter(uint32_t slot, WaveCtx K)
 {
     const DevCtx& C = c_ctx[slot];
@@ -289,7 +294,7 @@ __global__ void __launch_bounds__(128, 8) k_sb_curr_scatter(uint32_t slot, WaveC
     if (!any_gt0(integrand)) return;
     Recon crd = load_rec_rw(K.currRec, ri);
     SampleGen dummy = {0, C.sgKind};
-    Shifted sc = dev_scatter_shift(C, dummy, crd, crd.time + C.cm.artificialFrameTime, crd.firstHit, crd.lensSample, false);
+    Shifted sc = dev_scatter_shift<kEnv>(C, dummy, crd, crd.time + C.cm.artificialFrameTime, crd.firstHit, crd.lensSample, false);
     float scj = jac_scatter(sc, crd);
     float m2 = luminance(sc.radiance) * scj;
     m2 = f_isnan(m2) ? 0.f : m2;
@@ -300,6 +305,7 @@ __global__ void __launch_bounds__(128, 8) k_sb_curr_scatter(uint32_t slot, WaveC
 }
 
 // ---- stage 1: current sample -> previous domain by the gather shift (:116-129)
+template <bool kEnv>
 __global__ void __launch_bounds__(128, 9) k_sb_curr_gather(uint32_t slot, WaveCtx K)
 {
     const DevCtx& C = c_ctx[slot];
@@ -315,7 +321,7 @@ __global__ void __launch_bounds__(128, 9) k_sb_curr_gather(uint32_t slot, WaveCt
     {
         Recon crd = load_rec_rw(K.currRec, ri);
         SampleGen dummy = {0, C.sgKind};
-        Shifted gc = dev_gather_lens_copy(C, dummy, crd, crd.time + C.cm.artificialFrameTime, fc + cr.subPixel, crd.lensSample);
+        Shifted gc = dev_gather_lens_copy<kEnv>(C, dummy, crd, crd.time + C.cm.artificialFrameTime, fc + cr.subPixel, crd.lensSample);
         float gj = gc.secondaryPathJacobian / crd.secondaryPathJacobian;
         m3 = luminance(gc.radiance) * gj * 0.5f * (C.useConfTemporal ? br.confidence : 1.f);
     }
@@ -324,6 +330,7 @@ __global__ void __launch_bounds__(128, 9) k_sb_curr_gather(uint32_t slot, WaveCt
 }
 
 // ---- stage 1: backup sample -> current domain (:156-166)
+template <bool kEnv>
 __global__ void __launch_bounds__(128, 9) k_sb_backup_gather(uint32_t slot, WaveCtx K)
 {
     const DevCtx& C = c_ctx[slot];
@@ -335,7 +342,7 @@ __global__ void __launch_bounds__(128, 9) k_sb_backup_gather(uint32_t slot, Wave
     if (!any_gt0(br.integrand)) return;
     Recon brd = backup_rec(K, bi);
     SampleGen dummy = {0, C.sgKind};
-    Shifted sb = dev_gather_lens_copy(C, dummy, brd, brd.time, mk2((float)x + br.subPixel.x, (float)y + br.subPixel.y), brd.lensSample);
+    Shifted sb = dev_gather_lens_copy<kEnv>(C, dummy, brd, brd.time, mk2((float)x + br.subPixel.x, (float)y + br.subPixel.y), brd.lensSample);
     store_shift(K.backupShift, ri, sb);
     float sj = sb.secondaryPathJacobian / brd.secondaryPathJacobian;
     float currConf = load_confidence(K.curr, ri);
@@ -348,6 +355,7 @@ __global__ void __launch_bounds__(128, 9) k_sb_backup_gather(uint32_t slot, Wave
 }
 
 // ---- stage 2 (Balance): updated backup -> previous domain by reprojection (:171-189)
+template <bool kEnv>
 __global__ void __launch_bounds__(128, 8) k_sb_backup_scatter(uint32_t slot, WaveCtx K)
 {
     const DevCtx& C = c_ctx[slot];
@@ -362,7 +370,7 @@ __global__ void __launch_bounds__(128, 8) k_sb_backup_scatter(uint32_t slot, Wav
     recon_update(brd, sb);
     float sj = __ldg(&K.backupTerms[ri]).w;
     SampleGen dummy = {0, C.sgKind};
-    Shifted ss = dev_scatter_shift(C, dummy, brd, brd.time + C.cm.artificialFrameTime, brd.firstHit, brd.lensSample, false);
+    Shifted ss = dev_scatter_shift<kEnv>(C, dummy, brd, brd.time + C.cm.artificialFrameTime, brd.firstHit, brd.lensSample, false);
     float scj = jac_scatter(ss, brd);
     float m2 = luminance(ss.radiance) * scj * sj;
     m2 = f_isnan(m2) ? 0.f : m2;
@@ -373,6 +381,7 @@ __global__ void __launch_bounds__(128, 8) k_sb_backup_scatter(uint32_t slot, Wav
 }
 
 // ---- stage 1: splatted previous sample -> current domain (:218-235), one thread per splat
+template <bool kEnv>
 __global__ void __launch_bounds__(128, 9) k_sb_splat_scatter(uint32_t slot, WaveCtx K)
 {
     const DevCtx& C = c_ctx[slot];
@@ -384,7 +393,7 @@ __global__ void __launch_bounds__(128, 9) k_sb_splat_scatter(uint32_t slot, Wave
     if (!any_gt0(integrand)) return;
     Recon prd = load_rec(K.prevRec, si);
     SampleGen dummy = {0, C.sgKind};
-    Shifted sp = dev_scatter_shift(C, dummy, prd, prd.time, prd.firstHit, prd.lensSample, true);
+    Shifted sp = dev_scatter_shift<kEnv>(C, dummy, prd, prd.time, prd.firstHit, prd.lensSample, true);
     store_shift(K.splatShift, j, sp);
     float scj = jac_scatter(sp, prd);
     float m1 = luminance(sp.radiance) * scj * (C.useConfTemporal ? load_confidence(K.curr, cell) : 1.f);
@@ -396,6 +405,7 @@ __global__ void __launch_bounds__(128, 9) k_sb_splat_scatter(uint32_t slot, Wave
 }
 
 // ---- stage 2 (Balance): updated splat -> previous domain by the gather shift (:237-253)
+template <bool kEnv>
 __global__ void __launch_bounds__(128, 9) k_sb_splat_gather(uint32_t slot, WaveCtx K)
 {
     const DevCtx& C = c_ctx[slot];
@@ -418,7 +428,7 @@ __global__ void __launch_bounds__(128, 9) k_sb_splat_gather(uint32_t slot, WaveC
         recon_update(prd, sp);
         float scj = __ldg(&K.splatTerms[j]).w;
         SampleGen dummy = {0, C.sgKind};
-        Shifted gp = dev_gather_lens_copy(C, dummy, prd, prd.time + C.cm.artificialFrameTime, fp, prd.lensSample);
+        Shifted gp = dev_gather_lens_copy<kEnv>(C, dummy, prd, prd.time + C.cm.artificialFrameTime, fp, prd.lensSample);
         float gj = gp.secondaryPathJacobian / prd.secondaryPathJacobian;
         m3 = luminance(gp.radiance) * gj * scj * 0.5f * (C.useConfTemporal ? br.confidence : 1.f);
     }
@@ -555,6 +565,7 @@ __device__ __forceinline__ bool spatial_neighbor(const DevCtx& C, uint32_t itera
     return valid_int(C, nx, ny);
 }
 
+template <bool kEnv>
 __global__ void __launch_bounds__(128, 10) k_sp_central(uint32_t slot, SpatialCtx S)
 {
     const DevCtx& C = c_ctx[slot];
@@ -576,8 +587,8 @@ __global__ void __launch_bounds__(128, 10) k_sp_central(uint32_t slot, SpatialCt
         uint32_t ni = (uint32_t)ny * C.W + (uint32_t)nx;
         f2 fp = mk2((float)nx + cent.subPixel.x, (float)ny + cent.subPixel.y);
         SampleGen dummy = {0, C.sgKind};
-        Shifted sc = lensCopy ? dev_gather_lens_copy(C, dummy, centR, centR.time, fp, centR.lensSample)
-                              : dev_gather_primary_reconnect(C, dummy, centR, centR.time, fp, centR.firstHit);
+        Shifted sc = lensCopy ? dev_gather_lens_copy<kEnv>(C, dummy, centR, centR.time, fp, centR.lensSample)
+                              : dev_gather_primary_reconnect<kEnv>(C, dummy, centR, centR.time, fp, centR.firstHit);
         float sj = (lensCopy ? 1.f : (sc.lensVertexJacobian / centR.lensVertexJacobian)) * (sc.secondaryPathJacobian / centR.secondaryPathJacobian);
         m1 = luminance(sc.radiance) * sj * (C.useConfSpatial ? load_confidence(S.src, ni) : 1.f);
         m1 = f_isnan(m1) ? 0.f : m1;
@@ -585,6 +596,7 @@ __global__ void __launch_bounds__(128, 10) k_sp_central(uint32_t slot, SpatialCt
     S.m1[t] = m1;
 }
 
+template <bool kEnv>
 __global__ void __launch_bounds__(128, 9) k_sp_neighbor(uint32_t slot, SpatialCtx S)
 {
     const DevCtx& C = c_ctx[slot];
@@ -604,8 +616,8 @@ __global__ void __launch_bounds__(128, 9) k_sp_neighbor(uint32_t slot, SpatialCt
     Recon nrd = load_rec(S.srcRec, ni);
     f2 fp = mk2((float)x + nr.subPixel.x, (float)y + nr.subPixel.y);
     SampleGen dummy = {0, C.sgKind};
-    Shifted sn = lensCopy ? dev_gather_lens_copy(C, dummy, nrd, nrd.time, fp, nrd.lensSample)
-                          : dev_gather_primary_reconnect(C, dummy, nrd, nrd.time, fp, nrd.firstHit);
+    Shifted sn = lensCopy ? dev_gather_lens_copy<kEnv>(C, dummy, nrd, nrd.time, fp, nrd.lensSample)
+                          : dev_gather_primary_reconnect<kEnv>(C, dummy, nrd, nrd.time, fp, nrd.firstHit);
     store_shift(S.shift, t, sn);
     float sj = (lensCopy ? 1.f : (sn.lensVertexJacobian / nrd.lensVertexJacobian)) * (sn.secondaryPathJacobian / nrd.secondaryPathJacobian);
     float nw = luminance(sn.radiance) * sj * (C.useConfSpatial ? load_confidence(S.src, ri) : 1.f);
@@ -691,6 +703,7 @@ __global__ void __launch_bounds__(128) k_sp_combine(uint32_t slot, SpatialCtx S,
 // rebuilds only the selected record.
 
 // The current sample's scatter shift for its MIS weight (:96-117).
+template <bool kEnv>
 __global__ void __launch_bounds__(128, 8) k_ms_curr(uint32_t slot, MultiCtx M)
 {
     const DevCtx& C = c_ctx[slot];
@@ -708,7 +721,7 @@ __global__ void __launch_bounds__(128, 8) k_ms_curr(uint32_t slot, MultiCtx M)
         float fractionalTime = (crd.time - f_floor(crd.time / timePartitions) * timePartitions) / timePartitions;
         float shiftedTime = fractionalTime * C.camera.shutterSpeed;
         SampleGen dummy = {0, C.sgKind};
-        Shifted sc = dev_scatter_shift(C, dummy, crd, shiftedTime + C.cm.artificialFrameTime, crd.firstHit, crd.lensSample, false);
+        Shifted sc = dev_scatter_shift<kEnv>(C, dummy, crd, shiftedTime + C.cm.artificialFrameTime, crd.firstHit, crd.lensSample, false);
         float sj = jac_scatter(sc, crd);
         float m2 = luminance(sc.radiance) * sj;
         m2 = f_isnan(m2) ? 0.f : m2;
@@ -721,6 +734,7 @@ __global__ void __launch_bounds__(128, 8) k_ms_curr(uint32_t slot, MultiCtx M)
 }
 
 // One splat of partition j (sorted position g = j * N + k) shifted to its partition's time (:124-160).
+template <bool kEnv>
 __global__ void __launch_bounds__(128, 8) k_ms_splat(uint32_t slot, MultiCtx M)
 {
     const DevCtx& C = c_ctx[slot];
@@ -742,7 +756,7 @@ __global__ void __launch_bounds__(128, 8) k_ms_splat(uint32_t slot, MultiCtx M)
         float fractionalTime = prd.time / C.camera.shutterSpeed;
         float newTime = (fractionalTime + (float)j) * timePartitions;
         SampleGen dummy = {0, C.sgKind};
-        Shifted sp = dev_scatter_shift(C, dummy, prd, newTime, prd.firstHit, prd.lensSample, false);
+        Shifted sp = dev_scatter_shift<kEnv>(C, dummy, prd, newTime, prd.firstHit, prd.lensSample, false);
         store_shift(M.shift, g, sp);
         sj = jac_scatter(sp, prd);
         float m1 = luminance(sp.radiance) * sj * (useConf ? load_confidence(M.curr, cell) : 1.f);
