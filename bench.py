@@ -339,6 +339,8 @@ MODE_PROPS = {
     "MultiScatter-P4-shutter-1/24": {"temporalReuse": "MultiScatter", "numTimePartitions": 4, "artificialFrameTime": 1.0 / 48.0},
 }
 MODE_SHUTTER = {"MultiScatter-P4-shutter-1/24": 1.0 / 24.0}
+# modes rendered under the seeded sky environment map as well as the scene's emissive triangles
+MODE_ENV = {"ScatterBackup-Clamped-Balance+sky": {"temporalReuse": "ScatterBackup", "gatherOption": "Clamped"}}
 
 
 def run_modes(args, torch, rs, scene, stream):
@@ -348,9 +350,14 @@ def run_modes(args, torch, rs, scene, stream):
     W, H = W_FULL, H_FULL
     color = torch.empty((H, W, 4), dtype=torch.float32, device="cuda")
     out = {}
-    for name, props in MODE_PROPS.items():
+    sky = None
+    for name, props in list(MODE_PROPS.items()) + list(MODE_ENV.items()):
         p = rs.ReservoirSplatting(dict(props, maxSurfaceBounces=2, enableSpatialResampling=True), W, H)
         p.set_scene(scene)
+        if name in MODE_ENV:
+            import reservoir_splatting_b200.scenes as S
+            sky = sky if sky is not None else S.sky_env_map(1024, 512, seed=0)
+            p.set_env_map(sky)
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
         def cam(f):
@@ -371,7 +378,8 @@ def run_modes(args, torch, rs, scene, stream):
         p.close()
     out["how"] = (f"1920x1080, the benchmark scene and orbit, path length 4, spatial reuse on; {args.mode_frames} frames "
                   "after 4 warm-up frames per mode, CUDA events on the launching stream; MultiScatter with shutter 1/24 s and "
-                  "artificial frame time 1/48 s on the static scene")
+                  "artificial frame time 1/48 s on the static scene; '+sky' adds a seeded 1024x512 sky environment light (NEE picks "
+                  "sky or emissive triangles with probability 1/2 each)")
     return out
 
 

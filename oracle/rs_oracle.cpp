@@ -1217,7 +1217,8 @@ struct Pass
                 else
                 {
                     vbuffer[idx] = hit_none();
-                    mvec[idx] = mk2(0.f, 0.f);
+                    // writeMiss (VBufferRT.slang:128-149)
+                    mvec[idx] = env.present ? env_miss_motion_vector(camera, pc, dir, p) : mk2(0.f, 0.f);
                 }
             }
     }

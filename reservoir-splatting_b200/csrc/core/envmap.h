@@ -18,6 +18,7 @@
 // so host and device agree bit for bit.
 #pragma once
 #include "geom.h"
+#include "camera.h"
 
 namespace rs {
 
@@ -201,6 +202,19 @@ RS_HD float env_eval_pdf(const EnvMapView& E, f3 dir)
     const float avg = E.importance[env_mip_offset(kEnvImportanceMips - 1)];
     const float pdf = E.importance[(uint32_t)fy * kEnvImportanceDim + (uint32_t)fx] / avg;
     return pdf * (1.f / k4Pi);
+}
+
+// Motion vector of a primary miss when the environment light is on (VBufferRT.slang:128-149): the
+// ray direction projected through the previous frame's camera basis, with this frame's focal
+// length, frame height and aspect ratio; p is the pixel centre in [0,1]^2.
+RS_HD f2 env_miss_motion_vector(const CameraData& cam, const CameraData& prev, f3 rayDir, f2 p)
+{
+    float d = dot(rayDir, normalize(prev.cameraW));
+    const float tanFovY = cam.focalLength == 0.f ? 0.f : cam.frameHeight / cam.focalLength;
+    d *= tanFovY;
+    const f2 offset = mk2(dot(rayDir, normalize(prev.cameraU)), -dot(rayDir, normalize(prev.cameraV)));
+    const f2 newNDC = mk2(0.5f + offset.x / (d * cam.aspectRatio), 0.5f + offset.y / d);
+    return mk2(newNDC.x - p.x, newNDC.y - p.y);
 }
 
 // EnvMap transform from XYZ Euler angles in degrees (EnvMap::setRotation, EnvMap.cpp:60-72, with

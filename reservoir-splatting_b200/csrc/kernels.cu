@@ -50,7 +50,9 @@ __global__ void __launch_bounds__(256) k_vbuffer(uint32_t slot, uint4* __restric
     else
     {
         vbuffer[i] = make_uint4(0u, 0u, 0u, 0u);
-        mvec[i] = make_float2(0.f, 0.f);
+        f2 mv = mk2(0.f, 0.f);
+        if (C.env->present) mv = env_miss_motion_vector(cam, pc, dir, p); // writeMiss (VBufferRT.slang:128-149)
+        mvec[i] = make_float2(mv.x, mv.y);
     }
 }
 
