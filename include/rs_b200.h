@@ -295,10 +295,15 @@ typedef struct rs_tonemap_options {
     uint32_t clamp;
     float whiteMaxLuminance;    /* ReinhardModified */
     float whiteScale;           /* HableUc2 */
+    uint32_t whiteBalance;      /* colour grading: white balance to whitePoint (ToneMapper.cpp:530-536) */
+    float whitePoint;           /* Kelvin, 1905 .. 25000 (default 6500: identity) */
 } rs_tonemap_options;
 
 RS_API void rs_tonemap_default_options(rs_tonemap_options* options);
 RS_API size_t rs_tonemap_workspace_bytes(void);
+/* The 3x3 colour transform rs_tonemap applies after auto exposure (row-major, out[9]): the white
+ * balance matrix times the exposure scale (ToneMapper::updateColorTransform).  Host only. */
+RS_API rs_status rs_tonemap_color_transform(const rs_tonemap_options* options, float* out9);
 RS_API rs_status rs_tonemap(const void* colorDev, uint32_t width, uint32_t height, const rs_tonemap_options* options, void* rgba8Dev,
                             void* workspaceDev, void* cudaStream);
 

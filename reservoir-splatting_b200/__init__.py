@@ -60,6 +60,7 @@ def load_library():
     lib.rs_tonemap_workspace_bytes.argtypes = []
     lib.rs_tonemap_workspace_bytes.restype = C.c_size_t
     lib.rs_tonemap.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.POINTER(abi.RsTonemapOptions), C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.rs_tonemap_color_transform.argtypes = [C.POINTER(abi.RsTonemapOptions), C.c_void_p]
     lib.rs_last_launch_count.argtypes = [C.c_void_p]
     lib.rs_last_launch_count.restype = C.c_uint32
     lib.rs_last_error_string.restype = C.c_char_p
@@ -82,7 +83,7 @@ def load_library():
                  "rs_freeze", "rs_get_buffer", "rs_set_buffer", "rs_enable_stage_timing", "rs_get_stage_times",
                  "rs_debug_keep_candidates", "rs_batch_create", "rs_batch_execute", "rs_batch_destroy",
                  "rs_build_cell_lists_static", "rs_set_materials", "rs_checkpoint_bytes", "rs_checkpoint", "rs_backward",
-                 "rs_backward_stats", "rs_debug_trace_rays", "rs_debug_bvh_shape", "rs_debug_stage_rays", "rs_tonemap",
+                 "rs_backward_stats", "rs_debug_trace_rays", "rs_debug_bvh_shape", "rs_debug_stage_rays", "rs_tonemap", "rs_tonemap_color_transform",
                  "rs_set_bvh_builder",
                  "rs_update_geometry"):
         getattr(lib, name).restype = C.c_int

@@ -90,7 +90,7 @@ TONEMAP_OPERATOR = {"Linear": 0, "Reinhard": 1, "ReinhardModified": 2, "HejiHabl
 class RsTonemapOptions(C.Structure):
     _fields_ = [("op", C.c_uint32), ("exposureCompensation", C.c_float), ("autoExposure", C.c_uint32), ("filmSpeed", C.c_float),
                 ("fNumber", C.c_float), ("shutter", C.c_float), ("clamp", C.c_uint32), ("whiteMaxLuminance", C.c_float),
-                ("whiteScale", C.c_float)]
+                ("whiteScale", C.c_float), ("whiteBalance", C.c_uint32), ("whitePoint", C.c_float)]
 
 
 def default_options(width: int = 1920, height: int = 1080) -> RsOptions:

@@ -34,6 +34,16 @@ def tonemap_options(**kw) -> abi.RsTonemapOptions:
     return o
 
 
+def color_transform(options: abi.RsTonemapOptions) -> "np.ndarray":
+    """The 3x3 colour transform rs_tonemap applies (white balance times exposure), float32 [3, 3]."""
+    from . import load_library
+    m = (C.c_float * 9)()
+    st = load_library().rs_tonemap_color_transform(C.byref(options), m)
+    if st != 0:
+        raise ValueError("invalid tone mapper options")
+    return np.array(m[:], np.float32).reshape(3, 3)
+
+
 def tonemap(color, width: int, height: int, options: abi.RsTonemapOptions | None = None, out=None, stream: int = 0):
     """RGBA8 (uint8 [H, W, 4], CUDA) of a float4 [H, W, 4] CUDA colour tensor; `out` may be given."""
     import torch

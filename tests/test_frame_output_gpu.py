@@ -27,7 +27,7 @@ def uc2(x):
     return ((x * (A * x + C * B) + D * E) / (x * (A * x + B) + D * F)) - (E / F)
 
 
-def reference(color, op, clamp=True, auto=False, comp=0.0, film=100.0, fnum=1.0, shutter=1.0, wml=1.0, ws=11.2):
+def reference(color, op, clamp=True, auto=False, comp=0.0, film=100.0, fnum=1.0, shutter=1.0, wml=1.0, ws=11.2, matrix=None):
     f = np.float32
     c = color[..., :3].astype(f)
     with np.errstate(all="ignore"):
@@ -38,7 +38,11 @@ def reference(color, op, clamp=True, auto=False, comp=0.0, film=100.0, fnum=1.0,
         scale = f(2.0 ** comp)
         if not auto:
             scale = scale * (f(0.01) * f(film)) / (f(shutter) * f(fnum) * f(fnum))
-        c = c * scale
+        if matrix is None:
+            c = c * scale
+        else:  # the colour grading transform (white balance times exposure), applied in float32
+            m = matrix.astype(f)
+            c = (c[..., 0:1] * m[:, 0] + c[..., 1:2] * m[:, 1] + c[..., 2:3] * m[:, 2]).astype(f)
         if op == "Reinhard":
             l = lum(c)[..., None]
             c = c * ((l / (l + 1)) / l)
@@ -90,6 +94,25 @@ def test_tonemap_matches_the_shader(rs, op, clamp, auto, comp):
     ref = reference(img, op, clamp, auto, comp, film=200.0, fnum=1.4, shutter=2.0)
     diff = np.abs(out - ref)
     assert diff.max() <= 1, (op, np.argwhere(diff > 1)[:3].tolist())
+    assert (diff > 0).mean() < 0.01
+
+
+@pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
+@pytest.mark.parametrize("kelvin", [2500.0, 6500.0, 12000.0])
+def test_white_balance_matches_the_shader(rs, kelvin):
+    """ToneMapping.ps.slang:157-158: the white balance matrix (times exposure) before the operator."""
+    import torch
+    import reservoir_splatting_b200.frame_output as FO
+    img = _image(seed=3)
+    img[0, :8, :3] = np.abs(img[0, :8, :3])  # keep the matrix product free of NaN and inf rows
+    img[0, 3, :3] = 5.0
+    h, w = img.shape[:2]
+    o = FO.tonemap_options(op="Aces", whiteBalance=1, whitePoint=kelvin, exposureCompensation=0.5)
+    m = FO.color_transform(o)
+    out = FO.tonemap(torch.from_numpy(img).cuda(), w, h, o).cpu().numpy().astype(np.int32)
+    ref = reference(img, "Aces", comp=0.5, matrix=m)
+    diff = np.abs(out - ref)
+    assert diff.max() <= 1
     assert (diff > 0).mean() < 0.01
 
 
