@@ -20,7 +20,7 @@ from pathlib import Path
 
 import numpy as np
 
-from .scenes import Scene, spec_gloss_material
+from .scenes import Scene, material, spec_gloss_material
 
 
 def spec_power_to_roughness(ns: float) -> float:
@@ -134,3 +134,445 @@ def save_obj(scene: Scene, path, material_names=None, mtl_params=None):
             lines.append("v " + " ".join(repr(float(x)) for x in t[3 * k:3 * k + 3]))
         lines.append("f -3 -2 -1")
     path.write_text("\n".join(lines) + "\n")
+
+
+# ---------------------------------------------------------------------------------------- PBRT v4
+# A subset of the reference's PBRT importer (Source/plugins/importers/PBRTImporter: Parser.cpp for
+# the syntax, PBRTImporter.cpp for the conversion to StandardMaterials, the path without PBRT
+# materials):
+#   * the transform stack (Identity, Translate, Scale, Rotate, LookAt, ConcatTransform, Transform,
+#     AttributeBegin/End, ReverseOrientation), Camera "perspective", WorldBegin, Include/Import,
+#     ObjectBegin/End/ObjectInstance (flattened);
+#   * Shape "trianglemesh", "bilinearmesh", "sphere" (tessellated) and "plymesh" (ascii or binary
+#     little-endian PLY, polygons fan-triangulated);
+#   * materials by the StandardMaterial mapping of PBRTImporter.cpp:992-1175: diffuse (base =
+#     reflectance, roughness 1), coateddiffuse (roughness sqrt of the scalar roughness), conductor and
+#     coatedconductor (metallic, base = the Fresnel reflectance at normal incidence of eta, k or the
+#     given reflectance), dielectric (IoR eta; the pass has no transmission lobe, so only its
+#     reflection remains); the scalar roughness is getRoughness (:424-462) as written: float2(u + v),
+#     square-rooted when remaproughness, and getScalarRoughness averages the two equal components;
+#   * AreaLightSource "diffuse" (L * scale emitted by the shapes that follow, twosided);
+#   * LightSource "infinite" with a constant "rgb L" (an environment map of that radiance).
+# Textures, named spectra other than the defaults, image infinite lights, curves, disks and
+# cylinders are not read.
+
+_PBRT_COPPER_F0 = (0.955, 0.638, 0.538)  # RGB normal-incidence reflectance used for the default conductor (metal-Cu)
+
+
+def _pbrt_tokens(text: str):
+    i, n = 0, len(text)
+    while i < n:
+        c = text[i]
+        if c.isspace():
+            i += 1
+        elif c == "#":
+            while i < n and text[i] != "\n":
+                i += 1
+        elif c in "[]":
+            yield c
+            i += 1
+        elif c == '"':
+            j = text.index('"', i + 1)
+            yield text[i:j + 1]
+            i = j + 1
+        else:
+            j = i
+            while j < n and not text[j].isspace() and text[j] not in '[]"#':
+                j += 1
+            yield text[i:j]
+            i = j
+
+
+def _pbrt_value(tok: str):
+    if tok.startswith('"'):
+        return tok[1:-1]
+    if tok in ("true", "false"):
+        return tok == "true"
+    return float(tok)
+
+
+class _PbrtReader:
+    def __init__(self, tokens):
+        self.toks = list(tokens)
+        self.i = 0
+
+    def more(self):
+        return self.i < len(self.toks)
+
+    def next(self):
+        t = self.toks[self.i]
+        self.i += 1
+        return t
+
+    def peek(self):
+        return self.toks[self.i] if self.more() else None
+
+    def numbers(self, k):
+        out = []
+        if self.peek() == "[":
+            self.next()
+            while self.peek() != "]":
+                out.append(float(self.next()))
+            self.next()
+        else:
+            for _ in range(k):
+                out.append(float(self.next()))
+        return out
+
+    def params(self):
+        """The "type name" value lists after a directive's positional arguments."""
+        ps = {}
+        while self.more() and self.peek().startswith('"'):
+            decl = self.next()[1:-1].split()
+            if len(decl) != 2:
+                self.i -= 1
+                break
+            ptype, pname = decl
+            if self.peek() == "[":
+                self.next()
+                vals = []
+                while self.peek() != "]":
+                    vals.append(_pbrt_value(self.next()))
+                self.next()
+            else:
+                vals = [_pbrt_value(self.next())]
+            ps[pname] = (ptype, vals)
+        return ps
+
+
+def _rotate(deg, axis):
+    a = np.asarray(axis, np.float64)
+    a = a / np.linalg.norm(a)
+    s, c = math.sin(math.radians(deg)), math.cos(math.radians(deg))
+    x, y, z = a
+    m = np.eye(4)
+    m[:3, :3] = [[x * x + (1 - x * x) * c, x * y * (1 - c) - z * s, x * z * (1 - c) + y * s],
+                 [x * y * (1 - c) + z * s, y * y + (1 - y * y) * c, y * z * (1 - c) - x * s],
+                 [x * z * (1 - c) - y * s, y * z * (1 - c) + x * s, z * z + (1 - z * z) * c]]
+    return m
+
+
+def _look_at(eye, look, up):
+    """World-to-camera matrix of PBRT's LookAt (camera looks down +z, y up)."""
+    eye, look, up = (np.asarray(v, np.float64) for v in (eye, look, up))
+    d = look - eye
+    d = d / np.linalg.norm(d)
+    right = np.cross(up / np.linalg.norm(up), d)
+    right = right / np.linalg.norm(right)
+    new_up = np.cross(d, right)
+    cam_to_world = np.eye(4)
+    cam_to_world[:3, 0], cam_to_world[:3, 1], cam_to_world[:3, 2], cam_to_world[:3, 3] = right, new_up, d, eye
+    return np.linalg.inv(cam_to_world)
+
+
+def _read_ply(path: Path):
+    """Vertex positions [V, 3] and polygon index lists of an ascii or binary little-endian PLY."""
+    data = path.read_bytes()
+    end = data.index(b"end_header") + len(b"end_header")
+    while data[end:end + 1] in (b"\r", b"\n"):
+        end += 1
+        if data[end - 1:end] == b"\n":
+            break
+    header = data[:end].decode("ascii").splitlines()
+    fmt = next(l.split()[1] for l in header if l.startswith("format"))
+    elements, cur = [], None
+    for l in header:
+        t = l.split()
+        if t and t[0] == "element":
+            cur = {"name": t[1], "count": int(t[2]), "props": []}
+            elements.append(cur)
+        elif t and t[0] == "property":
+            cur["props"].append(t[1:])
+    np_t = {"char": "i1", "int8": "i1", "uchar": "u1", "uint8": "u1", "short": "i2", "int16": "i2", "ushort": "u2", "uint16": "u2",
+            "int": "i4", "int32": "i4", "uint": "u4", "uint32": "u4", "float": "f4", "float32": "f4", "double": "f8", "float64": "f8"}
+    verts, faces = None, []
+    if fmt == "ascii":
+        lines = data[end:].decode("ascii").split("\n")
+        li = 0
+        for el in elements:
+            rows = []
+            for _ in range(el["count"]):
+                while not lines[li].strip():
+                    li += 1
+                rows.append(lines[li].split())
+                li += 1
+            if el["name"] == "vertex":
+                names = [p[-1] for p in el["props"]]
+                idx = [names.index(k) for k in ("x", "y", "z")]
+                verts = np.array([[float(r[j]) for j in idx] for r in rows], np.float64)
+            elif el["name"] == "face":
+                faces = [[int(v) for v in r[1:1 + int(r[0])]] for r in rows]
+        return verts, faces
+    if fmt != "binary_little_endian":
+        raise ValueError(f"{path}: PLY format {fmt} is not read")
+    off = end
+    for el in elements:
+        if all(p[0] != "list" for p in el["props"]):
+            dt = np.dtype([(p[1], "<" + np_t[p[0]]) for p in el["props"]])
+            arr = np.frombuffer(data, dt, el["count"], off)
+            off += dt.itemsize * el["count"]
+            if el["name"] == "vertex":
+                verts = np.stack([arr["x"], arr["y"], arr["z"]], -1).astype(np.float64)
+        else:
+            rows = []
+            for _ in range(el["count"]):
+                row = []
+                for p in el["props"]:
+                    if p[0] == "list":
+                        ct, it = np.dtype("<" + np_t[p[1]]), np.dtype("<" + np_t[p[2]])
+                        k = int(np.frombuffer(data, ct, 1, off)[0])
+                        off += ct.itemsize
+                        row.append(np.frombuffer(data, it, k, off).tolist())
+                        off += it.itemsize * k
+                    else:
+                        off += np.dtype(np_t[p[0]]).itemsize
+                rows.append(row)
+            if el["name"] == "face":
+                faces = [r[0] for r in rows]
+    return verts, faces
+
+
+def _pbrt_rgb(ps, name, default):
+    if name not in ps:
+        return tuple(default)
+    ptype, vals = ps[name]
+    if ptype == "rgb":
+        return tuple(float(v) for v in vals[:3])
+    if ptype == "float":
+        return (float(vals[0]),) * 3
+    return tuple(default)  # named or sampled spectra are not converted
+
+
+def _pbrt_float(ps, name, default):
+    return float(ps[name][1][0]) if name in ps else float(default)
+
+
+def _pbrt_scalar_roughness(ps, prefix=""):
+    """getRoughness + getScalarRoughness (PBRTImporter.cpp:424-479), as written."""
+    r = _pbrt_float(ps, prefix + "roughness", 0.0)
+    u = _pbrt_float(ps, prefix + "uroughness", r)
+    v = _pbrt_float(ps, prefix + "vroughness", r)
+    both = u + v
+    if ps.get("remaproughness", ("bool", [True]))[1][0]:
+        both = math.sqrt(both)
+    return 0.5 * (both + both)
+
+
+def _conductor_f0(ps, prefix=""):
+    """getConductorSpecularAlbedo (PBRTImporter.cpp:496-587): the conductor Fresnel at normal
+    incidence, from rgb eta and k or directly from a reflectance."""
+    if prefix + "reflectance" in ps:
+        return _pbrt_rgb(ps, prefix + "reflectance", (0.0, 0.0, 0.0))
+    if ps.get(prefix + "eta", ("", []))[0] == "rgb" and ps.get(prefix + "k", ("", []))[0] == "rgb":
+        eta, k = _pbrt_rgb(ps, prefix + "eta", (1, 1, 1)), _pbrt_rgb(ps, prefix + "k", (0, 0, 0))
+        return tuple(((e - 1) ** 2 + kk ** 2) / ((e + 1) ** 2 + kk ** 2) for e, kk in zip(eta, k))
+    return _PBRT_COPPER_F0
+
+
+def _pbrt_material(mtype, ps):
+    """(base, roughness, metallic, ior) of the StandardMaterial the reference makes."""
+    if mtype in ("diffuse", "", "interface"):
+        return _pbrt_rgb(ps, "reflectance", (0.5, 0.5, 0.5)), 1.0, 0.0, 1.5
+    if mtype == "coateddiffuse":
+        return _pbrt_rgb(ps, "reflectance", (0.5, 0.5, 0.5)), math.sqrt(_pbrt_scalar_roughness(ps)), 0.0, 1.5
+    if mtype == "conductor":
+        return _conductor_f0(ps), math.sqrt(_pbrt_scalar_roughness(ps)), 1.0, 1.5
+    if mtype == "coatedconductor":
+        return _conductor_f0(ps, "conductor."), math.sqrt(_pbrt_scalar_roughness(ps, "conductor.")), 1.0, 1.5
+    if mtype in ("dielectric", "thindielectric"):
+        eta = _pbrt_float(ps, "eta", 1.5)
+        return (0.0, 0.0, 0.0), math.sqrt(_pbrt_scalar_roughness(ps)), 0.0, eta
+    raise ValueError(f"PBRT material {mtype!r} is not converted")
+
+
+def load_pbrt(path) -> Scene:
+    """A PBRT v4 scene file as the pass's triangle soup; info holds "camera" (position, target, up,
+    fovDegrees) and "env" (an [h, w, 3] radiance map for rs_set_env_map) when the file has them."""
+    path = Path(path)
+    tris, mids, mat_rows, mat_index = [], [], [], {}
+    state = {"ctm": np.eye(4), "material": ("diffuse", {}), "area": None, "reverse": False}
+    stack, named, objects = [], {}, {}
+    current_object = None
+    camera, env = None, None
+
+    def material_id(mat, area):
+        mtype, ps = mat
+        base, rough, metal, ior = _pbrt_material(mtype, ps)
+        emissive = (0.0, 0.0, 0.0)
+        two = True
+        if area is not None:
+            L = _pbrt_rgb(area, "L", (1.0, 1.0, 1.0))
+            scale = _pbrt_float(area, "scale", 1.0)
+            emissive = tuple(c * scale for c in L)
+            two = bool(area.get("twosided", ("bool", [False]))[1][0])
+        key = (base, rough, metal, ior, emissive, two)
+        if key not in mat_index:
+            mat_index[key] = len(mat_rows)
+            mat_rows.append(material(base=base, roughness=rough, emissive=emissive, metallic=metal, ior=ior, double_sided=two))
+        return mat_index[key]
+
+    def emit(points, faces, xform, mid, reverse):
+        p = np.c_[np.asarray(points, np.float64), np.ones(len(points))] @ xform.T
+        p = p[:, :3] / p[:, 3:4]
+        flip = reverse ^ (np.linalg.det(xform[:3, :3]) < 0)
+        for f in faces:
+            for k in range(1, len(f) - 1):
+                a, b, c = (f[0], f[k + 1], f[k]) if flip else (f[0], f[k], f[k + 1])
+                tris.append(np.concatenate([p[a], p[b], p[c]]))
+                mids.append(mid)
+
+    def shape(stype, ps, base_dir):
+        if stype == "trianglemesh":
+            P = np.asarray(ps["P"][1], np.float64).reshape(-1, 3)
+            idx = ps["indices"][1] if "indices" in ps else list(range(len(P)))
+            faces = np.asarray(idx, np.int64).reshape(-1, 3).tolist()
+        elif stype == "bilinearmesh":
+            P = np.asarray(ps["P"][1], np.float64).reshape(-1, 3)
+            idx = ps["indices"][1] if "indices" in ps else list(range(len(P)))
+            faces = [[q[0], q[1], q[3], q[2]] for q in np.asarray(idx, np.int64).reshape(-1, 4).tolist()]
+        elif stype == "sphere":
+            from .scenes import _icosphere
+            ico = _icosphere(3).reshape(-1, 3) * _pbrt_float(ps, "radius", 1.0)
+            P, faces = ico, np.arange(len(ico)).reshape(-1, 3).tolist()
+        elif stype == "plymesh":
+            P, faces = _read_ply(base_dir / ps["filename"][1][0])
+        else:
+            raise ValueError(f"PBRT shape {stype!r} is not converted")
+        return P, faces
+
+    def parse(file_path: Path):
+        nonlocal camera, env, current_object
+        r = _PbrtReader(_pbrt_tokens(file_path.read_text()))
+        base_dir = file_path.parent
+        while r.more():
+            d = r.next()
+            if d == "Identity":
+                state["ctm"] = np.eye(4)
+            elif d == "Translate":
+                t = np.eye(4)
+                t[:3, 3] = r.numbers(3)
+                state["ctm"] = state["ctm"] @ t
+            elif d == "Scale":
+                state["ctm"] = state["ctm"] @ np.diag(r.numbers(3) + [1.0])
+            elif d == "Rotate":
+                v = r.numbers(4)
+                state["ctm"] = state["ctm"] @ _rotate(v[0], v[1:])
+            elif d == "LookAt":
+                v = r.numbers(9)
+                state["ctm"] = state["ctm"] @ _look_at(v[0:3], v[3:6], v[6:9])
+            elif d in ("ConcatTransform", "Transform"):
+                m = np.asarray(r.numbers(16), np.float64).reshape(4, 4).T  # column-major in the file
+                state["ctm"] = (state["ctm"] @ m) if d == "ConcatTransform" else m
+            elif d == "Camera":
+                ctype = r.next()[1:-1]
+                ps = r.params()
+                c2w = np.linalg.inv(state["ctm"])
+                pos = c2w @ [0, 0, 0, 1]
+                tgt = c2w @ [0, 0, 1, 1]
+                up = c2w @ [0, 1, 0, 0]
+                camera = {"type": ctype, "position": tuple(float(x) for x in pos[:3]), "target": tuple(float(x) for x in tgt[:3]),
+                          "up": tuple(float(x) for x in up[:3]), "fovDegrees": _pbrt_float(ps, "fov", 90.0)}
+            elif d == "WorldBegin":
+                state["ctm"] = np.eye(4)
+            elif d == "AttributeBegin":
+                stack.append(dict(state))
+            elif d == "AttributeEnd":
+                state.update(stack.pop())
+            elif d == "ReverseOrientation":
+                state["reverse"] = not state["reverse"]
+            elif d == "Material":
+                mtype = r.next()[1:-1]
+                state["material"] = (mtype, r.params())
+            elif d == "MakeNamedMaterial":
+                name = r.next()[1:-1]
+                ps = r.params()
+                named[name] = (ps.pop("type", ("string", ["diffuse"]))[1][0], ps)
+            elif d == "NamedMaterial":
+                state["material"] = named[r.next()[1:-1]]
+            elif d == "AreaLightSource":
+                atype = r.next()[1:-1]
+                ps = r.params()
+                if atype != "diffuse":
+                    raise ValueError(f"PBRT area light {atype!r} is not converted")
+                state["area"] = ps
+            elif d == "LightSource":
+                ltype = r.next()[1:-1]
+                ps = r.params()
+                if ltype == "infinite":
+                    if "filename" in ps:
+                        raise ValueError("PBRT image infinite lights (equal-area maps) are not converted")
+                    L = np.asarray(_pbrt_rgb(ps, "L", (1.0, 1.0, 1.0)), np.float32) * _pbrt_float(ps, "scale", 1.0)
+                    env = np.broadcast_to(L, (8, 16, 3)).astype(np.float32).copy()
+                else:
+                    raise ValueError(f"PBRT light {ltype!r} is not converted (the pass samples emissive triangles and an env map)")
+            elif d == "Shape":
+                stype = r.next()[1:-1]
+                ps = r.params()
+                P, faces = shape(stype, ps, base_dir)
+                mid = material_id(state["material"], state["area"])
+                if current_object is not None:
+                    objects[current_object].append((P, faces, state["ctm"].copy(), mid, state["reverse"]))
+                else:
+                    emit(P, faces, state["ctm"], mid, state["reverse"])
+            elif d == "ObjectBegin":
+                current_object = r.next()[1:-1]
+                objects[current_object] = []
+                stack.append(dict(state))
+            elif d == "ObjectEnd":
+                current_object = None
+                state.update(stack.pop())
+            elif d == "ObjectInstance":
+                for P, faces, xf, mid, rev in objects[r.next()[1:-1]]:
+                    emit(P, faces, state["ctm"] @ xf, mid, rev)
+            elif d in ("Include", "Import"):
+                parse(base_dir / r.next()[1:-1])
+            elif d in ("Film", "Sampler", "Integrator", "PixelFilter", "Accelerator", "ColorSpace", "Option", "Texture",
+                       "CoordinateSystem", "CoordSysTransform", "MakeNamedMedium", "MediumInterface", "Attribute",
+                       "TransformBegin", "TransformEnd", "ActiveTransform", "TransformTimes", "WorldEnd"):
+                if d == "TransformBegin":
+                    stack.append(dict(state))
+                elif d == "TransformEnd":
+                    state.update(stack.pop())
+                elif d == "Texture":
+                    r.next(); r.next(); r.next()
+                    r.params()
+                elif d in ("CoordinateSystem", "CoordSysTransform", "ActiveTransform", "MediumInterface"):
+                    r.next()
+                    if d == "MediumInterface" and r.more() and r.peek().startswith('"') and len(r.peek().split()) == 1:
+                        r.next()
+                elif d == "TransformTimes":
+                    r.numbers(2)
+                elif d in ("MakeNamedMedium",):
+                    r.next(); r.params()
+                elif d in ("Option", "Attribute"):
+                    r.next()
+                    r.params()
+                elif d != "WorldEnd":
+                    if r.more() and r.peek().startswith('"') and len(r.peek()[1:-1].split()) == 1:
+                        r.next()
+                    r.params()
+            else:
+                raise ValueError(f"{file_path}: PBRT directive {d!r} is not read")
+
+    parse(path)
+    if not tris:
+        raise ValueError(f"{path}: no shapes")
+    info = {"triangles": len(tris), "materials": len(mat_rows)}
+    if camera:
+        info["camera"] = camera
+    if env is not None:
+        info["env"] = env
+    return Scene(np.asarray(tris, np.float32), np.asarray(mids, np.uint32), np.stack(mat_rows).astype(np.float32), path.stem, info)
+
+
+def pbrt_camera(scene: Scene, width: int, height: int):
+    """The pass camera of a load_pbrt scene: its LookAt, with the field of view taken across the
+    shorter image side (PBRT's "fov"), on a 24 mm film height."""
+    from .scenes import Camera
+    c = scene.info["camera"]
+    half = math.radians(c["fovDegrees"]) * 0.5
+    frame_height = 24.0
+    if width < height:  # fov spans the width: convert to the vertical extent
+        half = math.atan(math.tan(half) * height / width)
+    return Camera(position=c["position"], target=c["target"], up=c["up"], focal_length=0.5 * frame_height / math.tan(half),
+                  frame_height=frame_height, aspect_ratio=width / height)

@@ -118,3 +118,33 @@ def test_zero_intensity_env_is_no_env(rs, scenes):
         imgs.append(img)
         p.close()
     assert np.array_equal(imgs[0].view(np.uint32), imgs[1].view(np.uint32))
+
+
+@pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
+@pytest.mark.parametrize("mode", ["ScatterBackup", "GatherOnly"])
+def test_imported_pbrt_scene(rs, oracle_mod, scenes, monkeypatch, tmp_path, mode):
+    """A PBRT v4 file through importers.load_pbrt (area light, conductor, coated diffuse, dielectric,
+    instanced PLY, constant infinite light as the env map) rendered by the pass and the oracle."""
+    import reservoir_splatting_b200.importers as I
+    from test_importers_cpu import _write_pbrt
+    sc = I.load_pbrt(_write_pbrt(tmp_path))
+    env = sc.info["env"]
+    orig_gpu, orig_ora = rs.ReservoirSplatting.set_scene, oracle_mod.OraclePass.set_scene
+
+    def gpu_set_scene(self, scene):
+        orig_gpu(self, scene)
+        self.set_env_map(env)
+
+    def ora_set_scene(self, scene):
+        orig_ora(self, scene)
+        self.set_env_map(env)
+    monkeypatch.setattr(rs.ReservoirSplatting, "set_scene", gpu_set_scene)
+    monkeypatch.setattr(oracle_mod.OraclePass, "set_scene", ora_set_scene)
+
+    def camera_fn(f, w, h):
+        c = I.pbrt_camera(sc, w, h)
+        c.position = (c.position[0] + 0.02 * f, c.position[1], c.position[2])
+        return c
+    props = {"temporalReuse": mode, "gatherOption": "Clamped", "maxSurfaceBounces": 2, "enableSpatialResampling": True}
+    _, img = run_pair(rs, oracle_mod, sc, camera_fn, props, frames=3, width=48, height=36)
+    assert np.isfinite(img).all() and img[..., :3].mean() > 0.01

@@ -67,3 +67,93 @@ def test_empty_obj_is_rejected(rs, tmp_path):
     (tmp_path / "e.obj").write_text("v 0 0 0\n")
     with pytest.raises(ValueError):
         I.load_obj(tmp_path / "e.obj")
+
+
+PBRT_SCENE = """# a small PBRT v4 scene
+LookAt 0 1 -5   0 1 0   0 1 0
+Camera "perspective" "float fov" [ 40 ]
+Film "rgb" "integer xresolution" [64] "integer yresolution" [48] "string filename" "x.exr"
+WorldBegin
+LightSource "infinite" "rgb L" [0.2 0.3 0.5] "float scale" 2
+MakeNamedMaterial "floor" "string type" "diffuse" "rgb reflectance" [0.7 0.6 0.5]
+AttributeBegin
+  NamedMaterial "floor"
+  Shape "trianglemesh" "point3 P" [-5 0 -5  5 0 -5  5 0 5  -5 0 5] "integer indices" [0 1 2 0 2 3]
+AttributeEnd
+AttributeBegin
+  AreaLightSource "diffuse" "rgb L" [4 4 3] "float scale" 2
+  Translate 0 3 0
+  Shape "bilinearmesh" "point3 P" [-1 0 -1  1 0 -1  -1 0 1  1 0 1]
+AttributeEnd
+AttributeBegin
+  Material "conductor" "rgb eta" [0.2 0.9 1.1] "rgb k" [3.9 2.4 2.2] "float roughness" 0.08
+  Translate 1 1 0
+  Shape "sphere" "float radius" 0.5
+AttributeEnd
+ObjectBegin "quad"
+  Material "coateddiffuse" "rgb reflectance" [0.2 0.8 0.2] "float roughness" 0.1
+  Shape "plymesh" "string filename" "quad.ply"
+ObjectEnd
+AttributeBegin
+  Translate -1 0.5 0
+  ObjectInstance "quad"
+AttributeEnd
+AttributeBegin
+  Translate -2 0.5 0
+  Rotate 90 0 1 0
+  ObjectInstance "quad"
+AttributeEnd
+Include "more.pbrt"
+"""
+
+
+def _write_pbrt(tmp_path, binary_ply=False):
+    (tmp_path / "scene.pbrt").write_text(PBRT_SCENE)
+    (tmp_path / "more.pbrt").write_text('Material "dielectric" "float eta" 1.33\nShape "trianglemesh" "point3 P" [0 0 1 1 0 1 0 1 1]\n')
+    verts = np.array([[0, 0, 0], [0.5, 0, 0], [0.5, 0.5, 0], [0, 0.5, 0]], np.float32)
+    if binary_ply:
+        head = ("ply\nformat binary_little_endian 1.0\nelement vertex 4\nproperty float x\nproperty float y\nproperty float z\n"
+                "element face 1\nproperty list uchar int vertex_indices\nend_header\n").encode()
+        body = verts.tobytes() + bytes([4]) + np.array([0, 1, 2, 3], "<i4").tobytes()
+        (tmp_path / "quad.ply").write_bytes(head + body)
+    else:
+        (tmp_path / "quad.ply").write_text("ply\nformat ascii 1.0\nelement vertex 4\nproperty float x\nproperty float y\nproperty float z\n"
+                                          "element face 1\nproperty list uchar int vertex_indices\nend_header\n"
+                                          + "\n".join(" ".join(str(float(c)) for c in v) for v in verts) + "\n4 0 1 2 3\n")
+    return tmp_path / "scene.pbrt"
+
+
+@pytest.mark.parametrize("binary_ply", [False, True])
+def test_pbrt_scene(rs, tmp_path, binary_ply):
+    import reservoir_splatting_b200.importers as I
+    sc = I.load_pbrt(_write_pbrt(tmp_path, binary_ply))
+    # floor 2 + light quad 2 + icosphere 1280 + two instanced PLY quads 2 x 2 + included triangle 1
+    assert sc.positions.shape == (1289, 9) and sc.material_ids.shape == (1289,)
+    m = sc.materials
+    floor, light, metal, coated, glass = (m[sc.material_ids[i]] for i in (0, 2, 4, 1284, 1288))
+    assert np.allclose(floor[:3], [0.7, 0.6, 0.5]) and floor[3] == 1.0 and floor[7] == 0.0
+    assert np.allclose(light[4:7], [8, 8, 6]) and np.allclose(light[:3], 0.5)
+    eta, k = np.array([0.2, 0.9, 1.1]), np.array([3.9, 2.4, 2.2])
+    assert np.allclose(metal[:3], ((eta - 1) ** 2 + k ** 2) / ((eta + 1) ** 2 + k ** 2), rtol=1e-6) and metal[7] == 1.0
+    # getRoughness as written: sqrt(u + v), then the StandardMaterial takes its square root
+    assert abs(metal[3] - np.sqrt(np.sqrt(0.16))) < 1e-6 and abs(coated[3] - np.sqrt(np.sqrt(0.2))) < 1e-6
+    assert abs(glass[8] - 1.33) < 1e-6 and np.allclose(glass[:3], 0.0)
+    # the light quad is moved up by 3, the rotated instance lies in the x = -2 plane
+    assert np.allclose(sc.positions[2:4, 1::3], 3.0)
+    inst = sc.positions[1286:1288].reshape(-1, 3)
+    assert np.allclose(inst[:, 0], -2.0, atol=1e-6) and inst[:, 1].min() >= 0.5 - 1e-6
+    cam = sc.info["camera"]
+    assert np.allclose(cam["position"], [0, 1, -5]) and np.allclose(cam["target"], [0, 1, -4]) and cam["fovDegrees"] == 40.0
+    assert sc.info["env"].shape[2] == 3 and np.allclose(sc.info["env"][0, 0], [0.4, 0.6, 1.0])
+    c = I.pbrt_camera(sc, 64, 48)
+    assert abs(2 * np.degrees(np.arctan(0.5 * c.frame_height / c.focal_length)) - 40.0) < 1e-9
+
+
+def test_pbrt_rejects_what_it_does_not_convert(rs, tmp_path):
+    import reservoir_splatting_b200.importers as I
+    for body in ('Shape "disk"', 'LightSource "point" "rgb I" [1 1 1]', 'Material "measured"\nShape "sphere"',
+                 'LightSource "infinite" "string filename" "sky.exr"'):
+        p = tmp_path / "bad.pbrt"
+        p.write_text("WorldBegin\n" + body + "\n")
+        with pytest.raises(ValueError):
+            I.load_pbrt(p)
