@@ -576,3 +576,183 @@ def pbrt_camera(scene: Scene, width: int, height: int):
         half = math.atan(math.tan(half) * height / width)
     return Camera(position=c["position"], target=c["target"], up=c["up"], focal_length=0.5 * frame_height / math.tan(half),
                   frame_height=frame_height, aspect_ratio=width / height)
+
+
+# ---------------------------------------------------------------------------------------- Mitsuba
+# A subset of the reference's Mitsuba importer (Source/plugins/importers/MitsubaImporter/
+# MitsubaImporter.cpp:249-400 BSDFs, :468-530 shapes, :668-700 emitters), mapped to the one
+# StandardMaterial model the pass has: diffuse (reflectance, roughness 1), plastic / roughplastic
+# (diffuse_reflectance, IoR int_ior / ext_ior, roughness sqrt(alpha) for the rough one), conductor /
+# roughconductor (metallic, base = the normal-incidence Fresnel reflectance of rgb eta, k; copper
+# without them; roughness sqrt(alpha)), dielectric / roughdielectric / thindielectric (IoR only: no
+# transmission lobe), twosided (its nested BSDF); shapes obj, ply, rectangle, cube, sphere; area
+# emitters nested in shapes, constant emitters as an env map; a perspective sensor.  <default> and
+# $name substitution, refs by id, and to_world transforms (translate, scale, rotate, matrix, lookat).
+# Image environment maps, textures and other plugins are rejected with a message.
+
+_MITSUBA_IOR = {"vacuum": 1.0, "air": 1.00028, "water": 1.333, "acetone": 1.36, "ethanol": 1.361, "glycerol": 1.4729,
+                "bk7": 1.5046, "polypropylene": 1.49, "acrylic glass": 1.49, "pet": 1.575, "diamond": 2.419,
+                "fused quartz": 1.458, "sapphire": 1.77}
+
+
+def _mi_floats(text):
+    return [float(v) for v in text.replace(",", " ").split()]
+
+
+def _mi_transform(el):
+    m = np.eye(4)
+    for op in el:
+        a = op.attrib
+        if op.tag == "translate":
+            t = np.eye(4)
+            t[:3, 3] = [float(a.get(k, 0.0)) for k in "xyz"] if "value" not in a else _mi_floats(a["value"])
+            m = t @ m
+        elif op.tag == "scale":
+            if "value" in a:
+                v = _mi_floats(a["value"])
+                v = v * 3 if len(v) == 1 else v
+            else:
+                v = [float(a.get(k, 1.0)) for k in "xyz"]
+            m = np.diag(v + [1.0]) @ m
+        elif op.tag == "rotate":
+            axis = [float(a.get(k, 0.0)) for k in "xyz"] if "value" not in a else _mi_floats(a["value"])
+            m = _rotate(float(a["angle"]), axis) @ m
+        elif op.tag == "matrix":
+            m = np.asarray(_mi_floats(a["value"]), np.float64).reshape(4, 4) @ m
+        elif op.tag == "lookat":
+            m = np.linalg.inv(_look_at(_mi_floats(a["origin"]), _mi_floats(a["target"]), _mi_floats(a.get("up", "0 1 0")))) @ m
+        else:
+            raise ValueError(f"Mitsuba transform {op.tag!r} is not read")
+    return m
+
+
+def load_mitsuba(path) -> Scene:
+    """A Mitsuba 3 scene XML as the pass's triangle soup; info holds "camera" and "env" like load_pbrt."""
+    import xml.etree.ElementTree as ET
+    path = Path(path)
+    text = path.read_text()
+    root = ET.fromstring(text)
+    defaults = {d.attrib["name"]: d.attrib["value"] for d in root.iter("default")}
+
+    def sub(v):
+        for k, d in defaults.items():
+            v = v.replace("$" + k, d)
+        return v
+    for el in root.iter():
+        for k, v in list(el.attrib.items()):
+            el.attrib[k] = sub(v)
+    ids = {el.attrib["id"]: el for el in root.iter() if "id" in el.attrib and el.tag != "ref"}
+
+    def props(el):
+        out = {}
+        for c in el:
+            n = c.attrib.get("name")
+            if c.tag in ("float", "integer"):
+                out[n] = float(c.attrib["value"])
+            elif c.tag in ("rgb", "spectrum", "color"):
+                v = _mi_floats(c.attrib["value"])
+                out[n] = tuple(v * 3 if len(v) == 1 else v[:3])
+            elif c.tag in ("string", "boolean"):
+                out[n] = c.attrib["value"]
+            elif c.tag == "transform":
+                out[n] = _mi_transform(c)
+        return out
+
+    def ior(p, name, default):
+        v = p.get(name, default)
+        return _MITSUBA_IOR[v.lower()] if isinstance(v, str) else float(v)
+
+    def bsdf(el):
+        if el.tag == "ref":
+            el = ids[el.attrib["id"]]
+        t, p = el.attrib["type"], props(el)
+        if t == "twosided":
+            inner = [c for c in el if c.tag in ("bsdf", "ref")]
+            return bsdf(inner[0])
+        if t == "diffuse":
+            return p.get("reflectance", (0.5,) * 3), 1.0, 0.0, 1.5
+        if t in ("plastic", "roughplastic"):
+            rough = math.sqrt(p.get("alpha", 0.1)) if t == "roughplastic" else 0.0
+            return p.get("diffuse_reflectance", (0.5,) * 3), rough, 0.0, ior(p, "int_ior", "polypropylene") / ior(p, "ext_ior", "air")
+        if t in ("conductor", "roughconductor"):
+            if "eta" in p and "k" in p:
+                f0 = tuple(((e - 1) ** 2 + k ** 2) / ((e + 1) ** 2 + k ** 2) for e, k in zip(p["eta"], p["k"]))
+            else:
+                f0 = _PBRT_COPPER_F0
+            rough = math.sqrt(p.get("alpha", 0.1)) if t == "roughconductor" else 0.0
+            return f0, rough, 1.0, 1.5
+        if t in ("dielectric", "roughdielectric", "thindielectric"):
+            rough = math.sqrt(p.get("alpha", 0.1)) if t == "roughdielectric" else 0.0
+            return (0.0, 0.0, 0.0), rough, 0.0, ior(p, "int_ior", "bk7") / ior(p, "ext_ior", "air")
+        raise ValueError(f"Mitsuba BSDF {t!r} is not converted")
+
+    tris, mids, rows, index = [], [], [], {}
+    camera, env = None, None
+
+    def material_id(mat, emission):
+        base, rough, metal, eta = mat
+        key = (tuple(base), rough, metal, eta, tuple(emission))
+        if key not in index:
+            index[key] = len(rows)
+            rows.append(material(base=base, roughness=rough, emissive=emission, metallic=metal, ior=eta, double_sided=True))
+        return index[key]
+
+    cube_faces = [[0, 2, 3, 1], [4, 5, 7, 6], [0, 1, 5, 4], [2, 6, 7, 3], [0, 4, 6, 2], [1, 3, 7, 5]]
+    cube_verts = np.array([[x, y, z] for x in (-1, 1) for y in (-1, 1) for z in (-1, 1)], np.float64)
+    for el in root:
+        if el.tag == "sensor":
+            p = props(el)
+            c2w = p.get("to_world", np.eye(4))
+            pos, tgt, up = c2w @ [0, 0, 0, 1], c2w @ [0, 0, 1, 1], c2w @ [0, 1, 0, 0]
+            camera = {"type": el.attrib["type"], "position": tuple(float(x) for x in pos[:3]), "target": tuple(float(x) for x in tgt[:3]),
+                      "up": tuple(float(x) for x in up[:3]), "fovDegrees": float(p.get("fov", 45.0))}
+        elif el.tag == "emitter":
+            t, p = el.attrib["type"], props(el)
+            if t == "constant":
+                env = np.broadcast_to(np.asarray(p.get("radiance", (1.0,) * 3), np.float32), (8, 16, 3)).astype(np.float32).copy()
+            else:
+                raise ValueError(f"Mitsuba emitter {t!r} is not converted (area emitters belong inside shapes)")
+        elif el.tag == "shape":
+            t, p = el.attrib["type"], props(el)
+            xform = p.get("to_world", np.eye(4))
+            mat = (0.5, 0.5, 0.5), 1.0, 0.0, 1.5
+            emission = (0.0, 0.0, 0.0)
+            for c in el:
+                if c.tag in ("bsdf", "ref") and (c.tag == "bsdf" or ids[c.attrib["id"]].tag == "bsdf"):
+                    mat = bsdf(c)
+                elif c.tag == "emitter" and c.attrib["type"] == "area":
+                    emission = props(c).get("radiance", (1.0,) * 3)
+            if t == "obj":
+                s = load_obj(path.parent / p["filename"])
+                P, faces = s.positions.reshape(-1, 3).astype(np.float64), np.arange(len(s.positions) * 3).reshape(-1, 3).tolist()
+            elif t == "ply":
+                P, faces = _read_ply(path.parent / p["filename"])
+            elif t == "rectangle":
+                P, faces = np.array([[-1, -1, 0], [1, -1, 0], [1, 1, 0], [-1, 1, 0]], np.float64), [[0, 1, 2, 3]]
+            elif t == "cube":
+                P, faces = cube_verts, cube_faces
+            elif t == "sphere":
+                from .scenes import _icosphere
+                center = np.asarray(_mi_floats(el.find("point[@name='center']").attrib["value"])
+                                    if el.find("point[@name='center']") is not None else [0, 0, 0], np.float64)
+                P = _icosphere(3).reshape(-1, 3).astype(np.float64) * float(p.get("radius", 1.0)) + center
+                faces = np.arange(len(P)).reshape(-1, 3).tolist()
+            else:
+                raise ValueError(f"Mitsuba shape {t!r} is not converted")
+            mid = material_id(mat, emission)
+            hp = np.c_[np.asarray(P, np.float64), np.ones(len(P))] @ xform.T
+            hp = hp[:, :3] / hp[:, 3:4]
+            flip = np.linalg.det(xform[:3, :3]) < 0
+            for f in faces:
+                for k in range(1, len(f) - 1):
+                    a, b, c = (f[0], f[k + 1], f[k]) if flip else (f[0], f[k], f[k + 1])
+                    tris.append(np.concatenate([hp[a], hp[b], hp[c]]))
+                    mids.append(mid)
+    if not tris:
+        raise ValueError(f"{path}: no shapes")
+    info = {"triangles": len(tris), "materials": len(rows)}
+    if camera:
+        info["camera"] = camera
+    if env is not None:
+        info["env"] = env
+    return Scene(np.asarray(tris, np.float32), np.asarray(mids, np.uint32), np.stack(rows).astype(np.float32), path.stem, info)

@@ -148,3 +148,26 @@ def test_imported_pbrt_scene(rs, oracle_mod, scenes, monkeypatch, tmp_path, mode
     props = {"temporalReuse": mode, "gatherOption": "Clamped", "maxSurfaceBounces": 2, "enableSpatialResampling": True}
     _, img = run_pair(rs, oracle_mod, sc, camera_fn, props, frames=3, width=48, height=36)
     assert np.isfinite(img).all() and img[..., :3].mean() > 0.01
+
+
+@pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
+def test_imported_mitsuba_scene(rs, oracle_mod, scenes, monkeypatch, tmp_path):
+    """A Mitsuba 3 XML scene through importers.load_mitsuba, its constant emitter as the env map."""
+    import reservoir_splatting_b200.importers as I
+    from test_importers_cpu import _write_mitsuba
+    sc = I.load_mitsuba(_write_mitsuba(tmp_path))
+    env = sc.info["env"]
+    orig_gpu, orig_ora = rs.ReservoirSplatting.set_scene, oracle_mod.OraclePass.set_scene
+
+    def gpu_set_scene(self, scene):
+        orig_gpu(self, scene)
+        self.set_env_map(env)
+
+    def ora_set_scene(self, scene):
+        orig_ora(self, scene)
+        self.set_env_map(env)
+    monkeypatch.setattr(rs.ReservoirSplatting, "set_scene", gpu_set_scene)
+    monkeypatch.setattr(oracle_mod.OraclePass, "set_scene", ora_set_scene)
+    props = {"temporalReuse": "ScatterBackup", "gatherOption": "Clamped", "maxSurfaceBounces": 2, "enableSpatialResampling": True}
+    _, img = run_pair(rs, oracle_mod, sc, lambda f, w, h: I.pbrt_camera(sc, w, h), props, frames=3, width=48, height=36)
+    assert np.isfinite(img).all() and img[..., :3].mean() > 0.01

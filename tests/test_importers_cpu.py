@@ -157,3 +157,72 @@ def test_pbrt_rejects_what_it_does_not_convert(rs, tmp_path):
         p.write_text("WorldBegin\n" + body + "\n")
         with pytest.raises(ValueError):
             I.load_pbrt(p)
+
+
+MITSUBA_SCENE = """<scene version="3.0.0">
+  <default name="spp" value="16"/>
+  <default name="wall" value="0.6"/>
+  <sensor type="perspective">
+    <float name="fov" value="35"/>
+    <transform name="to_world"><lookat origin="0, 1, -6" target="0, 1, 0" up="0, 1, 0"/></transform>
+  </sensor>
+  <emitter type="constant"><rgb name="radiance" value="0.1, 0.2, 0.3"/></emitter>
+  <bsdf type="twosided" id="white"><bsdf type="diffuse"><rgb name="reflectance" value="$wall"/></bsdf></bsdf>
+  <shape type="rectangle">
+    <transform name="to_world"><scale value="4"/><rotate x="1" angle="90"/></transform>
+    <ref id="white"/>
+  </shape>
+  <shape type="rectangle">
+    <transform name="to_world"><rotate x="1" angle="90"/><translate y="3"/></transform>
+    <emitter type="area"><rgb name="radiance" value="5, 4, 3"/></emitter>
+  </shape>
+  <shape type="cube">
+    <transform name="to_world"><scale value="0.5"/><translate x="1" y="0.5"/></transform>
+    <bsdf type="roughconductor"><rgb name="eta" value="0.2, 0.9, 1.1"/><rgb name="k" value="3.9, 2.4, 2.2"/><float name="alpha" value="0.2"/></bsdf>
+  </shape>
+  <shape type="sphere">
+    <point name="center" value="-1, 0.5, 0"/><float name="radius" value="0.4"/>
+    <bsdf type="roughplastic"><rgb name="diffuse_reflectance" value="0.1, 0.3, 0.8"/><float name="alpha" value="0.3"/><string name="int_ior" value="bk7"/></bsdf>
+  </shape>
+  <shape type="obj"><string name="filename" value="tri.obj"/><bsdf type="dielectric"><float name="int_ior" value="1.33"/></bsdf></shape>
+</scene>
+"""
+
+
+def _write_mitsuba(tmp_path):
+    (tmp_path / "scene.xml").write_text(MITSUBA_SCENE)
+    (tmp_path / "tri.obj").write_text("v 0 0 2\nv 1 0 2\nv 0 1 2\nf 1 2 3\n")
+    return tmp_path / "scene.xml"
+
+
+def test_mitsuba_scene(rs, tmp_path):
+    import reservoir_splatting_b200.importers as I
+    sc = I.load_mitsuba(_write_mitsuba(tmp_path))
+    # floor 2 + light 2 + cube 12 + icosphere 1280 + obj 1
+    assert sc.positions.shape == (1297, 9)
+    m = sc.materials[sc.material_ids]
+    floor, light, cube, ball, glass = m[0], m[2], m[4], m[16], m[1296]
+    assert np.allclose(floor[:3], 0.6) and floor[3] == 1.0
+    # rectangle rotated about x by 90 degrees, scaled by 4: it lies in y = 0 with x, z in [-4, 4]
+    assert np.allclose(sc.positions[0:2, 1::3], 0.0, atol=1e-6) and np.abs(sc.positions[0:2, 0::3]).max() == 4.0
+    assert np.allclose(light[4:7], [5, 4, 3]) and np.allclose(sc.positions[2:4, 1::3], 3.0, atol=1e-6)
+    eta, k = np.array([0.2, 0.9, 1.1]), np.array([3.9, 2.4, 2.2])
+    assert np.allclose(cube[:3], ((eta - 1) ** 2 + k ** 2) / ((eta + 1) ** 2 + k ** 2), rtol=1e-6)
+    assert cube[7] == 1.0 and abs(cube[3] - np.sqrt(0.2)) < 1e-6
+    cube_pts = sc.positions[4:16].reshape(-1, 3)
+    assert np.allclose(cube_pts.min(0), [0.5, 0.0, -0.5]) and np.allclose(cube_pts.max(0), [1.5, 1.0, 0.5])
+    assert np.allclose(ball[:3], [0.1, 0.3, 0.8]) and abs(ball[3] - np.sqrt(0.3)) < 1e-6 and abs(ball[8] - 1.5046 / 1.00028) < 1e-5
+    assert abs(glass[8] - 1.33 / 1.00028) < 1e-5
+    cam = sc.info["camera"]
+    assert np.allclose(cam["position"], [0, 1, -6]) and np.allclose(cam["target"], [0, 1, -5]) and cam["fovDegrees"] == 35.0
+    assert np.allclose(sc.info["env"][0, 0], [0.1, 0.2, 0.3])
+
+
+def test_mitsuba_rejects_what_it_does_not_convert(rs, tmp_path):
+    import reservoir_splatting_b200.importers as I
+    for body in ('<shape type="disk"/>', '<emitter type="envmap"><string name="filename" value="sky.exr"/></emitter>',
+                 '<shape type="cube"><bsdf type="hair"/></shape>'):
+        p = tmp_path / "bad.xml"
+        p.write_text(f'<scene version="3.0.0">{body}</scene>')
+        with pytest.raises(ValueError):
+            I.load_mitsuba(p)
