@@ -1440,8 +1440,10 @@ extern "C" RS_API rs_status rs_batch_execute(rs_batch* b, const rs_frame_desc* f
         p->lastStream = s;
         p->stageNames.clear();
         colors[i] = frames[i].color;
-        // the graph depends on the ping-pong buffers in use and on whether temporal stages run
-        key[i] = (uint32_t)p->currIdx * 3u + (uint32_t)p->prevIdx + 9u * (p->frameCount == 0 || frames[i].sceneShouldReset ? 1u : 0u);
+        // the graph depends on the ping-pong buffers in use, on whether temporal stages run and on
+        // which kernel variants run (with or without the environment light)
+        key[i] = (uint32_t)p->currIdx * 3u + (uint32_t)p->prevIdx + 9u * (p->frameCount == 0 || frames[i].sceneShouldReset ? 1u : 0u) +
+                 18u * (p->envHost.present ? 1u : 0u);
     }
     cudaGraphExec_t exec = nullptr;
     for (auto& g : b->graphs)

@@ -15,7 +15,10 @@ def _cuda_ok():
 
 
 @pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
-def test_batch_matches_individual_passes(rs, scenes):
+@pytest.mark.parametrize("env_frame", [None, 5], ids=["no-env", "env-from-frame-5"])
+def test_batch_matches_individual_passes(rs, scenes, env_frame):
+    """With env_frame, the first instance gets a sky environment map at that frame: graphs captured
+    before it (the same buffer pattern recurs) must not be replayed with the kernels without it."""
     import torch
     terrain = scenes.terrain_spheres(seed=4, grid=32, spheres=6, subdiv=2, lights=6, extent=30.0, height=3.0)
     cfgs = [
@@ -31,7 +34,11 @@ def test_batch_matches_individual_passes(rs, scenes):
     outs = [torch.zeros((h, w, 4), dtype=torch.float32, device="cuda") for _, _, _, w, h in cfgs]
     batch = rs.Batch(batched)
     stream = torch.cuda.current_stream().cuda_stream
-    for f in range(5):
+    for f in range(5 if env_frame is None else 8):
+        if f == env_frame:
+            sky = scenes.sky_env_map(64, 32, seed=1)
+            solo[0].set_env_map(sky)
+            batched[0].set_env_map(sky)
         cams = [cfg[1](f, cfg[3], cfg[4]) for cfg in cfgs]
         ref = [p.render(c) for p, c in zip(solo, cams)]
         batch.execute(cams, [o.data_ptr() for o in outs], stream=stream)
