@@ -605,6 +605,71 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+RAY_STATS_MODES = {
+    "ScatterBackup": {"temporalReuse": "ScatterBackup", "gatherOption": "Clamped", "scatterBackupMISOption": "Balance"},
+    "ScatterOnly": {"temporalReuse": "ScatterOnly"},
+    "GatherClamped": {"temporalReuse": "GatherOnly", "gatherOption": "Clamped"},
+    "GatherRobust": {"temporalReuse": "GatherOnly", "gatherOption": "Robust"},
+}
+
+
+def _ray_stats_inner(lib_kind: str, mode: str, frames: int):
+    """One process of --ray-stats: stage times (default library) or ray counts (the library built
+    with -DRS_RAY_STATS), averaged over `frames` stage-timed 1080p frames after 4 warm-up frames."""
+    spec = importlib.util.spec_from_file_location("rs_build", PKG_DIR / "build.py")
+    b = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(b)
+    rs = _package()
+    rs.LIB_PATH = b.LIB_RAY_STATS if lib_kind == "counts" else b.LIB
+    import torch
+    W, H = W_FULL, H_FULL
+    p = rs.ReservoirSplatting(dict(RAY_STATS_MODES[mode], maxSurfaceBounces=2, enableSpatialResampling=True), W, H)
+    p.set_scene(build_scene())
+    color = torch.empty((H, W, 4), device="cuda")
+    for f in range(4):
+        p.execute(camera(f, W, H), color_ptr=color.data_ptr())
+    p.enable_stage_timing(True)
+    ms, rays = {}, {}
+    for f in range(4, 4 + frames):
+        p.execute(camera(f, W, H), color_ptr=color.data_ptr())
+        for k, v in p.stage_times().items():
+            ms[k] = ms.get(k, 0.0) + v / frames
+        for k, (c, v) in p.stage_rays().items():
+            a = rays.setdefault(k, [0.0, 0.0])
+            a[0] += c / frames
+            a[1] += v / frames
+    p.close()
+    print(json.dumps({"ms": ms, "rays": rays}))
+
+
+def run_ray_stats(args):
+    """Ray queries per stage and query rates (markdown table): counts from the counting library,
+    times from the default one, each in its own process."""
+    spec = importlib.util.spec_from_file_location("rs_build", PKG_DIR / "build.py")
+    b = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(b)
+    b.build_ray_stats()
+    b.build()
+    runs = {}
+    for inner in ("counts", "times"):
+        out = subprocess.run([sys.executable, __file__, "--ray-stats", args.ray_stats, "--ray-stats-inner", inner,
+                              "--mode-frames", str(args.mode_frames)], check=True, capture_output=True, text=True)
+        runs[inner] = json.loads(out.stdout.strip().splitlines()[-1])
+    rays, ms = runs["counts"]["rays"], runs["times"]["ms"]
+    npix = W_FULL * H_FULL
+    print("| stage | closest-hit | visibility | queries / pixel | ms | G queries / s |")
+    print("|---|---:|---:|---:|---:|---:|")
+    tc = tv = tms = 0.0
+    for k, t in ms.items():
+        c, v = rays.get(k, (0.0, 0.0))
+        if c + v == 0:
+            continue
+        tc, tv, tms = tc + c, tv + v, tms + t
+        print(f"| {k} | {c:,.0f} | {v:,.0f} | {(c + v) / npix:.2f} | {t:.3f} | {(c + v) / t / 1e6:.2f} |")
+    print(f"| all traversal stages | {tc:,.0f} | {tv:,.0f} | {(tc + tv) / npix:.2f} | {tms:.3f} | {(tc + tv) / tms / 1e6:.2f} |")
+    print(f"frame: {sum(ms.values()):.3f} ms of stages (stage timing serialises the side streams)")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -624,8 +689,15 @@ def main():
     ap.add_argument("--mode-frames", type=int, default=10)
     ap.add_argument("--gt-spp", type=int, default=512)
     ap.add_argument("--adjoint-reps", type=int, default=3)
+    ap.add_argument("--ray-stats", choices=sorted(RAY_STATS_MODES),
+                    help="print ray queries per stage of a 1080p frame in this mode instead of the bench line")
+    ap.add_argument("--ray-stats-inner", choices=["counts", "times"], help=argparse.SUPPRESS)
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.ray_stats and args.ray_stats_inner:
+        _ray_stats_inner(args.ray_stats_inner, args.ray_stats, args.mode_frames)
+    elif args.ray_stats:
+        run_ray_stats(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

@@ -132,11 +132,22 @@ typedef struct rs_camera {
     float farZ;
 } rs_camera;
 
-/* Per-frame inputs/outputs (the reflect() channels, ReservoirSplatting.cpp:64-96). */
+/* Per-frame inputs/outputs (the reflect() channels, ReservoirSplatting.cpp:64-96).
+ *
+ * mvec and vbuffer are the pass's two inputs (`mvec` RG32F and `vbuffer` PackedHitInfo,
+ * ReservoirSplatting.cpp:64-72).  When given, the pass reads them in place of its own: the motion
+ * vectors drive the backup gather and the scatter's motion checks; the primary hits give the
+ * circle of confusion that splits depth-of-field gathers between the lens-vertex copy and the
+ * primary-hit reconnection (GatherTemporalResampling.rt.slang:79, SpatialResampling.rt.slang:80).
+ * A hit is four words (HitInfo.slang's type, primitive and barycentrics): word 0 = hit type
+ * (0 miss, 1 triangle), word 1 = triangle index in the scene's order, words 2, 3 = barycentrics
+ * u, v as float bits (the layout rs_get_buffer(RS_BUF_VBUFFER) returns).
+ * When both are given the pass launches no primary-hit kernel of its own, and RS_BUF_MVEC /
+ * RS_BUF_VBUFFER keep the values of the last frame that computed them. */
 typedef struct rs_frame_desc {
     rs_camera camera;
     const float* mvec;                   /* optional device float2[W*H]; NULL: computed by the pass */
-    const uint32_t* vbuffer;             /* optional device uint4[W*H] packed hits; NULL: computed */
+    const uint32_t* vbuffer;             /* optional device uint4[W*H] packed hits; NULL: computed by the pass */
     float* color;                        /* device float4[W*H] output (may be NULL if colorHost set) */
     float* colorHost;                    /* optional host float4[W*H]; copied back and synchronised */
     uint32_t sceneShouldReset;           /* Scene::shouldReset(): restart the temporal history */
@@ -214,7 +225,9 @@ RS_API const char* rs_last_error_string(void);
  * the members' stage chains are graph branches that run concurrently.  frames[i] belongs to
  * passes[i] and must carry a device colour buffer; graphs are cached per set of colour buffers and
  * per buffer-parity pattern, so keep the buffers stable across frames.  The call returns after the
- * launch; the previous batch frame is awaited before a member's context is rewritten. */
+ * launch; the previous batch frame is awaited before a member's context is rewritten.  frames[i].mvec
+ * and .vbuffer work as in rs_execute; the graph holds their pointers too.  Changing a member's
+ * options, scene, environment map or size between two calls drops the cached graphs. */
 typedef struct rs_batch rs_batch;
 RS_API rs_status rs_batch_create(rs_pass* const* passes, uint32_t count, rs_batch** out);
 RS_API rs_status rs_batch_execute(rs_batch* batch, const rs_frame_desc* frames, void* cudaStream);
@@ -243,7 +256,7 @@ RS_API rs_status rs_set_bvh_builder(rs_pass* pass, uint32_t builder);
 /* Ray-query counts per stage of the last frame rendered with stage timing on (no reference
  * counterpart): rays[2i], rays[2i+1] = closest-hit and visibility queries of stage i, in the order of
  * rs_get_stage_times; *count = stages.  Only a library built with -DRS_RAY_STATS counts (build.py
- * build_ray_stats, raystats.py); the default library reports *count = 0.  Synchronises. */
+ * build_ray_stats; bench.py --ray-stats); the default library reports *count = 0.  Synchronises. */
 RS_API rs_status rs_debug_stage_rays(rs_pass* pass, uint64_t* rays, uint32_t* count);
 
 /* Path-replay adjoint (no reference counterpart: the reference pass renders forward only).

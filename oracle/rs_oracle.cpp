@@ -2707,6 +2707,232 @@ __attribute__((visibility("default"))) void ro_test_bsdf_grad(const float* mat, 
     oracle::replay_vertex_fp64(rv, q64, m.ior, valueFp64);
 }
 
+// ---- BSDF property hooks (the sampling test of Tests/Scene/Material/BSDFTests.cpp restated on the
+// shared BSDF; the checks themselves live in tests/test_core_properties_cpu.py).
+//
+// kind 0: FrostbiteDiffuseBRDF alone, albedo 1, roughness params[0]
+// kind 1: SpecularMicrofacetBRDF alone, albedo 1, GGX alpha params[0]
+// kind 2: StandardBSDF of the opaque metal-rough material baseColor params[0] (grey), roughness
+//         params[1], metallic params[2], ior params[3], all lobes (lobe mask 0)
+static StandardBSDF test_bsdf(uint32_t kind, const float* params, f3 wi)
+{
+    StandardBSDF b;
+    memset(&b, 0, sizeof(b));
+    if (kind == 0)
+    {
+        b.diffAlbedo = mk3(1.f); b.diffRoughness = params[0];
+        b.pDiffuseReflection = 1.f;
+    }
+    else if (kind == 1)
+    {
+        b.specAlbedo = mk3(1.f); b.alpha = params[0];
+        b.pSpecularReflection = 1.f;
+    }
+    else
+    {
+        MaterialData m;
+        memset(&m, 0, sizeof(m));
+        m.baseColor[0] = m.baseColor[1] = m.baseColor[2] = params[0];
+        m.roughness = params[1]; m.metallic = params[2]; m.ior = params[3];
+        b = make_bsdf(wi, setup_material(m, true), 0u);
+    }
+    return b;
+}
+
+// n samples of the BSDF for incident direction wi (local frame, normal +z), drawn from the PCG32
+// streams of pixels (0, seed) .. : wo[3n], pdf[n], weight[3n], valid[n], lobe[n].
+__attribute__((visibility("default"))) void ro_test_bsdf_sample(uint32_t kind, const float* params, const float* wi3, uint32_t n, uint32_t seed,
+                                                               float* wo, float* pdf, float* weight, uint32_t* valid, uint32_t* lobe)
+{
+    const f3 wi = normalize(mk3(wi3[0], wi3[1], wi3[2]));
+    const StandardBSDF b = test_bsdf(kind, params, wi);
+    const uint32_t chunk = 4096;
+    #pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t c = 0; c < (int64_t)((n + chunk - 1) / chunk); c++)
+    {
+        SampleGen sg = sg_create((uint32_t)c, seed, 12345u, kSgPCG32);
+        for (uint32_t i = (uint32_t)c * chunk; i < n && i < (uint32_t)(c + 1) * chunk; i++)
+        {
+            f3 w, wt; float p; uint32_t lt;
+            valid[i] = bsdf_sample_local(b, wi, w, p, wt, lt, sg) ? 1u : 0u;
+            wo[3 * i] = w.x; wo[3 * i + 1] = w.y; wo[3 * i + 2] = w.z;
+            weight[3 * i] = wt.x; weight[3 * i + 1] = wt.y; weight[3 * i + 2] = wt.z;
+            pdf[i] = p; lobe[i] = lt;
+        }
+    }
+}
+
+// eval (value * cos, as the BSDF returns it) and evalPdf of n direction pairs: value[3n], pdf[n].
+__attribute__((visibility("default"))) void ro_test_bsdf_eval(uint32_t kind, const float* params, const float* wi3, const float* wo3, uint32_t n,
+                                                             float* value, float* pdf)
+{
+    #pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < (int64_t)n; i++)
+    {
+        const f3 wi = mk3(wi3[3 * i], wi3[3 * i + 1], wi3[3 * i + 2]);
+        const f3 wo = mk3(wo3[3 * i], wo3[3 * i + 1], wo3[3 * i + 2]);
+        const StandardBSDF b = test_bsdf(kind, params, wi);
+        const f3 v = bsdf_eval_local(b, wi, wo);
+        value[3 * i] = v.x; value[3 * i + 1] = v.y; value[3 * i + 2] = v.z;
+        pdf[i] = bsdf_pdf_local(b, wi, wo);
+    }
+}
+
+// The sampling histograms of BSDFTests.cs.slang: sampled directions binned by (cos theta, phi)
+// (hist[cosBins * phiBins], samples within 1e-3 of the poles skipped), the pdf integrated over each
+// bin with binSamples^2 midpoint samples times the sample count (expected[...]), and the largest
+// relative error of the sample weight against eval / evalPdf and of the sample pdf against evalPdf
+// (maxErr[0], maxErr[1]).
+__attribute__((visibility("default"))) void ro_test_bsdf_histogram(uint32_t kind, const float* params, const float* wi3, uint32_t sampleCount,
+                                                                  uint32_t phiBins, uint32_t cosBins, uint32_t binSamples, uint32_t seed,
+                                                                  double* hist, double* expected, double* maxErr)
+{
+    const f3 wi = normalize(mk3(wi3[0], wi3[1], wi3[2]));
+    const StandardBSDF b = test_bsdf(kind, params, wi);
+    const double kCosThetaMargin = 1e-3;
+    const uint32_t bins = phiBins * cosBins;
+    const uint32_t chunk = 1u << 16;
+    const int64_t chunks = (sampleCount + chunk - 1) / chunk;
+    std::vector<std::vector<double>> part(omp_get_max_threads(), std::vector<double>(bins, 0.0));
+    std::vector<double> wErr(omp_get_max_threads(), 0.0), pErr(omp_get_max_threads(), 0.0);
+    #pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t c = 0; c < chunks; c++)
+    {
+        const int t = omp_get_thread_num();
+        SampleGen sg = sg_create((uint32_t)c, seed, 777u, kSgPCG32);
+        for (uint32_t i = (uint32_t)c * chunk; i < sampleCount && i < (uint32_t)(c + 1) * chunk; i++)
+        {
+            f3 wo, wt; float p; uint32_t lt;
+            if (!bsdf_sample_local(b, wi, wo, p, wt, lt, sg)) continue;
+            const f3 value = bsdf_eval_local(b, wi, wo);
+            const float pdfRef = bsdf_pdf_local(b, wi, wo);
+            const f3 wRef = pdfRef > 0.f ? value / pdfRef : mk3(0.f);
+            const double e = std::max({std::fabs(wt.x - wRef.x) / (wRef.x > 0.f ? wRef.x : 1.f),
+                                       std::fabs(wt.y - wRef.y) / (wRef.y > 0.f ? wRef.y : 1.f),
+                                       std::fabs(wt.z - wRef.z) / (wRef.z > 0.f ? wRef.z : 1.f)});
+            wErr[t] = std::max(wErr[t], e);
+            pErr[t] = std::max(pErr[t], (double)std::fabs(p - pdfRef) / (pdfRef > 0.f ? pdfRef : 1.0));
+            if (wo.z < -1.0 + kCosThetaMargin || wo.z > 1.0 - kCosThetaMargin) continue;
+            const uint32_t cb = std::min(cosBins - 1, (uint32_t)std::floor(((double)wo.z * 0.5 + 0.5) * cosBins));
+            double sp = std::atan2((double)wo.y, (double)wo.x) / (2.0 * M_PI);
+            if (sp < 0.0) sp += 1.0;
+            const uint32_t pb = std::min(phiBins - 1, (uint32_t)std::floor(sp * phiBins));
+            part[t][cb * phiBins + pb] += 1.0;
+        }
+    }
+    for (uint32_t k = 0; k < bins; k++)
+    {
+        double s = 0.0;
+        for (auto& v : part) s += v[k];
+        hist[k] = s;
+    }
+    maxErr[0] = *std::max_element(wErr.begin(), wErr.end());
+    maxErr[1] = *std::max_element(pErr.begin(), pErr.end());
+    #pragma omp parallel for schedule(dynamic, 4)
+    for (int64_t k = 0; k < (int64_t)bins; k++)
+    {
+        const uint32_t cb = (uint32_t)k / phiBins, pb = (uint32_t)k % phiBins;
+        const double phi0 = pb * 2.0 * M_PI / phiBins, phi1 = (pb + 1) * 2.0 * M_PI / phiBins;
+        const double c0 = std::max(-1.0 + cb * 2.0 / cosBins, -1.0 + kCosThetaMargin);
+        const double c1 = std::min(-1.0 + (cb + 1) * 2.0 / cosBins, 1.0 - kCosThetaMargin);
+        double acc = 0.0;
+        for (uint32_t ix = 0; ix < binSamples; ix++)
+            for (uint32_t iy = 0; iy < binSamples; iy++)
+            {
+                const double phi = phi0 + (phi1 - phi0) * (ix + 0.5) / binSamples;
+                const double ct = c0 + (c1 - c0) * (iy + 0.5) / binSamples;
+                const double st = std::sqrt(std::max(0.0, 1.0 - ct * ct));
+                const f3 wo = normalize(mk3((float)(st * std::cos(phi)), (float)(st * std::sin(phi)), (float)ct));
+                acc += bsdf_pdf_local(b, wi, wo);
+            }
+        expected[k] = acc * (c1 - c0) * (phi1 - phi0) / ((double)binSamples * binSamples) * sampleCount;
+    }
+}
+
+// Emissive NEE at shading point posW of the pass's light collection: n draws of
+// sample_emissive_power from PCG32 streams, each with the triangle picked, the sample's pdf, the
+// eval_emissive_pdf of the sampled point and the sampled position (tri[n], pdf[n], evalPdf[n],
+// pos[3n]; pdf = 0 for a sample rejected because the triangle faces away).
+__attribute__((visibility("default"))) int ro_test_emissive(ro_pass* r, const float* posW3, uint32_t n, uint32_t seed, uint32_t* tri, float* pdf,
+                                                           float* evalPdf, float* pos)
+{
+    const LightView& L = r->p.lv;
+    if (!L.count) return RS_NOT_READY;
+    const f3 x = mk3(posW3[0], posW3[1], posW3[2]);
+    #pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < (int64_t)n; i++)
+    {
+        // one stream per sample; pixel coordinates carry 16 bits each (interleave_32bit)
+        SampleGen sg = sg_create((uint32_t)i & 0xffffu, ((uint32_t)i >> 16) + (seed << 8), 99u, kSgPCG32);
+        TriangleLightSample ls;
+        ls.triangleIndex = kInvalidIndex;
+        const bool ok = sample_emissive_power(L, x, sg, ls);
+        tri[i] = ls.triangleIndex;
+        if (ok)
+        {
+            pdf[i] = ls.pdf;
+            evalPdf[i] = eval_emissive_pdf(L, x, ls.triangleIndex, ls.posW, ls.normalW);
+            pos[3 * i] = ls.posW.x; pos[3 * i + 1] = ls.posW.y; pos[3 * i + 2] = ls.posW.z;
+        }
+        else
+        {
+            pdf[i] = 0.f; evalPdf[i] = 0.f;
+            pos[3 * i] = pos[3 * i + 1] = pos[3 * i + 2] = 0.f;
+        }
+    }
+    return RS_OK;
+}
+// The light collection's records: per light 20 floats (p0, sceneTri bits, p1, area, p2, flux,
+// normal, materialID bits, Le, 0); returns the count.
+__attribute__((visibility("default"))) uint32_t ro_test_lights(ro_pass* r, float* out)
+{
+    const auto& v = r->p.scene.lights;
+    if (out) memcpy(out, v.data(), v.size() * sizeof(LightTriangle));
+    return (uint32_t)v.size();
+}
+
+// Camera basis (Camera.cpp:179-185) of cam: out = cameraU, cameraV, cameraW (9 floats).
+__attribute__((visibility("default"))) void ro_test_camera_basis(const rs_camera* cam, float* out)
+{
+    CameraData d;
+    memset(&d, 0, sizeof(d));
+    d.posW = mk3(cam->position[0], cam->position[1], cam->position[2]);
+    d.target = mk3(cam->target[0], cam->target[1], cam->target[2]);
+    d.up = mk3(cam->up[0], cam->up[1], cam->up[2]);
+    d.focalLength = cam->focalLength; d.frameHeight = cam->frameHeight; d.aspectRatio = cam->aspectRatio;
+    d.focalDistance = cam->focalDistance;
+    camera_update_basis(d);
+    const f3 v[3] = {d.cameraU, d.cameraV, d.cameraW};
+    for (int k = 0; k < 3; k++) { out[3 * k] = v[k].x; out[3 * k + 1] = v[k].y; out[3 * k + 2] = v[k].z; }
+}
+
+// orientCamera (CameraManager.slang:90-113) of cam over K keyframes (positions[3K], targets[3K]) at
+// frameCount and time: out = posW, cameraU, cameraV, cameraW (12 floats).
+__attribute__((visibility("default"))) void ro_test_orient_camera(const rs_camera* cam, uint32_t K, const float* positions, const float* targets,
+                                                                 float artificialFrameTime, uint32_t frameCount, float time, float* out)
+{
+    CameraData d;
+    memset(&d, 0, sizeof(d));
+    d.posW = mk3(cam->position[0], cam->position[1], cam->position[2]);
+    d.target = mk3(cam->target[0], cam->target[1], cam->target[2]);
+    d.up = mk3(cam->up[0], cam->up[1], cam->up[2]);
+    d.focalLength = cam->focalLength; d.frameHeight = cam->frameHeight; d.aspectRatio = cam->aspectRatio;
+    d.focalDistance = cam->focalDistance;
+    camera_update_basis(d);
+    CameraManager cm;
+    memset(&cm, 0, sizeof(cm));
+    cm.artificialFrameTime = artificialFrameTime;
+    cm.keyframes = K;
+    for (uint32_t i = 0; i < K; i++)
+    {
+        cm.positions[i] = mk3(positions[3 * i], positions[3 * i + 1], positions[3 * i + 2]);
+        cm.targets[i] = mk3(targets[3 * i], targets[3 * i + 1], targets[3 * i + 2]);
+    }
+    orient_camera(cm, d, frameCount, time);
+    const f3 v[4] = {d.posW, d.cameraU, d.cameraV, d.cameraW};
+    for (int k = 0; k < 4; k++) { out[3 * k] = v[k].x; out[3 * k + 1] = v[k].y; out[3 * k + 2] = v[k].z; }
+}
+
 // Closest hit of one ray against the oracle's BVH of a triangle soup (prim = -1 on a miss).
 __attribute__((visibility("default"))) int ro_test_closest(ro_pass* r, const float* ray, float* tuv)
 {

@@ -120,8 +120,8 @@ class ReservoirSplatting:
             pass
 
     # ---- reference-facing API
-    def set_properties(self, props: dict):
-        self.options = abi.options_from_properties(props, self.width, self.height)
+    def set_properties(self, props: dict, width: int | None = None, height: int | None = None):
+        self.options = abi.options_from_properties(props, width or self.width, height or self.height)
         _check(self._lib.rs_set_options(self._h, C.byref(self.options)))
         self.width, self.height = self.options.frameWidth, self.options.frameHeight
 
@@ -161,12 +161,13 @@ class ReservoirSplatting:
         _check(self._lib.rs_freeze(self._h, 1 if frozen else 0))
 
     def execute(self, camera, color_ptr: int | None = None, color_host: np.ndarray | None = None, stream: int = 0,
-                mvec_ptr: int | None = None, should_reset: bool = False):
-        """Renders one frame.  `color_ptr` is a device float4[W*H]; or pass `color_host` (float32 [H, W, 4])."""
+                mvec_ptr: int | None = None, vbuffer_ptr: int | None = None, should_reset: bool = False):
+        """Renders one frame.  `color_ptr` is a device float4[W*H]; or pass `color_host` (float32 [H, W, 4]).
+        `mvec_ptr` / `vbuffer_ptr` are the optional device inputs (float2 / uint4 per pixel)."""
         f = abi.RsFrameDesc()
         f.camera = abi.camera_struct(camera)
         f.mvec = mvec_ptr or None
-        f.vbuffer = None
+        f.vbuffer = vbuffer_ptr or None
         f.color = color_ptr or None
         if color_host is not None:
             assert color_host.dtype == np.float32 and color_host.flags.c_contiguous and color_host.size == 4 * self.width * self.height

@@ -165,6 +165,10 @@ struct rs_pass
     bool lastFusedCollect = false;
     cudaStream_t lastStream = 0;
     uint32_t launches = 0;
+    // Bumped by every call that can reallocate a buffer or change which kernels a frame launches
+    // (options, scene, env map, candidate snapshots, geometry updates): a batch graph captured
+    // under an older generation holds stale pointers, grids or kernel choices and is not replayed.
+    uint64_t generation = 0;
     // stage timing
     bool timing = false;
     std::vector<std::string> stageNames;
@@ -373,6 +377,7 @@ extern "C" RS_API rs_status rs_set_options(rs_pass* p, const rs_options* opts)
     s = allocate(p);
     if (s != RS_OK) return s;
     if (resized) p->frameCount = 0;
+    p->generation++;
     return RS_OK;
 }
 
@@ -408,6 +413,7 @@ extern "C" RS_API rs_status rs_set_scene(rs_pass* p, const rs_scene_desc* sd)
     p->hostTriStale = false;
     p->geometryMoved = false;
     p->frameCount = 0; // setScene resets the frame count (ReservoirSplatting.cpp:380)
+    p->generation++;
     return RS_OK;
 }
 
@@ -445,6 +451,7 @@ extern "C" RS_API rs_status rs_set_env_map(rs_pass* p, const rs_env_map* m)
     }
     else RS_CUDA(cudaDeviceSynchronize());
     p->envHost = v;
+    p->generation++;
     RS_CUDA(cudaMemcpy(p->envView.p, &p->envHost, sizeof(EnvMapView), cudaMemcpyHostToDevice));
     return RS_OK;
 }
@@ -592,7 +599,7 @@ static void end_frame(rs_pass* p)
 // slot by a stream-ordered copy from pinned memory: in graph mode from p->graphCtx (a replayed graph
 // reads the context current at replay time), otherwise from a ring entry that is not reused until
 // its copy has run.
-static rs_status enqueue_frame(rs_pass* p, cudaStream_t s, float4* colorDev, const float2* mvecIn, bool graphMode)
+static rs_status enqueue_frame(rs_pass* p, cudaStream_t s, float4* colorDev, const float2* mvecIn, const uint4* vbufIn, bool graphMode)
 {
     const bool env = p->envHost.present != 0; // which variant of the env-dependent kernels runs
     const uint32_t W = p->W, H = p->H;
@@ -619,7 +626,10 @@ static rs_status enqueue_frame(rs_pass* p, cudaStream_t s, float4* colorDev, con
     RS_CUDA(cudaMemsetAsync(p->fault.p, 0, sizeof(uint32_t), s));
     k_camera_table<<<1, kMaxCameraKeyframes, 0, s>>>(C, p->camTable.p); p->launches++;
 
+    // the caller's motion vectors and primary hits (the pass's mvec / vbuffer inputs) replace the
+    // pass's own; k_vbuffer computes whichever of the two is missing
     const float2* mvec = mvecIn ? mvecIn : p->mvec.p;
+    const uint4* vbuf = vbufIn ? vbufIn : p->vbuffer.p;
     if (p->keepCandidates) RS_CUDA(p->cand.ensure(N));
     shouldReset = shouldReset || p->frameCount == 0;
     const bool temporal = o.enableTemporalResampling && !shouldReset;
@@ -644,8 +654,11 @@ static rs_status enqueue_frame(rs_pass* p, cudaStream_t s, float4* colorDev, con
     // before the first kernel that reads two of them.
     cudaStream_t q[3];
     fork_streams(p, s, 3, q);
-    stage(p, "vbuffer", q[0]);
-    k_vbuffer<<<tiled_blocks(W, H, 256), 256, 0, q[0]>>>(C, p->vbuffer.p, p->mvec.p); p->launches++;
+    if (!(mvecIn && vbufIn))
+    {
+        stage(p, "vbuffer", q[0]);
+        k_vbuffer<<<tiled_blocks(W, H, 256), 256, 0, q[0]>>>(C, p->vbuffer.p, p->mvec.p); p->launches++;
+    }
     stage(p, "initialCandidates", q[1]);
     if (o.samplesPerPixel == 1) RS_ENV_LAUNCH(env, k_candidates_direct, tiled_blocks(W, H, 128), 128, q[1], C, curr.res(), curr.recp());
     else RS_ENV_LAUNCH(env, k_candidates, grid(N, 128), 128, q[1], C, curr.res(), curr.recp());
@@ -723,7 +736,7 @@ static rs_status enqueue_frame(rs_pass* p, cudaStream_t s, float4* colorDev, con
                 break;
             }
             stage(p, "gatherResample", s);
-            RS_ENV_LAUNCH(env, k_gather_resample, tiled_blocks(W, H, 128), 128, s, C, p->vbuffer.p, curr.res(), curr.recp(), p->inter.res(), p->inter.recp(), p->floatingCoords.p, temporalColor); p->launches++;
+            RS_ENV_LAUNCH(env, k_gather_resample, tiled_blocks(W, H, 128), 128, s, C, vbuf, curr.res(), curr.recp(), p->inter.res(), p->inter.recp(), p->floatingCoords.p, temporalColor); p->launches++;
             break;
         case RS_SCATTER_ONLY:
         {
@@ -836,7 +849,7 @@ static rs_status enqueue_frame(rs_pass* p, cudaStream_t s, float4* colorDev, con
             ReservoirSet& dst = p->sets[cur];
             SpatialCtx S;
             S.iteration = i;
-            S.vbuffer = p->vbuffer.p;
+            S.vbuffer = vbuf;
             S.neighborOffsets = p->neighborOffsets.p;
             S.src = src.res(); S.srcRec = src.recp();
             S.dst = dst.res(); S.dstRec = dst.recp();
@@ -888,7 +901,7 @@ extern "C" RS_API rs_status rs_execute(rs_pass* p, const rs_frame_desc* f, void*
         colorDev = p->scratchColor.p;
     }
     begin_frame(p, f);
-    rs_status st = enqueue_frame(p, s, colorDev, reinterpret_cast<const float2*>(f->mvec), false);
+    rs_status st = enqueue_frame(p, s, colorDev, reinterpret_cast<const float2*>(f->mvec), reinterpret_cast<const uint4*>(f->vbuffer), false);
     if (st != RS_OK) return st;
     if (f->colorHost)
     {
@@ -1357,6 +1370,7 @@ extern "C" RS_API rs_status rs_debug_keep_candidates(rs_pass* p, uint32_t keep)
 {
     if (!p) return fail(RS_INVALID_ARG, "pass is NULL");
     p->keepCandidates = keep != 0;
+    p->generation++;
     return RS_OK;
 }
 
@@ -1375,8 +1389,9 @@ struct rs_batch
     cudaEvent_t fork = nullptr, done = nullptr;
     cudaStream_t capture = nullptr;
     bool inFlight = false;
-    struct Cached { std::vector<uint32_t> key; std::vector<void*> colors; cudaGraphExec_t exec; };
+    struct Cached { std::vector<uint64_t> key; std::vector<void*> colors; cudaGraphExec_t exec; };
     std::vector<Cached> graphs;
+    std::vector<uint64_t> generations; // the members' generations when the cached graphs were captured
     uint32_t lastLaunches = 0;
     ~rs_batch()
     {
@@ -1430,8 +1445,8 @@ extern "C" RS_API rs_status rs_batch_execute(rs_batch* b, const rs_frame_desc* f
         if (!frames[i].color) return fail(RS_INVALID_ARG, "batched frames need device colour buffers");
     // the previous replay reads the pinned host contexts; wait for it before rewriting them
     if (b->inFlight) RS_CUDA(cudaEventSynchronize(b->done));
-    std::vector<uint32_t> key(n);
-    std::vector<void*> colors(n);
+    std::vector<uint64_t> key(n);
+    std::vector<void*> colors(3 * n); // colour, mvec and vbuffer pointers: the graph holds them
     for (size_t i = 0; i < n; i++)
     {
         rs_pass* p = b->passes[i];
@@ -1439,12 +1454,29 @@ extern "C" RS_API rs_status rs_batch_execute(rs_batch* b, const rs_frame_desc* f
         *p->graphCtx = *p->hostCtx;
         p->lastStream = s;
         p->stageNames.clear();
-        colors[i] = frames[i].color;
-        // the graph depends on the ping-pong buffers in use, on whether temporal stages run and on
-        // which kernel variants run (with or without the environment light)
-        key[i] = (uint32_t)p->currIdx * 3u + (uint32_t)p->prevIdx + 9u * (p->frameCount == 0 || frames[i].sceneShouldReset ? 1u : 0u) +
-                 18u * (p->envHost.present ? 1u : 0u);
+        colors[3 * i] = frames[i].color;
+        colors[3 * i + 1] = const_cast<float*>(frames[i].mvec);
+        colors[3 * i + 2] = const_cast<uint32_t*>(frames[i].vbuffer);
+        // the graph depends on the ping-pong buffers in use, on whether temporal stages run, on
+        // which kernel variants run (environment light, depth of field in the gather) and on the
+        // pass's buffers and options (its generation)
+        const uint32_t shape = (uint32_t)p->currIdx * 3u + (uint32_t)p->prevIdx + 9u * (p->frameCount == 0 || frames[i].sceneShouldReset ? 1u : 0u) +
+                               18u * (p->envHost.present ? 1u : 0u) + 36u * (p->camera.apertureRadius > 0.f ? 1u : 0u);
+        key[i] = (p->generation << 8) | shape;
     }
+    // a member whose buffers or options changed makes every graph of the older generation stale
+    if (!b->graphs.empty() && b->generations.size() == n)
+    {
+        bool changed = false;
+        for (size_t i = 0; i < n; i++) changed = changed || b->generations[i] != b->passes[i]->generation;
+        if (changed)
+        {
+            for (auto& g : b->graphs) cudaGraphExecDestroy(g.exec);
+            b->graphs.clear();
+        }
+    }
+    b->generations.resize(n);
+    for (size_t i = 0; i < n; i++) b->generations[i] = b->passes[i]->generation;
     cudaGraphExec_t exec = nullptr;
     for (auto& g : b->graphs)
         if (g.key == key && g.colors == colors) { exec = g.exec; break; }
@@ -1462,7 +1494,8 @@ extern "C" RS_API rs_status rs_batch_execute(rs_batch* b, const rs_frame_desc* f
             bool timing = p->timing;
             p->timing = false;
             p->launches = 0;
-            st = enqueue_frame(p, b->branch[i], reinterpret_cast<float4*>(frames[i].color), nullptr, true);
+            st = enqueue_frame(p, b->branch[i], reinterpret_cast<float4*>(frames[i].color), reinterpret_cast<const float2*>(frames[i].mvec),
+                               reinterpret_cast<const uint4*>(frames[i].vbuffer), true);
             p->timing = timing;
             launches += p->launches;
             cudaEventRecord(b->joins[i], b->branch[i]);

@@ -48,3 +48,44 @@ def test_batch_matches_individual_passes(rs, scenes, env_frame):
             np.testing.assert_array_equal(batched[k].get_buffer("curr_reservoirs"), solo[k].get_buffer("curr_reservoirs"))
     assert batch.launch_count() > 0
     batch.close()
+
+
+@pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
+def test_batch_member_changes_options_size_and_aperture(rs, scenes):
+    """A member's options and frame size change between two batch calls (rs_set_options
+    reallocates its buffers), and another member's camera opens its aperture (the gather switches to
+    its depth-of-field kernel): the batch must capture new graphs, not replay the stale ones, and
+    still match the passes rendered on their own."""
+    import torch
+    cfgs = [
+        (scenes.cornell_box(0), {"temporalReuse": "ScatterBackup", "gatherOption": "Clamped", "maxSurfaceBounces": 1}, 40, 32),
+        (scenes.cornell_box(1), {"temporalReuse": "GatherOnly", "gatherOption": "Fast", "maxSurfaceBounces": 1}, 32, 24),
+    ]
+    solo, batched = [], []
+    for sc, props, w, h in cfgs:
+        a = rs.ReservoirSplatting(props, w, h); a.set_scene(sc); solo.append(a)
+        b = rs.ReservoirSplatting(props, w, h); b.set_scene(sc); batched.append(b)
+    sizes = [(w, h) for _, _, w, h in cfgs]
+    batch = rs.Batch(batched)
+    stream = torch.cuda.current_stream().cuda_stream
+    new_props = {"temporalReuse": "ScatterOnly", "enableSpatialResampling": False, "maxSurfaceBounces": 2}
+    for f in range(8):
+        if f == 3:  # member 0: new mode and a new size
+            sizes[0] = (24, 40)
+            solo[0].set_properties(new_props, *sizes[0])
+            batched[0].set_properties(new_props, *sizes[0])
+        outs = [torch.zeros((h, w, 4), dtype=torch.float32, device="cuda") for w, h in sizes]
+        cams = []
+        for k, (w, h) in enumerate(sizes):
+            c = scenes.cornell_camera(f, w, h)
+            if k == 1 and f >= 5:
+                c.aperture_radius = 0.02
+            cams.append(c)
+        ref = [p.render(c) for p, c in zip(solo, cams)]
+        batch.execute(cams, [o.data_ptr() for o in outs], stream=stream)
+        torch.cuda.synchronize()
+        for k in range(len(cfgs)):
+            np.testing.assert_array_equal(outs[k].cpu().numpy(), ref[k], err_msg=f"instance {k} frame {f}")
+    batch.close()
+    for p in solo + batched:
+        p.close()

@@ -13,6 +13,7 @@ pytestmark = pytest.mark.gpu
 
 W = H = 64
 FRAMES = 5
+run_pair = P.run_pair
 
 
 def _cuda_ok():
@@ -21,41 +22,6 @@ def _cuda_ok():
         return torch.cuda.is_available()
     except Exception:
         return False
-
-
-def run_pair(rs, oracle_mod, scene, camera_fn, props, frames=FRAMES, width=W, height=H, shutter=0.0, aperture=0.0,
-             check_candidates=True, builder="PLOC"):
-    gpu = rs.ReservoirSplatting(props, width, height)
-    gpu.set_bvh_builder(builder)
-    gpu.keep_candidates(True)
-    ora = oracle_mod.OraclePass(props, width, height)
-    gpu.set_scene(scene)
-    ora.set_scene(scene)
-    mode = gpu.options.temporalReuse
-    report = {}
-    for f in range(frames):
-        cam = camera_fn(f, width, height)
-        cam.shutter_speed = shutter
-        cam.aperture_radius = aperture
-        img_g = gpu.render(cam)
-        img_o = ora.execute(cam)
-        P.assert_equal(f"frame{f}.vbuffer", gpu.get_buffer("vbuffer"), ora.get_buffer("vbuffer"))
-        P.assert_equal(f"frame{f}.mvec", gpu.get_buffer("mvec").view(np.uint32), ora.get_buffer("mvec").view(np.uint32))
-        if check_candidates:
-            P.compare_reservoirs(f"frame{f}.candidates", gpu.get_buffer("candidate_reservoirs"), ora.get_buffer("candidate_reservoirs"))
-            P.compare_recon(f"frame{f}.candidate_recon", gpu.get_buffer("candidate_reconnection"), ora.get_buffer("candidate_reconnection"))
-        if f > 0 and mode in (1, 2):  # ScatterOnly / ScatterBackup: the splat cell lists
-            P.assert_equal(f"frame{f}.splat_targets", gpu.get_buffer("splat_targets"), ora.get_buffer("splat_targets"))
-            P.assert_equal(f"frame{f}.cell_counters", gpu.get_buffer("cell_counters"), ora.get_buffer("cell_counters"))
-            P.assert_equal(f"frame{f}.cell_offsets", gpu.get_buffer("cell_offsets"), ora.get_buffer("cell_offsets"))
-            P.assert_equal(f"frame{f}.sorted_splats", gpu.get_buffer("sorted_splats"), ora.get_buffer("sorted_splats"))
-            report["splats"] = int(gpu.get_buffer("cell_counters").sum())
-        P.compare_reservoirs(f"frame{f}.reservoirs", gpu.get_buffer("curr_reservoirs"), ora.get_buffer("curr_reservoirs"))
-        P.compare_recon(f"frame{f}.reconnection", gpu.get_buffer("curr_reconnection"), ora.get_buffer("curr_reconnection"))
-        P.assert_close(f"frame{f}.color", img_g, img_o)
-        report[f"bits{f}"] = P.bit_mismatch_fraction(img_g, img_o)
-    gpu.close()
-    return report, img_g
 
 
 MODES = [
