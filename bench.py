@@ -129,7 +129,7 @@ STAGE_BYTES_PER_PIXEL = {
     "sortCells": 4 * 8,
 }
 STAGE_KERNEL = {"initialCandidates": "k_candidates_direct", "sbCombine": "k_sb_combine", "sbBackupScatter": "k_sb_backup_scatter",
-                "spatialNeighbor": "k_sp_neighbor", "sortCells": "k_rank_cells"}
+                "spatialNeighbor": "k_sp_neighbor", "sortCells": "k_rsort_scatter"}
 
 
 def measured_traffic():
@@ -231,27 +231,34 @@ def run_ours(args):
     p.enable_stage_timing(False)
     torch.cuda.synchronize()
 
-    # end to end through the public API: colour copied to pinned host memory every frame
+    # end to end through the public API, colour copied to pinned host memory every frame, over the
+    # same frames as `value`: the pass restarts (rs_reset: frame count and seed), renders the same
+    # warm-up frames and then the same timed frames, so both numbers time identical work
     host = torch.empty((H, W, 4), dtype=torch.float32, pin_memory=True)
     host_np = host.numpy()
-    e2e_steps = max(3, min(args.steps, 10))
+    p.reset()
+    frame = 0
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step(color.data_ptr())
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with torch.cuda.stream(stream):
         e0.record(stream)
-        for _ in range(e2e_steps):
+        for _ in range(args.steps):
             step(None, host_np)
         e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(e0.elapsed_time(e1), dist, dev)
-    e2e_value = world * e2e_steps / (e2e_ms / 1e3)
+    e2e_value = world * args.steps / (e2e_ms / 1e3)
 
     quality = None
     if rank == 0 and not args.no_quality:
         with torch.cuda.stream(stream):
-            quality = measure_quality(args, torch, rs, scene, camera(frame - 1 + rank_frame_offset(rank), W, H), host_np, W, H, stream)
+            cams = [camera(f + rank_frame_offset(rank), W, H) for f in range(frame)]
+            quality = measure_quality(args, torch, rs, scene, cams, torch.from_numpy(host_np), PROPS, W, H, stream)
 
     peak, peak_kind = _peaks()
     traffic = measured_traffic()
@@ -268,10 +275,7 @@ def run_ours(args):
             "metric": METRIC, "value": round(value, 3), "unit": "frames/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
-            "config": {"workload": "terrain512+500 icospheres(subdiv4)+64 emissive tris = %d tris, 1920x1080, ScatterBackup/Clamped/Balance, "
-                                   "path length 4, spatial reuse on, orbit 0.5 deg/frame" % scene.num_triangles,
-                       "resolution": [W, H], "triangles": scene.num_triangles, "parallelism": "replicas" if world > 1 else "single",
-                       "l2": "per-frame working set (3 x 144 B/pixel reservoir sets + 348 MB BVH) exceeds the 126 MB L2"},
+            "config": bench_config(scene.num_triangles, world, args),
             "e2e": {"value": round(e2e_value, 3), "unit": "frames/s", "h2d_bytes_per_step": int(C_frame_bytes()),
                     "d2h_bytes_per_step": int(W * H * 16)},
             "gpu_launches": int(launches),
@@ -289,43 +293,59 @@ def run_ours(args):
         if world == 1 and not args.no_adjoint:
             line["adjoint"] = run_adjoint(args, torch, rs, stream)
         if world == 1 and not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline(args, quiet=True)
+            cb = cpu_baseline(args, quiet=True)
+            cb.pop("triangles", None)
+            line["cpu_baseline"] = cb
         print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
 
 
-def measure_quality(args, torch, rs, scene, cam, image, W, H, stream):
-    """Error of the last rendered frame against an FP64 ground truth of the same camera.
+def measure_quality(args, torch, rs, scene, cams, image, props, W, H, stream, before_frame=None, spp=None, setup=None):
+    """Error of a rendered frame against an FP64 ground truth of the same frame.
 
-    The ground truth accumulates, in FP64 on the device, `gt_spp` frames of the pass with temporal
-    and spatial reuse off: each such frame is the initial-candidate estimate alone, an unbiased
-    one-path-per-pixel estimate, with its own seed.  Its first frame is also reported as the
-    one-path path-tracing baseline.  The ground truth's own noise (variance of the mean) is about
-    mse_1spp / gt_spp and is reported beside the numbers."""
-    props = dict(PROPS, enableTemporalResampling=False, enableSpatialResampling=False)
-    gt_pass = rs.ReservoirSplatting(props, W, H)
+    `cams` are the cameras of frames 0..f; `image` (float32 [H, W, 4], host or device) is frame f of
+    the measured pass.  The ground-truth pass (same options with temporal and spatial reuse off, so
+    each frame is the initial-candidate estimate alone: an unbiased one-path-per-pixel estimate)
+    renders frames 0..f-1 to fill the same camera-keyframe ring (the shutter interpolates between
+    those cameras), is frozen at frame f and accumulates `spp` renders of it in FP64, each with its
+    own seed.  `before_frame(pass, f)` moves the geometry of frame f (moving scenes); `setup(pass)`
+    adds what the scene lacks (an environment map).  The first
+    accumulated render is also reported as the one-path path-tracing baseline; the ground truth's own
+    noise (variance of the mean) is about mse_1spp / spp."""
+    spp = spp or args.gt_spp
+    gprops = dict(props, enableTemporalResampling=False, enableSpatialResampling=False)
+    gt_pass = rs.ReservoirSplatting(gprops, W, H)
     gt_pass.set_scene(scene)
+    if setup:
+        setup(gt_pass)
     col = torch.empty((H, W, 4), dtype=torch.float32, device="cuda")
     acc = torch.zeros((H, W, 3), dtype=torch.float64, device="cuda")
+    for f, c in enumerate(cams[:-1]):
+        if before_frame:
+            before_frame(gt_pass, f)
+        gt_pass.execute(c, color_ptr=col.data_ptr(), stream=stream.cuda_stream)
+    if before_frame:
+        before_frame(gt_pass, len(cams) - 1)
+    gt_pass.freeze(True)
     one = None
-    for k in range(args.gt_spp):
-        gt_pass.execute(cam, color_ptr=col.data_ptr(), stream=stream.cuda_stream)
+    for k in range(spp):
+        gt_pass.execute(cams[-1], color_ptr=col.data_ptr(), stream=stream.cuda_stream)
         acc += col[..., :3].double()
         if k == 0:
             one = col[..., :3].double().clone()
     torch.cuda.synchronize()
-    gt = acc / args.gt_spp
-    img = torch.from_numpy(image[..., :3]).cuda().double()
+    gt = acc / spp
+    img = image[..., :3].to(device="cuda", dtype=torch.float64)
     mse = float(((img - gt) ** 2).mean())
     mse1 = float(((one - gt) ** 2).mean())
     rel = lambda a: float((((a - gt) ** 2) / (gt ** 2 + 1e-2)).mean())
     gt_pass.close()
     return {"mse_vs_fp64_gt": mse, "relmse_vs_fp64_gt": rel(img), "mse_1spp_path_tracing": mse1, "relmse_1spp_path_tracing": rel(one),
-            "mse_ratio_1spp_over_restir": round(mse1 / mse, 3) if mse > 0 else None, "gt_spp": args.gt_spp,
-            "gt_noise_mse_estimate": mse1 / args.gt_spp, "gt_mean_radiance": float(gt.mean()),
-            "how": "last timed-configuration frame vs the FP64 mean of gt_spp independent candidate-only frames at the same camera "
-                   "(batched and plain passes run the same kernels per instance and give bit-identical images)"}
+            "mse_ratio_1spp_over_restir": round(mse1 / mse, 3) if mse > 0 else None, "gt_spp": spp,
+            "gt_noise_mse_estimate": mse1 / spp, "gt_mean_radiance": float(gt.mean()), "frame": len(cams) - 1,
+            "how": "the frame vs the FP64 mean of gt_spp independent candidate-only renders of the same frame (same cameras, "
+                   "keyframe ring and geometry; ground-truth pass frozen at that frame)"}
 
 
 BATCH_RESOLUTIONS = [(320, 240), (640, 480), (1280, 720), (1920, 1080)]
@@ -375,9 +395,16 @@ def run_modes(args, torch, rs, scene, stream):
         torch.cuda.synchronize()
         ms = a.elapsed_time(b) / args.mode_frames
         out[name] = {"frames_per_s": round(1000.0 / ms, 3), "ms_per_frame": round(ms, 4)}
+        if not args.no_quality:
+            q = measure_quality(args, torch, rs, scene, [cam(f) for f in range(4 + args.mode_frames)], color,
+                                dict(props, maxSurfaceBounces=2), W, H, stream, spp=args.mode_gt_spp,
+                                setup=(lambda gp: gp.set_env_map(sky)) if name in MODE_ENV else None)
+            out[name].update({k: q[k] for k in ("mse_vs_fp64_gt", "mse_1spp_path_tracing", "mse_ratio_1spp_over_restir",
+                                                "gt_noise_mse_estimate", "gt_spp")})
         p.close()
     out["how"] = (f"1920x1080, the benchmark scene and orbit, path length 4, spatial reuse on; {args.mode_frames} frames "
-                  "after 4 warm-up frames per mode, CUDA events on the launching stream; MultiScatter with shutter 1/24 s and "
+                  "after 4 warm-up frames per mode, CUDA events on the launching stream; MSE of each mode's last frame against "
+                  f"an FP64 ground truth of {args.mode_gt_spp} candidate-only renders of that frame; MultiScatter with shutter 1/24 s and "
                   "artificial frame time 1/48 s on the static scene; '+sky' adds a seeded 1024x512 sky environment light (NEE picks "
                   "sky or emissive triangles with probability 1/2 each)")
     return out
@@ -385,7 +412,8 @@ def run_modes(args, torch, rs, scene, stream):
 
 def batch_instances(count: int, seed: int = 11):
     """Seeded batched workload: resolutions uniform over BATCH_RESOLUTIONS, 10k-500k triangles each
-    from the same generator (terrain grid and sphere count scaled to the triangle target)."""
+    from the same generator at subdivision 4 (about 60% terrain, the rest icospheres of 5,120
+    triangles, at least one)."""
     _package()
     import reservoir_splatting_b200.scenes as S
     rng = np.random.default_rng(seed)
@@ -394,58 +422,102 @@ def batch_instances(count: int, seed: int = 11):
         w, h = BATCH_RESOLUTIONS[int(rng.integers(0, len(BATCH_RESOLUTIONS)))]
         target = int(rng.uniform(10_000, 500_000))
         grid = max(8, int((0.6 * target / 2) ** 0.5))
-        spheres = max(1, int(0.4 * target / 1280))
-        sc = S.terrain_spheres(seed=1000 + i, grid=grid, spheres=spheres, subdiv=3, lights=16)
+        spheres = max(1, int(0.4 * target / 5120))
+        sc = S.terrain_spheres(seed=1000 + i, grid=grid, spheres=spheres, subdiv=4, lights=16)
         out.append((sc, w, h, i))
     return out
 
 
+# ray queries per pixel of a ScatterBackup frame at path length 4 with spatial reuse (counted by the
+# ray-counting build on the benchmark scene: profiles/rays_1080p.md)
+QUERIES_PER_PIXEL = 12.48
+
+
 def run_batched(args, torch, rs, stream, dev):
-    """Plain (each instance's frame launched on its own, back to back) vs batched (one CUDA-graph
-    launch per frame for all instances); device time over the same frames."""
+    """Config "batched": 64 seeded scene/camera instances of uneven resolution, ScatterBackup, 16 timed
+    frames, in three forms over the same frames (every pass restarts its history before each form):
+    plain (rs_execute per instance back to back on one stream), per-member graph branches
+    (rs_batch_execute, flatten off) and the flattened form (rs_batch_execute: one persistent launch
+    per stage over all instances, tile widths and grid forms from rs_batch_tune).  The three render
+    identical images (checked here on every instance's last frame), so their MSE is matched by
+    construction; the MSE of the smallest and largest instance against an FP64 ground truth is
+    reported as well."""
     insts = batch_instances(args.batch_instances)
-    plain = [rs.ReservoirSplatting(PROPS, w, h) for _, w, h, _ in insts]
-    for (sc, _, _, _), a in zip(insts, plain):
+    passes = [rs.ReservoirSplatting(PROPS, w, h) for _, w, h, _ in insts]
+    for (sc, _, _, _), a in zip(insts, passes):
         a.set_scene(sc)
-    batched = plain  # the same passes render both ways (halves the memory of the 64 instances)
     outs = [torch.empty((h, w, 4), dtype=torch.float32, device=dev) for _, w, h, _ in insts]
-    batch = rs.Batch(batched)
     cams = lambda f: [camera(f + 13 * i, w, h) for _, w, h, i in insts]
     ev = lambda: torch.cuda.Event(enable_timing=True)
-
-    def time_frames(fn, first, frames):
-        a, b = ev(), ev()
-        a.record(stream)
-        for f in range(first, first + frames):
-            fn(f)
-        b.record(stream)
-        torch.cuda.synchronize()
-        return a.elapsed_time(b)
+    branch = rs.Batch(passes, flatten=False)
+    flat = rs.Batch(passes, flatten=True)
+    warm, frames = max(2, args.batch_warmup), args.batch_frames
 
     def plain_frame(f):
-        for p, c, o in zip(plain, cams(f), outs):
+        for p, c, o in zip(passes, cams(f), outs):
             p.execute(c, color_ptr=o.data_ptr(), stream=stream.cuda_stream)
 
-    def batch_frame(f):
-        batch.execute(cams(f), [o.data_ptr() for o in outs], stream=stream.cuda_stream)
+    def run_form(name, frame_fn, tune=False):
+        for p in passes:
+            p.reset()
+        torch.cuda.synchronize()
+        with torch.cuda.stream(stream):
+            for f in range(warm):
+                if tune and f == warm - 1:
+                    flat.tune(cams(f), [o.data_ptr() for o in outs], stream=stream.cuda_stream)
+                else:
+                    frame_fn(f)
+            torch.cuda.synchronize()
+            a, b = ev(), ev()
+            a.record(stream)
+            for f in range(warm, warm + frames):
+                frame_fn(f)
+            b.record(stream)
+        torch.cuda.synchronize()
+        last = [o.clone() for o in outs]
+        return a.elapsed_time(b), last
 
-    with torch.cuda.stream(stream):
-        time_frames(plain_frame, 0, args.batch_warmup)
-        time_frames(batch_frame, 0, args.batch_warmup)
-        ms_plain = time_frames(plain_frame, args.batch_warmup, args.batch_frames)
-        ms_batch = time_frames(batch_frame, args.batch_warmup, args.batch_frames)
+    ms_plain, img_plain = run_form("plain", plain_frame)
+    ms_branch, img_branch = run_form("branch", lambda f: branch.execute(cams(f), [o.data_ptr() for o in outs], stream=stream.cuda_stream))
+    ms_flat, img_flat = run_form("flat", lambda f: flat.execute(cams(f), [o.data_ptr() for o in outs], stream=stream.cuda_stream), tune=True)
+    identical = all(bool(torch.equal(x, y)) and bool(torch.equal(x, z)) for x, y, z in zip(img_plain, img_branch, img_flat))
+    flattened = flat.last_flattened()
     n = len(insts)
     pixels = sum(w * h for _, w, h, _ in insts)
     tris = [sc.num_triangles for sc, _, _, _ in insts]
-    res = {"instances": n, "frames": args.batch_frames, "pixels_per_batch_frame": pixels,
-           "triangles_min": min(tris), "triangles_max": max(tris),
-           "plain_instance_frames_per_s": round(n * args.batch_frames / (ms_plain / 1e3), 3),
-           "batched_instance_frames_per_s": round(n * args.batch_frames / (ms_batch / 1e3), 3),
-           "speedup": round(ms_plain / ms_batch, 4), "graph_launch_kernels": batch.launch_count(),
-           "how": "plain: rs_execute per instance back to back on one stream; batched: rs_batch_execute (one CUDA graph, per-instance branches)"}
-    batch.close()
-    for p in plain:
+    rate = lambda ms: n * frames / (ms / 1e3)
+    qps = lambda ms: QUERIES_PER_PIXEL * pixels * frames / (ms / 1e3) / 1e9
+    tuning = flat.tuning()
+    launch_count = flat.launch_count()
+    branch.close()
+    flat.close()
+    for p in passes:
         p.close()
+    quality = {}
+    if not args.no_quality:  # the ground-truth passes need the batch's pass slots back
+        order = sorted(range(n), key=lambda i: insts[i][1] * insts[i][2])
+        for k in (order[0], order[-1]):
+            sc, w, h, i = insts[k]
+            q = measure_quality(args, torch, rs, sc, [camera(f + 13 * i, w, h) for f in range(warm + frames)], img_flat[k], PROPS, w, h,
+                                stream, spp=args.mode_gt_spp)
+            quality[f"instance{k}_{w}x{h}"] = {kk: q[kk] for kk in ("mse_vs_fp64_gt", "mse_1spp_path_tracing", "gt_spp")}
+    res = {"instances": n, "frames": frames, "warmup_frames": warm, "pixels_per_batch_frame": pixels,
+           "resolutions": {f"{w}x{h}": sum(1 for _, ww, hh, _ in insts if (ww, hh) == (w, h)) for w, h in BATCH_RESOLUTIONS},
+           "triangles_min": min(tris), "triangles_max": max(tris),
+           "plain_instance_frames_per_s": round(rate(ms_plain), 3),
+           "branch_graph_instance_frames_per_s": round(rate(ms_branch), 3),
+           "batched_instance_frames_per_s": round(rate(ms_flat), 3),
+           "speedup": round(ms_plain / ms_flat, 4), "speedup_branch_graph": round(ms_plain / ms_branch, 4),
+           "flattened": flattened, "images_identical_across_forms": identical,
+           "g_queries_per_s": {"plain": round(qps(ms_plain), 3), "branch_graph": round(qps(ms_branch), 3), "flattened": round(qps(ms_flat), 3)},
+           "graph_launch_kernels": launch_count,
+           "tuning": [e for e in tuning if e["width"] > 0 and e["stage"] in ("candidates", "reproject", "sbCurrScatter", "sbBackupGather",
+                                                                                 "spatialCentral")]
+                     + [e for e in tuning if e["width"] == 0],
+           "quality": quality,
+           "how": "16 timed frames after warm-up per form on the same passes restarted before each form; flattened = one launch per "
+                  "stage over a work queue of all 64 instances (persistent kb_* kernels), tiles/grid forms from rs_batch_tune on the last "
+                  "warm-up frame; queries/s = 12.48 ray queries per pixel (counted for this mode) x pixels / time"}
     return res
 
 
@@ -491,8 +563,23 @@ def run_motion_blur(args, torch, rs, stream):
     torch.cuda.synchronize()
     ms = a.elapsed_time(b) / MB_FRAMES
     p.close()
+    quality = {}
+    if not args.no_quality:
+        def cam_of(f):
+            c = camera(f, W, H)
+            c.shutter_speed = 1.0 / 24.0
+            c.aperture_radius = 0.02
+            return c
+
+        def move(gp, f):
+            torch.add(base, vel, alpha=float(f), out=pos)
+            gp.update_geometry(pos, stream.cuda_stream)
+
+        q = measure_quality(args, torch, rs, sc, [cam_of(f) for f in range(3 + MB_FRAMES)], color, MB_PROPS, W, H, stream,
+                            before_frame=move, spp=args.mode_gt_spp)
+        quality = {k: q[k] for k in ("mse_vs_fp64_gt", "mse_1spp_path_tracing", "mse_ratio_1spp_over_restir", "gt_noise_mse_estimate", "gt_spp")}
     return {"frames_per_s": round(1000.0 / ms, 3), "ms_per_frame": round(ms, 4), "frames": MB_FRAMES, "resolution": [W, H],
-            "triangles": sc.num_triangles, "moving_spheres": 200, "time_partitions": 4,
+            "triangles": sc.num_triangles, "moving_spheres": 200, "time_partitions": 4, **quality,
             "how": "per frame: sphere positions on the device, rs_update_geometry (refit, previous positions), rs_execute; "
                    "camera orbiting 0.5 deg/frame with shutter 1/24 s and aperture 0.02"}
 
@@ -561,6 +648,16 @@ def run_adjoint(args, torch, rs, stream):
                    "from its checkpoint; the gradient check against FP64 central differences is in the tests"}
 
 
+def bench_config(triangles, world, args):
+    """The workload both arms report (the GPU arm and --impl reference print the same dict)."""
+    w, h = W_FULL // 4, H_FULL // 4
+    return {"workload": "terrain512+500 icospheres(subdiv4)+64 emissive tris = %d tris, 1920x1080, ScatterBackup/Clamped/Balance, "
+                        "path length 4, spatial reuse on, orbit 0.5 deg/frame; CPU sample: %d temporal frames at %dx%d, scaled x16"
+                        % (triangles, max(1, args.cpu_frames), w, h),
+            "resolution": [W_FULL, H_FULL], "triangles": triangles, "parallelism": "replicas" if world > 1 else "single",
+            "l2": "per-frame working set (3 x 144 B/pixel reservoir sets + 348 MB BVH) exceeds the 126 MB L2"}
+
+
 def C_frame_bytes():
     import ctypes
     rs = _package()
@@ -588,7 +685,8 @@ def cpu_baseline(args, quiet=False):
     dt = (time.time() - t0) / frames
     scale = (W_FULL * H_FULL) / (w * h)
     return {"value": round(1.0 / (dt * scale), 5), "unit": "frames/s", "cores": threads, "kind": "port",
-            "sample": f"{frames} temporal frame(s) at {w}x{h} (1/{scale:.0f} of 1080p), scaled by {scale:.0f}; scene setup {setup:.1f}s excluded"}
+            "sample": f"{frames} temporal frame(s) at {w}x{h} (1/{scale:.0f} of 1080p), scaled by {scale:.0f}; scene setup {setup:.1f}s excluded",
+            "triangles": scene.num_triangles}
 
 
 def run_reference(args):
@@ -599,7 +697,7 @@ def run_reference(args):
     line = {"metric": METRIC, "value": cb["value"], "unit": "frames/s", "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "impl": "reference",
             "dtype": "f32", "data": "synthetic (seeded procedural scene)",
-            "config": {"workload": "terrain512+500 icospheres(subdiv4)+64 emissive tris, 1920x1080, ScatterBackup/Clamped/Balance, path length 4, spatial reuse on"},
+            "config": bench_config(cb.pop("triangles"), int(os.environ.get("WORLD_SIZE", "1")), args),
             "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": "reference GPU path is Slang on D3D12/Vulkan DXR: unavailable on this box; timed: the CPU restatement of its algorithm"}
     print(json.dumps(line), flush=True)
@@ -676,18 +774,19 @@ def main():
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--cpu-frames", type=int, default=1)
+    ap.add_argument("--cpu-frames", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--batch-instances", type=int, default=64)
-    ap.add_argument("--batch-frames", type=int, default=4)
+    ap.add_argument("--batch-frames", type=int, default=16)
     ap.add_argument("--batch-warmup", type=int, default=2)
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-quality", action="store_true")
     ap.add_argument("--no-motion-blur", action="store_true")
     ap.add_argument("--no-modes", action="store_true")
     ap.add_argument("--mode-frames", type=int, default=10)
-    ap.add_argument("--gt-spp", type=int, default=512)
+    ap.add_argument("--gt-spp", type=int, default=4096)
+    ap.add_argument("--mode-gt-spp", type=int, default=1024)
     ap.add_argument("--adjoint-reps", type=int, default=3)
     ap.add_argument("--ray-stats", choices=sorted(RAY_STATS_MODES),
                     help="print ray queries per stage of a 1080p frame in this mode instead of the bench line")

@@ -234,6 +234,37 @@ RS_API rs_status rs_batch_execute(rs_batch* batch, const rs_frame_desc* frames, 
 RS_API rs_status rs_batch_destroy(rs_batch* batch);
 RS_API uint32_t rs_batch_launch_count(rs_batch* batch);
 
+/* The flattened batch form.  When every member renders ScatterBackup with the Clamped gather and one
+ * sample per pixel, with the same spatial settings and environment-light state, past its first
+ * frame and not frozen, rs_batch_execute runs each stage as ONE launch over all members: a flattened
+ * work queue (member k owns work items [start[k], start[k+1]), each one block of its own grid) that
+ * persistent kernels stride over, reading each member's context and buffers from device tables
+ * built at capture.  Otherwise (or with rs_batch_set_flatten(batch, 0)) each member's stage chain is
+ * a graph branch.  Results are bit-identical either way.  rs_batch_last_flattened tells which form
+ * the last rs_batch_execute used.
+ *
+ * Tuning: each stage's warp tile width (8, 16 or 32: a warp covers tw x 32/tw pixels) per
+ * resolution and its grid form (0 persistent: SMs x resident blocks; 1: one block per work item).
+ * rs_batch_tune renders one frame eagerly (synchronous) while timing every choice of every stage in
+ * place and keeps the fastest; rs_batch_get_tuning / rs_batch_set_tuning read and restore the choices
+ * (the Python layer caches them in a JSON file).  Entries with width = height = 0 carry a stage's
+ * grid form; the others a tile width for that resolution.  Stages: 0 candidates, 1-6 the ScatterBackup
+ * shifts (current scatter, current gather, backup gather, backup scatter, splat scatter, splat
+ * gather), 7-8 spatial central and neighbour shifts, 9 primary hits, 10 reprojection, 11 ScatterBackup
+ * combine (not tuned: it updates its input in place), 12 spatial combine. */
+typedef struct rs_batch_tuning_entry {
+    uint32_t stage;
+    uint32_t width, height;  /* 0, 0: the stage's grid form */
+    uint32_t tile;           /* 8, 16 or 32 */
+    uint32_t grid;           /* 0 persistent, 1 one block per work item */
+    float ms;                /* the tuning trial's time of the chosen tile (informative) */
+} rs_batch_tuning_entry;
+RS_API rs_status rs_batch_set_flatten(rs_batch* batch, uint32_t enable);
+RS_API uint32_t rs_batch_last_flattened(rs_batch* batch);
+RS_API rs_status rs_batch_tune(rs_batch* batch, const rs_frame_desc* frames, void* cudaStream);
+RS_API rs_status rs_batch_get_tuning(rs_batch* batch, rs_batch_tuning_entry* out, uint32_t* count);
+RS_API rs_status rs_batch_set_tuning(rs_batch* batch, const rs_batch_tuning_entry* entries, uint32_t count);
+
 /* Moving geometry (Falcor's animated-scene update, done by the caller).  rs_update_geometry moves
  * every triangle to `positions` (9 floats per triangle, the scene's count; host memory, or device
  * memory of the current device when onDevice != 0) for the next rs_execute: the previous positions
@@ -249,6 +280,15 @@ RS_API rs_status rs_update_geometry(rs_pass* pass, const float* positions, uint3
  * depth, internal children, leaf children, leaf triangles, surface-area cost}.  Both synchronise. */
 RS_API rs_status rs_debug_trace_rays(rs_pass* pass, const float* rays, uint32_t n, int32_t* prim, float* tuv, uint32_t* counts);
 RS_API rs_status rs_debug_bvh_shape(rs_pass* pass, double* out6);
+/* The library's own sort and scan on host data (no reference counterpart; synchronous, allocates):
+ * rs_debug_sort_keys64: order[i] = the index of the i-th smallest of n keys over their low keyBits
+ * bits, equal keys in ascending index order (the stable radix sort that orders the BVH build's
+ * Morton codes); rs_debug_sort_keys32: the same for 32-bit keys with every key >= clampMax treated
+ * as clampMax and sorted last (the cell-list sort of the temporal scatter, clampMax = cells);
+ * rs_debug_scan: out[i] = values[0] + ... + values[i - 1]. */
+RS_API rs_status rs_debug_sort_keys64(const uint64_t* keys, uint32_t n, uint32_t keyBits, uint32_t* order);
+RS_API rs_status rs_debug_sort_keys32(const uint32_t* keys, uint32_t n, uint32_t clampMax, uint32_t* order);
+RS_API rs_status rs_debug_scan(const uint32_t* values, uint32_t n, uint32_t* out);
 /* Binary-tree builder for the next rs_set_scene (no reference counterpart: the reference traces with
  * the driver's RT acceleration structures): 0 = PLOC clustering (the default, the better tree),
  * 1 = LBVH (Karras 2012 radix tree over the same Morton order).  Hits do not depend on it. */
@@ -326,14 +366,16 @@ RS_API rs_status rs_tonemap(const void* colorDev, uint32_t width, uint32_t heigh
  * out all device memory from its own fixed pool, an allocator-free real-time loop, or a plug-in
  * invoked while its host captures a CUDA graph.  The rs_pass calls allocate their buffers on the
  * first frame at a given size; this call never calls cudaMalloc, cudaFree or any other
- * allocating routine.  Its temporaries live in a 16 MiB array compiled into the library, which
+ * allocating routine.  Its temporaries live in a 9 MiB array compiled into the library, which
  * every GPU that loads the library holds until the process exits.
  *
  * Input:  targets[numSplats], device memory: the cell of each splat, or any value >= numCells
  *         (0xFFFFFFFF, say) for a splat that lands in no cell.
  * Output: counts[numCells] (splats per cell), offsets[numCells] (exclusive prefix sum of the
- *         counts) and sorted[numSplats] (splat indices grouped by cell, ascending within a cell;
- *         the first sum(counts) entries are written), all device memory on the current device.
+ *         counts) and sorted[numSplats] (splat indices grouped by cell, ascending within a cell,
+ *         in the first sum(counts) entries; the splats without a cell follow in ascending order),
+ *         all device memory on the current device.  The work per splat is bounded (a stable radix
+ *         sort by cell), however many splats share one cell.
  * These are the lists rs_execute builds for the temporal scatter, in the same order.
  *
  * Limits: 1 <= numCells <= RS_CELL_LISTS_STATIC_MAX and numSplats <= RS_CELL_LISTS_STATIC_MAX

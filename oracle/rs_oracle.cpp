@@ -2131,15 +2131,11 @@ static ReplayVertex replay_vertex(const Pass& p, const ShadingData& sd, uint32_t
     return v;
 }
 
-// The material whose front-face emission is the radiance the path carries.
-static uint32_t emitter_of(const Pass& p, const ShadingData& sd, f3 Le)
+// The emissive material of the triangle the path ends on (the primary hit, the record's second hit,
+// or the closest hit from x2 along the stored direction); its facing was decided by the forward pass.
+static uint32_t emitter_of(const Pass& p, const ShadingData& sd)
 {
-    f3 e = p.instance(sd).emission;
-    if (!any_gt0(e)) return kInvalidIndex;
-    const float a[3] = {e.x, e.y, e.z}, b[3] = {Le.x, Le.y, Le.z};
-    for (int c = 0; c < 3; c++)
-        if (f_abs(a[c] - b[c]) > 1e-5f * f_max(f_abs(a[c]), 1e-30f)) return kInvalidIndex;
-    return sd.materialID;
+    return material_is_emissive(p.scene.materials[sd.materialID]) ? sd.materialID : kInvalidIndex;
 }
 
 static bool replay_pixel(const Pass& p, const PathReservoir& r, const ReconnectionData& rd, Replay& out, uint64_t* stats)
@@ -2154,7 +2150,7 @@ static bool replay_pixel(const Pass& p, const PathReservoir& r, const Reconnecti
     if (rd.pathLength == 1)
     {
         out.s = 1.f;
-        out.emitter = emitter_of(p, sd1, rd.irradiance);
+        out.emitter = emitter_of(p, sd1);
     }
     else
     {
@@ -2182,7 +2178,7 @@ static bool replay_pixel(const Pass& p, const PathReservoir& r, const Reconnecti
                 out.s = p.mis(totalPdf, lightPdf) / lobePdf;
             }
             out.nv = 1;
-            out.emitter = emitter_of(p, p.loadSD(rd.secondHit, dir), rd.irradiance);
+            out.emitter = emitter_of(p, p.loadSD(rd.secondHit, dir));
         }
         else
         {
@@ -2208,7 +2204,7 @@ static bool replay_pixel(const Pass& p, const PathReservoir& r, const Reconnecti
             f3 o2 = computeRayOrigin(sd2.posW, dot(sd2.faceN, rd.secondWo) >= 0.f ? sd2.faceN : -sd2.faceN);
             HitInfo h; float t;
             if (p.bvh.closest(mk_ray(o2, rd.secondWo, 0.f, kRayTMax), h, t))
-                out.emitter = emitter_of(p, p.loadSD(h, rd.secondWo), rd.irradiance);
+                out.emitter = emitter_of(p, p.loadSD(h, rd.secondWo));
         }
     }
     f3 B = out.nv == 2 ? out.v[1].g.value : mk3(1.f);

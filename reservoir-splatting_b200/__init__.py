@@ -70,6 +70,12 @@ def load_library():
     lib.rs_batch_destroy.argtypes = [C.c_void_p]
     lib.rs_batch_launch_count.argtypes = [C.c_void_p]
     lib.rs_batch_launch_count.restype = C.c_uint32
+    lib.rs_batch_last_flattened.argtypes = [C.c_void_p]
+    lib.rs_batch_last_flattened.restype = C.c_uint32
+    lib.rs_batch_set_flatten.argtypes = [C.c_void_p, C.c_uint32]
+    lib.rs_batch_tune.argtypes = [C.c_void_p, C.POINTER(abi.RsFrameDesc), C.c_void_p]
+    lib.rs_batch_get_tuning.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_uint32)]
+    lib.rs_batch_set_tuning.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32]
     lib.rs_set_materials.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32]
     lib.rs_checkpoint_bytes.argtypes = [C.c_void_p, C.POINTER(C.c_size_t)]
     lib.rs_checkpoint.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
@@ -79,12 +85,16 @@ def load_library():
     lib.rs_debug_trace_rays.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]
     lib.rs_debug_bvh_shape.argtypes = [C.c_void_p, C.c_void_p]
     lib.rs_build_cell_lists_static.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.rs_debug_sort_keys64.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p]
+    lib.rs_debug_sort_keys32.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p]
+    lib.rs_debug_scan.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p]
     for name in ("rs_create", "rs_destroy", "rs_set_options", "rs_set_scene", "rs_set_env_map", "rs_execute", "rs_reset", "rs_set_seed",
                  "rs_freeze", "rs_get_buffer", "rs_set_buffer", "rs_enable_stage_timing", "rs_get_stage_times",
                  "rs_debug_keep_candidates", "rs_batch_create", "rs_batch_execute", "rs_batch_destroy",
                  "rs_build_cell_lists_static", "rs_set_materials", "rs_checkpoint_bytes", "rs_checkpoint", "rs_backward",
                  "rs_backward_stats", "rs_debug_trace_rays", "rs_debug_bvh_shape", "rs_debug_stage_rays", "rs_tonemap", "rs_tonemap_color_transform",
-                 "rs_set_bvh_builder",
+                 "rs_set_bvh_builder", "rs_debug_sort_keys64", "rs_debug_sort_keys32", "rs_debug_scan",
+                 "rs_batch_set_flatten", "rs_batch_tune", "rs_batch_get_tuning", "rs_batch_set_tuning",
                  "rs_update_geometry"):
         getattr(lib, name).restype = C.c_int
     _lib = lib
@@ -284,23 +294,89 @@ class ReservoirSplatting:
 
 
 class Batch:
-    """Renders one frame of several passes with one CUDA graph launch (rs_batch_execute)."""
+    """Renders one frame of several passes with one CUDA graph launch (rs_batch_execute).
 
-    def __init__(self, passes):
+    Members in the same ScatterBackup/Clamped configuration run the flattened form (one persistent
+    launch per stage over all members); `flatten=False` forces one graph branch per member.
+    `tuning_cache` names a JSON file of stage tile widths and grid forms: read when the batch is made,
+    written by `tune()`, keyed by the GPU name so that another GPU model tunes again."""
+
+    def __init__(self, passes, flatten: bool = True, tuning_cache: str | None = None):
         self._lib = load_library()
         self.passes = list(passes)
         arr = (C.c_void_p * len(self.passes))(*[p._h.value for p in self.passes])
         h = C.c_void_p()
         _check(self._lib.rs_batch_create(arr, len(self.passes), C.byref(h)))
         self._h = h
+        _check(self._lib.rs_batch_set_flatten(self._h, 1 if flatten else 0))
+        self.tuning_cache = tuning_cache
+        if tuning_cache:
+            self._load_tuning()
 
-    def execute(self, cameras, color_ptrs, stream: int = 0, should_reset: bool = False):
+    def _frames(self, cameras, color_ptrs, should_reset=False):
         frames = (abi.RsFrameDesc * len(self.passes))()
         for f, cam, ptr in zip(frames, cameras, color_ptrs):
             f.camera = abi.camera_struct(cam)
             f.color = ptr
             f.sceneShouldReset = 1 if should_reset else 0
-        _check(self._lib.rs_batch_execute(self._h, frames, C.c_void_p(stream)))
+        return frames
+
+    def execute(self, cameras, color_ptrs, stream: int = 0, should_reset: bool = False):
+        _check(self._lib.rs_batch_execute(self._h, self._frames(cameras, color_ptrs, should_reset), C.c_void_p(stream)))
+
+    def tune(self, cameras, color_ptrs, stream: int = 0) -> list:
+        """Renders one frame while timing every stage's tile widths and grid forms (rs_batch_tune),
+        keeps the fastest and, with a tuning cache, writes it."""
+        _check(self._lib.rs_batch_tune(self._h, self._frames(cameras, color_ptrs), C.c_void_p(stream)))
+        entries = self.tuning()
+        if self.tuning_cache:
+            self._save_tuning(entries)
+        return entries
+
+    def tuning(self) -> list:
+        n = C.c_uint32(0)
+        _check(self._lib.rs_batch_get_tuning(self._h, None, C.byref(n)))
+        arr = (abi.RsBatchTuningEntry * n.value)()
+        _check(self._lib.rs_batch_get_tuning(self._h, arr, C.byref(n)))
+        return [{"stage": abi.BATCH_STAGES[e.stage], "width": e.width, "height": e.height, "tile": e.tile, "grid": e.grid,
+                 "ms": round(float(e.ms), 4)} for e in arr]
+
+    def set_tuning(self, entries: list):
+        arr = (abi.RsBatchTuningEntry * len(entries))()
+        for a, e in zip(arr, entries):
+            a.stage = abi.BATCH_STAGES.index(e["stage"])
+            a.width, a.height = int(e["width"]), int(e["height"])
+            a.tile, a.grid, a.ms = int(e["tile"]), int(e["grid"]), float(e.get("ms", 0.0))
+        _check(self._lib.rs_batch_set_tuning(self._h, arr, len(entries)))
+
+    @staticmethod
+    def _gpu_key() -> str:
+        try:
+            import torch
+            return torch.cuda.get_device_name()
+        except Exception:
+            return "unknown"
+
+    def _load_tuning(self):
+        import json
+        from pathlib import Path
+        path = Path(self.tuning_cache)
+        if path.exists():
+            data = json.loads(path.read_text())
+            entries = data.get(self._gpu_key())
+            if entries:
+                self.set_tuning(entries)
+
+    def _save_tuning(self, entries):
+        import json
+        from pathlib import Path
+        path = Path(self.tuning_cache)
+        data = json.loads(path.read_text()) if path.exists() else {}
+        data[self._gpu_key()] = entries
+        path.write_text(json.dumps(data, indent=1))
+
+    def last_flattened(self) -> bool:
+        return bool(self._lib.rs_batch_last_flattened(self._h))
 
     def launch_count(self) -> int:
         return int(self._lib.rs_batch_launch_count(self._h))

@@ -87,6 +87,16 @@ class RsFrameDesc(C.Structure):
 TONEMAP_OPERATOR = {"Linear": 0, "Reinhard": 1, "ReinhardModified": 2, "HejiHableAlu": 3, "HableUc2": 4, "Aces": 5}
 
 
+class RsBatchTuningEntry(C.Structure):
+    _fields_ = [("stage", C.c_uint32), ("width", C.c_uint32), ("height", C.c_uint32), ("tile", C.c_uint32), ("grid", C.c_uint32),
+                ("ms", C.c_float)]
+
+
+# rs_batch_tuning_entry.stage
+BATCH_STAGES = ["candidates", "sbCurrScatter", "sbCurrGather", "sbBackupGather", "sbBackupScatter", "sbSplatScatter", "sbSplatGather",
+                "spatialCentral", "spatialNeighbor", "vbuffer", "reproject", "sbCombine", "spatialCombine"]
+
+
 class RsTonemapOptions(C.Structure):
     _fields_ = [("op", C.c_uint32), ("exposureCompensation", C.c_float), ("autoExposure", C.c_uint32), ("filmSpeed", C.c_float),
                 ("fNumber", C.c_float), ("shutter", C.c_float), ("clamp", C.c_uint32), ("whiteMaxLuminance", C.c_float),

@@ -22,15 +22,16 @@ namespace rs {
 
 enum : uint32_t { kAdjReplayed = 0, kAdjTooLong = 1, kAdjNoEmitter = 2, kAdjValueMismatch = 3 };
 
-// The material whose front-face emission is the radiance the path carries.
-__device__ __forceinline__ uint32_t dev_emitter_of(const DevCtx& C, const ShadingData& sd, f3 Le)
+// The emitter of a path is the triangle its last vertex lies on: the primary hit (length 1), the
+// reconnection vertex x2 (length 2: the record's second hit is the light sample's or the BSDF
+// hit's triangle) or the closest hit from x2 along the stored direction (length 3).  Its emissive
+// material owns the Le the path carries.  The forward pass already decided that the triangle emits
+// toward the path, so its facing is not tested again (a grazing light would flip the test by
+// rounding and drop the path's Le gradient).
+__device__ __forceinline__ uint32_t dev_emitter_of(const DevCtx& C, const ShadingData& sd)
 {
-    f3 e = dev_instance(C, sd).emission;
-    if (!any_gt0(e)) return kInvalidIndex;
-    if (f_abs(e.x - Le.x) > 1e-5f * f_max(f_abs(e.x), 1e-30f)) return kInvalidIndex;
-    if (f_abs(e.y - Le.y) > 1e-5f * f_max(f_abs(e.y), 1e-30f)) return kInvalidIndex;
-    if (f_abs(e.z - Le.z) > 1e-5f * f_max(f_abs(e.z), 1e-30f)) return kInvalidIndex;
-    return sd.materialID;
+    const MaterialData& m = C.materials[sd.materialID];
+    return (m.emissive[0] > 0.f || m.emissive[1] > 0.f || m.emissive[2] > 0.f) ? sd.materialID : kInvalidIndex;
 }
 
 // Per-pixel terms are FP32; their sums are FP64, because the roughness terms of sharp GGX lobes are
@@ -59,7 +60,7 @@ __device__ inline void adj_pixel(const DevCtx& C, const ResPlanes& res, const Re
     ShadingData sd1 = dev_sd(C, rd.firstHit, -rd.firstWi);
     if (rd.pathLength == 1)
     {
-        emitter = dev_emitter_of(C, sd1, rd.irradiance);
+        emitter = dev_emitter_of(C, sd1);
     }
     else
     {
@@ -88,7 +89,7 @@ __device__ inline void adj_pixel(const DevCtx& C, const ResPlanes& res, const Re
                 s = dev_mis(C, totalPdf, lightPdf) / lobePdf;
             }
             nv = 1;
-            emitter = dev_emitter_of(C, dev_sd(C, rd.secondHit, dir), rd.irradiance);
+            emitter = dev_emitter_of(C, dev_sd(C, rd.secondHit, dir));
         }
         else
         {
@@ -115,7 +116,7 @@ __device__ inline void adj_pixel(const DevCtx& C, const ResPlanes& res, const Re
             f3 o2 = computeRayOrigin(sd2.posW, dot(sd2.faceN, rd.secondWo) >= 0.f ? sd2.faceN : -sd2.faceN);
             HitInfo h; float t;
             if (trace_closest(C.bvh, mk_ray(o2, rd.secondWo, 0.f, kRayTMax), h, t, C.fault))
-                emitter = dev_emitter_of(C, dev_sd(C, h, rd.secondWo), rd.irradiance);
+                emitter = dev_emitter_of(C, dev_sd(C, h, rd.secondWo));
         }
     }
     const f3 A = nv >= 1 ? V[0].value : mk3(1.f);

@@ -1,7 +1,7 @@
 // BVH construction on the GPU, once per rs_set_scene.
 //
-// 1. Binary tree: 63-bit Morton codes (21 bits per axis) of the triangle centroids, a key/index
-//    radix sort, the triangles gathered in key order, then PLOC clustering of the ordered leaves
+// 1. Binary tree: 63-bit Morton codes (21 bits per axis) of the triangle centroids, a stable
+//    radix sort of the triangle indices by key (radix_sort.cu), the triangles gathered in key order, then PLOC clustering of the ordered leaves
 //    (below), or with kBvhLbvh the LBVH of k_karras (Karras 2012, "Maximizing parallelism in the
 //    construction of BVHs, octrees, and k-d trees": the radix tree of the sorted keys) with its boxes
 //    from k_refit, the bottom-up box pass with per-node arrival counters that also refits either
@@ -11,8 +11,8 @@
 //    the child of largest surface area that holds more than four triangles, up to four children;
 //    children of at most four triangles become leaves, which are ranges of the key-ordered
 //    triangles (the leaf-order array).
-#include <cub/device/device_radix_sort.cuh>
-#include <cub/device/device_scan.cuh>
+#include <algorithm>
+#include "radix_sort.h"
 #include "bvh_build.h"
 
 namespace rs {
@@ -63,6 +63,13 @@ __global__ void k_centroid_bounds(const float4* __restrict__ tri, uint32_t n, ui
             atomicMin(&bounds[k], ordered_bits(lo[k]));
             atomicMax(&bounds[3 + k], ordered_bits(hi[k]));
         }
+}
+
+// keysOut[i] = keys[order[i]]
+__global__ void k_gather_keys(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ order, uint32_t n, uint64_t* __restrict__ keysOut)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) keysOut[i] = keys[order[i]];
 }
 
 __global__ void k_morton(const float4* __restrict__ tri, uint32_t n, const uint32_t* __restrict__ bounds,
@@ -514,9 +521,11 @@ cudaError_t build_wide_bvh(const float4* dTri, uint32_t n, WideBvh* out, cudaStr
         RS_TRY(cudaMemcpyAsync(bounds, init, sizeof(init), cudaMemcpyHostToDevice, s));
         k_centroid_bounds<<<592, 256, 0, s>>>(dTri, n, bounds);
         k_morton<<<(n + 255) / 256, 256, 0, s>>>(dTri, n, bounds, keys, vals);
-        RS_TRY(cub::DeviceRadixSort::SortPairs(nullptr, tempBytes, keys, keys2, vals, vals2, (int)n, 0, 63, s));
+        // triangle indices in (Morton key, index) order, then the keys in that order for the Karras tree
+        tempBytes = 4 * std::max(radix_scratch_words(n, 63), scan_scratch_words(n));
         RS_TRY(cudaMalloc(&temp, tempBytes));
-        RS_TRY(cub::DeviceRadixSort::SortPairs(temp, tempBytes, keys, keys2, vals, vals2, (int)n, 0, 63, s));
+        RS_TRY(radix_sort_indices_u64(keys, n, 63, vals2, vals, static_cast<uint32_t*>(temp), s));
+        k_gather_keys<<<(n + 255) / 256, 256, 0, s>>>(keys, vals2, n, keys2);
         k_gather_sorted<<<(n + 255) / 256, 256, 0, s>>>(dTri, vals2, n, sorted);
         uint32_t levels = 0, numWide = 1;
         if (n == 1)
@@ -545,21 +554,18 @@ cudaError_t build_wide_bvh(const float4* dTri, uint32_t n, WideBvh* out, cudaStr
                 // PLOC over the key-ordered leaves (node 0 = root); the binary tree the rest uses
                 ClusterBox *ca = nullptr, *cb = nullptr;
                 uint32_t *nn = nullptr, *mflag = nullptr, *kflag = nullptr, *moff = nullptr, *koff = nullptr;
-                void* stemp = nullptr;
-                size_t stempBytes = 0;
+                uint32_t* stemp = static_cast<uint32_t*>(temp); // the sort's scratch, sized for an n-element scan too
                 RS_TRY(cudaMalloc(&ca, 32ull * n)); RS_TRY(cudaMalloc(&cb, 32ull * n));
                 RS_TRY(cudaMalloc(&nn, 4ull * n)); RS_TRY(cudaMalloc(&mflag, 4ull * n)); RS_TRY(cudaMalloc(&kflag, 4ull * n));
                 RS_TRY(cudaMalloc(&moff, 4ull * n)); RS_TRY(cudaMalloc(&koff, 4ull * n));
-                RS_TRY(cub::DeviceScan::ExclusiveSum(nullptr, stempBytes, mflag, moff, (int)n, s));
-                RS_TRY(cudaMalloc(&stemp, stempBytes));
                 k_ploc_init<<<(n + 255) / 256, 256, 0, s>>>(sorted, n, ca);
                 uint32_t c = n, top = n - 2;
                 while (c > 1 && e == cudaSuccess)
                 {
                     k_ploc_nn<<<(c + 127) / 128, 128, 0, s>>>(ca, c, nn);
                     k_ploc_flags<<<(c + 255) / 256, 256, 0, s>>>(nn, c, mflag, kflag);
-                    e = cub::DeviceScan::ExclusiveSum(stemp, stempBytes, mflag, moff, (int)c, s);
-                    if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(stemp, stempBytes, kflag, koff, (int)c, s);
+                    e = scan_exclusive_u32(mflag, moff, c, stemp, s);
+                    if (e == cudaSuccess) e = scan_exclusive_u32(kflag, koff, c, stemp, s);
                     uint32_t tail[4] = {0, 0, 0, 0};
                     if (e == cudaSuccess) e = cudaMemcpyAsync(&tail[0], moff + c - 1, 4, cudaMemcpyDeviceToHost, s);
                     if (e == cudaSuccess) e = cudaMemcpyAsync(&tail[1], mflag + c - 1, 4, cudaMemcpyDeviceToHost, s);
@@ -575,7 +581,7 @@ cudaError_t build_wide_bvh(const float4* dTri, uint32_t n, WideBvh* out, cudaStr
                     c = kept;
                     std::swap(ca, cb);
                 }
-                cudaFree(ca); cudaFree(cb); cudaFree(nn); cudaFree(mflag); cudaFree(kflag); cudaFree(moff); cudaFree(koff); cudaFree(stemp);
+                cudaFree(ca); cudaFree(cb); cudaFree(nn); cudaFree(mflag); cudaFree(kflag); cudaFree(moff); cudaFree(koff);
                 if (e != cudaSuccess) goto done;
             }
             const uint2 root = make_uint2(0u, 0u);

@@ -1,12 +1,13 @@
-// rs_build_cell_lists_static: the splat cell-list build (count, exclusive scan, fill, rank) with its
-// scratch memory in a fixed array that the library holds, so the call allocates nothing.
+// rs_build_cell_lists_static: the splat cell-list build (count, exclusive scan, stable radix sort of
+// the splat indices by cell) with its scratch memory in a fixed array that the library holds, so the
+// call allocates nothing.
 //
 // Who needs it: callers that may not allocate device memory at the time they run.  A host that
 // owns a fixed memory pool (and fails on any allocation it did not plan), an allocator-free
 // real-time frame loop, or a plug-in that runs while its host is capturing a CUDA graph cannot
 // call cudaMalloc, and the rs_pass entry points allocate their buffers on the first frame at a
-// given size.  Such a caller passes its own input and output buffers; the temporaries (per-cell
-// cursors, the unsorted splat list and the scan's tile sums) come from `g_cellScratch` below.
+// given size.  Such a caller passes its own input and output buffers; the temporaries (the sort's
+// second index buffer and digit counts, the scan's tile sums) come from `g_cellScratch` below.
 //
 // The lists are the per-cell splat lists of the temporal scatter (the cell counters and splat
 // indices that ReprojectTemporalSamples.rt.slang:64-175 fills, cleared at
@@ -17,6 +18,7 @@
 #include <string>
 #include "../../include/rs_b200.h"
 #include "kernels.h"
+#include "radix_sort.h"
 
 namespace rs {
 void set_last_error(const std::string& msg);
@@ -29,15 +31,18 @@ namespace {
 constexpr uint32_t kStaticMaxCells = RS_CELL_LISTS_STATIC_MAX;
 constexpr uint32_t kStaticMaxSplats = RS_CELL_LISTS_STATIC_MAX;
 constexpr uint32_t kStaticMaxTiles = (kStaticMaxCells + kScanTileElems - 1) / kScanTileElems;
-// Word offsets inside the scratch array; each part starts on a 256-byte boundary.
-constexpr size_t kCursorWords = kStaticMaxCells;
-constexpr size_t kUnsortedOffset = kCursorWords;
-constexpr size_t kTileSumsOffset = kUnsortedOffset + kStaticMaxSplats;
-constexpr size_t kScratchWords = kTileSumsOffset + ((kStaticMaxTiles + 63) / 64) * 64;
-static_assert(kUnsortedOffset % 64 == 0 && kTileSumsOffset % 64 == 0, "scratch parts must be 256-byte aligned");
+// Word offsets inside the scratch array; each part starts on a 256-byte boundary.  The radix sort
+// needs two 256-entry digit-count matrices over its tiles plus a little scan scratch
+// (radix_scratch_words; at most 8-bit digits because keys have at most 22 bits here).
+constexpr size_t kTmpWords = kStaticMaxSplats;
+constexpr size_t kTileSumsOffset = kTmpWords;
+constexpr size_t kRadixOffset = kTileSumsOffset + ((kStaticMaxTiles + 63) / 64) * 64;
+constexpr size_t kRadixWords = 2 * 256 * ((kStaticMaxSplats + kSortTile - 1) / kSortTile) + 1024;
+constexpr size_t kScratchWords = kRadixOffset + kRadixWords;
+static_assert(kTileSumsOffset % 64 == 0 && kRadixOffset % 64 == 0, "scratch parts must be 256-byte aligned");
 static_assert(kStaticMaxTiles <= kScanTileElems, "k_scan_tile_sums scans at most one tile of tile sums");
 
-// Every GPU that loads the library holds this array (16 MiB + 2 KiB) until the process exits.
+// Every GPU that loads the library holds this array (about 9 MiB) until the process exits.
 // Host code must not pass `g_cellScratch` to a kernel: on the host the name is only a stand-in
 // for the device symbol.  Its device address comes from cudaGetSymbolAddress below.
 static __device__ __align__(256) uint32_t g_cellScratch[kScratchWords];
@@ -54,33 +59,6 @@ __global__ void __launch_bounds__(256) k_static_count(const uint32_t* __restrict
     if (s >= n) return;
     uint32_t t = targets[s];
     if (t < numCells) atomicAdd(&counts[t], 1u);
-}
-
-// Places each splat at offset[target] + arrival rank in the unsorted list.
-__global__ void __launch_bounds__(256) k_static_fill(const uint32_t* __restrict__ targets, uint32_t n, uint32_t numCells,
-                                                     const uint32_t* __restrict__ offsets, uint32_t* __restrict__ cursor,
-                                                     uint32_t* __restrict__ unsorted)
-{
-    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= n) return;
-    uint32_t t = targets[s];
-    if (t >= numCells) return;
-    unsorted[offsets[t] + atomicAdd(&cursor[t], 1u)] = s;
-}
-
-// Final slot = offset + number of splats of the same cell with a smaller index.
-__global__ void __launch_bounds__(256) k_static_rank(const uint32_t* __restrict__ targets, uint32_t n, uint32_t numCells,
-                                                     const uint32_t* __restrict__ offsets, const uint32_t* __restrict__ counts,
-                                                     const uint32_t* __restrict__ unsorted, uint32_t* __restrict__ sorted)
-{
-    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= n) return;
-    uint32_t t = targets[s];
-    if (t >= numCells) return;
-    uint32_t off = offsets[t], cnt = counts[t];
-    uint32_t rank = 0;
-    for (uint32_t j = 0; j < cnt; j++) rank += (__ldg(&unsorted[off + j]) < s) ? 1u : 0u;
-    sorted[off + rank] = s;
 }
 
 rs_status static_fail(rs_status s, const std::string& msg)
@@ -130,28 +108,27 @@ extern "C" RS_API rs_status rs_build_cell_lists_static(const uint32_t* targets, 
     uint32_t* scratch = nullptr;
     rs_status st = scratch_for_current_device(&scratch);
     if (st != RS_OK) return st;
-    uint32_t* cursor = scratch;
-    uint32_t* unsorted = scratch + kUnsortedOffset;
+    uint32_t* tmp = scratch;
     uint32_t* tileSums = scratch + kTileSumsOffset;
+    uint32_t* radixScratch = scratch + kRadixOffset;
+    const uint32_t keyBits = bit_length(numCells); // targets >= numCells sort last as numCells
+    if (radix_scratch_words(numSplats, keyBits) > kRadixWords)
+        return static_fail(RS_INVALID_ARG, "rs_build_cell_lists_static: sort scratch larger than the static array");
 
     cudaStream_t s = static_cast<cudaStream_t>(cudaStream);
     const uint32_t numTiles = (numCells + kScanTileElems - 1) / kScanTileElems;
     const uint32_t cellBlocks = (numCells + 255) / 256, splatBlocks = (numSplats + 255) / 256;
-    // The counts (an output) and the cursors (kept from the previous call) must start at zero;
-    // the scan, fill and rank overwrite everything else they read.
+    // The counts (an output) must start at zero; the scan and the sort overwrite everything else
+    // they read (the array keeps the previous call's contents).
     cudaError_t e = cudaMemsetAsync(counts, 0, (size_t)numCells * 4, s);
     if (e != cudaSuccess) return cuda_fail("cudaMemsetAsync(counts)", e);
-    e = cudaMemsetAsync(cursor, 0, (size_t)numCells * 4, s);
-    if (e != cudaSuccess) return cuda_fail("cudaMemsetAsync(cursor)", e);
     if (splatBlocks) k_static_count<<<splatBlocks, 256, 0, s>>>(targets, numSplats, numCells, counts);
     k_scan_tiles<<<numTiles, 1024, 0, s>>>(counts, offsets, tileSums, numCells);
     k_scan_tile_sums<<<1, 1024, 0, s>>>(tileSums, numTiles, nullptr);
     k_scan_add<<<cellBlocks, 256, 0, s>>>(offsets, tileSums, numCells);
-    if (splatBlocks)
-    {
-        k_static_fill<<<splatBlocks, 256, 0, s>>>(targets, numSplats, numCells, offsets, cursor, unsorted);
-        k_static_rank<<<splatBlocks, 256, 0, s>>>(targets, numSplats, numCells, offsets, counts, unsorted, sorted);
-    }
+    // splat indices in (cell, index) order; the ones without a cell follow the last listed splat
+    e = radix_sort_indices_u32(targets, numCells, numSplats, keyBits, sorted, tmp, radixScratch, s);
+    if (e != cudaSuccess) return cuda_fail("radix sort launch", e);
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail("kernel launch", e);
     return RS_OK;

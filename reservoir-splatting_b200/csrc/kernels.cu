@@ -22,11 +22,11 @@ cudaError_t upload_ctx(uint32_t slot, const DevCtx* hostPinned, cudaStream_t s)
 // VBufferRT.slang:71-150 (samplePattern Center, pinhole): hit of the pixel-centre ray of the
 // frame's camera and mvec = prevScreen - (pixel + 0.5) / dim, prevScreen being the film
 // projection of the hit point through the previous frame's camera.
-__global__ void __launch_bounds__(256) k_vbuffer(uint32_t slot, uint4* __restrict__ vbuffer, float2* __restrict__ mvec)
+__device__ __forceinline__ void vbuffer_body(uint32_t slot, uint4* __restrict__ vbuffer, float2* __restrict__ mvec, Blk blk)
 {
     const DevCtx& C = c_ctx[slot];
     uint32_t i;
-    if (!tiled_pixel(C.W, C.H, i)) return;
+    if (!tiled_pixel_at(C.W, C.H, blk, i)) return;
     uint32_t x = i % C.W, y = i / C.W;
     const CameraData& cam = C.camera;
     const CameraData& pc = C.prevCamera;
@@ -56,6 +56,21 @@ __global__ void __launch_bounds__(256) k_vbuffer(uint32_t slot, uint4* __restric
     }
 }
 
+__global__ void __launch_bounds__(256) k_vbuffer(uint32_t slot, uint4* __restrict__ vbuffer, float2* __restrict__ mvec)
+{
+    vbuffer_body(slot, vbuffer, mvec, Blk{blockIdx.x, 8u});
+}
+
+__global__ void __launch_bounds__(256) kb_vbuffer(BatchQueue q, const VbufArgs* __restrict__ args)
+{
+    for (uint32_t t = blockIdx.x; t < q.total; t += gridDim.x)
+    {
+        const uint32_t inst = batch_instance(q, t);
+        const VbufArgs& a = args[inst];
+        vbuffer_body(__ldg(q.slot + inst), a.vbuffer, a.mvec, batch_blk(q, inst, t));
+    }
+}
+
 #ifdef RS_RAY_STATS
 // Closest-hit and visibility queries counted by the frame kernels since the last call (reset).
 cudaError_t ray_stats_take(unsigned long long out[2], cudaStream_t s)
@@ -74,7 +89,7 @@ cudaError_t ray_stats_take(unsigned long long out[2], cudaStream_t s)
 // ============================================================ camera table
 // The frame constants of orient_camera (CameraTable) for the context of `slot`; one block of
 // kMaxCameraKeyframes threads, launched after the context upload of the frame.
-__global__ void __launch_bounds__(kMaxCameraKeyframes) k_camera_table(uint32_t slot, CameraTable* __restrict__ table)
+__device__ __forceinline__ void camera_table_body(uint32_t slot, CameraTable* __restrict__ table)
 {
     const DevCtx& C = c_ctx[slot];
     __shared__ f3 forward[kMaxCameraKeyframes];
@@ -96,6 +111,16 @@ __global__ void __launch_bounds__(kMaxCameraKeyframes) k_camera_table(uint32_t s
         table->time[i] = t;
         table->at[i] = c;
     }
+}
+__global__ void __launch_bounds__(kMaxCameraKeyframes) k_camera_table(uint32_t slot, CameraTable* __restrict__ table)
+{
+    camera_table_body(slot, table);
+}
+
+// One block per batch member: block b builds the camera table of context slots[b].
+__global__ void __launch_bounds__(kMaxCameraKeyframes) kb_camera_table(const uint32_t* __restrict__ slots, CameraTable* const* __restrict__ tables)
+{
+    camera_table_body(slots[blockIdx.x], tables[blockIdx.x]);
 }
 
 // ============================================================ initial candidates
@@ -550,16 +575,33 @@ __global__ void __launch_bounds__(128, 3) k_candidates(uint32_t slot, ResPlanes 
 
 // One sample per pixel (the reference default): records go straight to the output planes.
 template <bool kEnv>
-__global__ void __launch_bounds__(128, 8) k_candidates_direct(uint32_t slot, ResPlanes curr, RecPlanes currRec)
+__device__ __forceinline__ void candidates_direct_body(uint32_t slot, const ResPlanes& curr, const RecPlanes& currRec, Blk blk)
 {
     const DevCtx& C = c_ctx[slot];
     uint32_t i;
-    if (!tiled_pixel(C.W, C.H, i)) return;
+    if (!tiled_pixel_at(C.W, C.H, blk, i)) return;
     PState path;
     path_init<true>(C, i % C.W, i / C.W, path);
     do path_step<true, kEnv>(C, path, currRec, i);
     while (path.flags & kPActive);
     path_finish<true>(path, 0, 1, curr, currRec, i);
+}
+
+template <bool kEnv>
+__global__ void __launch_bounds__(128, 8) k_candidates_direct(uint32_t slot, ResPlanes curr, RecPlanes currRec)
+{
+    candidates_direct_body<kEnv>(slot, curr, currRec, Blk{blockIdx.x, 8u});
+}
+
+template <bool kEnv>
+__global__ void __launch_bounds__(128, 8) kb_candidates_direct(BatchQueue q, const CandArgs* __restrict__ args)
+{
+    for (uint32_t t = blockIdx.x; t < q.total; t += gridDim.x)
+    {
+        const uint32_t inst = batch_instance(q, t);
+        const CandArgs& a = args[inst];
+        candidates_direct_body<kEnv>(__ldg(q.slot + inst), a.curr, a.currRec, batch_blk(q, inst, t));
+    }
 }
 
 // ============================================================ environment-map importance
@@ -582,13 +624,12 @@ __global__ void __launch_bounds__(256) k_env_reduce(float* __restrict__ importan
 
 // ============================================================ forward reprojection (splat)
 // ReprojectTemporalSamples.rt.slang:64-175.  Writes the destination cell of every source pixel
-// and counts splats per cell; the cell lists are built by k_fill / k_rank_cells.
-__global__ void __launch_bounds__(256, 4) k_reproject(uint32_t slot, ResPlanes prev, RecPlanes prevRec,
-                                                   uint32_t* __restrict__ targets, uint32_t* __restrict__ counts)
+// and counts splats per cell; the cell lists are built from the targets by a radix sort (pass.cu).
+__device__ __forceinline__ void reproject_body(uint32_t slot, const ResPlanes& prev, const RecPlanes& prevRec, uint32_t* __restrict__ targets, uint32_t* __restrict__ counts, Blk blk)
 {
     const DevCtx& C = c_ctx[slot];
     uint32_t ci;
-    if (!tiled_pixel(C.W, C.H, ci)) return;
+    if (!tiled_pixel_at(C.W, C.H, blk, ci)) return;
     uint32_t target = kInvalidIndex;
     f3 integrand = load_integrand(prev, ci);
     if (!all_eq0(integrand))
@@ -634,6 +675,22 @@ __global__ void __launch_bounds__(256, 4) k_reproject(uint32_t slot, ResPlanes p
     }
     targets[ci] = target;
     if (target != kInvalidIndex) atomicAdd(&counts[target], 1u);
+}
+
+__global__ void __launch_bounds__(256, 4) k_reproject(uint32_t slot, ResPlanes prev, RecPlanes prevRec,
+                                                   uint32_t* __restrict__ targets, uint32_t* __restrict__ counts)
+{
+    reproject_body(slot, prev, prevRec, targets, counts, Blk{blockIdx.x, 8u});
+}
+
+__global__ void __launch_bounds__(256, 4) kb_reproject(BatchQueue q, const ReprojArgs* __restrict__ args)
+{
+    for (uint32_t t = blockIdx.x; t < q.total; t += gridDim.x)
+    {
+        const uint32_t inst = batch_instance(q, t);
+        const ReprojArgs& a = args[inst];
+        reproject_body(__ldg(q.slot + inst), a.prev, a.prevRec, a.targets, a.counts, batch_blk(q, inst, t));
+    }
 }
 
 // MultiReprojectTemporalSamples.rt.slang:65-168 (P partitions; targets/counts hold P planes of N)
@@ -777,33 +834,15 @@ __global__ void __launch_bounds__(256) k_scan_add(uint32_t* __restrict__ out, co
     out[i] += tileSums[i / kScanTile];
 }
 
-// Places each splat at offset[target] + arrival rank (order within a cell is fixed up by k_rank_cells).
-__global__ void __launch_bounds__(256) k_fill(const uint32_t* __restrict__ targets, const uint32_t* __restrict__ offsets,
-                                              uint32_t* __restrict__ cursor, uint32_t* __restrict__ unsorted, uint32_t n)
+// The cell of each entry of the sorted splat list (the list holds source indices in (cell, source)
+// order; entries whose source has no cell, after the last valid one, are left alone).
+__global__ void __launch_bounds__(256) k_sorted_cells(const uint32_t* __restrict__ targets, const uint32_t* __restrict__ sorted,
+                                                      uint32_t* __restrict__ sortedCell, uint32_t n)
 {
-    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= n) return;
-    uint32_t t = targets[s];
-    if (t == kInvalidIndex) return;
-    uint32_t slot = offsets[t] + atomicAdd(&cursor[t], 1u);
-    unsorted[slot] = s;
-}
-
-// Canonical in-cell order: each splat's final slot is offset + (number of splats of the same
-// cell with a smaller source index).  Source indices are distinct, so the ranks are a permutation.
-__global__ void __launch_bounds__(256) k_rank_cells(const uint32_t* __restrict__ targets, const uint32_t* __restrict__ offsets,
-                                                    const uint32_t* __restrict__ counts, const uint32_t* __restrict__ unsorted,
-                                                    uint32_t* __restrict__ sorted, uint32_t* __restrict__ sortedCell, uint32_t n)
-{
-    uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= n) return;
-    uint32_t t = targets[s];
-    if (t == kInvalidIndex) return;
-    uint32_t off = offsets[t], cnt = counts[t];
-    uint32_t rank = 0;
-    for (uint32_t j = 0; j < cnt; j++) rank += (__ldg(&unsorted[off + j]) < s) ? 1u : 0u;
-    sorted[off + rank] = s;
-    if (sortedCell) sortedCell[off + rank] = t;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t t = targets[sorted[i]];
+    if (t < n) sortedCell[i] = t;
 }
 
 // ============================================================ backup gather (collect)
@@ -1183,6 +1222,84 @@ void launch_k_sp_neighbor(bool env, dim3 grid, dim3 block, cudaStream_t s, uint3
 {
     if (env) k_sp_neighbor<true><<<grid, block, 0, s>>>(slot, S);
     else k_sp_neighbor<false><<<grid, block, 0, s>>>(slot, S);
+}
+
+} // namespace rs
+
+namespace rs {
+
+template <typename Kern, typename Args>
+static void launch_q(Kern k, dim3 grid, dim3 block, cudaStream_t s, const BatchQueue& q, const void* args)
+{
+    k<<<grid, block, 0, s>>>(q, static_cast<const Args*>(args));
+}
+
+void launch_batched(BatchStage stage, bool env, dim3 grid, dim3 block, cudaStream_t s, const BatchQueue& q, const void* args)
+{
+    switch (stage)
+    {
+    case kBatchCandidates:
+        if (env) launch_q<decltype(&kb_candidates_direct<true>), CandArgs>(kb_candidates_direct<true>, grid, block, s, q, args);
+        else launch_q<decltype(&kb_candidates_direct<false>), CandArgs>(kb_candidates_direct<false>, grid, block, s, q, args);
+        break;
+#define RS_BATCH_WAVE(st, kern)                                                                                      \
+    case st:                                                                                                         \
+        if (env) launch_q<decltype(&kern<true>), WaveCtx>(kern<true>, grid, block, s, q, args);                      \
+        else launch_q<decltype(&kern<false>), WaveCtx>(kern<false>, grid, block, s, q, args);                        \
+        break;
+    RS_BATCH_WAVE(kBatchSbCurrScatter, kb_sb_curr_scatter)
+    RS_BATCH_WAVE(kBatchSbCurrGather, kb_sb_curr_gather)
+    RS_BATCH_WAVE(kBatchSbBackupGather, kb_sb_backup_gather)
+    RS_BATCH_WAVE(kBatchSbBackupScatter, kb_sb_backup_scatter)
+    RS_BATCH_WAVE(kBatchSbSplatScatter, kb_sb_splat_scatter)
+    RS_BATCH_WAVE(kBatchSbSplatGather, kb_sb_splat_gather)
+#undef RS_BATCH_WAVE
+    case kBatchSpCentral:
+        if (env) launch_q<decltype(&kb_sp_central<true>), SpatialCtx>(kb_sp_central<true>, grid, block, s, q, args);
+        else launch_q<decltype(&kb_sp_central<false>), SpatialCtx>(kb_sp_central<false>, grid, block, s, q, args);
+        break;
+    case kBatchSpNeighbor:
+        if (env) launch_q<decltype(&kb_sp_neighbor<true>), SpatialCtx>(kb_sp_neighbor<true>, grid, block, s, q, args);
+        else launch_q<decltype(&kb_sp_neighbor<false>), SpatialCtx>(kb_sp_neighbor<false>, grid, block, s, q, args);
+        break;
+    case kBatchVbuffer: launch_q<decltype(&kb_vbuffer), VbufArgs>(kb_vbuffer, grid, block, s, q, args); break;
+    case kBatchReproject: launch_q<decltype(&kb_reproject), ReprojArgs>(kb_reproject, grid, block, s, q, args); break;
+    case kBatchSbCombine: launch_q<decltype(&kb_sb_combine), WaveColorArgs>(kb_sb_combine, grid, block, s, q, args); break;
+    case kBatchSpCombine: launch_q<decltype(&kb_sp_combine), SpatialColorArgs>(kb_sp_combine, grid, block, s, q, args); break;
+    default: break;
+    }
+}
+
+uint32_t batched_threads(BatchStage stage) { return stage == kBatchVbuffer || stage == kBatchReproject ? 256u : 128u; }
+
+template <typename Kern>
+static int occupancy(Kern k, uint32_t threads)
+{
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, (int)threads, 0) != cudaSuccess) n = 1;
+    return n > 0 ? n : 1;
+}
+
+int batched_blocks_per_sm(BatchStage stage, bool env)
+{
+    const uint32_t t = batched_threads(stage);
+    switch (stage)
+    {
+    case kBatchCandidates: return env ? occupancy(kb_candidates_direct<true>, t) : occupancy(kb_candidates_direct<false>, t);
+    case kBatchSbCurrScatter: return env ? occupancy(kb_sb_curr_scatter<true>, t) : occupancy(kb_sb_curr_scatter<false>, t);
+    case kBatchSbCurrGather: return env ? occupancy(kb_sb_curr_gather<true>, t) : occupancy(kb_sb_curr_gather<false>, t);
+    case kBatchSbBackupGather: return env ? occupancy(kb_sb_backup_gather<true>, t) : occupancy(kb_sb_backup_gather<false>, t);
+    case kBatchSbBackupScatter: return env ? occupancy(kb_sb_backup_scatter<true>, t) : occupancy(kb_sb_backup_scatter<false>, t);
+    case kBatchSbSplatScatter: return env ? occupancy(kb_sb_splat_scatter<true>, t) : occupancy(kb_sb_splat_scatter<false>, t);
+    case kBatchSbSplatGather: return env ? occupancy(kb_sb_splat_gather<true>, t) : occupancy(kb_sb_splat_gather<false>, t);
+    case kBatchSpCentral: return env ? occupancy(kb_sp_central<true>, t) : occupancy(kb_sp_central<false>, t);
+    case kBatchSpNeighbor: return env ? occupancy(kb_sp_neighbor<true>, t) : occupancy(kb_sp_neighbor<false>, t);
+    case kBatchVbuffer: return occupancy(kb_vbuffer, t);
+    case kBatchReproject: return occupancy(kb_reproject, t);
+    case kBatchSbCombine: return occupancy(kb_sb_combine, t);
+    case kBatchSpCombine: return occupancy(kb_sp_combine, t);
+    default: return 1;
+    }
 }
 
 } // namespace rs

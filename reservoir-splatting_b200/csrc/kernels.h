@@ -17,9 +17,7 @@ __global__ void k_multi_reproject(uint32_t slot, ResPlanes prev, RecPlanes prevR
 __global__ void k_scan_tiles(const uint32_t* in, uint32_t* out, uint32_t* tileSums, uint32_t n);
 __global__ void k_scan_tile_sums(uint32_t* tileSums, uint32_t numTiles, uint32_t* totalOut);
 __global__ void k_scan_add(uint32_t* out, const uint32_t* tileSums, uint32_t n);
-__global__ void k_fill(const uint32_t* targets, const uint32_t* offsets, uint32_t* cursor, uint32_t* unsorted, uint32_t n);
-__global__ void k_rank_cells(const uint32_t* targets, const uint32_t* offsets, const uint32_t* counts, const uint32_t* unsorted,
-                             uint32_t* sorted, uint32_t* sortedCell, uint32_t n);
+__global__ void k_sorted_cells(const uint32_t* targets, const uint32_t* sorted, uint32_t* sortedCell, uint32_t n);
 __global__ void k_collect(uint32_t slot, const float2* mvec, ResPlanes prev, RecPlanes prevRec, ResPlanes inter, RecPlanes interRec,
                           float2* floatingCoords, const Shifted* shiftedPaths);
 __global__ void k_resolve(uint32_t n, ResPlanes curr, float4* color);
@@ -93,6 +91,32 @@ struct SpatialCtx
 
 __global__ void k_sb_combine(uint32_t slot, WaveCtx K, float4* color);
 __global__ void k_sp_combine(uint32_t slot, SpatialCtx S, float4* color);
+
+// ---- batched stages: one persistent launch per stage over a BatchQueue of instances, each
+// instance's own arguments at args[instance] in device memory (the kb_* kernels).
+struct VbufArgs { uint4* vbuffer; float2* mvec; };
+struct CandArgs { ResPlanes curr; RecPlanes currRec; };
+struct ReprojArgs { ResPlanes prev; RecPlanes prevRec; uint32_t* targets; uint32_t* counts; };
+struct WaveColorArgs { WaveCtx K; float4* color; };
+struct SpatialColorArgs { SpatialCtx S; float4* color; };
+__global__ void kb_camera_table(const uint32_t* slots, CameraTable* const* tables);
+__global__ void kb_vbuffer(BatchQueue q, const VbufArgs* args);
+__global__ void kb_reproject(BatchQueue q, const ReprojArgs* args);
+__global__ void kb_sb_combine(BatchQueue q, const WaveColorArgs* args);
+__global__ void kb_sp_combine(BatchQueue q, const SpatialColorArgs* args);
+// Batched stages with environment-light variants: the stage is picked by `stage`, args points to
+// the stage's argument array (CandArgs for candidates, WaveCtx for the six ScatterBackup shift
+// stages, SpatialCtx for the two spatial shift stages).
+enum BatchStage : uint32_t
+{
+    kBatchCandidates = 0, kBatchSbCurrScatter, kBatchSbCurrGather, kBatchSbBackupGather, kBatchSbBackupScatter,
+    kBatchSbSplatScatter, kBatchSbSplatGather, kBatchSpCentral, kBatchSpNeighbor, kBatchVbuffer, kBatchReproject,
+    kBatchSbCombine, kBatchSpCombine, kBatchStageCount
+};
+void launch_batched(BatchStage stage, bool env, dim3 grid, dim3 block, cudaStream_t s, const BatchQueue& q, const void* args);
+// Threads per block and resident blocks per SM (for the persistent grid) of a batched stage kernel.
+uint32_t batched_threads(BatchStage stage);
+int batched_blocks_per_sm(BatchStage stage, bool env);
 
 
 // The kernels that reach an environment-light branch are templates on it (kEnv), defined and

@@ -14,9 +14,11 @@
 #include <vector>
 #include <memory>
 #include <mutex>
+#include <functional>
 #include "../../include/rs_b200.h"
 #include "kernels.h"
 #include "bvh_build.h"
+#include "radix_sort.h"
 #include "core/scene_prep.h"
 
 using namespace rs;
@@ -129,7 +131,7 @@ struct rs_pass
     ReservoirSet inter, cand;
     DevBuf<float2> mvec, floatingCoords, neighborOffsets;
     DevBuf<uint4> vbuffer;
-    DevBuf<uint32_t> targets, counts, offsets, cursor, unsortedSplats, sortedSplats, tileSums, total;
+    DevBuf<uint32_t> targets, counts, offsets, unsortedSplats, sortedSplats, tileSums, total, radixScratch;
     DevBuf<Shifted> shiftedPaths;
     DevBuf<float4> scratchColor;
     // wavefront ScatterBackup / spatial buffers
@@ -259,7 +261,6 @@ static rs_status allocate(rs_pass* p)
     RS_CUDA(p->targets.ensure(P * N));
     RS_CUDA(p->counts.ensure(P * N));
     RS_CUDA(p->offsets.ensure(P * N));
-    RS_CUDA(p->cursor.ensure(P * N));
     RS_CUDA(p->unsortedSplats.ensure(P * N));
     RS_CUDA(p->sortedSplats.ensure(P * N));
     RS_CUDA(p->sortedCell.ensure(P * N));
@@ -290,6 +291,7 @@ static rs_status allocate(rs_pass* p)
         RS_CUDA(p->spM1.ensure(M)); RS_CUDA(p->spNw.ensure(M)); RS_CUDA(p->spShift.ensure(5 * M)); RS_CUDA(p->spTerms.ensure(M));
     }
     RS_CUDA(p->tileSums.ensure((N + kScanTileElems - 1) / kScanTileElems + 1));
+    RS_CUDA(p->radixScratch.ensure(radix_scratch_words((uint32_t)N, bit_length(N))));
     RS_CUDA(p->total.ensure(8));
     if (p->opt.gatherOption == RS_GATHER_ROBUST && needInter) RS_CUDA(p->shiftedPaths.ensure(8 * N));
     RS_CUDA(p->fault.ensure(1));
@@ -638,14 +640,18 @@ static rs_status enqueue_frame(rs_pass* p, cudaStream_t s, float4* colorDev, con
     p->lastFusedCollect = false;
     const uint32_t numTiles = (N + kScanTileElems - 1) / kScanTileElems;
 
-    auto buildCells = [&](cudaStream_t q, uint32_t* tg, uint32_t* cn, uint32_t* of, uint32_t* cu, uint32_t* un, uint32_t* so, uint32_t* sc,
-                          uint32_t* tot) {
+    // Cell lists of one partition: offsets = exclusive scan of the counts; the splats in (cell,
+    // source) order = a stable radix sort of the source indices by target (an invalid target sorts
+    // last), so the work per splat is bounded however many splats share a cell.
+    auto buildCells = [&](cudaStream_t q, const uint32_t* tg, uint32_t* cn, uint32_t* of, uint32_t* un, uint32_t* so, uint32_t* sc,
+                          uint32_t* tot) -> cudaError_t {
         k_scan_tiles<<<numTiles, 1024, 0, q>>>(cn, of, p->tileSums.p, N);
         k_scan_tile_sums<<<1, 1024, 0, q>>>(p->tileSums.p, numTiles, tot);
         k_scan_add<<<grid(N, 256), 256, 0, q>>>(of, p->tileSums.p, N);
-        k_fill<<<grid(N, 256), 256, 0, q>>>(tg, of, cu, un, N);
-        k_rank_cells<<<grid(N, 256), 256, 0, q>>>(tg, of, cn, un, so, sc, N);
-        p->launches += 5;
+        cudaError_t e = radix_sort_indices_u32(tg, N, N, bit_length(N), so, un, p->radixScratch.p, q);
+        k_sorted_cells<<<grid(N, 256), 256, 0, q>>>(tg, so, sc, N);
+        p->launches += 4 + radix_sort_launches(N, bit_length(N));
+        return e;
     };
 
     // Three independent chains: the primary hits and motion vectors (VBufferRT); the candidate path
@@ -681,25 +687,23 @@ static rs_status enqueue_frame(rs_pass* p, cudaStream_t s, float4* colorDev, con
         {
             stage(p, "reproject", q[2]);
             RS_CUDA(cudaMemsetAsync(p->counts.p, 0, N * 4ull, q[2]));
-            RS_CUDA(cudaMemsetAsync(p->cursor.p, 0, N * 4ull, q[2]));
             k_reproject<<<tiled_blocks(W, H, 256), 256, 0, q[2]>>>(C, prev.res(), prev.recp(), p->targets.p, p->counts.p); p->launches++;
             stage(p, "sortCells", q[2]);
-            buildCells(q[2], p->targets.p, p->counts.p, p->offsets.p, p->cursor.p, p->unsortedSplats.p, p->sortedSplats.p,
-                       p->sortedCell.p, p->total.p);
+            RS_CUDA(buildCells(q[2], p->targets.p, p->counts.p, p->offsets.p, p->unsortedSplats.p, p->sortedSplats.p,
+                               p->sortedCell.p, p->total.p));
         }
         else if (o.temporalReuse == RS_MULTI_SCATTER)
         {
             const uint32_t P = o.numTimePartitions;
             stage(p, "multiReproject", q[2]);
             RS_CUDA(cudaMemsetAsync(p->counts.p, 0, (size_t)P * N * 4ull, q[2]));
-            RS_CUDA(cudaMemsetAsync(p->cursor.p, 0, (size_t)P * N * 4ull, q[2]));
             k_multi_reproject<<<tiled_blocks(W, H, 256), 256, 0, q[2]>>>(C, prev.res(), prev.recp(), p->targets.p, p->counts.p); p->launches++;
             stage(p, "multiSortCells", q[2]);
             for (uint32_t j = 0; j < P; j++)
             {
                 size_t b = (size_t)j * N;
-                buildCells(q[2], p->targets.p + b, p->counts.p + b, p->offsets.p + b, p->cursor.p + b, p->unsortedSplats.p + b,
-                           p->sortedSplats.p + b, p->sortedCell.p + b, p->total.p + j);
+                RS_CUDA(buildCells(q[2], p->targets.p + b, p->counts.p + b, p->offsets.p + b, p->unsortedSplats.p + b,
+                                   p->sortedSplats.p + b, p->sortedCell.p + b, p->total.p + j));
             }
         }
     }
@@ -1375,12 +1379,76 @@ extern "C" RS_API rs_status rs_debug_keep_candidates(rs_pass* p, uint32_t keep)
 }
 
 // ------------------------------------------------------------------ batched instances
-// A batch renders one frame of every member pass with a single CUDA graph launch.  The graph
-// forks one branch per instance from the caller's stream (the instances' stage chains run
-// concurrently and fill the GPU when single instances are small) and joins them at the end.
-// Kernels read each instance's context from device memory, copied from the pinned host context
-// by a node of the graph, so one graph is replayed every frame; a graph is captured per
-// buffer-parity pattern of the members (at most two when spatial reuse is off).
+// A batch renders one frame of every member pass with a single CUDA graph launch.  Two forms:
+//
+// * Flattened (members in the same temporal mode: ScatterBackup with the Clamped gather, one sample
+//   per pixel, matching spatial settings and environment light, past their first frame): every stage
+//   is ONE launch for all members over a flattened work queue (instance k owns work items
+//   [start[k], start[k+1]), each a block of its own grid); the kb_* kernels are persistent by
+//   default (a grid of SMs x resident blocks striding over the queue) and read each instance's
+//   context slot, warp tile width and buffers from device tables built at capture.  The cell lists
+//   (scan and radix sort per member) run as member chains on a side stream.  Stage tile widths
+//   (per stage and resolution) and grid forms (per stage) come from the batch's tuning
+//   (rs_batch_tune times the candidates on a real frame; rs_batch_get/set_tuning carry it).
+// * Per member (any other mix): each member's stage chain is a graph branch.
+// Kernels read each instance's context from device memory, copied from the pinned host context by a
+// node of the graph, so one graph is replayed every frame; a graph is captured per buffer-parity
+// pattern of the members and set of colour buffers.
+namespace {
+
+constexpr uint32_t kBatchTileChoices[3] = {8u, 16u, 32u};
+enum : uint32_t { kGridPersistent = 0, kGridFull = 1 };
+
+// The pixel stages take a warp tile width; the per-splat ones do not.
+bool stage_is_pixel(BatchStage st) { return st != kBatchSbSplatScatter && st != kBatchSbSplatGather; }
+// Stages whose kernels are pure functions of their inputs (a repeated launch writes the same
+// values), so rs_batch_tune may run each candidate configuration in place; the reprojection's
+// counters are cleared before each trial.
+bool stage_tunable(BatchStage st) { return st != kBatchSbCombine; }
+
+struct DeviceBlob
+{
+    void* p = nullptr;
+    ~DeviceBlob() { if (p) cudaFree(p); }
+};
+
+// Host image of the device tables of one flattened frame; every array starts on 256 bytes.
+struct TableBuilder
+{
+    std::vector<uint8_t> bytes;
+    template <typename T> size_t add(const std::vector<T>& v)
+    {
+        size_t off = (bytes.size() + 255) & ~(size_t)255;
+        bytes.resize(off + std::max<size_t>(v.size() * sizeof(T), 1));
+        if (!v.empty()) memcpy(bytes.data() + off, v.data(), v.size() * sizeof(T));
+        return off;
+    }
+};
+
+} // namespace
+
+struct rs_batch_tuning_store
+{
+    // tile width per (stage, width, height); grid form per stage
+    std::vector<rs_batch_tuning_entry> tiles;
+    uint32_t grid[kBatchStageCount];
+    rs_batch_tuning_store() { for (auto& g : grid) g = kGridPersistent; }
+    uint32_t tile(BatchStage st, uint32_t w, uint32_t h) const
+    {
+        for (const auto& e : tiles)
+            if (e.stage == (uint32_t)st && e.width == w && e.height == h) return e.tile;
+        return 8u;
+    }
+    void set_tile(BatchStage st, uint32_t w, uint32_t h, uint32_t tw, float ms)
+    {
+        for (auto& e : tiles)
+            if (e.stage == (uint32_t)st && e.width == w && e.height == h) { e.tile = tw; e.ms = ms; return; }
+        rs_batch_tuning_entry e = {};
+        e.stage = st; e.width = w; e.height = h; e.tile = tw; e.grid = kGridPersistent; e.ms = ms;
+        tiles.push_back(e);
+    }
+};
+
 struct rs_batch
 {
     std::vector<rs_pass*> passes;
@@ -1388,17 +1456,34 @@ struct rs_batch
     std::vector<cudaEvent_t> joins;
     cudaEvent_t fork = nullptr, done = nullptr;
     cudaStream_t capture = nullptr;
+    static constexpr int kChains = 4; // chains of the flattened pipeline: the capture stream + 3
+    cudaStream_t chain[kChains - 1] = {};
+    cudaEvent_t chainFork = nullptr, chainJoin[kChains - 1] = {};
     bool inFlight = false;
-    struct Cached { std::vector<uint64_t> key; std::vector<void*> colors; cudaGraphExec_t exec; };
+    bool flatten = true;
+    uint32_t numSMs = 0;
+    rs_batch_tuning_store tuning;
+    uint64_t tuningVersion = 0; // bumped by rs_batch_tune / rs_batch_set_tuning: cached graphs go stale
+    struct Cached
+    {
+        std::vector<uint64_t> key;
+        std::vector<void*> colors;
+        cudaGraphExec_t exec;
+        std::shared_ptr<DeviceBlob> tables; // device tables of a flattened graph (kept alive with it)
+    };
     std::vector<Cached> graphs;
     std::vector<uint64_t> generations; // the members' generations when the cached graphs were captured
     uint32_t lastLaunches = 0;
+    bool lastFlattened = false;
     ~rs_batch()
     {
         if (done) cudaEventSynchronize(done);
         for (auto& g : graphs) cudaGraphExecDestroy(g.exec);
         for (auto e : joins) cudaEventDestroy(e);
         for (auto s : branch) cudaStreamDestroy(s);
+        for (auto s : chain) if (s) cudaStreamDestroy(s);
+        for (auto e : chainJoin) if (e) cudaEventDestroy(e);
+        if (chainFork) cudaEventDestroy(chainFork);
         if (fork) cudaEventDestroy(fork);
         if (done) cudaEventDestroy(done);
         if (capture) cudaStreamDestroy(capture);
@@ -1423,6 +1508,16 @@ extern "C" RS_API rs_status rs_batch_create(rs_pass* const* passes, uint32_t cou
     RS_CUDA(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
     RS_CUDA(cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming));
     RS_CUDA(cudaStreamCreateWithFlags(&b->capture, cudaStreamNonBlocking));
+    RS_CUDA(cudaEventCreateWithFlags(&b->chainFork, cudaEventDisableTiming));
+    for (int i = 0; i < rs_batch::kChains - 1; i++)
+    {
+        RS_CUDA(cudaStreamCreateWithFlags(&b->chain[i], cudaStreamNonBlocking));
+        RS_CUDA(cudaEventCreateWithFlags(&b->chainJoin[i], cudaEventDisableTiming));
+    }
+    int dev = 0, sms = 0;
+    RS_CUDA(cudaGetDevice(&dev));
+    RS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    b->numSMs = (uint32_t)sms;
     *out = b.release();
     return RS_OK;
 }
@@ -1434,19 +1529,353 @@ extern "C" RS_API rs_status rs_batch_destroy(rs_batch* b)
     return RS_OK;
 }
 
-// frames[i] is the frame of passes[i]; each frames[i].color must be a device buffer (graphs keep
-// the pointers; a new set of pointers captures a new graph).
-extern "C" RS_API rs_status rs_batch_execute(rs_batch* b, const rs_frame_desc* frames, void* streamPtr)
+extern "C" RS_API rs_status rs_batch_set_flatten(rs_batch* b, uint32_t enable)
 {
-    if (!b || !frames) return fail(RS_INVALID_ARG, "batch or frames is NULL");
-    cudaStream_t s = (cudaStream_t)streamPtr;
+    if (!b) return fail(RS_INVALID_ARG, "batch is NULL");
+    b->flatten = enable != 0;
+    return RS_OK;
+}
+
+// The flattened form applies when every member renders the same stage sequence this frame.
+static bool batch_flattenable(const rs_batch* b, const rs_frame_desc* frames)
+{
+    if (!b->flatten) return false;
+    const rs_options& o0 = b->passes[0]->opt;
+    const bool env0 = b->passes[0]->envHost.present != 0;
+    for (size_t i = 0; i < b->passes.size(); i++)
+    {
+        const rs_pass* p = b->passes[i];
+        const rs_options& o = p->opt;
+        if (o.temporalReuse != RS_SCATTER_BACKUP || o.gatherOption != RS_GATHER_CLAMPED || o.samplesPerPixel != 1 || !o.enableTemporalResampling)
+            return false;
+        if (o.enableSpatialResampling != o0.enableSpatialResampling || o.numSpatialIterations != o0.numSpatialIterations ||
+            o.neighborCount != o0.neighborCount || o.scatterBackupMISOption != o0.scatterBackupMISOption)
+            return false;
+        if ((p->envHost.present != 0) != env0 || p->keepCandidates || p->frozen || p->timing) return false;
+        if (p->frameCount == 0 || frames[i].sceneShouldReset || frames[i].mvec || frames[i].vbuffer) return false;
+    }
+    return true;
+}
+
+namespace {
+
+// Everything a flattened frame launches with: per stage its queue (starts, tiles) and grid, and the
+// per-instance argument arrays, as offsets into one device table blob.
+struct FlatPlan
+{
+    uint32_t n = 0;
+    bool env = false, spatial = false, balance = true;
+    uint32_t iterations = 0, neighborCount = 1;
+    uint32_t items[kBatchStageCount] = {};
+    size_t offStart[kBatchStageCount] = {}, offTile[kBatchStageCount] = {};
+    size_t offSlots = 0, offTables = 0, offVbuf = 0, offCand = 0, offReproj = 0, offWave = 0, offWaveColor = 0;
+    std::vector<size_t> offSpatial, offSpatialColor; // per spatial iteration
+    uint32_t grid[kBatchStageCount] = {};
+    TableBuilder tb;
+};
+
+uint32_t stage_items(BatchStage st, uint32_t W, uint32_t H, uint32_t tw)
+{
+    if (!stage_is_pixel(st)) return (W * H + 127u) / 128u;
+    return tiled_blocks_tw(W, H, batched_threads(st), tw);
+}
+
+} // namespace
+
+// Builds the tables of a flattened frame from the members' state after begin_frame.
+static void build_flat_plan(rs_batch* b, const rs_frame_desc* frames, FlatPlan& P)
+{
     const size_t n = b->passes.size();
+    P.n = (uint32_t)n;
+    const rs_options& o0 = b->passes[0]->opt;
+    P.env = b->passes[0]->envHost.present != 0;
+    P.spatial = o0.enableSpatialResampling != 0;
+    P.balance = o0.scatterBackupMISOption == RS_MIS_BALANCE;
+    P.iterations = P.spatial ? o0.numSpatialIterations : 0u;
+    P.neighborCount = o0.neighborCount;
+    std::vector<uint32_t> slots(n);
+    std::vector<CameraTable*> tables(n);
+    std::vector<VbufArgs> vbuf(n);
+    std::vector<CandArgs> cand(n);
+    std::vector<ReprojArgs> reproj(n);
+    std::vector<WaveCtx> wave(n);
+    std::vector<WaveColorArgs> waveColor(n);
+    std::vector<std::vector<SpatialCtx>> sp(P.iterations, std::vector<SpatialCtx>(n));
+    std::vector<std::vector<SpatialColorArgs>> spColor(P.iterations, std::vector<SpatialColorArgs>(n));
     for (size_t i = 0; i < n; i++)
-        if (!frames[i].color) return fail(RS_INVALID_ARG, "batched frames need device colour buffers");
-    // the previous replay reads the pinned host contexts; wait for it before rewriting them
-    if (b->inFlight) RS_CUDA(cudaEventSynchronize(b->done));
-    std::vector<uint64_t> key(n);
-    std::vector<void*> colors(3 * n); // colour, mvec and vbuffer pointers: the graph holds them
+    {
+        rs_pass* p = b->passes[i];
+        const uint32_t N = p->W * p->H;
+        ReservoirSet& curr = p->sets[p->currIdx];
+        ReservoirSet& prev = p->sets[p->prevIdx];
+        slots[i] = p->slot;
+        tables[i] = p->camTable.p;
+        vbuf[i] = VbufArgs{p->vbuffer.p, p->mvec.p};
+        cand[i] = CandArgs{curr.res(), curr.recp()};
+        reproj[i] = ReprojArgs{prev.res(), prev.recp(), p->targets.p, p->counts.p};
+        WaveCtx K;
+        K.fused = true;
+        K.mvec = p->mvec.p;
+        K.curr = curr.res(); K.currRec = curr.recp();
+        K.prev = prev.res(); K.prevRec = prev.recp();
+        K.inter = prev.res(); K.interRec = prev.recp();
+        K.floatingCoords = p->floatingCoords.p;
+        K.counts = p->counts.p; K.offsets = p->offsets.p; K.sorted = p->sortedSplats.p; K.sortedCell = p->sortedCell.p;
+        K.totalSplats = p->total.p;
+        K.m2curr = p->m2curr.p; K.m3curr = p->m3curr.p;
+        K.backupShift = ShiftPlanes{p->backupShift.p, (size_t)N}; K.backupTerms = p->backupTerms.p; K.backupM = p->backupM.p;
+        K.splatShift = ShiftPlanes{p->splatShift.p, (size_t)N}; K.splatTerms = p->splatTerms.p; K.splatM = p->splatM.p;
+        wave[i] = K;
+        float4* color = reinterpret_cast<float4*>(frames[i].color);
+        waveColor[i] = WaveColorArgs{K, P.spatial ? nullptr : color};
+        // the spatial ping-pong of enqueue_frame on local indices (members are not frozen)
+        int cur = p->currIdx, prv = p->prevIdx;
+        for (uint32_t it = 0; it < P.iterations; it++)
+        {
+            std::swap(cur, prv);
+            ReservoirSet& src = p->sets[prv];
+            ReservoirSet& dst = p->sets[cur];
+            SpatialCtx S;
+            S.iteration = it;
+            S.vbuffer = p->vbuffer.p;
+            S.neighborOffsets = p->neighborOffsets.p;
+            S.src = src.res(); S.srcRec = src.recp();
+            S.dst = dst.res(); S.dstRec = dst.recp();
+            S.m1 = p->spM1.p; S.nw = p->spNw.p; S.terms = p->spTerms.p;
+            S.shift = ShiftPlanes{p->spShift.p, (size_t)N * p->opt.neighborCount};
+            sp[it][i] = S;
+            spColor[it][i] = SpatialColorArgs{S, it + 1 == P.iterations ? color : nullptr};
+        }
+    }
+    for (uint32_t st = 0; st < kBatchStageCount; st++)
+    {
+        const BatchStage S = (BatchStage)st;
+        std::vector<uint32_t> start(n + 1), tile(n);
+        uint32_t total = 0;
+        for (size_t i = 0; i < n; i++)
+        {
+            const rs_pass* p = b->passes[i];
+            tile[i] = stage_is_pixel(S) ? b->tuning.tile(S, p->W, p->H) : 8u;
+            start[i] = total;
+            total += stage_items(S, p->W, p->H, tile[i]);
+        }
+        start[n] = total;
+        P.items[st] = total;
+        P.offStart[st] = P.tb.add(start);
+        P.offTile[st] = P.tb.add(tile);
+        const uint32_t resident = b->numSMs * (uint32_t)batched_blocks_per_sm(S, P.env);
+        P.grid[st] = b->tuning.grid[st] == kGridFull ? total : std::min(total, std::max(resident, 1u));
+    }
+    P.offSlots = P.tb.add(slots);
+    P.offTables = P.tb.add(tables);
+    P.offVbuf = P.tb.add(vbuf);
+    P.offCand = P.tb.add(cand);
+    P.offReproj = P.tb.add(reproj);
+    P.offWave = P.tb.add(wave);
+    P.offWaveColor = P.tb.add(waveColor);
+    for (uint32_t it = 0; it < P.iterations; it++)
+    {
+        P.offSpatial.push_back(P.tb.add(sp[it]));
+        P.offSpatialColor.push_back(P.tb.add(spColor[it]));
+    }
+}
+
+// One stage of a flattened frame: a launch over all instances (grid from the plan, or `gridOverride`).
+static void launch_flat(const FlatPlan& P, uint8_t* dev, BatchStage st, size_t argsOff, cudaStream_t s, uint32_t gridOverride = 0)
+{
+    BatchQueue q;
+    q.start = reinterpret_cast<const uint32_t*>(dev + P.offStart[st]);
+    q.tile = reinterpret_cast<const uint32_t*>(dev + P.offTile[st]);
+    q.slot = reinterpret_cast<const uint32_t*>(dev + P.offSlots);
+    q.count = P.n;
+    q.total = P.items[st];
+    if (q.total == 0) return;
+    const uint32_t grid = gridOverride ? gridOverride : P.grid[st];
+    const uint32_t y = (st == kBatchSpCentral || st == kBatchSpNeighbor) ? P.neighborCount : 1u;
+    launch_batched(st, P.env, dim3(grid, y), dim3(batched_threads(st)), s, q, dev + argsOff);
+}
+
+// Issues a flattened frame on `s` (and the batch's chain streams, joined back into s).  The members'
+// contexts are uploaded from their graphCtx staging copies.  With `tune`, every tunable stage first
+// runs each candidate tile width per resolution and each grid form, timed with events on `s`
+// (everything then runs on `s` in order), and the tuning keeps the fastest; the frame's results
+// are the same whichever configuration ran last.
+static rs_status enqueue_flat(rs_batch* b, const rs_frame_desc* frames, FlatPlan& P, uint8_t* dev, cudaStream_t s, bool tune, uint32_t& launches)
+{
+    const size_t n = b->passes.size();
+    launches = 0;
+    for (size_t i = 0; i < n; i++)
+    {
+        rs_pass* p = b->passes[i];
+        RS_CUDA(upload_ctx(p->slot, p->graphCtx, s));
+        RS_CUDA(cudaMemsetAsync(p->fault.p, 0, sizeof(uint32_t), s));
+    }
+    kb_camera_table<<<(uint32_t)n, kMaxCameraKeyframes, 0, s>>>(reinterpret_cast<const uint32_t*>(dev + P.offSlots),
+                                                                  reinterpret_cast<CameraTable* const*>(dev + P.offTables));
+    launches++;
+    cudaStream_t q[rs_batch::kChains];
+    q[0] = s;
+    for (int c = 1; c < rs_batch::kChains; c++) q[c] = tune ? s : b->chain[c - 1];
+    auto fork = [&](int chains) {
+        if (tune) return;
+        cudaEventRecord(b->chainFork, s);
+        for (int c = 1; c < chains; c++) cudaStreamWaitEvent(q[c], b->chainFork, 0);
+    };
+    auto join = [&](int chains) {
+        if (tune) return;
+        for (int c = 1; c < chains; c++)
+        {
+            cudaEventRecord(b->chainJoin[c - 1], q[c]);
+            cudaStreamWaitEvent(s, b->chainJoin[c - 1], 0);
+        }
+    };
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (tune)
+    {
+        RS_CUDA(cudaEventCreate(&e0));
+        RS_CUDA(cudaEventCreate(&e1));
+    }
+    // The stage, tuned first when asked: for each resolution (instances sharing a width and
+    // height) each tile width on that resolution's instances alone, then both grid forms on all.
+    // Each trial is a full launch of the stage over its instances, timed by events on `s`; all
+    // trials write the same values, so the last one leaves the stage's results in place.
+    uint32_t* tq = nullptr; // trial queue: starts (n + 1) and tiles (n)
+    if (tune) RS_CUDA(cudaMalloc(&tq, 4 * (2 * n + 1)));
+    auto stage = [&](BatchStage st, size_t argsOff, cudaStream_t qs, const std::function<void()>& before) -> rs_status {
+        if (!(tune && stage_tunable(st)))
+        {
+            if (before) before();
+            launch_flat(P, dev, st, argsOff, qs);
+            launches++;
+            return RS_OK;
+        }
+        const uint32_t resident = std::max(1u, b->numSMs * (uint32_t)batched_blocks_per_sm(st, P.env));
+        std::vector<uint32_t> tiles(n);
+        for (size_t i = 0; i < n; i++) tiles[i] = stage_is_pixel(st) ? b->tuning.tile(st, b->passes[i]->W, b->passes[i]->H) : 8u;
+        auto trial = [&](const std::vector<uint32_t>& tl, const std::vector<char>& on, uint32_t form, float& ms) -> rs_status {
+            std::vector<uint32_t> start(n + 1);
+            uint32_t total = 0;
+            for (size_t i = 0; i < n; i++)
+            {
+                start[i] = total;
+                if (on[i]) total += stage_items(st, b->passes[i]->W, b->passes[i]->H, tl[i]);
+            }
+            start[n] = total;
+            RS_CUDA(cudaMemcpy(tq, start.data(), 4 * (n + 1), cudaMemcpyHostToDevice));
+            RS_CUDA(cudaMemcpy(tq + n + 1, tl.data(), 4 * n, cudaMemcpyHostToDevice));
+            BatchQueue qq;
+            qq.start = tq; qq.tile = tq + n + 1;
+            qq.slot = reinterpret_cast<const uint32_t*>(dev + P.offSlots);
+            qq.count = (uint32_t)n; qq.total = total;
+            const uint32_t grid = form == kGridFull ? total : std::min(total, resident);
+            const uint32_t y = (st == kBatchSpCentral || st == kBatchSpNeighbor) ? P.neighborCount : 1u;
+            if (before) before();
+            RS_CUDA(cudaEventRecord(e0, s));
+            if (total) launch_batched(st, P.env, dim3(grid, y), dim3(batched_threads(st)), s, qq, dev + argsOff);
+            RS_CUDA(cudaEventRecord(e1, s));
+            RS_CUDA(cudaEventSynchronize(e1));
+            RS_CUDA(cudaGetLastError());
+            RS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            launches++;
+            return RS_OK;
+        };
+        if (stage_is_pixel(st))
+        {
+            std::vector<std::pair<uint32_t, uint32_t>> res;
+            for (const rs_pass* p : b->passes)
+                if (std::find(res.begin(), res.end(), std::make_pair(p->W, p->H)) == res.end()) res.push_back({p->W, p->H});
+            for (auto wh : res)
+            {
+                std::vector<char> on(n, 0);
+                for (size_t i = 0; i < n; i++) on[i] = b->passes[i]->W == wh.first && b->passes[i]->H == wh.second;
+                uint32_t bestTile = 8u;
+                float best = 3e38f;
+                for (uint32_t tw : kBatchTileChoices)
+                {
+                    std::vector<uint32_t> tl = tiles;
+                    for (size_t i = 0; i < n; i++) if (on[i]) tl[i] = tw;
+                    float ms = 0.f;
+                    rs_status r = trial(tl, on, kGridPersistent, ms);
+                    if (r != RS_OK) return r;
+                    if (ms < best) { best = ms; bestTile = tw; }
+                }
+                b->tuning.set_tile(st, wh.first, wh.second, bestTile, best);
+                for (size_t i = 0; i < n; i++) if (on[i]) tiles[i] = bestTile;
+            }
+        }
+        const std::vector<char> all(n, 1);
+        float tp = 0.f, tf = 0.f;
+        rs_status r = trial(tiles, all, kGridPersistent, tp);
+        if (r == RS_OK) r = trial(tiles, all, kGridFull, tf); // the last trial: full grid, chosen tiles
+        if (r != RS_OK) return r;
+        b->tuning.grid[st] = tf < tp ? kGridFull : kGridPersistent;
+        return RS_OK;
+    };
+    rs_status st = RS_OK;
+    auto run = [&](rs_status r) { if (st == RS_OK) st = r; };
+
+    // prologue: primary hits, candidates, and the previous frame's splats and cell lists
+    fork(3);
+    run(stage(kBatchVbuffer, P.offVbuf, q[0], nullptr));
+    run(stage(kBatchCandidates, P.offCand, q[1], nullptr));
+    auto clearCounts = [&]() {
+        for (size_t i = 0; i < n; i++)
+        {
+            rs_pass* p = b->passes[i];
+            cudaMemsetAsync(p->counts.p, 0, (size_t)p->W * p->H * 4ull, q[2]);
+        }
+    };
+    run(stage(kBatchReproject, P.offReproj, q[2], clearCounts));
+    for (size_t i = 0; i < n; i++)
+    {
+        // the member's cell lists (buildCells of enqueue_frame)
+        rs_pass* p = b->passes[i];
+        const uint32_t N = p->W * p->H;
+        const uint32_t numTiles = (N + kScanTileElems - 1) / kScanTileElems;
+        k_scan_tiles<<<numTiles, 1024, 0, q[2]>>>(p->counts.p, p->offsets.p, p->tileSums.p, N);
+        k_scan_tile_sums<<<1, 1024, 0, q[2]>>>(p->tileSums.p, numTiles, p->total.p);
+        k_scan_add<<<(N + 255) / 256, 256, 0, q[2]>>>(p->offsets.p, p->tileSums.p, N);
+        cudaError_t e = radix_sort_indices_u32(p->targets.p, N, N, bit_length(N), p->sortedSplats.p, p->unsortedSplats.p, p->radixScratch.p, q[2]);
+        if (e != cudaSuccess) run(fail(RS_CUDA_ERROR, std::string("batched cell lists: ") + cudaGetErrorString(e)));
+        k_sorted_cells<<<(N + 255) / 256, 256, 0, q[2]>>>(p->targets.p, p->sortedSplats.p, p->sortedCell.p, N);
+        launches += 4 + radix_sort_launches(N, bit_length(N));
+    }
+    join(3);
+    // ScatterBackup shifts: four independent chains, then the combine
+    fork(4);
+    run(stage(kBatchSbCurrScatter, P.offWave, q[0], nullptr));
+    run(stage(kBatchSbCurrGather, P.offWave, q[1], nullptr));
+    run(stage(kBatchSbBackupGather, P.offWave, q[2], nullptr));
+    run(stage(kBatchSbSplatScatter, P.offWave, q[3], nullptr));
+    if (P.balance)
+    {
+        run(stage(kBatchSbBackupScatter, P.offWave, q[2], nullptr));
+        run(stage(kBatchSbSplatGather, P.offWave, q[3], nullptr));
+    }
+    join(4);
+    run(stage(kBatchSbCombine, P.offWaveColor, q[0], nullptr));
+    for (uint32_t it = 0; it < P.iterations; it++)
+    {
+        fork(2);
+        run(stage(kBatchSpCentral, P.offSpatial[it], q[0], nullptr));
+        run(stage(kBatchSpNeighbor, P.offSpatial[it], q[1], nullptr));
+        join(2);
+        run(stage(kBatchSpCombine, P.offSpatialColor[it], q[0], nullptr));
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (tq) cudaFree(tq);
+    RS_CUDA(cudaGetLastError());
+    return st;
+}
+
+// Host-side frame setup of every member (begin_frame, staging of the contexts); the graph key.
+static void batch_begin(rs_batch* b, const rs_frame_desc* frames, cudaStream_t s, std::vector<uint64_t>& key, std::vector<void*>& colors,
+                        bool flat)
+{
+    const size_t n = b->passes.size();
+    key.assign(n + 1, 0);
+    colors.assign(3 * n, nullptr);
     for (size_t i = 0; i < n; i++)
     {
         rs_pass* p = b->passes[i];
@@ -1464,7 +1893,12 @@ extern "C" RS_API rs_status rs_batch_execute(rs_batch* b, const rs_frame_desc* f
                                18u * (p->envHost.present ? 1u : 0u) + 36u * (p->camera.apertureRadius > 0.f ? 1u : 0u);
         key[i] = (p->generation << 8) | shape;
     }
-    // a member whose buffers or options changed makes every graph of the older generation stale
+    key[n] = flat ? (1ull << 63) | b->tuningVersion : 0ull;
+}
+
+static void batch_drop_stale(rs_batch* b)
+{
+    const size_t n = b->passes.size();
     if (!b->graphs.empty() && b->generations.size() == n)
     {
         bool changed = false;
@@ -1477,29 +1911,61 @@ extern "C" RS_API rs_status rs_batch_execute(rs_batch* b, const rs_frame_desc* f
     }
     b->generations.resize(n);
     for (size_t i = 0; i < n; i++) b->generations[i] = b->passes[i]->generation;
+}
+
+// frames[i] is the frame of passes[i]; each frames[i].color must be a device buffer (graphs keep
+// the pointers; a new set of pointers captures a new graph).
+extern "C" RS_API rs_status rs_batch_execute(rs_batch* b, const rs_frame_desc* frames, void* streamPtr)
+{
+    if (!b || !frames) return fail(RS_INVALID_ARG, "batch or frames is NULL");
+    cudaStream_t s = (cudaStream_t)streamPtr;
+    const size_t n = b->passes.size();
+    for (size_t i = 0; i < n; i++)
+        if (!frames[i].color) return fail(RS_INVALID_ARG, "batched frames need device colour buffers");
+    // the previous replay reads the pinned host contexts; wait for it before rewriting them
+    if (b->inFlight) RS_CUDA(cudaEventSynchronize(b->done));
+    const bool flat = batch_flattenable(b, frames);
+    std::vector<uint64_t> key;
+    std::vector<void*> colors;
+    batch_begin(b, frames, s, key, colors, flat);
+    batch_drop_stale(b);
     cudaGraphExec_t exec = nullptr;
     for (auto& g : b->graphs)
         if (g.key == key && g.colors == colors) { exec = g.exec; break; }
     if (!exec)
     {
+        std::shared_ptr<DeviceBlob> tables;
+        FlatPlan plan;
+        if (flat)
+        {
+            build_flat_plan(b, frames, plan);
+            tables.reset(new DeviceBlob());
+            RS_CUDA(cudaMalloc(&tables->p, plan.tb.bytes.size()));
+            RS_CUDA(cudaMemcpy(tables->p, plan.tb.bytes.data(), plan.tb.bytes.size(), cudaMemcpyHostToDevice));
+        }
         cudaStream_t cs = b->capture; // capture never executes; the caller's stream may be the legacy default
         RS_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-        cudaEventRecord(b->fork, cs);
         uint32_t launches = 0;
         rs_status st = RS_OK;
-        for (size_t i = 0; i < n && st == RS_OK; i++)
+        if (flat)
+            st = enqueue_flat(b, frames, plan, static_cast<uint8_t*>(tables->p), cs, false, launches);
+        else
         {
-            rs_pass* p = b->passes[i];
-            cudaStreamWaitEvent(b->branch[i], b->fork, 0);
-            bool timing = p->timing;
-            p->timing = false;
-            p->launches = 0;
-            st = enqueue_frame(p, b->branch[i], reinterpret_cast<float4*>(frames[i].color), reinterpret_cast<const float2*>(frames[i].mvec),
-                               reinterpret_cast<const uint4*>(frames[i].vbuffer), true);
-            p->timing = timing;
-            launches += p->launches;
-            cudaEventRecord(b->joins[i], b->branch[i]);
-            cudaStreamWaitEvent(cs, b->joins[i], 0);
+            cudaEventRecord(b->fork, cs);
+            for (size_t i = 0; i < n && st == RS_OK; i++)
+            {
+                rs_pass* p = b->passes[i];
+                cudaStreamWaitEvent(b->branch[i], b->fork, 0);
+                bool timing = p->timing;
+                p->timing = false;
+                p->launches = 0;
+                st = enqueue_frame(p, b->branch[i], reinterpret_cast<float4*>(frames[i].color), reinterpret_cast<const float2*>(frames[i].mvec),
+                                   reinterpret_cast<const uint4*>(frames[i].vbuffer), true);
+                p->timing = timing;
+                launches += p->launches;
+                cudaEventRecord(b->joins[i], b->branch[i]);
+                cudaStreamWaitEvent(cs, b->joins[i], 0);
+            }
         }
         cudaGraph_t graph = nullptr;
         cudaError_t e = cudaStreamEndCapture(cs, &graph);
@@ -1508,8 +1974,14 @@ extern "C" RS_API rs_status rs_batch_execute(rs_batch* b, const rs_frame_desc* f
         e = cudaGraphInstantiate(&exec, graph, 0);
         cudaGraphDestroy(graph);
         if (e != cudaSuccess) return fail(RS_CUDA_ERROR, std::string("graph instantiate: ") + cudaGetErrorString(e));
-        b->graphs.push_back({key, colors, exec});
+        b->graphs.push_back({key, colors, exec, tables});
         b->lastLaunches = launches;
+        b->lastFlattened = flat;
+    }
+    else
+    {
+        for (auto& g : b->graphs)
+            if (g.exec == exec) b->lastFlattened = (g.key.back() >> 63) != 0;
     }
     RS_CUDA(cudaGraphLaunch(exec, s));
     RS_CUDA(cudaEventRecord(b->done, s));
@@ -1518,8 +1990,82 @@ extern "C" RS_API rs_status rs_batch_execute(rs_batch* b, const rs_frame_desc* f
     return RS_OK;
 }
 
+// Renders one frame like rs_batch_execute, but eagerly and with the tile widths and grid forms of
+// every tunable stage timed in place (the flattened form only); the choices replace the batch's
+// tuning and cached graphs are recaptured.  Synchronous.
+extern "C" RS_API rs_status rs_batch_tune(rs_batch* b, const rs_frame_desc* frames, void* streamPtr)
+{
+    if (!b || !frames) return fail(RS_INVALID_ARG, "batch or frames is NULL");
+    cudaStream_t s = (cudaStream_t)streamPtr;
+    const size_t n = b->passes.size();
+    for (size_t i = 0; i < n; i++)
+        if (!frames[i].color) return fail(RS_INVALID_ARG, "batched frames need device colour buffers");
+    if (b->inFlight) RS_CUDA(cudaEventSynchronize(b->done));
+    if (!batch_flattenable(b, frames))
+        return fail(RS_INVALID_ARG, "rs_batch_tune needs a flattenable frame (every member ScatterBackup/Clamped, one sample per pixel, "
+                                    "the same spatial settings, past its first frame)");
+    std::vector<uint64_t> key;
+    std::vector<void*> colors;
+    batch_begin(b, frames, s, key, colors, true);
+    FlatPlan plan;
+    build_flat_plan(b, frames, plan);
+    DeviceBlob tables;
+    RS_CUDA(cudaMalloc(&tables.p, plan.tb.bytes.size()));
+    RS_CUDA(cudaMemcpy(tables.p, plan.tb.bytes.data(), plan.tb.bytes.size(), cudaMemcpyHostToDevice));
+    uint32_t launches = 0;
+    rs_status st = enqueue_flat(b, frames, plan, static_cast<uint8_t*>(tables.p), s, true, launches);
+    RS_CUDA(cudaStreamSynchronize(s));
+    for (size_t i = 0; i < n; i++) end_frame(b->passes[i]);
+    if (st != RS_OK) return st;
+    b->tuningVersion++;
+    for (auto& g : b->graphs) cudaGraphExecDestroy(g.exec);
+    b->graphs.clear();
+    b->inFlight = false;
+    return RS_OK;
+}
+
+extern "C" RS_API rs_status rs_batch_get_tuning(rs_batch* b, rs_batch_tuning_entry* out, uint32_t* count)
+{
+    if (!b || !count) return fail(RS_INVALID_ARG, "batch or count is NULL");
+    std::vector<rs_batch_tuning_entry> all = b->tuning.tiles;
+    for (uint32_t st = 0; st < kBatchStageCount; st++)
+    {
+        rs_batch_tuning_entry e = {};
+        e.stage = st; e.width = 0; e.height = 0; e.tile = 0; e.grid = b->tuning.grid[st]; e.ms = 0.f;
+        all.push_back(e);
+    }
+    if (out)
+        for (uint32_t i = 0; i < std::min<uint32_t>(*count, (uint32_t)all.size()); i++) out[i] = all[i];
+    *count = (uint32_t)all.size();
+    return RS_OK;
+}
+
+extern "C" RS_API rs_status rs_batch_set_tuning(rs_batch* b, const rs_batch_tuning_entry* in, uint32_t count)
+{
+    if (!b || (count && !in)) return fail(RS_INVALID_ARG, "batch or entries are NULL");
+    for (uint32_t i = 0; i < count; i++)
+    {
+        const rs_batch_tuning_entry& e = in[i];
+        if (e.stage >= kBatchStageCount) return fail(RS_INVALID_ARG, "tuning entry: unknown stage");
+        if (e.width == 0 && e.height == 0)
+        {
+            if (e.grid > kGridFull) return fail(RS_INVALID_ARG, "tuning entry: grid form must be 0 (persistent) or 1 (one block per item)");
+            b->tuning.grid[e.stage] = e.grid;
+        }
+        else
+        {
+            if (e.tile != 8u && e.tile != 16u && e.tile != 32u) return fail(RS_INVALID_ARG, "tuning entry: tile width must be 8, 16 or 32");
+            b->tuning.set_tile((BatchStage)e.stage, e.width, e.height, e.tile, e.ms);
+        }
+    }
+    b->tuningVersion++;
+    return RS_OK;
+}
+
 extern "C" RS_API uint32_t rs_batch_launch_count(rs_batch* b)
 {
     if (!b) return 0u;
     return b->lastLaunches;
 }
+
+extern "C" RS_API uint32_t rs_batch_last_flattened(rs_batch* b) { return b && b->lastFlattened ? 1u : 0u; }

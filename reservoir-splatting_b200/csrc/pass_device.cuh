@@ -67,6 +67,61 @@ __device__ __forceinline__ bool tiled_pixel(uint32_t W, uint32_t H, uint32_t& i)
     return true;
 }
 
+// The work of one block of a stage kernel: its block index within the instance's grid and, for
+// pixel kernels, the warp tile width tw (8, 16 or 32: a warp covers tw x 32/tw pixels, two warps
+// side by side, the rest stacked).  The plain launch uses {blockIdx.x, 8}: tiled_pixel's mapping.
+// Results do not depend on the mapping (every pixel's work is independent of which thread does it).
+struct Blk { uint32_t b; uint32_t tw; };
+
+__device__ __forceinline__ bool tiled_pixel_at(uint32_t W, uint32_t H, Blk blk, uint32_t& i)
+{
+    const uint32_t tw = blk.tw, th = 32u / tw;
+    const uint32_t rowsPerBlock = (blockDim.x >> 6) * th;
+    const uint32_t tilesX = (W + 2u * tw - 1u) / (2u * tw);
+    const uint32_t bx = blk.b % tilesX, by = blk.b / tilesX;
+    const uint32_t w = threadIdx.x >> 5, l = threadIdx.x & 31u;
+    const uint32_t x = bx * 2u * tw + (w & 1u) * tw + (l % tw);
+    const uint32_t y = by * rowsPerBlock + (w >> 1) * th + l / tw;
+    if (x >= W || y >= H) return false;
+    i = y * W + x;
+    return true;
+}
+// Blocks of `threads` (a multiple of 64) that tiled_pixel_at needs for a W x H image at tile width tw.
+RS_HD uint32_t tiled_blocks_tw(uint32_t W, uint32_t H, uint32_t threads, uint32_t tw)
+{
+    const uint32_t rows = (threads / 64u) * (32u / tw);
+    return ((W + 2u * tw - 1u) / (2u * tw)) * ((H + rows - 1u) / rows);
+}
+
+// A flattened work queue over the instances of a batch: instance k owns the work items
+// [start[k], start[k + 1]) (blocks of its own grid), runs with context slot[k] and warp tile width
+// tile[k].  A persistent launch strides over all `total` items.
+struct BatchQueue
+{
+    const uint32_t* start; // count + 1 entries
+    const uint32_t* slot;
+    const uint32_t* tile;
+    uint32_t count, total;
+};
+__device__ __forceinline__ uint32_t batch_instance(const BatchQueue& q, uint32_t t)
+{
+    uint32_t lo = 0, hi = q.count; // start[lo] <= t < start[hi]
+    while (hi - lo > 1u)
+    {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(q.start + mid) <= t) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+__device__ __forceinline__ Blk batch_blk(const BatchQueue& q, uint32_t inst, uint32_t t)
+{
+    Blk b;
+    b.b = t - __ldg(q.start + inst);
+    b.tw = __ldg(q.tile + inst);
+    return b;
+}
+
 __device__ __forceinline__ bool dev_visible(const DevCtx& C, const Ray& r) { return trace_visible(C.bvh, r, C.fault); }
 // The environment light's evaluation, pdf and sampling as calls: the kernels reach them only on
 // misses and env light samples, and inlined they would add their registers to every kernel's

@@ -285,11 +285,11 @@ __global__ void __launch_bounds__(128) k_go_combine(uint32_t slot, WaveCtx K, fl
 
 // ---- stage 1: current sample -> previous domain by reprojection (ScatterBackup...:96-114)
 template <bool kEnv>
-__global__ void __launch_bounds__(128, 8) k_sb_curr_scatter(uint32_t slot, WaveCtx K)
+__device__ __forceinline__ void sb_curr_scatter_body(uint32_t slot, const WaveCtx& K, Blk blk)
 {
     const DevCtx& C = c_ctx[slot];
     uint32_t ri;
-    if (!tiled_pixel(C.W, C.H, ri)) return;
+    if (!tiled_pixel_at(C.W, C.H, blk, ri)) return;
     f3 integrand = load_integrand(K.curr, ri);
     if (!any_gt0(integrand)) return;
     Recon crd = load_rec_rw(K.currRec, ri);
@@ -304,13 +304,30 @@ __global__ void __launch_bounds__(128, 8) k_sb_curr_scatter(uint32_t slot, WaveC
     K.m2curr[ri] = m2;
 }
 
+template <bool kEnv>
+__global__ void __launch_bounds__(128, 8) k_sb_curr_scatter(uint32_t slot, WaveCtx K)
+{
+    sb_curr_scatter_body<kEnv>(slot, K, Blk{blockIdx.x, 8u});
+}
+
+template <bool kEnv>
+__global__ void __launch_bounds__(128, 8) kb_sb_curr_scatter(BatchQueue q, const WaveCtx* __restrict__ args)
+{
+    for (uint32_t t = blockIdx.x; t < q.total; t += gridDim.x)
+    {
+        const uint32_t inst = batch_instance(q, t);
+        const WaveCtx& a = args[inst];
+        sb_curr_scatter_body<kEnv>(__ldg(q.slot + inst), a, batch_blk(q, inst, t));
+    }
+}
+
 // ---- stage 1: current sample -> previous domain by the gather shift (:116-129)
 template <bool kEnv>
-__global__ void __launch_bounds__(128, 9) k_sb_curr_gather(uint32_t slot, WaveCtx K)
+__device__ __forceinline__ void sb_curr_gather_body(uint32_t slot, const WaveCtx& K, Blk blk)
 {
     const DevCtx& C = c_ctx[slot];
     uint32_t ri;
-    if (!tiled_pixel(C.W, C.H, ri)) return;
+    if (!tiled_pixel_at(C.W, C.H, blk, ri)) return;
     Res cr = load_res_rw(K.curr, ri);
     if (!any_gt0(cr.integrand)) return;
     uint32_t x = ri % C.W, y = ri / C.W;
@@ -329,13 +346,30 @@ __global__ void __launch_bounds__(128, 9) k_sb_curr_gather(uint32_t slot, WaveCt
     K.m3curr[ri] = m3;
 }
 
+template <bool kEnv>
+__global__ void __launch_bounds__(128, 9) k_sb_curr_gather(uint32_t slot, WaveCtx K)
+{
+    sb_curr_gather_body<kEnv>(slot, K, Blk{blockIdx.x, 8u});
+}
+
+template <bool kEnv>
+__global__ void __launch_bounds__(128, 9) kb_sb_curr_gather(BatchQueue q, const WaveCtx* __restrict__ args)
+{
+    for (uint32_t t = blockIdx.x; t < q.total; t += gridDim.x)
+    {
+        const uint32_t inst = batch_instance(q, t);
+        const WaveCtx& a = args[inst];
+        sb_curr_gather_body<kEnv>(__ldg(q.slot + inst), a, batch_blk(q, inst, t));
+    }
+}
+
 // ---- stage 1: backup sample -> current domain (:156-166)
 template <bool kEnv>
-__global__ void __launch_bounds__(128, 9) k_sb_backup_gather(uint32_t slot, WaveCtx K)
+__device__ __forceinline__ void sb_backup_gather_body(uint32_t slot, const WaveCtx& K, Blk blk)
 {
     const DevCtx& C = c_ctx[slot];
     uint32_t ri;
-    if (!tiled_pixel(C.W, C.H, ri)) return;
+    if (!tiled_pixel_at(C.W, C.H, blk, ri)) return;
     uint32_t x = ri % C.W, y = ri / C.W;
     Res br; uint32_t bi; f2 fc;
     backup_of(C, K, ri, x, y, br, bi, fc);
@@ -354,13 +388,30 @@ __global__ void __launch_bounds__(128, 9) k_sb_backup_gather(uint32_t slot, Wave
     K.backupM[ri] = make_float2(m1, 0.f);
 }
 
+template <bool kEnv>
+__global__ void __launch_bounds__(128, 9) k_sb_backup_gather(uint32_t slot, WaveCtx K)
+{
+    sb_backup_gather_body<kEnv>(slot, K, Blk{blockIdx.x, 8u});
+}
+
+template <bool kEnv>
+__global__ void __launch_bounds__(128, 9) kb_sb_backup_gather(BatchQueue q, const WaveCtx* __restrict__ args)
+{
+    for (uint32_t t = blockIdx.x; t < q.total; t += gridDim.x)
+    {
+        const uint32_t inst = batch_instance(q, t);
+        const WaveCtx& a = args[inst];
+        sb_backup_gather_body<kEnv>(__ldg(q.slot + inst), a, batch_blk(q, inst, t));
+    }
+}
+
 // ---- stage 2 (Balance): updated backup -> previous domain by reprojection (:171-189)
 template <bool kEnv>
-__global__ void __launch_bounds__(128, 8) k_sb_backup_scatter(uint32_t slot, WaveCtx K)
+__device__ __forceinline__ void sb_backup_scatter_body(uint32_t slot, const WaveCtx& K, Blk blk)
 {
     const DevCtx& C = c_ctx[slot];
     uint32_t ri;
-    if (!tiled_pixel(C.W, C.H, ri)) return;
+    if (!tiled_pixel_at(C.W, C.H, blk, ri)) return;
     uint32_t x = ri % C.W, y = ri / C.W;
     Res br; uint32_t bi; f2 fc;
     backup_of(C, K, ri, x, y, br, bi, fc);
@@ -380,12 +431,29 @@ __global__ void __launch_bounds__(128, 8) k_sb_backup_scatter(uint32_t slot, Wav
     K.backupM[ri].y = m2;
 }
 
+template <bool kEnv>
+__global__ void __launch_bounds__(128, 8) k_sb_backup_scatter(uint32_t slot, WaveCtx K)
+{
+    sb_backup_scatter_body<kEnv>(slot, K, Blk{blockIdx.x, 8u});
+}
+
+template <bool kEnv>
+__global__ void __launch_bounds__(128, 8) kb_sb_backup_scatter(BatchQueue q, const WaveCtx* __restrict__ args)
+{
+    for (uint32_t t = blockIdx.x; t < q.total; t += gridDim.x)
+    {
+        const uint32_t inst = batch_instance(q, t);
+        const WaveCtx& a = args[inst];
+        sb_backup_scatter_body<kEnv>(__ldg(q.slot + inst), a, batch_blk(q, inst, t));
+    }
+}
+
 // ---- stage 1: splatted previous sample -> current domain (:218-235), one thread per splat
 template <bool kEnv>
-__global__ void __launch_bounds__(128, 9) k_sb_splat_scatter(uint32_t slot, WaveCtx K)
+__device__ __forceinline__ void sb_splat_scatter_body(uint32_t slot, const WaveCtx& K, Blk blk)
 {
     const DevCtx& C = c_ctx[slot];
-    uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t j = blk.b * blockDim.x + threadIdx.x;
     if (j >= *K.totalSplats) return;
     uint32_t si = __ldg(&K.sorted[j]);
     uint32_t cell = __ldg(&K.sortedCell[j]);
@@ -404,12 +472,29 @@ __global__ void __launch_bounds__(128, 9) k_sb_splat_scatter(uint32_t slot, Wave
     K.splatM[j] = make_float4(m1, 0.f, sub.x, sub.y);
 }
 
+template <bool kEnv>
+__global__ void __launch_bounds__(128, 9) k_sb_splat_scatter(uint32_t slot, WaveCtx K)
+{
+    sb_splat_scatter_body<kEnv>(slot, K, Blk{blockIdx.x, 8u});
+}
+
+template <bool kEnv>
+__global__ void __launch_bounds__(128, 9) kb_sb_splat_scatter(BatchQueue q, const WaveCtx* __restrict__ args)
+{
+    for (uint32_t t = blockIdx.x; t < q.total; t += gridDim.x)
+    {
+        const uint32_t inst = batch_instance(q, t);
+        const WaveCtx& a = args[inst];
+        sb_splat_scatter_body<kEnv>(__ldg(q.slot + inst), a, batch_blk(q, inst, t));
+    }
+}
+
 // ---- stage 2 (Balance): updated splat -> previous domain by the gather shift (:237-253)
 template <bool kEnv>
-__global__ void __launch_bounds__(128, 9) k_sb_splat_gather(uint32_t slot, WaveCtx K)
+__device__ __forceinline__ void sb_splat_gather_body(uint32_t slot, const WaveCtx& K, Blk blk)
 {
     const DevCtx& C = c_ctx[slot];
-    uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t j = blk.b * blockDim.x + threadIdx.x;
     if (j >= *K.totalSplats) return;
     uint32_t si = __ldg(&K.sorted[j]);
     f3 integrand = load_integrand(K.prev, si);
@@ -436,12 +521,29 @@ __global__ void __launch_bounds__(128, 9) k_sb_splat_gather(uint32_t slot, WaveC
     K.splatM[j].y = m3;
 }
 
+template <bool kEnv>
+__global__ void __launch_bounds__(128, 9) k_sb_splat_gather(uint32_t slot, WaveCtx K)
+{
+    sb_splat_gather_body<kEnv>(slot, K, Blk{blockIdx.x, 8u});
+}
+
+template <bool kEnv>
+__global__ void __launch_bounds__(128, 9) kb_sb_splat_gather(BatchQueue q, const WaveCtx* __restrict__ args)
+{
+    for (uint32_t t = blockIdx.x; t < q.total; t += gridDim.x)
+    {
+        const uint32_t inst = batch_instance(q, t);
+        const WaveCtx& a = args[inst];
+        sb_splat_gather_body<kEnv>(__ldg(q.slot + inst), a, batch_blk(q, inst, t));
+    }
+}
+
 // ---- combine: the GRIS order of ScatterBackupTemporalResampling.rt.slang:91-283 on stored shifts
-__global__ void __launch_bounds__(128) k_sb_combine(uint32_t slot, WaveCtx K, float4* __restrict__ color)
+__device__ __forceinline__ void sb_combine_body(uint32_t slot, const WaveCtx& K, float4* __restrict__ color, Blk blk)
 {
     const DevCtx& C = c_ctx[slot];
     uint32_t ri;
-    if (!tiled_pixel(C.W, C.H, ri)) return;
+    if (!tiled_pixel_at(C.W, C.H, blk, ri)) return;
     uint32_t x = ri % C.W, y = ri / C.W;
     const bool useConf = C.useConfTemporal != 0;
     const bool balance = C.scatterBackupMIS == 0u;
@@ -550,6 +652,21 @@ __global__ void __launch_bounds__(128) k_sb_combine(uint32_t slot, WaveCtx K, fl
     }
 }
 
+__global__ void __launch_bounds__(128) k_sb_combine(uint32_t slot, WaveCtx K, float4* __restrict__ color)
+{
+    sb_combine_body(slot, K, color, Blk{blockIdx.x, 8u});
+}
+
+__global__ void __launch_bounds__(128) kb_sb_combine(BatchQueue q, const WaveColorArgs* __restrict__ args)
+{
+    for (uint32_t t = blockIdx.x; t < q.total; t += gridDim.x)
+    {
+        const uint32_t inst = batch_instance(q, t);
+        const WaveColorArgs& a = args[inst];
+        sb_combine_body(__ldg(q.slot + inst), a.K, a.color, batch_blk(q, inst, t));
+    }
+}
+
 // ============================================================ spatial resampling, wavefront form
 // Per (pixel, neighbour slot i): the central -> neighbour shift (m1) and the neighbour -> central
 // shift (SpatialResampling.rt.slang:110-174).  The start index of the neighbour sequence is the
@@ -566,13 +683,13 @@ __device__ __forceinline__ bool spatial_neighbor(const DevCtx& C, uint32_t itera
 }
 
 template <bool kEnv>
-__global__ void __launch_bounds__(128, 10) k_sp_central(uint32_t slot, SpatialCtx S)
+__device__ __forceinline__ void sp_central_body(uint32_t slot, const SpatialCtx& S, Blk blk)
 {
     const DevCtx& C = c_ctx[slot];
     // blockIdx.y: the neighbour; blockIdx.x / threadIdx.x: the pixel (tiled)
     const uint32_t N = C.W * C.H;
     uint32_t ri;
-    if (blockIdx.y >= C.neighborCount || !tiled_pixel(C.W, C.H, ri)) return;
+    if (blockIdx.y >= C.neighborCount || !tiled_pixel_at(C.W, C.H, blk, ri)) return;
     const uint32_t i = blockIdx.y, t = i * N + ri;
     uint32_t x = ri % C.W, y = ri / C.W;
     int nx, ny;
@@ -597,13 +714,30 @@ __global__ void __launch_bounds__(128, 10) k_sp_central(uint32_t slot, SpatialCt
 }
 
 template <bool kEnv>
-__global__ void __launch_bounds__(128, 9) k_sp_neighbor(uint32_t slot, SpatialCtx S)
+__global__ void __launch_bounds__(128, 10) k_sp_central(uint32_t slot, SpatialCtx S)
+{
+    sp_central_body<kEnv>(slot, S, Blk{blockIdx.x, 8u});
+}
+
+template <bool kEnv>
+__global__ void __launch_bounds__(128, 10) kb_sp_central(BatchQueue q, const SpatialCtx* __restrict__ args)
+{
+    for (uint32_t t = blockIdx.x; t < q.total; t += gridDim.x)
+    {
+        const uint32_t inst = batch_instance(q, t);
+        const SpatialCtx& a = args[inst];
+        sp_central_body<kEnv>(__ldg(q.slot + inst), a, batch_blk(q, inst, t));
+    }
+}
+
+template <bool kEnv>
+__device__ __forceinline__ void sp_neighbor_body(uint32_t slot, const SpatialCtx& S, Blk blk)
 {
     const DevCtx& C = c_ctx[slot];
     // blockIdx.y: the neighbour; blockIdx.x / threadIdx.x: the pixel (tiled)
     const uint32_t N = C.W * C.H;
     uint32_t ri;
-    if (blockIdx.y >= C.neighborCount || !tiled_pixel(C.W, C.H, ri)) return;
+    if (blockIdx.y >= C.neighborCount || !tiled_pixel_at(C.W, C.H, blk, ri)) return;
     const uint32_t i = blockIdx.y, t = i * N + ri;
     uint32_t x = ri % C.W, y = ri / C.W;
     int nx, ny;
@@ -628,12 +762,29 @@ __global__ void __launch_bounds__(128, 9) k_sp_neighbor(uint32_t slot, SpatialCt
     S.nw[t] = nw;
 }
 
-__global__ void __launch_bounds__(128) k_sp_combine(uint32_t slot, SpatialCtx S, float4* __restrict__ color)
+template <bool kEnv>
+__global__ void __launch_bounds__(128, 9) k_sp_neighbor(uint32_t slot, SpatialCtx S)
+{
+    sp_neighbor_body<kEnv>(slot, S, Blk{blockIdx.x, 8u});
+}
+
+template <bool kEnv>
+__global__ void __launch_bounds__(128, 9) kb_sp_neighbor(BatchQueue q, const SpatialCtx* __restrict__ args)
+{
+    for (uint32_t t = blockIdx.x; t < q.total; t += gridDim.x)
+    {
+        const uint32_t inst = batch_instance(q, t);
+        const SpatialCtx& a = args[inst];
+        sp_neighbor_body<kEnv>(__ldg(q.slot + inst), a, batch_blk(q, inst, t));
+    }
+}
+
+__device__ __forceinline__ void sp_combine_body(uint32_t slot, const SpatialCtx& S, float4* __restrict__ color, Blk blk)
 {
     const DevCtx& C = c_ctx[slot];
     uint32_t ri;
     const uint32_t N = C.W * C.H;
-    if (!tiled_pixel(C.W, C.H, ri)) return;
+    if (!tiled_pixel_at(C.W, C.H, blk, ri)) return;
     uint32_t x = ri % C.W, y = ri / C.W;
     const bool useConf = C.useConfSpatial != 0;
     const uint32_t neighborCount = C.neighborCount;
@@ -691,6 +842,21 @@ __global__ void __launch_bounds__(128) k_sp_combine(uint32_t slot, SpatialCtx S,
     {
         f3 c = dst.integrand * res_ucw(dst);
         color[ri] = make_float4(c.x, c.y, c.z, 1.f);
+    }
+}
+
+__global__ void __launch_bounds__(128) k_sp_combine(uint32_t slot, SpatialCtx S, float4* __restrict__ color)
+{
+    sp_combine_body(slot, S, color, Blk{blockIdx.x, 8u});
+}
+
+__global__ void __launch_bounds__(128) kb_sp_combine(BatchQueue q, const SpatialColorArgs* __restrict__ args)
+{
+    for (uint32_t t = blockIdx.x; t < q.total; t += gridDim.x)
+    {
+        const uint32_t inst = batch_instance(q, t);
+        const SpatialColorArgs& a = args[inst];
+        sp_combine_body(__ldg(q.slot + inst), a.S, a.color, batch_blk(q, inst, t));
     }
 }
 

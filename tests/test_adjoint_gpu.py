@@ -73,6 +73,7 @@ def test_backward_matches_oracle_and_fp64_differences(rs, oracle_mod, scenes):
             FD[m, k] += _richardson(loss, P0[m, k])
     g = G.cpu().numpy().astype(np.float64)
     assert stats[0] > 0 and stats[1] == 0
+    assert stats[2] == 0, f"{stats[2]} replayed paths without an identified emitter"
     assert np.abs(g - O).max() <= ORACLE_TOL * np.abs(O).max()
     assert np.abs(g - FD).max() <= GRAD_TOL * np.abs(FD).max()
     big = np.abs(FD) > 1e-2 * np.abs(FD).max()
@@ -159,3 +160,62 @@ def test_autograd_l2_loss_matches_direct_backward(rs, scenes):
     assert scale > 0
     assert (p.grad - direct).abs().max().item() <= 1e-5 * scale
     assert torch.all(p.grad[:, 7] == 0)
+
+
+@pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
+def test_replay_gradient_is_unbiased_over_seeds(rs, scenes):
+    """The estimator itself, not just the replay: for a linear loss (the sum of the last frame's
+    pixels), the mean over K seeds of rs_backward's gradient equals the central difference of the
+    mean image over the same seeds, to within the statistical error of the paired per-seed
+    differences.  Each seed fixes the random numbers (useFixedSeed), so the differences move only
+    the parameters; the resampling decisions still change with them, which is what the replay
+    estimator must average out (E[df(y)/dtheta W] = dI/dtheta because W is a contribution weight of y
+    for every theta)."""
+    import torch
+    import reservoir_splatting_b200.adjoint as adj
+    W = H = 24
+    K = 192
+    sc = scenes.inverse_scene(grid=40, spheres=6, subdiv=2, emitters=4)
+    renderer = adj.Renderer(sc, PROPS, W, H)
+    cams = [scenes.translate_camera(f, W, H) for f in range(2)]
+    theta = renderer.params().clone()
+    n = renderer.num_materials
+    # the terrain bands' albedos, one sphere material's roughness, one emitter's radiance
+    checks = [(0, 0), (1, 1), (2, 2), (3, 0), (5, 3), (n - 1, 4), (n - 2, 5)]
+    hs = {0: 0.02, 1: 0.02, 2: 0.02, 3: 0.02, 4: 0.5, 5: 0.5}
+    gsum = np.zeros(len(checks))
+    dsum = np.zeros(len(checks))
+    d2sum = np.zeros(len(checks))
+    gimg = torch.ones((len(cams), H, W, 4), device="cuda")
+    gimg[:-1] = 0.0
+    gimg[..., 3] = 0.0
+
+    def last_sum(params):
+        renderer.apply(params)
+        imgs, _ = renderer.render(cams, keep_checkpoints=False)
+        return float(imgs[-1, ..., :3].double().sum().item())
+
+    for k in range(K):
+        renderer.pass_.useFixedSeed = True
+        renderer.pass_.fixedSeed = 7919 * (k + 1)
+        renderer.apply(theta)
+        imgs, ckpts = renderer.render(cams)
+        g = renderer.backward(gimg, ckpts).cpu().numpy()
+        for j, (m, c) in enumerate(checks):
+            h = hs[c]
+            tp, tm = theta.clone(), theta.clone()
+            tp[m, c] += h
+            tm[m, c] -= h
+            fd = (last_sum(tp) - last_sum(tm)) / (2 * h)
+            gsum[j] += g[m, c]
+            d = g[m, c] - fd
+            dsum[j] += d
+            d2sum[j] += d * d
+    renderer.pass_.close()
+    gmean = gsum / K
+    dmean = dsum / K
+    se = np.sqrt(np.maximum(d2sum / K - dmean ** 2, 0.0) / (K - 1))
+    for j, (m, c) in enumerate(checks):
+        assert abs(dmean[j]) <= 4.0 * se[j] + 1e-3 * abs(gmean[j]) + 1e-6, \
+            f"material {m} param {c}: mean gradient {gmean[j]:.6g}, mean (gradient - difference) {dmean[j]:.3g} +- {se[j]:.3g}"
+    assert np.abs(gmean).max() > 0

@@ -89,3 +89,84 @@ def test_batch_member_changes_options_size_and_aperture(rs, scenes):
     batch.close()
     for p in solo + batched:
         p.close()
+
+
+def _uniform_members(rs, scenes, env=False):
+    terrain = scenes.terrain_spheres(seed=4, grid=32, spheres=6, subdiv=2, lights=6, extent=30.0, height=3.0)
+    props = {"temporalReuse": "ScatterBackup", "gatherOption": "Clamped", "maxSurfaceBounces": 2, "enableSpatialResampling": True,
+             "neighborCount": 2}
+    cfgs = [(scenes.cornell_box(0), scenes.cornell_camera, 48, 32), (terrain, lambda f, w, h: scenes.orbit_camera(f, w, h, radius=25.0, height_above=10.0), 64, 40),
+            (scenes.cornell_box(2), scenes.cornell_camera, 37, 23), (scenes.cornell_box(1), scenes.cornell_camera, 48, 32)]
+    solo, batched = [], []
+    sky = scenes.sky_env_map(64, 32, seed=1) if env else None
+    for sc, _, w, h in cfgs:
+        for lst in (solo, batched):
+            p = rs.ReservoirSplatting(props, w, h)
+            p.set_scene(sc)
+            if env:
+                p.set_env_map(sky)
+            lst.append(p)
+    return cfgs, solo, batched
+
+
+@pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
+@pytest.mark.parametrize("env", [False, True], ids=["emissive", "env"])
+def test_flattened_batch_matches_individual_passes(rs, scenes, env):
+    """Members in one ScatterBackup/Clamped configuration run the flattened form (one persistent launch
+    per stage over a work queue of all members, uneven resolutions) from their second frame on, and
+    give bit for bit the images and reservoirs of the passes rendered alone, at every tile width and
+    grid form, and after rs_batch_tune."""
+    import torch
+    cfgs, solo, batched = _uniform_members(rs, scenes, env)
+    outs = [torch.zeros((h, w, 4), dtype=torch.float32, device="cuda") for _, _, w, h in cfgs]
+    batch = rs.Batch(batched)
+    stream = torch.cuda.current_stream().cuda_stream
+    settings = [None, (16, 0), (32, 1), (8, 1), "tune", None]
+    for f in range(len(settings) + 1):
+        cams = [cfg[1](f, cfg[2], cfg[3]) for cfg in cfgs]
+        ref = [p.render(c) for p, c in zip(solo, cams)]
+        setting = settings[f - 1] if f > 0 else None
+        if setting == "tune":
+            batch.tune(cams, [o.data_ptr() for o in outs], stream=stream)
+            tuning = batch.tuning()
+            assert any(e["width"] > 0 for e in tuning) and all(e["tile"] in (0, 8, 16, 32) for e in tuning)
+        else:
+            if isinstance(setting, tuple):
+                tw, grid = setting
+                entries = [{"stage": st, "width": w, "height": h, "tile": tw, "grid": 0} for st in rs.abi.BATCH_STAGES for _, _, w, h in cfgs]
+                entries += [{"stage": st, "width": 0, "height": 0, "tile": 0, "grid": grid} for st in rs.abi.BATCH_STAGES]
+                batch.set_tuning(entries)
+            batch.execute(cams, [o.data_ptr() for o in outs], stream=stream)
+        torch.cuda.synchronize()
+        assert batch.last_flattened() == (f > 0 and setting != "tune") or setting == "tune"
+        for k in range(len(cfgs)):
+            np.testing.assert_array_equal(outs[k].cpu().numpy(), ref[k], err_msg=f"instance {k} frame {f} setting {setting}")
+            np.testing.assert_array_equal(batched[k].get_buffer("curr_reservoirs"), solo[k].get_buffer("curr_reservoirs"))
+    batch.close()
+    for p in solo + batched:
+        p.close()
+
+
+@pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
+def test_tuning_cache_round_trip(rs, scenes, tmp_path):
+    import torch
+    cfgs, solo, batched = _uniform_members(rs, scenes)
+    outs = [torch.zeros((h, w, 4), dtype=torch.float32, device="cuda") for _, _, w, h in cfgs]
+    cache = tmp_path / "tuning.json"
+    batch = rs.Batch(batched, tuning_cache=str(cache))
+    stream = torch.cuda.current_stream().cuda_stream
+    for f in range(2):
+        cams = [cfg[1](f, cfg[2], cfg[3]) for cfg in cfgs]
+        if f == 0:
+            batch.execute(cams, [o.data_ptr() for o in outs], stream=stream)
+        else:
+            tuned = batch.tune(cams, [o.data_ptr() for o in outs], stream=stream)
+    assert cache.exists()
+    again = rs.Batch(batched, tuning_cache=str(cache))
+    assert again.tuning() == [dict(e, ms=e["ms"]) for e in tuned]
+    with pytest.raises(rs.RsError, match="tile width"):
+        again.set_tuning([{"stage": "candidates", "width": 48, "height": 32, "tile": 12, "grid": 0}])
+    again.close()
+    batch.close()
+    for p in solo + batched:
+        p.close()

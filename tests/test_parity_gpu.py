@@ -190,3 +190,39 @@ def test_moving_spheres(rs, oracle_mod, scenes, mode, builder):
         P.compare_reservoirs(f"frame{f}.reservoirs", gpu.get_buffer("curr_reservoirs"), ora.get_buffer("curr_reservoirs"))
         P.assert_close(f"frame{f}.color", img_g, img_o)
     gpu.close()
+
+
+@pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
+@pytest.mark.parametrize("mode", ["ScatterOnly", "ScatterBackup"])
+def test_zoom_out_crowded_cells(rs, oracle_mod, scenes, mode):
+    """A zoom-out by 32x between frames (the focal length drops from 32x to 1x the base): the
+    previous frame's pixels splat into a small patch, hundreds of splats per cell.  The cell lists
+    (a stable radix sort by cell, bounded work per splat) and the resampling over them match the
+    oracle bit for bit."""
+    base = scenes.cornell_camera(0, 64, 64).focal_length
+
+    def cam(f, w, h):
+        c = scenes.cornell_camera(0, w, h)
+        c.focal_length = base * (32.0 if f % 2 == 0 else 1.0)
+        return c
+
+    props = {"temporalReuse": mode, "gatherOption": "Clamped", "maxSurfaceBounces": 1, "enableSpatialResampling": False}
+    gpu = rs.ReservoirSplatting(props, 64, 64)
+    gpu.keep_candidates(True)
+    ora = oracle_mod.OraclePass(props, 64, 64)
+    sc = scenes.cornell_box(0)
+    gpu.set_scene(sc)
+    ora.set_scene(sc)
+    most = 0
+    for f in range(4):
+        c = cam(f, 64, 64)
+        a, b = gpu.render(c), ora.execute(c)
+        if f > 0:
+            counts = gpu.get_buffer("cell_counters")
+            P.assert_equal(f"frame{f}.cell_counters", counts, ora.get_buffer("cell_counters"))
+            P.assert_equal(f"frame{f}.sorted_splats", gpu.get_buffer("sorted_splats"), ora.get_buffer("sorted_splats"))
+            most = max(most, int(counts.max()))
+        P.compare_reservoirs(f"frame{f}.reservoirs", gpu.get_buffer("curr_reservoirs"), ora.get_buffer("curr_reservoirs"))
+        assert P.bit_mismatch_fraction(a, b) == 0.0, f"frame {f}"
+    assert most >= 256, most
+    gpu.close()
