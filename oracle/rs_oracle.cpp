@@ -2205,6 +2205,8 @@ static bool replay_pixel(const Pass& p, const PathReservoir& r, const Reconnecti
             HitInfo h; float t;
             if (p.bvh.closest(mk_ray(o2, rd.secondWo, 0.f, kRayTMax), h, t))
                 out.emitter = emitter_of(p, p.loadSD(h, rd.secondWo));
+            // a light sample whose ray slips through the seam between two triangles of the light
+            if (out.emitter == kInvalidIndex && rd.lightIsNEE) out.emitter = emissive_material_with_radiance(p.lv, rd.irradiance);
         }
     }
     f3 B = out.nv == 2 ? out.v[1].g.value : mk3(1.f);

@@ -308,6 +308,7 @@ class Batch:
         h = C.c_void_p()
         _check(self._lib.rs_batch_create(arr, len(self.passes), C.byref(h)))
         self._h = h
+        self.flatten = flatten
         _check(self._lib.rs_batch_set_flatten(self._h, 1 if flatten else 0))
         self.tuning_cache = tuning_cache
         if tuning_cache:
@@ -332,6 +333,29 @@ class Batch:
         if self.tuning_cache:
             self._save_tuning(entries)
         return entries
+
+    def choose_form(self, camera_frames, color_ptrs, stream: int = 0) -> dict:
+        """Renders the frames of `camera_frames` (a list of per-member camera lists, an even number of
+        frames) alternately in the flattened form and as per-member graph branches, times each on the
+        device, and keeps the faster form (stored with the tuning cache).  Both forms render the same
+        images, so the choice changes only the speed."""
+        import torch
+        times = {True: 0.0, False: 0.0}
+        for k, cams in enumerate(camera_frames):
+            form = k % 2 == 0
+            _check(self._lib.rs_batch_set_flatten(self._h, 1 if form else 0))
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s = torch.cuda.ExternalStream(stream) if stream else torch.cuda.current_stream()
+            a.record(s)
+            self.execute(cams, color_ptrs, stream)
+            b.record(s)
+            torch.cuda.synchronize()
+            times[form] += a.elapsed_time(b)
+        self.flatten = times[True] <= times[False]
+        _check(self._lib.rs_batch_set_flatten(self._h, 1 if self.flatten else 0))
+        if self.tuning_cache:
+            self._save_tuning(self.tuning())
+        return {"flattened_ms": times[True], "branches_ms": times[False], "flatten": self.flatten}
 
     def tuning(self) -> list:
         n = C.c_uint32(0)
@@ -362,18 +386,23 @@ class Batch:
         from pathlib import Path
         path = Path(self.tuning_cache)
         if path.exists():
-            data = json.loads(path.read_text())
-            entries = data.get(self._gpu_key())
-            if entries:
-                self.set_tuning(entries)
+            data = json.loads(path.read_text()).get(self._gpu_key())
+            if data:
+                self.set_tuning(data["entries"])
+                self.flatten = bool(data.get("flatten", self.flatten))
+                _check(self._lib.rs_batch_set_flatten(self._h, 1 if self.flatten else 0))
 
     def _save_tuning(self, entries):
         import json
         from pathlib import Path
         path = Path(self.tuning_cache)
         data = json.loads(path.read_text()) if path.exists() else {}
-        data[self._gpu_key()] = entries
+        data[self._gpu_key()] = {"entries": entries, "flatten": self.flatten}
         path.write_text(json.dumps(data, indent=1))
+
+    def set_flatten(self, enable: bool):
+        self.flatten = bool(enable)
+        _check(self._lib.rs_batch_set_flatten(self._h, 1 if enable else 0))
 
     def last_flattened(self) -> bool:
         return bool(self._lib.rs_batch_last_flattened(self._h))

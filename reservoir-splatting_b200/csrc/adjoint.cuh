@@ -117,6 +117,8 @@ __device__ inline void adj_pixel(const DevCtx& C, const ResPlanes& res, const Re
             HitInfo h; float t;
             if (trace_closest(C.bvh, mk_ray(o2, rd.secondWo, 0.f, kRayTMax), h, t, C.fault))
                 emitter = dev_emitter_of(C, dev_sd(C, h, rd.secondWo));
+            // a light sample whose ray slips through the seam between two triangles of the light
+            if (emitter == kInvalidIndex && rd.lightIsNEE) emitter = emissive_material_with_radiance(C.lights, rd.irradiance);
         }
     }
     const f3 A = nv >= 1 ? V[0].value : mk3(1.f);

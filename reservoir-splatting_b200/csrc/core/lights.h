@@ -109,6 +109,25 @@ RS_HD bool sample_emissive_power(const LightView& L, f3 posW, SampleGen& sg, Tri
     return true;
 }
 
+// The material of the emissive triangles whose radiance is Le (each channel within 1e-5 relative),
+// when exactly one material qualifies; kInvalidIndex otherwise.  The adjoint's fallback for a light
+// sample it cannot find again by tracing (a ray through the seam between two triangles of a light).
+RS_HD uint32_t emissive_material_with_radiance(const LightView& L, f3 Le)
+{
+    uint32_t found = kInvalidIndex;
+    for (uint32_t i = 0; i < L.count; i++)
+    {
+        const LightTriangle& t = L.tris[i];
+        const float a[3] = {t.Le[0], t.Le[1], t.Le[2]}, b[3] = {Le.x, Le.y, Le.z};
+        bool match = true;
+        for (int c = 0; c < 3; c++) match = match && f_abs(a[c] - b[c]) <= 1e-5f * f_max(f_abs(a[c]), 1e-30f);
+        if (!match) continue;
+        if (found != kInvalidIndex && found != t.materialID) return kInvalidIndex;
+        found = t.materialID;
+    }
+    return found;
+}
+
 // EmissivePowerSampler::evalPdf + evalTrianglePdf: solid-angle pdf at posW of a hit on light triangleIndex.
 RS_HD float eval_emissive_pdf(const LightView& L, f3 posW, uint32_t triangleIndex, f3 hitPosW, f3 hitNormalW)
 {

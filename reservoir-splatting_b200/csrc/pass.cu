@@ -34,6 +34,12 @@ static rs_status fail(rs_status s, const std::string& msg)
 // Lets entry points defined in other files report through rs_last_error_string().
 namespace rs { void set_last_error(const std::string& msg) { g_lastError = msg; } }
 
+#define RS_CUDA_STATUS(call)                                                                        \
+    do {                                                                                            \
+        rs_status s_ = (call);                                                                      \
+        if (s_ != RS_OK) return s_;                                                                 \
+    } while (0)
+
 #define RS_CUDA(call)                                                                               \
     do {                                                                                            \
         cudaError_t e_ = (call);                                                                    \
@@ -1456,9 +1462,11 @@ struct rs_batch
     std::vector<cudaEvent_t> joins;
     cudaEvent_t fork = nullptr, done = nullptr;
     cudaStream_t capture = nullptr;
-    static constexpr int kChains = 4; // chains of the flattened pipeline: the capture stream + 3
-    cudaStream_t chain[kChains - 1] = {};
-    cudaEvent_t chainFork = nullptr, chainJoin[kChains - 1] = {};
+    static constexpr int kChains = 4; // chains of one group's flattened pipeline: its stream + 3
+    // Stream sets of the flattened groups (one group per resolution): group g uses
+    // groupStream[g * kChains + c], c = 0 its main stream; events likewise.
+    std::vector<cudaStream_t> groupStream;
+    std::vector<cudaEvent_t> groupFork, groupJoin; // per group: fork of its chains; per chain: join
     bool inFlight = false;
     bool flatten = true;
     uint32_t numSMs = 0;
@@ -1481,9 +1489,9 @@ struct rs_batch
         for (auto& g : graphs) cudaGraphExecDestroy(g.exec);
         for (auto e : joins) cudaEventDestroy(e);
         for (auto s : branch) cudaStreamDestroy(s);
-        for (auto s : chain) if (s) cudaStreamDestroy(s);
-        for (auto e : chainJoin) if (e) cudaEventDestroy(e);
-        if (chainFork) cudaEventDestroy(chainFork);
+        for (auto s : groupStream) cudaStreamDestroy(s);
+        for (auto e : groupFork) cudaEventDestroy(e);
+        for (auto e : groupJoin) cudaEventDestroy(e);
         if (fork) cudaEventDestroy(fork);
         if (done) cudaEventDestroy(done);
         if (capture) cudaStreamDestroy(capture);
@@ -1508,12 +1516,6 @@ extern "C" RS_API rs_status rs_batch_create(rs_pass* const* passes, uint32_t cou
     RS_CUDA(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
     RS_CUDA(cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming));
     RS_CUDA(cudaStreamCreateWithFlags(&b->capture, cudaStreamNonBlocking));
-    RS_CUDA(cudaEventCreateWithFlags(&b->chainFork, cudaEventDisableTiming));
-    for (int i = 0; i < rs_batch::kChains - 1; i++)
-    {
-        RS_CUDA(cudaStreamCreateWithFlags(&b->chain[i], cudaStreamNonBlocking));
-        RS_CUDA(cudaEventCreateWithFlags(&b->chainJoin[i], cudaEventDisableTiming));
-    }
     int dev = 0, sms = 0;
     RS_CUDA(cudaGetDevice(&dev));
     RS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
@@ -1563,6 +1565,7 @@ namespace {
 // per-instance argument arrays, as offsets into one device table blob.
 struct FlatPlan
 {
+    std::vector<uint32_t> members; // indices into the batch's passes
     uint32_t n = 0;
     bool env = false, spatial = false, balance = true;
     uint32_t iterations = 0, neighborCount = 1;
@@ -1582,13 +1585,15 @@ uint32_t stage_items(BatchStage st, uint32_t W, uint32_t H, uint32_t tw)
 
 } // namespace
 
-// Builds the tables of a flattened frame from the members' state after begin_frame.
-static void build_flat_plan(rs_batch* b, const rs_frame_desc* frames, FlatPlan& P)
+// Builds the tables of a flattened frame of the batch members `members` from their state after
+// begin_frame.
+static void build_flat_plan(rs_batch* b, const rs_frame_desc* frames, const std::vector<uint32_t>& members, FlatPlan& P)
 {
-    const size_t n = b->passes.size();
+    const size_t n = members.size();
+    P.members = members;
     P.n = (uint32_t)n;
-    const rs_options& o0 = b->passes[0]->opt;
-    P.env = b->passes[0]->envHost.present != 0;
+    const rs_options& o0 = b->passes[members[0]]->opt;
+    P.env = b->passes[members[0]]->envHost.present != 0;
     P.spatial = o0.enableSpatialResampling != 0;
     P.balance = o0.scatterBackupMISOption == RS_MIS_BALANCE;
     P.iterations = P.spatial ? o0.numSpatialIterations : 0u;
@@ -1604,7 +1609,8 @@ static void build_flat_plan(rs_batch* b, const rs_frame_desc* frames, FlatPlan& 
     std::vector<std::vector<SpatialColorArgs>> spColor(P.iterations, std::vector<SpatialColorArgs>(n));
     for (size_t i = 0; i < n; i++)
     {
-        rs_pass* p = b->passes[i];
+        rs_pass* p = b->passes[members[i]];
+        const rs_frame_desc& fr = frames[members[i]];
         const uint32_t N = p->W * p->H;
         ReservoirSet& curr = p->sets[p->currIdx];
         ReservoirSet& prev = p->sets[p->prevIdx];
@@ -1626,7 +1632,7 @@ static void build_flat_plan(rs_batch* b, const rs_frame_desc* frames, FlatPlan& 
         K.backupShift = ShiftPlanes{p->backupShift.p, (size_t)N}; K.backupTerms = p->backupTerms.p; K.backupM = p->backupM.p;
         K.splatShift = ShiftPlanes{p->splatShift.p, (size_t)N}; K.splatTerms = p->splatTerms.p; K.splatM = p->splatM.p;
         wave[i] = K;
-        float4* color = reinterpret_cast<float4*>(frames[i].color);
+        float4* color = reinterpret_cast<float4*>(fr.color);
         waveColor[i] = WaveColorArgs{K, P.spatial ? nullptr : color};
         // the spatial ping-pong of enqueue_frame on local indices (members are not frozen)
         int cur = p->currIdx, prv = p->prevIdx;
@@ -1654,7 +1660,7 @@ static void build_flat_plan(rs_batch* b, const rs_frame_desc* frames, FlatPlan& 
         uint32_t total = 0;
         for (size_t i = 0; i < n; i++)
         {
-            const rs_pass* p = b->passes[i];
+            const rs_pass* p = b->passes[members[i]];
             tile[i] = stage_is_pixel(S) ? b->tuning.tile(S, p->W, p->H) : 8u;
             start[i] = total;
             total += stage_items(S, p->W, p->H, tile[i]);
@@ -1700,13 +1706,15 @@ static void launch_flat(const FlatPlan& P, uint8_t* dev, BatchStage st, size_t a
 // runs each candidate tile width per resolution and each grid form, timed with events on `s`
 // (everything then runs on `s` in order), and the tuning keeps the fastest; the frame's results
 // are the same whichever configuration ran last.
-static rs_status enqueue_flat(rs_batch* b, const rs_frame_desc* frames, FlatPlan& P, uint8_t* dev, cudaStream_t s, bool tune, uint32_t& launches)
+static rs_status enqueue_flat(rs_batch* b, FlatPlan& P, uint8_t* dev, cudaStream_t s, const cudaStream_t* chains, cudaEvent_t forkEv,
+                              const cudaEvent_t* joinEv, bool tune, uint32_t& launches)
 {
-    const size_t n = b->passes.size();
+    const size_t n = P.n;
+    auto member = [&](size_t i) { return b->passes[P.members[i]]; };
     launches = 0;
     for (size_t i = 0; i < n; i++)
     {
-        rs_pass* p = b->passes[i];
+        rs_pass* p = member(i);
         RS_CUDA(upload_ctx(p->slot, p->graphCtx, s));
         RS_CUDA(cudaMemsetAsync(p->fault.p, 0, sizeof(uint32_t), s));
     }
@@ -1715,18 +1723,18 @@ static rs_status enqueue_flat(rs_batch* b, const rs_frame_desc* frames, FlatPlan
     launches++;
     cudaStream_t q[rs_batch::kChains];
     q[0] = s;
-    for (int c = 1; c < rs_batch::kChains; c++) q[c] = tune ? s : b->chain[c - 1];
-    auto fork = [&](int chains) {
+    for (int c = 1; c < rs_batch::kChains; c++) q[c] = tune ? s : chains[c - 1];
+    auto fork = [&](int nch) {
         if (tune) return;
-        cudaEventRecord(b->chainFork, s);
-        for (int c = 1; c < chains; c++) cudaStreamWaitEvent(q[c], b->chainFork, 0);
+        cudaEventRecord(forkEv, s);
+        for (int c = 1; c < nch; c++) cudaStreamWaitEvent(q[c], forkEv, 0);
     };
-    auto join = [&](int chains) {
+    auto join = [&](int nch) {
         if (tune) return;
-        for (int c = 1; c < chains; c++)
+        for (int c = 1; c < nch; c++)
         {
-            cudaEventRecord(b->chainJoin[c - 1], q[c]);
-            cudaStreamWaitEvent(s, b->chainJoin[c - 1], 0);
+            cudaEventRecord(joinEv[c - 1], q[c]);
+            cudaStreamWaitEvent(s, joinEv[c - 1], 0);
         }
     };
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -1751,14 +1759,14 @@ static rs_status enqueue_flat(rs_batch* b, const rs_frame_desc* frames, FlatPlan
         }
         const uint32_t resident = std::max(1u, b->numSMs * (uint32_t)batched_blocks_per_sm(st, P.env));
         std::vector<uint32_t> tiles(n);
-        for (size_t i = 0; i < n; i++) tiles[i] = stage_is_pixel(st) ? b->tuning.tile(st, b->passes[i]->W, b->passes[i]->H) : 8u;
+        for (size_t i = 0; i < n; i++) tiles[i] = stage_is_pixel(st) ? b->tuning.tile(st, member(i)->W, member(i)->H) : 8u;
         auto trial = [&](const std::vector<uint32_t>& tl, const std::vector<char>& on, uint32_t form, float& ms) -> rs_status {
             std::vector<uint32_t> start(n + 1);
             uint32_t total = 0;
             for (size_t i = 0; i < n; i++)
             {
                 start[i] = total;
-                if (on[i]) total += stage_items(st, b->passes[i]->W, b->passes[i]->H, tl[i]);
+                if (on[i]) total += stage_items(st, member(i)->W, member(i)->H, tl[i]);
             }
             start[n] = total;
             RS_CUDA(cudaMemcpy(tq, start.data(), 4 * (n + 1), cudaMemcpyHostToDevice));
@@ -1782,12 +1790,12 @@ static rs_status enqueue_flat(rs_batch* b, const rs_frame_desc* frames, FlatPlan
         if (stage_is_pixel(st))
         {
             std::vector<std::pair<uint32_t, uint32_t>> res;
-            for (const rs_pass* p : b->passes)
-                if (std::find(res.begin(), res.end(), std::make_pair(p->W, p->H)) == res.end()) res.push_back({p->W, p->H});
+            for (size_t i = 0; i < n; i++)
+                if (std::find(res.begin(), res.end(), std::make_pair(member(i)->W, member(i)->H)) == res.end()) res.push_back({member(i)->W, member(i)->H});
             for (auto wh : res)
             {
                 std::vector<char> on(n, 0);
-                for (size_t i = 0; i < n; i++) on[i] = b->passes[i]->W == wh.first && b->passes[i]->H == wh.second;
+                for (size_t i = 0; i < n; i++) on[i] = member(i)->W == wh.first && member(i)->H == wh.second;
                 uint32_t bestTile = 8u;
                 float best = 3e38f;
                 for (uint32_t tw : kBatchTileChoices)
@@ -1821,7 +1829,7 @@ static rs_status enqueue_flat(rs_batch* b, const rs_frame_desc* frames, FlatPlan
     auto clearCounts = [&]() {
         for (size_t i = 0; i < n; i++)
         {
-            rs_pass* p = b->passes[i];
+            rs_pass* p = member(i);
             cudaMemsetAsync(p->counts.p, 0, (size_t)p->W * p->H * 4ull, q[2]);
         }
     };
@@ -1829,7 +1837,7 @@ static rs_status enqueue_flat(rs_batch* b, const rs_frame_desc* frames, FlatPlan
     for (size_t i = 0; i < n; i++)
     {
         // the member's cell lists (buildCells of enqueue_frame)
-        rs_pass* p = b->passes[i];
+        rs_pass* p = member(i);
         const uint32_t N = p->W * p->H;
         const uint32_t numTiles = (N + kScanTileElems - 1) / kScanTileElems;
         k_scan_tiles<<<numTiles, 1024, 0, q[2]>>>(p->counts.p, p->offsets.p, p->tileSums.p, N);
@@ -1913,6 +1921,58 @@ static void batch_drop_stale(rs_batch* b)
     for (size_t i = 0; i < n; i++) b->generations[i] = b->passes[i]->generation;
 }
 
+// The groups of a flattened frame: the members of each resolution, in member order, in chunks of
+// at most kFlatGroupMax.  Each group's stages are their own flattened launches on their own
+// streams, so different groups' stages overlap (one group's latency-bound traversal with another's
+// bandwidth-bound combine, and a group's slowest member holds back only its group at each stage).
+// Measured on the 64-instance configuration: one group per resolution 246 instance-frames/s,
+// chunks of 8 242, one group for all 242.
+constexpr size_t kFlatGroupMax = 64;
+static std::vector<std::vector<uint32_t>> flat_groups(const rs_batch* b)
+{
+    std::vector<std::vector<uint32_t>> byRes;
+    std::vector<std::pair<uint32_t, uint32_t>> res;
+    for (uint32_t i = 0; i < (uint32_t)b->passes.size(); i++)
+    {
+        const auto wh = std::make_pair(b->passes[i]->W, b->passes[i]->H);
+        auto it = std::find(res.begin(), res.end(), wh);
+        if (it == res.end()) { res.push_back(wh); byRes.push_back({i}); }
+        else byRes[it - res.begin()].push_back(i);
+    }
+    std::vector<std::vector<uint32_t>> groups;
+    for (const auto& r : byRes)
+    {
+        const size_t chunks = (r.size() + kFlatGroupMax - 1) / kFlatGroupMax;
+        for (size_t c = 0; c < chunks; c++)
+        {
+            // near-equal chunks of the resolution's members
+            const size_t a = r.size() * c / chunks, e = r.size() * (c + 1) / chunks;
+            groups.emplace_back(r.begin() + a, r.begin() + e);
+        }
+    }
+    return groups;
+}
+
+static rs_status ensure_group_streams(rs_batch* b, size_t groups)
+{
+    while (b->groupFork.size() < groups)
+    {
+        for (int c = 0; c < rs_batch::kChains; c++)
+        {
+            cudaStream_t q;
+            cudaEvent_t e;
+            RS_CUDA(cudaStreamCreateWithFlags(&q, cudaStreamNonBlocking));
+            RS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            b->groupStream.push_back(q);
+            b->groupJoin.push_back(e); // c = 0: the group's join into the caller's stream
+        }
+        cudaEvent_t f;
+        RS_CUDA(cudaEventCreateWithFlags(&f, cudaEventDisableTiming));
+        b->groupFork.push_back(f);
+    }
+    return RS_OK;
+}
+
 // frames[i] is the frame of passes[i]; each frames[i].color must be a device buffer (graphs keep
 // the pointers; a new set of pointers captures a new graph).
 extern "C" RS_API rs_status rs_batch_execute(rs_batch* b, const rs_frame_desc* frames, void* streamPtr)
@@ -1935,20 +1995,46 @@ extern "C" RS_API rs_status rs_batch_execute(rs_batch* b, const rs_frame_desc* f
     if (!exec)
     {
         std::shared_ptr<DeviceBlob> tables;
-        FlatPlan plan;
+        std::vector<FlatPlan> plans;
+        std::vector<size_t> planOff;
         if (flat)
         {
-            build_flat_plan(b, frames, plan);
+            // one plan per resolution group, all tables in one blob
+            const auto groups = flat_groups(b);
+            RS_CUDA_STATUS(ensure_group_streams(b, groups.size()));
+            plans.resize(groups.size());
+            size_t total = 0;
+            for (size_t g = 0; g < groups.size(); g++)
+            {
+                build_flat_plan(b, frames, groups[g], plans[g]);
+                planOff.push_back(total);
+                total += (plans[g].tb.bytes.size() + 255) & ~(size_t)255;
+            }
             tables.reset(new DeviceBlob());
-            RS_CUDA(cudaMalloc(&tables->p, plan.tb.bytes.size()));
-            RS_CUDA(cudaMemcpy(tables->p, plan.tb.bytes.data(), plan.tb.bytes.size(), cudaMemcpyHostToDevice));
+            RS_CUDA(cudaMalloc(&tables->p, total));
+            for (size_t g = 0; g < plans.size(); g++)
+                RS_CUDA(cudaMemcpy(static_cast<uint8_t*>(tables->p) + planOff[g], plans[g].tb.bytes.data(), plans[g].tb.bytes.size(),
+                                   cudaMemcpyHostToDevice));
         }
         cudaStream_t cs = b->capture; // capture never executes; the caller's stream may be the legacy default
         RS_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
         uint32_t launches = 0;
         rs_status st = RS_OK;
         if (flat)
-            st = enqueue_flat(b, frames, plan, static_cast<uint8_t*>(tables->p), cs, false, launches);
+        {
+            cudaEventRecord(b->fork, cs);
+            for (size_t g = 0; g < plans.size() && st == RS_OK; g++)
+            {
+                cudaStream_t* gs = &b->groupStream[g * rs_batch::kChains];
+                cudaEvent_t* gj = &b->groupJoin[g * rs_batch::kChains];
+                cudaStreamWaitEvent(gs[0], b->fork, 0);
+                uint32_t l = 0;
+                st = enqueue_flat(b, plans[g], static_cast<uint8_t*>(tables->p) + planOff[g], gs[0], gs + 1, b->groupFork[g], gj + 1, false, l);
+                launches += l;
+                cudaEventRecord(gj[0], gs[0]);
+                cudaStreamWaitEvent(cs, gj[0], 0);
+            }
+        }
         else
         {
             cudaEventRecord(b->fork, cs);
@@ -2007,14 +2093,20 @@ extern "C" RS_API rs_status rs_batch_tune(rs_batch* b, const rs_frame_desc* fram
     std::vector<uint64_t> key;
     std::vector<void*> colors;
     batch_begin(b, frames, s, key, colors, true);
-    FlatPlan plan;
-    build_flat_plan(b, frames, plan);
-    DeviceBlob tables;
-    RS_CUDA(cudaMalloc(&tables.p, plan.tb.bytes.size()));
-    RS_CUDA(cudaMemcpy(tables.p, plan.tb.bytes.data(), plan.tb.bytes.size(), cudaMemcpyHostToDevice));
-    uint32_t launches = 0;
-    rs_status st = enqueue_flat(b, frames, plan, static_cast<uint8_t*>(tables.p), s, true, launches);
-    RS_CUDA(cudaStreamSynchronize(s));
+    rs_status st = RS_OK;
+    for (const auto& members : flat_groups(b))
+    {
+        // each resolution group in turn, everything on `s`
+        FlatPlan plan;
+        build_flat_plan(b, frames, members, plan);
+        DeviceBlob tables;
+        RS_CUDA(cudaMalloc(&tables.p, plan.tb.bytes.size()));
+        RS_CUDA(cudaMemcpy(tables.p, plan.tb.bytes.data(), plan.tb.bytes.size(), cudaMemcpyHostToDevice));
+        uint32_t launches = 0;
+        st = enqueue_flat(b, plan, static_cast<uint8_t*>(tables.p), s, nullptr, nullptr, nullptr, true, launches);
+        RS_CUDA(cudaStreamSynchronize(s));
+        if (st != RS_OK) break;
+    }
     for (size_t i = 0; i < n; i++) end_frame(b->passes[i]);
     if (st != RS_OK) return st;
     b->tuningVersion++;

@@ -162,7 +162,10 @@ def test_tuning_cache_round_trip(rs, scenes, tmp_path):
         else:
             tuned = batch.tune(cams, [o.data_ptr() for o in outs], stream=stream)
     assert cache.exists()
+    form = batch.choose_form([[cfg[1](f, cfg[2], cfg[3]) for cfg in cfgs] for f in range(2, 4)], [o.data_ptr() for o in outs], stream=stream)
+    assert set(form) == {"flattened_ms", "branches_ms", "flatten"} and form["flattened_ms"] > 0 and form["branches_ms"] > 0
     again = rs.Batch(batched, tuning_cache=str(cache))
+    assert again.flatten == form["flatten"]
     assert again.tuning() == [dict(e, ms=e["ms"]) for e in tuned]
     with pytest.raises(rs.RsError, match="tile width"):
         again.set_tuning([{"stage": "candidates", "width": 48, "height": 32, "tile": 12, "grid": 0}])

@@ -80,3 +80,40 @@ def test_static_cell_lists_match_rs_execute_on_two_calls(rs, scenes):
         np.testing.assert_array_equal(got[: ref_sorted.size], ref_sorted, err_msg=f"sorted splats, call {calls}")
     assert calls == 2
     p.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
+def test_static_cell_lists_fewer_cells_than_splats_and_crowded_cells(rs):
+    """Targets at and beyond the cell count (numCells, numCells + 5, 0xffffffff) mean "no cell";
+    fewer cells than splats, and one cell holding most splats (the work per splat stays bounded).
+    Counts, offsets and the listed splats against numpy, on two calls in a row."""
+    import torch
+
+    torch.cuda.set_device(0)
+    lib = rs.load_library()
+    rng = np.random.default_rng(5)
+    n, cells = 300_000, 4_000
+    t = rng.integers(0, cells, n).astype(np.uint32)
+    t[rng.random(n) < 0.6] = 17               # a crowded cell
+    t[::7] = cells
+    t[::11] = cells + 5
+    t[::13] = 0xFFFFFFFF
+    valid = t < cells
+    ref_counts = np.bincount(t[valid], minlength=cells).astype(np.uint32)
+    ref_offsets = np.concatenate([[0], np.cumsum(ref_counts)[:-1]]).astype(np.uint32)
+    ref_sorted = np.argsort(np.where(valid, t, cells), kind="stable")[: int(valid.sum())].astype(np.uint32)
+    targets = torch.from_numpy(t.view(np.int32)).cuda()
+    counts = torch.empty(cells, dtype=torch.int32, device="cuda")
+    offsets = torch.empty(cells, dtype=torch.int32, device="cuda")
+    sorted_ = torch.empty(n, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    for call in range(2):
+        sorted_.fill_(-1)
+        status = lib.rs_build_cell_lists_static(targets.data_ptr(), n, cells, counts.data_ptr(), offsets.data_ptr(),
+                                                sorted_.data_ptr(), C.c_void_p(stream))
+        assert status == 0, lib.rs_last_error_string().decode()
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(counts.cpu().numpy().view(np.uint32), ref_counts, err_msg=f"counts, call {call}")
+        np.testing.assert_array_equal(offsets.cpu().numpy().view(np.uint32), ref_offsets, err_msg=f"offsets, call {call}")
+        np.testing.assert_array_equal(sorted_.cpu().numpy().view(np.uint32)[: ref_sorted.size], ref_sorted, err_msg=f"sorted, call {call}")
