@@ -55,8 +55,8 @@ enum { RS_GATHER_ONLY = 0, RS_SCATTER_ONLY = 1, RS_SCATTER_BACKUP = 2, RS_MULTI_
 enum { RS_GATHER_FAST = 0, RS_GATHER_CLAMPED = 1, RS_GATHER_ROBUST = 2 };
 /* ScatterBackupMIS (ShiftOptions.slang:49-53) */
 enum { RS_MIS_BALANCE = 0, RS_MIS_PAIRWISE = 1 };
-/* MISHeuristic (Params.slang:48-53); PowerExp is not supported */
-enum { RS_MIS_HEURISTIC_BALANCE = 0, RS_MIS_HEURISTIC_POWER_TWO = 1 };
+/* MISHeuristic (Params.slang:48-53); PowerExp uses rs_options.misPowerExponent (0.01 .. 10) */
+enum { RS_MIS_HEURISTIC_BALANCE = 0, RS_MIS_HEURISTIC_POWER_TWO = 1, RS_MIS_HEURISTIC_POWER_EXP = 2 };
 /* sampleGenerator: SAMPLE_GENERATOR_TINY_UNIFORM = 0 (reference default); 2 = PCG32 */
 enum { RS_SG_TINY_UNIFORM = 0, RS_SG_PCG32 = 2 };
 

@@ -398,7 +398,7 @@ struct Pass
     ShadingData loadSD(const HitInfo& h, f3 rayDir) const { return load_shading_data(scene.tri.data(), scene.materials.data(), h, rayDir); }
     BsdfData instance(const ShadingData& sd) const { return setup_material(scene.materials[sd.materialID], sd.frontFacing); }
 
-    static float evalMIS(uint32_t heuristic, float p0, float p1)
+    static float evalMIS(uint32_t heuristic, float exponent, float p0, float p1)
     {
         // PathTracer.slang:480-508 with n0 = n1 = 1
         if (heuristic == RS_MIS_HEURISTIC_POWER_TWO)
@@ -406,10 +406,15 @@ struct Pass
             float q0 = (1.f * p0) * (1.f * p0), q1 = (1.f * p1) * (1.f * p1);
             return q0 / (q0 + q1);
         }
+        if (heuristic == RS_MIS_HEURISTIC_POWER_EXP) // :498-503, pow(n * p, kMISPowerExponent)
+        {
+            float q0 = f_pow_pos(1.f * p0, exponent), q1 = f_pow_pos(1.f * p1, exponent);
+            return q0 / (q0 + q1);
+        }
         float q0 = 1.f * p0, q1 = 1.f * p1;
         return q0 / (q0 + q1);
     }
-    float mis(float p0, float p1) const { return evalMIS(opt.misHeuristic, p0, p1); }
+    float mis(float p0, float p1) const { return evalMIS(opt.misHeuristic, opt.misPowerExponent, p0, p1); }
 
     void orient(CameraData& c, float t) const { c = camera; orient_camera(cm, c, frameCount, t); }
 
@@ -2654,6 +2659,11 @@ __attribute__((visibility("default"))) void ro_test_fmath(int kind, const float*
         default: y[i] = f_acos(v); break;
         }
     }
+}
+// f_pow_pos(x[i], e[i]) (the PowerExp MIS heuristic's power).
+__attribute__((visibility("default"))) void ro_test_pow(const float* x, const float* e, float* y, uint32_t n)
+{
+    for (uint32_t i = 0; i < n; i++) y[i] = f_pow_pos(x[i], e[i]);
 }
 __attribute__((visibility("default"))) void ro_test_f16(const float* x, uint16_t* h, float* back, uint32_t n)
 {

@@ -17,7 +17,7 @@ STATUS_NAMES = {0: "RS_OK", 1: "RS_INVALID_ARG", 2: "RS_OOM", 3: "RS_CUDA_ERROR"
 TEMPORAL_REUSE = {"GatherOnly": 0, "ScatterOnly": 1, "ScatterBackup": 2, "MultiScatter": 3}
 GATHER_MECHANISM = {"Fast": 0, "Clamped": 1, "Robust": 2}
 SCATTER_BACKUP_MIS = {"Balance": 0, "Pairwise": 1}
-MIS_HEURISTIC = {"Balance": 0, "PowerTwo": 1}
+MIS_HEURISTIC = {"Balance": 0, "PowerTwo": 1, "PowerExp": 2}
 SAMPLE_GENERATOR = {"TinyUniform": 0, "PCG32": 2}
 
 BUF = {

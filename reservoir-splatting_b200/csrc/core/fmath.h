@@ -210,4 +210,72 @@ RS_HDI float f16_to_f32(uint16_t h)
     return u2f(sign | ((exp + 112u) << 23) | (mant << 13));
 }
 
+// ---- x^e for the PowerExp MIS heuristic (PathTracer.slang:498-503), as 2^(e log2 x) in binary64
+// (correctly rounded +, -, *, / on host and device, so both produce the same bits), rounded once to
+// binary32.  log2: x = m 2^k with m in [sqrt(1/2), sqrt(2)), ln m = 2 atanh(s) = 2 (s + s^3/3 +
+// s^5/5 + ...) with s = (m - 1) / (m + 1), |s| <= 0.172 (terms to s^23).  2^f for the fraction
+// f in [-1/2, 1/2]: the Taylor series of exp(f ln 2) to its 17th power, then the power of two by
+// the exponent bits.  About 1 ulp of binary32 over the MIS weights' range.
+constexpr double kLn2D = 0.693147180559945309417232121458;
+constexpr double kInvLn2D = 1.442695040888963407359924681002;
+
+RS_HD uint64_t d2u(double d) { uint64_t u; memcpy(&u, &d, 8); return u; }
+RS_HD double u2d(uint64_t u) { double d; memcpy(&d, &u, 8); return d; }
+
+// log2 x for finite x > 0.
+RS_HD double d_log2(double x)
+{
+    int k = 0;
+    if (x < 2.2250738585072014e-308) { x = x * 18014398509481984.0; k = -54; } // subnormal: scale by 2^54
+    uint64_t b = d2u(x);
+    k += (int)((b >> 52) & 0x7ffu) - 1023;
+    double m = u2d((b & 0x000fffffffffffffull) | 0x3ff0000000000000ull); // [1, 2)
+    if (m > 1.4142135623730951) { m = m * 0.5; k += 1; }
+    const double s = (m - 1.0) / (m + 1.0), s2 = s * s;
+    double poly = 1.0 / 23.0;
+    poly = poly * s2 + 1.0 / 21.0;
+    poly = poly * s2 + 1.0 / 19.0;
+    poly = poly * s2 + 1.0 / 17.0;
+    poly = poly * s2 + 1.0 / 15.0;
+    poly = poly * s2 + 1.0 / 13.0;
+    poly = poly * s2 + 1.0 / 11.0;
+    poly = poly * s2 + 1.0 / 9.0;
+    poly = poly * s2 + 1.0 / 7.0;
+    poly = poly * s2 + 1.0 / 5.0;
+    poly = poly * s2 + 1.0 / 3.0;
+    poly = poly * s2 + 1.0;
+    return (double)k + (2.0 * s * poly) * kInvLn2D;
+}
+
+// 2^y for finite y (0 below 2^-1075, +inf above 2^1024).
+RS_HD double d_exp2(double y)
+{
+    if (y < -1075.0) return 0.0;
+    if (y >= 1024.0) return u2d(0x7ff0000000000000ull);
+    const double n = floor(y + 0.5);
+    const double t = (y - n) * kLn2D; // |t| <= ln2 / 2
+    // 1 / n! for n = 1 .. 17 (the n = 0 term is added last)
+    const double inv[17] = {1.0, 1.0 / 2.0, 1.0 / 6.0, 1.0 / 24.0, 1.0 / 120.0, 1.0 / 720.0, 1.0 / 5040.0, 1.0 / 40320.0,
+                            1.0 / 362880.0, 1.0 / 3628800.0, 1.0 / 39916800.0, 1.0 / 479001600.0, 1.0 / 6227020800.0,
+                            1.0 / 87178291200.0, 1.0 / 1307674368000.0, 1.0 / 20922789888000.0, 1.0 / 355687428096000.0};
+    double r = inv[16];
+#pragma unroll
+    for (int i = 15; i >= 0; i--) r = r * t + inv[i];
+    r = r * t + 1.0;
+    int e = (int)n;
+    // scale by 2^e in at most two exact steps (each factor a normal power of two)
+    if (e > 1023) { r = r * u2d(0x7fe0000000000000ull); e -= 1023; }
+    if (e < -1022) { r = r * u2d(0x0010000000000000ull); e += 1022; }
+    return r * u2d((uint64_t)(e + 1023) << 52);
+}
+
+// x^e for x >= 0 and e > 0 (0 for x = 0; NaN for NaN or negative x, as pow gives).
+RS_HD float f_pow_pos(float x, float e)
+{
+    if (x == 0.f) return 0.f;
+    if (!(x > 0.f)) return u2f(0x7fc00000u);
+    if (x == INFINITY) return x;
+    return (float)d_exp2((double)e * d_log2((double)x));
+}
+
 } // namespace rs

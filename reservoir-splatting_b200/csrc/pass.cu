@@ -242,7 +242,9 @@ static rs_status validate(const rs_options* o)
     if (o->frameWidth == 0 || o->frameHeight == 0 || o->frameWidth > 4096 || o->frameHeight > 4096)
         return fail(RS_INVALID_ARG, "Frame dimensions up to 4096 pixels width/height are supported");
     if (o->sampleGenerator != RS_SG_TINY_UNIFORM && o->sampleGenerator != RS_SG_PCG32) return fail(RS_INVALID_ARG, "unknown sampleGenerator");
-    if (o->misHeuristic > 1) return fail(RS_INVALID_ARG, "misHeuristic must be Balance or PowerTwo");
+    if (o->misHeuristic > 2) return fail(RS_INVALID_ARG, "misHeuristic must be Balance, PowerTwo or PowerExp");
+    if (o->misHeuristic == RS_MIS_HEURISTIC_POWER_EXP && !(o->misPowerExponent >= 0.01f && o->misPowerExponent <= 10.f))
+        return fail(RS_INVALID_ARG, "misPowerExponent must be in [0.01, 10]");
     if (o->temporalReuse > 3) return fail(RS_INVALID_ARG, "unknown temporalReuse");
     if (o->gatherOption > 2) return fail(RS_INVALID_ARG, "unknown gatherOption");
     if (o->scatterBackupMISOption > 1) return fail(RS_INVALID_ARG, "unknown scatterBackupMISOption");
@@ -568,6 +570,7 @@ static void begin_frame(rs_pass* p, const rs_frame_desc* f)
     C.maxSurfaceBounces = o.maxSurfaceBounces; C.maxDiffuseBounces = o.maxDiffuseBounces;
     C.maxSpecularBounces = o.maxSpecularBounces; C.maxTransmissionBounces = o.maxTransmissionBounces;
     C.useRussianRoulette = o.useRussianRoulette; C.misHeuristic = o.misHeuristic; C.disableCaustics = o.disableCaustics;
+    C.misPowerExponent = o.misPowerExponent;
     C.specularRoughnessThreshold = o.specularRoughnessThreshold;
     C.useConfTemporal = o.useConfidenceWeightsTemporally; C.useConfSpatial = o.useConfidenceWeightsSpatially;
     C.gatherOption = o.gatherOption; C.scatterBackupMIS = o.scatterBackupMISOption; C.numTimePartitions = o.numTimePartitions;

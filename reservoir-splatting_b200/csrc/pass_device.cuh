@@ -35,6 +35,7 @@ struct DevCtx
     uint32_t spp;
     uint32_t maxSurfaceBounces, maxDiffuseBounces, maxSpecularBounces, maxTransmissionBounces;
     uint32_t useRussianRoulette, misHeuristic, disableCaustics;
+    float misPowerExponent; // PowerExp heuristic (misHeuristic 2)
     float specularRoughnessThreshold;
     uint32_t useConfTemporal, useConfSpatial;
     uint32_t gatherOption, scatterBackupMIS, numTimePartitions;
@@ -148,6 +149,11 @@ __device__ __forceinline__ float dev_mis(const DevCtx& C, float p0, float p1) //
     if (C.misHeuristic == 1u)
     {
         float q0 = (1.f * p0) * (1.f * p0), q1 = (1.f * p1) * (1.f * p1);
+        return q0 / (q0 + q1);
+    }
+    if (C.misHeuristic == 2u)
+    {
+        float q0 = f_pow_pos(1.f * p0, C.misPowerExponent), q1 = f_pow_pos(1.f * p1, C.misPowerExponent);
         return q0 / (q0 + q1);
     }
     float q0 = 1.f * p0, q1 = 1.f * p1;

@@ -60,7 +60,9 @@ def test_properties_parse_like_the_render_graph_script(rs):
 
 
 @pytest.mark.parametrize("bad", [{"samplesPerPixel": 0}, {"samplesPerPixel": 17}, {"numTimePartitions": 9},
-                                 {"maxDiffuseBounces": 300}, {"specularRoughnessThreshold": 2.0}])
+                                 {"maxDiffuseBounces": 300}, {"specularRoughnessThreshold": 2.0},
+                                 {"misHeuristic": "PowerExp", "misPowerExponent": 0.0},
+                                 {"misHeuristic": "PowerExp", "misPowerExponent": 11.0}])
 def test_invalid_options_are_rejected_before_any_device_work(rs, bad):
     lib = rs.load_library()
     o = rs.abi.options_from_properties(bad, 64, 64)

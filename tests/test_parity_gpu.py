@@ -226,3 +226,14 @@ def test_zoom_out_crowded_cells(rs, oracle_mod, scenes, mode):
         assert P.bit_mismatch_fraction(a, b) == 0.0, f"frame {f}"
     assert most >= 256, most
     gpu.close()
+
+
+@pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
+@pytest.mark.parametrize("mode", ["ScatterBackup", "GatherOnly"])
+def test_power_exp_mis(rs, oracle_mod, scenes, mode):
+    """misHeuristic PowerExp (PathTracer.slang:498-503) with a non-integer exponent: the NEE / BSDF
+    MIS weights of the candidates and of every shift that re-evaluates them, GPU against the oracle."""
+    props = {"temporalReuse": mode, "gatherOption": "Clamped", "maxSurfaceBounces": 2, "misHeuristic": "PowerExp",
+             "misPowerExponent": 1.5, "enableSpatialResampling": True}
+    report, img = run_pair(rs, oracle_mod, scenes.cornell_box(0), scenes.cornell_camera, props, frames=4, width=48, height=40)
+    assert all(report[f"bits{f}"] == 0.0 for f in range(4)), report
