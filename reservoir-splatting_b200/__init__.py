@@ -19,7 +19,8 @@ from . import abi
 from .abi import BUF, BUFFER_LAYOUT
 
 PACKAGE_DIR = Path(__file__).resolve().parent
-LIB_PATH = PACKAGE_DIR / "lib" / "librs_b200.so"
+# RS_B200_LIB selects another build of the library (a variant built elsewhere for comparison)
+LIB_PATH = Path(os.environ["RS_B200_LIB"]) if os.environ.get("RS_B200_LIB") else PACKAGE_DIR / "lib" / "librs_b200.so"
 
 _lib = None
 

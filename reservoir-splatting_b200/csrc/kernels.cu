@@ -178,8 +178,10 @@ __device__ __forceinline__ void next_hit(const DevCtx& C, PState& p) // PathTrac
 // kDirect (one sample per pixel): a selected candidate's record is written straight to the
 // output planes (outRec, pixel pix) instead of being carried in the path state; the output is the
 // same, and ~28 registers of long-lived state are freed.
+// A call, not inlined: the path tracer's loop then keeps fewer values live across the shading code
+// (k_candidates_direct 4.50 -> 4.40 ms at 1080p, measured twice on separate boxes).
 template <bool kDirect, bool kEnv>
-__device__ void handle_hit(const DevCtx& C, PState& path, const RecPlanes& outRec, uint32_t pix)
+__device__ __noinline__ void handle_hit(const DevCtx& C, PState& path, const RecPlanes& outRec, uint32_t pix)
 {
     const bool isPrimaryHit = path.vertex == 1;
     ShadingData sd = dev_sd(C, path.hit, path.dir);
