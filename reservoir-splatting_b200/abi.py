@@ -138,12 +138,39 @@ _ENUMS = {"temporalReuse": TEMPORAL_REUSE, "gatherOption": GATHER_MECHANISM, "sc
 _ALIASES = {"hybridMISOption": "scatterBackupMISOption"}
 
 
+# Properties of ReservoirSplatting.cpp:99-131 that change nothing this build renders: alpha testing
+# (the scenes carry no alpha textures), shading-normal adjustment (shading uses face normals), nested
+# dielectrics and lights inside them (materials are opaque), texture LOD (no textures) and the
+# internal colour format (declared by the reference, read by none of its shaders).  They are
+# accepted so that a render-graph script runs unchanged.
+_NO_EFFECT = {"useAlphaTest", "adjustShadingNormals", "maxNestedMaterials", "useLightsInDielectricVolumes", "primaryLodMode",
+              "lodBias", "colorFormat", "lightBVHOptions"}
+# RenderPassHelpers::IOSize of the outputSize property: the frame size relative to the default
+# (the createPass width and height), or fixedOutputSize.
+_IO_SIZE = {"Default": 1.0, "Full": 1.0, "Half": 0.5, "Quarter": 0.25, "Double": 2.0}
+
+
 def options_from_properties(props: dict | None, width: int, height: int) -> RsOptions:
     """parseProperties (ReservoirSplatting.cpp:192-261) for a createPass() property dict."""
     o = default_options(width, height)
     props = dict(props or {})
     names = {f for f, _ in RsOptions._fields_}
+    size = props.get("outputSize")
+    if isinstance(size, str):
+        if size == "Fixed":
+            fixed = props.get("fixedOutputSize", (512, 512))
+            o.frameWidth, o.frameHeight = int(fixed[0]), int(fixed[1])
+        elif size in _IO_SIZE:
+            o.frameWidth, o.frameHeight = max(1, int(width * _IO_SIZE[size])), max(1, int(height * _IO_SIZE[size]))
+        else:
+            raise ValueError(f"unknown value {size!r} for property 'outputSize'")
     for key, value in props.items():
+        if key in _NO_EFFECT or key == "fixedOutputSize" or (key == "outputSize" and isinstance(value, str)):
+            continue
+        if key == "emissiveSampler":
+            if value not in ("Power", 2):
+                raise ValueError("emissiveSampler: only the power sampler (EmissivePowerSampler, the reference default) is built")
+            continue
         field = _ALIASES.get(key, key)
         if key in _ENUMS and isinstance(value, str):
             if value not in _ENUMS[key]:

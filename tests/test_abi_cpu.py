@@ -59,6 +59,30 @@ def test_properties_parse_like_the_render_graph_script(rs):
         rs.abi.options_from_properties({"temporalReuse": "Sideways"}, 64, 64)
 
 
+def test_every_reference_property_key_is_accepted(rs):
+    # every scripting key of ReservoirSplatting.cpp:99-131, with the reference's default values
+    props = {"samplesPerPixel": 1, "maxSurfaceBounces": 3, "maxDiffuseBounces": 3, "maxSpecularBounces": 3,
+             "maxTransmissionBounces": 10, "sampleGenerator": "TinyUniform", "fixedSeed": 1, "useRussianRoulette": False,
+             "misHeuristic": "Balance", "misPowerExponent": 2.0, "emissiveSampler": "Power", "lightBVHOptions": {},
+             "useAlphaTest": True, "adjustShadingNormals": False, "maxNestedMaterials": 2,
+             "useLightsInDielectricVolumes": False, "disableCaustics": False, "specularRoughnessThreshold": 0.25,
+             "primaryLodMode": "Mip0", "lodBias": 0.0, "outputSize": "Default", "fixedOutputSize": (512, 512),
+             "colorFormat": "LogLuvHDR", "enableTemporalResampling": True, "enableSpatialResampling": True,
+             "temporalReuse": "ScatterBackup", "scatterBackupMISOption": "Pairwise", "gatherOption": "Clamped",
+             "numTimePartitions": 2}
+    o = rs.abi.options_from_properties(props, 320, 240)
+    assert (o.frameWidth, o.frameHeight) == (320, 240) and o.temporalReuse == 2 and o.gatherOption == 1
+    assert o.scatterBackupMISOption == 1 and o.maxTransmissionBounces == 10 and o.useFixedSeed == 1
+    o = rs.abi.options_from_properties({"outputSize": "Half"}, 320, 240)
+    assert (o.frameWidth, o.frameHeight) == (160, 120)
+    o = rs.abi.options_from_properties({"outputSize": "Fixed", "fixedOutputSize": (96, 64)}, 320, 240)
+    assert (o.frameWidth, o.frameHeight) == (96, 64)
+    with pytest.raises(ValueError):
+        rs.abi.options_from_properties({"emissiveSampler": "LightBVH"}, 64, 64)
+    with pytest.raises(ValueError):
+        rs.abi.options_from_properties({"outputSize": "Triple"}, 64, 64)
+
+
 @pytest.mark.parametrize("bad", [{"samplesPerPixel": 0}, {"samplesPerPixel": 17}, {"numTimePartitions": 9},
                                  {"maxDiffuseBounces": 300}, {"specularRoughnessThreshold": 2.0},
                                  {"misHeuristic": "PowerExp", "misPowerExponent": 0.0},
