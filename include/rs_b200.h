@@ -203,6 +203,16 @@ typedef struct rs_env_map {
 } rs_env_map;
 RS_API rs_status rs_set_env_map(rs_pass* pass, const rs_env_map* env);
 RS_API rs_status rs_execute(rs_pass* pass, const rs_frame_desc* frame, void* cudaStream);
+/* Latency of host colour outputs (no reference counterpart: the reference presents on the GPU).
+ * 0 (default): rs_execute with frame.colorHost returns once the image is in host memory.
+ * 1: rs_execute renders into one of two pass-owned device images, queues the copy to
+ * frame.colorHost on the pass's own copy stream behind the frame, and returns once the PREVIOUS
+ * frame's copy is complete, so each copy overlaps the next frame's kernels; frame.colorHost must
+ * stay valid until the next rs_execute or rs_wait_host_output returns, which also reports that
+ * frame's device status (RS_DEVICE_FAULT).  frame.color, when also given, receives a device copy.
+ * rs_wait_host_output completes the copy in flight and orders the last stream after it. */
+RS_API rs_status rs_set_host_output_latency(rs_pass* pass, uint32_t frames);
+RS_API rs_status rs_wait_host_output(rs_pass* pass);
 RS_API rs_status rs_reset(rs_pass* pass);
 RS_API rs_status rs_set_seed(rs_pass* pass, uint32_t useFixedSeed, uint32_t fixedSeed);
 RS_API rs_status rs_freeze(rs_pass* pass, uint32_t frozen);

@@ -48,6 +48,8 @@ def load_library():
     lib.rs_set_env_map.argtypes = [C.c_void_p, C.POINTER(abi.RsEnvMap)]
     lib.rs_execute.argtypes = [C.c_void_p, C.POINTER(abi.RsFrameDesc), C.c_void_p]
     lib.rs_reset.argtypes = [C.c_void_p]
+    lib.rs_set_host_output_latency.argtypes = [C.c_void_p, C.c_uint32]
+    lib.rs_wait_host_output.argtypes = [C.c_void_p]
     lib.rs_set_seed.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32]
     lib.rs_freeze.argtypes = [C.c_void_p, C.c_uint32]
     lib.rs_get_buffer.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_size_t)]
@@ -187,6 +189,15 @@ class ReservoirSplatting:
             f.colorHost = None
         f.sceneShouldReset = 1 if should_reset else 0
         _check(self._lib.rs_execute(self._h, C.byref(f), C.c_void_p(stream)))
+
+    def set_host_output_latency(self, frames: int):
+        """0: execute(color_host=...) returns with the image on the host; 1: the copy overlaps the
+        next frame and completes when the next execute or wait_host_output returns."""
+        _check(self._lib.rs_set_host_output_latency(self._h, int(frames)))
+
+    def wait_host_output(self):
+        """Completes the host copy in flight (latency 1) and raises on that frame's device fault."""
+        _check(self._lib.rs_wait_host_output(self._h))
 
     def render(self, camera, **kw) -> np.ndarray:
         out = np.empty((self.height, self.width, 4), np.float32)

@@ -150,7 +150,17 @@ struct rs_pass
     DevBuf<uint4> msShift;
     DevBuf<float4> msTerms, msMisSub;
     DevBuf<uint32_t> fault;
-    uint32_t* hostFault = nullptr;
+    uint32_t* hostFault = nullptr; // two words: frames alternate between them when host output is pipelined
+    uint32_t faultSlot = 0;        // the word this frame's status is copied to
+    // pipelined host output (rs_set_host_output_latency 1): frame k's colour is copied to the host on
+    // copyStream from one of two device images while frame k + 1 renders on the caller's stream
+    uint32_t hostLatency = 0;
+    DevBuf<float4> pipeColor[2];
+    int pipeIdx = 0;
+    cudaStream_t copyStream = nullptr;
+    cudaEvent_t frameDoneEv = nullptr, copyDoneEv = nullptr;
+    bool copyPending = false;       // a host copy is in flight (copyDoneEv marks it)
+    uint32_t pendingFaultSlot = 0;  // the status word of the frame whose copy is in flight
     DevBuf<CameraTable> camTable;
     // side streams for independent kernels of a frame (fork/join through events on the frame's
     // stream, so the frame stays one ordered unit for the caller and for graph capture)
@@ -193,6 +203,9 @@ struct rs_pass
         for (auto e : joinEv) if (e) cudaEventDestroy(e);
         for (auto q : side) if (q) cudaStreamDestroy(q);
         if (forkEv) cudaEventDestroy(forkEv);
+        if (copyStream) cudaStreamDestroy(copyStream);
+        if (frameDoneEv) cudaEventDestroy(frameDoneEv);
+        if (copyDoneEv) cudaEventDestroy(copyDoneEv);
         if (hostFault) cudaFreeHost(hostFault);
         if (hostCtx) cudaFreeHost(hostCtx);
         if (ringCtx) cudaFreeHost(ringCtx);
@@ -313,7 +326,11 @@ static rs_status allocate(rs_pass* p)
             RS_CUDA(cudaEventCreateWithFlags(&p->joinEv[i], cudaEventDisableTiming));
         }
     }
-    if (!p->hostFault) RS_CUDA(cudaMallocHost(&p->hostFault, sizeof(uint32_t)));
+    if (!p->hostFault)
+    {
+        RS_CUDA(cudaMallocHost(&p->hostFault, 2 * sizeof(uint32_t)));
+        p->hostFault[0] = p->hostFault[1] = 0u;
+    }
     if (!p->hostCtx) RS_CUDA(cudaMallocHost(&p->hostCtx, sizeof(DevCtx)));
     if (!p->ringCtx)
     {
@@ -890,8 +907,58 @@ static rs_status enqueue_frame(rs_pass* p, cudaStream_t s, float4* colorDev, con
     }
     stage(p, "end", s);
     RS_CUDA(cudaGetLastError());
-    RS_CUDA(cudaMemcpyAsync(p->hostFault, p->fault.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    RS_CUDA(cudaMemcpyAsync(p->hostFault + p->faultSlot, p->fault.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     return RS_OK;
+}
+
+// Waits for the host copy in flight (pipelined host output), orders `s` after it, and reports the
+// device status word of the frame it belongs to.
+static rs_status wait_host_copy(rs_pass* p, cudaStream_t s)
+{
+    if (!p->copyPending) return RS_OK;
+    p->copyPending = false;
+    RS_CUDA(cudaEventSynchronize(p->copyDoneEv));
+    RS_CUDA(cudaStreamWaitEvent(s, p->copyDoneEv, 0));
+    if (p->hostFault[p->pendingFaultSlot]) return fail(RS_DEVICE_FAULT, "device status word set: BVH traversal stack overflow");
+    return RS_OK;
+}
+
+// rs_execute with a host colour output and one frame of latency: the frame renders into one of two
+// device images, an event on `s` lets copyStream copy that image to f->colorHost, and the call
+// returns once the previous frame's copy has finished (so that copy overlapped this frame's
+// kernels), reporting that frame's device status.  f->color, when given too, gets a device copy.
+static rs_status execute_pipelined(rs_pass* p, const rs_frame_desc* f, cudaStream_t s, size_t N)
+{
+    if (!p->copyStream)
+    {
+        RS_CUDA(cudaStreamCreateWithFlags(&p->copyStream, cudaStreamNonBlocking));
+        RS_CUDA(cudaEventCreateWithFlags(&p->frameDoneEv, cudaEventDisableTiming));
+        RS_CUDA(cudaEventCreateWithFlags(&p->copyDoneEv, cudaEventDisableTiming));
+    }
+    if (p->pipeColor[0].n < N || p->pipeColor[1].n < N)
+    {
+        rs_status w = wait_host_copy(p, s); // the images are about to be reallocated
+        if (w != RS_OK) return w;
+        RS_CUDA(p->pipeColor[0].ensure(N));
+        RS_CUDA(p->pipeColor[1].ensure(N));
+    }
+    // the image written two frames ago was copied before the previous call returned
+    p->pipeIdx ^= 1;
+    float4* colorDev = p->pipeColor[p->pipeIdx].p;
+    p->faultSlot ^= 1u;
+    begin_frame(p, f);
+    rs_status st = enqueue_frame(p, s, colorDev, reinterpret_cast<const float2*>(f->mvec), reinterpret_cast<const uint4*>(f->vbuffer), false);
+    if (st != RS_OK) return st;
+    if (f->color) RS_CUDA(cudaMemcpyAsync(f->color, colorDev, N * 16ull, cudaMemcpyDeviceToDevice, s));
+    RS_CUDA(cudaEventRecord(p->frameDoneEv, s));
+    RS_CUDA(cudaStreamWaitEvent(p->copyStream, p->frameDoneEv, 0));
+    RS_CUDA(cudaMemcpyAsync(f->colorHost, colorDev, N * 16ull, cudaMemcpyDeviceToHost, p->copyStream));
+    end_frame(p);
+    rs_status w = wait_host_copy(p, s); // the previous frame's copy
+    RS_CUDA(cudaEventRecord(p->copyDoneEv, p->copyStream));
+    p->copyPending = true;
+    p->pendingFaultSlot = p->faultSlot;
+    return w;
 }
 
 extern "C" RS_API rs_status rs_execute(rs_pass* p, const rs_frame_desc* f, void* streamPtr)
@@ -907,12 +974,15 @@ extern "C" RS_API rs_status rs_execute(rs_pass* p, const rs_frame_desc* f, void*
     p->stageRays.clear();
 #endif
     const size_t N = (size_t)p->W * p->H;
+    if (f->colorHost && p->hostLatency == 1) return execute_pipelined(p, f, s, N);
+    p->faultSlot = 0;
     float4* colorDev = reinterpret_cast<float4*>(f->color);
     if (!colorDev)
     {
         RS_CUDA(p->scratchColor.ensure(N)); // allocated on the first host-output frame only
         colorDev = p->scratchColor.p;
     }
+    if (p->copyPending) { rs_status w = wait_host_copy(p, s); if (w != RS_OK) return w; }
     begin_frame(p, f);
     rs_status st = enqueue_frame(p, s, colorDev, reinterpret_cast<const float2*>(f->mvec), reinterpret_cast<const uint4*>(f->vbuffer), false);
     if (st != RS_OK) return st;
@@ -924,6 +994,23 @@ extern "C" RS_API rs_status rs_execute(rs_pass* p, const rs_frame_desc* f, void*
     end_frame(p);
     if (f->colorHost && *p->hostFault) return fail(RS_DEVICE_FAULT, "device status word set: BVH traversal stack overflow");
     return RS_OK;
+}
+
+// Host colour outputs with 0 (default: rs_execute returns with the image on the host) or 1 frame of
+// latency (the copy overlaps the next frame; rs_wait_host_output completes the last one).
+extern "C" RS_API rs_status rs_set_host_output_latency(rs_pass* p, uint32_t frames)
+{
+    if (!p) return fail(RS_INVALID_ARG, "pass is NULL");
+    if (frames > 1) return fail(RS_INVALID_ARG, "host output latency must be 0 or 1 frames");
+    if (frames == 0 && p->copyPending) { rs_status w = wait_host_copy(p, p->lastStream); if (w != RS_OK) return w; }
+    p->hostLatency = frames;
+    return RS_OK;
+}
+
+extern "C" RS_API rs_status rs_wait_host_output(rs_pass* p)
+{
+    if (!p) return fail(RS_INVALID_ARG, "pass is NULL");
+    return wait_host_copy(p, p->lastStream);
 }
 
 // reset() (ReservoirSplatting.cpp:813-820): frame count and seed restart unless the scene is frozen.
