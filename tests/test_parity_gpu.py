@@ -50,10 +50,11 @@ ODD_MODES = MODES + [("MultiScatter", {"temporalReuse": "MultiScatter", "numTime
 
 @pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
 @pytest.mark.parametrize("name,props", ODD_MODES, ids=[m[0] for m in ODD_MODES])
-@pytest.mark.parametrize("size", [(37, 23), (1, 1)], ids=["37x23", "1x1"])
+@pytest.mark.parametrize("size", [(37, 23), (1, 1), (4096, 3), (3, 4096)], ids=["37x23", "1x1", "4096x3", "3x4096"])
 def test_odd_image_sizes(rs, oracle_mod, scenes, name, props, size):
-    """Images that are not a multiple of the 8 x 4 warp tile (and a single pixel): the tile-edge
-    guards of every pixel kernel and the bounds of the per-splat kernels, in every temporal mode."""
+    """Images that are not a multiple of the 8 x 4 warp tile, a single pixel, and the largest width
+    and height the pass accepts (4096): the tile-edge guards of every pixel kernel, the bounds of
+    the per-splat kernels and the cell indices at the extremes, in every temporal mode."""
     w, h = size
     props = dict(props, maxSurfaceBounces=2, enableSpatialResampling=True)
     shutter = 0.04 if name == "MultiScatter" else 0.0
