@@ -10,6 +10,7 @@
  *   rs_set_options              setProperties / parseProperties        ReservoirSplatting.cpp:177-261
  *   rs_set_scene                setScene (scene + light collection)    ReservoirSplatting.cpp:378-397
  *   rs_set_env_map              Scene envMap + EnvMapSampler setup     Scene/Lights/EnvMap.cpp:60-137, Rendering/Lights/EnvMapSampler.cpp:45-113
+ *   rs_set_analytic_lights      Scene analytic lights (getLight)       Scene/Lights/Light.cpp:174-397, Rendering/Lights/LightHelpers.slang:67-284
  *   rs_execute                  execute (one frame)                    ReservoirSplatting.cpp:399-509
  *   rs_reset                    reset()                                ReservoirSplatting.cpp:813-820
  *   rs_set_seed                 Python useFixedSeed / fixedSeed        ReservoirSplatting.cpp:142-156
@@ -202,6 +203,41 @@ typedef struct rs_env_map {
     float rotation[3];                   /* degrees */
 } rs_env_map;
 RS_API rs_status rs_set_env_map(rs_pass* pass, const rs_env_map* env);
+
+/* Analytic lights (Scene::getLight / useAnalyticLights; Scene/Lights/Light.cpp, LightData.slang),
+ * sampled by next-event estimation only (PathTracer.slang:567-599): uniform pick of a light, then
+ * LightHelpers.slang's sample of its type.  The light-type selection gives the environment map,
+ * the emissive triangles and the analytic lights equal probability when present.  As in the
+ * reference, a light sampled at the primary hit leaves the reconnection record without a light
+ * vertex (PathTracer.slang:1079-1104), and a point or directional light's stored radiance is
+ * Li * pdf = 0, so shifts of such samples contribute nothing; the sample still counts at its own
+ * pixel.  The reference's arithmetic for those records is kept as it is, and with it the few NaN
+ * values it makes in shifts (a delta light sampled at the second vertex stores lightPdf = 0, so the
+ * length-3 reconnection multiplies 0 by totalBsdf / 0, ShiftMapping.slang:479-493; a light vertex
+ * left unset loads as a zero vertex, LoadShadingData.slang:69-74, whose Jacobian is 0 / 0): some
+ * pixels of scenes with analytic lights and temporal or spatial reuse come out NaN, as they would
+ * in the reference.  Synchronous; replaces the previous list (count 0 removes them).  rs_backward
+ * rejects scenes with analytic lights. */
+typedef enum rs_light_type {
+    RS_LIGHT_POINT = 0,                  /* point, or spot when openingAngle < pi */
+    RS_LIGHT_DIRECTIONAL = 1,
+    RS_LIGHT_DISTANT = 2,                /* a cone of directions of half-angle `angle` */
+    RS_LIGHT_RECT = 3,                   /* the quad [-1, 1]^2 x {0} of object space, one-sided (+z) */
+    RS_LIGHT_DISC = 4,                   /* the unit disc of the z = 0 plane, one-sided (+z) */
+    RS_LIGHT_SPHERE = 5                  /* the unit sphere */
+} rs_light_type;
+typedef struct rs_analytic_light {
+    uint32_t type;                       /* rs_light_type */
+    float intensity[3];                  /* point: intensity; the others: radiance */
+    float position[3];                   /* point */
+    float direction[3];                  /* point (spot axis), directional, distant: the direction light travels */
+    float openingAngle;                  /* point: spot half-angle in radians, clamped to [0, pi] (pi: all directions) */
+    float penumbraAngle;                 /* point: smooth edge inside the cone, clamped to [0, openingAngle] */
+    float angle;                         /* distant: half-angle subtended, clamped to [0, pi/2] */
+    float transform[16];                 /* rect, disc, sphere: row-major 4x4 object-to-world matrix */
+    float scaling[3];                    /* rect, disc, sphere: object-space scale applied first */
+} rs_analytic_light;
+RS_API rs_status rs_set_analytic_lights(rs_pass* pass, const rs_analytic_light* lights, uint32_t count);
 RS_API rs_status rs_execute(rs_pass* pass, const rs_frame_desc* frame, void* cudaStream);
 /* Latency of host colour outputs (no reference counterpart: the reference presents on the GPU).
  * 0 (default): rs_execute with frame.colorHost returns once the image is in host memory.

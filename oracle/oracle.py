@@ -63,6 +63,7 @@ def load():
     lib.ro_set_threads.restype = C.c_int
     lib.ro_set_scene.argtypes = [C.c_void_p, C.POINTER(a.RsSceneDesc)]
     lib.ro_set_env_map.argtypes = [C.c_void_p, C.POINTER(a.RsEnvMap)]
+    lib.ro_set_analytic_lights.argtypes = [C.c_void_p, C.POINTER(a.RsAnalyticLight), C.c_uint32]
     lib.ro_get_env_importance.argtypes = [C.c_void_p, C.c_void_p]
     lib.ro_env_debug.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]
     lib.ro_execute.argtypes = [C.c_void_p, C.POINTER(a.RsFrameDesc), C.c_void_p, C.c_void_p]
@@ -118,6 +119,12 @@ class OraclePass:
         del keep
         if st != 0:
             raise RuntimeError(f"oracle set_env_map failed: {st}")
+
+    def set_analytic_lights(self, lights):
+        lights = list(lights or [])
+        st = self._lib.ro_set_analytic_lights(self._h, self._abi.analytic_lights_array(lights), len(lights))
+        if st != 0:
+            raise RuntimeError(f"oracle set_analytic_lights failed: {st}")
 
     def env_importance(self) -> np.ndarray:
         """The importance mips (512^2 .. 1 texels back to back)."""

@@ -34,6 +34,7 @@
 #include "../include/rs_b200.h"
 #include "../reservoir-splatting_b200/csrc/core/camera.h"
 #include "../reservoir-splatting_b200/csrc/core/envmap.h"
+#include "../reservoir-splatting_b200/csrc/core/analytic_lights.h"
 #include "../reservoir-splatting_b200/csrc/core/scene_prep.h"
 #include "../reservoir-splatting_b200/csrc/core/material_grad.h"
 #include <cmath>
@@ -362,6 +363,7 @@ struct Pass
     // environment map (PathTracer.slang kUseEnvLight = env.present): texels and importance mips
     EnvMapView env = {};
     std::vector<float> envTexels, envImportance;
+    std::vector<AnalyticLight> analytic; // the scene's analytic lights (ro_set_analytic_lights)
 
     uint32_t W = 0, H = 0;
     uint32_t frameCount = 0, seed = 0;
@@ -528,27 +530,30 @@ struct Pass
     struct LightSample
     {
         f3 Li; float pdf; f3 origin; float distance; f3 dir; uint32_t triangleId; f2 barycentrics; float geometryTerm;
-        uint32_t lightType; // 0 env map, 1 emissive (LightType)
+        uint32_t lightType; // 0 env map, 1 emissive, 2 analytic (LightType)
     };
 
-    // getLightTypeSelectionProbabilities (:606-622): p = {env, emissive, 0} normalised
-    void lightTypeProbabilities(float& pEnv, float& pEmissive) const { light_type_probabilities(env.present != 0, lv.count > 0, pEnv, pEmissive); }
+    // getLightTypeSelectionProbabilities (:606-622): p = {env, emissive, analytic} normalised
+    void lightTypeProbabilities(float& pEnv, float& pEmissive, float& pAnalytic) const
+    {
+        light_type_probabilities(env.present != 0, lv.count > 0, !analytic.empty(), pEnv, pEmissive, pAnalytic);
+    }
 
     // generateLightSample (:668-701); the type-selection draw is always taken.
     bool generateLightSample(f3 vpos, f3 vfaceN, bool vfront, bool sampleUpper, bool sampleLower, SampleGen& sg, LightSample& ls) const
     {
         ls = LightSample();
-        float p[2];
-        lightTypeProbabilities(p[0], p[1]);
+        float p[3];
+        lightTypeProbabilities(p[0], p[1], p[2]);
         float u = sampleNext1D(sg);
         // selectLightType (:634-656)
-        uint32_t lightType = 2;
-        for (uint32_t t = 0; t < 2; t++)
+        uint32_t lightType = 3;
+        for (uint32_t t = 0; t < 3; t++)
         {
             if (u < p[t]) { lightType = t; break; }
             u -= p[t];
         }
-        if (lightType == 2) return false;
+        if (lightType == 3) return false;
         float selectionPdf = p[lightType];
         ls.lightType = lightType;
         if (lightType == 0)
@@ -560,6 +565,20 @@ struct Pass
             ls.Li = ls.pdf > 0.f ? Le / ls.pdf : mk3(0.f);
             ls.origin = computeRayOrigin(vpos, dot(vfaceN, ls.dir) >= 0.f ? vfaceN : -vfaceN);
             ls.distance = kRayTMax;
+        }
+        else if (lightType == 2)
+        {
+            // generateAnalyticLightSample (:573-599)
+            AnalyticLightView av;
+            av.lights = analytic.data();
+            av.count = (uint32_t)analytic.size();
+            AnalyticSample as;
+            if (!analytic_light_sample(av, vpos, sg, as)) return false;
+            ls.Li = as.Li;
+            ls.pdf = as.pdf;
+            ls.dir = as.dir;
+            ls.distance = as.distance;
+            ls.origin = computeRayOrigin(vpos, dot(vfaceN, ls.dir) >= 0.f ? vfaceN : -vfaceN);
         }
         else
         {
@@ -633,8 +652,8 @@ struct Pass
             if (lv.count > 0 && !isPrimaryHit && path.isLightSampled() && isLightSamplable)
             {
                 // upperHemisphere is ignored by the power sampler
-                float pEnv, pEmissive;
-                lightTypeProbabilities(pEnv, pEmissive);
+                float pEnv, pEmissive, pAnalytic;
+                lightTypeProbabilities(pEnv, pEmissive, pAnalytic);
                 lightPdf = pEmissive * eval_emissive_pdf(lv, path.origin, sd.lightIndex, sd.posW, sd_oriented_face_normal(sd));
                 misWeight = mis(path.totalPdf, lightPdf);
             }
@@ -670,8 +689,9 @@ struct Pass
             if (validSample)
             {
                 f3 Le = ls.Li * ls.pdf;
-                float scatterPdf = mi_pdf(sd, d, 0u, ls.dir);
-                float misWeight = mis(ls.pdf, scatterPdf);
+                // analytic lights: no scatter pdf, MIS weight 1 (:1025-1031)
+                float scatterPdf = ls.lightType == 2 ? 0.f : mi_pdf(sd, d, 0u, ls.dir);
+                float misWeight = ls.lightType == 2 ? 1.f : mis(ls.pdf, scatterPdf);
                 f3 weight = mi_eval(sd, d, 0u, ls.dir);
                 f3 Lr = weight * misWeight * ls.Li;
                 if (any_gt0(Lr))
@@ -697,7 +717,7 @@ struct Pass
                                     s.secondaryPathJacobian = ls.pdf;
                                     s.lightPdf = ls.pdf; // a distant light: no area measure
                                 }
-                                else
+                                else if (ls.lightType == 1) // an analytic light leaves the light vertex unset
                                 {
                                     s.secondHit = hit_tri(lv.tris[ls.triangleId].sceneTri, ls.barycentrics.x, ls.barycentrics.y);
                                     s.secondaryPathJacobian = ls.pdf * ls.geometryTerm;
@@ -751,8 +771,8 @@ struct Pass
             float lightPdf = 0.f;
             if (path.isLightSampled() && isLightSamplable)
             {
-                float pEnv, pEmissive;
-                lightTypeProbabilities(pEnv, pEmissive);
+                float pEnv, pEmissive, pAnalytic;
+                lightTypeProbabilities(pEnv, pEmissive, pAnalytic);
                 lightPdf = pEnv * env_eval_pdf(env, path.dir);
                 misWeight = mis(path.totalPdf, lightPdf);
             }
@@ -815,7 +835,7 @@ struct Pass
         float rayLength = kRayTMax;
         if (!secondHitIsDistant)
         {
-            ShadingData secondSd = loadSD(rd.secondHit, mk3(0.f));
+            ShadingData secondSd = hit_valid(rd.secondHit) ? loadSD(rd.secondHit, mk3(0.f)) : sd_zero_vertex(); // LoadShadingData.slang:69-74
             f3 shiftedOffset = secondSd.posW - sd.posW;
             float shiftedDist2 = dot(shiftedOffset, shiftedOffset);
             float shiftedCosine = f_abs(dot(secondSd.faceN, -normalize(shiftedOffset)));
@@ -2373,6 +2393,21 @@ __attribute__((visibility("default"))) ro_pass* ro_create(const rs_options* opt)
 __attribute__((visibility("default"))) void ro_destroy(ro_pass* r) { delete r; }
 __attribute__((visibility("default"))) int ro_set_threads(int n) { if (n > 0) omp_set_num_threads(n); return omp_get_max_threads(); }
 
+// The scene's analytic lights, prepared as the pass prepares them (prepare_analytic_light).
+__attribute__((visibility("default"))) int ro_set_analytic_lights(ro_pass* r, const rs_analytic_light* lights, uint32_t count)
+{
+    if (count > 0 && !lights) return RS_INVALID_ARG;
+    std::vector<AnalyticLight> out(count);
+    for (uint32_t i = 0; i < count; i++)
+    {
+        AnalyticLightDesc d;
+        memcpy(&d, &lights[i], sizeof(d));
+        if (!prepare_analytic_light(d, out[i])) return RS_INVALID_ARG;
+    }
+    r->p.analytic.swap(out);
+    return RS_OK;
+}
+
 // Scene envMap + EnvMapSampler::createImportanceMap (EnvMap.cpp:60-137, EnvMapSampler.cpp:80-113):
 // the texels, the transform, and the importance mips built on the host with the device's
 // per-texel and reduction functions.
@@ -2661,6 +2696,34 @@ __attribute__((visibility("default"))) void ro_test_fmath(int kind, const float*
     }
 }
 // f_pow_pos(x[i], e[i]) (the PowerExp MIS heuristic's power).
+// One analytic light prepared from its description and sampled at a shading point with the given
+// two uniform numbers: out = {ok, posW.xyz, normalW.xyz, dir.xyz, distance, Li.xyz, pdf} and the
+// prepared record (out[15..]: cosOpeningAngle, penumbraAngle, cosSubtendedAngle, surfaceArea,
+// transMat[12], transMatIT[9]).  Returns 0 when the description is rejected.
+__attribute__((visibility("default"))) int ro_test_analytic(const rs_analytic_light* desc, const float* pos3, const float* u2, float* out)
+{
+    AnalyticLightDesc d;
+    memcpy(&d, desc, sizeof(d));
+    AnalyticLight L;
+    if (!prepare_analytic_light(d, L)) return 0;
+    AnalyticSample ls;
+    ls.posW = mk3(0.f); ls.normalW = mk3(0.f); ls.dir = mk3(0.f); ls.Li = mk3(0.f); ls.distance = 0.f; ls.pdf = 0.f;
+    const f3 x = mk3(pos3[0], pos3[1], pos3[2]);
+    const f2 u = mk2(u2[0], u2[1]);
+    bool ok;
+    if (L.type == kLightPoint) ok = al_sample_point(x, L, ls);
+    else if (L.type == kLightDirectional) ok = al_sample_directional(L, ls);
+    else if (L.type == kLightDistant) ok = al_sample_distant(L, u, ls);
+    else ok = al_sample_area(x, L, u, ls);
+    const float v[15] = {ok ? 1.f : 0.f, ls.posW.x, ls.posW.y, ls.posW.z, ls.normalW.x, ls.normalW.y, ls.normalW.z,
+                         ls.dir.x, ls.dir.y, ls.dir.z, ls.distance, ls.Li.x, ls.Li.y, ls.Li.z, ls.pdf};
+    for (int k = 0; k < 15; k++) out[k] = v[k];
+    out[15] = L.cosOpeningAngle; out[16] = L.penumbraAngle; out[17] = L.cosSubtendedAngle; out[18] = L.surfaceArea;
+    for (int k = 0; k < 12; k++) out[19 + k] = L.transMat[k];
+    for (int k = 0; k < 9; k++) out[31 + k] = L.transMatIT[k];
+    return 1;
+}
+
 __attribute__((visibility("default"))) void ro_test_pow(const float* x, const float* e, float* y, uint32_t n)
 {
     for (uint32_t i = 0; i < n; i++) y[i] = f_pow_pos(x[i], e[i]);

@@ -46,6 +46,7 @@ def load_library():
     lib.rs_set_options.argtypes = [C.c_void_p, C.POINTER(abi.RsOptions)]
     lib.rs_set_scene.argtypes = [C.c_void_p, C.POINTER(abi.RsSceneDesc)]
     lib.rs_set_env_map.argtypes = [C.c_void_p, C.POINTER(abi.RsEnvMap)]
+    lib.rs_set_analytic_lights.argtypes = [C.c_void_p, C.POINTER(abi.RsAnalyticLight), C.c_uint32]
     lib.rs_execute.argtypes = [C.c_void_p, C.POINTER(abi.RsFrameDesc), C.c_void_p]
     lib.rs_reset.argtypes = [C.c_void_p]
     lib.rs_set_host_output_latency.argtypes = [C.c_void_p, C.c_uint32]
@@ -148,6 +149,11 @@ class ReservoirSplatting:
         desc, keep = abi.env_map_struct(texels, intensity, tint, rotation)
         _check(self._lib.rs_set_env_map(self._h, C.byref(desc)))
         del keep
+
+    def set_analytic_lights(self, lights):
+        """The scene's analytic lights, a list of dicts (abi.analytic_lights_array); see rs_set_analytic_lights."""
+        lights = list(lights or [])
+        _check(self._lib.rs_set_analytic_lights(self._h, abi.analytic_lights_array(lights), len(lights)))
 
     def reset(self):
         _check(self._lib.rs_reset(self._h))

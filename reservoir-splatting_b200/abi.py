@@ -48,6 +48,38 @@ class RsEnvMap(C.Structure):
                 ("tint", C.c_float * 3), ("rotation", C.c_float * 3)]
 
 
+class RsAnalyticLight(C.Structure):
+    _fields_ = [("type", C.c_uint32), ("intensity", C.c_float * 3), ("position", C.c_float * 3), ("direction", C.c_float * 3),
+                ("openingAngle", C.c_float), ("penumbraAngle", C.c_float), ("angle", C.c_float), ("transform", C.c_float * 16),
+                ("scaling", C.c_float * 3)]
+
+
+LIGHT_TYPE = {"point": 0, "directional": 1, "distant": 2, "rect": 3, "disc": 4, "sphere": 5}
+
+
+def analytic_lights_array(lights) -> C.Array:
+    """rs_analytic_light[] from dicts with the keys of Falcor's light classes (Scene/Lights/Light.h):
+    "type" (point, directional, distant, rect, disc, sphere), "intensity", "position", "direction",
+    "openingAngle", "penumbraAngle", "angle", "transform" (4x4 object-to-world) and "scaling"."""
+    lights = list(lights or [])
+    arr = (RsAnalyticLight * max(1, len(lights)))()
+    for i, d in enumerate(lights):
+        L = arr[i]
+        t = d.get("type", "point")
+        if t not in LIGHT_TYPE:
+            raise ValueError(f"unknown analytic light type {t!r}")
+        L.type = LIGHT_TYPE[t]
+        L.intensity[:] = [float(v) for v in d.get("intensity", (1.0, 1.0, 1.0))]
+        L.position[:] = [float(v) for v in d.get("position", (0.0, 0.0, 0.0))]
+        L.direction[:] = [float(v) for v in d.get("direction", (0.0, -1.0, 0.0))]
+        L.openingAngle = float(d.get("openingAngle", np.pi))
+        L.penumbraAngle = float(d.get("penumbraAngle", 0.0))
+        L.angle = float(d.get("angle", 0.5 * np.pi / 180.0))
+        L.transform[:] = [float(v) for v in np.asarray(d.get("transform", np.eye(4)), np.float64).reshape(16)]
+        L.scaling[:] = [float(v) for v in d.get("scaling", (1.0, 1.0, 1.0))]
+    return arr
+
+
 def env_map_struct(texels, intensity=1.0, tint=(1.0, 1.0, 1.0), rotation=(0.0, 0.0, 0.0)) -> tuple[RsEnvMap, np.ndarray | None]:
     """Descriptor of a lat-long map given as float [H, W, 3] or [H, W, 4] (row 0 at the top), and the
     RGBA array it points into (keep it alive during the call).  None removes the map."""

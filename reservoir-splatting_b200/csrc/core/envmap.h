@@ -236,16 +236,19 @@ inline void env_transform(const float rotationDeg[3], float toWorld[9], float to
         }
 }
 
-// getLightTypeSelectionProbabilities (PathTracer.slang:606-622) without analytic lights.
-RS_HD void light_type_probabilities(bool env, bool emissive, float& pEnv, float& pEmissive)
+// getLightTypeSelectionProbabilities (PathTracer.slang:606-622): equal probabilities for the
+// light types the scene has (environment map, emissive triangles, analytic lights).
+RS_HD void light_type_probabilities(bool env, bool emissive, bool analytic, float& pEnv, float& pEmissive, float& pAnalytic)
 {
     pEnv = env ? 1.f : 0.f;
     pEmissive = emissive ? 1.f : 0.f;
-    const float sum = pEnv + pEmissive;
+    pAnalytic = analytic ? 1.f : 0.f;
+    const float sum = pEnv + pEmissive + pAnalytic;
     if (sum == 0.f) return;
     const float invSum = 1.f / sum;
     pEnv *= invSum;
     pEmissive *= invSum;
+    pAnalytic *= invSum;
 }
 
 } // namespace rs

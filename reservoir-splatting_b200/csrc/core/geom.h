@@ -134,6 +134,19 @@ RS_HD f3 perp_stark(f3 u)
     return normalize(cross(u, mk3((float)xm, (float)ym, (float)zm)));
 }
 
+// loadShadingData of a hit that is not a triangle hit (LoadShadingData.slang:69-74, 134-141): the
+// zero VertexData and material 0.  A record whose light vertex was an analytic light holds such a
+// hit; the reconnection then sees a vertex at the origin with a zero normal.
+RS_HD ShadingData sd_zero_vertex()
+{
+    ShadingData sd;
+    sd.posW = mk3(0.f); sd.V = mk3(0.f); sd.faceN = mk3(0.f);
+    sd.N = mk3(0.f); sd.T = mk3(0.f); sd.B = mk3(0.f);
+    sd.frontFacing = true; // dot(V, faceN) >= 0
+    sd.materialID = 0; sd.lightIndex = kInvalidIndex;
+    return sd;
+}
+
 RS_HD f3 sd_ray_origin(const ShadingData& sd, bool viewside = true)
 {
     return computeRayOrigin(sd.posW, (sd.frontFacing == viewside) ? sd.faceN : -sd.faceN);

@@ -227,7 +227,7 @@ __device__ __noinline__ void handle_hit(const DevCtx& C, PState& path, const Rec
         float lightPdf = 0.f;
         if (haveLights && !isPrimaryHit && isLightSampled && isLightSamplable)
         {
-            lightPdf = (kEnv ? C.pEmissiveLight : 1.f) * eval_emissive_pdf(C.lights, path.origin, sd.lightIndex, sd.posW, sd_oriented_face_normal(sd));
+            lightPdf = C.pEmissiveLight * eval_emissive_pdf(C.lights, path.origin, sd.lightIndex, sd.posW, sd_oriented_face_normal(sd));
             misWeight = dev_mis(C, path.totalPdf, lightPdf);
         }
         bool selected = cand_add_vertex(path, 1.f, path.earlyThroughput * path.thp * d.emission * misWeight);
@@ -257,15 +257,16 @@ __device__ __noinline__ void handle_hit(const DevCtx& C, PState& path, const Rec
         bool sampleUpper = (lobeTypes & kLobeNonDeltaReflection) != 0;
         bool sampleLower = (lobeTypes & kLobeNonDeltaTransmission) != 0;
         // generateLightSample (:668-701): the type-selection draw is always taken, then the env map
-        // (p = pEnvLight) or the emissive triangles (p = pEmissiveLight) are sampled.
-        bool validSample = false, lsEnv = false;
+        // (p = pEnvLight), the emissive triangles (p = pEmissiveLight) or the analytic lights
+        // (p = pAnalyticLight) are sampled.
+        bool validSample = false, lsEnv = false, lsAnalytic = false;
         TriangleLightSample tls;
         f3 lsLi = mk3(0.f), lsOrigin = mk3(0.f), lsDir = mk3(0.f);
         float lsPdf = 0.f, lsDistance = 0.f, selectionPdf = 0.f;
         bool sampled = false;
-        // without an env map p = {0, haveLights, 0} and the emissive sample's selection pdf is 1
+        // without an env map pEnv = 0, so u - pEnv is u (the reference's running subtraction)
         const float pEnv = kEnv ? C.pEnvLight : 0.f;
-        const float pEmissive = kEnv ? C.pEmissiveLight : (haveLights ? 1.f : 0.f);
+        const float pEmissive = C.pEmissiveLight;
         float u = sampleNext1D(path.sg);
         if (kEnv && u < pEnv)
         {
@@ -282,7 +283,7 @@ __device__ __noinline__ void handle_hit(const DevCtx& C, PState& path, const Rec
         }
         else if (u - pEnv < pEmissive)
         {
-            selectionPdf = kEnv ? pEmissive : 1.f;
+            selectionPdf = pEmissive;
             if (sample_emissive_power(C.lights, sd.posW, path.sg, tls))
             {
                 lsLi = tls.pdf > 0.f ? tls.Le / tls.pdf : mk3(0.f);
@@ -294,6 +295,23 @@ __device__ __noinline__ void handle_hit(const DevCtx& C, PState& path, const Rec
                 lsDistance = length(toLight);
                 lsDir = normalize(toLight);
                 sampled = any_gt0(lsLi);
+            }
+        }
+        else if ((u - pEnv) - pEmissive < C.pAnalyticLight)
+        {
+            // generateAnalyticLightSample (:573-599): no geometry, so the ray runs to the sampled
+            // distance unshortened
+            selectionPdf = C.pAnalyticLight;
+            lsAnalytic = true;
+            AnalyticSample as;
+            if (analytic_light_sample(C.analytic, sd.posW, path.sg, as))
+            {
+                lsLi = as.Li;
+                lsPdf = as.pdf;
+                lsDir = as.dir;
+                lsDistance = as.distance;
+                lsOrigin = computeRayOrigin(sd.posW, dot(sd.faceN, lsDir) >= 0.f ? sd.faceN : -sd.faceN);
+                sampled = true;
             }
         }
         if (sampled)
@@ -312,8 +330,9 @@ __device__ __noinline__ void handle_hit(const DevCtx& C, PState& path, const Rec
         {
             f3 Le = lsLi * lsPdf;
             const BsdfPair bp = mi_eval_pair(sd, d, 0u, lsDir); // all lobes: the pair's total
+            // analytic lights cannot be hit by scatter rays: MIS weight 1 (:1025-1031)
             float scatterPdf = bp.totalPdf;
-            float misWeight = dev_mis(C, lsPdf, scatterPdf);
+            float misWeight = lsAnalytic ? 1.f : dev_mis(C, lsPdf, scatterPdf);
             f3 weight = bp.totalBsdf;
             f3 Lr = weight * misWeight * lsLi;
             if (any_gt0(Lr) && dev_visible(C, mk_ray(lsOrigin, lsDir, 0.f, lsDistance)))
@@ -329,7 +348,10 @@ __device__ __noinline__ void handle_hit(const DevCtx& C, PState& path, const Rec
                     sel.lightIsDistant = lsEnv;
                     if (path.vertex == 1)
                     {
-                        if (lsEnv)
+                        // an analytic light leaves the record's light vertex unset (:1079-1104):
+                        // its second hit keeps the running record's (none)
+                        if (lsAnalytic) {}
+                        else if (lsEnv)
                         {
                             sel.secondHit = hit_direction(lsDir);
                             sel.secondaryPathJacobian = lsPdf;

@@ -123,6 +123,9 @@ struct rs_pass
     DevBuf<float> envTexels, envImportance;
     DevBuf<EnvMapView> envView;
     EnvMapView envHost = {};
+    // analytic lights (rs_set_analytic_lights): device records and their count
+    DevBuf<AnalyticLight> dAnalytic;
+    uint32_t numAnalytic = 0;
     // frame state
     uint32_t W = 0, H = 0;
     uint32_t frameCount = 0, seed = 0;
@@ -444,6 +447,33 @@ extern "C" RS_API rs_status rs_set_scene(rs_pass* p, const rs_scene_desc* sd)
     return RS_OK;
 }
 
+static_assert(sizeof(rs_analytic_light) == sizeof(AnalyticLightDesc), "rs_analytic_light mirrors AnalyticLightDesc");
+
+// The scene's analytic lights (Scene::getLight, used when Scene::useAnalyticLights): each is
+// prepared on the host as Falcor's light classes derive LightData, then copied to the device.
+extern "C" RS_API rs_status rs_set_analytic_lights(rs_pass* p, const rs_analytic_light* lights, uint32_t count)
+{
+    if (!p) return fail(RS_INVALID_ARG, "pass is NULL");
+    if (count > 0 && !lights) return fail(RS_INVALID_ARG, "lights is NULL");
+    std::vector<AnalyticLight> dev(count);
+    for (uint32_t i = 0; i < count; i++)
+    {
+        AnalyticLightDesc d;
+        memcpy(&d, &lights[i], sizeof(d));
+        if (d.type > kLightSphere) return fail(RS_INVALID_ARG, "analytic light " + std::to_string(i) + ": unknown type");
+        if (!prepare_analytic_light(d, dev[i]))
+            return fail(RS_INVALID_ARG, "analytic light " + std::to_string(i) + ": zero direction or singular transform");
+    }
+    if (count > 0)
+    {
+        RS_CUDA(p->dAnalytic.ensure(count));
+        RS_CUDA(cudaMemcpy(p->dAnalytic.p, dev.data(), sizeof(AnalyticLight) * count, cudaMemcpyHostToDevice));
+    }
+    p->numAnalytic = count;
+    p->generation++;
+    return RS_OK;
+}
+
 extern "C" RS_API rs_status rs_set_env_map(rs_pass* p, const rs_env_map* m)
 {
     if (!p) return fail(RS_INVALID_ARG, "pass is NULL");
@@ -574,7 +604,9 @@ static void begin_frame(rs_pass* p, const rs_frame_desc* f)
     C.lights.count = (uint32_t)p->scene.lights.size();
     C.lights.invWeightsSum = p->scene.invWeightsSum;
     C.env = p->envView.p;
-    light_type_probabilities(p->envHost.present != 0, C.lights.count > 0, C.pEnvLight, C.pEmissiveLight);
+    C.analytic.lights = p->dAnalytic.p;
+    C.analytic.count = p->numAnalytic;
+    light_type_probabilities(p->envHost.present != 0, C.lights.count > 0, p->numAnalytic > 0, C.pEnvLight, C.pEmissiveLight, C.pAnalyticLight);
     C.camera = p->camera;
     C.prevCamera = p->havePrevCamera ? p->prevCamera : p->camera;
     C.cm = p->cm;
@@ -1307,6 +1339,7 @@ extern "C" RS_API rs_status rs_backward(rs_pass* p, const void* checkpoint, cons
     if (p->opt.maxSurfaceBounces > 1)
         return fail(RS_INVALID_ARG, "rs_backward replays paths of at most three vertices: set maxSurfaceBounces <= 1");
     if (p->envHost.present) return fail(RS_INVALID_ARG, "rs_backward differentiates scenes lit by emissive triangles; the pass has an env map");
+    if (p->numAnalytic) return fail(RS_INVALID_ARG, "rs_backward differentiates scenes lit by emissive triangles; the pass has analytic lights");
     for (const MaterialData& m : p->scene.materials)
         if (m.flags & kMtlSpecGloss)
             return fail(RS_INVALID_ARG, "rs_backward differentiates metal-rough materials; the scene has a spec-gloss material");

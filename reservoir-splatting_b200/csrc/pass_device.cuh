@@ -9,6 +9,7 @@
 #include "core/camera.h"
 #include "core/lights.h"
 #include "core/envmap.h"
+#include "core/analytic_lights.h"
 
 namespace rs {
 
@@ -23,7 +24,8 @@ struct DevCtx
     const MaterialData* materials;
     LightView lights;
     const EnvMapView* env;  // environment map (present = 0 without one), in device memory
-    float pEnvLight, pEmissiveLight; // light-type selection probabilities (PathTracer.slang:606-622)
+    AnalyticLightView analytic; // the scene's analytic lights (count 0: none)
+    float pEnvLight, pEmissiveLight, pAnalyticLight; // light-type selection probabilities (PathTracer.slang:606-622)
     CameraData camera;      // gScene.camera of this frame
     CameraData prevCamera;  // previous frame's camera (motion vectors)
     CameraManager cm;
@@ -345,7 +347,7 @@ __device__ inline void dev_reconnection_hit(const DevCtx& C, ShiftPath& path, co
     float rayLength = kRayTMax;
     if (!secondHitIsDistant)
     {
-        ShadingData secondSd = dev_sd(C, rd.secondHit, mk3(0.f));
+        ShadingData secondSd = hit_valid(rd.secondHit) ? dev_sd(C, rd.secondHit, mk3(0.f)) : sd_zero_vertex();
         f3 shiftedOffset = secondSd.posW - sd.posW;
         float shiftedDist2 = dot(shiftedOffset, shiftedOffset);
         float shiftedCosine = f_abs(dot(secondSd.faceN, -normalize(shiftedOffset)));

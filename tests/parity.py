@@ -59,13 +59,16 @@ def bit_mismatch_fraction(g, o):
 
 
 def run_pair(rs, oracle_mod, scene, camera_fn, props, frames=5, width=64, height=64, shutter=0.0, aperture=0.0,
-             check_candidates=True, builder="PLOC"):
+             check_candidates=True, builder="PLOC", setup=None):
     gpu = rs.ReservoirSplatting(props, width, height)
     gpu.set_bvh_builder(builder)
     gpu.keep_candidates(True)
     ora = oracle_mod.OraclePass(props, width, height)
     gpu.set_scene(scene)
     ora.set_scene(scene)
+    if setup is not None:  # scene extras given to both passes alike (env map, analytic lights)
+        setup(gpu)
+        setup(ora)
     mode = gpu.options.temporalReuse
     report = {}
     for f in range(frames):
