@@ -16,6 +16,7 @@ groups, objects and smoothing.  Faces before any ``usemtl`` get a grey diffuse m
 from __future__ import annotations
 
 import math
+import warnings
 from pathlib import Path
 
 import numpy as np
@@ -152,7 +153,11 @@ def save_obj(scene: Scene, path, material_names=None, mtl_params=None):
 #     reflection remains); the scalar roughness is getRoughness (:424-462) as written: float2(u + v),
 #     square-rooted when remaproughness, and getScalarRoughness averages the two equal components;
 #   * AreaLightSource "diffuse" (L * scale emitted by the shapes that follow, twosided);
-#   * LightSource "infinite" with a constant "rgb L" (an environment map of that radiance).
+#   * LightSource "infinite" with a constant "rgb L" (an environment map of that radiance);
+#   * LightSource "distant" as a directional analytic light (createLight, PBRTImporter.cpp:676-699:
+#     intensity L * scale, times illuminance when it is positive; direction the transformed
+#     to - from); "point", "spot", "goniometric" and "projection" lights are skipped with a warning,
+#     as the reference importer does.
 # Textures, named spectra other than the defaults, image infinite lights, curves, disks and
 # cylinders are not read.
 
@@ -387,13 +392,15 @@ def _pbrt_material(mtype, ps):
 
 def load_pbrt(path) -> Scene:
     """A PBRT v4 scene file as the pass's triangle soup; info holds "camera" (position, target, up,
-    fovDegrees) and "env" (an [h, w, 3] radiance map for rs_set_env_map) when the file has them."""
+    fovDegrees), "env" (an [h, w, 3] radiance map for rs_set_env_map) and "lights" (analytic lights
+    for rs_set_analytic_lights) when the file has them."""
     path = Path(path)
     tris, mids, mat_rows, mat_index = [], [], [], {}
     state = {"ctm": np.eye(4), "material": ("diffuse", {}), "area": None, "reverse": False}
     stack, named, objects = [], {}, {}
     current_object = None
     camera, env = None, None
+    lights = []
 
     def material_id(mat, area):
         mtype, ps = mat
@@ -503,8 +510,17 @@ def load_pbrt(path) -> Scene:
                         raise ValueError("PBRT image infinite lights (equal-area maps) are not converted")
                     L = np.asarray(_pbrt_rgb(ps, "L", (1.0, 1.0, 1.0)), np.float32) * _pbrt_float(ps, "scale", 1.0)
                     env = np.broadcast_to(L, (8, 16, 3)).astype(np.float32).copy()
+                elif ltype == "distant":
+                    I = np.asarray(_pbrt_rgb(ps, "L", (1.0, 1.0, 1.0)), np.float64) * _pbrt_float(ps, "scale", 1.0)
+                    illum = _pbrt_float(ps, "illuminance", -1.0)
+                    if illum > 0.0:
+                        I = I * illum
+                    fr = np.asarray(ps["from"][1][:3], np.float64) if "from" in ps else np.zeros(3)
+                    to = np.asarray(ps["to"][1][:3], np.float64) if "to" in ps else np.array([0.0, 0.0, 1.0])
+                    d = state["ctm"][:3, :3] @ (to - fr)
+                    lights.append({"type": "directional", "intensity": tuple(I), "direction": tuple(d / np.linalg.norm(d))})
                 else:
-                    raise ValueError(f"PBRT light {ltype!r} is not converted (the pass samples emissive triangles and an env map)")
+                    warnings.warn(f"PBRT light type {ltype!r} is currently not supported and ignored")
             elif d == "Shape":
                 stype = r.next()[1:-1]
                 ps = r.params()
@@ -562,6 +578,8 @@ def load_pbrt(path) -> Scene:
         info["camera"] = camera
     if env is not None:
         info["env"] = env
+    if lights:
+        info["lights"] = lights
     return Scene(np.asarray(tris, np.float32), np.asarray(mids, np.uint32), np.stack(mat_rows).astype(np.float32), path.stem, info)
 
 
@@ -586,7 +604,8 @@ def pbrt_camera(scene: Scene, width: int, height: int):
 # roughconductor (metallic, base = the normal-incidence Fresnel reflectance of rgb eta, k; copper
 # without them; roughness sqrt(alpha)), dielectric / roughdielectric / thindielectric (IoR only: no
 # transmission lobe), twosided (its nested BSDF); shapes obj, ply, rectangle, cube, sphere; area
-# emitters nested in shapes, constant emitters as an env map; a perspective sensor.  <default> and
+# emitters nested in shapes, constant emitters as an env map (point, spot, projector and directional
+# emitters are skipped with a warning: the reference importer converts none of them); a perspective sensor.  <default> and
 # $name substitution, refs by id, and to_world transforms (translate, scale, rotate, matrix, lookat).
 # Image environment maps, textures and other plugins are rejected with a message.
 
@@ -710,6 +729,9 @@ def load_mitsuba(path) -> Scene:
             t, p = el.attrib["type"], props(el)
             if t == "constant":
                 env = np.broadcast_to(np.asarray(p.get("radiance", (1.0,) * 3), np.float32), (8, 16, 3)).astype(np.float32).copy()
+            elif t in ("point", "spot", "projector", "directional", "directionalarea"):
+                # MitsubaImporter.cpp:703-721 converts none of these (unsupportedType, a warning)
+                warnings.warn(f"Mitsuba emitter type {t!r} is not supported")
             else:
                 raise ValueError(f"Mitsuba emitter {t!r} is not converted (area emitters belong inside shapes)")
         elif el.tag == "shape":

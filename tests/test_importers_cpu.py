@@ -151,12 +151,33 @@ def test_pbrt_scene(rs, tmp_path, binary_ply):
 
 def test_pbrt_rejects_what_it_does_not_convert(rs, tmp_path):
     import reservoir_splatting_b200.importers as I
-    for body in ('Shape "disk"', 'LightSource "point" "rgb I" [1 1 1]', 'Material "measured"\nShape "sphere"',
+    for body in ('Shape "disk"', 'Material "measured"\nShape "sphere"',
                  'LightSource "infinite" "string filename" "sky.exr"'):
         p = tmp_path / "bad.pbrt"
         p.write_text("WorldBegin\n" + body + "\n")
         with pytest.raises(ValueError):
             I.load_pbrt(p)
+
+
+def test_pbrt_lights(rs, tmp_path):
+    """createLight (PBRTImporter.cpp:643-700): a distant light becomes a directional analytic light
+    (L * scale * illuminance, direction = transformed to - from); point and spot lights are skipped
+    with a warning, as the reference importer does."""
+    import reservoir_splatting_b200.importers as I
+    p = tmp_path / "lights.pbrt"
+    p.write_text('WorldBegin\nAttributeBegin\nRotate 90 0 0 1\n'
+                 'LightSource "distant" "rgb L" [1 2 3] "float scale" 2 "float illuminance" 1.5 "point3 from" [0 0 0] "point3 to" [1 0 0]\n'
+                 'AttributeEnd\nLightSource "point" "rgb I" [1 1 1]\nLightSource "spot" "rgb I" [1 1 1]\n'
+                 'Shape "trianglemesh" "point3 P" [0 0 0 1 0 0 0 1 0]\n')
+    with pytest.warns(UserWarning, match="not supported"):
+        sc = I.load_pbrt(p)
+    (L,) = sc.info["lights"]
+    assert L["type"] == "directional" and np.allclose(L["intensity"], [3, 6, 9])
+    assert np.allclose(L["direction"], [0, 1, 0], atol=1e-12)  # +x rotated by 90 degrees about z
+    m = tmp_path / "lights.xml"
+    m.write_text('<scene version="3.0.0"><emitter type="point"/><shape type="rectangle"/></scene>')
+    with pytest.warns(UserWarning, match="not supported"):
+        I.load_mitsuba(m)
 
 
 MITSUBA_SCENE = """<scene version="3.0.0">
