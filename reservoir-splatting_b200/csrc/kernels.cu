@@ -180,7 +180,22 @@ __device__ __forceinline__ void next_hit(const DevCtx& C, PState& p) // PathTrac
 // same, and ~28 registers of long-lived state are freed.
 // A call, not inlined: the path tracer's loop then keeps fewer values live across the shading code
 // (k_candidates_direct 4.50 -> 4.40 ms at 1080p, measured twice on separate boxes).
-template <bool kDirect, bool kEnv>
+// generateAnalyticLightSample (PathTracer.slang:573-599) as a call: only scenes with analytic
+// lights reach it, and inlined it would add its registers and code to every path tracer.
+static __device__ __noinline__ bool nee_analytic(const DevCtx& C, f3 posW, f3 faceN, SampleGen& sg, f3& Li, float& pdf, f3& dir,
+                                                 float& distance, f3& origin)
+{
+    AnalyticSample as;
+    if (!analytic_light_sample(C.analytic, posW, sg, as)) return false;
+    Li = as.Li;
+    pdf = as.pdf;
+    dir = as.dir;
+    distance = as.distance;
+    origin = computeRayOrigin(posW, dot(faceN, dir) >= 0.f ? faceN : -faceN);
+    return true;
+}
+
+template <bool kDirect, bool kEnv, bool kAnalytic>
 __device__ __noinline__ void handle_hit(const DevCtx& C, PState& path, const RecPlanes& outRec, uint32_t pix)
 {
     const bool isPrimaryHit = path.vertex == 1;
@@ -227,7 +242,7 @@ __device__ __noinline__ void handle_hit(const DevCtx& C, PState& path, const Rec
         float lightPdf = 0.f;
         if (haveLights && !isPrimaryHit && isLightSampled && isLightSamplable)
         {
-            lightPdf = C.pEmissiveLight * eval_emissive_pdf(C.lights, path.origin, sd.lightIndex, sd.posW, sd_oriented_face_normal(sd));
+            lightPdf = (kEnv || kAnalytic ? C.pEmissiveLight : 1.f) * eval_emissive_pdf(C.lights, path.origin, sd.lightIndex, sd.posW, sd_oriented_face_normal(sd));
             misWeight = dev_mis(C, path.totalPdf, lightPdf);
         }
         bool selected = cand_add_vertex(path, 1.f, path.earlyThroughput * path.thp * d.emission * misWeight);
@@ -264,9 +279,10 @@ __device__ __noinline__ void handle_hit(const DevCtx& C, PState& path, const Rec
         f3 lsLi = mk3(0.f), lsOrigin = mk3(0.f), lsDir = mk3(0.f);
         float lsPdf = 0.f, lsDistance = 0.f, selectionPdf = 0.f;
         bool sampled = false;
-        // without an env map pEnv = 0, so u - pEnv is u (the reference's running subtraction)
+        // with the emissive triangles alone p = {0, haveLights, 0} and the emissive sample's selection
+        // pdf is 1; without an env map pEnv = 0, so u - pEnv is u (the reference's running subtraction)
         const float pEnv = kEnv ? C.pEnvLight : 0.f;
-        const float pEmissive = C.pEmissiveLight;
+        const float pEmissive = (kEnv || kAnalytic) ? C.pEmissiveLight : (haveLights ? 1.f : 0.f);
         float u = sampleNext1D(path.sg);
         if (kEnv && u < pEnv)
         {
@@ -283,7 +299,7 @@ __device__ __noinline__ void handle_hit(const DevCtx& C, PState& path, const Rec
         }
         else if (u - pEnv < pEmissive)
         {
-            selectionPdf = pEmissive;
+            selectionPdf = (kEnv || kAnalytic) ? pEmissive : 1.f;
             if (sample_emissive_power(C.lights, sd.posW, path.sg, tls))
             {
                 lsLi = tls.pdf > 0.f ? tls.Le / tls.pdf : mk3(0.f);
@@ -297,22 +313,13 @@ __device__ __noinline__ void handle_hit(const DevCtx& C, PState& path, const Rec
                 sampled = any_gt0(lsLi);
             }
         }
-        else if ((u - pEnv) - pEmissive < C.pAnalyticLight)
+        else if (kAnalytic && (u - pEnv) - pEmissive < C.pAnalyticLight)
         {
             // generateAnalyticLightSample (:573-599): no geometry, so the ray runs to the sampled
             // distance unshortened
             selectionPdf = C.pAnalyticLight;
             lsAnalytic = true;
-            AnalyticSample as;
-            if (analytic_light_sample(C.analytic, sd.posW, path.sg, as))
-            {
-                lsLi = as.Li;
-                lsPdf = as.pdf;
-                lsDir = as.dir;
-                lsDistance = as.distance;
-                lsOrigin = computeRayOrigin(sd.posW, dot(sd.faceN, lsDir) >= 0.f ? sd.faceN : -sd.faceN);
-                sampled = true;
-            }
+            sampled = nee_analytic(C, sd.posW, sd.faceN, path.sg, lsLi, lsPdf, lsDir, lsDistance, lsOrigin);
         }
         if (sampled)
         {
@@ -332,7 +339,7 @@ __device__ __noinline__ void handle_hit(const DevCtx& C, PState& path, const Rec
             const BsdfPair bp = mi_eval_pair(sd, d, 0u, lsDir); // all lobes: the pair's total
             // analytic lights cannot be hit by scatter rays: MIS weight 1 (:1025-1031)
             float scatterPdf = bp.totalPdf;
-            float misWeight = lsAnalytic ? 1.f : dev_mis(C, lsPdf, scatterPdf);
+            float misWeight = (kAnalytic && lsAnalytic) ? 1.f : dev_mis(C, lsPdf, scatterPdf);
             f3 weight = bp.totalBsdf;
             f3 Lr = weight * misWeight * lsLi;
             if (any_gt0(Lr) && dev_visible(C, mk_ray(lsOrigin, lsDir, 0.f, lsDistance)))
@@ -350,7 +357,7 @@ __device__ __noinline__ void handle_hit(const DevCtx& C, PState& path, const Rec
                     {
                         // an analytic light leaves the record's light vertex unset (:1079-1104):
                         // its second hit keeps the running record's (none)
-                        if (lsAnalytic) {}
+                        if (kAnalytic && lsAnalytic) {}
                         else if (lsEnv)
                         {
                             sel.secondHit = hit_direction(lsDir);
@@ -534,11 +541,11 @@ __device__ void handle_miss(const DevCtx& C, PState& path, const RecPlanes& outR
 
 // One vertex of the tracePath loop (InitialCandidates.cs.slang:80-141): the next closest hit, then
 // handleHit, or handlePrimaryMiss / handleMiss, which end the path.
-template <bool kDirect, bool kEnv>
+template <bool kDirect, bool kEnv, bool kAnalytic>
 __device__ __forceinline__ void path_step(const DevCtx& C, PState& path, const RecPlanes& currRec, uint32_t i)
 {
     next_hit(C, path);
-    if (path.flags & kPHit) handle_hit<kDirect, kEnv>(C, path, currRec, i);
+    if (path.flags & kPHit) handle_hit<kDirect, kEnv, kAnalytic>(C, path, currRec, i);
     else
     {
         if (!kEnv)
@@ -580,7 +587,7 @@ __device__ __forceinline__ void path_finish(PState& path, uint32_t sIdx, uint32_
 }
 
 // InitialCandidates.cs.slang:80-141, several samples per pixel: one thread runs the pixel's paths.
-template <bool kEnv>
+template <bool kEnv, bool kAnalytic>
 __global__ void __launch_bounds__(128, 3) k_candidates(uint32_t slot, ResPlanes curr, RecPlanes currRec)
 {
     const DevCtx& C = c_ctx[slot];
@@ -591,14 +598,14 @@ __global__ void __launch_bounds__(128, 3) k_candidates(uint32_t slot, ResPlanes 
     {
         PState path;
         path_init<false>(C, x, y, path);
-        do path_step<false, kEnv>(C, path, currRec, i);
+        do path_step<false, kEnv, kAnalytic>(C, path, currRec, i);
         while (path.flags & kPActive);
         path_finish<false>(path, sIdx, C.spp, curr, currRec, i);
     }
 }
 
 // One sample per pixel (the reference default): records go straight to the output planes.
-template <bool kEnv>
+template <bool kEnv, bool kAnalytic>
 __device__ __forceinline__ void candidates_direct_body(uint32_t slot, const ResPlanes& curr, const RecPlanes& currRec, Blk blk)
 {
     const DevCtx& C = c_ctx[slot];
@@ -606,15 +613,17 @@ __device__ __forceinline__ void candidates_direct_body(uint32_t slot, const ResP
     if (!tiled_pixel_at(C.W, C.H, blk, i)) return;
     PState path;
     path_init<true>(C, i % C.W, i / C.W, path);
-    do path_step<true, kEnv>(C, path, currRec, i);
+    do path_step<true, kEnv, kAnalytic>(C, path, currRec, i);
     while (path.flags & kPActive);
     path_finish<true>(path, 0, 1, curr, currRec, i);
 }
 
-template <bool kEnv>
+// kAnalytic: the scene has analytic lights (USE_ANALYTIC_LIGHTS); without them the path tracer
+// carries none of their code.
+template <bool kEnv, bool kAnalytic>
 __global__ void __launch_bounds__(128, 8) k_candidates_direct(uint32_t slot, ResPlanes curr, RecPlanes currRec)
 {
-    candidates_direct_body<kEnv>(slot, curr, currRec, Blk{blockIdx.x, 8u});
+    candidates_direct_body<kEnv, kAnalytic>(slot, curr, currRec, Blk{blockIdx.x, 8u});
 }
 
 template <bool kEnv>
@@ -624,7 +633,7 @@ __global__ void __launch_bounds__(128, 8) kb_candidates_direct(BatchQueue q, con
     {
         const uint32_t inst = batch_instance(q, t);
         const CandArgs& a = args[inst];
-        candidates_direct_body<kEnv>(__ldg(q.slot + inst), a.curr, a.currRec, batch_blk(q, inst, t));
+        candidates_direct_body<kEnv, false>(__ldg(q.slot + inst), a.curr, a.currRec, batch_blk(q, inst, t)); // flattened batches have no analytic lights
     }
 }
 
@@ -1157,15 +1166,25 @@ namespace rs {
 // Launchers of both variants of the kernels that reach an environment-light branch: with
 // env = false the kernel carries none of it (the reference compiles its shaders with USE_ENV_LIGHT
 // 0 or 1 the same way).  They live beside the kernels so each launch finds its device code.
-void launch_k_candidates(bool env, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, ResPlanes curr, RecPlanes currRec)
+void launch_k_candidates(bool env, bool analytic, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, ResPlanes curr, RecPlanes currRec)
 {
-    if (env) k_candidates<true><<<grid, block, 0, s>>>(slot, curr, currRec);
-    else k_candidates<false><<<grid, block, 0, s>>>(slot, curr, currRec);
+    if (analytic)
+    {
+        if (env) k_candidates<true, true><<<grid, block, 0, s>>>(slot, curr, currRec);
+        else k_candidates<false, true><<<grid, block, 0, s>>>(slot, curr, currRec);
+    }
+    else if (env) k_candidates<true, false><<<grid, block, 0, s>>>(slot, curr, currRec);
+    else k_candidates<false, false><<<grid, block, 0, s>>>(slot, curr, currRec);
 }
-void launch_k_candidates_direct(bool env, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, ResPlanes curr, RecPlanes currRec)
+void launch_k_candidates_direct(bool env, bool analytic, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, ResPlanes curr, RecPlanes currRec)
 {
-    if (env) k_candidates_direct<true><<<grid, block, 0, s>>>(slot, curr, currRec);
-    else k_candidates_direct<false><<<grid, block, 0, s>>>(slot, curr, currRec);
+    if (analytic)
+    {
+        if (env) k_candidates_direct<true, true><<<grid, block, 0, s>>>(slot, curr, currRec);
+        else k_candidates_direct<false, true><<<grid, block, 0, s>>>(slot, curr, currRec);
+    }
+    else if (env) k_candidates_direct<true, false><<<grid, block, 0, s>>>(slot, curr, currRec);
+    else k_candidates_direct<false, false><<<grid, block, 0, s>>>(slot, curr, currRec);
 }
 void launch_k_robust(bool env, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, ResPlanes prev, RecPlanes prevRec, Shifted* __restrict__ shiftedPaths)
 {

@@ -724,8 +724,9 @@ static rs_status enqueue_frame(rs_pass* p, cudaStream_t s, float4* colorDev, con
         k_vbuffer<<<tiled_blocks(W, H, 256), 256, 0, q[0]>>>(C, p->vbuffer.p, p->mvec.p); p->launches++;
     }
     stage(p, "initialCandidates", q[1]);
-    if (o.samplesPerPixel == 1) RS_ENV_LAUNCH(env, k_candidates_direct, tiled_blocks(W, H, 128), 128, q[1], C, curr.res(), curr.recp());
-    else RS_ENV_LAUNCH(env, k_candidates, grid(N, 128), 128, q[1], C, curr.res(), curr.recp());
+    const bool analytic = p->numAnalytic > 0;
+    if (o.samplesPerPixel == 1) launch_k_candidates_direct(env, analytic, tiled_blocks(W, H, 128), 128, q[1], C, curr.res(), curr.recp());
+    else launch_k_candidates(env, analytic, grid(N, 128), 128, q[1], C, curr.res(), curr.recp());
     p->launches++;
     if (p->keepCandidates)
     {
@@ -1676,7 +1677,7 @@ static bool batch_flattenable(const rs_batch* b, const rs_frame_desc* frames)
         if (o.enableSpatialResampling != o0.enableSpatialResampling || o.numSpatialIterations != o0.numSpatialIterations ||
             o.neighborCount != o0.neighborCount || o.scatterBackupMISOption != o0.scatterBackupMISOption)
             return false;
-        if ((p->envHost.present != 0) != env0 || p->keepCandidates || p->frozen || p->timing) return false;
+        if ((p->envHost.present != 0) != env0 || p->numAnalytic || p->keepCandidates || p->frozen || p->timing) return false;
         if (p->frameCount == 0 || frames[i].sceneShouldReset || frames[i].mvec || frames[i].vbuffer) return false;
     }
     return true;
