@@ -148,6 +148,32 @@ def test_flattened_batch_matches_individual_passes(rs, scenes, env):
 
 
 @pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
+def test_batch_member_with_analytic_lights(rs, scenes):
+    """A member with analytic lights keeps the batch on per-member graphs (the flattened kernels
+    are built without them), and every member still matches its pass rendered alone."""
+    import torch
+    cfgs, solo, batched = _uniform_members(rs, scenes)
+    spot = {"type": "point", "position": (0.5, 0.9, 0.5), "direction": (0.0, -1.0, 0.0), "intensity": (1.0, 1.0, 1.0),
+            "openingAngle": 0.8, "penumbraAngle": 0.2}
+    for p in (solo[0], batched[0]):
+        p.set_analytic_lights([spot])
+    outs = [torch.zeros((h, w, 4), dtype=torch.float32, device="cuda") for _, _, w, h in cfgs]
+    batch = rs.Batch(batched)
+    stream = torch.cuda.current_stream().cuda_stream
+    for f in range(4):
+        cams = [cfg[1](f, cfg[2], cfg[3]) for cfg in cfgs]
+        ref = [p.render(c) for p, c in zip(solo, cams)]
+        batch.execute(cams, [o.data_ptr() for o in outs], stream=stream)
+        torch.cuda.synchronize()
+        assert not batch.last_flattened()
+        for k in range(len(cfgs)):
+            np.testing.assert_array_equal(outs[k].cpu().numpy(), ref[k], err_msg=f"instance {k} frame {f}")
+    batch.close()
+    for p in solo + batched:
+        p.close()
+
+
+@pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
 def test_tuning_cache_round_trip(rs, scenes, tmp_path):
     import torch
     cfgs, solo, batched = _uniform_members(rs, scenes)
