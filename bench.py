@@ -276,8 +276,8 @@ def run_ours(args):
     traffic = measured_traffic()
     dom = max(stage_ms, key=stage_ms.get) if stage_ms else "initialCandidates"
     roofline = roofline_entry(dom, stage_ms, W, H, peak, peak_kind, traffic)
-    roofline["note"] = ("the dominant kernel is BVH-traversal latency bound (ncu: DRAM 8.6% of peak, mostly its local frames; "
-                        "45% issue active, 8.8 of 32 lanes); the frame's bandwidth-bound kernel is reported in hbm_kernel")
+    roofline["note"] = ("the dominant kernel is BVH-traversal latency bound (ncu: DRAM 9.9% of peak, its writes mostly evicted local frames; "
+                        "46% issue active, 9.0 of 32 lanes); the frame's bandwidth-bound kernel is reported in hbm_kernel")
     if "sbCombine" in stage_ms:
         roofline["hbm_kernel"] = roofline_entry("sbCombine", stage_ms, W, H, peak, peak_kind, traffic)
     roofline["stage_ms"] = {k: round(v, 4) for k, v in stage_ms.items()}
