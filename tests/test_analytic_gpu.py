@@ -89,6 +89,18 @@ def test_each_light_type(rs, oracle_mod, scenes, kind, emissive):
 
 
 @pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
+@pytest.mark.parametrize("name,props", [MODES[0], ("GatherOnly-Fast", {"temporalReuse": "GatherOnly", "gatherOption": "Fast"})],
+                         ids=["ScatterBackup-Clamped", "GatherOnly-Fast"])
+def test_depth_of_field_with_analytic_lights(rs, oracle_mod, scenes, name, props):
+    """An open aperture: the gather's depth-of-field split between the lens-vertex copy and the
+    primary-hit reconnection (k_gather_resample) and the spatial shifts over analytic-light records."""
+    props = dict(props, maxSurfaceBounces=2, enableSpatialResampling=True)
+    report, img = P.run_pair(rs, oracle_mod, _lit(scenes), scenes.cornell_camera, props, frames=4, width=40, height=32, aperture=0.02,
+                             setup=lambda p: p.set_analytic_lights([LIGHTS["spot"], LIGHTS["disc"], LIGHTS["directional"]]))
+    assert _mostly_finite(img)
+
+
+@pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
 def test_three_light_types_with_env_map(rs, oracle_mod, scenes):
     """Environment map, emissive triangles and analytic lights: selection probability 1/3 each."""
     sky = scenes.sky_env_map(128, 64, seed=2)
