@@ -466,6 +466,7 @@ extern "C" RS_API rs_status rs_set_analytic_lights(rs_pass* p, const rs_analytic
     }
     if (count > 0)
     {
+        RS_CUDA(cudaDeviceSynchronize()); // frames in flight may still read the previous list
         RS_CUDA(p->dAnalytic.ensure(count));
         RS_CUDA(cudaMemcpy(p->dAnalytic.p, dev.data(), sizeof(AnalyticLight) * count, cudaMemcpyHostToDevice));
     }
