@@ -58,6 +58,8 @@ enum { RS_GATHER_FAST = 0, RS_GATHER_CLAMPED = 1, RS_GATHER_ROBUST = 2 };
 enum { RS_MIS_BALANCE = 0, RS_MIS_PAIRWISE = 1 };
 /* MISHeuristic (Params.slang:48-53); PowerExp uses rs_options.misPowerExponent (0.01 .. 10) */
 enum { RS_MIS_HEURISTIC_BALANCE = 0, RS_MIS_HEURISTIC_POWER_TWO = 1, RS_MIS_HEURISTIC_POWER_EXP = 2 };
+/* EmissiveLightSamplerType (EmissiveLightSamplerType.slangh:36-44): Uniform, LightBVH, Power (default) */
+enum { RS_EMISSIVE_UNIFORM = 0, RS_EMISSIVE_LIGHT_BVH = 1, RS_EMISSIVE_POWER = 2 };
 /* sampleGenerator: SAMPLE_GENERATOR_TINY_UNIFORM = 0 (reference default); 2 = PCG32 */
 enum { RS_SG_TINY_UNIFORM = 0, RS_SG_PCG32 = 2 };
 
@@ -91,6 +93,7 @@ typedef struct rs_options {
     float artificialFrameTime;           /* seconds between two frames' cameras */
     uint32_t frameWidth;                 /* outputSize, <= 4096 */
     uint32_t frameHeight;                /* <= 4096 */
+    uint32_t emissiveSampler;            /* RS_EMISSIVE_* (EmissiveLightSamplerType); LightBVH is not built */
 } rs_options;
 
 /* StandardMaterial parameters; 64 bytes.  flags bit 0 = double sided; bit 1 = the spec-gloss

@@ -584,7 +584,7 @@ struct Pass
         {
             // generateEmissiveSample (:543-565)
             TriangleLightSample tls;
-            if (!sample_emissive_power(lv, vpos, sg, tls)) return false;
+            if (!sample_emissive(lv, vpos, sg, tls)) return false;
             ls.Li = tls.pdf > 0.f ? tls.Le / tls.pdf : mk3(0.f);
             ls.pdf = tls.pdf;
             f3 lightPos = computeRayOrigin(tls.posW, tls.normalW);
@@ -2477,6 +2477,7 @@ __attribute__((visibility("default"))) int ro_set_scene(ro_pass* r, const rs_sce
     p.lv.aliasTable = p.scene.alias.data();
     p.lv.count = (uint32_t)p.scene.lights.size();
     p.lv.invWeightsSum = p.scene.invWeightsSum;
+    p.lv.sampler = p.opt.emissiveSampler;
     p.hasScene = true;
     p.frameCount = 0;
     return RS_OK;
@@ -2484,6 +2485,7 @@ __attribute__((visibility("default"))) int ro_set_scene(ro_pass* r, const rs_sce
 
 __attribute__((visibility("default"))) int ro_execute(ro_pass* r, const rs_frame_desc* f, const float* mvecHost, float* colorHost)
 {
+    r->p.lv.sampler = r->p.opt.emissiveSampler;
     return r->p.execute(f, mvecHost, colorHost);
 }
 
@@ -2599,6 +2601,7 @@ __attribute__((visibility("default"))) int ro_set_materials(ro_pass* r, const rs
     p.lv.aliasTable = p.scene.alias.data();
     p.lv.count = (uint32_t)p.scene.lights.size();
     p.lv.invWeightsSum = p.scene.invWeightsSum;
+    p.lv.sampler = p.opt.emissiveSampler;
     return RS_OK;
 }
 
@@ -2937,7 +2940,7 @@ __attribute__((visibility("default"))) int ro_test_emissive(ro_pass* r, const fl
         SampleGen sg = sg_create((uint32_t)i & 0xffffu, ((uint32_t)i >> 16) + (seed << 8), 99u, kSgPCG32);
         TriangleLightSample ls;
         ls.triangleIndex = kInvalidIndex;
-        const bool ok = sample_emissive_power(L, x, sg, ls);
+        const bool ok = sample_emissive(L, x, sg, ls);
         tri[i] = ls.triangleIndex;
         if (ok)
         {

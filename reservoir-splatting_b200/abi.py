@@ -18,6 +18,7 @@ TEMPORAL_REUSE = {"GatherOnly": 0, "ScatterOnly": 1, "ScatterBackup": 2, "MultiS
 GATHER_MECHANISM = {"Fast": 0, "Clamped": 1, "Robust": 2}
 SCATTER_BACKUP_MIS = {"Balance": 0, "Pairwise": 1}
 MIS_HEURISTIC = {"Balance": 0, "PowerTwo": 1, "PowerExp": 2}
+EMISSIVE_SAMPLER = {"Uniform": 0, "LightBVH": 1, "Power": 2}
 SAMPLE_GENERATOR = {"TinyUniform": 0, "PCG32": 2}
 
 BUF = {
@@ -39,7 +40,7 @@ class RsOptions(C.Structure):
         ("gatherOption", C.c_uint32), ("numTimePartitions", C.c_uint32), ("useConfidenceWeightsTemporally", C.c_uint32),
         ("numSpatialIterations", C.c_uint32), ("spatialGatherRadius", C.c_float), ("neighborCount", C.c_uint32),
         ("useConfidenceWeightsSpatially", C.c_uint32), ("artificialFrameTime", C.c_float), ("frameWidth", C.c_uint32),
-        ("frameHeight", C.c_uint32),
+        ("frameHeight", C.c_uint32), ("emissiveSampler", C.c_uint32),
     ]
 
 
@@ -162,6 +163,7 @@ def default_options(width: int = 1920, height: int = 1080) -> RsOptions:
     o.artificialFrameTime = 1.0 / 60.0
     o.frameWidth = width
     o.frameHeight = height
+    o.emissiveSampler = EMISSIVE_SAMPLER["Power"]
     return o
 
 
@@ -200,8 +202,12 @@ def options_from_properties(props: dict | None, width: int, height: int) -> RsOp
         if key in _NO_EFFECT or key == "fixedOutputSize" or (key == "outputSize" and isinstance(value, str)):
             continue
         if key == "emissiveSampler":
-            if value not in ("Power", 2):
-                raise ValueError("emissiveSampler: only the power sampler (EmissivePowerSampler, the reference default) is built")
+            v = EMISSIVE_SAMPLER.get(value, value) if isinstance(value, str) else int(value)
+            if isinstance(v, str):
+                raise ValueError(f"unknown value {value!r} for property 'emissiveSampler'")
+            if v not in (0, 2):
+                raise ValueError("emissiveSampler: the Uniform and Power samplers are built (LightBVH is not)")
+            o.emissiveSampler = v
             continue
         field = _ALIASES.get(key, key)
         if key in _ENUMS and isinstance(value, str):

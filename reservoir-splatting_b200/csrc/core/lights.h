@@ -41,13 +41,25 @@ RS_HD void light_set_vertices(LightTriangle& L, f3 p0, f3 p1, f3 p2)
     }
 }
 
+// EmissiveLightSamplerType (EmissiveLightSamplerType.slangh:36-44): the uniform and power samplers.
+enum : uint32_t { kEmissiveUniform = 0, kEmissiveLightBVH = 1, kEmissivePower = 2 };
+
 struct LightView
 {
     const LightTriangle* tris;
     const u2* aliasTable;
     uint32_t count;
     float invWeightsSum;
+    uint32_t sampler; // kEmissiveUniform or kEmissivePower
 };
+
+// evalTriangleSelectionPdf of the sampler: flux / total flux (power) or 1 / count (uniform,
+// EmissiveUniformSampler.slang:81-87).
+RS_HD float emissive_selection_pdf(const LightView& L, uint32_t triangleIndex)
+{
+    if (L.sampler == kEmissiveUniform) return L.count > 0 ? 1.f / (float)L.count : 0.f;
+    return L.tris[triangleIndex].flux * L.invWeightsSum;
+}
 
 struct TriangleLightSample
 {
@@ -109,6 +121,28 @@ RS_HD bool sample_emissive_power(const LightView& L, f3 posW, SampleGen& sg, Tri
     return true;
 }
 
+// EmissiveUniformSampler::sampleLight (EmissiveUniformSampler.slang:55-75): a triangle with
+// probability 1 / count, then a uniform point on it.  Draw order: uLight, then 2D on the triangle.
+RS_HD bool sample_emissive_uniform(const LightView& L, f3 posW, SampleGen& sg, TriangleLightSample& ls)
+{
+    if (L.count == 0) return false;
+    float uLight = sampleNext1D(sg);
+    uint32_t triangleCount = L.count;
+    uint32_t idx = (uint32_t)(uLight * (float)triangleCount);
+    uint32_t triangleIndex = idx < triangleCount - 1 ? idx : triangleCount - 1;
+    float triangleSelectionPdf = 1.f / (float)triangleCount;
+    f2 u; u.x = sampleNext1D(sg); u.y = sampleNext1D(sg);
+    if (!sample_triangle_light(L, posW, triangleIndex, u, ls)) return false;
+    ls.pdf *= triangleSelectionPdf;
+    return true;
+}
+
+// The scene's emissive sampler (EmissiveLightSampler.slang: the type the pass was compiled with).
+RS_HD bool sample_emissive(const LightView& L, f3 posW, SampleGen& sg, TriangleLightSample& ls)
+{
+    return L.sampler == kEmissiveUniform ? sample_emissive_uniform(L, posW, sg, ls) : sample_emissive_power(L, posW, sg, ls);
+}
+
 // The material of the emissive triangles whose radiance is Le (each channel within 1e-5 relative),
 // when exactly one material qualifies; kInvalidIndex otherwise.  The adjoint's fallback for a light
 // sample it cannot find again by tracing (a ray through the seam between two triangles of a light).
@@ -128,11 +162,12 @@ RS_HD uint32_t emissive_material_with_radiance(const LightView& L, f3 Le)
     return found;
 }
 
-// EmissivePowerSampler::evalPdf + evalTrianglePdf: solid-angle pdf at posW of a hit on light triangleIndex.
+// evalPdf + evalTrianglePdf of the power or uniform sampler: solid-angle pdf at posW of a hit on
+// light triangleIndex.
 RS_HD float eval_emissive_pdf(const LightView& L, f3 posW, uint32_t triangleIndex, f3 hitPosW, f3 hitNormalW)
 {
     if (triangleIndex == kInvalidIndex) return 0.f;
-    float triangleSelectionPdf = L.tris[triangleIndex].flux * L.invWeightsSum;
+    float triangleSelectionPdf = emissive_selection_pdf(L, triangleIndex);
     f3 toLight = hitPosW - posW;
     const float distSqr = dot(toLight, toLight);
     float trianglePdf;

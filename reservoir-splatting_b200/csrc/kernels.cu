@@ -195,7 +195,7 @@ static __device__ __noinline__ bool nee_analytic(const DevCtx& C, f3 posW, f3 fa
     return true;
 }
 
-template <bool kDirect, bool kEnv, bool kAnalytic>
+template <bool kDirect, bool kEnv, bool kAnalytic, bool kUniform>
 __device__ __noinline__ void handle_hit(const DevCtx& C, PState& path, const RecPlanes& outRec, uint32_t pix)
 {
     const bool isPrimaryHit = path.vertex == 1;
@@ -300,7 +300,7 @@ __device__ __noinline__ void handle_hit(const DevCtx& C, PState& path, const Rec
         else if (u - pEnv < pEmissive)
         {
             selectionPdf = (kEnv || kAnalytic) ? pEmissive : 1.f;
-            if (sample_emissive_power(C.lights, sd.posW, path.sg, tls))
+            if (kUniform ? sample_emissive_uniform(C.lights, sd.posW, path.sg, tls) : sample_emissive_power(C.lights, sd.posW, path.sg, tls))
             {
                 lsLi = tls.pdf > 0.f ? tls.Le / tls.pdf : mk3(0.f);
                 lsPdf = tls.pdf;
@@ -541,11 +541,15 @@ __device__ void handle_miss(const DevCtx& C, PState& path, const RecPlanes& outR
 
 // One vertex of the tracePath loop (InitialCandidates.cs.slang:80-141): the next closest hit, then
 // handleHit, or handlePrimaryMiss / handleMiss, which end the path.
-template <bool kDirect, bool kEnv, bool kAnalytic>
+// kLights: bit 0 environment map, bit 1 analytic lights, bit 2 the uniform emissive sampler (the
+// reference compiles its shaders per light configuration the same way: USE_ENV_LIGHT,
+// USE_ANALYTIC_LIGHTS, _EMISSIVE_LIGHT_SAMPLER_TYPE)
+template <bool kDirect, uint32_t kLights>
 __device__ __forceinline__ void path_step(const DevCtx& C, PState& path, const RecPlanes& currRec, uint32_t i)
 {
+    constexpr bool kEnv = (kLights & 1u) != 0;
     next_hit(C, path);
-    if (path.flags & kPHit) handle_hit<kDirect, kEnv, kAnalytic>(C, path, currRec, i);
+    if (path.flags & kPHit) handle_hit<kDirect, kEnv, (kLights & 2u) != 0, (kLights & 4u) != 0>(C, path, currRec, i);
     else
     {
         if (!kEnv)
@@ -587,7 +591,7 @@ __device__ __forceinline__ void path_finish(PState& path, uint32_t sIdx, uint32_
 }
 
 // InitialCandidates.cs.slang:80-141, several samples per pixel: one thread runs the pixel's paths.
-template <bool kEnv, bool kAnalytic>
+template <uint32_t kLights>
 __global__ void __launch_bounds__(128, 3) k_candidates(uint32_t slot, ResPlanes curr, RecPlanes currRec)
 {
     const DevCtx& C = c_ctx[slot];
@@ -598,14 +602,14 @@ __global__ void __launch_bounds__(128, 3) k_candidates(uint32_t slot, ResPlanes 
     {
         PState path;
         path_init<false>(C, x, y, path);
-        do path_step<false, kEnv, kAnalytic>(C, path, currRec, i);
+        do path_step<false, kLights>(C, path, currRec, i);
         while (path.flags & kPActive);
         path_finish<false>(path, sIdx, C.spp, curr, currRec, i);
     }
 }
 
 // One sample per pixel (the reference default): records go straight to the output planes.
-template <bool kEnv, bool kAnalytic>
+template <uint32_t kLights>
 __device__ __forceinline__ void candidates_direct_body(uint32_t slot, const ResPlanes& curr, const RecPlanes& currRec, Blk blk)
 {
     const DevCtx& C = c_ctx[slot];
@@ -613,17 +617,17 @@ __device__ __forceinline__ void candidates_direct_body(uint32_t slot, const ResP
     if (!tiled_pixel_at(C.W, C.H, blk, i)) return;
     PState path;
     path_init<true>(C, i % C.W, i / C.W, path);
-    do path_step<true, kEnv, kAnalytic>(C, path, currRec, i);
+    do path_step<true, kLights>(C, path, currRec, i);
     while (path.flags & kPActive);
     path_finish<true>(path, 0, 1, curr, currRec, i);
 }
 
-// kAnalytic: the scene has analytic lights (USE_ANALYTIC_LIGHTS); without them the path tracer
-// carries none of their code.
-template <bool kEnv, bool kAnalytic>
+// kLights as in path_step: the default variant (emissive triangles, power sampler) carries no
+// code of the other light configurations.
+template <uint32_t kLights>
 __global__ void __launch_bounds__(128, 8) k_candidates_direct(uint32_t slot, ResPlanes curr, RecPlanes currRec)
 {
-    candidates_direct_body<kEnv, kAnalytic>(slot, curr, currRec, Blk{blockIdx.x, 8u});
+    candidates_direct_body<kLights>(slot, curr, currRec, Blk{blockIdx.x, 8u});
 }
 
 template <bool kEnv>
@@ -633,7 +637,7 @@ __global__ void __launch_bounds__(128, 8) kb_candidates_direct(BatchQueue q, con
     {
         const uint32_t inst = batch_instance(q, t);
         const CandArgs& a = args[inst];
-        candidates_direct_body<kEnv, false>(__ldg(q.slot + inst), a.curr, a.currRec, batch_blk(q, inst, t)); // flattened batches have no analytic lights
+        candidates_direct_body<kEnv ? 1u : 0u>(__ldg(q.slot + inst), a.curr, a.currRec, batch_blk(q, inst, t)); // flattened members: power sampler, no analytic lights
     }
 }
 
@@ -1166,26 +1170,28 @@ namespace rs {
 // Launchers of both variants of the kernels that reach an environment-light branch: with
 // env = false the kernel carries none of it (the reference compiles its shaders with USE_ENV_LIGHT
 // 0 or 1 the same way).  They live beside the kernels so each launch finds its device code.
-void launch_k_candidates(bool env, bool analytic, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, ResPlanes curr, RecPlanes currRec)
-{
-    if (analytic)
-    {
-        if (env) k_candidates<true, true><<<grid, block, 0, s>>>(slot, curr, currRec);
-        else k_candidates<false, true><<<grid, block, 0, s>>>(slot, curr, currRec);
+#define RS_LIGHT_VARIANTS(kernel)                                                                                  \
+    switch (lights & 7u)                                                                                           \
+    {                                                                                                              \
+    case 0: kernel<0u><<<grid, block, 0, s>>>(slot, curr, currRec); break;                                        \
+    case 1: kernel<1u><<<grid, block, 0, s>>>(slot, curr, currRec); break;                                        \
+    case 2: kernel<2u><<<grid, block, 0, s>>>(slot, curr, currRec); break;                                        \
+    case 3: kernel<3u><<<grid, block, 0, s>>>(slot, curr, currRec); break;                                        \
+    case 4: kernel<4u><<<grid, block, 0, s>>>(slot, curr, currRec); break;                                        \
+    case 5: kernel<5u><<<grid, block, 0, s>>>(slot, curr, currRec); break;                                        \
+    case 6: kernel<6u><<<grid, block, 0, s>>>(slot, curr, currRec); break;                                        \
+    default: kernel<7u><<<grid, block, 0, s>>>(slot, curr, currRec); break;                                       \
     }
-    else if (env) k_candidates<true, false><<<grid, block, 0, s>>>(slot, curr, currRec);
-    else k_candidates<false, false><<<grid, block, 0, s>>>(slot, curr, currRec);
-}
-void launch_k_candidates_direct(bool env, bool analytic, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, ResPlanes curr, RecPlanes currRec)
+// lights: bit 0 environment map, bit 1 analytic lights, bit 2 uniform emissive sampler
+void launch_k_candidates(uint32_t lights, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, ResPlanes curr, RecPlanes currRec)
 {
-    if (analytic)
-    {
-        if (env) k_candidates_direct<true, true><<<grid, block, 0, s>>>(slot, curr, currRec);
-        else k_candidates_direct<false, true><<<grid, block, 0, s>>>(slot, curr, currRec);
-    }
-    else if (env) k_candidates_direct<true, false><<<grid, block, 0, s>>>(slot, curr, currRec);
-    else k_candidates_direct<false, false><<<grid, block, 0, s>>>(slot, curr, currRec);
+    RS_LIGHT_VARIANTS(k_candidates)
 }
+void launch_k_candidates_direct(uint32_t lights, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, ResPlanes curr, RecPlanes currRec)
+{
+    RS_LIGHT_VARIANTS(k_candidates_direct)
+}
+#undef RS_LIGHT_VARIANTS
 void launch_k_robust(bool env, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, ResPlanes prev, RecPlanes prevRec, Shifted* __restrict__ shiftedPaths)
 {
     if (env) k_robust<true><<<grid, block, 0, s>>>(slot, prev, prevRec, shiftedPaths);

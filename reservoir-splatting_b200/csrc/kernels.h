@@ -121,8 +121,8 @@ int batched_blocks_per_sm(BatchStage stage, bool env);
 
 // The kernels that reach an environment-light branch are templates on it (kEnv), defined and
 // launched in kernels.cu: launch one of the two variants (env: the pass has an environment light).
-void launch_k_candidates(bool env, bool analytic, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, ResPlanes curr, RecPlanes currRec);
-void launch_k_candidates_direct(bool env, bool analytic, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, ResPlanes curr, RecPlanes currRec);
+void launch_k_candidates(uint32_t lights, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, ResPlanes curr, RecPlanes currRec);
+void launch_k_candidates_direct(uint32_t lights, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, ResPlanes curr, RecPlanes currRec);
 void launch_k_robust(bool env, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, ResPlanes prev, RecPlanes prevRec, Shifted* __restrict__ shiftedPaths);
 void launch_k_gather_resample(bool env, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, const uint4* __restrict__ vbuffer, ResPlanes curr, RecPlanes currRec, ResPlanes inter, RecPlanes interRec, const float2* __restrict__ floatingCoords, float4* __restrict__ color);
 void launch_k_so_curr(bool env, dim3 grid, dim3 block, cudaStream_t s, uint32_t slot, WaveCtx K);

@@ -245,6 +245,7 @@ extern "C" RS_API void rs_default_options(rs_options* o)
     o->useConfidenceWeightsSpatially = 1;
     o->artificialFrameTime = 1.f / 60.f;
     o->frameWidth = 1920; o->frameHeight = 1080;
+    o->emissiveSampler = RS_EMISSIVE_POWER;
 }
 
 // validateOptions (ReservoirSplatting.cpp:263-301): out-of-range values are rejected here
@@ -259,6 +260,8 @@ static rs_status validate(const rs_options* o)
         return fail(RS_INVALID_ARG, "Frame dimensions up to 4096 pixels width/height are supported");
     if (o->sampleGenerator != RS_SG_TINY_UNIFORM && o->sampleGenerator != RS_SG_PCG32) return fail(RS_INVALID_ARG, "unknown sampleGenerator");
     if (o->misHeuristic > 2) return fail(RS_INVALID_ARG, "misHeuristic must be Balance, PowerTwo or PowerExp");
+    if (o->emissiveSampler != RS_EMISSIVE_UNIFORM && o->emissiveSampler != RS_EMISSIVE_POWER)
+        return fail(RS_INVALID_ARG, "emissiveSampler must be Uniform or Power (the LightBVH sampler is not built)");
     if (o->misHeuristic == RS_MIS_HEURISTIC_POWER_EXP && !(o->misPowerExponent >= 0.01f && o->misPowerExponent <= 10.f))
         return fail(RS_INVALID_ARG, "misPowerExponent must be in [0.01, 10]");
     if (o->temporalReuse > 3) return fail(RS_INVALID_ARG, "unknown temporalReuse");
@@ -604,6 +607,7 @@ static void begin_frame(rs_pass* p, const rs_frame_desc* f)
     C.lights.aliasTable = p->dAlias.p;
     C.lights.count = (uint32_t)p->scene.lights.size();
     C.lights.invWeightsSum = p->scene.invWeightsSum;
+    C.lights.sampler = p->opt.emissiveSampler;
     C.env = p->envView.p;
     C.analytic.lights = p->dAnalytic.p;
     C.analytic.count = p->numAnalytic;
@@ -725,9 +729,10 @@ static rs_status enqueue_frame(rs_pass* p, cudaStream_t s, float4* colorDev, con
         k_vbuffer<<<tiled_blocks(W, H, 256), 256, 0, q[0]>>>(C, p->vbuffer.p, p->mvec.p); p->launches++;
     }
     stage(p, "initialCandidates", q[1]);
-    const bool analytic = p->numAnalytic > 0;
-    if (o.samplesPerPixel == 1) launch_k_candidates_direct(env, analytic, tiled_blocks(W, H, 128), 128, q[1], C, curr.res(), curr.recp());
-    else launch_k_candidates(env, analytic, grid(N, 128), 128, q[1], C, curr.res(), curr.recp());
+    // the path tracer's light configuration: env map, analytic lights, uniform emissive sampler
+    const uint32_t lights = (env ? 1u : 0u) | (p->numAnalytic > 0 ? 2u : 0u) | (o.emissiveSampler == RS_EMISSIVE_UNIFORM ? 4u : 0u);
+    if (o.samplesPerPixel == 1) launch_k_candidates_direct(lights, tiled_blocks(W, H, 128), 128, q[1], C, curr.res(), curr.recp());
+    else launch_k_candidates(lights, grid(N, 128), 128, q[1], C, curr.res(), curr.recp());
     p->launches++;
     if (p->keepCandidates)
     {
@@ -1678,7 +1683,9 @@ static bool batch_flattenable(const rs_batch* b, const rs_frame_desc* frames)
         if (o.enableSpatialResampling != o0.enableSpatialResampling || o.numSpatialIterations != o0.numSpatialIterations ||
             o.neighborCount != o0.neighborCount || o.scatterBackupMISOption != o0.scatterBackupMISOption)
             return false;
-        if ((p->envHost.present != 0) != env0 || p->numAnalytic || p->keepCandidates || p->frozen || p->timing) return false;
+        if ((p->envHost.present != 0) != env0 || p->numAnalytic || o.emissiveSampler != RS_EMISSIVE_POWER || p->keepCandidates || p->frozen ||
+            p->timing)
+            return false;
         if (p->frameCount == 0 || frames[i].sceneShouldReset || frames[i].mvec || frames[i].vbuffer) return false;
     }
     return true;

@@ -77,6 +77,8 @@ def test_every_reference_property_key_is_accepted(rs):
     assert (o.frameWidth, o.frameHeight) == (160, 120)
     o = rs.abi.options_from_properties({"outputSize": "Fixed", "fixedOutputSize": (96, 64)}, 320, 240)
     assert (o.frameWidth, o.frameHeight) == (96, 64)
+    assert rs.abi.options_from_properties({"emissiveSampler": "Uniform"}, 64, 64).emissiveSampler == 0
+    assert o.emissiveSampler == 2  # Power, the default (EmissiveLightSamplerType::Power)
     with pytest.raises(ValueError):
         rs.abi.options_from_properties({"emissiveSampler": "LightBVH"}, 64, 64)
     with pytest.raises(ValueError):
@@ -94,6 +96,15 @@ def test_invalid_options_are_rejected_before_any_device_work(rs, bad):
     st = lib.rs_create(C.byref(o), C.byref(h))
     assert st == rs.abi.RS_INVALID_ARG
     assert lib.rs_last_error_string()
+
+
+def test_light_bvh_sampler_is_rejected(rs):
+    lib = rs.load_library()
+    o = rs.abi.default_options(64, 64)
+    o.emissiveSampler = 1  # EmissiveLightSamplerType::LightBVH, not built
+    h = C.c_void_p()
+    assert lib.rs_create(C.byref(o), C.byref(h)) == rs.abi.RS_INVALID_ARG
+    assert b"LightBVH" in lib.rs_last_error_string()
 
 
 def test_oversized_frame_is_rejected(rs):

@@ -312,7 +312,11 @@ def _solid_angle(p0, p1, p2, x):
     return 2.0 * math.atan2(num, den)
 
 
-def test_emissive_sampling_pdf_selection_and_solid_angle(lib, oracle_mod, rs):
+@pytest.mark.parametrize("sampler", ["Power", "Uniform"])
+def test_emissive_sampling_pdf_selection_and_solid_angle(lib, oracle_mod, rs, sampler):
+    """EmissivePowerSampler (triangles in proportion to their flux) and EmissiveUniformSampler
+    (each triangle with probability 1 / count): the sample's pdf is evalPdf, the selection follows
+    the sampler, and E[1 / pdf] over a light's samples is its solid angle."""
     import reservoir_splatting_b200.scenes as S
     # a floor and five emissive triangles of different radiance, area and orientation
     tris, mats, mids = [], [S.material((0.5, 0.5, 0.5))], []
@@ -333,7 +337,7 @@ def test_emissive_sampling_pdf_selection_and_solid_angle(lib, oracle_mod, rs):
     mats.append(S.material((0, 0, 0), emissive=(10.0, 10.0, 10.0)))
     mids.append(len(mats) - 1)
     sc = S.Scene(np.asarray(tris, np.float32), np.asarray(mids, np.uint32), np.stack(mats).astype(np.float32))
-    ora = oracle_mod.OraclePass({"temporalReuse": "GatherOnly"}, 8, 8)
+    ora = oracle_mod.OraclePass({"temporalReuse": "GatherOnly", "emissiveSampler": sampler}, 8, 8)
     ora.set_scene(sc)
     n_l = lib.ro_test_lights(ora._h, None)
     rec = np.zeros((n_l, 20), np.float32)
@@ -349,9 +353,10 @@ def test_emissive_sampling_pdf_selection_and_solid_angle(lib, oracle_mod, rs):
     ok = pdf > 0
     # the sample's pdf is evalPdf at the sampled point
     assert np.all(np.abs(pdf[ok] - epdf[ok]) <= 1e-5 * epdf[ok])
-    # triangles are picked in proportion to their flux (before the facing test)
+    # triangles are picked in proportion to their flux, or uniformly (before the facing test)
     counts = np.bincount(tri, minlength=n_l).astype(np.float64)
-    passed, pval, msg = chi2_test(counts, flux / flux.sum() * n, n)
+    expected = flux / flux.sum() * n if sampler == "Power" else np.full(n_l, n / n_l)
+    passed, pval, msg = chi2_test(counts, expected, n)
     assert passed, msg
     # E[1 / pdf; sample of light t] = solid angle of t (a light facing away contributes 0)
     for t in range(n_l):

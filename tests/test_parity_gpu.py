@@ -93,6 +93,20 @@ def test_terrain_scene_scatter_backup(rs, oracle_mod, scenes, builder):
 
 
 @pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
+@pytest.mark.parametrize("mode", ["ScatterBackup", "GatherOnly", "MultiScatter"])
+def test_uniform_emissive_sampler(rs, oracle_mod, scenes, mode):
+    """emissiveSampler = Uniform (EmissiveUniformSampler): NEE picks each emissive triangle with
+    probability 1 / count and the BSDF-hit MIS uses the same selection pdf, on the GPU as in the oracle."""
+    sc = scenes.terrain_spheres(seed=7, grid=48, spheres=12, subdiv=2, lights=8, extent=40.0, height=4.0)
+    props = {"temporalReuse": mode, "gatherOption": "Clamped", "maxSurfaceBounces": 2, "emissiveSampler": "Uniform",
+             "enableSpatialResampling": True}
+    cam = lambda f, w, h: scenes.orbit_camera(f, w, h, radius=30.0, height_above=12.0)
+    report, img = run_pair(rs, oracle_mod, sc, cam, props, frames=4, width=80, height=48,
+                           shutter=0.04 if mode == "MultiScatter" else 0.0)
+    assert np.isfinite(img).all() and img[..., :3].mean() > 0.0
+
+
+@pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
 @pytest.mark.parametrize("mode", ["ScatterBackup", "GatherOnly"])
 def test_imported_obj_spec_gloss_scene(rs, oracle_mod, scenes, tmp_path, mode):
     """A Cornell box written as OBJ + MTL and imported with the Assimp importer's OBJ mapping:
