@@ -778,3 +778,347 @@ def load_mitsuba(path) -> Scene:
     if env is not None:
         info["env"] = env
     return Scene(np.asarray(tris, np.float32), np.asarray(mids, np.uint32), np.stack(rows).astype(np.float32), path.stem, info)
+
+
+# ---------------------------------------------------------------- Falcor Python scenes (.pyscene)
+# The reference's PythonImporter (Source/plugins/importers/PythonImporter/PythonImporter.cpp) runs a
+# .pyscene file as a Python script with `sceneBuilder` and Falcor's scene classes in scope.  This
+# runs it with stand-ins for the classes the pass renders, with the semantics of their Falcor
+# definitions:
+#   * float2 / float3 / float4 (one argument broadcasts);
+#   * Transform (Scene/Transform.cpp): translation, scaling, rotationEuler (radians, the quaternion
+#     of Utils/Math/QuaternionMath.h:398-409) or rotationEulerDeg, lookAt(position, target, up);
+#     matrix = T x R x S (the default ScaleRotateTranslate order);
+#   * TriangleMesh (Scene/TriangleMesh.cpp:58-194): createQuad, createDisk, createCube, createSphere
+#     with their vertex and index layouts, createFromFile for OBJ files, and addVertex / addTriangle;
+#   * StandardMaterial (alias Material; Scene/Material/BasicMaterial.cpp, StandardMaterial.cpp):
+#     baseColor, roughness, metallic, specularParams (occlusion, roughness, metallic; or specular
+#     colour and glossiness with ShadingModel.SpecGloss), emissiveColor x emissiveFactor,
+#     indexOfRefraction, doubleSided; defaults baseColor 1, roughness 0, metallic 0, IoR 1.5,
+#     single-sided;
+#   * Camera (Scene/Camera/Camera.cpp:426-440, CameraData.slang defaults);
+#   * PointLight, DirectionalLight, DistantLight, RectLight, DiscLight, SphereLight (Scene/Lights/
+#     Light.cpp:404-440) as analytic lights (info["lights"], for rs_set_analytic_lights);
+#   * sceneBuilder: addTriangleMesh, addMaterial, getMaterial, addNode (with parents), addMeshInstance,
+#     addLight, getLight, addCamera.
+# Meshes are flattened to world space per instance; the winding is flipped when the mesh's front face
+# is clockwise or the instance transform mirrors, as Falcor flips the face normal then.  Textures,
+# environment maps from files, SDF grids, volumes, curves and animations raise ValueError.
+
+def _pys_vec(n):
+    def make(*a):
+        if len(a) == 1 and not isinstance(a[0], (int, float)):
+            a = tuple(a[0])
+        if len(a) == 1:
+            a = a * n
+        if len(a) != n:
+            raise ValueError(f"float{n} takes 1 or {n} values")
+        return tuple(float(x) for x in a)
+    return make
+
+
+class _PysTransform:
+    def __init__(self):
+        self.translation = (0.0, 0.0, 0.0)
+        self.scaling = (1.0, 1.0, 1.0)
+        self._R = np.eye(3)
+
+    @property
+    def rotationEuler(self):
+        raise AttributeError("reading rotationEuler is not supported")
+
+    @rotationEuler.setter
+    def rotationEuler(self, a):
+        c, s = np.cos(np.asarray(a, np.float64) * 0.5), np.sin(np.asarray(a, np.float64) * 0.5)
+        x = s[0] * c[1] * c[2] - c[0] * s[1] * s[2]
+        y = c[0] * s[1] * c[2] + s[0] * c[1] * s[2]
+        z = c[0] * c[1] * s[2] - s[0] * s[1] * c[2]
+        w = c[0] * c[1] * c[2] + s[0] * s[1] * s[2]
+        self._R = np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y)],
+                            [2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x)],
+                            [2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)]])
+
+    @property
+    def rotationEulerDeg(self):
+        raise AttributeError("reading rotationEulerDeg is not supported")
+
+    @rotationEulerDeg.setter
+    def rotationEulerDeg(self, a):
+        self.rotationEuler = tuple(math.radians(float(v)) for v in a)
+
+    def lookAt(self, position, target, up):
+        # Transform::lookAt: translation = position; rotation columns (right, up', -dir), right handed
+        self.translation = tuple(float(v) for v in position)
+        d = np.asarray(target, np.float64) - np.asarray(position, np.float64)
+        d /= np.linalg.norm(d)
+        zc = -d
+        right = np.cross(np.asarray(up, np.float64), zc)
+        right /= np.linalg.norm(right)
+        self._R = np.stack([right, np.cross(zc, right), zc], axis=1)
+
+    @property
+    def matrix(self):
+        M = np.eye(4)
+        M[:3, :3] = self._R @ np.diag(np.asarray(self.scaling, np.float64))
+        M[:3, 3] = self.translation
+        return M
+
+
+class _PysMesh:
+    def __init__(self, positions=None, indices=None, front_face_cw=False):
+        self.positions = [] if positions is None else [tuple(map(float, p)) for p in positions]
+        self.indices = [] if indices is None else [int(i) for i in indices]
+        self.frontFaceCW = bool(front_face_cw)
+        self.name = ""
+
+    def addVertex(self, position, normal=None, texCoord=None):
+        self.positions.append(tuple(float(v) for v in position))
+        return len(self.positions) - 1
+
+    def addTriangle(self, i0, i1, i2):
+        self.indices += [int(i0), int(i1), int(i2)]
+
+    @staticmethod
+    def createQuad(size=(1.0, 1.0)):
+        hx, hy = 0.5 * float(size[0]), 0.5 * float(size[1])
+        return _PysMesh([(-hx, 0, -hy), (hx, 0, -hy), (-hx, 0, hy), (hx, 0, hy)], [2, 1, 0, 1, 2, 3], float(size[0]) * float(size[1]) < 0)
+
+    @staticmethod
+    def createDisk(radius=1.0, segments=32):
+        P, I = [(0.0, 0.0, 0.0)], []
+        for i in range(segments):
+            phi = np.float32(i) / np.float32(segments) * np.float32(2.0 * math.pi)
+            P.append((math.cos(phi) * radius, 0.0, -math.sin(phi) * radius))
+            I += [0, i + 1, (i + 1) % segments + 1]
+        return _PysMesh(P, I)
+
+    @staticmethod
+    def createCube(size=(1.0, 1.0, 1.0)):
+        faces = [[(-.5, -.5, -.5), (-.5, -.5, .5), (.5, -.5, .5), (.5, -.5, -.5)], [(-.5, .5, .5), (-.5, .5, -.5), (.5, .5, -.5), (.5, .5, .5)],
+                 [(-.5, .5, -.5), (-.5, -.5, -.5), (.5, -.5, -.5), (.5, .5, -.5)], [(.5, .5, .5), (.5, -.5, .5), (-.5, -.5, .5), (-.5, .5, .5)],
+                 [(-.5, .5, .5), (-.5, -.5, .5), (-.5, -.5, -.5), (-.5, .5, -.5)], [(.5, .5, -.5), (.5, -.5, -.5), (.5, -.5, .5), (.5, .5, .5)]]
+        s = np.asarray(size, np.float64)
+        P, I = [], []
+        for f in faces:
+            b = len(P)
+            I += [b, b + 2, b + 1, b, b + 3, b + 2]
+            P += [tuple(np.asarray(v) * s) for v in f]
+        return _PysMesh(P, I, float(s[0] * s[1] * s[2]) < 0)
+
+    @staticmethod
+    def createSphere(radius=1.0, segmentsU=32, segmentsV=32):
+        P, I = [], []
+        for v in range(segmentsV + 1):
+            for u in range(segmentsU + 1):
+                th, ph = u / segmentsU * 2 * math.pi, v / segmentsV * math.pi
+                P.append((math.cos(th) * math.sin(ph) * radius, math.cos(ph) * radius, math.sin(th) * math.sin(ph) * radius))
+        for v in range(segmentsV):
+            for u in range(segmentsU):
+                i0, i1 = v * (segmentsU + 1) + u, v * (segmentsU + 1) + (u + 1) % (segmentsU + 1)
+                i2, i3 = (v + 1) * (segmentsU + 1) + u, (v + 1) * (segmentsU + 1) + (u + 1) % (segmentsU + 1)
+                I += [i0, i1, i2, i2, i1, i3]
+        return _PysMesh(P, I)
+
+
+class _PysMaterial:
+    def __init__(self, name="", model=0):
+        self.name = name
+        self.model = int(model)  # 0 MetalRough, 1 SpecGloss (ShadingModel)
+        self.baseColor = (1.0, 1.0, 1.0, 1.0)
+        self.specularParams = (0.0, 0.0, 0.0, 0.0)
+        self.emissiveColor = (0.0, 0.0, 0.0)
+        self.emissiveFactor = 1.0
+        self.indexOfRefraction = 1.5
+        self.doubleSided = False
+        self.specularTransmission = 0.0
+        self.diffuseTransmission = 0.0
+        self.thinSurface = False
+
+    roughness = property(lambda self: self.specularParams[1],
+                         lambda self, v: setattr(self, "specularParams", (self.specularParams[0], float(v)) + tuple(self.specularParams[2:])))
+    metallic = property(lambda self: self.specularParams[2],
+                        lambda self, v: setattr(self, "specularParams", tuple(self.specularParams[:2]) + (float(v), self.specularParams[3])))
+
+    def loadTexture(self, *a, **k):
+        raise ValueError("pyscene: textures are not read")
+
+    load_texture = setTexture = loadTexture
+
+    def row(self):
+        if self.specularTransmission > 0 or self.diffuseTransmission > 0:
+            warnings.warn(f"pyscene material {self.name!r}: transmission is not built; the pass shades it opaque")
+        em = tuple(float(c) * float(self.emissiveFactor) for c in self.emissiveColor[:3])
+        base = tuple(float(c) for c in self.baseColor[:3])
+        if self.model == 1:
+            return spec_gloss_material(base, tuple(self.specularParams[:3]), float(self.specularParams[3]), em, float(self.indexOfRefraction),
+                                       bool(self.doubleSided))
+        return material(base, float(self.specularParams[1]), em, float(self.specularParams[2]), float(self.indexOfRefraction), bool(self.doubleSided))
+
+
+class _PysCamera:
+    def __init__(self, name=""):
+        self.name = name
+        self.position, self.target, self.up = (0.0, 0.0, 0.0), (0.0, 0.0, -1.0), (0.0, 1.0, 0.0)
+        self.focalLength, self.frameHeight, self.aspectRatio = 21.0, 24.0, 1.7777777
+        self.focalDistance, self.apertureRadius, self.shutterSpeed = 10000.0, 0.0, 0.0
+        self.nearPlane, self.farPlane = 0.1, 1000.0
+
+
+class _PysLight:
+    kind = "point"
+
+    def __init__(self, name=""):
+        self.name = name
+        self.intensity = (1.0, 1.0, 1.0)
+        self.active = True
+        self.position = (0.0, 0.0, 0.0)
+        self.direction = (0.0, -1.0, 0.0)  # LightData.dirW's default
+        self.openingAngle = math.pi
+        self.penumbraAngle = 0.0
+        self.angle = 0.5 * 0.53 * math.pi / 180.0  # DistantLight's default: about the sun's half-angle
+        self.transform = None
+        self.scaling = (1.0, 1.0, 1.0)
+
+    def desc(self):
+        d = {"type": self.kind, "intensity": tuple(float(v) for v in self.intensity)}
+        if self.kind in ("point", "directional", "distant"):
+            d["direction"] = tuple(float(v) for v in self.direction)
+        if self.kind == "point":
+            d.update(position=tuple(float(v) for v in self.position), openingAngle=float(self.openingAngle),
+                     penumbraAngle=float(self.penumbraAngle))
+        if self.kind == "distant":
+            d["angle"] = float(self.angle)
+        if self.kind in ("rect", "disc", "sphere"):
+            T = self.transform
+            d["transform"] = np.eye(4) if T is None else (T.matrix if isinstance(T, _PysTransform) else np.asarray(T, np.float64))
+            d["scaling"] = tuple(float(v) for v in self.scaling)
+        return d
+
+
+def _pys_light_class(kind):
+    return type(f"_Pys_{kind}", (_PysLight,), {"kind": kind})
+
+
+def _pys_unsupported(what):
+    def f(*a, **k):
+        raise ValueError(f"pyscene: {what} is not supported by the pass")
+    return f
+
+
+class _PysSceneBuilder:
+    def __init__(self, base_dir):
+        self.base_dir = base_dir
+        self.meshes, self.nodes, self.instances = [], [], []
+        self.materials, self.lights, self.cameras = [], [], []
+
+    def addMaterial(self, m):
+        if m not in self.materials:
+            self.materials.append(m)
+        return m
+
+    def getMaterial(self, name):
+        return next((m for m in self.materials if m.name == name), None)
+
+    def addTriangleMesh(self, triangleMesh, material, isAnimated=False):
+        self.addMaterial(material)
+        self.meshes.append((triangleMesh, material))
+        return len(self.meshes) - 1
+
+    def addNode(self, name, transform=None, parent=None):
+        M = np.eye(4) if transform is None else (transform.matrix if isinstance(transform, _PysTransform) else np.asarray(transform, np.float64))
+        if parent is not None and parent >= 0:
+            M = self.nodes[parent] @ M
+        self.nodes.append(M)
+        return len(self.nodes) - 1
+
+    def addMeshInstance(self, nodeID, meshID):
+        self.instances.append((nodeID, meshID))
+
+    def addLight(self, light):
+        self.lights.append(light)
+        return len(self.lights) - 1
+
+    def getLight(self, name):
+        return next((l for l in self.lights if l.name == name), None)
+
+    def addCamera(self, camera):
+        self.cameras.append(camera)
+        return len(self.cameras) - 1
+
+    @property
+    def envMap(self):
+        return None
+
+    @envMap.setter
+    def envMap(self, value):
+        if value is not None:
+            raise ValueError("pyscene: environment maps from files are not read")
+
+    addSDFGrid = addSDFGridInstance = property(lambda self: _pys_unsupported("an SDF grid"))
+    addGridVolume = addVolume = property(lambda self: _pys_unsupported("a grid volume"))
+    addCustomPrimitive = property(lambda self: _pys_unsupported("a custom primitive"))
+    addAnimation = property(lambda self: _pys_unsupported("an animation"))
+    addCurve = property(lambda self: _pys_unsupported("a curve"))
+
+
+def load_pyscene(path) -> Scene:
+    """A Falcor .pyscene file as the pass's triangle soup; info holds "camera" (the first camera the
+    script adds, as Camera keyword arguments for pyscene_camera) and "lights" (its analytic lights)."""
+    path = Path(path)
+    sb = _PysSceneBuilder(path.parent)
+
+    def mesh_from_file(p, *a, **k):
+        p = Path(p)
+        p = p if p.is_absolute() else path.parent / p
+        if p.suffix.lower() != ".obj":
+            raise ValueError(f"pyscene: TriangleMesh.createFromFile reads OBJ files here, not {p.suffix}")
+        s = load_obj(p)
+        return _PysMesh(s.positions.reshape(-1, 3), list(range(len(s.positions) * 3)))
+
+    _PysMesh.createFromFile = staticmethod(mesh_from_file)
+    ns = {
+        "sceneBuilder": sb, "float2": _pys_vec(2), "float3": _pys_vec(3), "float4": _pys_vec(4), "Transform": _PysTransform,
+        "TriangleMesh": _PysMesh, "StandardMaterial": _PysMaterial, "Material": _PysMaterial,
+        "ShadingModel": type("ShadingModel", (), {"MetalRough": 0, "SpecGloss": 1}), "Camera": _PysCamera,
+        "PointLight": _pys_light_class("point"), "DirectionalLight": _pys_light_class("directional"),
+        "DistantLight": _pys_light_class("distant"), "RectLight": _pys_light_class("rect"), "DiscLight": _pys_light_class("disc"),
+        "SphereLight": _pys_light_class("sphere"), "EnvMap": _pys_unsupported("an environment map from a file"),
+        "SDFGrid": type("SDFGrid", (), {"__getattr__": lambda self, n: _pys_unsupported("an SDF grid")}),
+        "__file__": str(path), "__name__": "__pyscene__",
+    }
+    for n in ("createSBS", "createNDGrid", "createSVS", "createSVO"):
+        setattr(ns["SDFGrid"], n, staticmethod(_pys_unsupported("an SDF grid")))
+    exec(compile(path.read_text(), str(path), "exec"), ns)
+    rows = [m.row() for m in sb.materials]
+    tris, mids = [], []
+    for node, mesh_id in sb.instances:
+        mesh, mat = sb.meshes[mesh_id]
+        M = sb.nodes[node]
+        P = np.asarray(mesh.positions, np.float64).reshape(-1, 3)
+        W = P @ M[:3, :3].T + M[:3, 3]
+        flip = mesh.frontFaceCW != (np.linalg.det(M[:3, :3]) < 0)
+        I = np.asarray(mesh.indices, np.int64).reshape(-1, 3)
+        for a, b, c in I:
+            tris.append(np.concatenate([W[a], W[c], W[b]]) if flip else np.concatenate([W[a], W[b], W[c]]))
+            mids.append(sb.materials.index(mat))
+    if not tris:
+        raise ValueError(f"{path}: no triangle mesh instances")
+    info = {"triangles": len(tris), "materials": len(rows)}
+    if sb.cameras:
+        c = sb.cameras[0]
+        info["camera"] = {"position": tuple(c.position), "target": tuple(c.target), "up": tuple(c.up), "focal_length": float(c.focalLength),
+                          "frame_height": float(c.frameHeight), "aspect_ratio": float(c.aspectRatio), "focal_distance": float(c.focalDistance),
+                          "aperture_radius": float(c.apertureRadius), "shutter_speed": float(c.shutterSpeed), "near_z": float(c.nearPlane),
+                          "far_z": float(c.farPlane)}
+    lights = [l.desc() for l in sb.lights if getattr(l, "active", True)]
+    if lights:
+        info["lights"] = lights
+    return Scene(np.asarray(tris, np.float32), np.asarray(mids, np.uint32), np.stack(rows).astype(np.float32), path.stem, info)
+
+
+def pyscene_camera(scene: Scene, width: int, height: int):
+    """The pass camera of a load_pyscene scene (its first camera) at the image's aspect ratio."""
+    from .scenes import Camera
+    c = dict(scene.info["camera"])
+    c["aspect_ratio"] = width / height
+    return Camera(**c)

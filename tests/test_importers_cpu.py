@@ -247,3 +247,115 @@ def test_mitsuba_rejects_what_it_does_not_convert(rs, tmp_path):
         p.write_text(f'<scene version="3.0.0">{body}</scene>')
         with pytest.raises(ValueError):
             I.load_mitsuba(p)
+
+
+PYSCENE = """
+white = StandardMaterial('white')
+white.baseColor = float4(0.7, 0.7, 0.7, 1.0)
+white.roughness = 0.8
+light = StandardMaterial('light')
+light.emissiveColor = float3(1.0, 0.9, 0.8)
+light.emissiveFactor = 10.0
+metal = Material('metal')
+metal.specularParams = float4(0.0, 0.3, 1.0, 0.0)
+plain = StandardMaterial('plain')
+
+floor = sceneBuilder.addTriangleMesh(TriangleMesh.createQuad(), white)
+lamp = sceneBuilder.addTriangleMesh(TriangleMesh.createQuad(float2(0.25)), light)
+box = sceneBuilder.addTriangleMesh(TriangleMesh.createCube(float3(0.3)), metal)
+ball = sceneBuilder.addTriangleMesh(TriangleMesh.createSphere(0.2, 16, 8), plain)
+disk = sceneBuilder.addTriangleMesh(TriangleMesh.createDisk(0.5, 12), white)
+
+t = Transform(); t.scaling = float3(2.0, 1.0, 2.0)
+sceneBuilder.addMeshInstance(sceneBuilder.addNode('floor', t), floor)
+t = Transform(); t.translation = float3(0.0, 1.0, 0.0); t.rotationEulerDeg = float3(180.0, 0.0, 0.0)
+sceneBuilder.addMeshInstance(sceneBuilder.addNode('lamp', t), lamp)
+g = Transform(); g.translation = float3(0.0, 0.0, -0.5)
+root = sceneBuilder.addNode('group', g)
+t = Transform(); t.translation = float3(0.3, 0.15, 0.0)
+sceneBuilder.addMeshInstance(sceneBuilder.addNode('box', t, root), box)
+t = Transform(); t.translation = float3(-0.3, 0.2, 0.0); t.scaling = float3(-1.0, 1.0, 1.0)
+sceneBuilder.addMeshInstance(sceneBuilder.addNode('ball', t, root), ball)
+t = Transform(); t.lookAt(float3(0.0, 0.5, 0.9), float3(1.0, 0.5, 0.9), float3(0.0, 1.0, 0.0))
+sceneBuilder.addMeshInstance(sceneBuilder.addNode('wall', t), disk)
+
+spot = PointLight('spot')
+spot.position = float3(0.0, 0.9, 0.0)
+spot.openingAngle = 0.6
+spot.intensity = float3(2.0, 2.0, 2.0)
+sceneBuilder.addLight(spot)
+sun = DistantLight('sun')
+sun.direction = float3(0.2, -1.0, 0.1)
+sceneBuilder.addLight(sun)
+off = DirectionalLight('off')
+off.active = False
+sceneBuilder.addLight(off)
+
+camera = Camera()
+camera.position = float3(0.0, 0.5, 2.5)
+camera.target = float3(0.0, 0.4, 0.0)
+camera.focalLength = 30.0
+sceneBuilder.addCamera(camera)
+"""
+
+
+def test_pyscene_scene(rs, tmp_path):
+    """A Falcor Python scene (PythonImporter): TriangleMesh generators with Falcor's layouts, node
+    hierarchies, Transform (T x R x S, Euler degrees, lookAt), a mirrored instance, StandardMaterial
+    parameters and defaults, analytic lights and the camera."""
+    import reservoir_splatting_b200.importers as I
+    p = tmp_path / "room.pyscene"
+    p.write_text(PYSCENE)
+    sc = I.load_pyscene(p)
+    # quad 2 + quad 2 + cube 12 + sphere 16 x 8 x 2 + disk 12
+    assert sc.positions.shape == (2 + 2 + 12 + 256 + 12, 9)
+    t = sc.positions.reshape(-1, 3, 3).astype(np.float64)
+    n = np.cross(t[:, 1] - t[:, 0], t[:, 2] - t[:, 0])
+    assert np.all(n[0:2, 1] > 0) and np.all(n[2:4, 1] < 0)  # createQuad faces +y; the lamp is turned over
+    assert np.allclose(np.abs(t[0:2, :, [0, 2]]).max(), 1.0)  # scaled by 2 in x and z
+    assert np.allclose(t[2:4, :, 1], 1.0)
+    box = t[4:16].reshape(-1, 3)
+    assert np.allclose(box.min(0), [0.15, 0.0, -0.65]) and np.allclose(box.max(0), [0.45, 0.3, -0.35])  # parent and child
+    cb = box.mean(0)
+    assert np.all(np.einsum("ij,ij->i", n[4:16], t[4:16].mean(1) - cb) > 0)  # the cube's faces point out
+    ball = t[16:272]
+    centre = np.array([-0.3, 0.2, -0.5])
+    assert np.allclose(np.linalg.norm(ball.reshape(-1, 3) - centre, axis=1), 0.2, atol=1e-6)
+    outward = np.einsum("ij,ij->i", n[16:272], ball.mean(1) - centre)
+    big = np.linalg.norm(n[16:272], axis=1) > 1e-9
+    # the sphere's own winding faces outward; mirroring keeps it outward (Falcor flips the normal of
+    # a mirrored instance)
+    assert np.all(outward[big] > 0) or np.all(outward[big] < 0)
+    p2 = tmp_path / "room2.pyscene"
+    p2.write_text(PYSCENE.replace("t.scaling = float3(-1.0, 1.0, 1.0)", ""))
+    n2 = (lambda tt: np.cross(tt[:, 1] - tt[:, 0], tt[:, 2] - tt[:, 0]))(I.load_pyscene(p2).positions.reshape(-1, 3, 3).astype(np.float64))
+    out2 = np.einsum("ij,ij->i", n2[16:272], I.load_pyscene(p2).positions.reshape(-1, 3, 3)[16:272].mean(1) - centre)
+    assert np.all(np.sign(outward[big]) == np.sign(out2[big]))
+    disk = t[272:]
+    # lookAt toward +x: columns (right, up, -dir) = (+z, +y, -x), so the disk stays level at y = 0.5
+    # and its first rim vertex, object (r, 0, 0), lands at position + r * right
+    assert np.allclose(disk[:, :, 1], 0.5, atol=1e-6) and np.all(n[272:, 1] > 0)
+    assert np.allclose(disk[0, 1], [0.0, 0.5, 1.4], atol=1e-6)
+    m = sc.materials
+    white, light, metal, plain = m[0], m[1], m[2], m[3]
+    assert np.allclose(white[:3], 0.7) and abs(white[3] - 0.8) < 1e-6
+    assert np.allclose(light[4:7], [10.0, 9.0, 8.0]) and np.allclose(metal[[3, 7]], [0.3, 1.0])
+    assert np.allclose(plain[:3], 1.0) and plain[3] == 0.0 and abs(plain[8] - 1.5) < 1e-6  # BasicMaterial defaults
+    lights = sc.info["lights"]
+    assert [l["type"] for l in lights] == ["point", "distant"]  # the inactive light is dropped
+    assert lights[0]["openingAngle"] == 0.6 and np.allclose(lights[1]["direction"], [0.2, -1.0, 0.1])
+    assert abs(lights[1]["angle"] - 0.5 * 0.53 * np.pi / 180.0) < 1e-9
+    cam = I.pyscene_camera(sc, 64, 48)
+    assert cam.focal_length == 30.0 and cam.frame_height == 24.0 and np.allclose(cam.position, [0.0, 0.5, 2.5])
+
+
+def test_pyscene_rejects_what_it_does_not_convert(rs, tmp_path):
+    import reservoir_splatting_b200.importers as I
+    for body in ("g = SDFGrid.createSBS()", "sceneBuilder.envMap = EnvMap('sky.exr')",
+                 "m = StandardMaterial('t')\nm.loadTexture(0, 'albedo.png')",
+                 "m = StandardMaterial('t')\nsceneBuilder.addTriangleMesh(TriangleMesh.createFromFile('mesh.fbx'), m)",
+                 "x = 1"):
+        p = tmp_path / "bad.pyscene"
+        p.write_text(body + "\n")
+        with pytest.raises(ValueError):
+            I.load_pyscene(p)

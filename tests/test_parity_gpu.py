@@ -107,6 +107,26 @@ def test_uniform_emissive_sampler(rs, oracle_mod, scenes, mode):
 
 
 @pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
+def test_imported_pyscene(rs, oracle_mod, scenes, tmp_path):
+    """A Falcor .pyscene (generated meshes, a node hierarchy, an emissive quad, a spot and a distant
+    light) imported and rendered with its analytic lights, on the GPU as in the oracle."""
+    import dataclasses
+    import reservoir_splatting_b200.importers as I
+    from test_importers_cpu import PYSCENE
+    path = tmp_path / "room.pyscene"
+    path.write_text(PYSCENE)
+    sc = I.load_pyscene(path)
+
+    def cam(f, w, h):
+        c = I.pyscene_camera(sc, w, h)
+        return dataclasses.replace(c, position=(c.position[0] + 0.01 * f, c.position[1], c.position[2]))
+    props = {"temporalReuse": "ScatterBackup", "gatherOption": "Clamped", "maxSurfaceBounces": 2, "enableSpatialResampling": True}
+    report, img = run_pair(rs, oracle_mod, sc, cam, props, frames=4, width=48, height=36,
+                           setup=lambda p: p.set_analytic_lights(sc.info["lights"]))
+    assert np.nanmax(img[..., :3]) > 0.0
+
+
+@pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
 @pytest.mark.parametrize("mode", ["ScatterBackup", "GatherOnly"])
 def test_imported_obj_spec_gloss_scene(rs, oracle_mod, scenes, tmp_path, mode):
     """A Cornell box written as OBJ + MTL and imported with the Assimp importer's OBJ mapping:
