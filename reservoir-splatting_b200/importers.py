@@ -604,7 +604,8 @@ def pbrt_camera(scene: Scene, width: int, height: int):
 # roughconductor (metallic, base = the normal-incidence Fresnel reflectance of rgb eta, k; copper
 # without them; roughness sqrt(alpha)), dielectric / roughdielectric / thindielectric (IoR only: no
 # transmission lobe), twosided (its nested BSDF); shapes obj, ply, rectangle, cube, sphere; area
-# emitters nested in shapes, constant emitters as an env map (point, spot, projector and directional
+# emitters nested in shapes, constant emitters as an env map, envmap emitters from .hdr / .pfm images
+# (point, spot, projector and directional
 # emitters are skipped with a warning: the reference importer converts none of them); a perspective sensor.  <default> and
 # $name substitution, refs by id, and to_world transforms (translate, scale, rotate, matrix, lookat).
 # Image environment maps, textures and other plugins are rejected with a message.
@@ -646,7 +647,8 @@ def _mi_transform(el):
 
 
 def load_mitsuba(path) -> Scene:
-    """A Mitsuba 3 scene XML as the pass's triangle soup; info holds "camera" and "env" like load_pbrt."""
+    """A Mitsuba 3 scene XML as the pass's triangle soup; info holds "camera" and "env" like load_pbrt,
+    and "env_params" (intensity, tint, rotation for rs_set_env_map) with an envmap emitter."""
     import xml.etree.ElementTree as ET
     path = Path(path)
     text = path.read_text()
@@ -706,7 +708,7 @@ def load_mitsuba(path) -> Scene:
         raise ValueError(f"Mitsuba BSDF {t!r} is not converted")
 
     tris, mids, rows, index = [], [], [], {}
-    camera, env = None, None
+    camera, env, env_params = None, None, None
 
     def material_id(mat, emission):
         base, rough, metal, eta = mat
@@ -729,6 +731,17 @@ def load_mitsuba(path) -> Scene:
             t, p = el.attrib["type"], props(el)
             if t == "constant":
                 env = np.broadcast_to(np.asarray(p.get("radiance", (1.0,) * 3), np.float32), (8, 16, 3)).astype(np.float32).copy()
+            elif t == "envmap":
+                # MitsubaImporter.cpp:686-701: the image, intensity = scale, and the rotation as the XYZ
+                # Euler angles (extractEulerAngleXYZ, MatrixMath.h:331-342) of to_world x flipZ
+                env = read_env_image(path.parent / str(p["filename"]))
+                m = np.asarray(p.get("to_world", np.eye(4)), np.float64) @ np.diag([1.0, 1.0, -1.0, 1.0])
+                t1 = math.atan2(m[1][2], m[2][2])
+                t2 = math.atan2(-m[0][2], math.sqrt(m[0][0] * m[0][0] + m[0][1] * m[0][1]))
+                s1, c1 = math.sin(t1), math.cos(t1)
+                t3 = math.atan2(s1 * m[2][0] - c1 * m[1][0], c1 * m[1][1] - s1 * m[2][1])
+                env_params = {"intensity": float(p.get("scale", 1.0)), "tint": (1.0, 1.0, 1.0),
+                              "rotation": tuple(math.degrees(-a) for a in (t1, t2, t3))}
             elif t in ("point", "spot", "projector", "directional", "directionalarea"):
                 # MitsubaImporter.cpp:703-721 converts none of these (unsupportedType, a warning)
                 warnings.warn(f"Mitsuba emitter type {t!r} is not supported")
@@ -777,6 +790,8 @@ def load_mitsuba(path) -> Scene:
         info["camera"] = camera
     if env is not None:
         info["env"] = env
+    if env_params is not None:
+        info["env_params"] = env_params
     return Scene(np.asarray(tris, np.float32), np.asarray(mids, np.uint32), np.stack(rows).astype(np.float32), path.stem, info)
 
 
@@ -799,11 +814,13 @@ def load_mitsuba(path) -> Scene:
 #   * Camera (Scene/Camera/Camera.cpp:426-440, CameraData.slang defaults);
 #   * PointLight, DirectionalLight, DistantLight, RectLight, DiscLight, SphereLight (Scene/Lights/
 #     Light.cpp:404-440) as analytic lights (info["lights"], for rs_set_analytic_lights);
+#   * EnvMap (Scene/Lights/EnvMap.cpp:140-157) from .hdr or .pfm images, with rotation, intensity and
+#     tint (info["env"], info["env_params"], for rs_set_env_map);
 #   * sceneBuilder: addTriangleMesh, addMaterial, getMaterial, addNode (with parents), addMeshInstance,
-#     addLight, getLight, addCamera.
+#     addLight, getLight, addCamera, envMap.
 # Meshes are flattened to world space per instance; the winding is flipped when the mesh's front face
 # is clockwise or the instance transform mirrors, as Falcor flips the face normal then.  Textures,
-# environment maps from files, SDF grids, volumes, curves and animations raise ValueError.
+# environment images other than .hdr / .pfm, SDF grids, volumes, curves and animations raise ValueError.
 
 def _pys_vec(n):
     def make(*a):
@@ -995,6 +1012,24 @@ class _PysLight:
         return d
 
 
+class _PysEnvMap:
+    """EnvMap (Scene/Lights/EnvMap.cpp:140-157): a lat-long image with rotation (degrees), intensity
+    and tint; read from .hdr or .pfm files here."""
+    base_dir = Path(".")
+
+    def __init__(self, path):
+        p = Path(path)
+        self.path = str(p)
+        self.texels = read_env_image(p if p.is_absolute() else self.base_dir / p)
+        self.rotation = (0.0, 0.0, 0.0)
+        self.intensity = 1.0
+        self.tint = (1.0, 1.0, 1.0)
+
+    @classmethod
+    def createFromFile(cls, path):
+        return cls(path)
+
+
 def _pys_light_class(kind):
     return type(f"_Pys_{kind}", (_PysLight,), {"kind": kind})
 
@@ -1010,6 +1045,7 @@ class _PysSceneBuilder:
         self.base_dir = base_dir
         self.meshes, self.nodes, self.instances = [], [], []
         self.materials, self.lights, self.cameras = [], [], []
+        self.env = None
 
     def addMaterial(self, m):
         if m not in self.materials:
@@ -1047,12 +1083,11 @@ class _PysSceneBuilder:
 
     @property
     def envMap(self):
-        return None
+        return self.env
 
     @envMap.setter
     def envMap(self, value):
-        if value is not None:
-            raise ValueError("pyscene: environment maps from files are not read")
+        self.env = value
 
     addSDFGrid = addSDFGridInstance = property(lambda self: _pys_unsupported("an SDF grid"))
     addGridVolume = addVolume = property(lambda self: _pys_unsupported("a grid volume"))
@@ -1063,7 +1098,8 @@ class _PysSceneBuilder:
 
 def load_pyscene(path) -> Scene:
     """A Falcor .pyscene file as the pass's triangle soup; info holds "camera" (the first camera the
-    script adds, as Camera keyword arguments for pyscene_camera) and "lights" (its analytic lights)."""
+    script adds, as Camera keyword arguments for pyscene_camera), "lights" (its analytic lights) and
+    "env" / "env_params" (its environment map and the map's intensity, tint and rotation)."""
     path = Path(path)
     sb = _PysSceneBuilder(path.parent)
 
@@ -1082,7 +1118,7 @@ def load_pyscene(path) -> Scene:
         "ShadingModel": type("ShadingModel", (), {"MetalRough": 0, "SpecGloss": 1}), "Camera": _PysCamera,
         "PointLight": _pys_light_class("point"), "DirectionalLight": _pys_light_class("directional"),
         "DistantLight": _pys_light_class("distant"), "RectLight": _pys_light_class("rect"), "DiscLight": _pys_light_class("disc"),
-        "SphereLight": _pys_light_class("sphere"), "EnvMap": _pys_unsupported("an environment map from a file"),
+        "SphereLight": _pys_light_class("sphere"), "EnvMap": type("EnvMap", (_PysEnvMap,), {"base_dir": path.parent}),
         "SDFGrid": type("SDFGrid", (), {"__getattr__": lambda self, n: _pys_unsupported("an SDF grid")}),
         "__file__": str(path), "__name__": "__pyscene__",
     }
@@ -1113,6 +1149,10 @@ def load_pyscene(path) -> Scene:
     lights = [l.desc() for l in sb.lights if getattr(l, "active", True)]
     if lights:
         info["lights"] = lights
+    if sb.env is not None:
+        info["env"] = sb.env.texels
+        info["env_params"] = {"intensity": float(sb.env.intensity), "tint": tuple(float(v) for v in sb.env.tint),
+                              "rotation": tuple(float(v) for v in sb.env.rotation)}
     return Scene(np.asarray(tris, np.float32), np.asarray(mids, np.uint32), np.stack(rows).astype(np.float32), path.stem, info)
 
 
@@ -1122,3 +1162,86 @@ def pyscene_camera(scene: Scene, width: int, height: int):
     c = dict(scene.info["camera"])
     c["aspect_ratio"] = width / height
     return Camera(**c)
+
+
+# ---------------------------------------------------------------- HDR images for environment maps
+# Latitude-longitude environment maps from Radiance .hdr (RGBE, flat or run-length encoded
+# scanlines) and Portable Float Map .pfm files, as float32 [H, W, 3] with row 0 at the top (the
+# layout rs_set_env_map reads).  OpenEXR and other formats are not decoded.
+
+def _read_hdr(path: Path) -> np.ndarray:
+    data = path.read_bytes()
+    pos = 0
+
+    def line():
+        nonlocal pos
+        end = data.index(b"\n", pos)
+        s = data[pos:end].decode("ascii", "replace")
+        pos = end + 1
+        return s
+
+    if not line().startswith("#?"):
+        raise ValueError(f"{path}: not a Radiance HDR file")
+    while True:
+        s = line()
+        if s == "":
+            break
+        if s.startswith("FORMAT=") and s != "FORMAT=32-bit_rle_rgbe":
+            raise ValueError(f"{path}: {s} is not read (only 32-bit_rle_rgbe)")
+    res = line().split()
+    if len(res) != 4 or res[0] != "-Y" or res[2] != "+X":
+        raise ValueError(f"{path}: resolution line {' '.join(res)!r} is not read (only -Y H +X W)")
+    h, w = int(res[1]), int(res[3])
+    rgbe = np.zeros((h, w, 4), np.uint8)
+    buf = np.frombuffer(data, np.uint8)
+    for y in range(h):
+        if 8 <= w < 32768 and buf[pos] == 2 and buf[pos + 1] == 2 and (int(buf[pos + 2]) << 8 | int(buf[pos + 3])) == w:
+            pos += 4
+            for c in range(4):  # each channel run-length encoded on its own
+                x = 0
+                while x < w:
+                    n = int(buf[pos]); pos += 1
+                    if n > 128:
+                        n -= 128
+                        rgbe[y, x:x + n, c] = buf[pos]; pos += 1
+                    else:
+                        rgbe[y, x:x + n, c] = buf[pos:pos + n]; pos += n
+                    x += n
+        else:
+            rgbe[y] = buf[pos:pos + 4 * w].reshape(w, 4)
+            pos += 4 * w
+    e = rgbe[..., 3].astype(np.int32)
+    scale = np.where(e > 0, np.ldexp(1.0, e - 136), 0.0).astype(np.float32)
+    return rgbe[..., :3].astype(np.float32) * scale[..., None]
+
+
+def _read_pfm(path: Path) -> np.ndarray:
+    data = path.read_bytes()
+    parts, pos = [], 0
+    while len(parts) < 4:  # "PF" | "Pf", width, height, scale (negative: little endian)
+        while data[pos:pos + 1].isspace():
+            pos += 1
+        end = pos
+        while not data[end:end + 1].isspace():
+            end += 1
+        parts.append(data[pos:end].decode("ascii"))
+        pos = end
+    pos += 1
+    kind, w, h, scale = parts[0], int(parts[1]), int(parts[2]), float(parts[3])
+    if kind not in ("PF", "Pf"):
+        raise ValueError(f"{path}: not a PFM file")
+    ch = 3 if kind == "PF" else 1
+    img = np.frombuffer(data, "<f4" if scale < 0 else ">f4", count=w * h * ch, offset=pos).reshape(h, w, ch)
+    img = img[::-1].astype(np.float32)  # PFM rows run bottom to top
+    return np.repeat(img, 3, axis=2) if ch == 1 else img
+
+
+def read_env_image(path) -> np.ndarray:
+    """A lat-long environment image (.hdr or .pfm) as float32 [H, W, 3], row 0 at the top."""
+    path = Path(path)
+    ext = path.suffix.lower()
+    if ext == ".hdr":
+        return _read_hdr(path)
+    if ext == ".pfm":
+        return _read_pfm(path)
+    raise ValueError(f"{path}: environment images are read from .hdr or .pfm files, not {ext}")

@@ -359,3 +359,77 @@ def test_pyscene_rejects_what_it_does_not_convert(rs, tmp_path):
         p.write_text(body + "\n")
         with pytest.raises(ValueError):
             I.load_pyscene(p)
+
+
+def _rgbe(img):
+    """float [H, W, 3] -> RGBE bytes (mantissa = c * 2^(136 - e), the exponent of the largest channel)."""
+    mx = img.max(-1)
+    e = np.where(mx > 1e-32, np.floor(np.log2(np.maximum(mx, 1e-32))) + 1 + 128, 0).astype(np.int32)
+    m = np.where(e[..., None] > 0, img * np.ldexp(1.0, 136 - e)[..., None], 0)
+    return np.concatenate([np.clip(np.floor(m), 0, 255), e[..., None]], -1).astype(np.uint8)
+
+
+def _write_hdr(path, img, rle):
+    h, w = img.shape[:2]
+    px = _rgbe(img)
+    out = bytearray(b"#?RADIANCE\nFORMAT=32-bit_rle_rgbe\n\n" + f"-Y {h} +X {w}\n".encode())
+    for y in range(h):
+        if not rle:
+            out += px[y].tobytes()
+            continue
+        out += bytes([2, 2, w >> 8, w & 255])
+        for c in range(4):
+            row, x = px[y, :, c], 0
+            while x < w:
+                n = 1
+                while x + n < w and n < 127 and row[x + n] == row[x]:
+                    n += 1
+                if n >= 3:
+                    out += bytes([128 + n, row[x]])
+                else:
+                    n = min(128, w - x)
+                    out += bytes([n]) + row[x:x + n].tobytes()
+                x += n
+    path.write_bytes(bytes(out))
+    e = px[..., 3].astype(np.int32)
+    return np.where(e[..., None] > 0, px[..., :3] * np.ldexp(1.0, e - 136)[..., None], 0.0).astype(np.float32)
+
+
+@pytest.mark.parametrize("rle", [False, True], ids=["flat", "rle"])
+def test_hdr_and_pfm_environment_images(rs, tmp_path, rle):
+    import reservoir_splatting_b200.importers as I
+    rng = np.random.default_rng(1)
+    img = (rng.uniform(0, 4, (6, 40, 3)) ** 2).astype(np.float32)
+    img[2] = 1.5  # long runs of one value
+    img[3, :5] = 0.0
+    want = _write_hdr(tmp_path / "sky.hdr", img, rle)
+    got = I.read_env_image(tmp_path / "sky.hdr")
+    assert got.shape == (6, 40, 3) and np.array_equal(got, want)
+    assert np.all(np.abs(got - img) <= img.max(-1, keepdims=True) / 64)  # 8-bit mantissas on the largest channel's exponent
+    for scale, dt in ((-1.0, "<f4"), (1.0, ">f4")):
+        body = np.ascontiguousarray(img[::-1]).astype(dt).tobytes()  # rows bottom to top
+        (tmp_path / "sky.pfm").write_bytes(f"PF\n40 6\n{scale}\n".encode() + body)
+        assert np.array_equal(I.read_env_image(tmp_path / "sky.pfm"), img)
+    with pytest.raises(ValueError):
+        I.read_env_image(tmp_path / "sky.exr")
+
+
+def test_environment_maps_from_mitsuba_and_pyscene(rs, tmp_path):
+    """Mitsuba envmap (MitsubaImporter.cpp:686-701: intensity = scale, rotation = the XYZ Euler angles
+    of to_world x flipZ) and a pyscene EnvMap (rotation, intensity, tint)."""
+    import reservoir_splatting_b200.importers as I
+    img = np.full((4, 8, 3), 0.5, np.float32)
+    _write_hdr(tmp_path / "sky.hdr", img, False)
+    (tmp_path / "env.xml").write_text('<scene version="3.0.0"><emitter type="envmap"><string name="filename" value="sky.hdr"/>'
+                                      '<float name="scale" value="2.5"/></emitter><shape type="rectangle"/></scene>')
+    sc = I.load_mitsuba(tmp_path / "env.xml")
+    assert np.allclose(sc.info["env"], 0.5) and sc.info["env_params"]["intensity"] == 2.5
+    # identity to_world: flipZ alone, whose XYZ Euler angles are (-180, 0, -180) degrees
+    assert np.allclose(sc.info["env_params"]["rotation"], (-180.0, 0.0, -180.0))
+    (tmp_path / "env.pyscene").write_text("e = EnvMap('sky.hdr')\ne.intensity = 3.0\ne.rotation = float3(0, 90, 0)\n"
+                                          "e.tint = float3(1, 0.5, 0.25)\nsceneBuilder.envMap = e\n"
+                                          "sceneBuilder.addMeshInstance(sceneBuilder.addNode('q'), "
+                                          "sceneBuilder.addTriangleMesh(TriangleMesh.createQuad(), StandardMaterial('m')))\n")
+    sc = I.load_pyscene(tmp_path / "env.pyscene")
+    assert sc.info["env"].shape == (4, 8, 3)
+    assert sc.info["env_params"] == {"intensity": 3.0, "tint": (1.0, 0.5, 0.25), "rotation": (0.0, 90.0, 0.0)}

@@ -127,6 +127,32 @@ def test_imported_pyscene(rs, oracle_mod, scenes, tmp_path):
 
 
 @pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
+def test_imported_pyscene_with_hdr_environment(rs, oracle_mod, scenes, tmp_path):
+    """The pyscene's EnvMap read from a Radiance .hdr image, with its intensity, tint and rotation
+    given to rs_set_env_map, on the GPU as in the oracle."""
+    import dataclasses
+    import reservoir_splatting_b200.importers as I
+    from test_importers_cpu import PYSCENE, _write_hdr
+    _write_hdr(tmp_path / "sky.hdr", scenes.sky_env_map(64, 32, seed=3), True)
+    path = tmp_path / "room.pyscene"
+    path.write_text(PYSCENE + "e = EnvMap('sky.hdr')\ne.intensity = 0.7\ne.rotation = float3(0, 40, 0)\ne.tint = float3(1, 0.9, 0.8)\n"
+                    "sceneBuilder.envMap = e\n")
+    sc = I.load_pyscene(path)
+    env, ep = sc.info["env"], sc.info["env_params"]
+
+    def setup(p):
+        p.set_env_map(env, ep["intensity"], ep["tint"], ep["rotation"])
+        p.set_analytic_lights(sc.info["lights"])
+
+    def cam(f, w, h):
+        c = I.pyscene_camera(sc, w, h)
+        return dataclasses.replace(c, position=(c.position[0] + 0.01 * f, c.position[1], c.position[2]))
+    props = {"temporalReuse": "ScatterBackup", "gatherOption": "Clamped", "maxSurfaceBounces": 2, "enableSpatialResampling": True}
+    report, img = run_pair(rs, oracle_mod, sc, cam, props, frames=3, width=40, height=30, setup=setup)
+    assert np.nanmax(img[..., :3]) > 0.0
+
+
+@pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
 @pytest.mark.parametrize("mode", ["ScatterBackup", "GatherOnly"])
 def test_imported_obj_spec_gloss_scene(rs, oracle_mod, scenes, tmp_path, mode):
     """A Cornell box written as OBJ + MTL and imported with the Assimp importer's OBJ mapping:
