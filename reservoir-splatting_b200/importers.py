@@ -153,12 +153,14 @@ def save_obj(scene: Scene, path, material_names=None, mtl_params=None):
 #     reflection remains); the scalar roughness is getRoughness (:424-462) as written: float2(u + v),
 #     square-rooted when remaproughness, and getScalarRoughness averages the two equal components;
 #   * AreaLightSource "diffuse" (L * scale emitted by the shapes that follow, twosided);
-#   * LightSource "infinite" with a constant "rgb L" (an environment map of that radiance);
+#   * LightSource "infinite" with a constant "rgb L" (an environment map of that radiance), or with an
+#     equal-area octahedral image (.hdr / .pfm here) converted to lat-long as the reference's
+#     EnvMapConverter does, with intensity = scale and the light transform's XYZ Euler rotation;
 #   * LightSource "distant" as a directional analytic light (createLight, PBRTImporter.cpp:676-699:
 #     intensity L * scale, times illuminance when it is positive; direction the transformed
 #     to - from); "point", "spot", "goniometric" and "projection" lights are skipped with a warning,
 #     as the reference importer does.
-# Textures, named spectra other than the defaults, image infinite lights, curves, disks and
+# Textures, named spectra other than the defaults, .exr images, curves, disks and
 # cylinders are not read.
 
 _PBRT_COPPER_F0 = (0.955, 0.638, 0.538)  # RGB normal-incidence reflectance used for the default conductor (metal-Cu)
@@ -399,7 +401,7 @@ def load_pbrt(path) -> Scene:
     state = {"ctm": np.eye(4), "material": ("diffuse", {}), "area": None, "reverse": False}
     stack, named, objects = [], {}, {}
     current_object = None
-    camera, env = None, None
+    camera, env, env_params = None, None, None
     lights = []
 
     def material_id(mat, area):
@@ -448,7 +450,7 @@ def load_pbrt(path) -> Scene:
         return P, faces
 
     def parse(file_path: Path):
-        nonlocal camera, env, current_object
+        nonlocal camera, env, env_params, current_object
         r = _PbrtReader(_pbrt_tokens(file_path.read_text()))
         base_dir = file_path.parent
         while r.more():
@@ -506,10 +508,17 @@ def load_pbrt(path) -> Scene:
                 ltype = r.next()[1:-1]
                 ps = r.params()
                 if ltype == "infinite":
+                    if "filename" in ps and "L" in ps:
+                        raise ValueError("PBRT infinite light: both L and filename")
                     if "filename" in ps:
-                        raise ValueError("PBRT image infinite lights (equal-area maps) are not converted")
-                    L = np.asarray(_pbrt_rgb(ps, "L", (1.0, 1.0, 1.0)), np.float32) * _pbrt_float(ps, "scale", 1.0)
-                    env = np.broadcast_to(L, (8, 16, 3)).astype(np.float32).copy()
+                        # createLight (PBRTImporter.cpp:722-737): the equal-area octahedral image to
+                        # lat-long, intensity = scale, rotation = XYZ Euler angles of the light's transform
+                        env = equal_area_oct_to_latlong(read_env_image(file_path.parent / ps["filename"][1][0]))
+                        env_params = {"intensity": _pbrt_float(ps, "scale", 1.0), "tint": (1.0, 1.0, 1.0),
+                                      "rotation": _euler_xyz_degrees(state["ctm"])}
+                    else:
+                        L = np.asarray(_pbrt_rgb(ps, "L", (1.0, 1.0, 1.0)), np.float32) * _pbrt_float(ps, "scale", 1.0)
+                        env = np.broadcast_to(L, (8, 16, 3)).astype(np.float32).copy()
                 elif ltype == "distant":
                     I = np.asarray(_pbrt_rgb(ps, "L", (1.0, 1.0, 1.0)), np.float64) * _pbrt_float(ps, "scale", 1.0)
                     illum = _pbrt_float(ps, "illuminance", -1.0)
@@ -580,6 +589,8 @@ def load_pbrt(path) -> Scene:
         info["env"] = env
     if lights:
         info["lights"] = lights
+    if env_params is not None:
+        info["env_params"] = env_params
     return Scene(np.asarray(tris, np.float32), np.asarray(mids, np.uint32), np.stack(mat_rows).astype(np.float32), path.stem, info)
 
 
@@ -1245,3 +1256,44 @@ def read_env_image(path) -> np.ndarray:
     if ext == ".pfm":
         return _read_pfm(path)
     raise ValueError(f"{path}: environment images are read from .hdr or .pfm files, not {ext}")
+
+
+def _euler_xyz_degrees(m) -> tuple:
+    """extractEulerAngleXYZ (Utils/Math/MatrixMath.h:331-342) of a row-major matrix, in degrees."""
+    t1 = math.atan2(m[1][2], m[2][2])
+    t2 = math.atan2(-m[0][2], math.sqrt(m[0][0] * m[0][0] + m[0][1] * m[0][1]))
+    s1, c1 = math.sin(t1), math.cos(t1)
+    t3 = math.atan2(s1 * m[2][0] - c1 * m[1][0], c1 * m[1][1] - s1 * m[2][1])
+    return tuple(math.degrees(-a) for a in (t1, t2, t3))
+
+
+def equal_area_oct_to_latlong(img: np.ndarray) -> np.ndarray:
+    """EnvMapConverter (PBRTImporter/EnvMapConverter.cs.slang, .h): a square equal-area octahedral map
+    [N, N, 3] to a lat-long map [N, 2N, 3]: per output texel centre its direction
+    (latlong_map_to_world, MathHelpers.slang:128-137), that direction's equal-area octahedral
+    coordinates (ndir_to_oct_equal_area_unorm, :213-230), and a bilinear, clamp-to-edge fetch."""
+    n = img.shape[0]
+    if img.shape[1] != n:
+        raise ValueError("an equal-area octahedral map is square")
+    h, w = n, 2 * n
+    u = (np.arange(w, dtype=np.float64) + 0.5) / w
+    v = (np.arange(h, dtype=np.float64) + 0.5) / h
+    phi = math.pi * (2.0 * u[None, :] - 1.0)
+    theta = math.pi * v[:, None]
+    dx, dy, dz = np.sin(theta) * np.sin(phi), np.cos(theta) * np.ones_like(phi), -np.sin(theta) * np.cos(phi)
+    r = np.sqrt(1.0 - np.abs(dz))
+    ang = np.arctan2(np.abs(dy), np.abs(dx))
+    py = r * ang * (2.0 / math.pi)
+    px = r - py
+    lower = dz < 0.0
+    px, py = np.where(lower, 1.0 - py, px), np.where(lower, 1.0 - px, py)
+    px, py = px * np.sign(dx), py * np.sign(dy)
+    ou, ov = px * 0.5 + 0.5, py * 0.5 + 0.5
+    fx, fy = ou * n - 0.5, ov * n - 0.5
+    x0, y0 = np.floor(fx).astype(np.int64), np.floor(fy).astype(np.int64)
+    ax, ay = (fx - x0)[..., None], (fy - y0)[..., None]
+    cl = lambda i: np.clip(i, 0, n - 1)
+    src = img.astype(np.float64)
+    top = src[cl(y0), cl(x0)] * (1 - ax) + src[cl(y0), cl(x0 + 1)] * ax
+    bot = src[cl(y0 + 1), cl(x0)] * (1 - ax) + src[cl(y0 + 1), cl(x0 + 1)] * ax
+    return (top * (1 - ay) + bot * ay).astype(np.float32)
