@@ -1110,7 +1110,8 @@ class _PysSceneBuilder:
 def load_pyscene(path) -> Scene:
     """A Falcor .pyscene file as the pass's triangle soup; info holds "camera" (the first camera the
     script adds, as Camera keyword arguments for pyscene_camera), "lights" (its analytic lights) and
-    "env" / "env_params" (its environment map and the map's intensity, tint and rotation)."""
+    "env" / "env_params" (its environment map and the map's intensity, tint and rotation).
+    The file runs as a Python script, as it does in Falcor: load only scene files you trust."""
     path = Path(path)
     sb = _PysSceneBuilder(path.parent)
 
@@ -1122,10 +1123,10 @@ def load_pyscene(path) -> Scene:
         s = load_obj(p)
         return _PysMesh(s.positions.reshape(-1, 3), list(range(len(s.positions) * 3)))
 
-    _PysMesh.createFromFile = staticmethod(mesh_from_file)
+    mesh_class = type("TriangleMesh", (_PysMesh,), {"createFromFile": staticmethod(mesh_from_file)})
     ns = {
         "sceneBuilder": sb, "float2": _pys_vec(2), "float3": _pys_vec(3), "float4": _pys_vec(4), "Transform": _PysTransform,
-        "TriangleMesh": _PysMesh, "StandardMaterial": _PysMaterial, "Material": _PysMaterial,
+        "TriangleMesh": mesh_class, "StandardMaterial": _PysMaterial, "Material": _PysMaterial,
         "ShadingModel": type("ShadingModel", (), {"MetalRough": 0, "SpecGloss": 1}), "Camera": _PysCamera,
         "PointLight": _pys_light_class("point"), "DirectionalLight": _pys_light_class("directional"),
         "DistantLight": _pys_light_class("distant"), "RectLight": _pys_light_class("rect"), "DiscLight": _pys_light_class("disc"),
