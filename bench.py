@@ -304,6 +304,12 @@ def run_ours(args):
             line["modes"] = run_modes(args, torch, rs, scene, stream)
         if world == 1 and not args.no_batched:
             line["batched"] = run_batched(args, torch, rs, stream, dev)
+            # beyond the configuration: all instances small (320 x 240, 10k-100k triangles), where one
+            # instance's launches do not fill the GPU and batching has launches and idle SMs to save
+            line["batched_small"] = run_batched(
+                args, torch, rs, stream, dev, with_quality=False,
+                insts=batch_instances(args.batch_instances, seed=12, resolutions=[(320, 240)], tri_range=(10_000, 100_000)),
+                how="; an added workload, not the configuration: every instance 320 x 240 with 10k-100k triangles")
         if world == 1 and not args.no_motion_blur:
             line["motion_blur"] = run_motion_blur(args, torch, rs, stream)
         if world == 1 and not args.no_adjoint:
@@ -426,17 +432,18 @@ def run_modes(args, torch, rs, scene, stream):
     return out
 
 
-def batch_instances(count: int, seed: int = 11):
-    """Seeded batched workload: resolutions uniform over BATCH_RESOLUTIONS, 10k-500k triangles each
-    from the same generator at subdivision 4 (about 60% terrain, the rest icospheres of 5,120
-    triangles, at least one)."""
+def batch_instances(count: int, seed: int = 11, resolutions=None, tri_range=(10_000, 500_000)):
+    """Seeded batched workload: resolutions uniform over `resolutions` (BATCH_RESOLUTIONS), triangles
+    uniform over `tri_range` (10k-500k) each from the same generator at subdivision 4 (about 60%
+    terrain, the rest icospheres of 5,120 triangles, at least one)."""
+    resolutions = resolutions or BATCH_RESOLUTIONS
     _package()
     import reservoir_splatting_b200.scenes as S
     rng = np.random.default_rng(seed)
     out = []
     for i in range(count):
-        w, h = BATCH_RESOLUTIONS[int(rng.integers(0, len(BATCH_RESOLUTIONS)))]
-        target = int(rng.uniform(10_000, 500_000))
+        w, h = resolutions[int(rng.integers(0, len(resolutions)))]
+        target = int(rng.uniform(*tri_range))
         grid = max(8, int((0.6 * target / 2) ** 0.5))
         spheres = max(1, int(0.4 * target / 5120))
         sc = S.terrain_spheres(seed=1000 + i, grid=grid, spheres=spheres, subdiv=4, lights=16)
@@ -449,7 +456,7 @@ def batch_instances(count: int, seed: int = 11):
 QUERIES_PER_PIXEL = 12.48
 
 
-def run_batched(args, torch, rs, stream, dev):
+def run_batched(args, torch, rs, stream, dev, insts=None, with_quality=True, how=""):
     """Config "batched": 64 seeded scene/camera instances of uneven resolution, ScatterBackup, 16 timed
     frames, in three forms over the same frames (every pass restarts its history before each form):
     plain (rs_execute per instance back to back on one stream), per-member graph branches
@@ -460,7 +467,7 @@ def run_batched(args, torch, rs, stream, dev):
     identical images (checked here on every instance's last frame), so their MSE is matched by
     construction; the MSE of the smallest and largest instance against an FP64 ground truth is
     reported as well."""
-    insts = batch_instances(args.batch_instances)
+    insts = insts or batch_instances(args.batch_instances)
     passes = [rs.ReservoirSplatting(PROPS, w, h) for _, w, h, _ in insts]
     for (sc, _, _, _), a in zip(insts, passes):
         a.set_scene(sc)
@@ -518,7 +525,7 @@ def run_batched(args, torch, rs, stream, dev):
     for p in passes:
         p.close()
     quality = {}
-    if not args.no_quality:  # the ground-truth passes need the batch's pass slots back
+    if with_quality and not args.no_quality:  # the ground-truth passes need the batch's pass slots back
         order = sorted(range(n), key=lambda i: insts[i][1] * insts[i][2])
         for k in (order[0], order[-1]):
             sc, w, h, i = insts[k]
@@ -526,7 +533,7 @@ def run_batched(args, torch, rs, stream, dev):
                                 stream, spp=args.mode_gt_spp)
             quality[f"instance{k}_{w}x{h}"] = {kk: q[kk] for kk in ("mse_vs_fp64_gt", "mse_1spp_path_tracing", "gt_spp")}
     res = {"instances": n, "frames": frames, "warmup_frames": warm, "pixels_per_batch_frame": pixels,
-           "resolutions": {f"{w}x{h}": sum(1 for _, ww, hh, _ in insts if (ww, hh) == (w, h)) for w, h in BATCH_RESOLUTIONS},
+           "resolutions": {f"{w}x{h}": sum(1 for _, ww, hh, _ in insts if (ww, hh) == (w, h)) for w, h in sorted({(w, h) for _, w, h, _ in insts})},
            "triangles_min": min(tris), "triangles_max": max(tris),
            "plain_instance_frames_per_s": round(rate(ms_plain), 3),
            "branch_graph_instance_frames_per_s": round(rate(ms_branch), 3),
@@ -545,7 +552,7 @@ def run_batched(args, torch, rs, stream, dev):
            "quality": quality,
            "how": "16 timed frames after warm-up per form on the same passes restarted before each form; flattened = one launch per "
                   "stage over a work queue of all 64 instances (persistent kb_* kernels), tiles/grid forms from rs_batch_tune on the last "
-                  "warm-up frame; queries/s = 12.48 ray queries per pixel (counted for this mode) x pixels / time"}
+                  "warm-up frame; queries/s = 12.48 ray queries per pixel (counted for this mode) x pixels / time" + how}
     return res
 
 
