@@ -107,6 +107,29 @@ def test_uniform_emissive_sampler(rs, oracle_mod, scenes, mode):
 
 
 @pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
+@pytest.mark.parametrize("spp", [2, 5, 16])
+@pytest.mark.parametrize("lights", ["emissive", "env+analytic", "uniform"])
+def test_several_samples_per_pixel(rs, oracle_mod, scenes, spp, lights):
+    """samplesPerPixel > 1 (InitialCandidates.cs.slang:80-141: the pixel's paths stream into one
+    candidate reservoir; k_candidates, one thread per pixel) up to the maximum of 16, with each light
+    configuration the path tracer is compiled for."""
+    props = {"temporalReuse": "ScatterBackup", "gatherOption": "Clamped", "maxSurfaceBounces": 2, "enableSpatialResampling": True,
+             "samplesPerPixel": spp}
+    if lights == "uniform":
+        props["emissiveSampler"] = "Uniform"
+    sky = scenes.sky_env_map(64, 32, seed=5)
+    spot = {"type": "point", "position": (0.5, 0.9, 0.5), "direction": (0.0, -1.0, 0.0), "intensity": (1.0, 1.0, 1.0),
+            "openingAngle": 0.7, "penumbraAngle": 0.2}
+
+    def setup(p):
+        if lights == "env+analytic":
+            p.set_env_map(sky, 0.8)
+            p.set_analytic_lights([spot])
+    report, img = run_pair(rs, oracle_mod, scenes.cornell_box(0), scenes.cornell_camera, props, frames=3, width=32, height=24, setup=setup)
+    assert np.nanmax(img[..., :3]) > 0.0
+
+
+@pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
 def test_imported_pyscene(rs, oracle_mod, scenes, tmp_path):
     """A Falcor .pyscene (generated meshes, a node hierarchy, an emissive quad, a spot and a distant
     light) imported and rendered with its analytic lights, on the GPU as in the oracle."""
