@@ -106,6 +106,52 @@ def test_uniform_emissive_sampler(rs, oracle_mod, scenes, mode):
     assert np.isfinite(img).all() and img[..., :3].mean() > 0.0
 
 
+OPTION_CASES = [
+    ("numSpatialIterations=3", {"numSpatialIterations": 3}),
+    ("spatialGatherRadius=5", {"spatialGatherRadius": 5.0, "neighborCount": 3}),
+    ("noConfidenceTemporal", {"useConfidenceWeightsTemporally": False}),
+    ("noConfidenceSpatial", {"useConfidenceWeightsSpatially": False, "neighborCount": 2}),
+    ("noRussianRoulette", {"useRussianRoulette": False}),
+    ("disableCaustics", {"disableCaustics": True, "maxSurfaceBounces": 3}),
+    ("specularRoughnessThreshold=0.6", {"specularRoughnessThreshold": 0.6, "maxSpecularBounces": 1}),
+    ("maxDiffuseBounces=1", {"maxSurfaceBounces": 3, "maxDiffuseBounces": 1}),
+    ("maxSpecularBounces=0", {"maxSurfaceBounces": 3, "maxSpecularBounces": 0}),
+]
+
+
+def _glossy_cornell(scenes):
+    """The Cornell box with a mirror-like tall box (metallic, roughness 0.05) and a glossy short box
+    (roughness 0.3): specular vertices for the caustics and roughness-threshold options."""
+    sc = scenes.cornell_box(0)
+    mats = np.concatenate([sc.materials, scenes.material((0.9, 0.8, 0.6), roughness=0.05, metallic=1.0)[None],
+                           scenes.material((0.5, 0.6, 0.7), roughness=0.3)[None]]).astype(np.float32)
+    mids = sc.material_ids.copy()
+    mids[22:34] = len(mats) - 2  # the tall box (triangles 22-33: the second box)
+    mids[10:22] = len(mats) - 1  # the short box
+    return scenes.Scene(sc.positions, mids, mats, "cornell_glossy")
+
+
+@pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
+@pytest.mark.parametrize("mode", ["ScatterBackup", "GatherOnly"])
+@pytest.mark.parametrize("name,extra", OPTION_CASES, ids=[c[0] for c in OPTION_CASES])
+def test_option_values(rs, oracle_mod, scenes, mode, name, extra):
+    """Each option of ReservoirSplatting.h:124-184 at a non-default value, on a scene with specular
+    surfaces, against the oracle."""
+    base = {"temporalReuse": mode, "gatherOption": "Clamped", "maxSurfaceBounces": 2, "enableSpatialResampling": True}
+    props = dict(base, **extra)
+    sc = _glossy_cornell(scenes)
+    report, img = run_pair(rs, oracle_mod, sc, scenes.cornell_camera, props, frames=4, width=40, height=32)
+    assert np.isfinite(img).all() and img[..., :3].mean() > 0.0
+    # the option takes effect: without it (the companion settings kept) the frames differ
+    companion = {k: v for k, v in extra.items() if k in ("maxSurfaceBounces", "neighborCount")}
+    other = rs.ReservoirSplatting(dict(base, **companion), 40, 32)
+    other.set_scene(sc)
+    for f in range(4):
+        ref = other.render(scenes.cornell_camera(f, 40, 32))
+    other.close()
+    assert not np.array_equal(ref, img), f"{name} changed nothing" 
+
+
 @pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
 @pytest.mark.parametrize("spp", [2, 5, 16])
 @pytest.mark.parametrize("lights", ["emissive", "env+analytic", "uniform"])
