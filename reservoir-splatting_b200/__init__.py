@@ -121,6 +121,9 @@ class ReservoirSplatting:
         _check(lib.rs_create(C.byref(self.options), C.byref(h)))
         self._h = h
         self.width, self.height = self.options.frameWidth, self.options.frameHeight
+        # the render graph's default size, which outputSize selections are relative to
+        self._default_size = (width, height)
+        self._output_size = abi.output_size_selection(props)
 
     def close(self):
         if getattr(self, "_h", None):
@@ -135,9 +138,23 @@ class ReservoirSplatting:
 
     # ---- reference-facing API
     def set_properties(self, props: dict, width: int | None = None, height: int | None = None):
-        self.options = abi.options_from_properties(props, width or self.width, height or self.height)
-        _check(self._lib.rs_set_options(self._h, C.byref(self.options)))
+        """setProperties (ReservoirSplatting.cpp:182-190): the options not named keep their values,
+        and so does the outputSize selection, which is relative to the default size (the
+        constructor's, unless width/height are given)."""
+        default = (width or self._default_size[0], height or self._default_size[1])
+        props = dict(props)
+        if "outputSize" not in props:
+            props["outputSize"] = self._output_size[0]
+            props.setdefault("fixedOutputSize", self._output_size[1])
+        options = abi.options_from_properties(props, *default, base=self.options)
+        _check(self._lib.rs_set_options(self._h, C.byref(options)))
+        self.options, self._default_size, self._output_size = options, default, abi.output_size_selection(props)
         self.width, self.height = self.options.frameWidth, self.options.frameHeight
+
+    def get_properties(self) -> dict:
+        """getProperties (ReservoirSplatting.cpp:303-344), followed by the ReSTIR keys; passing the
+        dict back to set_properties restores these options."""
+        return abi.properties_from_options(self.options, *self._output_size)
 
     def set_scene(self, scene):
         desc, keep = abi.scene_struct(scene)

@@ -184,9 +184,14 @@ _NO_EFFECT = {"useAlphaTest", "adjustShadingNormals", "maxNestedMaterials", "use
 _IO_SIZE = {"Default": 1.0, "Full": 1.0, "Half": 0.5, "Quarter": 0.25, "Double": 2.0}
 
 
-def options_from_properties(props: dict | None, width: int, height: int) -> RsOptions:
-    """parseProperties (ReservoirSplatting.cpp:192-261) for a createPass() property dict."""
+def options_from_properties(props: dict | None, width: int, height: int, base: RsOptions | None = None) -> RsOptions:
+    """parseProperties (ReservoirSplatting.cpp:192-261) for a createPass() property dict: keys not
+    given keep their values in `base` (the defaults without one); width and height are the default
+    frame size that outputSize selects from."""
     o = default_options(width, height)
+    if base is not None:
+        C.memmove(C.byref(o), C.byref(base), C.sizeof(RsOptions))
+        o.frameWidth, o.frameHeight = width, height
     props = dict(props or {})
     names = {f for f, _ in RsOptions._fields_}
     size = props.get("outputSize")
@@ -233,6 +238,53 @@ def options_from_properties(props: dict | None, width: int, height: int) -> RsOp
         o.maxSurfaceBounces = max(o.maxDiffuseBounces, o.maxSpecularBounces, o.maxTransmissionBounces)
     o.maxSurfaceBounces = max(o.maxSurfaceBounces, o.maxDiffuseBounces, o.maxSpecularBounces, o.maxTransmissionBounces)
     return o
+
+
+def _enum_name(table: dict, value: int) -> str | int:
+    return next((k for k, v in table.items() if v == value), int(value))
+
+
+def properties_from_options(o: RsOptions, output_size="Default", fixed_output_size=(512, 512)) -> dict:
+    """getProperties (ReservoirSplatting.cpp:303-344): the scripting keys in the reference's order,
+    fixedSeed only when a fixed seed is set, fixedOutputSize only with outputSize "Fixed", and the
+    keys that change nothing here at the values this build renders with.  The reference leaves the
+    ReSTIR keys (:125-130) out of its dict; they follow here, with the further ReSTIR parameters of
+    the options struct, so that options_from_properties(properties_from_options(o)) gives o back."""
+    p = {"samplesPerPixel": int(o.samplesPerPixel), "maxSurfaceBounces": int(o.maxSurfaceBounces),
+         "maxDiffuseBounces": int(o.maxDiffuseBounces), "maxSpecularBounces": int(o.maxSpecularBounces),
+         "maxTransmissionBounces": int(o.maxTransmissionBounces),
+         "sampleGenerator": _enum_name(SAMPLE_GENERATOR, o.sampleGenerator)}
+    if o.useFixedSeed:
+        p["fixedSeed"] = int(o.fixedSeed)
+    p.update({"useRussianRoulette": bool(o.useRussianRoulette), "misHeuristic": _enum_name(MIS_HEURISTIC, o.misHeuristic),
+              "misPowerExponent": float(o.misPowerExponent), "emissiveSampler": _enum_name(EMISSIVE_SAMPLER, o.emissiveSampler),
+              "useAlphaTest": True, "adjustShadingNormals": False, "maxNestedMaterials": 2,
+              "useLightsInDielectricVolumes": False, "disableCaustics": bool(o.disableCaustics),
+              "specularRoughnessThreshold": float(o.specularRoughnessThreshold), "primaryLodMode": "Mip0", "lodBias": 0.0,
+              "outputSize": output_size})
+    if output_size == "Fixed":
+        p["fixedOutputSize"] = (int(fixed_output_size[0]), int(fixed_output_size[1]))
+    p["colorFormat"] = "LogLuvHDR"
+    p.update({"enableTemporalResampling": bool(o.enableTemporalResampling),
+              "enableSpatialResampling": bool(o.enableSpatialResampling),
+              "temporalReuse": _enum_name(TEMPORAL_REUSE, o.temporalReuse),
+              "scatterBackupMISOption": _enum_name(SCATTER_BACKUP_MIS, o.scatterBackupMISOption),
+              "gatherOption": _enum_name(GATHER_MECHANISM, o.gatherOption), "numTimePartitions": int(o.numTimePartitions),
+              "useConfidenceWeightsTemporally": int(o.useConfidenceWeightsTemporally),
+              "numSpatialIterations": int(o.numSpatialIterations), "spatialGatherRadius": float(o.spatialGatherRadius),
+              "neighborCount": int(o.neighborCount), "useConfidenceWeightsSpatially": int(o.useConfidenceWeightsSpatially),
+              "artificialFrameTime": float(o.artificialFrameTime)})
+    return p
+
+
+def output_size_selection(props: dict | None) -> tuple:
+    """The outputSize selection and fixedOutputSize a property dict makes (ReservoirSplatting.cpp:223-225);
+    a (width, height) pair given as outputSize counts as a fixed size."""
+    props = props or {}
+    size = props.get("outputSize", "Default")
+    if isinstance(size, str):
+        return size, tuple(props.get("fixedOutputSize", (512, 512)))
+    return "Fixed", (int(size[0]), int(size[1]))
 
 
 def camera_struct(cam) -> RsCamera:

@@ -127,3 +127,40 @@ def test_missing_library_fails_loudly(rs, tmp_path, monkeypatch):
     monkeypatch.setattr(rs, "LIB_PATH", tmp_path / "librs_b200.so")
     with pytest.raises(RuntimeError, match="CUDA library missing"):
         rs.ReservoirSplatting({}, 16, 16)
+
+
+def _fields(o):
+    return {name: getattr(o, name) for name, _ in o._fields_}
+
+
+@pytest.mark.parametrize("props", [{}, {"fixedSeed": 9, "misHeuristic": "PowerExp", "misPowerExponent": 3.5, "emissiveSampler": "Uniform",
+                                        "temporalReuse": "MultiScatter", "numTimePartitions": 4, "gatherOption": "Robust",
+                                        "maxDiffuseBounces": 2, "maxSpecularBounces": 5, "maxTransmissionBounces": 1,
+                                        "neighborCount": 3, "spatialGatherRadius": 12.5, "disableCaustics": True},
+                                   {"outputSize": "Fixed", "fixedOutputSize": (96, 64), "samplesPerPixel": 4, "maxSurfaceBounces": 2},
+                                   {"outputSize": "Half", "enableTemporalResampling": False, "scatterBackupMISOption": "Pairwise"}])
+def test_get_properties_round_trips(rs, props):
+    """properties_from_options is getProperties (ReservoirSplatting.cpp:303-344): parsing its dict
+    gives the same options back, and the reference's keys come first, in its order."""
+    o = rs.abi.options_from_properties(props, 320, 240)
+    got = rs.abi.properties_from_options(o, *rs.abi.output_size_selection(props))
+    assert _fields(rs.abi.options_from_properties(got, 320, 240)) == _fields(o)
+    keys = list(got)
+    assert keys[:5] == ["samplesPerPixel", "maxSurfaceBounces", "maxDiffuseBounces", "maxSpecularBounces", "maxTransmissionBounces"]
+    assert ("fixedSeed" in got) == bool(o.useFixedSeed) and ("fixedOutputSize" in got) == (got["outputSize"] == "Fixed")
+    assert keys.index("colorFormat") < keys.index("enableTemporalResampling")
+    assert "lightBVHOptions" not in got
+
+
+def test_properties_given_later_keep_the_others(rs):
+    """setProperties parses only the keys it is given (ReservoirSplatting.cpp:192-261): the others
+    keep their values; maxSurfaceBounces resets the per-type limits not named beside it (:236-241)."""
+    base = rs.abi.options_from_properties({"temporalReuse": "ScatterBackup", "gatherOption": "Clamped", "fixedSeed": 3,
+                                           "maxDiffuseBounces": 2, "maxSpecularBounces": 4}, 64, 64)
+    o = rs.abi.options_from_properties({"enableSpatialResampling": False}, 64, 64, base=base)
+    assert o.temporalReuse == 2 and o.gatherOption == 1 and o.useFixedSeed == 1 and o.fixedSeed == 3
+    assert o.enableSpatialResampling == 0 and (o.maxDiffuseBounces, o.maxSpecularBounces, o.maxSurfaceBounces) == (2, 4, 9)
+    o = rs.abi.options_from_properties({"maxSurfaceBounces": 3, "maxSpecularBounces": 1}, 64, 64, base=base)
+    assert (o.maxSurfaceBounces, o.maxDiffuseBounces, o.maxSpecularBounces, o.maxTransmissionBounces) == (3, 3, 1, 3)
+    o = rs.abi.options_from_properties({"outputSize": "Quarter"}, 64, 64, base=base)
+    assert (o.frameWidth, o.frameHeight) == (16, 16) and o.temporalReuse == 2
