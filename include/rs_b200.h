@@ -355,15 +355,19 @@ RS_API rs_status rs_debug_stage_rays(rs_pass* pass, uint64_t* rays, uint32_t* co
  * differentiates f(y) with respect to every material's baseColor (per channel), roughness and
  * emissive radiance (per channel).  E[df(y)/dtheta * W] is the derivative of the pixel integral, so
  * the gradient is unbiased.  Only the final reservoirs of a frame are needed: rs_checkpoint copies
- * them (rs_checkpoint_bytes = 144 bytes per pixel) and rs_backward recomputes the rest.  Paths must
- * have at most three vertices (maxSurfaceBounces <= 1); metallic and ior are not differentiated.
+ * them (rs_checkpoint_bytes = 144 bytes per pixel) and rs_backward recomputes the rest.  A path of
+ * four or more vertices is re-run from its third vertex with the sample-generator state, bounce
+ * counters and flags its record saved there (word 27 and bits 15-26 of word 5), which needs the
+ * TinyUniform generator; paths past x2 with a delta lobe, or of more than 8 BSDF vertices, are
+ * skipped and counted.  The scene must be lit by emissive triangles alone (no env map, no analytic
+ * lights); metallic and ior are not differentiated.
  *
  *   rs_set_materials   replace material parameters in place (same count; geometry and BVH stay)
  *   rs_checkpoint      copy the last frame's final reservoirs to caller device memory
  *   rs_backward        gradMaterials[m * 8 + k] += d loss / d (baseColor.xyz, roughness, emissive.xyz, -)
  *                      for d loss / d colour `gradColor` (device float4 per pixel); checkpoint NULL
  *                      means the last frame; the materials must be those the frame used
- *   rs_backward_stats  read and clear {paths replayed, paths too long, emitter not found, value mismatch} */
+ *   rs_backward_stats  read and clear {paths replayed, paths skipped, emitter not found, value mismatch} */
 RS_API rs_status rs_set_materials(rs_pass* pass, const rs_material* materials, uint32_t count);
 RS_API rs_status rs_checkpoint_bytes(rs_pass* pass, size_t* bytes);
 RS_API rs_status rs_checkpoint(rs_pass* pass, void* dstDevice, void* cudaStream);

@@ -220,6 +220,9 @@ struct ReconnectionData
     float secondaryPathJacobian = 1.f;
     f3 irradiance = mk3(0.f);
     f3 earlyThroughput = mk3(1.f);
+    // suffix replay state of the adjoint (no reference counterpart): the sample generator's state
+    // and the packed bounce counters and path flags on entering the third vertex
+    uint32_t suffixSeed = 0, suffixState = 0;
 };
 
 // ReconnectionData.slang:35-82
@@ -312,6 +315,18 @@ enum PathFlags : uint32_t
     kInsideDielectric = 0x0020, kLightSampledUpper = 0x0040, kLightSampledLower = 0x0080,
 };
 static const uint32_t kVertexIndexBits = 10u;
+
+// The bounce counters (two bits each: on entering x3 each is at most 2) and the path flags 4..128
+// on entering the third vertex, in the 12 bits of ReconnectionData::suffixState.
+static uint32_t suffix_state_pack(uint32_t bounces, uint32_t flags)
+{
+    return (bounces & 3u) | (((bounces >> 8) & 3u) << 2) | (((bounces >> 16) & 3u) << 4) | (((flags >> 2) & 0x3fu) << 6);
+}
+static void suffix_state_unpack(uint32_t st, uint32_t& bounces, uint32_t& flags)
+{
+    bounces = (st & 3u) | (((st >> 2) & 3u) << 8) | (((st >> 4) & 3u) << 16);
+    flags = ((st >> 6) & 0x3fu) << 2;
+}
 
 struct PathState
 {
@@ -495,7 +510,8 @@ struct Pass
     }
 
     // generateScatterRay(sd, mi, path) (:331-382)
-    bool generateScatterRay(const ShadingData& sd, const BsdfData& d, PathState& path) const
+    // componentOut (the adjoint's suffix replay): the sampled lobe's BSDF component type
+    bool generateScatterRay(const ShadingData& sd, const BsdfData& d, PathState& path, uint32_t* componentOut = nullptr) const
     {
         BSDFSample result;
         result.wo = mk3(0.f); result.pdf = 0.f; result.weight = mk3(0.f); result.lobeType = 0;
@@ -518,6 +534,7 @@ struct Pass
             path.reconnection.secondWo = result.wo;
         }
         path.totalPdf = mi_pdf(sd, d, 0xFu, result.wo);
+        if (componentOut) *componentOut = componentType;
         if (valid) generateScatterRayBS(result, sd, d, path);
         if (path.getVertexIndex() == 1 || path.getVertexIndex() == 2)
         {
@@ -640,6 +657,8 @@ struct Pass
         else if (path.getVertexIndex() == 3)
         {
             path.reconnection.secondaryPathJacobian *= prevScatterPdf;
+            path.reconnection.suffixSeed = (uint32_t)path.sg.state;
+            path.reconnection.suffixState = suffix_state_pack(path.bounceCounters, path.flagsAndVertexIndex >> kVertexIndexBits);
         }
 
         BsdfData d = instance(sd);
@@ -2090,34 +2109,41 @@ static void export_recon(const ReconnectionData& r, uint32_t* o)
     o[0] = f2u(r.subPixel.x); o[1] = f2u(r.subPixel.y); o[2] = f2u(r.lensSample.x); o[3] = f2u(r.lensSample.y);
     o[4] = f2u(r.time);
     o[5] = (r.pathLength & 0xffu) | ((r.firstBSDFComponentType & 3u) << 8) | ((r.secondBSDFComponentType & 3u) << 10) |
-           ((r.transmissionEvent ? 1u : 0u) << 12) | ((r.lightIsNEE ? 1u : 0u) << 13) | ((r.lightIsDistant ? 1u : 0u) << 14);
+           ((r.transmissionEvent ? 1u : 0u) << 12) | ((r.lightIsNEE ? 1u : 0u) << 13) | ((r.lightIsDistant ? 1u : 0u) << 14) |
+           ((r.suffixState & 0xfffu) << 15);
     o[6] = f2u(r.lightPdf); o[7] = f2u(r.subPixelJacobian);
     for (int k = 0; k < 4; k++) { o[8 + k] = r.firstHit.w[k]; o[12 + k] = r.secondHit.w[k]; }
     o[16] = f2u(r.firstWi.x); o[17] = f2u(r.firstWi.y); o[18] = f2u(r.firstWi.z); o[19] = f2u(r.lensVertexJacobian);
     o[20] = f2u(r.secondWo.x); o[21] = f2u(r.secondWo.y); o[22] = f2u(r.secondWo.z); o[23] = f2u(r.secondaryPathJacobian);
-    o[24] = f2u(r.irradiance.x); o[25] = f2u(r.irradiance.y); o[26] = f2u(r.irradiance.z); o[27] = 0;
+    o[24] = f2u(r.irradiance.x); o[25] = f2u(r.irradiance.y); o[26] = f2u(r.irradiance.z); o[27] = r.suffixSeed;
 }
 static void import_recon(ReconnectionData& r, const uint32_t* o)
 {
     r.subPixel = mk2(u2f(o[0]), u2f(o[1])); r.lensSample = mk2(u2f(o[2]), u2f(o[3])); r.time = u2f(o[4]);
     r.pathLength = o[5] & 0xffu; r.firstBSDFComponentType = (o[5] >> 8) & 3u; r.secondBSDFComponentType = (o[5] >> 10) & 3u;
     r.transmissionEvent = (o[5] >> 12) & 1u; r.lightIsNEE = (o[5] >> 13) & 1u; r.lightIsDistant = (o[5] >> 14) & 1u;
+    r.suffixState = (o[5] >> 15) & 0xfffu;
     r.lightPdf = u2f(o[6]); r.subPixelJacobian = u2f(o[7]);
     for (int k = 0; k < 4; k++) { r.firstHit.w[k] = o[8 + k]; r.secondHit.w[k] = o[12 + k]; }
     r.firstWi = mk3(u2f(o[16]), u2f(o[17]), u2f(o[18])); r.lensVertexJacobian = u2f(o[19]);
     r.secondWo = mk3(u2f(o[20]), u2f(o[21]), u2f(o[22])); r.secondaryPathJacobian = u2f(o[23]);
     r.irradiance = mk3(u2f(o[24]), u2f(o[25]), u2f(o[26]));
+    r.suffixSeed = o[27];
 }
 
 // ================================================= path-replay adjoint (no reference counterpart)
 // The resolved colour of a pixel is f(y) * W (ResolveReSTIR.cs.slang:45-63).  The adjoint holds the
 // frame's selected path y, its contribution weight W, the sampling densities and the MIS weights at
 // their values for the pass's materials, and differentiates f(y) with respect to each material's
-// baseColor and roughness (BSDF factors at x1 and x2) and emitted radiance (the Le the path carries).
-// f(y) is the reconnection-shift evaluation of the record at its own primary hit
+// baseColor and roughness (the BSDF factor of every vertex) and emitted radiance (the Le the path
+// carries).  f(y) is the reconnection-shift evaluation of the record at its own primary hit
 // (handleReconnectionHit / pathReconnectionShift above) without the visibility ray, which does not
-// depend on materials.  Paths longer than three vertices carry suffix radiance from materials that
-// the record does not name; they are counted and skipped.
+// depend on materials.  A path of four or more vertices carries the radiance of its suffix (x3 on)
+// in the record; the suffix is re-run from x3 by the path tracer's own steps (handleHit below) from
+// the sample generator's state and the bounce counters and flags the record saved on entering x3,
+// which gives its vertices, their BSDF factors and the emitter.
+static const uint32_t kReplayMaxVertices = 8; // BSDF factors on a replayed path (x1, x2 and the suffix)
+
 struct ReplayVertex
 {
     uint32_t material = kInvalidIndex;
@@ -2133,12 +2159,12 @@ struct Replay
     float s = 0.f;                    // detached factor: MIS weight over the sampling densities
     f3 Le = mk3(0.f);                 // emitted radiance the path carries
     uint32_t emitter = kInvalidIndex; // material that emits Le, when the replay finds it
-    uint32_t nv = 0;                  // BSDF vertices on the path (0, 1 or 2)
-    ReplayVertex v[2];
-    f3 value = mk3(0.f);              // replayed f(y)
+    uint32_t nv = 0;                  // BSDF vertices on the path
+    ReplayVertex v[kReplayMaxVertices];
+    f3 value = mk3(0.f);              // prod factors * Le * s
     f3 k = mk3(1.f);                  // integrand / value per channel (detached; 1 where value is 0)
 };
-enum { kStatReplayed = 0, kStatTooLong = 1, kStatNoEmitter = 2, kStatValueMismatch = 3 };
+enum { kStatReplayed = 0, kStatSkipped = 1, kStatNoEmitter = 2, kStatValueMismatch = 3 };
 
 static ReplayVertex replay_vertex(const Pass& p, const ShadingData& sd, uint32_t lobeMask, f3 wo)
 {
@@ -2163,14 +2189,92 @@ static uint32_t emitter_of(const Pass& p, const ShadingData& sd)
     return material_is_emissive(p.scene.materials[sd.materialID]) ? sd.materialID : kInvalidIndex;
 }
 
+// The suffix of a path of four or more vertices: handleHit re-run from x3 (the closest hit from x2
+// along the stored direction) with the sample generator's state, bounce counters and flags the
+// record saved there, taking every draw the path tracer takes (the candidate selections', Russian
+// roulette's, the light and BSDF samples'), up to the light sample that ends the path.  Appends the
+// BSDF factor of each suffix vertex (the sampled lobe's; at the last vertex all lobes' toward the
+// light) and sets the emitter, its radiance and the replayed suffix radiance S, which equals the
+// record's irradiance.  Emitted radiance beyond x2 that a BSDF sample reaches counts only after a
+// delta lobe (handleHit's computeEmissive), whose factor is no BSDF evaluation: such paths, delta
+// lobes on the suffix and paths of more than kReplayMaxVertices factors are not replayed.
+static bool replay_suffix(const Pass& p, const ReconnectionData& rd, const ShadingData& sd2, Replay& out, f3& S)
+{
+    PathState path;
+    uint32_t bounces, flags;
+    suffix_state_unpack(rd.suffixState, bounces, flags);
+    path.bounceCounters = bounces;
+    path.flagsAndVertexIndex = ((flags | kActive) << kVertexIndexBits) | 2u;
+    path.sg.state = rd.suffixSeed;
+    path.sg.kind = p.opt.sampleGenerator;
+    path.thp = mk3(1.f);
+    path.dir = rd.secondWo;
+    path.origin = computeRayOrigin(sd2.posW, dot(sd2.faceN, rd.secondWo) >= 0.f ? sd2.faceN : -sd2.faceN);
+    while (true)
+    {
+        path.incrementVertexIndex();
+        const uint32_t v = path.getVertexIndex();
+        HitInfo h; float t;
+        if (v >= rd.pathLength || !p.bvh.closest(mk_ray(path.origin, path.dir, 0.f, kRayTMax), h, t)) return false;
+        ShadingData sd = p.loadSD(h, path.dir);
+        BsdfData d = p.instance(sd);
+        if (p.lv.count > 0 && (!path.isLightSampled() || !path.isLightSamplable()) && any_gt0(d.emission))
+            sampleNext1D(path.sg); // the emissive candidate's selection draw (addVertex)
+        if (p.hasFinishedSurfaceBounces(path)) return false;
+        path.origin = sd_ray_origin(sd, true);
+        const uint32_t lobeTypes = mi_lobe_types(d);
+        path.setFlag(kLightSampledUpper, false); path.setFlag(kLightSampledLower, false);
+        if ((lobeTypes & kLobeNonDelta) != 0)
+        {
+            bool sampleUpper = (lobeTypes & kLobeNonDeltaReflection) != 0;
+            bool sampleLower = (lobeTypes & kLobeNonDeltaTransmission) != 0;
+            Pass::LightSample ls;
+            bool validSample = p.generateLightSample(sd.posW, sd.faceN, sd.frontFacing, sampleUpper, sampleLower, path.sg, ls);
+            path.setFlag(kLightSampledUpper, sampleUpper); path.setFlag(kLightSampledLower, sampleLower);
+            if (validSample)
+            {
+                float misWeight = p.mis(ls.pdf, mi_pdf(sd, d, 0u, ls.dir));
+                f3 Lr = mi_eval(sd, d, 0u, ls.dir) * misWeight * ls.Li;
+                if (any_gt0(Lr) && p.traceVisibilityRay(mk_ray(ls.origin, ls.dir, 0.f, ls.distance)))
+                {
+                    sampleNext1D(path.sg); // the light candidate's selection draw (addVertex)
+                    if (rd.lightIsNEE && v + 1 == rd.pathLength)
+                    {
+                        if (out.nv == kReplayMaxVertices) return false;
+                        out.v[out.nv++] = replay_vertex(p, sd, 0u, ls.dir);
+                        S = path.thp * Lr;
+                        out.Le = ls.Li * ls.pdf;
+                        const HitInfo lh = hit_tri(p.lv.tris[ls.triangleId].sceneTri, ls.barycentrics.x, ls.barycentrics.y);
+                        out.emitter = emitter_of(p, p.loadSD(lh, ls.dir));
+                        return true;
+                    }
+                }
+            }
+        }
+        if (p.opt.useRussianRoulette)
+        {
+            float u = sampleNext1D(path.sg);
+            const float prob = f_max(0.f, 1.f - luminance(path.thp));
+            if (u < prob) return false;
+            path.thp /= 1.f - prob;
+        }
+        uint32_t comp = 0;
+        bool valid = p.generateScatterRay(sd, d, path, &comp);
+        if (!valid || path.isDelta() || (comp != 0 && comp != 2) || out.nv == kReplayMaxVertices) return false;
+        out.v[out.nv++] = replay_vertex(p, sd, 1u << comp, path.dir);
+        if (p.hasFinishedSurfaceBounces(path)) return false; // the path ends here: no later light sample
+        if (p.opt.disableCaustics && path.getBounces(0) > 0 && path.isSpecular()) return false;
+    }
+}
+
 static bool replay_pixel(const Pass& p, const PathReservoir& r, const ReconnectionData& rd, Replay& out, uint64_t* stats)
 {
     out = Replay();
     out.W = r.computeUCW();
     if (!(out.W > 0.f) || rd.pathLength == 0) return false;
-    if (rd.pathLength > 3) { stats[kStatTooLong]++; return false; }
     out.L = rd.pathLength;
     out.Le = rd.irradiance;
+    bool suffixMismatch = false;
     ShadingData sd1 = p.loadSD(rd.firstHit, -rd.firstWi);
     if (rd.pathLength == 1)
     {
@@ -2214,38 +2318,57 @@ static bool replay_pixel(const Pass& p, const PathReservoir& r, const Reconnecti
             uint32_t mask2 = 1u << rd.secondBSDFComponentType;
             float lsp = mi_pdf(sd2, d2, mask2, rd.secondWo), tp = mi_pdf(sd2, d2, 0xFu, rd.secondWo);
             if (!any_gt0(mi_eval(sd2, d2, 0xFu, rd.secondWo))) return false;
-            if (rd.lightIsNEE)
+            if (rd.pathLength > 3)
             {
-                out.v[1] = replay_vertex(p, sd2, 0xFu, rd.secondWo);
-                out.s = (1.f / lobePdf) * (p.mis(rd.lightPdf, tp) / rd.lightPdf);
+                // pathReconnectionShift's lobe-specific x2 term; the suffix follows from x3
+                if (!(lsp > 0.f)) return false;
+                if (p.opt.sampleGenerator != kSgTinyUniform) { stats[kStatSkipped]++; return false; }
+                out.v[1] = replay_vertex(p, sd2, mask2, rd.secondWo);
+                out.s = (1.f / lobePdf) * (1.f / lsp);
+                out.nv = 2;
+                f3 S;
+                if (!replay_suffix(p, rd, sd2, out, S)) { stats[kStatSkipped]++; return false; }
+                suffixMismatch = !(S.x == rd.irradiance.x && S.y == rd.irradiance.y && S.z == rd.irradiance.z);
             }
             else
             {
-                if (!(lsp > 0.f)) return false;
-                out.v[1] = replay_vertex(p, sd2, mask2, rd.secondWo);
-                out.s = (1.f / lobePdf) * (p.mis(tp, rd.lightPdf) / lsp);
+                if (rd.lightIsNEE)
+                {
+                    out.v[1] = replay_vertex(p, sd2, 0xFu, rd.secondWo);
+                    out.s = (1.f / lobePdf) * (p.mis(rd.lightPdf, tp) / rd.lightPdf);
+                }
+                else
+                {
+                    if (!(lsp > 0.f)) return false;
+                    out.v[1] = replay_vertex(p, sd2, mask2, rd.secondWo);
+                    out.s = (1.f / lobePdf) * (p.mis(tp, rd.lightPdf) / lsp);
+                }
+                out.nv = 2;
+                f3 o2 = computeRayOrigin(sd2.posW, dot(sd2.faceN, rd.secondWo) >= 0.f ? sd2.faceN : -sd2.faceN);
+                HitInfo h; float t;
+                if (p.bvh.closest(mk_ray(o2, rd.secondWo, 0.f, kRayTMax), h, t))
+                    out.emitter = emitter_of(p, p.loadSD(h, rd.secondWo));
+                // a light sample whose ray slips through the seam between two triangles of the light
+                if (out.emitter == kInvalidIndex && rd.lightIsNEE) out.emitter = emissive_material_with_radiance(p.lv, rd.irradiance);
             }
-            out.nv = 2;
-            f3 o2 = computeRayOrigin(sd2.posW, dot(sd2.faceN, rd.secondWo) >= 0.f ? sd2.faceN : -sd2.faceN);
-            HitInfo h; float t;
-            if (p.bvh.closest(mk_ray(o2, rd.secondWo, 0.f, kRayTMax), h, t))
-                out.emitter = emitter_of(p, p.loadSD(h, rd.secondWo));
-            // a light sample whose ray slips through the seam between two triangles of the light
-            if (out.emitter == kInvalidIndex && rd.lightIsNEE) out.emitter = emissive_material_with_radiance(p.lv, rd.irradiance);
         }
     }
-    f3 B = out.nv == 2 ? out.v[1].g.value : mk3(1.f);
-    f3 A = out.nv >= 1 ? out.v[0].g.value : mk3(1.f);
-    out.value = A * B * out.Le * out.s;
-    // The differentiated function is k * W * s * A(theta) * B(theta) * Le(theta) with k fixed, so that
+    f3 prod = mk3(1.f);
+    for (uint32_t k = 0; k < out.nv; k++) prod = prod * out.v[k].g.value;
+    out.value = prod * out.Le * out.s;
+    // a suffix path's value is checked through the record's irradiance (the replayed suffix
+    // radiance equals it bit for bit); the suffix's densities and MIS weights fall into k
+    const f3 check = out.L > 3 ? out.v[0].g.value * out.v[1].g.value * rd.irradiance * out.s : out.value;
+    // The differentiated function is k * W * s * prod_k F_k(theta) * Le(theta) with k fixed, so that
     // at the pass's materials it equals the resolved colour integrand * W exactly (the replay and the
     // path tracer place ray origins slightly differently, which moves f(y) by ~1e-5 relative).
     out.k = mk3(out.value.x != 0.f ? r.integrand.x / out.value.x : 1.f, out.value.y != 0.f ? r.integrand.y / out.value.y : 1.f,
                 out.value.z != 0.f ? r.integrand.z / out.value.z : 1.f);
     stats[kStatReplayed]++;
     if (out.emitter == kInvalidIndex) stats[kStatNoEmitter]++;
-    f3 diff = out.value - r.integrand;
-    if (f_abs(diff.x) + f_abs(diff.y) + f_abs(diff.z) > 1e-3f * (f_abs(r.integrand.x) + f_abs(r.integrand.y) + f_abs(r.integrand.z)))
+    f3 diff = check - r.integrand;
+    if (suffixMismatch ||
+        f_abs(diff.x) + f_abs(diff.y) + f_abs(diff.z) > 1e-3f * (f_abs(r.integrand.x) + f_abs(r.integrand.y) + f_abs(r.integrand.z)))
         stats[kStatValueMismatch]++;
     return true;
 }
@@ -2254,24 +2377,27 @@ static bool replay_pixel(const Pass& p, const PathReservoir& r, const Reconnecti
 static void replay_accumulate(const Replay& q, f3 gradColor, double* grad)
 {
     f3 g = gradColor * q.W * q.k;
-    f3 A = q.nv >= 1 ? q.v[0].g.value : mk3(1.f);
-    f3 B = q.nv == 2 ? q.v[1].g.value : mk3(1.f);
+    // before[k] = F_0 ... F_{k-1}, after = F_{k+1} ... (products of the other factors, no division)
+    f3 before[kReplayMaxVertices];
+    f3 run = mk3(1.f);
+    for (uint32_t k = 0; k < q.nv; k++) { before[k] = run; run = run * q.v[k].g.value; }
     if (q.emitter != kInvalidIndex)
     {
-        f3 dLe = g * A * B * q.s;
+        f3 dLe = g * run * q.s;
         double* e = grad + (size_t)q.emitter * kGradStride + kGradEmissive;
         e[0] += dLe.x; e[1] += dLe.y; e[2] += dLe.z;
     }
-    for (uint32_t k = 0; k < q.nv; k++)
+    f3 after = mk3(1.f);
+    for (uint32_t k = q.nv; k-- > 0;)
     {
         const ReplayVertex& v = q.v[k];
-        f3 other = (k == 0) ? B : A;
-        f3 common = g * other * q.Le * q.s;
+        f3 common = g * (before[k] * after) * q.Le * q.s;
         f3 dB = common * v.g.dBase;
         f3 dR = common * v.g.dRough;
         double* m = grad + (size_t)v.material * kGradStride;
         m[kGradBase + 0] += dB.x; m[kGradBase + 1] += dB.y; m[kGradBase + 2] += dB.z;
         m[kGradRough] += (double)dR.x + (double)dR.y + (double)dR.z;
+        after = after * v.g.value;
     }
 }
 
@@ -2332,18 +2458,14 @@ static ParamsFp64 params_of(const MaterialData& m)
 // it equals the resolved colour at the pass's materials theta0 and moves with the FP64 factors.
 static void replay_fp64(const Replay& q, const ParamsFp64* params, const MaterialData* mats, const f3& integrand, double out[3])
 {
-    double A[3] = {1.0, 1.0, 1.0}, B[3] = {1.0, 1.0, 1.0}, A0[3] = {1.0, 1.0, 1.0}, B0[3] = {1.0, 1.0, 1.0};
-    if (q.nv >= 1)
+    double F[3] = {1.0, 1.0, 1.0}, F0[3] = {1.0, 1.0, 1.0};
+    for (uint32_t k = 0; k < q.nv; k++)
     {
-        const uint32_t m = q.v[0].material;
-        replay_vertex_fp64(q.v[0], params[m], mats[m].ior, A);
-        replay_vertex_fp64(q.v[0], params_of(mats[m]), mats[m].ior, A0);
-    }
-    if (q.nv == 2)
-    {
-        const uint32_t m = q.v[1].material;
-        replay_vertex_fp64(q.v[1], params[m], mats[m].ior, B);
-        replay_vertex_fp64(q.v[1], params_of(mats[m]), mats[m].ior, B0);
+        const uint32_t m = q.v[k].material;
+        double a[3], a0[3];
+        replay_vertex_fp64(q.v[k], params[m], mats[m].ior, a);
+        replay_vertex_fp64(q.v[k], params_of(mats[m]), mats[m].ior, a0);
+        for (int c = 0; c < 3; c++) { F[c] *= a[c]; F0[c] *= a0[c]; }
     }
     double Le[3] = {q.Le.x, q.Le.y, q.Le.z}, Le0[3] = {q.Le.x, q.Le.y, q.Le.z};
     if (q.emitter != kInvalidIndex)
@@ -2351,8 +2473,8 @@ static void replay_fp64(const Replay& q, const ParamsFp64* params, const Materia
     const double I[3] = {integrand.x, integrand.y, integrand.z};
     for (int c = 0; c < 3; c++)
     {
-        double den = A0[c] * B0[c] * Le0[c];
-        out[c] = den != 0.0 ? I[c] * (double)q.W * (A[c] * B[c] * Le[c] / den) : 0.0;
+        double den = F0[c] * Le0[c];
+        out[c] = den != 0.0 ? I[c] * (double)q.W * (F[c] * Le[c] / den) : 0.0;
     }
 }
 
@@ -2607,8 +2729,10 @@ __attribute__((visibility("default"))) int ro_set_materials(ro_pass* r, const rs
 
 // Analytic path-replay gradient of the last frame: adds d loss / d material parameters (count x 8
 // doubles: baseColor.xyz, roughness, emissive.xyz, 0) given d loss / d colour (float4 per pixel).
-// stats: replayed paths, paths longer than three vertices, paths without an identified emitter,
-// replays whose value differs from the reservoir's integrand by more than 1e-3.
+// stats: replayed paths, paths whose suffix is not replayed (a delta lobe or an emissive hit past
+// x2, more than kReplayMaxVertices factors, a PCG32 sample generator), paths without an identified
+// emitter, replays whose value differs from the reservoir's integrand by more than 1e-3 (or whose
+// replayed suffix radiance is not the record's).
 __attribute__((visibility("default"))) int ro_backward(ro_pass* r, const float* gradColor, double* gradOut, uint64_t* stats)
 {
     oracle::Pass& p = r->p;

@@ -146,6 +146,17 @@ struct PState
 enum : uint32_t { kPActive = 1u, kPHit = 2u, kPSpecular = 8u, kPDelta = 16u, kPLightUpper = 64u, kPLightLower = 128u };
 
 __device__ __forceinline__ uint32_t pbounces(const PState& p, uint32_t type) { return (p.bounces >> (type << 3)) & 0xffu; }
+// The bounce counters (two bits each: on entering x3 each is at most 2) and the path flags 4..128
+// on entering the third vertex, in the 12 bits of Recon::suffixState.
+__device__ __forceinline__ uint32_t suffix_state_pack(uint32_t bounces, uint32_t flags)
+{
+    return (bounces & 3u) | (((bounces >> 8) & 3u) << 2) | (((bounces >> 16) & 3u) << 4) | (((flags >> 2) & 0x3fu) << 6);
+}
+__device__ __forceinline__ void suffix_state_unpack(uint32_t st, uint32_t& bounces, uint32_t& flags)
+{
+    bounces = (st & 3u) | (((st >> 2) & 3u) << 8) | (((st >> 4) & 3u) << 16);
+    flags = ((st >> 6) & 0x3fu) << 2;
+}
 __device__ __forceinline__ bool finished_bounces(const DevCtx& C, const PState& p) // PathTracer.slang:161-172
 {
     uint32_t d = pbounces(p, 0), s = pbounces(p, 1), t = pbounces(p, 2);
@@ -229,6 +240,8 @@ __device__ __noinline__ void handle_hit(const DevCtx& C, PState& path, const Rec
     else if (path.vertex == 3)
     {
         path.rec.secondaryPathJacobian *= prevScatterPdf;
+        path.rec.suffixSeed = (uint32_t)path.sg.state;
+        path.rec.suffixState = suffix_state_pack(path.bounces, path.flags);
     }
 
     BsdfData d = dev_instance(C, sd);

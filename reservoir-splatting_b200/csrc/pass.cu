@@ -1343,8 +1343,6 @@ extern "C" RS_API rs_status rs_backward(rs_pass* p, const void* checkpoint, cons
 {
     if (!p || !gradColor || !gradMaterials) return fail(RS_INVALID_ARG, "pass, gradColor or gradMaterials is NULL");
     if (!p->hasScene || !p->haveFrameCtx) return fail(RS_NOT_READY, "rs_backward needs a rendered frame");
-    if (p->opt.maxSurfaceBounces > 1)
-        return fail(RS_INVALID_ARG, "rs_backward replays paths of at most three vertices: set maxSurfaceBounces <= 1");
     if (p->envHost.present) return fail(RS_INVALID_ARG, "rs_backward differentiates scenes lit by emissive triangles; the pass has an env map");
     if (p->numAnalytic) return fail(RS_INVALID_ARG, "rs_backward differentiates scenes lit by emissive triangles; the pass has analytic lights");
     for (const MaterialData& m : p->scene.materials)

@@ -184,6 +184,11 @@ struct Recon // ReconnectionData.slang:89-166 (earlyThroughput lives in the path
     float subPixelJacobian, lensVertexJacobian, secondaryPathJacobian;
     HitInfo firstHit, secondHit;
     f3 firstWi, secondWo, irradiance;
+    // Suffix replay state (no reference counterpart; word 27 and bits 15-26 of word 5, which the
+    // reference's record leaves unused): the sample generator's state and the packed bounce
+    // counters and path flags on entering the third vertex, so that the adjoint can re-run the
+    // path tracer from x3 (suffix_state_pack).  Zero for paths that end before x3.
+    uint32_t suffixSeed, suffixState;
 };
 __device__ __forceinline__ Recon recon_default()
 {
@@ -194,6 +199,7 @@ __device__ __forceinline__ Recon recon_default()
     r.lightPdf = 0.f; r.subPixelJacobian = 1.f; r.lensVertexJacobian = 1.f; r.secondaryPathJacobian = 1.f;
     r.firstHit = hit_none(); r.secondHit = hit_none();
     r.firstWi = mk3(0.f); r.secondWo = mk3(0.f); r.irradiance = mk3(0.f);
+    r.suffixSeed = 0u; r.suffixState = 0u;
     return r;
 }
 
@@ -279,7 +285,8 @@ __device__ __forceinline__ float load_confidence(const ResPlanes& P, uint32_t i)
 __device__ __forceinline__ uint32_t recon_flags(const Recon& r)
 {
     return (r.pathLength & 0xffu) | ((r.firstComp & 3u) << 8) | ((r.secondComp & 3u) << 10) |
-           ((r.transmissionEvent ? 1u : 0u) << 12) | ((r.lightIsNEE ? 1u : 0u) << 13) | ((r.lightIsDistant ? 1u : 0u) << 14);
+           ((r.transmissionEvent ? 1u : 0u) << 12) | ((r.lightIsNEE ? 1u : 0u) << 13) | ((r.lightIsDistant ? 1u : 0u) << 14) |
+           ((r.suffixState & 0xfffu) << 15);
 }
 __device__ __forceinline__ void store_rec(const RecPlanes& P, uint32_t i, const Recon& r)
 {
@@ -291,7 +298,7 @@ __device__ __forceinline__ void store_rec(const RecPlanes& P, uint32_t i, const 
     p[3 * s] = make_uint4(r.secondHit.w[0], r.secondHit.w[1], r.secondHit.w[2], r.secondHit.w[3]);
     p[4 * s] = make_uint4(f2u(r.firstWi.x), f2u(r.firstWi.y), f2u(r.firstWi.z), f2u(r.lensVertexJacobian));
     p[5 * s] = make_uint4(f2u(r.secondWo.x), f2u(r.secondWo.y), f2u(r.secondWo.z), f2u(r.secondaryPathJacobian));
-    p[6 * s] = make_uint4(f2u(r.irradiance.x), f2u(r.irradiance.y), f2u(r.irradiance.z), 0u);
+    p[6 * s] = make_uint4(f2u(r.irradiance.x), f2u(r.irradiance.y), f2u(r.irradiance.z), r.suffixSeed);
 }
 template <bool RO>
 __device__ __forceinline__ Recon load_rec_t(const RecPlanes& P, uint32_t i)
@@ -306,12 +313,14 @@ __device__ __forceinline__ Recon load_rec_t(const RecPlanes& P, uint32_t i)
     r.time = u2f(q1.x);
     r.pathLength = q1.y & 0xffu; r.firstComp = (q1.y >> 8) & 3u; r.secondComp = (q1.y >> 10) & 3u;
     r.transmissionEvent = (q1.y >> 12) & 1u; r.lightIsNEE = (q1.y >> 13) & 1u; r.lightIsDistant = (q1.y >> 14) & 1u;
+    r.suffixState = (q1.y >> 15) & 0xfffu;
     r.lightPdf = u2f(q1.z); r.subPixelJacobian = u2f(q1.w);
     r.firstHit.w[0] = q2.x; r.firstHit.w[1] = q2.y; r.firstHit.w[2] = q2.z; r.firstHit.w[3] = q2.w;
     r.secondHit.w[0] = q3.x; r.secondHit.w[1] = q3.y; r.secondHit.w[2] = q3.z; r.secondHit.w[3] = q3.w;
     r.firstWi = mk3(u2f(q4.x), u2f(q4.y), u2f(q4.z)); r.lensVertexJacobian = u2f(q4.w);
     r.secondWo = mk3(u2f(q5.x), u2f(q5.y), u2f(q5.z)); r.secondaryPathJacobian = u2f(q5.w);
     r.irradiance = mk3(u2f(q6.x), u2f(q6.y), u2f(q6.z));
+    r.suffixSeed = q6.w;
     return r;
 }
 __device__ __forceinline__ Recon load_rec(const RecPlanes& P, uint32_t i) { return load_rec_t<true>(P, i); }

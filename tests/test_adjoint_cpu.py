@@ -55,7 +55,8 @@ def test_bsdf_derivatives_match_fp64_differences(oracle_mod):
 
 def _replay_check(oracle_mod, scene, camera_fn, width, height, frames, props, perturb_seed=1):
     """Analytic oracle gradient vs FP64 Richardson differences of the replay L2 loss against a
-    target rendered with perturbed parameters; returns (max error / max |grad|, stats)."""
+    target rendered with perturbed parameters; returns (max error / max |grad|, stats, gradient,
+    differences, the number of final reservoirs holding paths of more than three vertices)."""
     mats = np.array(scene.materials, np.float32).reshape(len(scene.materials), -1)
     emissive = mats[:, 4:7].max(1) > 0
     rng = np.random.default_rng(perturb_seed)
@@ -73,6 +74,7 @@ def _replay_check(oracle_mod, scene, camera_fn, width, height, frames, props, pe
     G = np.zeros((len(mats), 8))
     FD = np.zeros((len(mats), 8))
     stats = np.zeros(4, np.uint64)
+    long_paths = 0
     for f in range(frames):
         cam = camera_fn(f, width, height)
         target = tgt.execute(cam)
@@ -80,25 +82,31 @@ def _replay_check(oracle_mod, scene, camera_fn, width, height, frames, props, pe
         g, st = ora.backward(2.0 * (img - target), len(mats))
         G += g
         stats += st
+        long_paths += int(((ora.get_buffer("curr_reconnection").reshape(-1, 28)[:, 5] & 0xff) > 3).sum())
         for m, k in params:
             def loss(x):
                 q = P0.copy()
                 q[m, k] = x
                 return ora.replay_loss(target, q)
             FD[m, k] += _richardson(loss, P0[m, k])
-    return np.abs(G - FD).max() / np.abs(FD).max(), stats, G, FD
+    return np.abs(G - FD).max() / np.abs(FD).max(), stats, G, FD, long_paths
 
 
-@pytest.mark.parametrize("case", ["cornell", "inverse_scene"])
-def test_oracle_replay_gradient_matches_fp64_differences(oracle_mod, scenes, case):
-    props = {"temporalReuse": "ScatterBackup", "gatherOption": "Clamped", "maxSurfaceBounces": 1,
+@pytest.mark.parametrize("case,bounces", [("cornell", 1), ("inverse_scene", 1), ("cornell", 2), ("cornell", 3), ("inverse_scene", 2)])
+def test_oracle_replay_gradient_matches_fp64_differences(oracle_mod, scenes, case, bounces):
+    """With more than one bounce the final reservoirs hold paths of four and five vertices, whose
+    suffix the replay re-runs from x3 (the records' sample-generator state, bounce counters and
+    flags there); every one of them is replayed and differentiated."""
+    props = {"temporalReuse": "ScatterBackup", "gatherOption": "Clamped", "maxSurfaceBounces": bounces,
              "enableSpatialResampling": True}
     if case == "cornell":
-        err, stats, G, FD = _replay_check(oracle_mod, scenes.cornell_box(0), scenes.cornell_camera, 32, 32, 3, props)
+        err, stats, G, FD, long_paths = _replay_check(oracle_mod, scenes.cornell_box(0), scenes.cornell_camera, 32, 32, 3, props)
     else:
         sc = scenes.inverse_scene(grid=64, spheres=6, subdiv=2)
-        err, stats, G, FD = _replay_check(oracle_mod, sc, scenes.translate_camera, 40, 40, 3, props)
+        err, stats, G, FD, long_paths = _replay_check(oracle_mod, sc, scenes.translate_camera, 40, 40, 3, props)
     assert stats[0] > 0 and stats[1] == 0
+    if bounces > 1:
+        assert long_paths > (100 if case == "cornell" else 5)
     assert err < GRAD_TOL, err
     big = np.abs(FD) > 1e-2 * np.abs(FD).max()
     assert (np.abs(G - FD)[big] / np.abs(FD)[big]).max() < GRAD_TOL

@@ -26,11 +26,11 @@ PROPS = {"temporalReuse": "ScatterBackup", "gatherOption": "Clamped", "maxSurfac
          "enableSpatialResampling": True}
 
 
-def _setup(rs, oracle_mod, scenes, width=64, height=64):
-    sc = scenes.inverse_scene(grid=80, spheres=8, subdiv=2)
-    gpu = rs.ReservoirSplatting(PROPS, width, height)
+def _setup(rs, oracle_mod, scenes, width=64, height=64, props=PROPS, scene=None):
+    sc = scene if scene is not None else scenes.inverse_scene(grid=80, spheres=8, subdiv=2)
+    gpu = rs.ReservoirSplatting(props, width, height)
     gpu.set_scene(sc)
-    ora = oracle_mod.OraclePass(PROPS, width, height)
+    ora = oracle_mod.OraclePass(props, width, height)
     ora.set_scene(sc)
     mats = np.array(sc.materials, np.float32).reshape(len(sc.materials), -1)
     return sc, gpu, ora, mats
@@ -42,10 +42,15 @@ def _richardson(f, x, h=1e-3):
 
 
 @pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
-def test_backward_matches_oracle_and_fp64_differences(rs, oracle_mod, scenes):
+@pytest.mark.parametrize("case,bounces", [("inverse_scene", 1), ("inverse_scene", 2), ("cornell", 2), ("cornell", 3)])
+def test_backward_matches_oracle_and_fp64_differences(rs, oracle_mod, scenes, case, bounces):
+    """With more than one bounce, paths of four and five vertices are differentiated through the
+    suffix replay from x3; none is skipped, and the replayed suffix radiance is the record's."""
     import torch
-    W = H = 64
-    sc, gpu, ora, mats = _setup(rs, oracle_mod, scenes, W, H)
+    W = H = 64 if case == "inverse_scene" else 40
+    props = dict(PROPS, maxSurfaceBounces=bounces)
+    sc, gpu, ora, mats = _setup(rs, oracle_mod, scenes, W, H, props, None if case == "inverse_scene" else scenes.cornell_box(0))
+    camera = scenes.translate_camera if case == "inverse_scene" else scenes.cornell_camera
     rng = np.random.default_rng(2)
     n = len(mats)
     G = torch.zeros((n, 8), dtype=torch.float32, device="cuda")
@@ -55,10 +60,12 @@ def test_backward_matches_oracle_and_fp64_differences(rs, oracle_mod, scenes):
     emissive = mats[:, 4:7].max(1) > 0
     params = [(m, k) for m in range(n) for k in (range(4, 7) if emissive[m] else range(4))]
     stats = np.zeros(4, np.uint64)
+    long_paths = 0
     for f in range(3):
-        cam = scenes.translate_camera(f, W, H)
+        cam = camera(f, W, H)
         img = gpu.render(cam)
         np.testing.assert_array_equal(img, ora.execute(cam))
+        long_paths += int(((gpu.get_buffer("curr_reconnection").reshape(-1, 28)[:, 5] & 0xff) > 3).sum())
         target = (img * rng.uniform(0.9, 1.1, img.shape)).astype(np.float32)
         gc = (2.0 * (img - target)).astype(np.float32)
         gpu.backward(torch.from_numpy(gc).cuda().data_ptr(), G.data_ptr())
@@ -74,6 +81,8 @@ def test_backward_matches_oracle_and_fp64_differences(rs, oracle_mod, scenes):
     g = G.cpu().numpy().astype(np.float64)
     assert stats[0] > 0 and stats[1] == 0
     assert stats[2] == 0, f"{stats[2]} replayed paths without an identified emitter"
+    if bounces > 1:
+        assert long_paths > (20 if case == "inverse_scene" else 100), long_paths
     assert np.abs(g - O).max() <= ORACLE_TOL * np.abs(O).max()
     assert np.abs(g - FD).max() <= GRAD_TOL * np.abs(FD).max()
     big = np.abs(FD) > 1e-2 * np.abs(FD).max()
@@ -122,16 +131,26 @@ def test_set_materials_renders_like_the_oracle(rs, oracle_mod, scenes):
 
 
 @pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
-def test_backward_rejects_paths_longer_than_three_vertices(rs, scenes):
+def test_suffix_replay_needs_the_tiny_uniform_generator(rs, oracle_mod, scenes):
+    """A record keeps 32 bits of the sample generator's state at x3: PCG32's 64-bit state cannot be
+    re-run, so with PCG32 the paths of four or more vertices are skipped and counted, by the GPU and
+    the oracle alike, and the shorter ones are still differentiated."""
     import torch
-    p = rs.ReservoirSplatting(dict(PROPS, maxSurfaceBounces=2), 16, 16)
-    p.set_scene(scenes.cornell_box(0))
-    p.render(scenes.cornell_camera(0, 16, 16))
-    g = torch.zeros((16, 16, 4), device="cuda")
-    out = torch.zeros((len(scenes.cornell_box(0).materials), 8), device="cuda")
-    with pytest.raises(rs.RsError, match="maxSurfaceBounces"):
-        p.backward(g.data_ptr(), out.data_ptr())
-    p.close()
+    W = H = 40
+    props = dict(PROPS, maxSurfaceBounces=2, sampleGenerator="PCG32")
+    sc, gpu, ora, mats = _setup(rs, oracle_mod, scenes, W, H, props, scenes.cornell_box(0))
+    n = len(mats)
+    img = gpu.render(scenes.cornell_camera(0, W, H))
+    np.testing.assert_array_equal(img, ora.execute(scenes.cornell_camera(0, W, H)))
+    gc = np.ones_like(img)
+    G = torch.zeros((n, 8), dtype=torch.float32, device="cuda")
+    gpu.backward(torch.from_numpy(gc).cuda().data_ptr(), G.data_ptr())
+    torch.cuda.synchronize()
+    st = gpu.backward_stats()
+    O, ost = ora.backward(gc, n)
+    assert st[1] > 0 and st[1] == ost[1] and st[0] == ost[0]
+    assert np.abs(G.cpu().numpy() - O).max() <= ORACLE_TOL * np.abs(O).max()
+    gpu.close()
 
 
 @pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
@@ -163,7 +182,8 @@ def test_autograd_l2_loss_matches_direct_backward(rs, scenes):
 
 
 @pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
-def test_replay_gradient_is_unbiased_over_seeds(rs, scenes):
+@pytest.mark.parametrize("bounces", [1, 2])
+def test_replay_gradient_is_unbiased_over_seeds(rs, scenes, bounces):
     """The estimator itself, not just the replay: for a linear loss (the sum of the last frame's
     pixels), the mean over K seeds of rs_backward's gradient equals the central difference of the
     mean image over the same seeds, to within the statistical error of the paired per-seed
@@ -176,7 +196,7 @@ def test_replay_gradient_is_unbiased_over_seeds(rs, scenes):
     W = H = 24
     K = 192
     sc = scenes.inverse_scene(grid=40, spheres=6, subdiv=2, emitters=4)
-    renderer = adj.Renderer(sc, PROPS, W, H)
+    renderer = adj.Renderer(sc, dict(PROPS, maxSurfaceBounces=bounces), W, H)
     cams = [scenes.translate_camera(f, W, H) for f in range(2)]
     theta = renderer.params().clone()
     n = renderer.num_materials
@@ -224,7 +244,8 @@ def test_replay_gradient_is_unbiased_over_seeds(rs, scenes):
 @pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
 def test_differentiation_config_at_its_stated_size(rs, oracle_mod, scenes):
     """The differentiation configuration as specified: 512 x 512, the seeded 199k-triangle scene with
-    32 materials and 8 emitters, ScatterBackup over 8 frames of a translating camera, L2 loss against a
+    32 materials and 8 emitters, ScatterBackup with paths of up to four vertices (the headline path
+    length, as the bench measures it) over 8 frames of a translating camera, L2 loss against a
     target rendered with the parameters perturbed by N(0, 0.05).  Every frame's image is bit-exact
     with the oracle, and the summed rs_backward gradient matches the oracle's FP64-summed replay
     gradient within 1e-4 of its largest component; no replayed path lacks an emitter."""
@@ -235,8 +256,9 @@ def test_differentiation_config_at_its_stated_size(rs, oracle_mod, scenes):
     W = H = 512
     sc = scenes.inverse_scene()
     assert sc.num_triangles == 199_298
-    renderer = adj.Renderer(sc, PROPS, W, H)
-    ora = oracle_mod.OraclePass(PROPS, W, H)
+    props = dict(PROPS, maxSurfaceBounces=2)
+    renderer = adj.Renderer(sc, props, W, H)
+    ora = oracle_mod.OraclePass(props, W, H)
     ora.set_scene(sc)
     cams = [scenes.translate_camera(f, W, H) for f in range(8)]
     theta = renderer.params().clone()
