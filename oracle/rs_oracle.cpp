@@ -2244,8 +2244,11 @@ static bool replay_suffix(const Pass& p, const ReconnectionData& rd, const Shadi
                         out.v[out.nv++] = replay_vertex(p, sd, 0u, ls.dir);
                         S = path.thp * Lr;
                         out.Le = ls.Li * ls.pdf;
-                        const HitInfo lh = hit_tri(p.lv.tris[ls.triangleId].sceneTri, ls.barycentrics.x, ls.barycentrics.y);
-                        out.emitter = emitter_of(p, p.loadSD(lh, ls.dir));
+                        if (ls.lightType == 1) // an environment-map sample's radiance is no material's
+                        {
+                            const HitInfo lh = hit_tri(p.lv.tris[ls.triangleId].sceneTri, ls.barycentrics.x, ls.barycentrics.y);
+                            out.emitter = emitter_of(p, p.loadSD(lh, ls.dir));
+                        }
                         return true;
                     }
                 }
@@ -2272,6 +2275,8 @@ static bool replay_pixel(const Pass& p, const PathReservoir& r, const Reconnecti
     out = Replay();
     out.W = r.computeUCW();
     if (!(out.W > 0.f) || rd.pathLength == 0) return false;
+    // a primary miss sees the environment map: no material on the path
+    if (rd.pathLength == 1 && rd.lightIsDistant) return false;
     out.L = rd.pathLength;
     out.Le = rd.irradiance;
     bool suffixMismatch = false;
@@ -2285,10 +2290,19 @@ static bool replay_pixel(const Pass& p, const PathReservoir& r, const Reconnecti
     {
         BsdfData d1 = p.instance(sd1);
         f3 origin = sd_ray_origin(sd1, !rd.transmissionEvent);
-        ShadingData sec = p.loadSD(rd.secondHit, mk3(0.f));
-        f3 off = sec.posW - sd1.posW;
-        float jac = f_abs(dot(sec.faceN, -normalize(off))) / dot(off, off);
-        f3 dir = normalize(sec.posW - origin);
+        // a length-2 path to the environment stores a direction as its second hit and has no
+        // geometry term (handleReconnectionHit's secondHitIsDistant)
+        const bool distant2 = rd.pathLength == 2 && rd.lightIsDistant;
+        float jac = 1.f;
+        f3 dir;
+        if (distant2) dir = hit_as_direction(rd.secondHit);
+        else
+        {
+            ShadingData sec = p.loadSD(rd.secondHit, mk3(0.f));
+            f3 off = sec.posW - sd1.posW;
+            jac = f_abs(dot(sec.faceN, -normalize(off))) / dot(off, off);
+            dir = normalize(sec.posW - origin);
+        }
         uint32_t mask1 = 1u << rd.firstBSDFComponentType;
         float lobePdf = mi_pdf(sd1, d1, mask1, dir), totalPdf = mi_pdf(sd1, d1, 0u, dir);
         if (rd.pathLength == 2)
@@ -2307,7 +2321,7 @@ static bool replay_pixel(const Pass& p, const PathReservoir& r, const Reconnecti
                 out.s = p.mis(totalPdf, lightPdf) / lobePdf;
             }
             out.nv = 1;
-            out.emitter = emitter_of(p, p.loadSD(rd.secondHit, dir));
+            if (!distant2) out.emitter = emitter_of(p, p.loadSD(rd.secondHit, dir));
         }
         else
         {
@@ -2344,12 +2358,15 @@ static bool replay_pixel(const Pass& p, const PathReservoir& r, const Reconnecti
                     out.s = (1.f / lobePdf) * (p.mis(tp, rd.lightPdf) / lsp);
                 }
                 out.nv = 2;
-                f3 o2 = computeRayOrigin(sd2.posW, dot(sd2.faceN, rd.secondWo) >= 0.f ? sd2.faceN : -sd2.faceN);
-                HitInfo h; float t;
-                if (p.bvh.closest(mk_ray(o2, rd.secondWo, 0.f, kRayTMax), h, t))
-                    out.emitter = emitter_of(p, p.loadSD(h, rd.secondWo));
-                // a light sample whose ray slips through the seam between two triangles of the light
-                if (out.emitter == kInvalidIndex && rd.lightIsNEE) out.emitter = emissive_material_with_radiance(p.lv, rd.irradiance);
+                if (!rd.lightIsDistant)
+                {
+                    f3 o2 = computeRayOrigin(sd2.posW, dot(sd2.faceN, rd.secondWo) >= 0.f ? sd2.faceN : -sd2.faceN);
+                    HitInfo h; float t;
+                    if (p.bvh.closest(mk_ray(o2, rd.secondWo, 0.f, kRayTMax), h, t))
+                        out.emitter = emitter_of(p, p.loadSD(h, rd.secondWo));
+                    // a light sample whose ray slips through the seam between two triangles of the light
+                    if (out.emitter == kInvalidIndex && rd.lightIsNEE) out.emitter = emissive_material_with_radiance(p.lv, rd.irradiance);
+                }
             }
         }
     }
@@ -2365,7 +2382,8 @@ static bool replay_pixel(const Pass& p, const PathReservoir& r, const Reconnecti
     out.k = mk3(out.value.x != 0.f ? r.integrand.x / out.value.x : 1.f, out.value.y != 0.f ? r.integrand.y / out.value.y : 1.f,
                 out.value.z != 0.f ? r.integrand.z / out.value.z : 1.f);
     stats[kStatReplayed]++;
-    if (out.emitter == kInvalidIndex) stats[kStatNoEmitter]++;
+    // a path that ends at the environment map carries its radiance, no material's
+    if (out.emitter == kInvalidIndex && !rd.lightIsDistant) stats[kStatNoEmitter]++;
     f3 diff = check - r.integrand;
     if (suffixMismatch ||
         f_abs(diff.x) + f_abs(diff.y) + f_abs(diff.z) > 1e-3f * (f_abs(r.integrand.x) + f_abs(r.integrand.y) + f_abs(r.integrand.z)))

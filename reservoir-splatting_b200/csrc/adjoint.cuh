@@ -57,8 +57,9 @@ __device__ __forceinline__ bool adj_finished(const DevCtx& C, uint32_t bounces) 
 // light) and sets the emitter, its radiance and the replayed suffix radiance S, which equals the
 // record's irradiance.  Emitted radiance beyond x2 that a BSDF sample reaches counts only after a
 // delta lobe (handle_hit's computeEmissive), whose factor is no BSDF evaluation: such paths, delta
-// lobes on the suffix and paths of more than kAdjMaxFactors factors are not replayed.  The host
-// accepts only emissive-triangle lighting here (no env map, no analytic lights).
+// lobes on the suffix and paths of more than kAdjMaxFactors factors are not replayed.  A light
+// sample of the environment map leaves emitter = kInvalidIndex: its radiance is no material's.
+// The host accepts emissive triangles and an environment map here (no analytic lights).
 __device__ __noinline__ bool adj_replay_suffix(const DevCtx& C, const Recon& rd, const ShadingData& sd2, uint32_t& nv, uint32_t* mat,
                                                BsdfGrad* V, uint32_t& emitter, f3& Le, f3& S)
 {
@@ -67,7 +68,11 @@ __device__ __noinline__ bool adj_replay_suffix(const DevCtx& C, const Recon& rd,
     SampleGen sg; sg.state = rd.suffixSeed; sg.kind = C.sgKind;
     f3 thp = mk3(1.f), dir = rd.secondWo;
     f3 origin = computeRayOrigin(sd2.posW, dot(sd2.faceN, dir) >= 0.f ? sd2.faceN : -sd2.faceN);
-    const bool haveLights = C.lights.count > 0;
+    const bool haveLights = C.lights.count > 0, haveEnv = C.env->present != 0;
+    // handle_hit's light-type probabilities: with the emissive triangles alone p = {0, haveLights}
+    // and the selection pdf is 1; without an env map pEnv = 0, so u - pEnv is u
+    const float pEnv = haveEnv ? C.pEnvLight : 0.f;
+    const float pEmissive = haveEnv ? C.pEmissiveLight : (haveLights ? 1.f : 0.f);
     for (uint32_t v = 3; v < rd.pathLength; v++)
     {
         HitInfo h; float t;
@@ -87,27 +92,43 @@ __device__ __noinline__ bool adj_replay_suffix(const DevCtx& C, const Recon& rd,
             const bool sampleLower = (lobeTypes & kLobeNonDeltaTransmission) != 0;
             TriangleLightSample tls;
             f3 lsLi = mk3(0.f), lsOrigin = mk3(0.f), lsDir = mk3(0.f);
-            float lsPdf = 0.f, lsDistance = 0.f;
-            bool sampled = false;
-            // the type-selection draw; emissive triangles alone: p = {0, 1, 0}, selection pdf 1
-            float u = sampleNext1D(sg);
-            if (u < (haveLights ? 1.f : 0.f) && sample_emissive(C.lights, sd.posW, sg, tls))
+            float lsPdf = 0.f, lsDistance = 0.f, selectionPdf = 0.f;
+            bool sampled = false, lsEnv = false;
+            float u = sampleNext1D(sg); // the type-selection draw
+            if (haveEnv && u < pEnv)
             {
-                lsLi = tls.pdf > 0.f ? tls.Le / tls.pdf : mk3(0.f);
-                lsPdf = tls.pdf;
-                f3 lightPos = computeRayOrigin(tls.posW, tls.normalW);
-                f3 toL = lightPos - sd.posW;
-                lsOrigin = computeRayOrigin(sd.posW, dot(sd.faceN, toL) >= 0.f ? sd.faceN : -sd.faceN);
-                f3 toLight = lightPos - lsOrigin;
-                lsDistance = length(toLight);
-                lsDir = normalize(toLight);
+                selectionPdf = pEnv;
+                lsEnv = true;
+                f2 r2; r2.x = sampleNext1D(sg); r2.y = sampleNext1D(sg);
+                const EnvSample es = dev_env_sample(C.env, r2);
+                lsDir = es.dir; lsPdf = es.pdf;
+                lsLi = lsPdf > 0.f ? es.Le / lsPdf : mk3(0.f);
+                lsOrigin = computeRayOrigin(sd.posW, dot(sd.faceN, lsDir) >= 0.f ? sd.faceN : -sd.faceN);
+                lsDistance = kRayTMax;
                 sampled = any_gt0(lsLi);
+            }
+            else if (u - pEnv < pEmissive)
+            {
+                selectionPdf = haveEnv ? pEmissive : 1.f;
+                if (sample_emissive(C.lights, sd.posW, sg, tls))
+                {
+                    lsLi = tls.pdf > 0.f ? tls.Le / tls.pdf : mk3(0.f);
+                    lsPdf = tls.pdf;
+                    f3 lightPos = computeRayOrigin(tls.posW, tls.normalW);
+                    f3 toL = lightPos - sd.posW;
+                    lsOrigin = computeRayOrigin(sd.posW, dot(sd.faceN, toL) >= 0.f ? sd.faceN : -sd.faceN);
+                    f3 toLight = lightPos - lsOrigin;
+                    lsDistance = length(toLight);
+                    lsDir = normalize(toLight);
+                    sampled = any_gt0(lsLi);
+                }
             }
             bool validSample = false;
             if (sampled)
             {
                 float NdotL = dot(sd_oriented_face_normal(sd), lsDir);
                 validSample = !((!sampleUpper && NdotL >= -kMinCosTheta) || (!sampleLower && NdotL <= kMinCosTheta));
+                if (validSample) { lsPdf *= selectionPdf; lsLi /= selectionPdf; }
             }
             if (sampleUpper) flags |= kPLightUpper;
             if (sampleLower) flags |= kPLightLower;
@@ -126,7 +147,8 @@ __device__ __noinline__ bool adj_replay_suffix(const DevCtx& C, const Recon& rd,
                         V[nv++] = mi_eval_grad(sd, d, 0u, lsDir);
                         S = thp * Lr;
                         Le = lsLi * lsPdf;
-                        emitter = dev_emitter_of(C, dev_sd(C, hit_tri(C.lights.tris[tls.triangleIndex].sceneTri, tls.uv.x, tls.uv.y), lsDir));
+                        emitter = lsEnv ? kInvalidIndex
+                                        : dev_emitter_of(C, dev_sd(C, hit_tri(C.lights.tris[tls.triangleIndex].sceneTri, tls.uv.x, tls.uv.y), lsDir));
                         return true;
                     }
                 }
@@ -176,6 +198,8 @@ __device__ inline void adj_pixel(const DevCtx& C, const ResPlanes& res, const Re
     if (gc.x == 0.f && gc.y == 0.f && gc.z == 0.f) return;
     Recon rd = load_rec(rec, i);
     if (rd.pathLength == 0) return;
+    // a primary miss sees the environment map: no material on the path
+    if (rd.pathLength == 1 && rd.lightIsDistant) return;
 
     uint32_t nv = 0, emitter = kInvalidIndex;
     uint32_t mat[kAdjMaxFactors];
@@ -192,10 +216,19 @@ __device__ inline void adj_pixel(const DevCtx& C, const ResPlanes& res, const Re
     {
         BsdfData d1 = dev_instance(C, sd1);
         f3 origin = sd_ray_origin(sd1, !rd.transmissionEvent);
-        ShadingData sec = dev_sd(C, rd.secondHit, mk3(0.f));
-        f3 off = sec.posW - sd1.posW;
-        float jac = f_abs(dot(sec.faceN, -normalize(off))) / dot(off, off);
-        f3 dir = normalize(sec.posW - origin);
+        // a length-2 path to the environment stores a direction as its second hit and has no
+        // geometry term (handleReconnectionHit's secondHitIsDistant)
+        const bool distant2 = rd.pathLength == 2 && rd.lightIsDistant;
+        float jac = 1.f;
+        f3 dir;
+        if (distant2) dir = hit_as_direction(rd.secondHit);
+        else
+        {
+            ShadingData sec = dev_sd(C, rd.secondHit, mk3(0.f));
+            f3 off = sec.posW - sd1.posW;
+            jac = f_abs(dot(sec.faceN, -normalize(off))) / dot(off, off);
+            dir = normalize(sec.posW - origin);
+        }
         uint32_t mask1 = 1u << rd.firstComp;
         float lobePdf = mi_pdf(sd1, d1, mask1, dir), totalPdf = mi_pdf(sd1, d1, 0u, dir);
         mat[0] = sd1.materialID;
@@ -215,7 +248,7 @@ __device__ inline void adj_pixel(const DevCtx& C, const ResPlanes& res, const Re
                 s = dev_mis(C, totalPdf, lightPdf) / lobePdf;
             }
             nv = 1;
-            emitter = dev_emitter_of(C, dev_sd(C, rd.secondHit, dir));
+            if (!distant2) emitter = dev_emitter_of(C, dev_sd(C, rd.secondHit, dir));
         }
         else
         {
@@ -252,12 +285,15 @@ __device__ inline void adj_pixel(const DevCtx& C, const ResPlanes& res, const Re
                     V[1] = mi_eval_grad(sd2, d2, mask2, rd.secondWo);
                     s = (1.f / lobePdf) * (dev_mis(C, tp, rd.lightPdf) / lsp);
                 }
-                f3 o2 = computeRayOrigin(sd2.posW, dot(sd2.faceN, rd.secondWo) >= 0.f ? sd2.faceN : -sd2.faceN);
-                HitInfo h; float t;
-                if (trace_closest(C.bvh, mk_ray(o2, rd.secondWo, 0.f, kRayTMax), h, t, C.fault))
-                    emitter = dev_emitter_of(C, dev_sd(C, h, rd.secondWo));
-                // a light sample whose ray slips through the seam between two triangles of the light
-                if (emitter == kInvalidIndex && rd.lightIsNEE) emitter = emissive_material_with_radiance(C.lights, rd.irradiance);
+                if (!rd.lightIsDistant)
+                {
+                    f3 o2 = computeRayOrigin(sd2.posW, dot(sd2.faceN, rd.secondWo) >= 0.f ? sd2.faceN : -sd2.faceN);
+                    HitInfo h; float t;
+                    if (trace_closest(C.bvh, mk_ray(o2, rd.secondWo, 0.f, kRayTMax), h, t, C.fault))
+                        emitter = dev_emitter_of(C, dev_sd(C, h, rd.secondWo));
+                    // a light sample whose ray slips through the seam between two triangles of the light
+                    if (emitter == kInvalidIndex && rd.lightIsNEE) emitter = emissive_material_with_radiance(C.lights, rd.irradiance);
+                }
             }
         }
     }
@@ -269,7 +305,8 @@ __device__ inline void adj_pixel(const DevCtx& C, const ResPlanes& res, const Re
     const f3 k = mk3(value.x != 0.f ? r.integrand.x / value.x : 1.f, value.y != 0.f ? r.integrand.y / value.y : 1.f,
                      value.z != 0.f ? r.integrand.z / value.z : 1.f);
     atomicAdd(cnt + kAdjReplayed, 1u);
-    if (emitter == kInvalidIndex) atomicAdd(cnt + kAdjNoEmitter, 1u);
+    // a path that ends at the environment map carries its radiance, no material's
+    if (emitter == kInvalidIndex && !rd.lightIsDistant) atomicAdd(cnt + kAdjNoEmitter, 1u);
     // a suffix path's value is checked through the record's irradiance (the replayed suffix radiance
     // equals it bit for bit); the suffix's densities and MIS weights fall into k
     const f3 check = rd.pathLength > 3 ? V[0].value * V[1].value * rd.irradiance * s : value;

@@ -1343,8 +1343,8 @@ extern "C" RS_API rs_status rs_backward(rs_pass* p, const void* checkpoint, cons
 {
     if (!p || !gradColor || !gradMaterials) return fail(RS_INVALID_ARG, "pass, gradColor or gradMaterials is NULL");
     if (!p->hasScene || !p->haveFrameCtx) return fail(RS_NOT_READY, "rs_backward needs a rendered frame");
-    if (p->envHost.present) return fail(RS_INVALID_ARG, "rs_backward differentiates scenes lit by emissive triangles; the pass has an env map");
-    if (p->numAnalytic) return fail(RS_INVALID_ARG, "rs_backward differentiates scenes lit by emissive triangles; the pass has analytic lights");
+    if (p->numAnalytic)
+        return fail(RS_INVALID_ARG, "rs_backward differentiates scenes lit by emissive triangles and an env map; the pass has analytic lights");
     for (const MaterialData& m : p->scene.materials)
         if (m.flags & kMtlSpecGloss)
             return fail(RS_INVALID_ARG, "rs_backward differentiates metal-rough materials; the scene has a spec-gloss material");

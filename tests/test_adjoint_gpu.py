@@ -42,14 +42,21 @@ def _richardson(f, x, h=1e-3):
 
 
 @pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
-@pytest.mark.parametrize("case,bounces", [("inverse_scene", 1), ("inverse_scene", 2), ("cornell", 2), ("cornell", 3)])
-def test_backward_matches_oracle_and_fp64_differences(rs, oracle_mod, scenes, case, bounces):
+@pytest.mark.parametrize("case,bounces,env", [("inverse_scene", 1, False), ("inverse_scene", 2, False), ("cornell", 2, False),
+                                              ("cornell", 3, False), ("inverse_scene", 2, True), ("cornell", 3, True)])
+def test_backward_matches_oracle_and_fp64_differences(rs, oracle_mod, scenes, case, bounces, env):
     """With more than one bounce, paths of four and five vertices are differentiated through the
-    suffix replay from x3; none is skipped, and the replayed suffix radiance is the record's."""
+    suffix replay from x3; none is skipped, and the replayed suffix radiance is the record's.  With
+    an environment map, the paths that end at it carry its radiance (held fixed) and have no emitter
+    material, and the suffix replay's light-type selection takes the env branch too."""
     import torch
     W = H = 64 if case == "inverse_scene" else 40
     props = dict(PROPS, maxSurfaceBounces=bounces)
     sc, gpu, ora, mats = _setup(rs, oracle_mod, scenes, W, H, props, None if case == "inverse_scene" else scenes.cornell_box(0))
+    if env:
+        sky = scenes.sky_env_map(64, 32, seed=3)
+        gpu.set_env_map(sky)
+        ora.set_env_map(sky)
     camera = scenes.translate_camera if case == "inverse_scene" else scenes.cornell_camera
     rng = np.random.default_rng(2)
     n = len(mats)
