@@ -360,7 +360,9 @@ RS_API rs_status rs_debug_stage_rays(rs_pass* pass, uint64_t* rays, uint32_t* co
  * counters and flags its record saved there (word 27 and bits 15-26 of word 5), which needs the
  * TinyUniform generator; paths past x2 with a delta lobe, or of more than 8 BSDF vertices, are
  * skipped and counted.  The scene may be lit by emissive triangles and an environment map, whose
- * radiance is held fixed (no analytic lights); metallic and ior are not differentiated.
+ * radiance is held fixed (no analytic lights); metallic and ior are not differentiated.  For a
+ * spec-gloss material baseColor is its diffuse colour and the roughness slot its glossiness; its
+ * specular colour is held fixed.
  *
  *   rs_set_materials   replace material parameters in place (same count; geometry and BVH stay)
  *   rs_checkpoint      copy the last frame's final reservoirs to caller device memory

@@ -212,10 +212,16 @@ class OraclePass:
         return float(self._lib.ro_replay_loss(self._h, t.ctypes.data, q.ctypes.data, len(q)))
 
 
-def bsdf_grad(material, wi, wo, lobe_mask: int = 0):
-    """(value, dBase, dRough) in FP32 and the FP64 value, for the BSDF derivative check."""
+def bsdf_grad(material, wi, wo, lobe_mask: int = 0, specular=None):
+    """(value, dBase, dRough) in FP32 and the FP64 value, for the BSDF derivative check.  material:
+    baseColor.xyz, roughness, metallic, ior; with `specular` (a colour) the material is spec-gloss
+    and material[3] its glossiness."""
     lib = load()
-    m = np.asarray(material, np.float32)
+    m = np.zeros(10, np.float32)
+    m[:len(material)] = material
+    if specular is not None:
+        m[6] = 1.0
+        m[7:10] = specular
     a, b = np.asarray(wi, np.float32), np.asarray(wo, np.float32)
     out = np.zeros(9, np.float32)
     vd = np.zeros(3, np.float64)

@@ -2178,7 +2178,7 @@ static ReplayVertex replay_vertex(const Pass& p, const ShadingData& sd, uint32_t
     uint32_t mask = lobeMask == 0 ? 0xfu : lobeMask;
     v.diffuseOn = b.pDiffuseReflection > 0.f && (mask & 0x1u);
     v.specularOn = b.pSpecularReflection > 0.f && (mask & 0x4u) && b.alpha != 0.f;
-    v.g = mi_eval_grad(sd, d, lobeMask, wo);
+    v.g = mi_eval_grad(sd, d, lobeMask, wo, (p.scene.materials[sd.materialID].flags & kMtlSpecGloss) != 0);
     return v;
 }
 
@@ -2424,15 +2424,19 @@ static void replay_accumulate(const Replay& q, f3 gradColor, double* grad)
 // FP64 material parameters of the replay: baseColor.xyz, roughness, emissive.xyz, metallic.
 struct ParamsFp64 { double v[kGradStride]; };
 
-static void replay_vertex_fp64(const ReplayVertex& v, const ParamsFp64& q, float ior, double out[3])
+// Spec-gloss materials (kMtlSpecGloss): the diffuse albedo is baseColor, the specular colour the
+// material's own, and the roughness 1 - the stored glossiness (setup_material).
+static void replay_vertex_fp64(const ReplayVertex& v, const ParamsFp64& q, const MaterialData& mat, double out[3])
 {
+    const bool specGloss = (mat.flags & kMtlSpecGloss) != 0;
+    const float ior = mat.ior;
     out[0] = out[1] = out[2] = 0.0;
     if (!v.valid) return;
     const double wi[3] = {v.wi.x, v.wi.y, v.wi.z}, wo[3] = {v.wo.x, v.wo.y, v.wo.z};
     double h[3] = {wi[0] + wo[0], wi[1] + wo[1], wi[2] + wo[2]};
     double hl = std::sqrt(h[0] * h[0] + h[1] * h[1] + h[2] * h[2]);
     for (double& x : h) x /= hl;
-    const double r = q.v[kGradRough], metal = q.v[7];
+    const double r = specGloss ? 1.0 - q.v[kGradRough] : q.v[kGradRough], metal = q.v[7];
     const double kPiD = 3.14159265358979323846;
     if (v.diffuseOn)
     {
@@ -2441,7 +2445,7 @@ static void replay_vertex_fp64(const ReplayVertex& v, const ParamsFp64& q, float
         double fd90 = 0.5 * r + 2.0 * woDotH * woDotH * r;
         double Pi = std::pow(std::max(1.0 - wi[2], 0.0), 5.0), Po = std::pow(std::max(1.0 - wo[2], 0.0), 5.0);
         double S = (1.0 + (fd90 - 1.0) * Pi) * (1.0 + (fd90 - 1.0) * Po) * E / kPiD * wo[2];
-        for (int c = 0; c < 3; c++) out[c] += q.v[kGradBase + c] * (1.0 - metal) * S;
+        for (int c = 0; c < 3; c++) out[c] += q.v[kGradBase + c] * (specGloss ? 1.0 : 1.0 - metal) * S;
     }
     if (v.specularOn)
     {
@@ -2457,7 +2461,7 @@ static void replay_vertex_fp64(const ReplayVertex& v, const ParamsFp64& q, float
         double F0 = f * f;
         for (int k = 0; k < 3; k++)
         {
-            double spec = F0 + (q.v[kGradBase + k] - F0) * metal;
+            double spec = specGloss ? (double)mat.specular[k] : F0 + (q.v[kGradBase + k] - F0) * metal;
             out[k] += (spec + (1.0 - spec) * P) * D * G * 0.25 / wi[2];
         }
     }
@@ -2481,8 +2485,8 @@ static void replay_fp64(const Replay& q, const ParamsFp64* params, const Materia
     {
         const uint32_t m = q.v[k].material;
         double a[3], a0[3];
-        replay_vertex_fp64(q.v[k], params[m], mats[m].ior, a);
-        replay_vertex_fp64(q.v[k], params_of(mats[m]), mats[m].ior, a0);
+        replay_vertex_fp64(q.v[k], params[m], mats[m], a);
+        replay_vertex_fp64(q.v[k], params_of(mats[m]), mats[m], a0);
         for (int c = 0; c < 3; c++) { F[c] *= a[c]; F0[c] *= a0[c]; }
     }
     double Le[3] = {q.Le.x, q.Le.y, q.Le.z}, Le0[3] = {q.Le.x, q.Le.y, q.Le.z};
@@ -2897,6 +2901,11 @@ __attribute__((visibility("default"))) void ro_test_bsdf_grad(const float* mat, 
     memset(&m, 0, sizeof(m));
     m.baseColor[0] = mat[0]; m.baseColor[1] = mat[1]; m.baseColor[2] = mat[2];
     m.roughness = mat[3]; m.metallic = mat[4]; m.ior = mat[5];
+    if (mat[6] != 0.f) // spec-gloss: mat[3] is the glossiness, mat[7..9] the specular colour
+    {
+        m.flags = kMtlSpecGloss;
+        m.specular[0] = mat[7]; m.specular[1] = mat[8]; m.specular[2] = mat[9];
+    }
     ShadingData sd;
     memset(&sd, 0, sizeof(sd));
     sd.N = mk3(0.f, 0.f, 1.f); sd.T = mk3(1.f, 0.f, 0.f); sd.B = mk3(0.f, 1.f, 0.f); sd.faceN = sd.N;
@@ -2904,7 +2913,7 @@ __attribute__((visibility("default"))) void ro_test_bsdf_grad(const float* mat, 
     sd.frontFacing = true;
     f3 w = mk3(wo[0], wo[1], wo[2]);
     BsdfData d = setup_material(m, true);
-    BsdfGrad g = mi_eval_grad(sd, d, lobeMask, w);
+    BsdfGrad g = mi_eval_grad(sd, d, lobeMask, w, (m.flags & kMtlSpecGloss) != 0);
     const f3 v[3] = {g.value, g.dBase, g.dRough};
     for (int k = 0; k < 3; k++) { out[3 * k] = v[k].x; out[3 * k + 1] = v[k].y; out[3 * k + 2] = v[k].z; }
     oracle::ParamsFp64 q64;
@@ -2920,7 +2929,7 @@ __attribute__((visibility("default"))) void ro_test_bsdf_grad(const float* mat, 
     uint32_t mask = lobeMask == 0 ? 0xfu : lobeMask;
     rv.diffuseOn = b.pDiffuseReflection > 0.f && (mask & 0x1u);
     rv.specularOn = b.pSpecularReflection > 0.f && (mask & 0x4u) && b.alpha != 0.f;
-    oracle::replay_vertex_fp64(rv, q64, m.ior, valueFp64);
+    oracle::replay_vertex_fp64(rv, q64, m, valueFp64);
 }
 
 // ---- BSDF property hooks (the sampling test of Tests/Scene/Material/BSDFTests.cpp restated on the

@@ -43,6 +43,12 @@ __device__ __forceinline__ void adj_add(double* acc, uint32_t idx, float v)
     if (v != 0.f) atomicAdd(acc + idx, (double)v);
 }
 
+// Spec-gloss materials map their parameters onto the BSDF differently (material_grad.h).
+__device__ __forceinline__ bool adj_spec_gloss(const DevCtx& C, const ShadingData& sd)
+{
+    return (C.materials[sd.materialID].flags & kMtlSpecGloss) != 0;
+}
+
 __device__ __forceinline__ bool adj_finished(const DevCtx& C, uint32_t bounces) // finished_bounces
 {
     uint32_t d = bounces & 0xffu, sp = (bounces >> 8) & 0xffu, t = (bounces >> 16) & 0xffu;
@@ -144,7 +150,7 @@ __device__ __noinline__ bool adj_replay_suffix(const DevCtx& C, const Recon& rd,
                     {
                         if (nv == kAdjMaxFactors) return false;
                         mat[nv] = sd.materialID;
-                        V[nv++] = mi_eval_grad(sd, d, 0u, lsDir);
+                        V[nv++] = mi_eval_grad(sd, d, 0u, lsDir, adj_spec_gloss(C, sd));
                         S = thp * Lr;
                         Le = lsLi * lsPdf;
                         emitter = lsEnv ? kInvalidIndex
@@ -172,7 +178,7 @@ __device__ __noinline__ bool adj_replay_suffix(const DevCtx& C, const Recon& rd,
         else if (specOrDelta) comp = 2;
         if (!valid || (result.lobeType & kLobeDelta) || (comp != 0 && comp != 2) || nv == kAdjMaxFactors) return false;
         mat[nv] = sd.materialID;
-        V[nv++] = mi_eval_grad(sd, d, 1u << comp, result.wo);
+        V[nv++] = mi_eval_grad(sd, d, 1u << comp, result.wo, adj_spec_gloss(C, sd));
         dir = result.wo;
         thp *= result.weight;
         flags &= ~(4u | kPSpecular | kPDelta);
@@ -237,13 +243,13 @@ __device__ inline void adj_pixel(const DevCtx& C, const ResPlanes& res, const Re
             float lightPdf = rd.lightPdf / jac;
             if (rd.lightIsNEE)
             {
-                V[0] = mi_eval_grad(sd1, d1, 0u, dir);
+                V[0] = mi_eval_grad(sd1, d1, 0u, dir, adj_spec_gloss(C, sd1));
                 if (!any_gt0(V[0].value) || totalPdf == 0.f) return;
                 s = dev_mis(C, lightPdf, totalPdf) / lightPdf;
             }
             else
             {
-                V[0] = mi_eval_grad(sd1, d1, mask1, dir);
+                V[0] = mi_eval_grad(sd1, d1, mask1, dir, adj_spec_gloss(C, sd1));
                 if (!any_gt0(V[0].value) || lobePdf == 0.f) return;
                 s = dev_mis(C, totalPdf, lightPdf) / lobePdf;
             }
@@ -252,7 +258,7 @@ __device__ inline void adj_pixel(const DevCtx& C, const ResPlanes& res, const Re
         }
         else
         {
-            V[0] = mi_eval_grad(sd1, d1, mask1, dir);
+            V[0] = mi_eval_grad(sd1, d1, mask1, dir, adj_spec_gloss(C, sd1));
             if (!any_gt0(V[0].value) || lobePdf == 0.f) return;
             ShadingData sd2 = dev_sd(C, rd.secondHit, dir);
             BsdfData d2 = dev_instance(C, sd2);
@@ -266,7 +272,7 @@ __device__ inline void adj_pixel(const DevCtx& C, const ResPlanes& res, const Re
                 // pathReconnectionShift's lobe-specific x2 term; the suffix follows from x3
                 if (!(lsp > 0.f)) return;
                 if (C.sgKind != kSgTinyUniform) { atomicAdd(cnt + kAdjSkipped, 1u); return; }
-                V[1] = mi_eval_grad(sd2, d2, mask2, rd.secondWo);
+                V[1] = mi_eval_grad(sd2, d2, mask2, rd.secondWo, adj_spec_gloss(C, sd2));
                 s = (1.f / lobePdf) * (1.f / lsp);
                 f3 S;
                 if (!adj_replay_suffix(C, rd, sd2, nv, mat, V, emitter, Le, S)) { atomicAdd(cnt + kAdjSkipped, 1u); return; }
@@ -276,13 +282,13 @@ __device__ inline void adj_pixel(const DevCtx& C, const ResPlanes& res, const Re
             {
                 if (rd.lightIsNEE)
                 {
-                    V[1] = mi_eval_grad(sd2, d2, 0xFu, rd.secondWo);
+                    V[1] = mi_eval_grad(sd2, d2, 0xFu, rd.secondWo, adj_spec_gloss(C, sd2));
                     s = (1.f / lobePdf) * (dev_mis(C, rd.lightPdf, tp) / rd.lightPdf);
                 }
                 else
                 {
                     if (!(lsp > 0.f)) return;
-                    V[1] = mi_eval_grad(sd2, d2, mask2, rd.secondWo);
+                    V[1] = mi_eval_grad(sd2, d2, mask2, rd.secondWo, adj_spec_gloss(C, sd2));
                     s = (1.f / lobePdf) * (dev_mis(C, tp, rd.lightPdf) / lsp);
                 }
                 if (!rd.lightIsDistant)

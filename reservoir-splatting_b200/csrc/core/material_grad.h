@@ -1,11 +1,14 @@
 // Derivatives of the StandardBSDF evaluation (material.h) with respect to the
-// metal-rough material parameters that the path-replay adjoint differentiates:
-// baseColor (per channel) and roughness.  metallic and ior are held fixed.
+// material parameters that the path-replay adjoint differentiates: baseColor (per
+// channel) and the roughness slot.  metallic, ior and the specular colour are held fixed.
 //
 // With metallic m and F0 = ((ior - 1) / (ior + 1))^2 (StandardMaterial.slang:48-115):
 //   diffuse albedo  = baseColor * (1 - m)          d/d baseColor.c = (1 - m)
 //   specular colour = F0 + (baseColor - F0) * m    d/d baseColor.c = m
 //   GGX alpha       = max(roughness^2, 0.0064)     d/d roughness   = 2 * roughness above the clamp
+// Spec-gloss (kMtlSpecGloss, ShadingUtils.slang:57-71): diffuse albedo = baseColor (d/d baseColor.c
+//   = 1), specular colour = the material's specular (no baseColor term), roughness = 1 - the stored
+//   glossiness (d/d slot = -d/d roughness); its derived metallic only sets the lobe probabilities.
 // Frostbite diffuse (FrostbiteDiffuseBRDF.slang): albedo * Fi * Fo * E / pi * cos(wo) with
 //   fd90 = 0.5 r + 2 (wo.h)^2 r, F(c) = 1 + (fd90 - 1) (1 - c)^5, E = 1 + (1/1.51 - 1) r.
 // GGX reflection (SpecularMicrofacet.slang:49-200): F * D * G / (4 cos(wi)) with
@@ -35,7 +38,7 @@ RS_HD float ggx_tan2(f3 w)
 // cancellation (the GGX denominator as sin^2 + cos^2 alpha^2 of the half vector, Smith's Lambda as
 // x / (2 (sqrt(1 + x) + 1))), so near a sharp specular peak it is more accurate than the pass's own
 // float evaluation; both agree wherever that one is well conditioned.
-RS_HD BsdfGrad mi_eval_grad(const ShadingData& sd, const BsdfData& d, uint32_t lobeMask, f3 wo)
+RS_HD BsdfGrad mi_eval_grad(const ShadingData& sd, const BsdfData& d, uint32_t lobeMask, f3 wo, bool specGloss = false)
 {
     BsdfGrad g;
     g.value = mk3(0.f); g.dBase = mk3(0.f); g.dRough = mk3(0.f);
@@ -61,7 +64,7 @@ RS_HD BsdfGrad mi_eval_grad(const ShadingData& sd, const BsdfData& d, uint32_t l
         float dfd90 = 0.5f + 2.f * woDotH * woDotH;
         float dS = (dfd90 * (Pi * Fo + Fi * Po) * E + Fi * Fo * (1.f / 1.51f - 1.f)) * k;
         g.value += b.diffAlbedo * S;
-        g.dBase += mk3((1.f - d.metallic) * S);
+        g.dBase += mk3(specGloss ? S : (1.f - d.metallic) * S);
         g.dRough += b.diffAlbedo * dS;
     }
     if (b.pSpecularReflection > 0.f && (mask & 0x4u) && b.alpha != 0.f)
@@ -80,11 +83,12 @@ RS_HD BsdfGrad mi_eval_grad(const ShadingData& sd, const BsdfData& d, uint32_t l
         f3 F = b.specAlbedo + (mk3(1.f) - b.specAlbedo) * P;
         float k = 0.25f / wi.z;
         g.value += F * (D * G * k);
-        g.dBase += mk3(d.metallic * (1.f - P) * D * G * k);
+        if (!specGloss) g.dBase += mk3(d.metallic * (1.f - P) * D * G * k);
         float r = d.roughness;
         float dAlpha = (lobeMask != 5u && r * r > kMinGGXAlpha) ? 2.f * r : 0.f;
         g.dRough += F * (k * (dD * G + D * dG) * 2.f * a * dAlpha);
     }
+    if (specGloss) g.dRough = -g.dRough;
     return g;
 }
 

@@ -1345,9 +1345,6 @@ extern "C" RS_API rs_status rs_backward(rs_pass* p, const void* checkpoint, cons
     if (!p->hasScene || !p->haveFrameCtx) return fail(RS_NOT_READY, "rs_backward needs a rendered frame");
     if (p->numAnalytic)
         return fail(RS_INVALID_ARG, "rs_backward differentiates scenes lit by emissive triangles and an env map; the pass has analytic lights");
-    for (const MaterialData& m : p->scene.materials)
-        if (m.flags & kMtlSpecGloss)
-            return fail(RS_INVALID_ARG, "rs_backward differentiates metal-rough materials; the scene has a spec-gloss material");
     cudaStream_t s = static_cast<cudaStream_t>(streamPtr);
     const size_t N = (size_t)p->W * p->H;
     if (!p->adjStats.p)

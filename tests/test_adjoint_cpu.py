@@ -21,11 +21,18 @@ def _richardson(f, x, h=1e-3):
     return (4 * _cd(f, x, h / 2) - _cd(f, x, h)) / 3
 
 
-def test_bsdf_derivatives_match_fp64_differences(oracle_mod):
+@pytest.mark.parametrize("model", ["metal_rough", "spec_gloss"])
+def test_bsdf_derivatives_match_fp64_differences(oracle_mod, model):
+    """Spec-gloss: baseColor is the diffuse albedo, the specular colour is held fixed and the
+    roughness slot holds the glossiness (roughness = 1 - slot)."""
     rng = np.random.default_rng(0)
     worst = 0.0
     for _ in range(300):
         mat = np.array([*rng.uniform(0.05, 0.95, 3), rng.uniform(0.12, 0.95), rng.choice([0.0, 0.3, 1.0]), 1.5])
+        spec = None
+        if model == "spec_gloss":
+            mat[3] = 1.0 - mat[3]
+            spec = rng.uniform(0.02, 0.9, 3)
 
         def unit():
             v = rng.normal(size=3)
@@ -34,7 +41,7 @@ def test_bsdf_derivatives_match_fp64_differences(oracle_mod):
 
         wi, wo = unit(), unit()
         mask = int(rng.choice([0, 1, 4, 0xF]))
-        value, d_base, d_rough, value64 = oracle_mod.bsdf_grad(mat, wi, wo, mask)
+        value, d_base, d_rough, value64 = oracle_mod.bsdf_grad(mat, wi, wo, mask, spec)
         scale = max(np.abs(value64).max(), 1e-9)
         assert np.abs(value - value64).max() <= 1e-5 * scale
 
@@ -42,7 +49,7 @@ def test_bsdf_derivatives_match_fp64_differences(oracle_mod):
             def f(x):
                 m = mat.copy()
                 m[k] = x
-                return oracle_mod.bsdf_grad(m, wi, wo, mask)[3]
+                return oracle_mod.bsdf_grad(m, wi, wo, mask, spec)[3]
             return f
 
         fd_base = np.array([_richardson(val(c), mat[c])[c] for c in range(3)])
@@ -148,6 +155,30 @@ def test_oracle_replay_gradient_with_an_env_map(oracle_mod, scenes, case, bounce
     else:
         sc = scenes.inverse_scene(grid=64, spheres=6, subdiv=2)
         err, stats, G, FD, long_paths = _replay_check(oracle_mod, sc, scenes.translate_camera, 40, 40, 3, props, env=sky)
+    assert stats[0] > 0 and stats[1] == 0 and stats[2] == 0
+    assert err < GRAD_TOL, err
+    big = np.abs(FD) > 1e-2 * np.abs(FD).max()
+    assert (np.abs(G - FD)[big] / np.abs(FD)[big]).max() < GRAD_TOL
+
+
+@pytest.mark.parametrize("bounces", [1, 2])
+def test_oracle_replay_gradient_spec_gloss(oracle_mod, scenes, tmp_path, bounces):
+    """The Cornell box through the OBJ importer, whose materials are spec-gloss (Falcor's OBJ
+    model): the diffuse colour and the glossiness slot are differentiated, the specular colour is
+    held fixed; the replay gradient matches FP64 differences."""
+    import reservoir_splatting_b200.importers as I
+    sc = scenes.cornell_box(0)
+    I.save_obj(sc, tmp_path / "cb.obj", ["white", "red", "green", "light"],
+               {"white": {"Kd": (0.7, 0.7, 0.7), "Ks": (0.05, 0.05, 0.05), "Ns": 30.0},
+                "red": {"Kd": (0.6, 0.05, 0.05), "Ks": (0.3, 0.3, 0.3), "Ns": 400.0},
+                "green": {"Kd": (0.1, 0.4, 0.1), "Ks": (0.02, 0.02, 0.02), "Ns": 5.0},
+                "light": {"Kd": (0, 0, 0), "Ke": (17, 12, 4)}})
+    imported = I.load_obj(tmp_path / "cb.obj")
+    flags = np.array(imported.materials, np.float32).reshape(len(imported.materials), -1)[:, 9].view(np.uint32)
+    assert np.all((flags & 2) != 0)  # kMtlSpecGloss
+    props = {"temporalReuse": "ScatterBackup", "gatherOption": "Clamped", "maxSurfaceBounces": bounces,
+             "enableSpatialResampling": True}
+    err, stats, G, FD, long_paths = _replay_check(oracle_mod, imported, scenes.cornell_camera, 32, 32, 3, props)
     assert stats[0] > 0 and stats[1] == 0 and stats[2] == 0
     assert err < GRAD_TOL, err
     big = np.abs(FD) > 1e-2 * np.abs(FD).max()

@@ -226,7 +226,8 @@ def test_imported_pyscene_with_hdr_environment(rs, oracle_mod, scenes, tmp_path)
 def test_imported_obj_spec_gloss_scene(rs, oracle_mod, scenes, tmp_path, mode):
     """A Cornell box written as OBJ + MTL and imported with the Assimp importer's OBJ mapping:
     spec-gloss materials (diffuse, specular colour, glossiness from the Phong exponent, derived
-    metallic), shaded the same on the GPU and in the oracle.  The adjoint rejects the scene."""
+    metallic), shaded the same on the GPU and in the oracle.  The adjoint differentiates its diffuse
+    colours and glossiness like the oracle's replay."""
     import torch
     import reservoir_splatting_b200.importers as I
     sc = scenes.cornell_box(0)
@@ -238,13 +239,20 @@ def test_imported_obj_spec_gloss_scene(rs, oracle_mod, scenes, tmp_path, mode):
     imported = I.load_obj(tmp_path / "cb.obj")
     props = {"temporalReuse": mode, "gatherOption": "Clamped", "maxSurfaceBounces": 2, "enableSpatialResampling": True}
     run_pair(rs, oracle_mod, imported, scenes.cornell_camera, props, frames=4)
-    p = rs.ReservoirSplatting(dict(props, maxSurfaceBounces=1), W, H)
+    p = rs.ReservoirSplatting(props, W, H)
     p.set_scene(imported)
-    p.render(scenes.cornell_camera(0, W, H))
-    g = torch.zeros((H, W, 4), device="cuda")
+    ora = oracle_mod.OraclePass(props, W, H)
+    ora.set_scene(imported)
+    img = p.render(scenes.cornell_camera(0, W, H))
+    np.testing.assert_array_equal(img, ora.execute(scenes.cornell_camera(0, W, H)))
+    gc = np.random.default_rng(5).uniform(-1.0, 1.0, img.shape).astype(np.float32)
     gm = torch.zeros((len(imported.materials), 8), device="cuda")
-    with pytest.raises(rs.RsError, match="spec-gloss"):
-        p.backward(g.data_ptr(), gm.data_ptr())
+    p.backward(torch.from_numpy(gc).cuda().data_ptr(), gm.data_ptr())
+    torch.cuda.synchronize()
+    O, ost = ora.backward(gc, len(imported.materials))
+    st = p.backward_stats()
+    assert st[0] > 0 and st[0] == ost[0] and st[1] == 0 and st[2] == 0
+    assert np.abs(gm.cpu().numpy() - O).max() <= 1e-4 * np.abs(O).max()
     p.close()
 
 
