@@ -352,21 +352,21 @@ RS_API rs_status rs_debug_stage_rays(rs_pass* pass, uint64_t* rays, uint32_t* co
  *
  * A pixel's colour is f(y) * W, y being the path its final reservoir selected.  rs_backward holds
  * each pixel's y, W, sampling densities and MIS weights at their rendered values and
- * differentiates f(y) with respect to every material's baseColor (per channel), roughness and
- * emissive radiance (per channel).  E[df(y)/dtheta * W] is the derivative of the pixel integral, so
+ * differentiates f(y) with respect to every material's baseColor (per channel), roughness, metallic
+ * and emissive radiance (per channel).  E[df(y)/dtheta * W] is the derivative of the pixel integral, so
  * the gradient is unbiased.  Only the final reservoirs of a frame are needed: rs_checkpoint copies
  * them (rs_checkpoint_bytes = 144 bytes per pixel) and rs_backward recomputes the rest.  A path of
  * four or more vertices is re-run from its third vertex with the sample-generator state, bounce
  * counters and flags its record saved there (word 27 and bits 15-26 of word 5), which needs the
  * TinyUniform generator; paths past x2 with a delta lobe, or of more than 8 BSDF vertices, are
  * skipped and counted.  The scene may be lit by emissive triangles and an environment map, whose
- * radiance is held fixed (no analytic lights); metallic and ior are not differentiated.  For a
- * spec-gloss material baseColor is its diffuse colour and the roughness slot its glossiness; its
- * specular colour is held fixed.
+ * radiance is held fixed (no analytic lights); ior is not differentiated.  For a spec-gloss
+ * material baseColor is its diffuse colour and the roughness slot its glossiness; its specular
+ * colour is held fixed and its metallic slot gets no gradient.
  *
  *   rs_set_materials   replace material parameters in place (same count; geometry and BVH stay)
  *   rs_checkpoint      copy the last frame's final reservoirs to caller device memory
- *   rs_backward        gradMaterials[m * 8 + k] += d loss / d (baseColor.xyz, roughness, emissive.xyz, -)
+ *   rs_backward        gradMaterials[m * 8 + k] += d loss / d (baseColor.xyz, roughness, emissive.xyz, metallic)
  *                      for d loss / d colour `gradColor` (device float4 per pixel); checkpoint NULL
  *                      means the last frame; the materials must be those the frame used
  *   rs_backward_stats  read and clear {paths replayed, paths skipped, emitter not found, value mismatch} */

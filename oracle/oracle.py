@@ -213,7 +213,8 @@ class OraclePass:
 
 
 def bsdf_grad(material, wi, wo, lobe_mask: int = 0, specular=None):
-    """(value, dBase, dRough) in FP32 and the FP64 value, for the BSDF derivative check.  material:
+    """(value, dBase, dRough) in FP32, the FP64 value and dMetal in FP32, for the BSDF derivative
+    check.  material:
     baseColor.xyz, roughness, metallic, ior; with `specular` (a colour) the material is spec-gloss
     and material[3] its glossiness."""
     lib = load()
@@ -223,7 +224,7 @@ def bsdf_grad(material, wi, wo, lobe_mask: int = 0, specular=None):
         m[6] = 1.0
         m[7:10] = specular
     a, b = np.asarray(wi, np.float32), np.asarray(wo, np.float32)
-    out = np.zeros(9, np.float32)
+    out = np.zeros(12, np.float32)
     vd = np.zeros(3, np.float64)
     lib.ro_test_bsdf_grad(m.ctypes.data, a.ctypes.data, b.ctypes.data, lobe_mask, out.ctypes.data, vd.ctypes.data)
-    return out[0:3], out[3:6], out[6:9], vd
+    return out[0:3], out[3:6], out[6:9], vd, out[9:12]

@@ -2178,7 +2178,7 @@ static ReplayVertex replay_vertex(const Pass& p, const ShadingData& sd, uint32_t
     uint32_t mask = lobeMask == 0 ? 0xfu : lobeMask;
     v.diffuseOn = b.pDiffuseReflection > 0.f && (mask & 0x1u);
     v.specularOn = b.pSpecularReflection > 0.f && (mask & 0x4u) && b.alpha != 0.f;
-    v.g = mi_eval_grad(sd, d, lobeMask, wo, (p.scene.materials[sd.materialID].flags & kMtlSpecGloss) != 0);
+    v.g = mi_eval_grad(sd, d, p.scene.materials[sd.materialID], lobeMask, wo);
     return v;
 }
 
@@ -2412,9 +2412,11 @@ static void replay_accumulate(const Replay& q, f3 gradColor, double* grad)
         f3 common = g * (before[k] * after) * q.Le * q.s;
         f3 dB = common * v.g.dBase;
         f3 dR = common * v.g.dRough;
+        f3 dM = common * v.g.dMetal;
         double* m = grad + (size_t)v.material * kGradStride;
         m[kGradBase + 0] += dB.x; m[kGradBase + 1] += dB.y; m[kGradBase + 2] += dB.z;
         m[kGradRough] += (double)dR.x + (double)dR.y + (double)dR.z;
+        m[kGradMetal] += (double)dM.x + (double)dM.y + (double)dM.z;
         after = after * v.g.value;
     }
 }
@@ -2891,9 +2893,10 @@ __attribute__((visibility("default"))) double ro_test_alias(const float* w, uint
     for (uint32_t i = 0; i < n; i++) { table[2 * i] = t[i].x; table[2 * i + 1] = t[i].y; }
     return sum;
 }
-// BSDF derivative check: material = (baseColor.xyz, roughness, metallic, ior), directions in the
-// local frame (normal +z).  out = value.xyz, dBase.xyz, dRough.xyz (FP32 analytic); valueFp64 = the
-// FP64 value at the same parameters (for central differences).
+// BSDF derivative check: material = (baseColor.xyz, roughness, metallic, ior, spec-gloss flag,
+// specular.xyz), directions in the local frame (normal +z).  out = value.xyz, dBase.xyz, dRough.xyz,
+// dMetal.xyz (FP32 analytic); valueFp64 = the FP64 value at the same parameters (for central
+// differences).
 __attribute__((visibility("default"))) void ro_test_bsdf_grad(const float* mat, const float* wi, const float* wo, uint32_t lobeMask,
                                                              float* out, double* valueFp64)
 {
@@ -2913,9 +2916,9 @@ __attribute__((visibility("default"))) void ro_test_bsdf_grad(const float* mat, 
     sd.frontFacing = true;
     f3 w = mk3(wo[0], wo[1], wo[2]);
     BsdfData d = setup_material(m, true);
-    BsdfGrad g = mi_eval_grad(sd, d, lobeMask, w, (m.flags & kMtlSpecGloss) != 0);
-    const f3 v[3] = {g.value, g.dBase, g.dRough};
-    for (int k = 0; k < 3; k++) { out[3 * k] = v[k].x; out[3 * k + 1] = v[k].y; out[3 * k + 2] = v[k].z; }
+    BsdfGrad g = mi_eval_grad(sd, d, m, lobeMask, w);
+    const f3 v[4] = {g.value, g.dBase, g.dRough, g.dMetal};
+    for (int k = 0; k < 4; k++) { out[3 * k] = v[k].x; out[3 * k + 1] = v[k].y; out[3 * k + 2] = v[k].z; }
     oracle::ParamsFp64 q64;
     for (int k = 0; k < 8; k++) q64.v[k] = 0.0;
     for (int k = 0; k < 3; k++) q64.v[kGradBase + k] = mat[k];

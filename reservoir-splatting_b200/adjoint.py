@@ -4,10 +4,12 @@
 pass and is differentiable with respect to `params`, a (materials x 8) float32 tensor in the order
 baseColor.xyz, roughness, emissive.xyz, metallic (the layout of the first eight floats of a material
 record).  Forward keeps one checkpoint per frame (the final reservoirs, 144 bytes per pixel); backward
-calls rs_backward once per frame with that frame's checkpoint and d loss / d image.  metallic is an
-input only: its gradient is zero.
+calls rs_backward once per frame with that frame's checkpoint and d loss / d image.  Every column is
+differentiated; for a spec-gloss material the baseColor columns are its diffuse colour, the roughness
+column its glossiness, and its metallic column (derived from its colours) gets no gradient.
 
-The estimator and its conditions (paths of at most three vertices) are those of rs_backward.
+The estimator and its conditions (emissive triangles and an environment map, no analytic lights;
+the TinyUniform generator for paths of four or more vertices) are those of rs_backward.
 """
 from __future__ import annotations
 

@@ -3,8 +3,8 @@
 // A pixel's colour is f(y) * W (ResolveReSTIR.cs.slang:45-63), y being the path its final
 // reservoir selected.  k_backward holds y, W, the sampling densities and the MIS weights at their
 // values for the current materials and differentiates f(y) with respect to each material's
-// baseColor and roughness (the BSDF factor of every vertex) and its emitted radiance (the Le the
-// path carries).  f(y) is the reconnection-shift evaluation of the pixel's record at its own
+// baseColor, roughness and metallic (the BSDF factor of every vertex) and its emitted radiance (the
+// Le the path carries).  f(y) is the reconnection-shift evaluation of the pixel's record at its own
 // primary hit (handleReconnectionHit / pathReconnectionShift, PathTracer.slang:1177-1397,
 // ShiftMapping.slang:430-513) without the visibility ray, which no material changes.  A per-channel
 // factor k = integrand / f(y), held fixed, makes the differentiated function equal the resolved
@@ -41,12 +41,6 @@ __device__ __forceinline__ uint32_t dev_emitter_of(const DevCtx& C, const Shadin
 __device__ __forceinline__ void adj_add(double* acc, uint32_t idx, float v)
 {
     if (v != 0.f) atomicAdd(acc + idx, (double)v);
-}
-
-// Spec-gloss materials map their parameters onto the BSDF differently (material_grad.h).
-__device__ __forceinline__ bool adj_spec_gloss(const DevCtx& C, const ShadingData& sd)
-{
-    return (C.materials[sd.materialID].flags & kMtlSpecGloss) != 0;
 }
 
 __device__ __forceinline__ bool adj_finished(const DevCtx& C, uint32_t bounces) // finished_bounces
@@ -150,7 +144,7 @@ __device__ __noinline__ bool adj_replay_suffix(const DevCtx& C, const Recon& rd,
                     {
                         if (nv == kAdjMaxFactors) return false;
                         mat[nv] = sd.materialID;
-                        V[nv++] = mi_eval_grad(sd, d, 0u, lsDir, adj_spec_gloss(C, sd));
+                        V[nv++] = mi_eval_grad(sd, d, C.materials[sd.materialID], 0u, lsDir);
                         S = thp * Lr;
                         Le = lsLi * lsPdf;
                         emitter = lsEnv ? kInvalidIndex
@@ -178,7 +172,7 @@ __device__ __noinline__ bool adj_replay_suffix(const DevCtx& C, const Recon& rd,
         else if (specOrDelta) comp = 2;
         if (!valid || (result.lobeType & kLobeDelta) || (comp != 0 && comp != 2) || nv == kAdjMaxFactors) return false;
         mat[nv] = sd.materialID;
-        V[nv++] = mi_eval_grad(sd, d, 1u << comp, result.wo, adj_spec_gloss(C, sd));
+        V[nv++] = mi_eval_grad(sd, d, C.materials[sd.materialID], 1u << comp, result.wo);
         dir = result.wo;
         thp *= result.weight;
         flags &= ~(4u | kPSpecular | kPDelta);
@@ -243,13 +237,13 @@ __device__ inline void adj_pixel(const DevCtx& C, const ResPlanes& res, const Re
             float lightPdf = rd.lightPdf / jac;
             if (rd.lightIsNEE)
             {
-                V[0] = mi_eval_grad(sd1, d1, 0u, dir, adj_spec_gloss(C, sd1));
+                V[0] = mi_eval_grad(sd1, d1, C.materials[sd1.materialID], 0u, dir);
                 if (!any_gt0(V[0].value) || totalPdf == 0.f) return;
                 s = dev_mis(C, lightPdf, totalPdf) / lightPdf;
             }
             else
             {
-                V[0] = mi_eval_grad(sd1, d1, mask1, dir, adj_spec_gloss(C, sd1));
+                V[0] = mi_eval_grad(sd1, d1, C.materials[sd1.materialID], mask1, dir);
                 if (!any_gt0(V[0].value) || lobePdf == 0.f) return;
                 s = dev_mis(C, totalPdf, lightPdf) / lobePdf;
             }
@@ -258,7 +252,7 @@ __device__ inline void adj_pixel(const DevCtx& C, const ResPlanes& res, const Re
         }
         else
         {
-            V[0] = mi_eval_grad(sd1, d1, mask1, dir, adj_spec_gloss(C, sd1));
+            V[0] = mi_eval_grad(sd1, d1, C.materials[sd1.materialID], mask1, dir);
             if (!any_gt0(V[0].value) || lobePdf == 0.f) return;
             ShadingData sd2 = dev_sd(C, rd.secondHit, dir);
             BsdfData d2 = dev_instance(C, sd2);
@@ -272,7 +266,7 @@ __device__ inline void adj_pixel(const DevCtx& C, const ResPlanes& res, const Re
                 // pathReconnectionShift's lobe-specific x2 term; the suffix follows from x3
                 if (!(lsp > 0.f)) return;
                 if (C.sgKind != kSgTinyUniform) { atomicAdd(cnt + kAdjSkipped, 1u); return; }
-                V[1] = mi_eval_grad(sd2, d2, mask2, rd.secondWo, adj_spec_gloss(C, sd2));
+                V[1] = mi_eval_grad(sd2, d2, C.materials[sd2.materialID], mask2, rd.secondWo);
                 s = (1.f / lobePdf) * (1.f / lsp);
                 f3 S;
                 if (!adj_replay_suffix(C, rd, sd2, nv, mat, V, emitter, Le, S)) { atomicAdd(cnt + kAdjSkipped, 1u); return; }
@@ -282,13 +276,13 @@ __device__ inline void adj_pixel(const DevCtx& C, const ResPlanes& res, const Re
             {
                 if (rd.lightIsNEE)
                 {
-                    V[1] = mi_eval_grad(sd2, d2, 0xFu, rd.secondWo, adj_spec_gloss(C, sd2));
+                    V[1] = mi_eval_grad(sd2, d2, C.materials[sd2.materialID], 0xFu, rd.secondWo);
                     s = (1.f / lobePdf) * (dev_mis(C, rd.lightPdf, tp) / rd.lightPdf);
                 }
                 else
                 {
                     if (!(lsp > 0.f)) return;
-                    V[1] = mi_eval_grad(sd2, d2, mask2, rd.secondWo, adj_spec_gloss(C, sd2));
+                    V[1] = mi_eval_grad(sd2, d2, C.materials[sd2.materialID], mask2, rd.secondWo);
                     s = (1.f / lobePdf) * (dev_mis(C, tp, rd.lightPdf) / lsp);
                 }
                 if (!rd.lightIsDistant)
@@ -334,9 +328,11 @@ __device__ inline void adj_pixel(const DevCtx& C, const ResPlanes& res, const Re
         f3 common = g * (before[v] * after) * Le * s;
         f3 dB = common * V[v].dBase;
         f3 dR = common * V[v].dRough;
+        f3 dM = common * V[v].dMetal;
         const uint32_t m = mat[v] * kGradStride;
         adj_add(acc, m + kGradBase + 0, dB.x); adj_add(acc, m + kGradBase + 1, dB.y); adj_add(acc, m + kGradBase + 2, dB.z);
         adj_add(acc, m + kGradRough, dR.x + dR.y + dR.z);
+        adj_add(acc, m + kGradMetal, dM.x + dM.y + dM.z);
         after = after * V[v].value;
     }
 }

@@ -23,8 +23,9 @@ def _richardson(f, x, h=1e-3):
 
 @pytest.mark.parametrize("model", ["metal_rough", "spec_gloss"])
 def test_bsdf_derivatives_match_fp64_differences(oracle_mod, model):
-    """Spec-gloss: baseColor is the diffuse albedo, the specular colour is held fixed and the
-    roughness slot holds the glossiness (roughness = 1 - slot)."""
+    """Derivatives with respect to baseColor, roughness and (metal-rough) metallic.  Spec-gloss:
+    baseColor is the diffuse albedo, the specular colour is held fixed and the roughness slot holds
+    the glossiness (roughness = 1 - slot)."""
     rng = np.random.default_rng(0)
     worst = 0.0
     for _ in range(300):
@@ -41,7 +42,7 @@ def test_bsdf_derivatives_match_fp64_differences(oracle_mod, model):
 
         wi, wo = unit(), unit()
         mask = int(rng.choice([0, 1, 4, 0xF]))
-        value, d_base, d_rough, value64 = oracle_mod.bsdf_grad(mat, wi, wo, mask, spec)
+        value, d_base, d_rough, value64, d_metal = oracle_mod.bsdf_grad(mat, wi, wo, mask, spec)
         scale = max(np.abs(value64).max(), 1e-9)
         assert np.abs(value - value64).max() <= 1e-5 * scale
 
@@ -56,6 +57,12 @@ def test_bsdf_derivatives_match_fp64_differences(oracle_mod, model):
         fd_rough = _richardson(val(3), mat[3])
         err = max(np.abs(fd_base - d_base).max() / max(np.abs(fd_base).max(), 1e-9),
                   np.abs(fd_rough - d_rough).max() / max(np.abs(fd_rough).max(), 1e-3 * scale))
+        if model == "metal_rough" and mat[4] < 1.0:
+            # metallic = 1 switches the diffuse lobe off: a one-sided point, not differenced
+            fd_metal = _richardson(val(4), mat[4])
+            err = max(err, np.abs(fd_metal - d_metal).max() / max(np.abs(fd_metal).max(), 1e-3 * scale))
+        elif model == "spec_gloss":
+            assert np.all(d_metal == 0.0)  # the derived metallic has no derivative of its own
         worst = max(worst, err)
     assert worst < GRAD_TOL, worst
 
@@ -80,7 +87,10 @@ def _replay_check(oracle_mod, scene, camera_fn, width, height, frames, props, pe
         tgt.set_env_map(env)
         ora.set_env_map(env)
     P0 = mats[:, :8].astype(np.float64)
-    params = [(m, k) for m in range(len(mats)) for k in (range(4, 7) if emissive[m] else range(4))]
+    metal_rough = (mats[:, 9].view(np.uint32) & 2) == 0  # kMtlSpecGloss clear
+    # metallic too where it is below 1 (at 1 the diffuse lobe is switched off: a one-sided point)
+    params = [(m, k) for m in range(len(mats))
+              for k in (list(range(4, 7)) if emissive[m] else list(range(4)) + ([7] if metal_rough[m] and mats[m, 7] < 1.0 else []))]
     G = np.zeros((len(mats), 8))
     FD = np.zeros((len(mats), 8))
     stats = np.zeros(4, np.uint64)
