@@ -193,3 +193,20 @@ def test_oracle_replay_gradient_spec_gloss(oracle_mod, scenes, tmp_path, bounces
     assert err < GRAD_TOL, err
     big = np.abs(FD) > 1e-2 * np.abs(FD).max()
     assert (np.abs(G - FD)[big] / np.abs(FD)[big]).max() < GRAD_TOL
+
+
+@pytest.mark.parametrize("mode", [{"temporalReuse": "GatherOnly", "gatherOption": "Robust"},
+                                  {"temporalReuse": "GatherOnly", "gatherOption": "Fast"},
+                                  {"temporalReuse": "ScatterOnly"},
+                                  {"temporalReuse": "ScatterBackup", "gatherOption": "Fast", "scatterBackupMISOption": "Pairwise"},
+                                  {"temporalReuse": "MultiScatter", "numTimePartitions": 3}],
+                         ids=["GatherOnly-Robust", "GatherOnly-Fast", "ScatterOnly", "ScatterBackup-Pairwise", "MultiScatter"])
+def test_oracle_replay_gradient_in_every_temporal_mode(oracle_mod, scenes, mode):
+    """The suffix-replay state travels with the record through every mode's shifts and copies: the
+    final reservoirs of four-vertex paths replay exactly (no value mismatch) and the gradient
+    matches FP64 differences."""
+    props = dict(mode, maxSurfaceBounces=2, enableSpatialResampling=True)
+    err, stats, G, FD, long_paths = _replay_check(oracle_mod, scenes.cornell_box(0), scenes.cornell_camera, 32, 32, 3, props)
+    assert stats[0] > 0 and stats[1] == 0 and stats[2] == 0 and stats[3] == 0
+    assert long_paths > 100
+    assert err < GRAD_TOL, err
