@@ -679,7 +679,7 @@ def run_adjoint(args, torch, rs, stream):
             "params": int(sc.info["materials"]) * 4 + int(sc.info["emitters"]) * 3,
             "fwd_ms_per_frame": round(fwd, 4), "bwd_ms_per_frame": round(bwd, 4), "bwd_over_fwd": round(bwd / fwd, 4),
             "loss": loss, "grad_norm": float(grad.norm().item()),
-            "replayed_paths": int(stats[0]), "paths_skipped": int(stats[1]), "emitter_not_found": int(stats[2]),
+            "replayed_paths": int(stats[0]), "suffixes_held_fixed": int(stats[1]), "emitter_not_found": int(stats[2]),
             "how": "fwd: rs_execute x 8 frames + rs_checkpoint (144 B/pixel) per frame; bwd: rs_backward per frame "
                    "from its checkpoint; the gradient check against FP64 central differences is in the tests"}
 

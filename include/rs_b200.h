@@ -358,8 +358,9 @@ RS_API rs_status rs_debug_stage_rays(rs_pass* pass, uint64_t* rays, uint32_t* co
  * them (rs_checkpoint_bytes = 144 bytes per pixel) and rs_backward recomputes the rest.  A path of
  * four or more vertices is re-run from its third vertex with the sample-generator state, bounce
  * counters and flags its record saved there (word 27 and bits 15-26 of word 5), which needs the
- * TinyUniform generator; paths past x2 with a delta lobe, or of more than 8 BSDF vertices, are
- * skipped and counted.  The scene may be lit by emissive triangles and an environment map, whose
+ * TinyUniform generator.  Where the suffix cannot be re-run (a delta lobe past x2, more than 8 BSDF
+ * vertices, the PCG32 generator, or geometry moved since the record was made) it is held fixed at
+ * the record's radiance, x1 and x2 are still differentiated, and the path is counted.  The scene may be lit by emissive triangles and an environment map, whose
  * radiance is held fixed (no analytic lights); ior is not differentiated.  For a spec-gloss
  * material baseColor is its diffuse colour and the roughness slot its glossiness; its specular
  * colour is held fixed and its metallic slot gets no gradient.
@@ -369,7 +370,7 @@ RS_API rs_status rs_debug_stage_rays(rs_pass* pass, uint64_t* rays, uint32_t* co
  *   rs_backward        gradMaterials[m * 8 + k] += d loss / d (baseColor.xyz, roughness, emissive.xyz, metallic)
  *                      for d loss / d colour `gradColor` (device float4 per pixel); checkpoint NULL
  *                      means the last frame; the materials must be those the frame used
- *   rs_backward_stats  read and clear {paths replayed, paths skipped, emitter not found, value mismatch} */
+ *   rs_backward_stats  read and clear {paths replayed, suffixes held fixed, emitter not found, value mismatch} */
 RS_API rs_status rs_set_materials(rs_pass* pass, const rs_material* materials, uint32_t count);
 RS_API rs_status rs_checkpoint_bytes(rs_pass* pass, size_t* bytes);
 RS_API rs_status rs_checkpoint(rs_pass* pass, void* dstDevice, void* cudaStream);

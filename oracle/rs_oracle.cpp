@@ -2197,7 +2197,9 @@ static uint32_t emitter_of(const Pass& p, const ShadingData& sd)
 // light) and sets the emitter, its radiance and the replayed suffix radiance S, which equals the
 // record's irradiance.  Emitted radiance beyond x2 that a BSDF sample reaches counts only after a
 // delta lobe (handleHit's computeEmissive), whose factor is no BSDF evaluation: such paths, delta
-// lobes on the suffix and paths of more than kReplayMaxVertices factors are not replayed.
+// lobes on the suffix and paths of more than kReplayMaxVertices factors are not replayed, and in
+// geometry that has moved since the record was made the replay differs from the record's radiance:
+// replay_pixel then holds the suffix fixed.
 static bool replay_suffix(const Pass& p, const ReconnectionData& rd, const ShadingData& sd2, Replay& out, f3& S)
 {
     PathState path;
@@ -2279,7 +2281,7 @@ static bool replay_pixel(const Pass& p, const PathReservoir& r, const Reconnecti
     if (rd.pathLength == 1 && rd.lightIsDistant) return false;
     out.L = rd.pathLength;
     out.Le = rd.irradiance;
-    bool suffixMismatch = false;
+    bool suffixHeld = false;
     ShadingData sd1 = p.loadSD(rd.firstHit, -rd.firstWi);
     if (rd.pathLength == 1)
     {
@@ -2336,13 +2338,23 @@ static bool replay_pixel(const Pass& p, const PathReservoir& r, const Reconnecti
             {
                 // pathReconnectionShift's lobe-specific x2 term; the suffix follows from x3
                 if (!(lsp > 0.f)) return false;
-                if (p.opt.sampleGenerator != kSgTinyUniform) { stats[kStatSkipped]++; return false; }
                 out.v[1] = replay_vertex(p, sd2, mask2, rd.secondWo);
                 out.s = (1.f / lobePdf) * (1.f / lsp);
                 out.nv = 2;
                 f3 S;
-                if (!replay_suffix(p, rd, sd2, out, S)) { stats[kStatSkipped]++; return false; }
-                suffixMismatch = !(S.x == rd.irradiance.x && S.y == rd.irradiance.y && S.z == rd.irradiance.z);
+                const bool replayed = p.opt.sampleGenerator == kSgTinyUniform && replay_suffix(p, rd, sd2, out, S) &&
+                                      S.x == rd.irradiance.x && S.y == rd.irradiance.y && S.z == rd.irradiance.z;
+                if (!replayed)
+                {
+                    // the suffix is held fixed at the record's radiance and only x1 and x2 are
+                    // differentiated: a delta lobe past x2, a PCG32 state, or a suffix traced in
+                    // geometry that has moved since (a record reused from an earlier frame)
+                    out.nv = 2;
+                    out.emitter = kInvalidIndex;
+                    out.Le = rd.irradiance;
+                    suffixHeld = true;
+                    stats[kStatSkipped]++;
+                }
             }
             else
             {
@@ -2383,10 +2395,9 @@ static bool replay_pixel(const Pass& p, const PathReservoir& r, const Reconnecti
                 out.value.z != 0.f ? r.integrand.z / out.value.z : 1.f);
     stats[kStatReplayed]++;
     // a path that ends at the environment map carries its radiance, no material's
-    if (out.emitter == kInvalidIndex && !rd.lightIsDistant) stats[kStatNoEmitter]++;
+    if (out.emitter == kInvalidIndex && !rd.lightIsDistant && !suffixHeld) stats[kStatNoEmitter]++;
     f3 diff = check - r.integrand;
-    if (suffixMismatch ||
-        f_abs(diff.x) + f_abs(diff.y) + f_abs(diff.z) > 1e-3f * (f_abs(r.integrand.x) + f_abs(r.integrand.y) + f_abs(r.integrand.z)))
+    if (f_abs(diff.x) + f_abs(diff.y) + f_abs(diff.z) > 1e-3f * (f_abs(r.integrand.x) + f_abs(r.integrand.y) + f_abs(r.integrand.z)))
         stats[kStatValueMismatch]++;
     return true;
 }
@@ -2753,10 +2764,10 @@ __attribute__((visibility("default"))) int ro_set_materials(ro_pass* r, const rs
 
 // Analytic path-replay gradient of the last frame: adds d loss / d material parameters (count x 8
 // doubles: baseColor.xyz, roughness, emissive.xyz, 0) given d loss / d colour (float4 per pixel).
-// stats: replayed paths, paths whose suffix is not replayed (a delta lobe or an emissive hit past
-// x2, more than kReplayMaxVertices factors, a PCG32 sample generator), paths without an identified
-// emitter, replays whose value differs from the reservoir's integrand by more than 1e-3 (or whose
-// replayed suffix radiance is not the record's).
+// stats: replayed paths, paths whose suffix is held fixed (a delta lobe or an emissive hit past x2,
+// more than kReplayMaxVertices factors, a PCG32 sample generator, geometry that moved since the
+// record was made), paths without an identified emitter, replays whose value differs from the
+// reservoir's integrand by more than 1e-3.
 __attribute__((visibility("default"))) int ro_backward(ro_pass* r, const float* gradColor, double* gradOut, uint64_t* stats)
 {
     oracle::Pass& p = r->p;

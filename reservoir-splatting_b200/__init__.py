@@ -322,7 +322,7 @@ class ReservoirSplatting:
         return dict(zip(["nodes", "depth", "internal_children", "leaf_children", "leaf_triangles", "sah_cost"], out.tolist()))
 
     def backward_stats(self) -> np.ndarray:
-        """Counters since the last read: replayed, skipped (suffix not replayable), emitter not found, value mismatch."""
+        """Counters since the last read: replayed, suffixes held fixed (not replayable), emitter not found, value mismatch."""
         out = np.zeros(4, np.uint64)
         _check(self._lib.rs_backward_stats(self._h, out.ctypes.data))
         return out

@@ -55,9 +55,10 @@ __device__ __forceinline__ bool adj_finished(const DevCtx& C, uint32_t bounces) 
 // roulette's, the light and BSDF samples'), up to the light sample that ends the path.  Appends the
 // BSDF factor of each suffix vertex (the sampled lobe's; at the last vertex all lobes' toward the
 // light) and sets the emitter, its radiance and the replayed suffix radiance S, which equals the
-// record's irradiance.  Emitted radiance beyond x2 that a BSDF sample reaches counts only after a
-// delta lobe (handle_hit's computeEmissive), whose factor is no BSDF evaluation: such paths, delta
-// lobes on the suffix and paths of more than kAdjMaxFactors factors are not replayed.  A light
+// record's irradiance when the geometry has not moved since the record was made.  Emitted radiance
+// beyond x2 that a BSDF sample reaches counts only after a delta lobe (handle_hit's computeEmissive),
+// whose factor is no BSDF evaluation: such paths, delta lobes on the suffix and paths of more than
+// kAdjMaxFactors factors are not replayed (adj_pixel then holds the suffix fixed).  A light
 // sample of the environment map leaves emitter = kInvalidIndex: its radiance is no material's.
 // The host accepts emissive triangles and an environment map here (no analytic lights).
 __device__ __noinline__ bool adj_replay_suffix(const DevCtx& C, const Recon& rd, const ShadingData& sd2, uint32_t& nv, uint32_t* mat,
@@ -206,7 +207,7 @@ __device__ inline void adj_pixel(const DevCtx& C, const ResPlanes& res, const Re
     BsdfGrad V[kAdjMaxFactors];
     float s = 1.f;
     f3 Le = rd.irradiance;
-    bool suffixMismatch = false;
+    bool suffixHeld = false;
     ShadingData sd1 = dev_sd(C, rd.firstHit, -rd.firstWi);
     if (rd.pathLength == 1)
     {
@@ -265,12 +266,22 @@ __device__ inline void adj_pixel(const DevCtx& C, const ResPlanes& res, const Re
             {
                 // pathReconnectionShift's lobe-specific x2 term; the suffix follows from x3
                 if (!(lsp > 0.f)) return;
-                if (C.sgKind != kSgTinyUniform) { atomicAdd(cnt + kAdjSkipped, 1u); return; }
                 V[1] = mi_eval_grad(sd2, d2, C.materials[sd2.materialID], mask2, rd.secondWo);
                 s = (1.f / lobePdf) * (1.f / lsp);
                 f3 S;
-                if (!adj_replay_suffix(C, rd, sd2, nv, mat, V, emitter, Le, S)) { atomicAdd(cnt + kAdjSkipped, 1u); return; }
-                suffixMismatch = !(S.x == rd.irradiance.x && S.y == rd.irradiance.y && S.z == rd.irradiance.z);
+                const bool replayed = C.sgKind == kSgTinyUniform && adj_replay_suffix(C, rd, sd2, nv, mat, V, emitter, Le, S) &&
+                                      S.x == rd.irradiance.x && S.y == rd.irradiance.y && S.z == rd.irradiance.z;
+                if (!replayed)
+                {
+                    // the suffix is held fixed at the record's radiance and only x1 and x2 are
+                    // differentiated: a delta lobe past x2, a PCG32 state, or a suffix traced in
+                    // geometry that has moved since (a record reused from an earlier frame)
+                    nv = 2;
+                    emitter = kInvalidIndex;
+                    Le = rd.irradiance;
+                    suffixHeld = true;
+                    atomicAdd(cnt + kAdjSkipped, 1u);
+                }
             }
             else
             {
@@ -306,13 +317,12 @@ __device__ inline void adj_pixel(const DevCtx& C, const ResPlanes& res, const Re
                      value.z != 0.f ? r.integrand.z / value.z : 1.f);
     atomicAdd(cnt + kAdjReplayed, 1u);
     // a path that ends at the environment map carries its radiance, no material's
-    if (emitter == kInvalidIndex && !rd.lightIsDistant) atomicAdd(cnt + kAdjNoEmitter, 1u);
-    // a suffix path's value is checked through the record's irradiance (the replayed suffix radiance
+    if (emitter == kInvalidIndex && !rd.lightIsDistant && !suffixHeld) atomicAdd(cnt + kAdjNoEmitter, 1u);
+    // a suffix path's value is checked through the record's irradiance (a replayed suffix radiance
     // equals it bit for bit); the suffix's densities and MIS weights fall into k
     const f3 check = rd.pathLength > 3 ? V[0].value * V[1].value * rd.irradiance * s : value;
     f3 diff = check - r.integrand;
-    if (suffixMismatch ||
-        f_abs(diff.x) + f_abs(diff.y) + f_abs(diff.z) > 1e-3f * (f_abs(r.integrand.x) + f_abs(r.integrand.y) + f_abs(r.integrand.z)))
+    if (f_abs(diff.x) + f_abs(diff.y) + f_abs(diff.z) > 1e-3f * (f_abs(r.integrand.x) + f_abs(r.integrand.y) + f_abs(r.integrand.z)))
         atomicAdd(cnt + kAdjValueMismatch, 1u);
 
     const f3 g = mk3(gc.x, gc.y, gc.z) * W * k;

@@ -43,7 +43,8 @@ def _richardson(f, x, h=1e-3):
 
 @pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
 @pytest.mark.parametrize("case,bounces,env", [("inverse_scene", 1, False), ("inverse_scene", 2, False), ("cornell", 2, False),
-                                              ("cornell", 3, False), ("inverse_scene", 2, True), ("cornell", 3, True)])
+                                              ("cornell", 3, False), ("inverse_scene", 2, True), ("cornell", 3, True),
+                                              ("cornell_dof", 2, False)])
 def test_backward_matches_oracle_and_fp64_differences(rs, oracle_mod, scenes, case, bounces, env):
     """With more than one bounce, paths of four and five vertices are differentiated through the
     suffix replay from x3; none is skipped, and the replayed suffix radiance is the record's.  With
@@ -58,6 +59,12 @@ def test_backward_matches_oracle_and_fp64_differences(rs, oracle_mod, scenes, ca
         gpu.set_env_map(sky)
         ora.set_env_map(sky)
     camera = scenes.translate_camera if case == "inverse_scene" else scenes.cornell_camera
+    if case == "cornell_dof":  # an open aperture: lens-vertex copies and primary-hit reconnections
+        def camera(f, w, h):
+            c = scenes.cornell_camera(f, w, h)
+            c.aperture_radius = 0.03
+            c.focal_distance = 1.6
+            return c
     rng = np.random.default_rng(2)
     n = len(mats)
     G = torch.zeros((n, 8), dtype=torch.float32, device="cuda")
@@ -143,8 +150,9 @@ def test_set_materials_renders_like_the_oracle(rs, oracle_mod, scenes):
 @pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
 def test_suffix_replay_needs_the_tiny_uniform_generator(rs, oracle_mod, scenes):
     """A record keeps 32 bits of the sample generator's state at x3: PCG32's 64-bit state cannot be
-    re-run, so with PCG32 the paths of four or more vertices are skipped and counted, by the GPU and
-    the oracle alike, and the shorter ones are still differentiated."""
+    re-run, so with PCG32 the paths of four or more vertices have their suffix held fixed at the
+    record's radiance (x1 and x2 are still differentiated) and are counted, by the GPU and the oracle
+    alike."""
     import torch
     W = H = 40
     props = dict(PROPS, maxSurfaceBounces=2, sampleGenerator="PCG32")
@@ -301,3 +309,36 @@ def test_differentiation_config_at_its_stated_size(rs, oracle_mod, scenes):
     assert stats[0] > 0 and stats[1] == 0 and stats[2] == 0
     assert np.abs(g - O).max() <= 1e-4 * np.abs(O).max()
     renderer.pass_.close()
+
+
+@pytest.mark.skipif(not _cuda_ok(), reason="no CUDA device")
+def test_backward_with_moving_geometry_matches_oracle(rs, oracle_mod, scenes):
+    """The Cornell box's two boxes slide each frame (rs_update_geometry): frames bit-exact with the
+    oracle, and each frame's gradient equals the oracle's, including the suffixes held fixed because
+    they were traced in an earlier frame's geometry (counted alike)."""
+    import torch
+    W = H = 40
+    props = dict(PROPS, maxSurfaceBounces=2)
+    sc, gpu, ora, mats = _setup(rs, oracle_mod, scenes, W, H, props, scenes.cornell_box(0))
+    base = np.array(sc.positions, np.float32).reshape(len(sc.positions), -1).copy()
+    boxes = (np.arange(len(base)) >= 10) & (np.arange(len(base)) < 34)
+    n = len(mats)
+    rng = np.random.default_rng(4)
+    for f in range(4):
+        if f > 0:
+            pos = base.copy()
+            pos[boxes, 0::3] += 0.01 * f
+            gpu.update_geometry(pos)
+            ora.update_geometry(pos)
+        cam = scenes.cornell_camera(f, W, H)
+        img = gpu.render(cam)
+        np.testing.assert_array_equal(img, ora.execute(cam), err_msg=f"frame {f}")
+        gc = rng.uniform(-1.0, 1.0, img.shape).astype(np.float32)
+        G = torch.zeros((n, 8), dtype=torch.float32, device="cuda")
+        gpu.backward(torch.from_numpy(gc).cuda().data_ptr(), G.data_ptr())
+        torch.cuda.synchronize()
+        st = gpu.backward_stats()
+        O, ost = ora.backward(gc, n)
+        assert list(st) == list(ost), (f, st, ost)
+        assert np.abs(G.cpu().numpy() - O).max() <= ORACLE_TOL * np.abs(O).max()
+    gpu.close()
