@@ -257,7 +257,23 @@ RS_API rs_status rs_set_seed(rs_pass* pass, uint32_t useFixedSeed, uint32_t fixe
 RS_API rs_status rs_freeze(rs_pass* pass, uint32_t frozen);
 /* Copies a pass buffer to host memory (synchronises the pass's last stream).
  * *bytes is the destination capacity in, and the number of bytes written (or
- * needed when dst is NULL) out. */
+ * needed when dst is NULL) out.
+ *
+ * Reservoirs (PathReservoir, Reservoir.slang:73-132): 8 words per pixel, float integrand.xyz,
+ * totalWeight, subPixel.xy, confidence, 0.
+ * Reconnection records (ReconnectionData.slang:89-166): 28 words per pixel,
+ *   0-3   float subPixel.xy, lensSample.xy        4  float time
+ *   5     flags: pathLength (bits 0-7), firstBSDFComponentType (8-9), secondBSDFComponentType
+ *         (10-11), transmissionEvent (12), lightIsNEE (13), lightIsDistant (14), and the adjoint's
+ *         suffix state on entering the third vertex (15-26: bounce counters diffuse, specular,
+ *         transmission, two bits each, then path flags 4..128 shifted down by 2)
+ *   6     float lightPdf                             7  float subPixelJacobian
+ *   8-11  firstHit (HitInfo, four words)            12-15 secondHit
+ *   16-18 float firstWi                              19 float lensVertexJacobian
+ *   20-22 float secondWo                             23 float secondaryPathJacobian
+ *   24-26 float irradiance                           27 the sample generator's state on entering
+ *                                                       the third vertex (adjoint; 0 before it)
+ * Bits 15-26 of word 5 and word 27 have no reference counterpart (its record has no such fields). */
 RS_API rs_status rs_get_buffer(rs_pass* pass, rs_buffer_id id, void* dst, size_t* bytes);
 /* Restores a reservoir / reconnection buffer from host memory (checkpoint restore). */
 RS_API rs_status rs_set_buffer(rs_pass* pass, rs_buffer_id id, const void* src, size_t bytes);
