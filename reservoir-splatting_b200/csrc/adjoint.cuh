@@ -351,9 +351,10 @@ __device__ inline void adj_pixel(const DevCtx& C, const ResPlanes& res, const Re
 // for d loss / d colour `gradColor`, over the reservoirs `res` / `rec` of one frame, into the FP64
 // accumulator `acc`.  A grid of at most a few blocks per SM walks the pixels; each block stages its
 // sums in shared memory (when they fit) and flushes them with one atomic per non-zero entry.
-// 8 blocks of 128 per SM (64 registers; the replay's per-path arrays live in the local frame either
-// way): 0.234 against 0.256 ms per 512^2 frame at path length 4 with 4 blocks at 128 registers.
-__global__ void __launch_bounds__(kAdjointThreads, 8) k_backward(uint32_t slot, ResPlanes res, RecPlanes rec, const float4* __restrict__ gradColor,
+// 10 blocks of 128 per SM (the replay's per-path arrays live in the local frame either way), the
+// grid sized to them: 0.194 ms per 512^2 frame at path length 4, against 0.233 at 8 blocks, 0.220 at
+// 12 and 0.256 at 4 blocks of 128 registers.
+__global__ void __launch_bounds__(kAdjointThreads, kAdjointBlocksPerSm) k_backward(uint32_t slot, ResPlanes res, RecPlanes rec, const float4* __restrict__ gradColor,
                                                               double* __restrict__ acc, uint32_t numMaterials,
                                                               unsigned long long* __restrict__ stats)
 {

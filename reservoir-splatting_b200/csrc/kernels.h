@@ -26,6 +26,7 @@ __global__ void k_backward(uint32_t slot, ResPlanes res, RecPlanes rec, const fl
                            unsigned long long* stats);
 __global__ void k_grad_flush(const double* acc, float* grad, uint32_t n);
 constexpr uint32_t kAdjointThreads = 128;        // k_backward block size
+constexpr uint32_t kAdjointBlocksPerSm = 10;     // k_backward's resident blocks per SM (launch bounds and grid)
 constexpr uint32_t kAdjointSharedDoubles = 6016; // k_backward stages numMaterials x 8 sums in shared memory up to this (47 KB)
 
 // Blocks of `threads` (a multiple of 64) covering a W x H image for tiled_pixel.

@@ -1377,7 +1377,7 @@ extern "C" RS_API rs_status rs_backward(rs_pass* p, const void* checkpoint, cons
     RS_CUDA(p->adjAcc.ensure(M));
     RS_CUDA(cudaMemsetAsync(p->adjAcc.p, 0, M * sizeof(double), s));
     const size_t smem = M <= kAdjointSharedDoubles ? M * sizeof(double) : 0;
-    const uint32_t blocks = (uint32_t)std::min<size_t>((N + kAdjointThreads - 1) / kAdjointThreads, 148ull * 8ull);
+    const uint32_t blocks = (uint32_t)std::min<size_t>((N + kAdjointThreads - 1) / kAdjointThreads, 148ull * kAdjointBlocksPerSm);
     k_backward<<<blocks, kAdjointThreads, smem, s>>>(p->slot, res, rec, reinterpret_cast<const float4*>(gradColor), p->adjAcc.p,
                                                      numMaterials, p->adjStats.p);
     k_grad_flush<<<(M + 255) / 256, 256, 0, s>>>(p->adjAcc.p, gradMaterials, M);
