@@ -255,3 +255,22 @@ def test_oracle_replay_gradient_with_moving_geometry(oracle_mod, scenes):
     # replay in the moved geometry does not give its radiance back, the suffix is held fixed
     assert stats[0] > 0 and stats[2] == 0 and 0 < stats[1] < stats[0] // 20, stats
     assert err < GRAD_TOL, err
+
+
+def test_suffix_fields_of_the_records(oracle_mod, scenes):
+    """The record's suffix fields (word 27 and bits 15-26 of word 5): zero for paths that end before
+    x3; for longer ones the bounce counters on entering x3 count the two scatter samples at x1 and
+    x2 (reflection lobes only in these scenes), and the generator state is the TinyUniform LCG's."""
+    props = {"temporalReuse": "ScatterBackup", "gatherOption": "Clamped", "maxSurfaceBounces": 3}
+    o = oracle_mod.OraclePass(props, 32, 32)
+    o.set_scene(scenes.cornell_box(0))
+    o.execute(scenes.cornell_camera(0, 32, 32))
+    rec = o.get_buffer("curr_reconnection").reshape(-1, 28)
+    length = rec[:, 5] & 0xff
+    state = (rec[:, 5] >> 15) & 0xfff
+    short, long_ = length <= 3, length > 3
+    assert long_.sum() > 50
+    assert np.all(state[short] == 0) and np.all(rec[short, 27] == 0)
+    diffuse, specular, transmission = state & 3, (state >> 2) & 3, (state >> 4) & 3
+    assert np.all((diffuse + specular)[long_] == 2) and np.all(transmission[long_] == 0)
+    assert np.all(rec[long_, 27] != 0)
